@@ -1,0 +1,33 @@
+"""fresco_b200: B200-native loss-and-gradient path of FReSCo.
+
+``fresco_b200.potentials`` and ``fresco_b200.optimize`` mirror the reference's
+``fresco.potentials`` and ``fresco.optimize``.  ``install_alias()`` registers
+them under the reference's import names so existing scripts run unchanged::
+
+    import fresco_b200
+    fresco_b200.install_alias()
+    from fresco.potentials import NUwU
+    from fresco.optimize import LBFGS_CPP
+"""
+from __future__ import annotations
+
+import sys
+import types
+
+from . import _lib  # noqa: F401  (loads the CUDA library; raises ImportError if missing)
+from . import optimize, potentials
+from .potentials import CombinedPotential, InversePower, NUwNU, NUwU, UwNU, UwU
+
+__all__ = ["potentials", "optimize", "install_alias", "NUwU", "UwU", "UwNU", "NUwNU", "InversePower",
+           "CombinedPotential"]
+
+
+def install_alias() -> None:
+    """Makes ``import fresco.potentials`` / ``fresco.optimize`` resolve to this package."""
+    pkg = types.ModuleType("fresco")
+    pkg.__path__ = []  # namespace-like
+    pkg.potentials = potentials
+    pkg.optimize = optimize
+    sys.modules.setdefault("fresco", pkg)
+    sys.modules.setdefault("fresco.potentials", potentials)
+    sys.modules.setdefault("fresco.optimize", optimize)

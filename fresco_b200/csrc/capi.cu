@@ -1,0 +1,388 @@
+// C-ABI entry points (include/fresco_b200.h): argument checks, exception ->
+// status translation, and the host-buffer call forms.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fresco_b200.h"
+#include "optimizer.cuh"
+#include "potential.cuh"
+
+struct fresco_potential_s {
+  fb::PotentialPtr pot;
+  cudaStream_t stream = nullptr;
+  fb::DevBuf<double> dx, dg, de;
+  int64_t cap = -1;
+};
+
+struct fresco_optimizer_s {
+  std::unique_ptr<fb::Optimizer> opt;
+  fresco_potential_s* pot = nullptr;  // borrowed; the Python layer keeps it alive
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    g_last_error.clear();
+    return f();
+  } catch (const fb::InvalidArgument& e) {
+    return fail(FRESCO_ERR_INVALID, e.what());
+  } catch (const std::invalid_argument& e) {
+    return fail(FRESCO_ERR_INVALID, e.what());
+  } catch (const std::exception& e) {
+    return fail(FRESCO_ERR_RUNTIME, e.what());
+  } catch (...) {
+    return fail(FRESCO_ERR_RUNTIME, "unknown error");
+  }
+}
+
+fresco_potential_s* wrap(fb::PotentialPtr p) {
+  auto* h = new fresco_potential_s;
+  h->pot = std::move(p);
+  FB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  return h;
+}
+
+void ensure_io(fresco_potential_s* h, int64_t n) {
+  if (h->cap >= n && h->de.p) return;
+  h->dx.alloc(std::max<int64_t>(n, 1));
+  h->dg.alloc(std::max<int64_t>(n, 1));
+  if (!h->de.p) h->de.alloc(1);
+  h->cap = n;
+}
+
+void check_n(fresco_potential_s* h, int64_t n) {
+  const int64_t want = h->pot->ndof();
+  if (n < 0) throw fb::InvalidArgument("negative coordinate count");
+  if (want >= 0 && n != want) {
+    throw fb::InvalidArgument("the coordinate array has size " + std::to_string(n) + ", the potential expects " +
+                              std::to_string(want));
+  }
+}
+
+std::vector<double> vec(const double* p, int64_t n) {
+  if (n < 0) throw fb::InvalidArgument("negative size");
+  if (n > 0 && !p) throw fb::InvalidArgument("null array");
+  return std::vector<double>(p, p + n);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fresco_last_error(void) { return g_last_error.c_str(); }
+int fresco_abi_version(void) { return 100; }
+
+int fresco_nuwu_create(const double* radii, int64_t n_points, double K, const double* sk, const double* v,
+                       int64_t n_sk, const double* L, int ndim, double eps, int precision, fresco_potential* out) {
+  return guarded([&] {
+    if (!out) throw fb::InvalidArgument("null output handle");
+    if (ndim < 1 || ndim > 3) throw std::runtime_error("Invalid dimension: " + std::to_string(ndim));
+    auto p = fb::make_nuwu(vec(radii, n_points), K, vec(sk, n_sk), vec(v, n_sk), vec(L, ndim), eps, precision);
+    *out = wrap(p);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_uwu_create(const int* grid, int ndim, double K, const double* sk, const double* v, int64_t n_sk,
+                      const double* L, double eps, int precision, fresco_potential* out) {
+  return guarded([&] {
+    if (!out || !grid) throw fb::InvalidArgument("null argument");
+    std::vector<int> g(grid, grid + ndim);
+    auto p = fb::make_uwu(g, K, vec(sk, n_sk), vec(v, n_sk), vec(L, ndim), eps, precision);
+    *out = wrap(p);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_uwnu_create(const int* grid, int ndim, const double* kpts, int64_t n_k, const double* sk,
+                       const double* v, const double* L, double eps, int precision, fresco_potential* out) {
+  return guarded([&] {
+    if (!out || !grid) throw fb::InvalidArgument("null argument");
+    std::vector<int> g(grid, grid + ndim);
+    auto p = fb::make_uwnu(g, vec(kpts, n_k * ndim), vec(sk, n_k), vec(v, n_k), vec(L, ndim), eps, precision);
+    *out = wrap(p);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_nuwnu_create(const double* radii, int64_t n_points, const double* kpts, int64_t n_k, const double* sk,
+                        const double* v, const double* L, int ndim, double eps, int precision,
+                        fresco_potential* out) {
+  return guarded([&] {
+    if (!out) throw fb::InvalidArgument("null output handle");
+    auto p = fb::make_nuwnu(vec(radii, n_points), vec(kpts, n_k * ndim), vec(sk, n_k), vec(v, n_k), vec(L, ndim),
+                            eps, precision);
+    *out = wrap(p);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_inversepower_create(double a, double eps, const double* radii, int64_t n_points, const double* boxv,
+                               int ndim, int periodic, int use_cell_lists, double ncellx_scale,
+                               fresco_potential* out) {
+  return guarded([&] {
+    if (!out) throw fb::InvalidArgument("null output handle");
+    auto p = fb::make_inversepower(a, eps, vec(radii, n_points), vec(boxv, ndim), periodic != 0,
+                                   use_cell_lists != 0, ncellx_scale);
+    *out = wrap(p);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_combined_create(fresco_potential* out) {
+  return guarded([&] {
+    if (!out) throw fb::InvalidArgument("null output handle");
+    *out = wrap(std::make_shared<fb::CombinedPotential>());
+    return FRESCO_OK;
+  });
+}
+
+int fresco_combined_add(fresco_potential combined, fresco_potential part) {
+  return guarded([&] {
+    if (!combined || !part) throw fb::InvalidArgument("null handle");
+    auto* c = dynamic_cast<fb::CombinedPotential*>(combined->pot.get());
+    if (!c) throw fb::InvalidArgument("not a CombinedPotential");
+    c->add(part->pot);
+    return FRESCO_OK;
+  });
+}
+
+void fresco_potential_destroy(fresco_potential p) {
+  if (!p) return;
+  if (p->stream) {
+    cudaStreamSynchronize(p->stream);
+    cudaStreamDestroy(p->stream);
+  }
+  delete p;
+}
+
+int64_t fresco_potential_ndof(fresco_potential p) { return p ? p->pot->ndof() : -1; }
+
+int fresco_potential_energy(fresco_potential p, const double* x, int64_t n, double* energy) {
+  return guarded([&] {
+    if (!p || !energy || (n > 0 && !x)) throw fb::InvalidArgument("null argument");
+    check_n(p, n);
+    ensure_io(p, n);
+    FB_CUDA(cudaMemcpyAsync(p->dx.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, p->stream));
+    p->pot->energy(p->dx.p, n, p->de.p, false, p->stream);
+    p->pot->timer_collect();
+    FB_CUDA(cudaMemcpyAsync(energy, p->de.p, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    FB_CUDA(cudaStreamSynchronize(p->stream));
+    return FRESCO_OK;
+  });
+}
+
+int fresco_potential_energy_gradient(fresco_potential p, const double* x, int64_t n, double* grad,
+                                     double* energy) {
+  return guarded([&] {
+    if (!p || !energy || (n > 0 && (!x || !grad))) throw fb::InvalidArgument("null argument");
+    check_n(p, n);
+    ensure_io(p, n);
+    FB_CUDA(cudaMemcpyAsync(p->dx.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, p->stream));
+    p->pot->energy_gradient(p->dx.p, n, p->dg.p, p->de.p, false, p->stream);
+    p->pot->timer_collect();
+    FB_CUDA(cudaMemcpyAsync(grad, p->dg.p, sizeof(double) * n, cudaMemcpyDeviceToHost, p->stream));
+    FB_CUDA(cudaMemcpyAsync(energy, p->de.p, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    FB_CUDA(cudaStreamSynchronize(p->stream));
+    return FRESCO_OK;
+  });
+}
+
+int fresco_potential_energy_device(fresco_potential p, const double* d_x, int64_t n, double* d_energy,
+                                   int accumulate, void* stream) {
+  return guarded([&] {
+    if (!p || !d_energy || (n > 0 && !d_x)) throw fb::InvalidArgument("null argument");
+    check_n(p, n);
+    p->pot->energy(d_x, n, d_energy, accumulate != 0, static_cast<cudaStream_t>(stream));
+    return FRESCO_OK;
+  });
+}
+
+int fresco_potential_energy_gradient_device(fresco_potential p, const double* d_x, int64_t n, double* d_grad,
+                                            double* d_energy, int accumulate, void* stream) {
+  return guarded([&] {
+    if (!p || !d_energy || (n > 0 && (!d_x || !d_grad))) throw fb::InvalidArgument("null argument");
+    check_n(p, n);
+    p->pot->energy_gradient(d_x, n, d_grad, d_energy, accumulate != 0, static_cast<cudaStream_t>(stream));
+    return FRESCO_OK;
+  });
+}
+
+int fresco_potential_status(fresco_potential p, void* stream, int* status) {
+  return guarded([&] {
+    if (!p || !status) throw fb::InvalidArgument("null argument");
+    *status = p->pot->read_and_clear_status(stream ? static_cast<cudaStream_t>(stream) : p->stream);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_potential_set_timing(fresco_potential p, int enabled) {
+  return guarded([&] {
+    if (!p) throw fb::InvalidArgument("null handle");
+    p->pot->timer.enabled = enabled != 0;
+    auto& t = p->pot->timer;
+    std::fill(t.total_ms.begin(), t.total_ms.end(), 0.0);
+    std::fill(t.count.begin(), t.count.end(), 0);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_potential_get_timing(fresco_potential p, int max_stages, char* names, int names_len, double* total_ms,
+                                int* counts, int* n_stages) {
+  return guarded([&] {
+    if (!p || !n_stages) throw fb::InvalidArgument("null argument");
+    p->pot->timer_collect();
+    auto& t = p->pot->timer;
+    int k = 0, pos = 0;
+    for (size_t i = 1; i < t.names.size() && k < max_stages; ++i, ++k) {
+      if (names) {
+        const std::string& s = t.names[i];
+        if (pos + int(s.size()) + 1 <= names_len) {
+          std::memcpy(names + pos, s.c_str(), s.size() + 1);
+          pos += int(s.size()) + 1;
+        }
+      }
+      if (total_ms) total_ms[k] = t.total_ms[i];
+      if (counts) counts[k] = t.count[i];
+    }
+    *n_stages = k;
+    return FRESCO_OK;
+  });
+}
+
+int fresco_potential_describe(fresco_potential p, char* buf, int buf_len) {
+  return guarded([&] {
+    if (!p || !buf || buf_len <= 0) throw fb::InvalidArgument("null argument");
+    std::string s = p->pot->describe();
+    std::strncpy(buf, s.c_str(), size_t(buf_len - 1));
+    buf[buf_len - 1] = 0;
+    return FRESCO_OK;
+  });
+}
+
+// ---- optimisers ----------------------------------------------------------
+
+int fresco_lbfgs_create(fresco_potential p, const double* x0, int64_t n, double tol, int M, double maxstep,
+                        double max_f_rise, double H0, int rel_energy, int nsteps, int iprint, int verbosity,
+                        fresco_optimizer* out) {
+  return guarded([&] {
+    if (!p || !out || (n > 0 && !x0)) throw fb::InvalidArgument("null argument");
+    check_n(p, n);
+    fb::LbfgsParams prm;
+    prm.tol = tol;
+    prm.M = M;
+    prm.maxstep = maxstep;
+    prm.max_f_rise = max_f_rise;
+    prm.H0 = H0;
+    prm.rel_energy = rel_energy != 0;
+    prm.maxiter = nsteps;
+    prm.iprint = iprint;
+    prm.verbosity = verbosity;
+    auto* h = new fresco_optimizer_s;
+    h->pot = p;
+    h->opt = fb::make_lbfgs(p->pot, x0, n, prm);
+    *out = h;
+    return FRESCO_OK;
+  });
+}
+
+int fresco_fire_create(fresco_potential p, const double* x0, int64_t n, double dtstart, double dtmax,
+                       double maxstep, int Nmin, double finc, double fdec, double fa, double astart, double tol,
+                       int stepback, int nsteps, int iprint, int verbosity, fresco_optimizer* out) {
+  return guarded([&] {
+    if (!p || !out || (n > 0 && !x0)) throw fb::InvalidArgument("null argument");
+    check_n(p, n);
+    fb::FireParams prm;
+    prm.dtstart = dtstart;
+    prm.dtmax = dtmax;
+    prm.maxstep = maxstep;
+    prm.Nmin = Nmin;
+    prm.finc = finc;
+    prm.fdec = fdec;
+    prm.fa = fa;
+    prm.astart = astart;
+    prm.tol = tol;
+    prm.stepback = stepback != 0;
+    prm.maxiter = nsteps;
+    prm.iprint = iprint;
+    prm.verbosity = verbosity;
+    auto* h = new fresco_optimizer_s;
+    h->pot = p;
+    h->opt = fb::make_fire(p->pot, x0, n, prm);
+    *out = h;
+    return FRESCO_OK;
+  });
+}
+
+int fresco_optimizer_set_func_gradient(fresco_optimizer o, double f, const double* grad, int64_t n) {
+  return guarded([&] {
+    if (!o || (n > 0 && !grad)) throw fb::InvalidArgument("null argument");
+    o->opt->set_func_gradient(f, grad, n);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_optimizer_run(fresco_optimizer o, int niter) {
+  return guarded([&] {
+    if (!o) throw fb::InvalidArgument("null handle");
+    if (niter < 0) o->opt->run();
+    else o->opt->run(niter);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_optimizer_one_iteration(fresco_optimizer o) {
+  return guarded([&] {
+    if (!o) throw fb::InvalidArgument("null handle");
+    o->opt->one_iteration();
+    return FRESCO_OK;
+  });
+}
+
+int fresco_optimizer_reset(fresco_optimizer o, const double* x0, int64_t n) {
+  return guarded([&] {
+    if (!o || (n > 0 && !x0)) throw fb::InvalidArgument("null argument");
+    o->opt->reset(x0, n);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_optimizer_stop_criterion_satisfied(fresco_optimizer o, int* out) {
+  return guarded([&] {
+    if (!o || !out) throw fb::InvalidArgument("null argument");
+    *out = o->opt->stop_criterion_satisfied() ? 1 : 0;
+    return FRESCO_OK;
+  });
+}
+
+int fresco_optimizer_get_state(fresco_optimizer o, double* x, double* g, double* f, double* rms, int* nfev,
+                               int* niter, int* maxiter, double* H0) {
+  return guarded([&] {
+    if (!o) throw fb::InvalidArgument("null handle");
+    o->opt->get_state(x, g, f, rms, nfev, niter, maxiter, H0);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_optimizer_device_state(fresco_optimizer o, double** d_x, double** d_g) {
+  return guarded([&] {
+    if (!o) throw fb::InvalidArgument("null handle");
+    if (d_x) *d_x = o->opt->device_x();
+    if (d_g) *d_g = o->opt->device_g();
+    return FRESCO_OK;
+  });
+}
+
+void fresco_optimizer_destroy(fresco_optimizer o) { delete o; }
+
+}  // extern "C"

@@ -1,0 +1,132 @@
+// Shared helpers for the fresco_b200 CUDA library: error handling, status
+// words, reductions and small device math.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+namespace fb {
+
+// Error classes thrown inside the library and turned into C status codes at
+// the C-ABI boundary (capi.cu).  They mirror the reference's exception types:
+// std::invalid_argument -> ValueError and std::runtime_error -> RuntimeError
+// in the Cython layer (fresco/potentials/nuwu.pxd:9-11).
+struct InvalidArgument : std::invalid_argument {
+  using std::invalid_argument::invalid_argument;
+};
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+inline void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
+  if (e != cudaSuccess) {
+    throw CudaError(std::string(what) + " failed: " + cudaGetErrorString(e) + " at " + file + ":" +
+                    std::to_string(line));
+  }
+}
+inline void cufft_check(cufftResult r, const char* what, const char* file, int line) {
+  if (r != CUFFT_SUCCESS) {
+    throw CudaError(std::string(what) + " failed with cufftResult " + std::to_string(int(r)) + " at " +
+                    file + ":" + std::to_string(line));
+  }
+}
+#define FB_CUDA(x) ::fb::cuda_check((x), #x, __FILE__, __LINE__)
+#define FB_CUFFT(x) ::fb::cufft_check((x), #x, __FILE__, __LINE__)
+#define FB_LAUNCH_CHECK() ::fb::cuda_check(cudaPeekAtLastError(), "kernel launch", __FILE__, __LINE__)
+
+// Sticky status bits a kernel can raise; read back by the host after a call.
+enum StatusBits : int {
+  STATUS_NONFINITE_INPUT = 1,  // a coordinate was NaN or +-inf
+  STATUS_OVERFLOW = 2,         // a bounded buffer was too small (kernel skipped the excess)
+};
+
+// RAII device buffer (cudaMalloc'ed once at set-up, never on the evaluation path).
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t count) { alloc(count); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) FB_CUDA(cudaMalloc(&p, count * sizeof(T)));
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+template <typename T> struct Complex;
+template <> struct Complex<float> { using type = float2; };
+template <> struct Complex<double> { using type = double2; };
+template <typename T> using cplx_t = typename Complex<T>::type;
+
+__host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Warp + block reduction of a double, then one atomicAdd per block.
+__device__ inline double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Adds the block-wide sum of v into *out (one atomic per block).  Every
+// thread of the block must call it.
+__device__ inline void block_sum_atomic(double v, double* out) {
+  __shared__ double red[32];
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    double s = lane < nw ? red[lane] : 0.0;
+    s = warp_sum(s);
+    if (lane == 0 && s != 0.0) atomicAdd(out, s);
+  }
+  __syncthreads();
+}
+
+// Same, for several accumulators at once (k <= 4).
+template <int K>
+__device__ inline void block_sum_atomic_k(double (&v)[K], double* out) {
+  __shared__ double red[K][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    double s = warp_sum(v[i]);
+    if (lane == 0) red[i][wid] = s;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      double s = lane < nw ? red[i][lane] : 0.0;
+      s = warp_sum(s);
+      if (lane == 0) atomicAdd(out + i, s);
+    }
+  }
+  __syncthreads();
+}
+
+// Number of SMs of the current device (cached per process for device 0..15).
+int sm_count();
+
+}  // namespace fb

@@ -1,0 +1,6 @@
+// FP64 instantiation of the NUFFT building blocks.
+#include "nufft_kernels.cuh"
+
+namespace fb {
+FB_INSTANTIATE_NUFFT(double)
+}  // namespace fb

@@ -1,0 +1,346 @@
+// NUwU: structure-factor loss of a point pattern on a uniform k-grid and its
+// gradient with respect to the points (source/fresco/nuwu.hpp:17-318).
+//
+// Per evaluation (get_energy_gradient, nuwu.hpp:210-317):
+//   1. bin-sort the points by fine-grid tile (replaces finufft_setpts x2,
+//      nuwu.hpp:256-257: one sort serves both transforms);
+//   2. spread the real weights c_j with the ES kernel (type 1, iflag +1,
+//      nuwu.hpp:50,258) and R2C-transform the real fine grid (cuFFT);
+//   3. one pass over the active modes (V(k) != 0 or V(-k) != 0): deconvolve,
+//      S = |rho|^2/N, d = (S - S0)/S0', phi += V d^2 (FP64), and the packed
+//      type-2 field (nuwu.hpp:260-287);
+//   4. C2C-transform the packed field (iflag -1, nuwu.hpp:51,291-309);
+//   5. interpolate at the points and write grad = c_j * Re(...) (nuwu.hpp:294-315).
+//
+// Packing.  The reference computes grad[d*j+a] = Re(conj(c_j) T2(f_a)(x_j))
+// with f_a(k) = -i k_a F(k), F = (4/N) V d rho / S0'.  For real c (always the
+// case, nuwu.hpp:125-149) Re T2(f) = T2(f^H) with the Hermitian part
+// f^H(k) = (f(k) + conj f(-k))/2, so T2 of h = f_x^H + i f_y^H returns the x
+// and y components as its real and imaginary parts: one FFT and one
+// interpolation pass serve two dimensions.  f_a^H = -i k_a F^H with
+// F^H(k) = (2/N) rho(k) [A(k) q - B(k)], q = |rho|^2/N, where A and B fold
+// V and S0 at k and -k (precomputed per mode at set-up).
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "nufft.cuh"
+#include "potential.cuh"
+
+namespace fb {
+
+namespace {
+
+struct ModeCoef {
+  double A, B, w2, s0;  // A, B as above; w2 = V/S0'^2, s0 = S0 (phi = w2 (q - s0)^2)
+};
+
+template <int D, typename T>
+__global__ void __launch_bounds__(256) nuwu_modes_kernel(
+    int n, int K, double invN, const int* __restrict__ mode_idx, const ModeCoef* __restrict__ coef, int n_active,
+    const cplx_t<T>* __restrict__ bhat, int nh0, Geom g, const double* __restrict__ corr0, const double* __restrict__ corr1,
+    const double* __restrict__ corr2, cplx_t<T>* hgrid, int64_t G, double* energy, const int* __restrict__ status,
+    int want_grad) {
+  double phi = 0.0;
+  const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_active; i += gridDim.x * blockDim.x) {
+    const int m = mode_idx[i];
+    const int kx = m % n - K;
+    const int ky = (D >= 2) ? (m / n) % n - K : 0;
+    const int kz = (D >= 3) ? m / (n * n) - K : 0;
+    double p = corr0[kx + K];
+    if (D >= 2) p *= corr1[ky + K];
+    if (D >= 3) p *= corr2[kz + K];
+    // R2C output holds k_x >= 0; rho(k) = conj(B(k)) for k_x >= 0 (iflag +1
+    // from a sign -1 transform) and rho(k) = B(-k) otherwise.
+    int64_t bi;
+    bool cj;
+    if (kx >= 0) {
+      const int yy = ky < 0 ? ky + nf1 : ky;
+      const int zz = kz < 0 ? kz + nf2 : kz;
+      bi = kx + int64_t(nh0) * (yy + int64_t(nf1) * zz);
+      cj = true;
+    } else {
+      const int yy = ky > 0 ? nf1 - ky : -ky;
+      const int zz = kz > 0 ? nf2 - kz : -kz;
+      bi = -kx + int64_t(nh0) * (yy + int64_t(nf1) * zz);
+      cj = false;
+    }
+    const cplx_t<T> b = bhat[bi];
+    const double rr = double(b.x) / p;
+    const double ri = (cj ? -double(b.y) : double(b.y)) / p;
+    const double q = (rr * rr + ri * ri) * invN;
+    const ModeCoef c = coef[i];
+    const double dq = q - c.s0;
+    phi += c.w2 * dq * dq;
+    if (want_grad) {
+      const double a = (c.A * q - c.B) * (2.0 * invN) / p;  // includes the type-2 pre-correction 1/p
+      const double fr = rr * a, fi = ri * a;                 // F^H / p
+      const int x0 = kx < 0 ? kx + nf0 : kx;
+      const int y0 = ky < 0 ? ky + nf1 : ky;
+      const int z0 = kz < 0 ? kz + nf2 : kz;
+      const int64_t hi = x0 + int64_t(nf0) * (y0 + int64_t(nf1) * z0);
+      cplx_t<T> h;
+      if (D == 1) {
+        // -i kx F
+        h.x = T(fi * kx);
+        h.y = T(-fr * kx);
+      } else {
+        // F (ky - i kx)
+        h.x = T(fr * ky + fi * kx);
+        h.y = T(fi * ky - fr * kx);
+      }
+      hgrid[hi] = h;
+      if (D == 3) {
+        cplx_t<T> h2;
+        h2.x = T(fi * kz);
+        h2.y = T(-fr * kz);
+        hgrid[G + hi] = h2;
+      }
+    }
+  }
+  block_sum_atomic(phi, energy);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && status != nullptr && ((*status) & STATUS_NONFINITE_INPUT)) {
+    atomicAdd(energy, __longlong_as_double(0x7ff8000000000000ULL));
+  }
+}
+
+template <int D, typename T>
+class NUwUImpl final : public Potential {
+ public:
+  NUwUImpl(const std::vector<double>& radii, double K, const std::vector<double>& sk, const std::vector<double>& v,
+           const std::vector<double>& L, double eps)
+      : N_(int64_t(radii.size())), Karg_(K) {
+    init_status();
+    if (sk.size() != v.size()) throw InvalidArgument("len(Sk) must equal len(V)");
+    if (int(L.size()) != D) throw InvalidArgument("len(L) must equal the dimension");
+    for (int a = 0; a < D; ++a) L_[a] = L[a];
+    // nuwu.hpp:54-79: K_ = int((sqrt(len V) - 1) / 2) (cbrt in 3D)
+    const double vs = double(v.size());
+    size_t kk;
+    if (D == 1) kk = size_t((v.size() - 1) / 2);
+    else if (D == 2) kk = size_t((std::sqrt(vs) - 1) / 2);
+    else kk = size_t((std::cbrt(vs) - 1) / 2);
+    K_ = int(kk);
+    n_ = 2 * K_ + 1;
+    int64_t nm = 1;
+    for (int a = 0; a < D; ++a) nm *= n_;
+    if (nm > int64_t(v.size())) throw InvalidArgument("V too short for its mode grid");
+    nmodes_ = nm;
+
+    // weights, nuwu.hpp:125-149 (area factor applied once per dimension)
+    std::vector<double> c(radii.size(), 1.0);
+    double sum = 0.0;
+    for (size_t i = 0; i < c.size(); ++i) {
+      for (int j = 0; j < D; ++j) {
+        if (D == 2) c[i] = c[i] * M_PI * radii[i] * radii[i];
+        else if (D == 3) c[i] = c[i] * M_PI * radii[i] * radii[i] * radii[i] * 4.0 / 3.0;
+      }
+      sum += c[i];
+    }
+    bool uniform = true;
+    for (size_t i = 0; i < c.size(); ++i) {
+      c[i] *= double(c.size()) / sum;
+      if (c[i] != c[0]) uniform = false;
+    }
+    if (uniform && !c.empty()) {
+      uniform_c_ = c[0];
+    } else if (!c.empty()) {
+      cw_.alloc(c.size());
+      FB_CUDA(cudaMemcpy(cw_.p, c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice));
+    }
+
+    // ES kernel and fine grid
+    es_ = es_params(eps, sizeof(T) == 4 ? 10 : 16);
+    int64_t nf[3] = {1, 1, 1};
+    for (int a = 0; a < D; ++a) nf[a] = fine_grid_size(n_, es_.w);
+    int tile[3];
+    if (D == 1) { tile[0] = 1024; tile[1] = tile[2] = 1; }
+    else if (D == 2) { tile[0] = 32; tile[1] = 32; tile[2] = 1; }
+    else if (sizeof(T) == 4) { tile[0] = 16; tile[1] = 16; tile[2] = 8; }
+    else { tile[0] = 8; tile[1] = 8; tile[2] = 8; }
+    geom_ = make_geom(D, nf, es_.w, tile);
+    alloc_sort(sort_, N_, geom_);
+    pts_.alloc(std::max<int64_t>(N_, 1), D);
+
+    const int64_t G = geom_.G();
+    nh0_ = geom_.nf[0] / 2 + 1;
+    const int64_t GH = int64_t(nh0_) * geom_.nf[1] * geom_.nf[2];
+    spread_grid_.alloc(G);
+    bhat_.alloc(GH);
+    nfields_ = (D == 3) ? 2 : 1;
+    hgrid_.alloc(G * nfields_);
+    ggrid_.alloc(G * nfields_);
+    FB_CUDA(cudaMemset(hgrid_.p, 0, hgrid_.bytes()));
+
+    // correction factors per dimension, k = -K..K
+    for (int a = 0; a < D; ++a) {
+      std::vector<double> pc = es_correction(es_, geom_.nf[a], -K_, n_);
+      corr_[a].alloc(n_);
+      FB_CUDA(cudaMemcpy(corr_[a].p, pc.data(), sizeof(double) * n_, cudaMemcpyHostToDevice));
+    }
+
+    // active modes and their coefficients
+    std::vector<int> idx;
+    std::vector<ModeCoef> coef;
+    auto mirror = [&](int64_t m) {
+      int64_t r = m, out = 0, stride = 1;
+      for (int a = 0; a < D; ++a) {
+        const int64_t ia = r % n_;
+        r /= n_;
+        out += (n_ - 1 - ia) * stride;
+        stride *= n_;
+      }
+      return out;
+    };
+    for (int64_t m = 0; m < nm; ++m) {
+      const int64_t mm = mirror(m);
+      const double vk = v[m], vm = v[mm];
+      if (vk == 0.0 && vm == 0.0) continue;
+      const double s0k = sk[m], s0m = sk[mm];
+      const double dk = s0k != 0.0 ? s0k : 1.0, dm = s0m != 0.0 ? s0m : 1.0;
+      ModeCoef cc;
+      cc.A = vk / (dk * dk) + vm / (dm * dm);
+      cc.B = vk * s0k / (dk * dk) + vm * s0m / (dm * dm);
+      cc.w2 = vk / (dk * dk);
+      cc.s0 = s0k;
+      idx.push_back(int(m));
+      coef.push_back(cc);
+    }
+    n_active_ = int(idx.size());
+    if (n_active_) {
+      mode_idx_.alloc(n_active_);
+      coef_.alloc(n_active_);
+      FB_CUDA(cudaMemcpy(mode_idx_.p, idx.data(), sizeof(int) * n_active_, cudaMemcpyHostToDevice));
+      FB_CUDA(cudaMemcpy(coef_.p, coef.data(), sizeof(ModeCoef) * n_active_, cudaMemcpyHostToDevice));
+    }
+
+    // cuFFT plans (dims slowest first)
+    int dims[3];
+    for (int a = 0; a < D; ++a) dims[a] = geom_.nf[D - 1 - a];
+    const bool f32 = sizeof(T) == 4;
+    FB_CUFFT(cufftPlanMany(&plan_r2c_, D, dims, nullptr, 1, 0, nullptr, 1, 0, f32 ? CUFFT_R2C : CUFFT_D2Z, 1));
+    FB_CUFFT(cufftPlanMany(&plan_c2c_, D, dims, nullptr, 1, int(G), nullptr, 1, int(G),
+                           f32 ? CUFFT_C2C : CUFFT_Z2Z, nfields_));
+    FB_CUDA(cudaDeviceSynchronize());
+  }
+
+  ~NUwUImpl() override {
+    if (plan_r2c_) cufftDestroy(plan_r2c_);
+    if (plan_c2c_) cufftDestroy(plan_c2c_);
+  }
+
+  int64_t ndof() const override { return N_ * D; }
+  std::string kind() const override { return "NUwU"; }
+
+  void energy(const double* x, int64_t n, double* e, bool acc, cudaStream_t s) override {
+    run(x, nullptr, e, acc, s);
+  }
+  void energy_gradient(const double* x, int64_t n, double* g, double* e, bool acc, cudaStream_t s) override {
+    run(x, g, e, acc, s);
+  }
+
+  std::string describe() const override {
+    std::string s = "NUwU D=" + std::to_string(D) + " precision=" + (sizeof(T) == 4 ? "fp32" : "fp64") +
+                    " N=" + std::to_string(N_) + " modes/dim=" + std::to_string(n_) + " w=" + std::to_string(es_.w) +
+                    " beta=" + std::to_string(es_.beta) + " nf=";
+    for (int a = 0; a < D; ++a) s += (a ? "x" : "") + std::to_string(geom_.nf[a]);
+    s += " tile=";
+    for (int a = 0; a < D; ++a) s += (a ? "x" : "") + std::to_string(geom_.tile[a]);
+    s += " bins=" + std::to_string(geom_.nbins()) + " active_modes=" + std::to_string(n_active_);
+    return s;
+  }
+
+  const Geom& geom() const { return geom_; }
+  const ESParams& es() const { return es_; }
+  int n_active() const { return n_active_; }
+
+ private:
+  void run(const double* x, double* g, double* e, bool acc, cudaStream_t s) {
+    timer_begin(s);
+    if (!acc) FB_CUDA(cudaMemsetAsync(e, 0, sizeof(double), s));
+    MapParams mp;
+    mp.kind = 0;
+    mp.stride = D;
+    for (int a = 0; a < D; ++a) mp.L[a] = L_[a];
+    bin_sort<T>(x, N_, mp, geom_, cw_.p, uniform_c_, sort_, pts_, status_.p, s);
+    timer_mark("sort", s);
+    FB_CUDA(cudaMemsetAsync(spread_grid_.p, 0, spread_grid_.bytes(), s));
+    spread_real<T>(pts_.view(), sort_, geom_, es_.beta, spread_grid_.p, s);
+    timer_mark("spread", s);
+    FB_CUFFT(cufftSetStream(plan_r2c_, s));
+    if (sizeof(T) == 4) {
+      FB_CUFFT(cufftExecR2C(plan_r2c_, reinterpret_cast<cufftReal*>(spread_grid_.p),
+                            reinterpret_cast<cufftComplex*>(bhat_.p)));
+    } else {
+      FB_CUFFT(cufftExecD2Z(plan_r2c_, reinterpret_cast<cufftDoubleReal*>(spread_grid_.p),
+                            reinterpret_cast<cufftDoubleComplex*>(bhat_.p)));
+    }
+    timer_mark("fft_type1", s);
+    if (n_active_ > 0) {
+      const int grid = int(std::min<int64_t>(ceil_div(n_active_, 256), int64_t(sm_count()) * 8));
+      nuwu_modes_kernel<D, T><<<grid, 256, 0, s>>>(
+          n_, K_, 1.0 / double(N_), mode_idx_.p, coef_.p, n_active_, bhat_.p, nh0_, geom_, corr_[0].p,
+          D >= 2 ? corr_[1].p : corr_[0].p, D >= 3 ? corr_[2].p : corr_[0].p, hgrid_.p, geom_.G(), e, status_.p,
+          g != nullptr);
+      FB_LAUNCH_CHECK();
+    } else {
+      nuwu_modes_kernel<D, T><<<1, 32, 0, s>>>(n_, K_, 1.0, mode_idx_.p, coef_.p, 0, bhat_.p, nh0_, geom_,
+                                               corr_[0].p, corr_[0].p, corr_[0].p, hgrid_.p, geom_.G(), e,
+                                               status_.p, 0);
+      FB_LAUNCH_CHECK();
+    }
+    timer_mark("modes", s);
+    if (!g) return;
+    FB_CUFFT(cufftSetStream(plan_c2c_, s));
+    if (sizeof(T) == 4) {
+      FB_CUFFT(cufftExecC2C(plan_c2c_, reinterpret_cast<cufftComplex*>(hgrid_.p),
+                            reinterpret_cast<cufftComplex*>(ggrid_.p), CUFFT_FORWARD));
+    } else {
+      FB_CUFFT(cufftExecZ2Z(plan_c2c_, reinterpret_cast<cufftDoubleComplex*>(hgrid_.p),
+                            reinterpret_cast<cufftDoubleComplex*>(ggrid_.p), CUFFT_FORWARD));
+    }
+    timer_mark("fft_type2", s);
+    interp<T>(pts_.view(), N_, geom_, es_.beta, ggrid_.p, nfields_, INTERP_GRAD, g, nullptr, acc ? 1 : 0,
+              status_.p, s);
+    timer_mark("interp", s);
+  }
+
+  int64_t N_;
+  double Karg_;
+  double L_[3] = {1, 1, 1};
+  int K_ = 0, n_ = 1;
+  int64_t nmodes_ = 1;
+  double uniform_c_ = 1.0;
+  DevBuf<double> cw_;
+  ESParams es_;
+  Geom geom_;
+  SortBufs sort_;
+  SortedStore<T> pts_;
+  int nh0_ = 1;
+  int nfields_ = 1;
+  DevBuf<T> spread_grid_;
+  DevBuf<cplx_t<T>> bhat_, hgrid_, ggrid_;
+  DevBuf<double> corr_[3];
+  DevBuf<int> mode_idx_;
+  DevBuf<ModeCoef> coef_;
+  int n_active_ = 0;
+  cufftHandle plan_r2c_ = 0, plan_c2c_ = 0;
+};
+
+}  // namespace
+
+PotentialPtr make_nuwu(const std::vector<double>& radii, double K, const std::vector<double>& sk,
+                       const std::vector<double>& v, const std::vector<double>& L, double eps, int precision) {
+  const int D = int(L.size());
+  const bool f32 = precision == 1;
+  if (D == 1) return f32 ? PotentialPtr(new NUwUImpl<1, float>(radii, K, sk, v, L, eps))
+                         : PotentialPtr(new NUwUImpl<1, double>(radii, K, sk, v, L, eps));
+  if (D == 2) return f32 ? PotentialPtr(new NUwUImpl<2, float>(radii, K, sk, v, L, eps))
+                         : PotentialPtr(new NUwUImpl<2, double>(radii, K, sk, v, L, eps));
+  if (D == 3) return f32 ? PotentialPtr(new NUwUImpl<3, float>(radii, K, sk, v, L, eps))
+                         : PotentialPtr(new NUwUImpl<3, double>(radii, K, sk, v, L, eps));
+  throw std::runtime_error("Invalid dimension: " + std::to_string(D));
+}
+
+}  // namespace fb

@@ -1,0 +1,726 @@
+// Device-resident LBFGS and modified FIRE (see optimizer.cuh).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "optimizer.cuh"
+
+namespace fb {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// Sum of P block partials, the same value on every thread (fixed order).
+__device__ double sum_parts(const double* __restrict__ part, int P) {
+  __shared__ double sh[32];
+  __shared__ double result;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) v += part[i];
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    s = warp_sum(s);
+    if (threadIdx.x == 0) result = s;
+  }
+  __syncthreads();
+  const double r = result;
+  __syncthreads();
+  return r;
+}
+
+// Writes the block sums of v[0..K-1] to part[slot[k] * P + blockIdx.x].
+template <int K>
+__device__ void block_partials(double (&v)[K], double* part, int P, const int (&slot)[K]) {
+  __shared__ double red[K][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const double s = warp_sum(v[k]);
+    if (lane == 0) red[k][wid] = s;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double s = lane < nw ? red[k][lane] : 0.0;
+      s = warp_sum(s);
+      if (lane == 0) part[int64_t(slot[k]) * P + blockIdx.x] = s;
+    }
+  }
+  __syncthreads();
+}
+
+#define GRID_LOOP(i, n) \
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < (n); i += int64_t(gridDim.x) * blockDim.x)
+
+// ---------------------------------------------------------------------------
+// shared kernels
+// ---------------------------------------------------------------------------
+
+__global__ void dot_kernel(const double* __restrict__ a, const double* __restrict__ b, int64_t n, double* part, int P,
+                           int slot) {
+  double v[1] = {0.0};
+  GRID_LOOP(i, n) v[0] += a[i] * b[i];
+  const int sl[1] = {slot};
+  block_partials<1>(v, part, P, sl);
+}
+
+// ---------------------------------------------------------------------------
+// LBFGS (source/lbfgs.cpp)
+// ---------------------------------------------------------------------------
+
+struct LbState {
+  double f, fnew, rms, H0, stepnorm, factor;
+  double inv_sqrt_n, maxstep, max_f_rise;
+  int k, nred, accepted, rel, M;
+};
+
+enum LbSlot { S_IN = 0, S_OUT = 1, S_SG = 2, S_SS = 3, S_GG = 4, S_YS = 5, S_YY = 6, S_TMP = 7, S_NSLOT = 8 };
+
+// k == 0 (lbfgs.cpp:109-124): step = -H0 * gn * g with gn = 1/|g| if |g| > 1 else |g|.
+__global__ void lb_first_step(const double* __restrict__ g, double* __restrict__ step, int64_t n, LbState* st,
+                              double* part, int P) {
+  double gnorm = sqrt(sum_parts(part + int64_t(S_GG) * P, P));
+  if (gnorm > 1.0) gnorm = 1.0 / gnorm;
+  const double pref = -gnorm * st->H0;
+  double v[2] = {0.0, 0.0};
+  GRID_LOOP(i, n) {
+    const double s = pref * g[i];
+    step[i] = s;
+    v[0] += s * g[i];
+    v[1] += s * s;
+  }
+  const int sl[2] = {S_SG, S_SS};
+  block_partials<2>(v, part, P, sl);
+}
+
+// step = g and the first backward dot s_i . g.
+__global__ void lb_start(const double* __restrict__ g, double* __restrict__ step, const double* __restrict__ s_i,
+                         int64_t n, double* part, int P) {
+  double v[1] = {0.0};
+  GRID_LOOP(i, n) {
+    const double gi = g[i];
+    step[i] = gi;
+    v[0] += s_i[i] * gi;
+  }
+  const int sl[1] = {S_OUT};
+  block_partials<1>(v, part, P, sl);
+}
+
+// One two-loop update (lbfgs.cpp:136-169).
+//  backward: a = rho_i (s_i . step); step -= a y_i; [last: step *= -H0]
+//  forward : b = -rho_i (y_i . step); step -= (alpha_i - b) s_i
+// followed by the next dot product (dnext . step), or for the final forward
+// update the line-search dots (step . g, step . step).
+__global__ void lb_update(int forward, int last, double* __restrict__ step, const double* __restrict__ vec,
+                          const double* __restrict__ dnext, const double* __restrict__ g, int64_t n, LbState* st,
+                          double* rho, double* alpha, int mi, double* part, int P) {
+  const double dotin = sum_parts(part + int64_t(S_IN) * P, P);
+  double coef;
+  if (!forward) {
+    coef = rho[mi] * dotin;
+    if (blockIdx.x == 0 && threadIdx.x == 0) alpha[mi] = coef;
+  } else {
+    const double beta = -rho[mi] * dotin;
+    coef = alpha[mi] - beta;
+  }
+  const double h0 = -st->H0;
+  const bool scale = !forward && last;
+  const bool ls = forward && last;
+  double v[2] = {0.0, 0.0};
+  GRID_LOOP(i, n) {
+    double s = step[i] - coef * vec[i];
+    if (scale) s *= h0;
+    step[i] = s;
+    if (ls) {
+      v[0] += s * g[i];
+      v[1] += s * s;
+    } else {
+      v[0] += dnext[i] * s;
+    }
+  }
+  if (ls) {
+    const int sl[2] = {S_SG, S_SS};
+    block_partials<2>(v, part, P, sl);
+  } else {
+    double w[1] = {v[0]};
+    const int sl[1] = {S_OUT};
+    block_partials<1>(w, part, P, sl);
+  }
+}
+
+// Moves the S_OUT partials to S_IN (between two-loop steps).
+__global__ void lb_shift(double* part, int P) {
+  for (int i = threadIdx.x; i < P; i += blockDim.x) part[int64_t(S_IN) * P + i] = part[int64_t(S_OUT) * P + i];
+}
+
+// Trial point of the backtracking line search (lbfgs.cpp:176-204).
+__global__ void lb_trial(const double* __restrict__ xold, const double* __restrict__ step, double* __restrict__ xnew,
+                         int64_t n, LbState* st, double* part, int P) {
+  const double dsg = sum_parts(part + int64_t(S_SG) * P, P);
+  const double ss = sum_parts(part + int64_t(S_SS) * P, P);
+  const double sgn = dsg > 0.0 ? -1.0 : 1.0;
+  const double stepnorm = sqrt(ss);
+  double factor = 1.0;
+  if (factor * stepnorm > st->maxstep) factor = st->maxstep / stepnorm;
+  for (int r = 0; r < st->nred; ++r) factor *= 0.5;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->stepnorm = stepnorm;
+    st->factor = factor;
+  }
+  GRID_LOOP(i, n) xnew[i] = xold[i] + factor * (sgn * step[i]);
+}
+
+// s = xnew - xold, y = gnew - gold into memory slot; |g|^2, y.s, y.y (lbfgs.cpp:74-84).
+__global__ void lb_post(const double* __restrict__ xnew, const double* __restrict__ xold,
+                        const double* __restrict__ gnew, const double* __restrict__ gold, double* __restrict__ s_k,
+                        double* __restrict__ y_k, int64_t n, double* part, int P) {
+  double v[3] = {0.0, 0.0, 0.0};
+  GRID_LOOP(i, n) {
+    const double gi = gnew[i];
+    const double yi = gi - gold[i];
+    const double si = xnew[i] - xold[i];
+    y_k[i] = yi;
+    s_k[i] = si;
+    v[0] += gi * gi;
+    v[1] += yi * si;
+    v[2] += yi * yi;
+  }
+  const int sl[3] = {S_GG, S_YS, S_YY};
+  block_partials<3>(v, part, P, sl);
+}
+
+// Accept test and memory update (lbfgs.cpp:206-245, 86-104).  One block.
+// out: [accepted, f, rms, H0, printed step norm, fnew]
+__global__ void lb_finalize(LbState* st, const double* __restrict__ fnew_dev, double* rho, int kl, double* part, int P,
+                            double* out) {
+  const double gg = sum_parts(part + int64_t(S_GG) * P, P);
+  double ys = sum_parts(part + int64_t(S_YS) * P, P);
+  double yy = sum_parts(part + int64_t(S_YY) * P, P);
+  if (threadIdx.x != 0) return;
+  const double fnew = *fnew_dev;
+  double df = fnew - st->f;
+  if (st->rel) {
+    double absf = 1e-100;
+    if (st->f != 0) absf = fabs(st->f);
+    df /= absf;
+  }
+  const bool ok = df < st->max_f_rise;
+  const bool accept = ok || st->nred >= 9;
+  double printed = st->stepnorm * st->factor;
+  if (!ok) printed *= 0.5;
+  st->fnew = fnew;
+  if (accept) {
+    st->f = fnew;
+    st->rms = sqrt(gg) * st->inv_sqrt_n;
+    if (ys == 0.0) ys = 1.0;
+    rho[kl] = 1.0 / ys;
+    if (yy == 0.0) yy = 1.0;
+    st->H0 = ys / yy;
+    st->k += 1;
+    st->nred = 0;
+    st->accepted = 1;
+  } else {
+    st->nred += 1;
+    st->accepted = 0;
+  }
+  out[0] = accept ? 1.0 : 0.0;
+  out[1] = st->f;
+  out[2] = st->rms;
+  out[3] = st->H0;
+  out[4] = printed;
+  out[5] = fnew;
+}
+
+// Initial f, rms (optimizer.hpp:203-210: rms = sqrt(|g|^2 / n)).
+__global__ void lb_init_fin(LbState* st, const double* __restrict__ e, double inv_n, double* part, int P, double* out) {
+  const double gg = sum_parts(part + int64_t(S_GG) * P, P);
+  if (threadIdx.x != 0) return;
+  st->f = *e;
+  st->rms = sqrt(gg * inv_n);
+  out[1] = st->f;
+  out[2] = st->rms;
+  out[3] = st->H0;
+}
+
+__global__ void lb_set_scalars(LbState* st, double f, double rms, int reset_k, int set_h0, double h0) {
+  st->f = f;
+  st->rms = rms;
+  if (reset_k) {
+    st->k = 0;
+    st->nred = 0;
+  }
+  if (set_h0) st->H0 = h0;
+}
+
+// ---------------------------------------------------------------------------
+// FIRE (source/fresco/modified_fire.hpp)
+// ---------------------------------------------------------------------------
+
+struct FiState {
+  double f, dt, a, ifnorm, vnorm, rms, P, sqrtN;
+  double dtmax, maxstep, finc, fdec, fa, astart;
+  int fire_iter, Nmin, stepback, restore;
+};
+
+enum FiSlot { F_DD = 0, F_PV = 1, F_GG = 2, F_VV = 3, F_NSLOT = 4 };
+
+// v = -g dt and the norms (modified_fire.cpp:313-324).
+__global__ void fi_init_v(const double* __restrict__ g, double* __restrict__ v, int64_t n, FiState* st, double* part,
+                          int P) {
+  const double dt = st->dt;
+  double acc[2] = {0.0, 0.0};
+  GRID_LOOP(i, n) {
+    const double vi = -g[i] * dt;
+    v[i] = vi;
+    acc[0] += g[i] * g[i];
+    acc[1] += vi * vi;
+  }
+  const int sl[2] = {F_GG, F_VV};
+  block_partials<2>(acc, part, P, sl);
+}
+
+__global__ void fi_init_fin(FiState* st, const double* __restrict__ e, double* part, int P, double* out) {
+  const double gg = sum_parts(part + int64_t(F_GG) * P, P);
+  const double vv = sum_parts(part + int64_t(F_VV) * P, P);
+  if (threadIdx.x != 0) return;
+  st->f = *e;
+  st->ifnorm = 1.0 / sqrt(gg);
+  st->vnorm = sqrt(vv);
+  st->rms = 1.0 / (st->ifnorm * st->sqrtN);
+  out[0] = st->f;
+  out[1] = st->rms;
+  out[2] = st->dt;
+  out[3] = st->a;
+  out[4] = 0.0;
+  out[5] = st->vnorm;
+  out[6] = double(st->fire_iter);
+}
+
+// Inertial mixing and the forward-Euler velocity update (modified_fire.hpp:172-174, 141-144).
+__global__ void fi_mix(double* __restrict__ v, const double* __restrict__ g, int64_t n, FiState* st, double* part,
+                       int P) {
+  const double a = st->a, ifn = st->ifnorm, vn = st->vnorm, dt = st->dt;
+  double acc[1] = {0.0};
+  GRID_LOOP(i, n) {
+    double vi = (1.0 - a) * v[i] - a * g[i] * ifn * vn;
+    vi -= dt * g[i];
+    v[i] = vi;
+    const double dx = dt * vi;
+    acc[0] += dx * dx;
+  }
+  const int sl[1] = {F_DD};
+  block_partials<1>(acc, part, P, sl);
+}
+
+// x_old = x, g_old = g, x += dx * factor (modified_fire.hpp:146-155).
+__global__ void fi_step(double* __restrict__ x, double* __restrict__ xo, const double* __restrict__ g,
+                        double* __restrict__ go, const double* __restrict__ v, int64_t n, FiState* st, double* part,
+                        int P) {
+  const double normdx = sqrt(sum_parts(part + int64_t(F_DD) * P, P));
+  double factor = 1.0;
+  if (normdx > st->maxstep) factor = st->maxstep / normdx;
+  const double dt = st->dt;
+  GRID_LOOP(i, n) {
+    const double xi = x[i];
+    xo[i] = xi;
+    go[i] = g[i];
+    const double dx = dt * v[i];
+    x[i] = xi + dx * factor;
+  }
+}
+
+__global__ void fi_post(const double* __restrict__ v, const double* __restrict__ g, int64_t n, double* part, int P) {
+  double acc[3] = {0.0, 0.0, 0.0};
+  GRID_LOOP(i, n) {
+    acc[0] += v[i] * g[i];
+    acc[1] += g[i] * g[i];
+    acc[2] += v[i] * v[i];
+  }
+  const int sl[3] = {F_PV, F_GG, F_VV};
+  block_partials<3>(acc, part, P, sl);
+}
+
+// modified_fire.hpp:180-216.  out: [f, rms, dt, a, P, vnorm, fire_iter]
+__global__ void fi_fin(FiState* st, const double* __restrict__ e, double* part, int P, double* out) {
+  const double pv = sum_parts(part + int64_t(F_PV) * P, P);
+  const double gg = sum_parts(part + int64_t(F_GG) * P, P);
+  const double vv = sum_parts(part + int64_t(F_VV) * P, P);
+  if (threadIdx.x != 0) return;
+  st->fire_iter += 1;
+  const double Pw = -pv;
+  st->P = Pw;
+  if (Pw > 0) {
+    if (st->fire_iter > st->Nmin) {
+      st->dt = fmin(st->dt * st->finc, st->dtmax);
+      st->a *= st->fa;
+    }
+    st->ifnorm = 1.0 / sqrt(gg);
+    st->vnorm = sqrt(vv);
+    st->rms = 1.0 / (st->ifnorm * st->sqrtN);
+    st->f = *e;
+    st->restore = 0;
+  } else {
+    st->dt *= st->fdec;
+    st->a = st->astart;
+    st->fire_iter = 0;
+    st->restore = 1;
+    if (!st->stepback) st->f = *e;
+  }
+  out[0] = st->f;
+  out[1] = st->rms;
+  out[2] = st->dt;
+  out[3] = st->a;
+  out[4] = Pw;
+  out[5] = st->vnorm;
+  out[6] = double(st->fire_iter);
+}
+
+// P <= 0: v = 0 and, with stepback, x = x_old, g = g_old (modified_fire.hpp:204-212).
+__global__ void fi_restore(double* __restrict__ x, const double* __restrict__ xo, double* __restrict__ g,
+                           const double* __restrict__ go, double* __restrict__ v, int64_t n, const FiState* st) {
+  if (!st->restore) return;
+  const bool sb = st->stepback != 0;
+  GRID_LOOP(i, n) {
+    v[i] = 0.0;
+    if (sb) {
+      x[i] = xo[i];
+      g[i] = go[i];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host classes
+// ---------------------------------------------------------------------------
+
+class Lbfgs final : public Optimizer {
+ public:
+  Lbfgs(PotentialPtr pot, const double* x0, int64_t n, const LbfgsParams& p)
+      : Optimizer(pot, n, p.tol, p.maxiter, p.iprint, p.verbosity), prm_(p) {
+    if (p.M < 1) throw InvalidArgument("LBFGS memory M must be >= 1");
+    const int64_t nn = std::max<int64_t>(n, 1);
+    for (int b = 0; b < 2; ++b) {
+      X_[b].alloc(nn);
+      G_[b].alloc(nn);
+    }
+    step_.alloc(nn);
+    sm_.alloc(nn * p.M);
+    ym_.alloc(nn * p.M);
+    rho_.alloc(p.M);
+    alpha_.alloc(p.M);
+    e_.alloc(1);
+    st_.alloc(1);
+    part_.alloc(int64_t(S_NSLOT) * P_);
+    FB_CUDA(cudaMemsetAsync(rho_.p, 0, rho_.bytes(), s_));
+    FB_CUDA(cudaMemsetAsync(alpha_.p, 0, alpha_.bytes(), s_));
+    FB_CUDA(cudaMemsetAsync(part_.p, 0, part_.bytes(), s_));
+    LbState h{};
+    h.f = 0.0;
+    h.rms = 1e10;
+    h.H0 = p.H0;
+    h.inv_sqrt_n = 1.0 / std::sqrt(double(n));
+    h.maxstep = p.maxstep;
+    h.max_f_rise = p.max_f_rise;
+    h.rel = p.rel_energy ? 1 : 0;
+    h.M = p.M;
+    FB_CUDA(cudaMemcpyAsync(st_.p, &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+    if (n > 0) FB_CUDA(cudaMemcpyAsync(X_[0].p, x0, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
+    h0_ = p.H0;
+  }
+
+  double* device_x() override { return X_[cur_].p; }
+  double* device_g() override { return G_[cur_].p; }
+  double h0() const override { return h0_; }
+
+  void set_func_gradient(double f, const double* grad, int64_t n) override {
+    if (n != n_) throw InvalidArgument("the gradient has the wrong size");
+    if (iter_ > 0) std::printf("warning: setting f and grad after the first iteration.  this is dangerous.\n");
+    double gnorm = 0.0;
+    for (int64_t i = 0; i < n; ++i) gnorm += grad[i] * grad[i];
+    f_ = f;
+    rms_ = std::sqrt(gnorm / double(n));
+    FB_CUDA(cudaMemcpyAsync(G_[cur_].p, grad, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
+    lb_set_scalars<<<1, 1, 0, s_>>>(st_.p, f_, rms_, 0, 0, 0.0);
+    FB_LAUNCH_CHECK();
+    FB_CUDA(cudaStreamSynchronize(s_));
+    func_initialized_ = true;
+  }
+
+  void reset(const double* x0, int64_t n) override {
+    if (n != n_)
+      throw InvalidArgument("The number of degrees of freedom (x0.size()) cannot change when calling reset()");
+    k_ = 0;
+    iter_ = 0;
+    nfev_ = 0;
+    FB_CUDA(cudaMemcpyAsync(X_[cur_].p, x0, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
+    lb_set_scalars<<<1, 1, 0, s_>>>(st_.p, f_, rms_, 1, 0, 0.0);
+    FB_LAUNCH_CHECK();
+    initialize_func_gradient();
+  }
+
+  void one_iteration() override {
+    if (!func_initialized_) initialize_func_gradient();
+    const int c = cur_, o = 1 - cur_;
+    const double* g = G_[c].p;
+    const int M = prm_.M;
+    // compute_lbfgs_step (lbfgs.cpp:107-170)
+    if (k_ == 0) {
+      dot_kernel<<<P_, kThreads, 0, s_>>>(g, g, n_, part_.p, P_, S_GG);
+      lb_first_step<<<P_, kThreads, 0, s_>>>(g, step_.p, n_, st_.p, part_.p, P_);
+    } else {
+      const int jmin = std::max(0, k_ - M), jmax = k_;
+      const int m = jmax - jmin;
+      int i0 = (jmax - 1) % M;
+      lb_start<<<P_, kThreads, 0, s_>>>(g, step_.p, sm_.p + int64_t(i0) * n_, n_, part_.p, P_);
+      for (int t = 0; t < m; ++t) {
+        const int j = jmax - 1 - t;
+        const int i = j % M;
+        const bool last = (t == m - 1);
+        const int inext = last ? (jmin % M) : ((j - 1) % M);
+        const double* dnext = last ? ym_.p + int64_t(inext) * n_ : sm_.p + int64_t(inext) * n_;
+        lb_shift<<<1, 256, 0, s_>>>(part_.p, P_);
+        lb_update<<<P_, kThreads, 0, s_>>>(0, last, step_.p, ym_.p + int64_t(i) * n_, dnext, g, n_, st_.p, rho_.p,
+                                           alpha_.p, i, part_.p, P_);
+      }
+      for (int t = 0; t < m; ++t) {
+        const int j = jmin + t;
+        const int i = j % M;
+        const bool last = (t == m - 1);
+        const int inext = (j + 1) % M;
+        const double* dnext = last ? nullptr : ym_.p + int64_t(inext) * n_;
+        lb_shift<<<1, 256, 0, s_>>>(part_.p, P_);
+        lb_update<<<P_, kThreads, 0, s_>>>(1, last, step_.p, sm_.p + int64_t(i) * n_, dnext, g, n_, st_.p, rho_.p,
+                                           alpha_.p, i, part_.p, P_);
+      }
+    }
+    FB_LAUNCH_CHECK();
+    // backtracking_linesearch (lbfgs.cpp:172-245) + update_memory (:66-105)
+    const int kl = k_ % M;
+    double printed = 0.0;
+    for (int nred = 0; nred < 10; ++nred) {
+      lb_trial<<<P_, kThreads, 0, s_>>>(X_[c].p, step_.p, X_[o].p, n_, st_.p, part_.p, P_);
+      FB_LAUNCH_CHECK();
+      ++nfev_;
+      eval(X_[o].p, G_[o].p, e_.p);
+      lb_post<<<P_, kThreads, 0, s_>>>(X_[o].p, X_[c].p, G_[o].p, G_[c].p, sm_.p + int64_t(kl) * n_,
+                                       ym_.p + int64_t(kl) * n_, n_, part_.p, P_);
+      lb_finalize<<<1, 256, 0, s_>>>(st_.p, e_.p, rho_.p, kl, part_.p, P_, host_);
+      FB_LAUNCH_CHECK();
+      FB_CUDA(cudaStreamSynchronize(s_));
+      if (verbosity_ > 2 && host_[0] == 0.0) {
+        std::printf("energy increased by %.17g to %.17g from %.17g\n", host_[5] - f_, host_[5], f_);
+      }
+      if (host_[0] != 0.0) {
+        printed = host_[4];
+        if (nred == 9 && verbosity_ > 0 && !(host_[5] - f_ < prm_.max_f_rise))
+          std::printf("warning: the line search backtracked too many times\n");
+        break;
+      }
+    }
+    cur_ = o;
+    f_ = host_[1];
+    rms_ = host_[2];
+    h0_ = host_[3];
+    k_ += 1;
+    if (iprint_ > 0 && iter_ % iprint_ == 0) {
+      std::printf("lbgs: %d E %.17g rms %.17g nfev %d step norm %.17g\n", iter_, f_, rms_, nfev_, printed);
+      std::fflush(stdout);
+    }
+    iter_ += 1;
+  }
+
+ private:
+  void initialize_func_gradient() override {
+    ++nfev_;
+    eval(X_[cur_].p, G_[cur_].p, e_.p);
+    dot_kernel<<<P_, kThreads, 0, s_>>>(G_[cur_].p, G_[cur_].p, n_, part_.p, P_, S_GG);
+    lb_init_fin<<<1, 256, 0, s_>>>(st_.p, e_.p, 1.0 / double(n_), part_.p, P_, host_);
+    FB_LAUNCH_CHECK();
+    FB_CUDA(cudaStreamSynchronize(s_));
+    f_ = host_[1];
+    rms_ = host_[2];
+    func_initialized_ = true;
+  }
+
+  LbfgsParams prm_;
+  DevBuf<double> X_[2], G_[2], step_, sm_, ym_, rho_, alpha_, e_;
+  DevBuf<LbState> st_;
+  int cur_ = 0;
+  int k_ = 0;
+  double h0_ = 0.1;
+};
+
+class Fire final : public Optimizer {
+ public:
+  Fire(PotentialPtr pot, const double* x0, int64_t n, const FireParams& p)
+      : Optimizer(pot, n, p.tol, p.maxiter, p.iprint, p.verbosity), prm_(p) {
+    const int64_t nn = std::max<int64_t>(n, 1);
+    X_.alloc(nn);
+    XO_.alloc(nn);
+    G_.alloc(nn);
+    GO_.alloc(nn);
+    V_.alloc(nn);
+    e_.alloc(1);
+    st_.alloc(1);
+    part_.alloc(int64_t(F_NSLOT) * P_);
+    FB_CUDA(cudaMemsetAsync(V_.p, 0, V_.bytes(), s_));
+    FB_CUDA(cudaMemsetAsync(G_.p, 0, G_.bytes(), s_));
+    FB_CUDA(cudaMemsetAsync(part_.p, 0, part_.bytes(), s_));
+    FiState h{};
+    h.f = 0.0;
+    h.dt = p.dtstart;
+    h.a = p.astart;
+    h.rms = 1e10;
+    h.sqrtN = std::sqrt(double(n));
+    h.dtmax = p.dtmax;
+    h.maxstep = p.maxstep;
+    h.finc = p.finc;
+    h.fdec = p.fdec;
+    h.fa = p.fa;
+    h.astart = p.astart;
+    h.Nmin = p.Nmin;
+    h.stepback = p.stepback ? 1 : 0;
+    FB_CUDA(cudaMemcpyAsync(st_.p, &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+    if (n > 0) FB_CUDA(cudaMemcpyAsync(X_.p, x0, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
+  }
+
+  double* device_x() override { return X_.p; }
+  double* device_g() override { return G_.p; }
+
+  void set_func_gradient(double f, const double* grad, int64_t n) override {
+    if (n != n_) throw InvalidArgument("the gradient has the wrong size");
+    if (iter_ > 0) std::printf("warning: setting f and grad after the first iteration.  this is dangerous.\n");
+    FB_CUDA(cudaMemcpyAsync(G_.p, grad, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
+    FB_CUDA(cudaMemcpyAsync(e_.p, &f, sizeof(double), cudaMemcpyHostToDevice, s_));
+    init_from_gradient();
+  }
+
+  void reset(const double* x0, int64_t n) override {
+    if (n != n_) throw InvalidArgument("The number of degrees of freedom (x0.size()) cannot change when calling reset()");
+    if (!func_initialized_) initialize_func_gradient();
+    iter_ = 0;
+    FB_CUDA(cudaMemcpyAsync(X_.p, x0, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
+    eval(X_.p, G_.p, e_.p);
+    nfev_ = 1;
+    FiState h{};
+    FB_CUDA(cudaMemcpyAsync(&h, st_.p, sizeof(h), cudaMemcpyDeviceToHost, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
+    h.fire_iter = 0;
+    h.dt = prm_.dtstart;
+    h.a = prm_.astart;
+    FB_CUDA(cudaMemcpyAsync(st_.p, &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+    init_from_gradient();
+  }
+
+  void one_iteration() override {
+    if (!func_initialized_) initialize_func_gradient();
+    ++nfev_;
+    ++iter_;
+    fi_mix<<<P_, kThreads, 0, s_>>>(V_.p, G_.p, n_, st_.p, part_.p, P_);
+    fi_step<<<P_, kThreads, 0, s_>>>(X_.p, XO_.p, G_.p, GO_.p, V_.p, n_, st_.p, part_.p, P_);
+    FB_LAUNCH_CHECK();
+    eval(X_.p, G_.p, e_.p);
+    fi_post<<<P_, kThreads, 0, s_>>>(V_.p, G_.p, n_, part_.p, P_);
+    fi_fin<<<1, 256, 0, s_>>>(st_.p, e_.p, part_.p, P_, host_);
+    fi_restore<<<P_, kThreads, 0, s_>>>(X_.p, XO_.p, G_.p, GO_.p, V_.p, n_, st_.p);
+    FB_LAUNCH_CHECK();
+    FB_CUDA(cudaStreamSynchronize(s_));
+    f_ = host_[0];
+    rms_ = host_[1];
+    if (verbosity_ > 1 && !(host_[4] > 0)) std::printf("warning: step direction was uphill.  inverting\n");
+    if (iprint_ > 0 && iter_ % iprint_ == 0) {
+      std::printf("fire: %d fire_iter_number %d dt %.17g a %.17g P %.17g vnorm %.17g E %.17g rms %.17g nfev %d\n",
+                  iter_, int(host_[6]), host_[2], host_[3], host_[4], host_[5], f_, rms_, nfev_);
+      std::fflush(stdout);
+    }
+  }
+
+ private:
+  void init_from_gradient() {
+    fi_init_v<<<P_, kThreads, 0, s_>>>(G_.p, V_.p, n_, st_.p, part_.p, P_);
+    fi_init_fin<<<1, 256, 0, s_>>>(st_.p, e_.p, part_.p, P_, host_);
+    FB_LAUNCH_CHECK();
+    FB_CUDA(cudaStreamSynchronize(s_));
+    f_ = host_[0];
+    rms_ = host_[1];
+    func_initialized_ = true;
+  }
+
+  void initialize_func_gradient() override {
+    ++nfev_;
+    eval(X_.p, G_.p, e_.p);
+    init_from_gradient();
+  }
+
+  FireParams prm_;
+  DevBuf<double> X_, XO_, G_, GO_, V_, e_;
+  DevBuf<FiState> st_;
+};
+
+}  // namespace
+
+Optimizer::Optimizer(PotentialPtr pot, int64_t n, double tol, int maxiter, int iprint, int verbosity)
+    : pot_(std::move(pot)), n_(n), tol_(tol), maxiter_(maxiter), iprint_(iprint), verbosity_(verbosity) {
+  if (!pot_) throw InvalidArgument("null potential");
+  if (n <= 0) throw InvalidArgument("empty coordinate array");
+  FB_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+  P_ = std::max(1, std::min(1024, 2 * sm_count()));
+  FB_CUDA(cudaMallocHost(&host_, 16 * sizeof(double)));
+  for (int i = 0; i < 16; ++i) host_[i] = 0.0;
+}
+
+Optimizer::~Optimizer() {
+  if (s_) {
+    cudaStreamSynchronize(s_);
+    cudaStreamDestroy(s_);
+  }
+  if (host_) cudaFreeHost(host_);
+}
+
+void Optimizer::eval(const double* x, double* g, double* e) { pot_->energy_gradient(x, n_, g, e, false, s_); }
+
+void Optimizer::run(int niter) {
+  if (!func_initialized_) initialize_func_gradient();
+  for (int i = 0; i < niter; ++i) {
+    if (stop_criterion_satisfied()) break;
+    one_iteration();
+  }
+}
+
+void Optimizer::run() { run(maxiter_ - iter_); }
+
+bool Optimizer::stop_criterion_satisfied() {
+  if (!func_initialized_) initialize_func_gradient();
+  return rms_ <= tol_;
+}
+
+void Optimizer::get_state(double* x, double* g, double* f, double* rms, int* nfev, int* niter, int* maxiter,
+                          double* H0) {
+  if (x) FB_CUDA(cudaMemcpyAsync(x, device_x(), sizeof(double) * n_, cudaMemcpyDeviceToHost, s_));
+  if (g) FB_CUDA(cudaMemcpyAsync(g, device_g(), sizeof(double) * n_, cudaMemcpyDeviceToHost, s_));
+  FB_CUDA(cudaStreamSynchronize(s_));
+  if (f) *f = f_;
+  if (rms) *rms = rms_;
+  if (nfev) *nfev = nfev_;
+  if (niter) *niter = iter_;
+  if (maxiter) *maxiter = maxiter_;
+  if (H0) *H0 = h0();
+}
+
+std::unique_ptr<Optimizer> make_lbfgs(PotentialPtr pot, const double* x0, int64_t n, const LbfgsParams& p) {
+  return std::unique_ptr<Optimizer>(new Lbfgs(std::move(pot), x0, n, p));
+}
+
+std::unique_ptr<Optimizer> make_fire(PotentialPtr pot, const double* x0, int64_t n, const FireParams& p) {
+  return std::unique_ptr<Optimizer>(new Fire(std::move(pot), x0, n, p));
+}
+
+}  // namespace fb

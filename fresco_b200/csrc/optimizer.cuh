@@ -1,0 +1,76 @@
+// Device-resident gradient optimisers: LBFGS (source/lbfgs.cpp:9-258) and
+// modified FIRE (source/fresco/modified_fire.hpp:44-230, source/
+// modified_fire.cpp:43-118), with the GradientOptimizer driver of
+// source/fresco/optimizer.hpp:55-241.
+//
+// Vectors (x, g, LBFGS memory, FIRE velocities) stay in HBM; every dot
+// product is an FP64 two-stage reduction with a fixed block count, so
+// results are deterministic for a given device.  The host keeps only the
+// control flow: it reads a few scalars once per potential evaluation (the
+// line-search accept test and the stop criterion).
+#pragma once
+
+#include <memory>
+
+#include "potential.cuh"
+
+namespace fb {
+
+struct LbfgsParams {
+  double tol = 1e-5;
+  int M = 4;
+  double maxstep = 0.1;
+  double max_f_rise = 1e-4;
+  double H0 = 0.1;
+  bool rel_energy = false;
+  int maxiter = 10000;
+  int iprint = -1;
+  int verbosity = 0;
+};
+
+struct FireParams {
+  double dtstart = 0.1, dtmax = 1.0, maxstep = 0.5;
+  int Nmin = 5;
+  double finc = 1.1, fdec = 0.5, fa = 0.99, astart = 0.1, tol = 1e-3;
+  bool stepback = true;
+  int maxiter = 10000;
+  int iprint = -1;
+  int verbosity = 0;
+};
+
+class Optimizer {
+ public:
+  virtual ~Optimizer();
+  virtual void one_iteration() = 0;
+  void run(int niter);  // optimizer.hpp:97-112
+  void run();           // optimizer.hpp:118-121
+  bool stop_criterion_satisfied();
+  virtual void set_func_gradient(double f, const double* grad, int64_t n) = 0;
+  virtual void reset(const double* x0, int64_t n) = 0;
+  void get_state(double* x, double* g, double* f, double* rms, int* nfev, int* niter, int* maxiter, double* H0);
+  virtual double* device_x() = 0;
+  virtual double* device_g() = 0;
+  virtual double h0() const { return 0.0; }
+
+ protected:
+  Optimizer(PotentialPtr pot, int64_t n, double tol, int maxiter, int iprint, int verbosity);
+  virtual void initialize_func_gradient() = 0;
+  void eval(const double* x, double* g, double* e);  // one potential call (nfev not touched)
+
+  PotentialPtr pot_;
+  cudaStream_t s_ = nullptr;
+  int64_t n_;
+  int P_;  // reduction blocks
+  double tol_;
+  int maxiter_, iprint_, verbosity_;
+  int iter_ = 0, nfev_ = 0;
+  double f_ = 0.0, rms_ = 1e10;
+  bool func_initialized_ = false;
+  DevBuf<double> part_;  // reduction partials [slots][P_]
+  double* host_ = nullptr;  // pinned scalar mirror
+};
+
+std::unique_ptr<Optimizer> make_lbfgs(PotentialPtr pot, const double* x0, int64_t n, const LbfgsParams& p);
+std::unique_ptr<Optimizer> make_fire(PotentialPtr pot, const double* x0, int64_t n, const FireParams& p);
+
+}  // namespace fb

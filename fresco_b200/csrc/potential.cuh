@@ -1,0 +1,91 @@
+// Device-side potential interface: the B200 counterpart of
+// fresco::BasePotential (source/fresco/base_potential.hpp:15-156).  All
+// pointers are device pointers; every call is asynchronous on the given
+// stream and allocates nothing.
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace fb {
+
+class Potential {
+ public:
+  virtual ~Potential() = default;
+
+  // Number of coordinates the potential expects (-1: any).
+  virtual int64_t ndof() const = 0;
+
+  // E(x) -> *energy (or += when accumulate).  base_potential.hpp:28-31.
+  virtual void energy(const double* x, int64_t n, double* energy, bool accumulate, cudaStream_t s) = 0;
+
+  // E(x), grad E(x).  With accumulate the gradient and energy are added to
+  // what the buffers hold (base_potential.hpp:50-58 add_energy_gradient, here
+  // without the temporary vector).
+  virtual void energy_gradient(const double* x, int64_t n, double* grad, double* energy, bool accumulate,
+                               cudaStream_t s) = 0;
+
+  // Sticky status bits (StatusBits) raised by kernels since the last read.
+  virtual int read_and_clear_status(cudaStream_t s);
+
+  virtual std::string kind() const = 0;
+  // Human-readable set-up summary (kernel width, grids, ...).
+  virtual std::string describe() const { return kind(); }
+
+  int device = 0;
+
+  // Per-stage CUDA-event timing (for the benchmark's roofline figures).
+  struct StageTimer {
+    bool enabled = false;
+    std::vector<std::string> names;
+    std::vector<cudaEvent_t> ev;
+    std::vector<double> total_ms;
+    std::vector<int> count;
+    int next = 0;
+  };
+  StageTimer timer;
+  void timer_mark(const char* name, cudaStream_t s);  // records the end of a stage
+  void timer_begin(cudaStream_t s);
+  void timer_collect();  // host sync; accumulates elapsed times
+
+ protected:
+  DevBuf<int> status_;
+  void init_status();
+};
+
+using PotentialPtr = std::shared_ptr<Potential>;
+
+// CombinedPotential (source/fresco/combine_potentials.hpp:16-59).
+class CombinedPotential : public Potential {
+ public:
+  CombinedPotential();
+  void add(PotentialPtr p);
+  int64_t ndof() const override;
+  void energy(const double* x, int64_t n, double* e, bool acc, cudaStream_t s) override;
+  void energy_gradient(const double* x, int64_t n, double* g, double* e, bool acc, cudaStream_t s) override;
+  int read_and_clear_status(cudaStream_t s) override;
+  std::string kind() const override { return "CombinedPotential"; }
+  const std::vector<PotentialPtr>& parts() const { return parts_; }
+
+ private:
+  std::vector<PotentialPtr> parts_;
+};
+
+// Factories (defined per potential family).
+PotentialPtr make_nuwu(const std::vector<double>& radii, double K, const std::vector<double>& sk,
+                       const std::vector<double>& v, const std::vector<double>& L, double eps, int precision);
+PotentialPtr make_uwu(const std::vector<int>& grid, double K, const std::vector<double>& sk,
+                      const std::vector<double>& v, const std::vector<double>& L, double eps, int precision);
+PotentialPtr make_uwnu(const std::vector<int>& grid, const std::vector<double>& kpts, const std::vector<double>& sk,
+                       const std::vector<double>& v, const std::vector<double>& L, double eps, int precision);
+PotentialPtr make_nuwnu(const std::vector<double>& radii, const std::vector<double>& kpts,
+                        const std::vector<double>& sk, const std::vector<double>& v, const std::vector<double>& L,
+                        double eps, int precision);
+PotentialPtr make_inversepower(double a, double eps, const std::vector<double>& radii,
+                               const std::vector<double>& boxv, bool periodic, bool use_cell_lists,
+                               double ncellx_scale);
+
+}  // namespace fb

@@ -1,0 +1,174 @@
+/*
+ * fresco_b200 C ABI: the drop-in boundary of the B200 implementation of
+ * FReSCo's loss-and-gradient path.
+ *
+ * The reference binds its C++ classes from Cython (fresco/potentials/*.pxd,
+ * fresco/optimize/*.pyx).  Each entry point below replaces one C++ member
+ * the Cython layer calls; the citation names the reference declaration (paths
+ * relative to the reference project root).  Arguments are plain pointers and
+ * sizes; "host" pointers are ordinary CPU memory, "device" pointers are CUDA
+ * global memory on the handle's device.
+ *
+ * Return value: FRESCO_OK (0) or an error code; fresco_last_error() gives the
+ * message for the calling thread.  FRESCO_ERR_INVALID corresponds to the
+ * reference's std::invalid_argument (Python ValueError), the others to
+ * std::runtime_error (Python RuntimeError).
+ *
+ * Threading: like the reference objects (which mutate plan and gradient
+ * members), a handle is not re-entrant; calls on one handle must not overlap.
+ */
+#ifndef FRESCO_B200_H
+#define FRESCO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef struct fresco_potential_s* fresco_potential;
+typedef struct fresco_optimizer_s* fresco_optimizer;
+
+enum {
+  FRESCO_OK = 0,
+  FRESCO_ERR_INVALID = 1,     /* bad argument (reference: std::invalid_argument) */
+  FRESCO_ERR_RUNTIME = 2,     /* CUDA/cuFFT failure or other runtime error */
+  FRESCO_ERR_NONFINITE = 3,   /* a coordinate was NaN/inf: energy and gradient are NaN */
+};
+
+enum { FRESCO_FP64 = 0, FRESCO_FP32 = 1 };
+
+/* Message of the last error on this thread ("" if none). */
+const char* fresco_last_error(void);
+/* ABI version (major * 100 + minor). */
+int fresco_abi_version(void);
+
+/* ---- potentials: constructors ------------------------------------------ */
+
+/* fresco::NUwU(radii, K, Sk, V, L, eps)  (source/fresco/nuwu.hpp:35-52;
+ * Cython binding fresco/potentials/nuwu.pxd:9).  sk and v hold n_sk doubles
+ * each (flattened, dimension 0 fastest); ndim = len(L).  precision selects
+ * the FP64 form or the FP32 spread/FFT/interpolation form (FP64 reduction). */
+int fresco_nuwu_create(const double* radii, int64_t n_points, double K, const double* sk, const double* v,
+                       int64_t n_sk, const double* L, int ndim, double eps, int precision, fresco_potential* out);
+
+/* fresco::UwU(N, K, Sk, V, L, eps)  (source/fresco/uwu.hpp:34-50; uwu.pxd).
+ * sk and v are already ifftshifted (natural FFT order, as uwu.pyx:14-15
+ * passes them).  grid holds ndim ints, slowest first (FFTW row-major). */
+int fresco_uwu_create(const int* grid, int ndim, double K, const double* sk, const double* v, int64_t n_sk,
+                      const double* L, double eps, int precision, fresco_potential* out);
+
+/* fresco::UwNU(N, K, Sk, V, L, eps)  (source/fresco/uwnu.hpp:231-282; uwnu.pxd).
+ * kpts holds n_k*ndim doubles interleaved; grid holds ndim ints with
+ * grid[0] the fastest dimension (FINUFFT's n_modes order). */
+int fresco_uwnu_create(const int* grid, int ndim, const double* kpts, int64_t n_k, const double* sk,
+                       const double* v, const double* L, double eps, int precision, fresco_potential* out);
+
+/* fresco::NUwNU(radii, K, Sk, V, L, eps)  (source/fresco/nuwnu.hpp:36-79; nuwnu.pxd). */
+int fresco_nuwnu_create(const double* radii, int64_t n_points, const double* kpts, int64_t n_k, const double* sk,
+                        const double* v, const double* L, int ndim, double eps, int precision,
+                        fresco_potential* out);
+
+/* fresco::InversePowerPeriodicCellLists<ndim>(pow, eps, radii, boxv,
+ * ncellx_scale, balance_omp) and InversePowerPeriodic / InversePowerCartesian
+ * (source/fresco/inversepower_potential.hpp:80-124;
+ * fresco/potentials/inversepower_potential.pyx:16-79).  periodic = 0 selects
+ * the Cartesian distance. */
+int fresco_inversepower_create(double a, double eps, const double* radii, int64_t n_points, const double* boxv,
+                               int ndim, int periodic, int use_cell_lists, double ncellx_scale,
+                               fresco_potential* out);
+
+/* fresco::CombinedPotential() and add_potential()  (source/fresco/combine_potentials.hpp:
+ * 28-37; fresco/potentials/_fresco.pxd:39-44).  The combined handle keeps a
+ * reference to each part. */
+int fresco_combined_create(fresco_potential* out);
+int fresco_combined_add(fresco_potential combined, fresco_potential part);
+
+void fresco_potential_destroy(fresco_potential p);
+/* Coordinates expected by the potential (-1 when any size is accepted). */
+int64_t fresco_potential_ndof(fresco_potential p);
+
+/* ---- potentials: evaluation --------------------------------------------- */
+
+/* BasePotential::get_energy(x)  (source/fresco/base_potential.hpp:28-31),
+ * host buffers: x[n] in, *energy out.  Synchronous. */
+int fresco_potential_energy(fresco_potential p, const double* x, int64_t n, double* energy);
+
+/* BasePotential::get_energy_gradient(x, grad)  (base_potential.hpp:38-43),
+ * host buffers: x[n] in, grad[n] and *energy out.  Synchronous. */
+int fresco_potential_energy_gradient(fresco_potential p, const double* x, int64_t n, double* grad,
+                                     double* energy);
+
+/* Device-resident forms of the two calls above: d_x, d_grad, d_energy are
+ * device pointers; the work is enqueued on `stream` (a cudaStream_t; NULL
+ * selects the legacy default stream) and the call returns without waiting.
+ * accumulate != 0 adds into d_grad / d_energy (BasePotential::
+ * add_energy_gradient, base_potential.hpp:50-58). */
+int fresco_potential_energy_device(fresco_potential p, const double* d_x, int64_t n, double* d_energy,
+                                   int accumulate, void* stream);
+int fresco_potential_energy_gradient_device(fresco_potential p, const double* d_x, int64_t n, double* d_grad,
+                                            double* d_energy, int accumulate, void* stream);
+
+/* Sticky status bits raised since the last call (1: non-finite input).
+ * Synchronises `stream`.  No reference counterpart (FINUFFT's return codes
+ * are ignored at source/fresco/nuwu.hpp:191-192, 256-258). */
+int fresco_potential_status(fresco_potential p, void* stream, int* status);
+
+/* Per-stage device timing of the next evaluations (CUDA events). */
+int fresco_potential_set_timing(fresco_potential p, int enabled);
+/* Copies up to max_stages (name, total ms, count) triples; names are
+ * written NUL-separated into names (capacity names_len). */
+int fresco_potential_get_timing(fresco_potential p, int max_stages, char* names, int names_len, double* total_ms,
+                                int* counts, int* n_stages);
+/* Describes the NUFFT set-up of a NUwU/UwNU handle: kernel width, fine grid
+ * per dimension, active modes, FFT precision bytes. */
+int fresco_potential_describe(fresco_potential p, char* buf, int buf_len);
+
+/* ---- optimisers ---------------------------------------------------------- */
+
+/* fresco::LBFGS(potential, x0, tol, M) plus set_H0 / set_maxstep /
+ * set_max_f_rise / set_max_iter / set_verbosity / set_iprint /
+ * set_use_relative_f  (source/fresco/lbfgs.hpp:316-342;
+ * fresco/optimize/_lbfgs_cpp.pyx:22-66).  All state lives on the device. */
+int fresco_lbfgs_create(fresco_potential p, const double* x0, int64_t n, double tol, int M, double maxstep,
+                        double max_f_rise, double H0, int rel_energy, int nsteps, int iprint, int verbosity,
+                        fresco_optimizer* out);
+
+/* fresco::MODIFIED_FIRE(potential, x0, dtstart, dtmax, maxstep, Nmin, finc,
+ * fdec, fa, astart, tol, stepback)  (source/fresco/modified_fire.hpp:57-60;
+ * fresco/optimize/_modified_fire_cpp.pyx:18-37). */
+int fresco_fire_create(fresco_potential p, const double* x0, int64_t n, double dtstart, double dtmax,
+                       double maxstep, int Nmin, double finc, double fdec, double fa, double astart, double tol,
+                       int stepback, int nsteps, int iprint, int verbosity, fresco_optimizer* out);
+
+/* GradientOptimizer::set_func_gradient(f, grad)  (source/fresco/optimizer.hpp:127-144). */
+int fresco_optimizer_set_func_gradient(fresco_optimizer o, double f, const double* grad, int64_t n);
+/* GradientOptimizer::run(niter) / run()  (optimizer.hpp:97-121); niter < 0 runs to maxiter. */
+int fresco_optimizer_run(fresco_optimizer o, int niter);
+/* one_iteration()  (lbfgs.cpp:36-64, modified_fire.hpp:160-230). */
+int fresco_optimizer_one_iteration(fresco_optimizer o);
+/* reset(x0)  (lbfgs.cpp:247-257, modified_fire.hpp:84-112). */
+int fresco_optimizer_reset(fresco_optimizer o, const double* x0, int64_t n);
+/* stop_criterion_satisfied()  (optimizer.hpp:174-180). */
+int fresco_optimizer_stop_criterion_satisfied(fresco_optimizer o, int* out);
+/* get_x / get_g / get_f / get_rms / get_nfev / get_niter / get_maxiter and
+ * LBFGS::get_H0  (optimizer.hpp:160-168, lbfgs.hpp:345).  x and g may be NULL. */
+int fresco_optimizer_get_state(fresco_optimizer o, double* x, double* g, double* f, double* rms, int* nfev,
+                               int* niter, int* maxiter, double* H0);
+/* Device pointers of the optimiser's x and g (valid until destroy). */
+int fresco_optimizer_device_state(fresco_optimizer o, double** d_x, double** d_g);
+void fresco_optimizer_destroy(fresco_optimizer o);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FRESCO_B200_H */

@@ -1,0 +1,599 @@
+// Oracle implementation of the FINUFFT and FFTW entry points the reference
+// calls (test infrastructure only; see finufft.h / fftw3.h in this folder).
+//
+//  * exact mode: direct FP64 sums, the quantity FINUFFT approximates;
+//  * ES mode: a CPU ES-kernel NUFFT (types 1 and 2) restated from Barnett,
+//    Magland & af Klinteberg, SIAM J. Sci. Comput. 41(5), 2019: fine grid
+//    nf = smallest 2,3,5-smooth even number >= max(2n, 2w), kernel
+//    exp(beta (sqrt(1 - t^2) - 1)) of w = ceil(log10(10/tol)) points,
+//    beta = 2.30 w, correction by Gauss-Legendre quadrature of the kernel's
+//    Fourier transform.  Spreading uses a tile colouring so that OpenMP
+//    threads never write the same grid cell; everything is FP64.
+//  * the FFT is a mixed-radix Cooley-Tukey (radix 4, 2 and generic odd
+//    primes) on the CPU.
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "fftw3.h"
+#include "finufft.h"
+
+namespace {
+
+using cd = std::complex<double>;
+constexpr double kPi = 3.14159265358979323846;
+
+int g_mode = 0;  // 0 auto, 1 exact, 2 ES
+
+// ---------------------------------------------------------------------------
+// mixed-radix FFT
+// ---------------------------------------------------------------------------
+
+struct Fft1 {
+  int n = 1;
+  int sign = 1;
+  std::vector<cd> tw;  // exp(sign 2 pi i j / n)
+  std::vector<int> fac;
+
+  Fft1(int n_, int sign_) : n(n_), sign(sign_) {
+    tw.resize(n);
+    for (int j = 0; j < n; ++j) {
+      const double a = sign * 2.0 * kPi * double(j) / double(n);
+      tw[j] = cd(std::cos(a), std::sin(a));
+    }
+    int r = n;
+    while (r % 4 == 0) { fac.push_back(4); r /= 4; }
+    while (r % 2 == 0) { fac.push_back(2); r /= 2; }
+    for (int p = 3; p * p <= r; p += 2)
+      while (r % p == 0) { fac.push_back(p); r /= p; }
+    if (r > 1) fac.push_back(r);
+  }
+
+  void rec(const cd* in, long istride, cd* out, int m_n, size_t fi, int ts) const {
+    if (m_n == 1) {
+      out[0] = in[0];
+      return;
+    }
+    const int p = fac[fi];
+    const int m = m_n / p;
+    for (int q = 0; q < p; ++q) rec(in + q * istride, istride * p, out + q * m, m, fi + 1, ts * p);
+    if (p == 2) {
+      for (int k = 0; k < m; ++k) {
+        const cd a = out[k], b = out[m + k] * tw[size_t(k) * ts];
+        out[k] = a + b;
+        out[m + k] = a - b;
+      }
+    } else if (p == 4) {
+      const cd wi(0.0, double(sign));
+      for (int k = 0; k < m; ++k) {
+        const cd a0 = out[k];
+        const cd a1 = out[m + k] * tw[size_t(k) * ts];
+        const cd a2 = out[2 * m + k] * tw[size_t(2 * k) * ts];
+        const cd a3 = out[3 * m + k] * tw[size_t(3 * k) * ts];
+        const cd t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, t3 = (a1 - a3) * wi;
+        out[k] = t0 + t2;
+        out[m + k] = t1 + t3;
+        out[2 * m + k] = t0 - t2;
+        out[3 * m + k] = t1 - t3;
+      }
+    } else {
+      std::vector<cd> a(p), r(p);
+      const int np = n / p;
+      for (int k = 0; k < m; ++k) {
+        for (int q = 0; q < p; ++q) a[q] = out[q * m + k] * tw[size_t(q) * k * ts];
+        for (int s = 0; s < p; ++s) {
+          cd acc = 0.0;
+          for (int q = 0; q < p; ++q) acc += a[q] * tw[size_t((q * s) % p) * np];
+          r[s] = acc;
+        }
+        for (int s = 0; s < p; ++s) out[k + m * s] = r[s];
+      }
+    }
+  }
+
+  void exec(const cd* in, long istride, cd* out) const { rec(in, istride, out, n, 0, 1); }
+};
+
+// In-place unnormalised multi-dimensional DFT, row-major dims (last fastest).
+void fft_nd(cd* data, const std::vector<int>& dims, int sign) {
+  const int r = int(dims.size());
+  size_t total = 1;
+  for (int d : dims) total *= size_t(d);
+  for (int a = 0; a < r; ++a) {
+    const int n = dims[a];
+    if (n == 1) continue;
+    size_t stride = 1;
+    for (int b = a + 1; b < r; ++b) stride *= size_t(dims[b]);
+    const size_t nlines = total / size_t(n);
+    Fft1 f(n, sign);
+#pragma omp parallel
+    {
+      std::vector<cd> buf(n), line(n);
+#pragma omp for schedule(static)
+      for (long li = 0; li < long(nlines); ++li) {
+        const size_t inner = size_t(li) % stride, outer = size_t(li) / stride;
+        cd* base = data + outer * stride * n + inner;
+        for (int j = 0; j < n; ++j) line[j] = base[size_t(j) * stride];
+        f.exec(line.data(), 1, buf.data());
+        for (int j = 0; j < n; ++j) base[size_t(j) * stride] = buf[j];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// ES kernel helpers
+// ---------------------------------------------------------------------------
+
+int64_t next235even(int64_t n) {
+  if (n < 2) n = 2;
+  if (n % 2) ++n;
+  for (;; n += 2) {
+    int64_t r = n;
+    for (int f : {2, 3, 5})
+      while (r % f == 0) r /= f;
+    if (r == 1) return n;
+  }
+}
+
+void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+  x.assign(n, 0.0);
+  w.assign(n, 0.0);
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    double z = std::cos(kPi * (i + 0.75) / (n + 0.5)), pp = 0.0;
+    for (int it = 0; it < 100; ++it) {
+      double p1 = 1.0, p2 = 0.0;
+      for (int j = 1; j <= n; ++j) {
+        const double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = n * (z * p1 - p2) / (z * z - 1.0);
+      const double dz = p1 / pp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    x[i] = -z;
+    x[n - 1 - i] = z;
+    w[i] = w[n - 1 - i] = 2.0 / ((1.0 - z * z) * pp * pp);
+  }
+}
+
+inline double es_phi(double t, double beta) {
+  const double a = 1.0 - t * t;
+  return a >= 0.0 ? std::exp(beta * (std::sqrt(a) - 1.0)) : 0.0;
+}
+
+// Fourier correction p(k) = psi_hat(k)/h for k = -n/2 .. (n-1)/2.
+std::vector<double> correction(int w, double beta, int64_t nf, int64_t n) {
+  const int nq = std::max(64, 8 * w + 64);
+  std::vector<double> xq, wq;
+  gauss_legendre(nq, xq, wq);
+  std::vector<double> out(n);
+  for (int64_t i = 0; i < n; ++i) {
+    const double k = double(i - n / 2);
+    double s = 0.0;
+    for (int q = 0; q < nq; ++q) s += wq[q] * es_phi(xq[q], beta) * std::cos(k * w * kPi / double(nf) * xq[q]);
+    out[i] = 0.5 * w * s;
+  }
+  return out;
+}
+
+// Kernel taps of a point at fractional cell offset f (see the device code).
+inline int taps(int w, double beta, double f, double* kv) {
+  const int s = (w % 2 == 0) ? (-w / 2 + (f > 0.0 ? 1 : 0)) : (-(w - 1) / 2 + (f > 0.5 ? 1 : 0));
+  for (int m = 0; m < w; ++m) kv[m] = es_phi((double(s + m) - f) * 2.0 / w, beta);
+  return s;
+}
+
+inline int64_t wrap(int64_t x, int64_t n) {
+  x %= n;
+  return x < 0 ? x + n : x;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// FINUFFT API
+// ---------------------------------------------------------------------------
+
+struct finufft_plan_s {
+  int type = 1, dim = 1, iflag = 1;
+  double tol = 1e-6;
+  int64_t nm[3] = {1, 1, 1};
+  int64_t M = 0, Nt = 0;
+  double* X[3] = {nullptr, nullptr, nullptr};
+  double* S[3] = {nullptr, nullptr, nullptr};
+  // ES set-up
+  int w = 7;
+  double beta = 16.1;
+  int64_t nf[3] = {1, 1, 1};
+  std::vector<double> corr[3];
+  std::vector<int64_t> cell;   // per point, per dim (M*dim)
+  std::vector<double> frac;    // per point, per dim
+  int tile = 32;
+  int64_t nb[3] = {1, 1, 1};
+  std::vector<int64_t> tstart;  // tile offsets into torder
+  std::vector<int64_t> torder;  // points sorted by tile
+};
+
+extern "C" void fresco_shim_set_mode(int mode) { g_mode = mode; }
+extern "C" int fresco_shim_get_mode(void) { return g_mode; }
+
+void finufft_default_opts(finufft_opts* o) {
+  if (!o) return;
+  o->modeord = 0;
+  o->debug = 0;
+  o->upsampfac = 2.0;
+}
+
+int finufft_makeplan(int type, int dim, int64_t* n_modes, int iflag, int ntrans, double tol, finufft_plan* plan,
+                     finufft_opts* o) {
+  if (type < 1 || type > 3 || dim < 1 || dim > 3 || ntrans != 1) return 1;
+  auto* p = new finufft_plan_s;
+  p->type = type;
+  p->dim = dim;
+  p->iflag = iflag >= 0 ? 1 : -1;
+  p->tol = tol;
+  if (type != 3)
+    for (int a = 0; a < dim; ++a) p->nm[a] = n_modes[a];
+  int w = int(std::ceil(-std::log10(tol / 10.0)));
+  w = std::max(2, std::min(16, w));
+  p->w = w;
+  double bw = 2.30;
+  if (w == 2) bw = 2.20;
+  else if (w == 3) bw = 2.26;
+  else if (w == 4) bw = 2.38;
+  p->beta = bw * w;
+  if (type != 3) {
+    for (int a = 0; a < dim; ++a) {
+      p->nf[a] = next235even(std::max<int64_t>(2 * p->nm[a], 2 * w));
+      p->corr[a] = correction(w, p->beta, p->nf[a], p->nm[a]);
+    }
+  }
+  *plan = p;
+  return 0;
+}
+
+namespace {
+
+bool use_exact(const finufft_plan_s* p) {
+  if (p->type == 3) return true;
+  if (g_mode == 1) return true;
+  if (g_mode == 2) return false;
+  double nmt = 1.0;
+  for (int a = 0; a < p->dim; ++a) nmt *= double(p->nm[a]);
+  return double(p->M) * nmt <= 2e7;
+}
+
+void es_setpts(finufft_plan_s* p) {
+  const int d = p->dim;
+  const int64_t M = p->M;
+  p->cell.assign(size_t(M) * d, 0);
+  p->frac.assign(size_t(M) * d, 0.0);
+  p->tile = std::max(p->w, d == 3 ? 16 : 32);
+  for (int a = 0; a < 3; ++a) p->nb[a] = a < d ? (p->nf[a] + p->tile - 1) / p->tile : 1;
+  const int64_t ntiles = p->nb[0] * p->nb[1] * p->nb[2];
+  std::vector<int64_t> tid(M);
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < M; ++j) {
+    int64_t b[3] = {0, 0, 0};
+    for (int a = 0; a < d; ++a) {
+      const double nfd = double(p->nf[a]);
+      double u = p->X[a][j] * (nfd / (2.0 * kPi));
+      u -= nfd * std::floor(u / nfd);
+      double fl = std::floor(u);
+      int64_t c = int64_t(fl);
+      double f = u - fl;
+      if (c >= p->nf[a]) c -= p->nf[a];
+      if (c < 0) c += p->nf[a];
+      p->cell[size_t(j) * d + a] = c;
+      p->frac[size_t(j) * d + a] = f;
+      b[a] = c / p->tile;
+    }
+    tid[j] = b[0] + p->nb[0] * (b[1] + p->nb[1] * b[2]);
+  }
+  p->tstart.assign(ntiles + 1, 0);
+  for (int64_t j = 0; j < M; ++j) p->tstart[tid[j] + 1]++;
+  for (int64_t t = 0; t < ntiles; ++t) p->tstart[t + 1] += p->tstart[t];
+  std::vector<int64_t> pos(p->tstart.begin(), p->tstart.end() - 1);
+  p->torder.resize(M);
+  for (int64_t j = 0; j < M; ++j) p->torder[pos[tid[j]]++] = j;
+}
+
+// Spreads complex strengths c onto the fine grid (row-major, dim 0 fastest).
+void es_spread(const finufft_plan_s* p, const cd* c, std::vector<cd>& grid) {
+  const int d = p->dim, w = p->w;
+  const int64_t nf0 = p->nf[0], nf1 = p->nf[1], nf2 = p->nf[2];
+  grid.assign(size_t(nf0 * nf1 * nf2), cd(0.0, 0.0));
+  auto color = [&](int64_t b, int a) -> int {
+    if (p->nb[a] % 2 == 1 && b == p->nb[a] - 1 && p->nb[a] > 1) return 2;
+    return int(b % 2);
+  };
+  for (int col = 0; col < 27; ++col) {
+    const int c0 = col % 3, c1 = (col / 3) % 3, c2 = col / 9;
+    std::vector<int64_t> tl;
+    for (int64_t b2 = 0; b2 < p->nb[2]; ++b2)
+      for (int64_t b1 = 0; b1 < p->nb[1]; ++b1)
+        for (int64_t b0 = 0; b0 < p->nb[0]; ++b0) {
+          if (color(b0, 0) != c0) continue;
+          if (d >= 2 && color(b1, 1) != c1) continue;
+          if (d < 2 && c1 != 0) continue;
+          if (d >= 3 && color(b2, 2) != c2) continue;
+          if (d < 3 && c2 != 0) continue;
+          tl.push_back(b0 + p->nb[0] * (b1 + p->nb[1] * b2));
+        }
+    if (tl.empty()) continue;
+#pragma omp parallel for schedule(dynamic)
+    for (long ti = 0; ti < long(tl.size()); ++ti) {
+      const int64_t t = tl[ti];
+      double k0[16], k1[16], k2[16];
+      int64_t i0[16], i1[16], i2[16];
+      for (int64_t q = p->tstart[t]; q < p->tstart[t + 1]; ++q) {
+        const int64_t j = p->torder[q];
+        const int s0 = taps(w, p->beta, p->frac[size_t(j) * d], k0);
+        for (int m = 0; m < w; ++m) i0[m] = wrap(p->cell[size_t(j) * d] + s0 + m, nf0);
+        int ny = 1, nz = 1;
+        k1[0] = k2[0] = 1.0;
+        i1[0] = i2[0] = 0;
+        if (d >= 2) {
+          const int s1 = taps(w, p->beta, p->frac[size_t(j) * d + 1], k1);
+          for (int m = 0; m < w; ++m) i1[m] = wrap(p->cell[size_t(j) * d + 1] + s1 + m, nf1);
+          ny = w;
+        }
+        if (d >= 3) {
+          const int s2 = taps(w, p->beta, p->frac[size_t(j) * d + 2], k2);
+          for (int m = 0; m < w; ++m) i2[m] = wrap(p->cell[size_t(j) * d + 2] + s2 + m, nf2);
+          nz = w;
+        }
+        const cd cj = c[j];
+        for (int mz = 0; mz < nz; ++mz)
+          for (int my = 0; my < ny; ++my) {
+            const cd v = cj * (k2[mz] * k1[my]);
+            cd* row = grid.data() + (i2[mz] * nf1 + i1[my]) * nf0;
+            for (int mx = 0; mx < w; ++mx) row[i0[mx]] += v * k0[mx];
+          }
+      }
+    }
+  }
+}
+
+void es_interp(const finufft_plan_s* p, const std::vector<cd>& grid, cd* c) {
+  const int d = p->dim, w = p->w;
+  const int64_t nf0 = p->nf[0], nf1 = p->nf[1], nf2 = p->nf[2];
+#pragma omp parallel for schedule(static)
+  for (int64_t q = 0; q < p->M; ++q) {
+    const int64_t j = p->torder[q];
+    double k0[16], k1[16], k2[16];
+    int64_t i0[16], i1[16], i2[16];
+    const int s0 = taps(w, p->beta, p->frac[size_t(j) * d], k0);
+    for (int m = 0; m < w; ++m) i0[m] = wrap(p->cell[size_t(j) * d] + s0 + m, nf0);
+    int ny = 1, nz = 1;
+    k1[0] = k2[0] = 1.0;
+    i1[0] = i2[0] = 0;
+    if (d >= 2) {
+      const int s1 = taps(w, p->beta, p->frac[size_t(j) * d + 1], k1);
+      for (int m = 0; m < w; ++m) i1[m] = wrap(p->cell[size_t(j) * d + 1] + s1 + m, nf1);
+      ny = w;
+    }
+    if (d >= 3) {
+      const int s2 = taps(w, p->beta, p->frac[size_t(j) * d + 2], k2);
+      for (int m = 0; m < w; ++m) i2[m] = wrap(p->cell[size_t(j) * d + 2] + s2 + m, nf2);
+      nz = w;
+    }
+    cd acc(0.0, 0.0);
+    for (int mz = 0; mz < nz; ++mz)
+      for (int my = 0; my < ny; ++my) {
+        const cd* row = grid.data() + (i2[mz] * nf1 + i1[my]) * nf0;
+        cd r(0.0, 0.0);
+        for (int mx = 0; mx < w; ++mx) r += row[i0[mx]] * k0[mx];
+        acc += r * (k2[mz] * k1[my]);
+      }
+    c[j] = acc;
+  }
+}
+
+std::vector<int> fft_dims(const finufft_plan_s* p) {
+  std::vector<int> dims;
+  for (int a = p->dim - 1; a >= 0; --a) dims.push_back(int(p->nf[a]));
+  return dims;
+}
+
+// mode index -> fine index and correction
+void es_type1(const finufft_plan_s* p, const cd* c, cd* f) {
+  std::vector<cd> grid;
+  es_spread(p, c, grid);
+  fft_nd(grid.data(), fft_dims(p), p->iflag);
+  const int64_t n0 = p->nm[0], n1 = p->nm[1], n2 = p->nm[2];
+#pragma omp parallel for schedule(static)
+  for (int64_t i2 = 0; i2 < n2; ++i2)
+    for (int64_t i1 = 0; i1 < n1; ++i1)
+      for (int64_t i0 = 0; i0 < n0; ++i0) {
+        const int64_t g0 = wrap(i0 - n0 / 2, p->nf[0]);
+        const int64_t g1 = p->dim >= 2 ? wrap(i1 - n1 / 2, p->nf[1]) : 0;
+        const int64_t g2 = p->dim >= 3 ? wrap(i2 - n2 / 2, p->nf[2]) : 0;
+        double pc = p->corr[0][i0];
+        if (p->dim >= 2) pc *= p->corr[1][i1];
+        if (p->dim >= 3) pc *= p->corr[2][i2];
+        f[i0 + n0 * (i1 + n1 * i2)] = grid[size_t((g2 * p->nf[1] + g1) * p->nf[0] + g0)] / pc;
+      }
+}
+
+void es_type2(const finufft_plan_s* p, cd* c, const cd* f) {
+  std::vector<cd> grid(size_t(p->nf[0] * p->nf[1] * p->nf[2]), cd(0.0, 0.0));
+  const int64_t n0 = p->nm[0], n1 = p->nm[1], n2 = p->nm[2];
+#pragma omp parallel for schedule(static)
+  for (int64_t i2 = 0; i2 < n2; ++i2)
+    for (int64_t i1 = 0; i1 < n1; ++i1)
+      for (int64_t i0 = 0; i0 < n0; ++i0) {
+        const int64_t g0 = wrap(i0 - n0 / 2, p->nf[0]);
+        const int64_t g1 = p->dim >= 2 ? wrap(i1 - n1 / 2, p->nf[1]) : 0;
+        const int64_t g2 = p->dim >= 3 ? wrap(i2 - n2 / 2, p->nf[2]) : 0;
+        double pc = p->corr[0][i0];
+        if (p->dim >= 2) pc *= p->corr[1][i1];
+        if (p->dim >= 3) pc *= p->corr[2][i2];
+        grid[size_t((g2 * p->nf[1] + g1) * p->nf[0] + g0)] = f[i0 + n0 * (i1 + n1 * i2)] / pc;
+      }
+  fft_nd(grid.data(), fft_dims(p), p->iflag);
+  es_interp(p, grid, c);
+}
+
+// exact direct sums
+void phase_table(const double* x, int64_t M, int64_t n, int iflag, std::vector<cd>& E) {
+  E.resize(size_t(M * n));
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < M; ++j)
+    for (int64_t i = 0; i < n; ++i) {
+      const double a = iflag * double(i - n / 2) * x[j];
+      E[size_t(j * n + i)] = cd(std::cos(a), std::sin(a));
+    }
+}
+
+void exact_type1(const finufft_plan_s* p, const cd* c, cd* f) {
+  const int d = p->dim;
+  const int64_t n0 = p->nm[0], n1 = p->nm[1], n2 = p->nm[2], M = p->M;
+  std::vector<cd> E0, E1, E2;
+  phase_table(p->X[0], M, n0, p->iflag, E0);
+  if (d >= 2) phase_table(p->X[1], M, n1, p->iflag, E1);
+  if (d >= 3) phase_table(p->X[2], M, n2, p->iflag, E2);
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int64_t i2 = 0; i2 < n2; ++i2)
+    for (int64_t i1 = 0; i1 < n1; ++i1) {
+      std::vector<cd> row(n0, cd(0.0, 0.0));
+      for (int64_t j = 0; j < M; ++j) {
+        cd v = c[j];
+        if (d >= 2) v *= E1[size_t(j * n1 + i1)];
+        if (d >= 3) v *= E2[size_t(j * n2 + i2)];
+        const cd* e0 = E0.data() + j * n0;
+        for (int64_t i0 = 0; i0 < n0; ++i0) row[i0] += v * e0[i0];
+      }
+      for (int64_t i0 = 0; i0 < n0; ++i0) f[i0 + n0 * (i1 + n1 * i2)] = row[i0];
+    }
+}
+
+void exact_type2(const finufft_plan_s* p, cd* c, const cd* f) {
+  const int d = p->dim;
+  const int64_t n0 = p->nm[0], n1 = p->nm[1], n2 = p->nm[2], M = p->M;
+#pragma omp parallel
+  {
+    std::vector<cd> e0(n0), e1(n1), e2(n2);
+#pragma omp for schedule(static)
+    for (int64_t j = 0; j < M; ++j) {
+      for (int64_t i = 0; i < n0; ++i) {
+        const double a = p->iflag * double(i - n0 / 2) * p->X[0][j];
+        e0[i] = cd(std::cos(a), std::sin(a));
+      }
+      for (int64_t i = 0; i < n1; ++i) {
+        const double a = d >= 2 ? p->iflag * double(i - n1 / 2) * p->X[1][j] : 0.0;
+        e1[i] = cd(std::cos(a), std::sin(a));
+      }
+      for (int64_t i = 0; i < n2; ++i) {
+        const double a = d >= 3 ? p->iflag * double(i - n2 / 2) * p->X[2][j] : 0.0;
+        e2[i] = cd(std::cos(a), std::sin(a));
+      }
+      cd acc(0.0, 0.0);
+      for (int64_t i2 = 0; i2 < n2; ++i2)
+        for (int64_t i1 = 0; i1 < n1; ++i1) {
+          cd r(0.0, 0.0);
+          const cd* fr = f + n0 * (i1 + n1 * i2);
+          for (int64_t i0 = 0; i0 < n0; ++i0) r += fr[i0] * e0[i0];
+          acc += r * e1[i1] * e2[i2];
+        }
+      c[j] = acc;
+    }
+  }
+}
+
+void exact_type3(const finufft_plan_s* p, const cd* c, cd* f) {
+  const int d = p->dim;
+#pragma omp parallel for schedule(static)
+  for (int64_t k = 0; k < p->Nt; ++k) {
+    cd acc(0.0, 0.0);
+    for (int64_t j = 0; j < p->M; ++j) {
+      double ph = p->S[0][k] * p->X[0][j];
+      if (d >= 2) ph += p->S[1][k] * p->X[1][j];
+      if (d >= 3) ph += p->S[2][k] * p->X[2][j];
+      ph *= p->iflag;
+      acc += c[j] * cd(std::cos(ph), std::sin(ph));
+    }
+    f[k] = acc;
+  }
+}
+
+}  // namespace
+
+int finufft_setpts(finufft_plan plan, int64_t M, double* x, double* y, double* z, int64_t N, double* s, double* t,
+                   double* u) {
+  if (!plan) return 1;
+  plan->M = M;
+  plan->X[0] = x;
+  plan->X[1] = y;
+  plan->X[2] = z;
+  if (plan->type == 3) {
+    plan->Nt = N;
+    plan->S[0] = s;
+    plan->S[1] = t;
+    plan->S[2] = u;
+  }
+  if (!use_exact(plan)) es_setpts(plan);
+  return 0;
+}
+
+int finufft_execute(finufft_plan plan, std::complex<double>* weights, std::complex<double>* result) {
+  if (!plan) return 1;
+  if (plan->type == 3) {
+    exact_type3(plan, weights, result);
+  } else if (use_exact(plan)) {
+    if (plan->type == 1) exact_type1(plan, weights, result);
+    else exact_type2(plan, weights, result);
+  } else {
+    if (plan->cell.size() != size_t(plan->M * plan->dim)) es_setpts(plan);
+    if (plan->type == 1) es_type1(plan, weights, result);
+    else es_type2(plan, weights, result);
+  }
+  return 0;
+}
+
+int finufft_destroy(finufft_plan plan) {
+  delete plan;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// FFTW API
+// ---------------------------------------------------------------------------
+
+struct fftw_plan_s {
+  std::vector<int> dims;
+  fftw_complex* in = nullptr;
+  fftw_complex* out = nullptr;
+  int sign = -1;
+};
+
+void* fftw_malloc(size_t n) { return std::malloc(n); }
+void fftw_free(void* p) { std::free(p); }
+
+fftw_plan fftw_plan_dft(int rank, const int* n, fftw_complex* in, fftw_complex* out, int sign, unsigned flags) {
+  (void)flags;
+  auto* p = new fftw_plan_s;
+  p->dims.assign(n, n + rank);
+  p->in = in;
+  p->out = out;
+  p->sign = sign;
+  return p;
+}
+
+void fftw_execute(const fftw_plan p) {
+  size_t total = 1;
+  for (int d : p->dims) total *= size_t(d);
+  cd* out = reinterpret_cast<cd*>(p->out);
+  if (p->out != p->in) std::memcpy(out, p->in, total * sizeof(cd));
+  fft_nd(out, p->dims, p->sign);
+}
+
+void fftw_destroy_plan(fftw_plan p) { delete p; }

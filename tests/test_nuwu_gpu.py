@@ -1,0 +1,122 @@
+"""NUwU on the device against the oracle (exact FP64 direct sums of the reference's formulas)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+# (precision, eps, relative tolerance on energy and on the gradient's 2-norm)
+PRECISIONS = [("fp64", 1e-12, 1e-10), ("fp32", 1e-6, 1e-5)]
+
+
+def _inputs(ndim, N, K, kmax, seed, L=None, random_weights=False, radii_spread=True):
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(N, K, kmax, ndim=ndim, seed=seed, L=L)
+    rng = np.random.default_rng(seed + 100)
+    if radii_spread:
+        radii = 0.5 + rng.random(N)
+    if random_weights:
+        V = rng.random(V.shape) * (rng.random(V.shape) < 0.7)
+        Sk = rng.random(Sk.shape) * 2.0 * (rng.random(Sk.shape) < 0.5)
+    return x, radii, Sk, V, L
+
+
+def _check(pot, ref, x, tol):
+    e_ref, g_ref = ref.get_energy_gradient(x)
+    e, g = pot.get_energy_gradient(x)
+    assert abs(e - e_ref) <= tol * abs(e_ref), (e, e_ref)
+    err = np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref)
+    assert err <= tol, err
+    e2 = pot.get_energy(x)
+    assert abs(e2 - ref.get_energy(x)) <= tol * abs(e_ref)
+    assert pot.status() == 0
+
+
+@pytest.mark.parametrize("prec,eps,tol", PRECISIONS)
+@pytest.mark.parametrize("ndim,N,K,kmax", [(2, 400, 10, 8), (3, 150, 4, 3), (1, 120, 24, 18)])
+def test_nuwu_stealthy(prec, eps, tol, ndim, N, K, kmax):
+    from fresco_b200 import NUwU
+
+    x, radii, Sk, V, L = _inputs(ndim, N, K, kmax, seed=ndim)
+    ref = O.NUwU(radii, K, Sk, V, L)
+    pot = NUwU(radii, K, Sk, V, L, eps=eps, precision=prec)
+    _check(pot, ref, x, tol)
+
+
+@pytest.mark.parametrize("prec,eps,tol", PRECISIONS)
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_nuwu_asymmetric_targets(prec, eps, tol, ndim):
+    """V and S0 with no k <-> -k symmetry and S0 != 0 entries (exercises the Hermitian packing)."""
+    from fresco_b200 import NUwU
+
+    N, K = (300, 7) if ndim == 2 else (120, 3)
+    x, radii, Sk, V, L = _inputs(ndim, N, K, K, seed=11 + ndim, random_weights=True)
+    ref = O.NUwU(radii, K, Sk, V, L)
+    pot = NUwU(radii, K, Sk, V, L, eps=eps, precision=prec)
+    _check(pot, ref, x, tol)
+
+
+@pytest.mark.parametrize("L", [1.0, 2 * np.pi, 3.7])
+def test_nuwu_box_map_quirk(L):
+    """Points inside and outside the box under the reference's coordinate map (nuwu.hpp:216-250)."""
+    from fresco_b200 import NUwU
+
+    rng = np.random.default_rng(5)
+    N, K = 200, 6
+    x, radii, Sk, V, Lv = _inputs(2, N, K, 5, seed=5, L=np.full(2, L))
+    x = x + rng.normal(scale=L, size=x.shape)  # points far outside [0, L)
+    ref = O.NUwU(radii, K, Sk, V, Lv)
+    pot = NUwU(radii, K, Sk, V, Lv, eps=1e-12)
+    _check(pot, ref, x, 1e-10)
+
+
+def test_nuwu_nonfinite_input():
+    from fresco_b200 import NUwU
+
+    x, radii, Sk, V, L = _inputs(2, 50, 4, 3, seed=9)
+    pot = NUwU(radii, 4, Sk, V, L)
+    x[7] = np.nan
+    e, g = pot.get_energy_gradient(x)
+    assert np.isnan(e) and np.all(np.isnan(g))
+    assert pot.status() & 1
+    x[7] = 0.3
+    e, g = pot.get_energy_gradient(x)
+    assert np.isfinite(e) and np.all(np.isfinite(g))
+    assert pot.status() == 0
+
+
+def test_nuwu_no_active_modes_and_empty_weights():
+    from fresco_b200 import NUwU
+
+    x, radii, Sk, V, L = _inputs(2, 30, 3, 2, seed=4)
+    pot = NUwU(radii, 3, Sk, np.zeros_like(V), L)
+    e, g = pot.get_energy_gradient(x)
+    assert e == 0.0 and np.all(g == 0.0)
+
+
+def test_nuwu_device_path_matches_host_path():
+    import torch
+
+    from fresco_b200 import NUwU
+
+    x, radii, Sk, V, L = _inputs(2, 500, 12, 10, seed=3)
+    pot = NUwU(radii, 12, Sk, V, L, eps=1e-10)
+    e_h, g_h = pot.get_energy_gradient(x)
+    xt = torch.tensor(x, device="cuda")
+    e_d, g_d = pot.energy_gradient_device(xt)
+    torch.cuda.synchronize()
+    assert abs(e_d.item() - e_h) <= 1e-12 * abs(e_h)
+    assert np.allclose(g_d.cpu().numpy(), g_h, rtol=1e-11, atol=1e-11 * np.abs(g_h).max())
+
+
+def test_nuwu_bad_arguments():
+    from fresco_b200 import NUwU
+
+    x, radii, Sk, V, L = _inputs(2, 20, 3, 2, seed=1)
+    with pytest.raises(AssertionError):
+        NUwU(radii, 3, Sk[:-1], V, L)
+    pot = NUwU(radii, 3, Sk, V, L)
+    with pytest.raises(ValueError):
+        pot.get_energy_gradient(x[:-1])
+    with pytest.raises(ValueError):
+        NUwU(radii, 3, Sk, V, L, precision="fp16")
