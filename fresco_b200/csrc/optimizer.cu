@@ -620,8 +620,9 @@ class Fire final : public Optimizer {
     init_from_gradient();
   }
 
+  // As modified_fire.hpp:160-178, no initialisation here: before run() the
+  // step starts from f = 0, g = 0 (LBFGS initialises, lbfgs.cpp:38-40).
   void one_iteration() override {
-    if (!func_initialized_) initialize_func_gradient();
     ++nfev_;
     ++iter_;
     fi_mix<<<P_, kThreads, 0, s_>>>(V_.p, G_.p, n_, st_.p, part_.p, P_);

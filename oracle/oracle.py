@@ -550,8 +550,8 @@ class ModifiedFire:
         return self.rms <= self.tol
 
     def one_iteration(self):
-        if not self.init:
-            self._initialize()
+        # modified_fire.hpp:160-178 does not initialise f and g here (LBFGS
+        # does, lbfgs.cpp:38-40): before run() it steps from f = 0, g = 0.
         self.nfev += 1
         self.iter += 1
         self.fire_iter += 1

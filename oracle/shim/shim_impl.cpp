@@ -9,8 +9,8 @@
 //    beta = 2.30 w, correction by Gauss-Legendre quadrature of the kernel's
 //    Fourier transform.  Spreading uses a tile colouring so that OpenMP
 //    threads never write the same grid cell; everything is FP64.
-//  * the FFT is a mixed-radix Cooley-Tukey (radix 4, 2 and generic odd
-//    primes) on the CPU.
+//  * the FFT is a self-sorting mixed-radix (4, 2, 3 and generic odd primes)
+//    transform on the CPU.
 #include <omp.h>
 
 #include <algorithm>
@@ -18,6 +18,8 @@
 #include <complex>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
+#include <mutex>
 #include <vector>
 
 #include "fftw3.h"
@@ -34,6 +36,11 @@ int g_mode = 0;  // 0 auto, 1 exact, 2 ES
 // mixed-radix FFT
 // ---------------------------------------------------------------------------
 
+// Self-sorting (Stockham) mixed-radix FFT.  Stage t splits each of the s
+// current sub-transforms of length L = p m as j = j1 + m j2, k = p k1 + k2:
+//   C[j1 s p + s k2 + q] = W_L^(j1 k2) sum_j2 B[(j1 + m j2) s + q] W_p^(j2 k2),
+// so the sub-transform index q stays the fastest-varying part of the output
+// index and no bit reversal is needed.
 struct Fft1 {
   int n = 1;
   int sign = 1;
@@ -54,53 +61,85 @@ struct Fft1 {
     if (r > 1) fac.push_back(r);
   }
 
-  void rec(const cd* in, long istride, cd* out, int m_n, size_t fi, int ts) const {
-    if (m_n == 1) {
-      out[0] = in[0];
-      return;
-    }
-    const int p = fac[fi];
-    const int m = m_n / p;
-    for (int q = 0; q < p; ++q) rec(in + q * istride, istride * p, out + q * m, m, fi + 1, ts * p);
-    if (p == 2) {
-      for (int k = 0; k < m; ++k) {
-        const cd a = out[k], b = out[m + k] * tw[size_t(k) * ts];
-        out[k] = a + b;
-        out[m + k] = a - b;
-      }
-    } else if (p == 4) {
-      const cd wi(0.0, double(sign));
-      for (int k = 0; k < m; ++k) {
-        const cd a0 = out[k];
-        const cd a1 = out[m + k] * tw[size_t(k) * ts];
-        const cd a2 = out[2 * m + k] * tw[size_t(2 * k) * ts];
-        const cd a3 = out[3 * m + k] * tw[size_t(3 * k) * ts];
-        const cd t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, t3 = (a1 - a3) * wi;
-        out[k] = t0 + t2;
-        out[m + k] = t1 + t3;
-        out[2 * m + k] = t0 - t2;
-        out[3 * m + k] = t1 - t3;
-      }
-    } else {
-      std::vector<cd> a(p), r(p);
-      const int np = n / p;
-      for (int k = 0; k < m; ++k) {
-        for (int q = 0; q < p; ++q) a[q] = out[q * m + k] * tw[size_t(q) * k * ts];
-        for (int s = 0; s < p; ++s) {
-          cd acc = 0.0;
-          for (int q = 0; q < p; ++q) acc += a[q] * tw[size_t((q * s) % p) * np];
-          r[s] = acc;
+  // In-place transform of a contiguous array; work holds n elements.
+  void exec(cd* x, cd* work) const {
+    cd* a = x;
+    cd* b = work;
+    long s = 1, L = n;
+    const cd wi(0.0, double(sign));
+    const double s3 = sign * 0.86602540378443864676;
+    std::vector<cd> gen;
+    for (int p : fac) {
+      const long m = L / p;
+      if (p > 4 && p != 3 && int(gen.size()) < p) gen.resize(2 * p);
+      for (long j1 = 0; j1 < m; ++j1) {
+        const cd* in = a + j1 * s;
+        cd* out = b + j1 * s * p;
+        if (p == 4) {
+          const cd w1 = tw[size_t(j1 * s)], w2 = tw[size_t(2 * j1 * s)], w3 = tw[size_t(3 * j1 * s)];
+          for (long q = 0; q < s; ++q) {
+            const cd u0 = in[q], u1 = in[m * s + q], u2 = in[2 * m * s + q], u3 = in[3 * m * s + q];
+            const cd t0 = u0 + u2, t1 = u0 - u2, t2 = u1 + u3, t3 = (u1 - u3) * wi;
+            out[q] = t0 + t2;
+            out[s + q] = (t1 + t3) * w1;
+            out[2 * s + q] = (t0 - t2) * w2;
+            out[3 * s + q] = (t1 - t3) * w3;
+          }
+        } else if (p == 2) {
+          const cd w1 = tw[size_t(j1 * s)];
+          for (long q = 0; q < s; ++q) {
+            const cd u0 = in[q], u1 = in[m * s + q];
+            out[q] = u0 + u1;
+            out[s + q] = (u0 - u1) * w1;
+          }
+        } else if (p == 3) {
+          const cd w1 = tw[size_t(j1 * s)], w2 = tw[size_t(2 * j1 * s)];
+          for (long q = 0; q < s; ++q) {
+            const cd u0 = in[q], u1 = in[m * s + q], u2 = in[2 * m * s + q];
+            const cd t1 = u1 + u2, t2 = u0 - 0.5 * t1, t3 = (u1 - u2) * cd(0.0, s3);
+            out[q] = u0 + t1;
+            out[s + q] = (t2 + t3) * w1;
+            out[2 * s + q] = (t2 - t3) * w2;
+          }
+        } else {
+          cd* u = gen.data();
+          cd* v = gen.data() + p;
+          const int np = n / p;
+          for (long q = 0; q < s; ++q) {
+            for (int j2 = 0; j2 < p; ++j2) u[j2] = in[j2 * m * s + q];
+            for (int k2 = 0; k2 < p; ++k2) {
+              cd acc = 0.0;
+              for (int j2 = 0; j2 < p; ++j2) acc += u[j2] * tw[size_t((j2 * k2) % p) * np];
+              v[k2] = acc;
+            }
+            for (int k2 = 0; k2 < p; ++k2) out[s * k2 + q] = v[k2] * tw[size_t(j1 * k2 * s)];
+          }
         }
-        for (int s = 0; s < p; ++s) out[k + m * s] = r[s];
       }
+      std::swap(a, b);
+      s *= p;
+      L = m;
     }
+    if (a != x) std::memcpy(x, a, sizeof(cd) * n);
   }
-
-  void exec(const cd* in, long istride, cd* out) const { rec(in, istride, out, n, 0, 1); }
 };
 
+// Twiddle tables are built once per (size, sign).
+const Fft1& fft_plan_cached(int n, int sign) {
+  static std::vector<std::unique_ptr<Fft1>> cache;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  for (auto& f : cache)
+    if (f->n == n && f->sign == sign) return *f;
+  cache.emplace_back(new Fft1(n, sign));
+  return *cache.back();
+}
+
 // In-place unnormalised multi-dimensional DFT, row-major dims (last fastest).
+// Lines along a strided axis are gathered in blocks of kBlk neighbouring
+// lines so that every cache line read is fully used.
 void fft_nd(cd* data, const std::vector<int>& dims, int sign) {
+  constexpr int kBlk = 16;
   const int r = int(dims.size());
   size_t total = 1;
   for (int d : dims) total *= size_t(d);
@@ -109,18 +148,35 @@ void fft_nd(cd* data, const std::vector<int>& dims, int sign) {
     if (n == 1) continue;
     size_t stride = 1;
     for (int b = a + 1; b < r; ++b) stride *= size_t(dims[b]);
-    const size_t nlines = total / size_t(n);
-    Fft1 f(n, sign);
+    const size_t nouter = total / (size_t(n) * stride);
+    const Fft1& f = fft_plan_cached(n, sign);
+    if (stride == 1) {
+#pragma omp parallel
+      {
+        std::vector<cd> work(n);
+#pragma omp for schedule(static)
+        for (long li = 0; li < long(nouter); ++li) f.exec(data + size_t(li) * n, work.data());
+      }
+      continue;
+    }
+    const size_t nblk = (stride + kBlk - 1) / kBlk;
 #pragma omp parallel
     {
-      std::vector<cd> buf(n), line(n);
+      std::vector<cd> blk(size_t(n) * kBlk), line(n), work(n);
 #pragma omp for schedule(static)
-      for (long li = 0; li < long(nlines); ++li) {
-        const size_t inner = size_t(li) % stride, outer = size_t(li) / stride;
-        cd* base = data + outer * stride * n + inner;
-        for (int j = 0; j < n; ++j) line[j] = base[size_t(j) * stride];
-        f.exec(line.data(), 1, buf.data());
-        for (int j = 0; j < n; ++j) base[size_t(j) * stride] = buf[j];
+      for (long bi = 0; bi < long(nouter * nblk); ++bi) {
+        const size_t outer = size_t(bi) / nblk, i0 = (size_t(bi) % nblk) * kBlk;
+        const int w = int(std::min<size_t>(kBlk, stride - i0));
+        cd* base = data + outer * stride * n + i0;
+        for (int j = 0; j < n; ++j)
+          for (int b = 0; b < w; ++b) blk[size_t(j) * kBlk + b] = base[size_t(j) * stride + b];
+        for (int b = 0; b < w; ++b) {
+          for (int j = 0; j < n; ++j) line[j] = blk[size_t(j) * kBlk + b];
+          f.exec(line.data(), work.data());
+          for (int j = 0; j < n; ++j) blk[size_t(j) * kBlk + b] = line[j];
+        }
+        for (int j = 0; j < n; ++j)
+          for (int b = 0; b < w; ++b) base[size_t(j) * stride + b] = blk[size_t(j) * kBlk + b];
       }
     }
   }
