@@ -1,0 +1,375 @@
+"""Benchmark: NUwU loss+gradient evaluations per second on B200.
+
+Workload (one "step" = one NUwU ``get_energy_gradient``): 2D NUwU with
+N = 1,048,576 seeded uniform points in [0, 2 pi)^2, a 1025 x 1025 mode grid
+(K = 512; the reference supports only odd grids), target S0(k) = 0 for
+0 < |k| <= 256 with weight 1, unconstrained elsewhere, L = 2 pi, eps = 1e-6,
+in the FP32 spread/FFT/interpolation form with FP64 reductions.  Synthetic
+seeded inputs stand in for data (the reference uses none).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank evaluates its own independent pattern (the
+batched-ensemble sharding: no data-path collective), timing is the max over
+ranks and ``value`` aggregates all ranks.  ``--impl reference`` times the
+reference's own CPU implementation (its C++ compiled unchanged against the
+FINUFFT-API shim backed by the CPU ES-kernel NUFFT restatement) on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "NUwU loss+grad evals/s, 2D N=1M: FP32 vs FP64 on B200 at ≤1e-5 grad rel err"
+N_POINTS = 1 << 20
+K_MODES = 512
+K_CONSTRAINED = 256
+EPS = 1e-6
+L2_FLUSH_BYTES = 256 << 20
+
+WORKLOAD = (
+    "2D NUwU loss+grad: N=1048576 seeded uniform points in [0,2pi)^2, 1025x1025 modes (K=512), "
+    "S0=0 & V=1 on 0<|k|<=256, L=2pi, eps=1e-6"
+)
+
+
+def inputs(seed):
+    from oracle import oracle as O
+
+    return O.stealthy_nuwu_inputs(N_POINTS, K_MODES, K_CONSTRAINED, ndim=2, seed=seed)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """Samples nvidia-smi clocks/throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_bytes(geom_nf, n_active, N, s_r, s_c, s_w, d=2, d_f=2):
+    """Per-eval algorithmic bytes (SURVEY 8(d) formula) and per-kernel figures."""
+    G = geom_nf * geom_nf
+    n_modes = (2 * K_MODES + 1) ** 2
+    b_points = N * (4 * d * s_r + 12)
+    b_grid = G * s_c * (3 + 4 * d_f)
+    b_modes = n_modes * (s_c + 2 * s_w)
+    per_kernel = {
+        # read x (d doubles), write the sorted record (cell, d fractions, index)
+        "sort": N * (8 * d + 4 + d * s_r + 4),
+        # read the sorted record, write the real fine grid
+        "spread": N * (4 + d * s_r + s_r) + G * s_r,
+        # real-to-complex FFT: read G reals, write G/2 complex
+        "fft_type1": G * s_r + (G // 2) * s_c,
+        # active modes: read rho + coefficients (idx + 4 doubles), write the packed field
+        "modes": n_active * (s_c + 4 + 32 + s_c),
+        # complex FFT of the packed field
+        "fft_type2": 2 * G * s_c,
+        # read the sorted record and the packed grid, write the gradient
+        "interp": N * (4 + d * s_r + s_r + 4 + 8 * d) + G * s_c,
+    }
+    return b_points + b_grid + b_modes, per_kernel
+
+
+def run_ours(args):
+    import torch
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    import fresco_b200
+    from fresco_b200 import NUwU
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    x, radii, Sk, V, L = inputs(seed=2 + rank)
+    pot32 = NUwU(radii, K_MODES, Sk, V, L, eps=EPS, precision="fp32")
+    desc = pot32.describe()
+    nf = int(desc.split("nf=")[1].split("x")[0])
+    n_active = int(desc.split("active_modes=")[1].split()[0])
+    xt = torch.tensor(x, device=dev)
+    g = torch.empty_like(xt)
+    e = torch.zeros((), dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed_loop(pot, steps, warmup, record_stages=False):
+        for _ in range(warmup):
+            pot.energy_gradient_device(xt, g, e)
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        if record_stages:
+            pot.set_timing(True)
+        total = 0.0
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.fill_(float(i))  # write > L2 between timed steps
+            evs[i][0].record(stream)
+            pot.energy_gradient_device(xt, g, e)
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        for a, b in evs:
+            total += a.elapsed_time(b)
+        if ws > 1:
+            torch.distributed.barrier()
+        stages = pot.get_timing() if record_stages else {}
+        if record_stages:
+            pot.set_timing(False)
+        return total, stages
+
+    clocks = Clocks(local)
+    clocks.start()
+    t32_ms, stages = timed_loop(pot32, args.steps, args.warmup, record_stages=True)
+    clk = clocks.stop()
+    e32 = float(e.item())
+    g32 = g.clone()
+
+    # slowest rank decides the job time
+    tt = torch.tensor([t32_ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+    t_job_ms = float(tt.item())
+    ms_per_step = t_job_ms / args.steps
+    value = ws * args.steps / (t_job_ms / 1000.0)
+
+    # FP64 form (same eps) and the FP64 reference gradient (eps = 1e-12)
+    pot64 = NUwU(radii, K_MODES, Sk, V, L, eps=EPS, precision="fp64")
+    t64_ms, _ = timed_loop(pot64, max(3, args.steps // 2), 2)
+    ms64 = t64_ms / max(3, args.steps // 2)
+    g64 = g.clone()
+    potref = NUwU(radii, K_MODES, Sk, V, L, eps=1e-12, precision="fp64")
+    potref.energy_gradient_device(xt, g, e)
+    torch.cuda.synchronize()
+    eref = float(e.item())
+    gref = g.clone()
+    err32 = float(torch.linalg.norm(g32 - gref) / torch.linalg.norm(gref))
+    err64 = float(torch.linalg.norm(g64 - gref) / torch.linalg.norm(gref))
+    eerr32 = abs(e32 - eref) / abs(eref)
+    del potref
+
+    # end to end through the public API: pinned host x in, host gradient out
+    x_host = torch.tensor(x).pin_memory().numpy()
+    for _ in range(2):
+        pot32.get_energy_gradient(x_host)
+    torch.cuda.synchronize()
+    ne2e = max(5, args.steps)
+    t0 = time.perf_counter()
+    for _ in range(ne2e):
+        eh, gh = pot32.get_energy_gradient(x_host)
+    e2e_s = (time.perf_counter() - t0) / ne2e
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if ws > 1:
+        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = ws / float(e2e_t.item())
+
+    # roofline: per-stage device times from CUDA events on the launch stream
+    b_eval, per_kernel = algorithmic_bytes(nf, n_active, N_POINTS, 4, 8, 8)
+    stage_ms = {k: v[0] / max(v[1], 1) for k, v in stages.items()}
+    top = max(stage_ms, key=stage_ms.get) if stage_ms else "spread"
+    top_ms = stage_ms.get(top, ms_per_step)
+    achieved = per_kernel.get(top, b_eval) / (top_ms * 1e-3) / 1e9
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        traffic = prof.get(top)
+    except Exception:
+        pass
+    roofline = {"kernel": top, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(achieved / hbm_peak, 4), "traffic": traffic, "peak_source": peak_src,
+                "algorithmic_bytes": per_kernel.get(top)}
+    eval_achieved = b_eval / (ms_per_step * 1e-3) / 1e9
+    roofline_eval = {"bound": "hbm", "algorithmic_bytes": b_eval, "achieved": round(eval_achieved, 1),
+                     "peak": hbm_peak, "unit": "GB/s", "frac": round(eval_achieved / hbm_peak, 4)}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline(x, radii, Sk, V, L, samples=args.cpu_samples)
+
+    # kernels of ours per eval: bin_count, build_subproblems, scatter, spread, modes, interp
+    launches = 6 * args.steps
+    out = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "evals/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_per_step, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded uniform points, rank r uses seed 2+r)",
+        "config": {"workload": WORKLOAD, "precision": "fp32 spread/FFT/interp, fp64 loss reduction",
+                   "setup": desc, "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"independent pattern per GPU x{ws}"},
+        "e2e": {"value": round(e2e_value, 2), "unit": "evals/s", "h2d_bytes_per_step": int(x.nbytes),
+                "d2h_bytes_per_step": int(x.nbytes + 8)},
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "roofline_eval": roofline_eval,
+        "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+        "fp64": {"evals_per_s": round(ws * 1000.0 / ms64, 2), "ms_per_step": round(ms64, 5),
+                 "fp32_over_fp64": round(ms64 / ms_per_step, 3)},
+        "accuracy": {"grad_rel_err_fp32": err32, "grad_rel_err_fp64_eps1e-6": err64, "energy_rel_err_fp32": eerr32,
+                     "oracle": "GPU FP64 form at eps=1e-12 (parity-tested against exact sums)"},
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    del pot32, pot64
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def cpu_baseline(x, radii, Sk, V, L, samples=2):
+    """The reference's CPU path on this host (oracle/_ref, ES-kernel NUFFT shim, all cores)."""
+    try:
+        from oracle import refimpl as R
+
+        if not R.available():
+            return {"value": None, "unit": "evals/s", "cores": 0, "kind": "reference", "sample": "oracle/_ref missing"}
+        R.set_mode(R.ES)
+        cores = R.host_cores()
+        R.set_threads(cores)
+        p = R.NUwU(radii, K_MODES, Sk, V, L, eps=EPS)
+        p.get_energy_gradient(x)
+        t0 = time.perf_counter()
+        for _ in range(samples):
+            p.get_energy_gradient(x)
+        dt = (time.perf_counter() - t0) / samples
+        return {"value": round(1.0 / dt, 4), "unit": "evals/s", "cores": cores, "kind": "reference",
+                "sample": f"{samples} evals of the full workload after 1 warm-up; reference nuwu.hpp compiled "
+                          "unchanged against the FINUFFT-API shim (CPU ES-kernel NUFFT restatement, FP64, "
+                          "eps=1e-6), not FINUFFT itself"}
+    except Exception as ex:  # the baseline is reported, never fatal
+        return {"value": None, "unit": "evals/s", "cores": 0, "kind": "reference", "sample": f"failed: {ex}"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import refimpl as R
+
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfresco_ref.so not built"}))
+        return
+    R.set_mode(R.ES)
+    cores = R.host_cores()
+    R.set_threads(cores)
+    x, radii, Sk, V, L = inputs(seed=2)
+    p = R.NUwU(radii, K_MODES, Sk, V, L, eps=EPS)
+    for _ in range(max(1, min(args.warmup, 2))):
+        p.get_energy_gradient(x)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        p.get_energy_gradient(x)
+    dt = time.perf_counter() - t0
+    value = args.steps / dt
+    sample = (f"{args.steps} full evals of the workload (reference nuwu.hpp compiled unchanged against the "
+              f"FINUFFT-API shim: CPU ES-kernel NUFFT restatement, FP64, eps=1e-6; FINUFFT itself is not "
+              f"installable here)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "evals/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * dt / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded uniform points, seed 2)",
+        "config": {"workload": WORKLOAD, "precision": "fp64 (reference)", "parallelism": f"{cores} host threads"},
+        "cpu_baseline": {"value": round(value, 4), "unit": "evals/s", "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-samples", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -229,10 +229,12 @@ int fresco_potential_status(fresco_potential p, void* stream, int* status) {
 int fresco_potential_set_timing(fresco_potential p, int enabled) {
   return guarded([&] {
     if (!p) throw fb::InvalidArgument("null handle");
-    p->pot->timer.enabled = enabled != 0;
     auto& t = p->pot->timer;
-    std::fill(t.total_ms.begin(), t.total_ms.end(), 0.0);
-    std::fill(t.count.begin(), t.count.end(), 0);
+    t.enabled = enabled != 0;
+    t.used = 0;
+    t.total_names.clear();
+    t.total_ms.clear();
+    t.count.clear();
     return FRESCO_OK;
   });
 }
@@ -244,9 +246,9 @@ int fresco_potential_get_timing(fresco_potential p, int max_stages, char* names,
     p->pot->timer_collect();
     auto& t = p->pot->timer;
     int k = 0, pos = 0;
-    for (size_t i = 1; i < t.names.size() && k < max_stages; ++i, ++k) {
+    for (size_t i = 0; i < t.total_names.size() && k < max_stages; ++i, ++k) {
       if (names) {
-        const std::string& s = t.names[i];
+        const std::string& s = t.total_names[i];
         if (pos + int(s.size()) + 1 <= names_len) {
           std::memcpy(names + pos, s.c_str(), s.size() + 1);
           pos += int(s.size()) + 1;

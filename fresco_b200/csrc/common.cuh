@@ -44,6 +44,14 @@ enum StatusBits : int {
   STATUS_OVERFLOW = 2,         // a bounded buffer was too small (kernel skipped the excess)
 };
 
+// A potential's status block holds two words: [0] the flags of the current
+// evaluation (cleared when it starts) and [1] the flags accumulated since the
+// host last read them.
+__device__ inline void raise_status(int* st, int bit) {
+  atomicOr(st, bit);
+  atomicOr(st + 1, bit);
+}
+
 // RAII device buffer (cudaMalloc'ed once at set-up, never on the evaluation path).
 template <typename T>
 struct DevBuf {

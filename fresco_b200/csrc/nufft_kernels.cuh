@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(kSortThreads) bin_count_kernel(const double* _
       double f;
       ok &= map_coord(pts, j, mp, g.nf[a], a, c[a], f);
     }
-    if (!ok) atomicOr(status, STATUS_NONFINITE_INPUT);
+    if (!ok) raise_status(status, STATUS_NONFINITE_INPUT);
     const int bin = c[0] / g.tile[0] + g.nb[0] * (c[1] / g.tile[1] + g.nb[1] * (c[2] / g.tile[2]));
     rank[j] = uint32_t(atomicAdd(&bin_count[bin], 1));
   }

@@ -258,6 +258,7 @@ class NUwUImpl final : public Potential {
  private:
   void run(const double* x, double* g, double* e, bool acc, cudaStream_t s) {
     timer_begin(s);
+    begin_eval_status(s);
     if (!acc) FB_CUDA(cudaMemsetAsync(e, 0, sizeof(double), s));
     MapParams mp;
     mp.kind = 0;

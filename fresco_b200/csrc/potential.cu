@@ -5,50 +5,65 @@ namespace fb {
 
 void Potential::init_status() {
   FB_CUDA(cudaGetDevice(&device));
-  status_.alloc(1);
-  FB_CUDA(cudaMemset(status_.p, 0, sizeof(int)));
+  status_.alloc(2);
+  FB_CUDA(cudaMemset(status_.p, 0, 2 * sizeof(int)));
 }
 
 int Potential::read_and_clear_status(cudaStream_t s) {
   if (!status_.p) return 0;
   int h = 0;
-  FB_CUDA(cudaMemcpyAsync(&h, status_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-  FB_CUDA(cudaMemsetAsync(status_.p, 0, sizeof(int), s));
+  FB_CUDA(cudaMemcpyAsync(&h, status_.p + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FB_CUDA(cudaMemsetAsync(status_.p + 1, 0, sizeof(int), s));
   FB_CUDA(cudaStreamSynchronize(s));
   return h;
 }
 
 void Potential::timer_begin(cudaStream_t s) {
   if (!timer.enabled) return;
-  timer.next = 0;
+  if (timer.used == int(timer.sets.size())) {
+    timer.sets.emplace_back();
+    timer.names.emplace_back();
+  }
+  timer.names[timer.used].clear();
+  ++timer.used;
   timer_mark("__begin", s);
 }
 
 void Potential::timer_mark(const char* name, cudaStream_t s) {
-  if (!timer.enabled) return;
-  const int i = timer.next++;
-  if (i >= int(timer.ev.size())) {
+  if (!timer.enabled || timer.used == 0) return;
+  auto& set = timer.sets[timer.used - 1];
+  auto& nm = timer.names[timer.used - 1];
+  const size_t i = nm.size();
+  if (i >= set.size()) {
     cudaEvent_t e;
     FB_CUDA(cudaEventCreate(&e));
-    timer.ev.push_back(e);
-    timer.names.push_back(name);
-    timer.total_ms.push_back(0.0);
-    timer.count.push_back(0);
+    set.push_back(e);
   }
-  timer.names[i] = name;
-  FB_CUDA(cudaEventRecord(timer.ev[i], s));
+  nm.push_back(name);
+  FB_CUDA(cudaEventRecord(set[i], s));
 }
 
 void Potential::timer_collect() {
-  if (!timer.enabled || timer.next < 2) return;
-  FB_CUDA(cudaEventSynchronize(timer.ev[timer.next - 1]));
-  for (int i = 1; i < timer.next; ++i) {
-    float ms = 0.f;
-    FB_CUDA(cudaEventElapsedTime(&ms, timer.ev[i - 1], timer.ev[i]));
-    timer.total_ms[i] += ms;
-    timer.count[i] += 1;
+  for (int u = 0; u < timer.used; ++u) {
+    auto& set = timer.sets[u];
+    auto& nm = timer.names[u];
+    if (nm.size() < 2) continue;
+    FB_CUDA(cudaEventSynchronize(set[nm.size() - 1]));
+    for (size_t i = 1; i < nm.size(); ++i) {
+      float ms = 0.f;
+      FB_CUDA(cudaEventElapsedTime(&ms, set[i - 1], set[i]));
+      size_t k = 0;
+      while (k < timer.total_names.size() && timer.total_names[k] != nm[i]) ++k;
+      if (k == timer.total_names.size()) {
+        timer.total_names.push_back(nm[i]);
+        timer.total_ms.push_back(0.0);
+        timer.count.push_back(0);
+      }
+      timer.total_ms[k] += ms;
+      timer.count[k] += 1;
+    }
   }
-  timer.next = 0;
+  timer.used = 0;
 }
 
 CombinedPotential::CombinedPotential() { init_status(); }

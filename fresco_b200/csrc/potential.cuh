@@ -37,23 +37,27 @@ class Potential {
 
   int device = 0;
 
-  // Per-stage CUDA-event timing (for the benchmark's roofline figures).
+  // Per-stage CUDA-event timing (for the benchmark's roofline figures).  Each
+  // evaluation records its own event set on the launch stream; collection
+  // (a host sync) happens only when the totals are read.
   struct StageTimer {
     bool enabled = false;
-    std::vector<std::string> names;
-    std::vector<cudaEvent_t> ev;
+    std::vector<std::vector<cudaEvent_t>> sets;
+    std::vector<std::vector<std::string>> names;
+    int used = 0;
+    std::vector<std::string> total_names;
     std::vector<double> total_ms;
     std::vector<int> count;
-    int next = 0;
   };
   StageTimer timer;
-  void timer_mark(const char* name, cudaStream_t s);  // records the end of a stage
   void timer_begin(cudaStream_t s);
-  void timer_collect();  // host sync; accumulates elapsed times
+  void timer_mark(const char* name, cudaStream_t s);  // records the end of a stage
+  void timer_collect();                              // host sync; accumulates elapsed times
 
  protected:
-  DevBuf<int> status_;
+  DevBuf<int> status_;  // [0] current evaluation, [1] accumulated for the host
   void init_status();
+  void begin_eval_status(cudaStream_t s) { FB_CUDA(cudaMemsetAsync(status_.p, 0, sizeof(int), s)); }
 };
 
 using PotentialPtr = std::shared_ptr<Potential>;

@@ -5,10 +5,6 @@
 
 namespace fb {
 
-PotentialPtr make_uwu(const std::vector<int>&, double, const std::vector<double>&, const std::vector<double>&,
-                      const std::vector<double>&, double, int) {
-  throw std::runtime_error("UwU is not available in this build");
-}
 PotentialPtr make_uwnu(const std::vector<int>&, const std::vector<double>&, const std::vector<double>&,
                        const std::vector<double>&, const std::vector<double>&, double, int) {
   throw std::runtime_error("UwNU is not available in this build");
@@ -17,9 +13,4 @@ PotentialPtr make_nuwnu(const std::vector<double>&, const std::vector<double>&, 
                         const std::vector<double>&, const std::vector<double>&, double, int) {
   throw std::runtime_error("NUwNU is not available in this build");
 }
-PotentialPtr make_inversepower(double, double, const std::vector<double>&, const std::vector<double>&, bool, bool,
-                               double) {
-  throw std::runtime_error("InversePower is not available in this build");
-}
-
 }  // namespace fb

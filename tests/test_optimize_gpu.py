@@ -1,0 +1,139 @@
+"""Device-resident LBFGS / FIRE against the reference optimisers (golden trajectories) and the oracle."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300))
+
+
+def test_lbfgs_golden_trajectory():
+    from fresco_b200 import CombinedPotential, InversePower, NUwU
+    from fresco_b200.optimize import LBFGS_CPP
+
+    d = dict(np.load(os.path.join(GOLDEN, "lbfgs_combined_2d.npz")))
+    nu = NUwU(d["radii"], float(d["K"]), d["Sk"], d["V"], d["L"], eps=1e-13)
+    rep = InversePower(2.0, 1.0, d["rep_radii"], d["L"], use_cell_lists=True)
+    comb = CombinedPotential()
+    comb.add_potential(nu)
+    comb.add_potential(rep)
+    opt = LBFGS_CPP(d["x"], comb, tol=1e-12, M=10)
+    for i in range(len(d["traj_energy"])):
+        res = opt.one_iteration()
+        assert rel(res.energy, d["traj_energy"][i]) < 1e-8, i
+        assert res.nfev == d["traj_nfev"][i], i
+    res = opt.get_result()
+    assert rel(res.coords, d["x_final"]) < 1e-8
+    assert rel(res.H0, d["H0"]) < 1e-6
+    assert res.nsteps == len(d["traj_energy"])
+
+
+def test_lbfgs_matches_oracle_with_backtracking():
+    """Small maxstep / maxErise so the line search backtracks; rel_energy variant too."""
+    from fresco_b200 import NUwU
+    from fresco_b200.optimize import LBFGS_CPP
+
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(300, 6, 4, ndim=2, seed=8)
+    for kw in [dict(maxstep=0.5, maxErise=1e-12), dict(maxstep=0.05, rel_energy=True, maxErise=1e-9)]:
+        pot = NUwU(radii, 6, Sk, V, L, eps=1e-13)
+        ref = O.NUwU(radii, 6, Sk, V, L)
+        opt = LBFGS_CPP(x, pot, M=5, **kw)
+        oref = O.LBFGS(x, ref, M=5, maxstep=kw["maxstep"], maxErise=kw["maxErise"],
+                       rel_energy=kw.get("rel_energy", False))
+        for _ in range(12):
+            opt.one_iteration()
+            oref.one_iteration()
+        res = opt.get_result()
+        assert rel(res.energy, oref.f) < 1e-8
+        assert res.nfev == oref.nfev
+        assert rel(res.coords, oref.x) < 1e-8
+
+
+def test_lbfgs_run_stop_and_reset():
+    from fresco_b200 import NUwU
+    from fresco_b200.optimize import LBFGS_CPP
+
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(200, 5, 3, ndim=2, seed=9)
+    pot = NUwU(radii, 5, Sk, V, L, eps=1e-13)
+    opt = LBFGS_CPP(x, pot, tol=1e-4, M=8, nsteps=500)
+    res = opt.run()
+    assert res.success and res.rms <= 1e-4
+    assert opt.stop_criterion_satisfied()
+    n1 = opt.get_niter()
+    res2 = opt.run(10)  # already converged: no iteration
+    assert opt.get_niter() == n1 and res2.energy == res.energy
+    opt.reset(x)
+    assert opt.get_niter() == 0 and opt.get_result().nfev == 1
+    assert opt.get_maxiter() == 500
+
+
+def test_lbfgs_config1_converges_below_1e12():
+    """2D NUwU, N=4096, 65x65 modes, S0=0 on 0<|k|<=16, M=10, FP64, run in chunks until E < 1e-12."""
+    from fresco_b200 import NUwU
+    from fresco_b200.optimize import LBFGS_CPP
+
+    d = dict(np.load(os.path.join(GOLDEN, "nuwu_2d_n4096.npz")))
+    pot = NUwU(d["radii"], 32, d["Sk"], d["V"], d["L"], eps=1e-13)
+    e0, _ = pot.get_energy_gradient(d["x"])
+    assert abs(e0 - float(d["energy"])) <= 1e-10 * abs(float(d["energy"]))
+    opt = LBFGS_CPP(d["x"], pot, tol=0.0, M=10, nsteps=100000)
+    energy = e0
+    for _ in range(40):
+        res = opt.run(250)
+        energy = res.energy
+        if energy < 1e-12:
+            break
+    assert energy < 1e-12, energy
+
+
+def test_fire_matches_oracle():
+    from fresco_b200 import NUwU
+    from fresco_b200.optimize import ModifiedFireCPP
+
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(300, 6, 4, ndim=2, seed=10)
+    pot = NUwU(radii, 6, Sk, V, L, eps=1e-13)
+    ref = O.NUwU(radii, 6, Sk, V, L)
+    opt = ModifiedFireCPP(x, pot, dtstart=0.01, dtmax=0.1, maxstep=0.05, tol=1e-12)
+    oref = O.ModifiedFire(x, ref, dtstart=0.01, dtmax=0.1, maxstep=0.05, tol=1e-12)
+    for _ in range(30):
+        opt.run(1)
+        oref.run(1)
+        assert rel(opt.get_result().energy, oref.f) < 1e-8
+    res = opt.get_result()
+    assert rel(res.coords, oref.x) < 1e-8
+    assert res.nfev == oref.nfev
+
+
+def test_fire_one_iteration_before_run_keeps_zero_state():
+    from fresco_b200 import NUwU
+    from fresco_b200.optimize import ModifiedFireCPP
+
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(100, 4, 3, ndim=2, seed=11)
+    pot = NUwU(radii, 4, Sk, V, L)
+    opt = ModifiedFireCPP(x, pot)
+    for _ in range(3):
+        opt.one_iteration()
+    r = opt.get_result()
+    assert r.energy == 0.0 and r.rms == 1e10 and r.nfev == 3
+    assert np.array_equal(r.coords, x)
+
+
+def test_result_container_and_events():
+    from fresco_b200 import NUwU
+    from fresco_b200.optimize import LBFGS_CPP
+
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(100, 4, 3, ndim=2, seed=12)
+    pot = NUwU(radii, 4, Sk, V, L)
+    seen = []
+    opt = LBFGS_CPP(x, pot, events=[lambda coords, energy, rms: seen.append(energy)])
+    res = opt.run(5)
+    assert len(seen) == 5 and seen[-1] == res.energy
+    coords, energy, rms, nfev, same = res
+    assert energy == res[1] and rms == res.rms and nfev == res.nfev and same is res
