@@ -3,6 +3,7 @@
 #include <string>
 
 #include "nufft.cuh"
+#include "scan.cuh"
 
 namespace fb {
 
@@ -24,25 +25,46 @@ Geom make_geom(int D, const int64_t* nf, int w, const int* tile_pref) {
   g.w = w;
   g.pad = w / 2;
   const int64_t lim[3][3] = {{int64_t(1) << 31, 1, 1}, {65536, 65536, 1}, {2048, 2048, 1024}};
+  int tile[3] = {1, 1, 1};
+  for (int a = 0; a < D; ++a) {
+    if (nf[a] > lim[D - 1][a]) throw InvalidArgument("fine grid too large for dimension " + std::to_string(D));
+    g.nf[a] = int(nf[a]);
+    // 2D uses fixed 64-cell tiles (phased spreading); other dimensions clamp to the grid
+    tile[a] = (D == 2) ? kTile2D : std::max(1, std::min(tile_pref[a], g.nf[a]));
+  }
+  for (;;) {
+    int64_t nb = 1;
+    for (int a = 0; a < D; ++a) nb *= ceil_div(g.nf[a], tile[a]);
+    if (nb <= kMaxBins || D == 2) break;
+    // grow the smallest tile edge that is still below its grid edge
+    int best = -1;
+    for (int a = 0; a < D; ++a)
+      if (tile[a] < g.nf[a] && (best < 0 || tile[a] < tile[best])) best = a;
+    if (best < 0) break;
+    tile[best] = std::min(2 * tile[best], g.nf[best]);
+  }
   for (int a = 0; a < 3; ++a) {
     if (a < D) {
-      if (nf[a] > lim[D - 1][a]) throw InvalidArgument("fine grid too large for dimension " + std::to_string(D));
-      g.nf[a] = int(nf[a]);
-      g.tile[a] = std::max(1, std::min(tile_pref[a], g.nf[a]));
+      g.tile[a] = tile[a];
       g.nb[a] = int(ceil_div(g.nf[a], g.tile[a]));
       g.tw[a] = g.tile[a] + w;
     } else {
       g.nf[a] = g.tile[a] = g.nb[a] = g.tw[a] = 1;
     }
   }
-  if (g.nbins() > (int64_t(1) << 30)) throw InvalidArgument("too many bins");
+  if (g.nbins() > kMaxBins) throw InvalidArgument("fine grid needs too many bins for the block-local sort");
   return g;
 }
 
 void alloc_sort(SortBufs& sb, int64_t N, const Geom& g) {
   const int64_t nb = g.nbins();
-  sb.bin_count.alloc(nb);
-  sb.bin_start.alloc(nb);
+  const int sms = sm_count();
+  sb.NB = int(std::max<int64_t>(1, std::min<int64_t>(2 * sms, ceil_div(std::max<int64_t>(N, 1), 1024))));
+  sb.chunk = ceil_div(std::max<int64_t>(N, 1), sb.NB);
+  const int64_t nh = nb * sb.NB + 1;
+  sb.hist.alloc(nh);
+  sb.offs.alloc(nh);
+  sb.scan_tmp.alloc(scan_tmp_size(nh));
   sb.max_sub = nb + ceil_div(std::max<int64_t>(N, 1), kMaxSub);
   sb.sub_bin.alloc(sb.max_sub);
   sb.sub_start.alloc(sb.max_sub);

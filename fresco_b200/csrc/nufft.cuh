@@ -1,6 +1,7 @@
-// Non-uniform FFT building blocks on sm_100a: point binning (counting sort),
-// subproblem table, ES-kernel spreading into shared-memory tiles flushed to
-// the fine grid with atomics, and interpolation from the fine grid.
+// Non-uniform FFT building blocks on sm_100a: point binning (counting sort
+// with block-local histograms), subproblem table, ES-kernel spreading into
+// shared-memory tiles flushed to the fine grid with atomics, and
+// interpolation from the fine grid.
 //
 // The method (bin-sort, spread, FFT, deconvolve / pre-correct, FFT,
 // interpolate) is the one of Barnett, Magland & af Klinteberg (SIAM J. Sci.
@@ -10,19 +11,22 @@
 // Layout conventions (all arrays in HBM):
 //  * fine grid: nf[0] x nf[1] x nf[2], dimension 0 fastest (cuFFT row-major
 //    with the dims passed slowest first);
-//  * points are sorted by bin (a tile of `tile[]` fine cells); within the
-//    sorted order each point carries its packed absolute fine cell, its
-//    fractional offset inside the cell per dimension (so FP32 keeps full
-//    phase accuracy), its strength and its original index.
+//  * sorted points: one packed record per point (Rec<D,T>: absolute fine
+//    cell, per-dimension fractional offset inside the cell, original index),
+//    grouped by bin (a tile of `tile[]` fine cells).  Keeping the fractional
+//    offset rather than the coordinate keeps full phase accuracy in FP32.
 #pragma once
+
+#include <algorithm>
 
 #include "common.cuh"
 #include "es.cuh"
 
 namespace fb {
 
-constexpr int kMaxSub = 1024;      // points per spreading subproblem
-constexpr int kSortThreads = 256;
+constexpr int kMaxSub = 1024;     // points per spreading/interpolation subproblem
+constexpr int kMaxBins = 32768;   // bins per geometry (block-local histograms live in shared memory)
+constexpr int kTile2D = 64;       // 2D tile edge (phased spreading needs a multiple of the sub-block edge)
 
 struct Geom {
   int D = 2;
@@ -37,7 +41,8 @@ struct Geom {
   __host__ __device__ int64_t tile_cells() const { return int64_t(tw[0]) * tw[1] * tw[2]; }
 };
 
-// Builds the geometry for fine sizes nf[0..D-1] and kernel width w.
+// Builds the geometry for fine sizes nf[0..D-1] and kernel width w; tiles
+// grow (doubling) until there are at most kMaxBins bins.
 Geom make_geom(int D, const int64_t* nf, int w, const int* tile_pref);
 
 // How raw input coordinates become fine-grid coordinates u in [0, nf).
@@ -50,40 +55,29 @@ struct MapParams {
   int stride = 2;  // doubles between consecutive points (interleaved layout)
 };
 
+// Packed sorted-point records (16 or 32 bytes, read with one vector load).
+template <int D, typename T> struct Rec;
+template <> struct alignas(16) Rec<1, float> { uint32_t cell; float f[1]; uint32_t idx; uint32_t pad_; };
+template <> struct alignas(16) Rec<2, float> { uint32_t cell; float f[2]; uint32_t idx; };
+template <> struct alignas(16) Rec<3, float> { uint32_t cell; float f[3]; uint32_t idx; uint32_t pad_[3]; };
+template <> struct alignas(16) Rec<1, double> { uint32_t cell; uint32_t idx; double f[1]; };
+template <> struct alignas(16) Rec<2, double> { uint32_t cell; uint32_t idx; double f[2]; };
+template <> struct alignas(16) Rec<3, double> { uint32_t cell; uint32_t idx; double f[3]; };
+
+inline size_t rec_bytes(int D, bool f32) {
+  if (f32) return D == 3 ? 32 : 16;
+  return D == 1 ? 16 : 32;
+}
+
 struct SortBufs {
-  DevBuf<int> bin_count, bin_start;
+  int NB = 1;            // sort blocks (each owns a contiguous chunk of points)
+  int64_t chunk = 1;     // points per sort block
+  DevBuf<int> hist;      // nbins * NB + 1 counts, bin-major; scanned in place into offsets
+  DevBuf<int> offs;      // exclusive scan of hist
+  DevBuf<int> scan_tmp;
   DevBuf<int> sub_bin, sub_start, sub_count, num_sub;
   DevBuf<uint32_t> rank;
   int64_t max_sub = 0;
-};
-
-template <typename T>
-struct SortedPts {
-  uint32_t* cell = nullptr;  // packed absolute fine cell
-  T* frac[3] = {nullptr, nullptr, nullptr};
-  T* cw = nullptr;           // strength (real), sorted order
-  uint32_t* idx = nullptr;   // original point index
-};
-
-template <typename T>
-struct SortedStore {
-  DevBuf<uint32_t> cell, idx;
-  DevBuf<T> frac[3];
-  DevBuf<T> cw;
-  void alloc(int64_t n, int D) {
-    cell.alloc(n);
-    idx.alloc(n);
-    for (int a = 0; a < D; ++a) frac[a].alloc(n);
-    cw.alloc(n);
-  }
-  SortedPts<T> view() {
-    SortedPts<T> v;
-    v.cell = cell.p;
-    v.idx = idx.p;
-    for (int a = 0; a < 3; ++a) v.frac[a] = frac[a].p;
-    v.cw = cw.p;
-    return v;
-  }
 };
 
 // Packing of an absolute fine cell (c0, c1, c2) into 32 bits.
@@ -98,40 +92,35 @@ __host__ __device__ inline void unpack_cell(int D, uint32_t v, int& c0, int& c1,
   else { c0 = int(v & 0x7ffu); c1 = int((v >> 11) & 0x7ffu); c2 = int(v >> 22); }
 }
 
-// Host driver for the binning sort.  `pts` are device doubles; `weights`
-// (device, original order) may be null, in which case every strength is
-// `uniform_weight`.
-template <typename T>
-void bin_sort(const double* pts, int64_t N, const MapParams& mp, const Geom& g, const double* weights,
-              double uniform_weight, SortBufs& sb, SortedStore<T>& out, int* status, cudaStream_t s);
-
 // Allocates the sort buffers for N points on geometry g.
 void alloc_sort(SortBufs& sb, int64_t N, const Geom& g);
 
-// Spreads real strengths of the sorted points onto a real fine grid (grid is
-// accumulated into; the caller zeroes it).
+// Sorts the points into packed records (device buffer of N * rec_bytes).
 template <typename T>
-void spread_real(const SortedPts<T>& sp, const SortBufs& sb, const Geom& g, double beta, T* grid,
+void bin_sort(const double* pts, int64_t N, const MapParams& mp, const Geom& g, SortBufs& sb, void* recs, int* status,
+              cudaStream_t s);
+
+// Spreads real strengths (weights[idx], or `uniform` when weights is null)
+// onto a real fine grid (accumulated into; the caller zeroes it).
+template <typename T>
+void spread_real(const void* recs, const T* weights, T uniform, const SortBufs& sb, const Geom& g, double beta, T* grid,
                  cudaStream_t s);
 
-// Spreads complex strengths (given in ORIGINAL point order, cplx) onto a
-// complex fine grid.
+// Spreads complex strengths (original point order) onto a complex fine grid.
 template <typename T>
-void spread_cplx(const SortedPts<T>& sp, const SortBufs& sb, const Geom& g, double beta,
-                 const cplx_t<T>* strengths, cplx_t<T>* grid, cudaStream_t s);
+void spread_cplx(const void* recs, const cplx_t<T>* strengths, const SortBufs& sb, const Geom& g, double beta,
+                 cplx_t<T>* grid, cudaStream_t s);
 
 // Interpolation epilogues.
 enum InterpOut : int {
-  INTERP_GRAD = 0,   // NUwU gradient from packed fields (see nuwu.cu)
-  INTERP_CPLX = 1,   // complex value per point, original order, written as double2
+  INTERP_GRAD = 0,  // grad[idx*D + a] (+)= w_idx * component, components (Re f0, Im f0, Re f1)
+  INTERP_CPLX = 1,  // out2[idx] = value of field 0 (double2)
 };
 
-// Interpolates `nfields` complex fine grids (field stride G) at the sorted
-// points.  INTERP_GRAD: grad[idx*D + a] (+)= cw * component, components
-// (Re f0, Im f0, Re f1) for a = 0, 1, 2.  INTERP_CPLX: out2[idx] = value.
+// Interpolates `nfields` complex fine grids (field stride G) at the sorted points.
 template <typename T>
-void interp(const SortedPts<T>& sp, int64_t N, const Geom& g, double beta, const cplx_t<T>* fields,
-            int nfields, int mode, double* grad, double2* out2, int accumulate, const int* status,
-            cudaStream_t s);
+void interp(const void* recs, int64_t N, const T* weights, T uniform, const SortBufs& sb, const Geom& g, double beta,
+            const cplx_t<T>* fields, int nfields, int mode, double* grad, double2* out2, int accumulate,
+            const int* status, cudaStream_t s);
 
 }  // namespace fb

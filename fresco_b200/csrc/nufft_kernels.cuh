@@ -5,12 +5,14 @@
 #include <algorithm>
 
 #include "nufft.cuh"
+#include "scan.cuh"
 
 namespace fb {
 
 namespace {
 constexpr double kPi = 3.14159265358979323846;
-}
+constexpr int kSortThreads = 512;
+}  // namespace
 
 __device__ __forceinline__ int wrap_index(int x, int n) {
   if (x < 0) x += n;
@@ -25,8 +27,8 @@ __device__ __forceinline__ int wrap_index(int x, int n) {
 // Maps coordinate a of point j to (cell, fraction).  Returns false for a
 // non-finite coordinate (then cell = 0, fraction = 0 so all later accesses
 // stay in bounds).
-__device__ __forceinline__ bool map_coord(const double* __restrict__ pts, int64_t j, const MapParams& mp,
-                                          int nf, int a, int& c, double& f) {
+__device__ __forceinline__ bool map_coord(const double* __restrict__ pts, int64_t j, const MapParams& mp, int nf, int a,
+                                          int& c, double& f) {
   const double p = pts[j * mp.stride + a];
   const double L = mp.L[a];
   double x;
@@ -43,100 +45,113 @@ __device__ __forceinline__ bool map_coord(const double* __restrict__ pts, int64_
     return false;
   }
   u -= double(nf) * floor(u / double(nf));
-  double fl = floor(u);
+  const double fl = floor(u);
   int ci = int(fl);
   f = u - fl;
   if (ci >= nf) ci -= nf;
   if (ci < 0) ci += nf;
-  if (ci < 0 || ci >= nf) { ci = 0; f = 0.0; }
+  if (ci < 0 || ci >= nf) {
+    ci = 0;
+    f = 0.0;
+  }
   c = ci;
   return true;
 }
 
 template <int D>
-__global__ void __launch_bounds__(kSortThreads) bin_count_kernel(const double* __restrict__ pts, int64_t N,
-                                                                 MapParams mp, Geom g, int* bin_count,
-                                                                 uint32_t* rank, int* status) {
-  for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < N; j += int64_t(gridDim.x) * blockDim.x) {
-    int c[3] = {0, 0, 0};
-    bool ok = true;
+__device__ __forceinline__ int point_bin(const double* __restrict__ pts, int64_t j, const MapParams& mp, const Geom& g,
+                                         int (&c)[3], double (&f)[3], bool& ok) {
+  ok = true;
 #pragma unroll
-    for (int a = 0; a < D; ++a) {
-      double f;
-      ok &= map_coord(pts, j, mp, g.nf[a], a, c[a], f);
-    }
-    if (!ok) raise_status(status, STATUS_NONFINITE_INPUT);
-    const int bin = c[0] / g.tile[0] + g.nb[0] * (c[1] / g.tile[1] + g.nb[1] * (c[2] / g.tile[2]));
-    rank[j] = uint32_t(atomicAdd(&bin_count[bin], 1));
+  for (int a = 0; a < D; ++a) ok &= map_coord(pts, j, mp, g.nf[a], a, c[a], f[a]);
+  return c[0] / g.tile[0] + g.nb[0] * (c[1] / g.tile[1] + g.nb[1] * (c[2] / g.tile[2]));
+}
+
+// Pass 1: per-block histogram in shared memory; rank = position among the
+// block's points of the same bin.  hist is bin-major: hist[bin * NB + block].
+template <int D>
+__global__ void __launch_bounds__(kSortThreads) local_hist_kernel(const double* __restrict__ pts, int64_t N,
+                                                                  int64_t chunk, MapParams mp, Geom g, int* hist,
+                                                                  uint32_t* rank, int* status) {
+  extern __shared__ int sh_hist[];
+  const int nbins = int(g.nbins());
+  const int NB = gridDim.x;
+  for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh_hist[i] = 0;
+  __syncthreads();
+  const int64_t j0 = int64_t(blockIdx.x) * chunk, j1 = min(N, j0 + chunk);
+  bool bad = false;
+  for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+    int c[3] = {0, 0, 0};
+    double f[3];
+    bool ok;
+    const int bin = point_bin<D>(pts, j, mp, g, c, f, ok);
+    bad |= !ok;
+    rank[j] = uint32_t(atomicAdd(&sh_hist[bin], 1));
+  }
+  if (bad) raise_status(status, STATUS_NONFINITE_INPUT);
+  __syncthreads();
+  for (int i = threadIdx.x; i < nbins; i += blockDim.x) hist[int64_t(i) * NB + blockIdx.x] = sh_hist[i];
+}
+
+// Pass 3: packed records at offs[bin * NB + block] + rank.
+template <int D, typename T>
+__global__ void __launch_bounds__(kSortThreads) scatter_kernel(const double* __restrict__ pts, int64_t N, int64_t chunk,
+                                                               MapParams mp, Geom g, const uint32_t* __restrict__ rank,
+                                                               const int* __restrict__ offs, Rec<D, T>* out) {
+  const int NB = gridDim.x;
+  const int64_t j0 = int64_t(blockIdx.x) * chunk, j1 = min(N, j0 + chunk);
+  for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+    int c[3] = {0, 0, 0};
+    double f[3] = {0, 0, 0};
+    bool ok;
+    const int bin = point_bin<D>(pts, j, mp, g, c, f, ok);
+    const int64_t dest = int64_t(offs[int64_t(bin) * NB + blockIdx.x]) + rank[j];
+    Rec<D, T> r;
+    r.cell = pack_cell(D, c[0], c[1], c[2]);
+#pragma unroll
+    for (int a = 0; a < D; ++a) r.f[a] = T(f[a]);
+    r.idx = uint32_t(j);
+    out[dest] = r;
   }
 }
 
-// One block: bin offsets (exclusive scan of counts) and the subproblem table
-// (each bin cut into chunks of at most kMaxSub points).
-static __global__ void __launch_bounds__(1024) build_subproblems_kernel(int nbins, const int* __restrict__ bin_count,
-                                                                 int* bin_start, int* sub_bin, int* sub_start,
-                                                                 int* sub_count, int* num_sub, int max_sub) {
-  __shared__ int s_pts[1024];
+// One block: subproblem table (each bin cut into chunks of at most kMaxSub
+// points) from the scanned per-block offsets (bin b starts at offs[b * NB]).
+static __global__ void __launch_bounds__(1024) build_subproblems_kernel(int nbins, int NB, const int* __restrict__ offs,
+                                                                        int* sub_bin, int* sub_start, int* sub_count,
+                                                                        int* num_sub, int max_sub) {
   __shared__ int s_sub[1024];
   const int tid = threadIdx.x;
   const int per = (nbins + blockDim.x - 1) / blockDim.x;
   const int b0 = min(nbins, tid * per), b1 = min(nbins, b0 + per);
-  int np = 0, ns = 0;
+  int ns = 0;
   for (int b = b0; b < b1; ++b) {
-    const int c = bin_count[b];
-    np += c;
+    const int c = offs[int64_t(b + 1) * NB] - offs[int64_t(b) * NB];
     ns += (c + kMaxSub - 1) / kMaxSub;
   }
-  s_pts[tid] = np;
   s_sub[tid] = ns;
   __syncthreads();
   for (int off = 1; off < int(blockDim.x); off <<= 1) {
-    const int a = tid >= off ? s_pts[tid - off] : 0;
     const int b = tid >= off ? s_sub[tid - off] : 0;
     __syncthreads();
-    s_pts[tid] += a;
     s_sub[tid] += b;
     __syncthreads();
   }
-  int pbase = s_pts[tid] - np, sbase = s_sub[tid] - ns;
+  int sbase = s_sub[tid] - ns;
   for (int b = b0; b < b1; ++b) {
-    const int c = bin_count[b];
-    bin_start[b] = pbase;
+    const int start = offs[int64_t(b) * NB];
+    const int c = offs[int64_t(b + 1) * NB] - start;
     const int nsub = (c + kMaxSub - 1) / kMaxSub;
     for (int s = 0; s < nsub; ++s) {
       if (sbase < max_sub) {
         sub_bin[sbase] = b;
-        sub_start[sbase] = pbase + s * kMaxSub;
+        sub_start[sbase] = start + s * kMaxSub;
         sub_count[sbase] = min(kMaxSub, c - s * kMaxSub);
       }
       ++sbase;
     }
-    pbase += c;
   }
   if (tid == int(blockDim.x) - 1) *num_sub = min(s_sub[tid], max_sub);
-}
-
-template <int D, typename T>
-__global__ void __launch_bounds__(kSortThreads) scatter_kernel(const double* __restrict__ pts, int64_t N,
-                                                               MapParams mp, Geom g,
-                                                               const double* __restrict__ weights,
-                                                               double uniform_weight,
-                                                               const uint32_t* __restrict__ rank,
-                                                               const int* __restrict__ bin_start,
-                                                               SortedPts<T> out) {
-  for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < N; j += int64_t(gridDim.x) * blockDim.x) {
-    int c[3] = {0, 0, 0};
-    double f[3] = {0, 0, 0};
-#pragma unroll
-    for (int a = 0; a < D; ++a) map_coord(pts, j, mp, g.nf[a], a, c[a], f[a]);
-    const int bin = c[0] / g.tile[0] + g.nb[0] * (c[1] / g.tile[1] + g.nb[1] * (c[2] / g.tile[2]));
-    const int64_t dest = int64_t(bin_start[bin]) + rank[j];
-    out.cell[dest] = pack_cell(D, c[0], c[1], c[2]);
-#pragma unroll
-    for (int a = 0; a < D; ++a) out.frac[a][dest] = T(f[a]);
-    out.cw[dest] = T(weights ? weights[j] : uniform_weight);
-    out.idx[dest] = uint32_t(j);
-  }
 }
 
 template <typename T>
@@ -151,16 +166,182 @@ __device__ __forceinline__ void atomic_add_cplx<double>(double2* p, double re, d
   atomicAdd(&p->y, im);
 }
 
-// One block per subproblem: spread its points into a shared tile (tile +
-// halo of w/2 cells on each side), then add the tile to the fine grid with
-// global atomics (periodic wrap).
+// Adds a shared tile (origin org - pad per used dimension) to the fine grid
+// with global atomics and periodic wrap.
+template <int D, typename T, bool CPLX>
+__device__ __forceinline__ void flush_tile(const T* tile, const Geom& g, int org0, int org1, int org2, int pad,
+                                           T* grid_real, cplx_t<T>* grid_cplx) {
+  const int tw0 = g.tw[0], tw1 = g.tw[1];
+  const int tsize = int(g.tile_cells());
+  const int o0 = org0 - pad;
+  const int o1 = (D >= 2) ? org1 - pad : 0;
+  const int o2 = (D >= 3) ? org2 - pad : 0;
+  const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
+  for (int i = threadIdx.x; i < tsize; i += blockDim.x) {
+    const int i0 = i % tw0;
+    const int r = i / tw0;
+    const int i1 = r % tw1;
+    const int i2 = r / tw1;
+    const int a0 = wrap_index(o0 + i0, nf0);
+    const int a1 = (D >= 2) ? wrap_index(o1 + i1, nf1) : 0;
+    const int a2 = (D >= 3) ? wrap_index(o2 + i2, nf2) : 0;
+    const int64_t gi = (int64_t(a2) * nf1 + a1) * nf0 + a0;
+    if (CPLX) {
+      const T re = tile[2 * i], im = tile[2 * i + 1];
+      if (re != T(0) || im != T(0)) atomic_add_cplx<T>(grid_cplx + gi, re, im);
+    } else {
+      const T v = tile[i];
+      if (v != T(0)) atomicAdd(grid_real + gi, v);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2D spreading without shared-memory atomics.
+//
+// The 64 x 64-cell tile is cut into sub-blocks of SB x SB cells (SB = 8 for
+// w <= 8, 16 for w <= 16).  A point's w x w footprint only reaches the
+// neighbouring sub-blocks, so sub-blocks whose (a, b) indices have the same
+// parities never touch the same cell: the tile is spread in four phases, one
+// per parity class.  Within a phase a warp handles GPW sub-blocks at once,
+// one point from each, with one lane per footprint row; a lane adds its row
+// with plain shared-memory read-modify-writes.  Points of one sub-block are
+// taken one after another by the same lane group (__syncwarp between them),
+// so no two lanes ever update the same cell concurrently.
+// ---------------------------------------------------------------------------
+
+template <int W>
+struct Phased2D {
+  static constexpr int SB = W <= 8 ? 8 : 16;
+  static constexpr int NSB = kTile2D / SB;       // sub-blocks per tile edge
+  static constexpr int GROUP = W <= 8 ? 8 : 16;  // lanes per point (one per footprint row)
+  static constexpr int GPW = 32 / GROUP;         // points per warp step
+  static constexpr int PER_PHASE = (NSB / 2) * (NSB / 2);
+  static constexpr int NWARP = PER_PHASE / GPW;
+  static constexpr int THREADS = 32 * NWARP;
+};
+
+template <int W, typename T, bool CPLX>
+__global__ void __launch_bounds__(Phased2D<W>::THREADS) spread2d_phased_kernel(
+    const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, T uniform,
+    const cplx_t<T>* __restrict__ strengths, const int* __restrict__ sub_bin, const int* __restrict__ sub_start,
+    const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g, T beta, T* grid_real,
+    cplx_t<T>* grid_cplx) {
+  using P = Phased2D<W>;
+  constexpr int NC = CPLX ? 2 : 1;
+  constexpr int PAD = W / 2;
+  constexpr int TW = kTile2D + W;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tile = reinterpret_cast<T*>(smem_raw);
+  int* list = reinterpret_cast<int*>(tile + TW * TW * NC);
+  int* code = list + kMaxSub;
+  int* sb_count = code + kMaxSub;
+  int* sb_start = sb_count + P::NSB * P::NSB;
+
+  const int sub = blockIdx.x;
+  if (sub >= *num_sub) return;
+  const int bin = sub_bin[sub];
+  const int start = sub_start[sub], cnt = sub_count[sub];
+  const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
+
+  for (int i = threadIdx.x; i < TW * TW * NC; i += blockDim.x) tile[i] = T(0);
+  for (int i = threadIdx.x; i < P::NSB * P::NSB; i += blockDim.x) sb_count[i] = 0;
+  __syncthreads();
+  // group the subproblem's points by sub-block (integer shared atomics)
+  for (int p = threadIdx.x; p < cnt; p += blockDim.x) {
+    int c0, c1, c2;
+    unpack_cell(2, recs[start + p].cell, c0, c1, c2);
+    const int sbi = ((c0 - org0) / P::SB) + P::NSB * ((c1 - org1) / P::SB);
+    code[p] = (sbi << 16) | atomicAdd(&sb_count[sbi], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int i = 0; i < P::NSB * P::NSB; ++i) {
+      sb_start[i] = acc;
+      acc += sb_count[i];
+    }
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < cnt; p += blockDim.x) list[sb_start[code[p] >> 16] + (code[p] & 0xffff)] = p;
+  __syncthreads();
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = lane / P::GROUP, row = lane % P::GROUP;
+  const int q = warp * P::GPW + grp;  // this lane group's slot within a phase
+  const int qa = q % (P::NSB / 2), qb = q / (P::NSB / 2);
+  const T inv_half = T(2) / T(W);
+  for (int phase = 0; phase < 4; ++phase) {
+    const int sbi = (2 * qa + (phase & 1)) + P::NSB * (2 * qb + (phase >> 1));
+    const int my_n = sb_count[sbi], my_base = sb_start[sbi];
+    int n_max = my_n;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n_max = max(n_max, __shfl_xor_sync(0xffffffffu, n_max, o));
+    for (int it = 0; it < n_max; ++it) {
+      const bool active = it < my_n;
+      T kx = T(0), ky = T(0), sr = T(0), si = T(0);
+      int l0 = 0, l1 = 0;
+      if (active) {
+        const int p = list[my_base + it];
+        const Rec<2, T> r = recs[start + p];
+        int c0, c1, c2;
+        unpack_cell(2, r.cell, c0, c1, c2);
+        const T f0 = r.f[0], f1 = r.f[1];
+        const int s0 = (W % 2 == 0) ? (-W / 2 + (f0 > T(0) ? 1 : 0)) : (-(W - 1) / 2 + (f0 > T(0.5) ? 1 : 0));
+        const int s1 = (W % 2 == 0) ? (-W / 2 + (f1 > T(0) ? 1 : 0)) : (-(W - 1) / 2 + (f1 > T(0.5) ? 1 : 0));
+        l0 = c0 - org0 + s0 + PAD;
+        l1 = c1 - org1 + s1 + PAD;
+        if (row < W) {
+          const T zx = (T(s0 + row) - f0) * inv_half, zy = (T(s1 + row) - f1) * inv_half;
+          const T ax = T(1) - zx * zx, ay = T(1) - zy * zy;
+          if (sizeof(T) == 4) {
+            kx = ax >= T(0) ? T(expf(float(beta) * (sqrtf(float(ax)) - 1.0f))) : T(0);
+            ky = ay >= T(0) ? T(expf(float(beta) * (sqrtf(float(ay)) - 1.0f))) : T(0);
+          } else {
+            kx = ax >= T(0) ? T(exp(double(beta) * (sqrt(double(ax)) - 1.0))) : T(0);
+            ky = ay >= T(0) ? T(exp(double(beta) * (sqrt(double(ay)) - 1.0))) : T(0);
+          }
+        }
+        if (CPLX) {
+          const cplx_t<T> v = strengths[r.idx];
+          sr = v.x;
+          si = v.y;
+        } else {
+          sr = weights ? weights[r.idx] : uniform;
+        }
+      }
+      const T wr = sr * ky, wi = si * ky;
+      T* rowp = tile + ((l1 + row) * TW + l0) * NC;
+#pragma unroll
+      for (int m = 0; m < W; ++m) {
+        const T km = __shfl_sync(0xffffffffu, kx, grp * P::GROUP + m);
+        if (active && row < W) {
+          if (CPLX) {
+            rowp[2 * m] += wr * km;
+            rowp[2 * m + 1] += wi * km;
+          } else {
+            rowp[m] += wr * km;
+          }
+        }
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+  Geom gt = g;
+  gt.tw[0] = TW;
+  gt.tw[1] = TW;
+  gt.tw[2] = 1;
+  flush_tile<2, T, CPLX>(tile, gt, org0, org1, 0, PAD, grid_real, grid_cplx);
+}
+
+// Generic spreading (1D, 3D): one thread per point, shared-memory atomics.
 template <int D, int W, typename T, bool CPLX>
-__global__ void __launch_bounds__(256) spread_kernel(SortedPts<T> sp, const int* __restrict__ sub_bin,
-                                                     const int* __restrict__ sub_start,
-                                                     const int* __restrict__ sub_count,
-                                                     const int* __restrict__ num_sub, Geom g, T beta,
-                                                     const cplx_t<T>* __restrict__ strengths, T* grid_real,
-                                                     cplx_t<T>* grid_cplx) {
+__global__ void __launch_bounds__(256) spread_kernel(const Rec<D, T>* __restrict__ recs, const T* __restrict__ weights,
+                                                     T uniform, const cplx_t<T>* __restrict__ strengths,
+                                                     const int* __restrict__ sub_bin, const int* __restrict__ sub_start,
+                                                     const int* __restrict__ sub_count, const int* __restrict__ num_sub,
+                                                     Geom g, T beta, T* grid_real, cplx_t<T>* grid_cplx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tile = reinterpret_cast<T*>(smem_raw);
   const int sub = blockIdx.x;
@@ -181,19 +362,19 @@ __global__ void __launch_bounds__(256) spread_kernel(SortedPts<T> sp, const int*
   constexpr int PAD = W / 2;
 
   for (int p = threadIdx.x; p < cnt; p += blockDim.x) {
-    const int j = start + p;
+    const Rec<D, T> rec = recs[start + p];
     int c0, c1, c2;
-    unpack_cell(D, sp.cell[j], c0, c1, c2);
+    unpack_cell(D, rec.cell, c0, c1, c2);
     T sr, si = T(0);
     if (CPLX) {
-      const cplx_t<T> v = strengths[sp.idx[j]];
+      const cplx_t<T> v = strengths[rec.idx];
       sr = v.x;
       si = v.y;
     } else {
-      sr = sp.cw[j];
+      sr = weights ? weights[rec.idx] : uniform;
     }
     T k0[W];
-    const int l0 = c0 - org0 + es_taps<W, T>(sp.frac[0][j], beta, k0) + PAD;
+    const int l0 = c0 - org0 + es_taps<W, T>(rec.f[0], beta, k0) + PAD;
     if (D == 1) {
 #pragma unroll
       for (int m0 = 0; m0 < W; ++m0) {
@@ -207,12 +388,12 @@ __global__ void __launch_bounds__(256) spread_kernel(SortedPts<T> sp, const int*
       continue;
     }
     T k1[W];
-    const int l1 = c1 - org1 + es_taps<W, T>(sp.frac[1][j], beta, k1) + PAD;
+    const int l1 = c1 - org1 + es_taps<W, T>(rec.f[D >= 2 ? 1 : 0], beta, k1) + PAD;
     int nz = 1;
     T k2[W];
     int l2 = 0;
     if (D == 3) {
-      l2 = c2 - org2 + es_taps<W, T>(sp.frac[2][j], beta, k2) + PAD;
+      l2 = c2 - org2 + es_taps<W, T>(rec.f[D >= 3 ? 2 : 0], beta, k2) + PAD;
       nz = W;
     }
     for (int m2 = 0; m2 < nz; ++m2) {
@@ -235,50 +416,101 @@ __global__ void __launch_bounds__(256) spread_kernel(SortedPts<T> sp, const int*
     }
   }
   __syncthreads();
+  flush_tile<D, T, CPLX>(tile, g, org0, org1, org2, PAD, grid_real, grid_cplx);
+}
 
-  const int o0 = org0 - PAD;
-  const int o1 = (D >= 2) ? org1 - PAD : 0;
-  const int o2 = (D >= 3) ? org2 - PAD : 0;
-  const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
-  for (int i = threadIdx.x; i < tsize; i += blockDim.x) {
-    const int i0 = i % tw0;
-    const int r = i / tw0;
-    const int i1 = r % tw1;
-    const int i2 = r / tw1;
-    const int a0 = wrap_index(o0 + i0, nf0);
-    const int a1 = (D >= 2) ? wrap_index(o1 + i1, nf1) : 0;
-    const int a2 = (D >= 3) ? wrap_index(o2 + i2, nf2) : 0;
-    const int64_t gi = (int64_t(a2) * nf1 + a1) * nf0 + a0;
-    if (CPLX) {
-      const T re = tile[2 * i], im = tile[2 * i + 1];
-      if (re != T(0) || im != T(0)) atomic_add_cplx<T>(grid_cplx + gi, re, im);
-    } else {
-      const T v = tile[i];
-      if (v != T(0)) atomicAdd(grid_real + gi, v);
+// Epilogue shared by the interpolation kernels.
+template <int D, typename T>
+__device__ __forceinline__ void interp_store(int mode, uint32_t o, T wgt, T v0r, T v0i, T v1r, bool bad, double* grad,
+                                             double2* out2, int accumulate) {
+  if (mode == INTERP_GRAD) {
+    const double cw = double(wgt);
+    const double gv[3] = {cw * double(v0r), cw * double(v0i), cw * double(v1r)};
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      const double val = bad ? __longlong_as_double(0x7ff8000000000000ULL) : gv[a];
+      double* dst = grad + int64_t(o) * D + a;
+      *dst = accumulate ? *dst + val : val;
     }
+  } else {
+    out2[o] = make_double2(double(v0r), double(v0i));
   }
 }
 
-// Thread per sorted point: gathers W^D fine-grid values directly from HBM/L2
-// (the bin-sorted order gives neighbouring threads overlapping footprints).
+// 2D interpolation: one block per subproblem stages the tile (+ halo) of the
+// field in shared memory, then one thread per point sums its w x w taps.
+template <int W, typename T>
+__global__ void __launch_bounds__(256) interp2d_tile_kernel(
+    const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, T uniform, const int* __restrict__ sub_bin,
+    const int* __restrict__ sub_start, const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g, T beta,
+    const cplx_t<T>* __restrict__ field, int mode, double* grad, double2* out2, int accumulate,
+    const int* __restrict__ status) {
+  constexpr int PAD = W / 2;
+  constexpr int TW = kTile2D + W;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx_t<T>* tile = reinterpret_cast<cplx_t<T>*>(smem_raw);
+  const int sub = blockIdx.x;
+  if (sub >= *num_sub) return;
+  const bool bad = status != nullptr && ((*status) & STATUS_NONFINITE_INPUT);
+  const int bin = sub_bin[sub];
+  const int start = sub_start[sub], cnt = sub_count[sub];
+  const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
+  const int nf0 = g.nf[0], nf1 = g.nf[1];
+  for (int i = threadIdx.x; i < TW * TW; i += blockDim.x) {
+    const int i0 = i % TW, i1 = i / TW;
+    const int a0 = wrap_index(org0 - PAD + i0, nf0), a1 = wrap_index(org1 - PAD + i1, nf1);
+    tile[i] = field[int64_t(a1) * nf0 + a0];
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < cnt; p += blockDim.x) {
+    const Rec<2, T> r = recs[start + p];
+    int c0, c1, c2;
+    unpack_cell(2, r.cell, c0, c1, c2);
+    T k0[W], k1[W];
+    const int s0 = es_taps<W, T>(r.f[0], beta, k0);
+    const int s1 = es_taps<W, T>(r.f[1], beta, k1);
+    const int l0 = c0 - org0 + s0 + PAD, l1 = c1 - org1 + s1 + PAD;
+    T vr = 0, vi = 0;
+#pragma unroll
+    for (int m1 = 0; m1 < W; ++m1) {
+      const cplx_t<T>* rowp = tile + (l1 + m1) * TW + l0;
+      T rr = 0, ri = 0;
+#pragma unroll
+      for (int m0 = 0; m0 < W; ++m0) {
+        const cplx_t<T> a = rowp[m0];
+        rr += a.x * k0[m0];
+        ri += a.y * k0[m0];
+      }
+      vr += k1[m1] * rr;
+      vi += k1[m1] * ri;
+    }
+    const T wgt = (mode == INTERP_GRAD) ? (weights ? weights[r.idx] : uniform) : T(1);
+    interp_store<2, T>(mode, r.idx, wgt, vr, vi, T(0), bad, grad, out2, accumulate);
+  }
+}
+
+// Generic interpolation (1D, 3D): thread per sorted point, taps gathered
+// directly from HBM/L2 (neighbouring threads share footprints).
 template <int D, int W, typename T, int NF>
-__global__ void __launch_bounds__(256) interp_kernel(SortedPts<T> sp, int64_t N, Geom g, T beta,
-                                                     const cplx_t<T>* __restrict__ fields, int64_t G,
-                                                     int mode, double* grad, double2* out2, int accumulate,
+__global__ void __launch_bounds__(256) interp_kernel(const Rec<D, T>* __restrict__ recs, int64_t N,
+                                                     const T* __restrict__ weights, T uniform, Geom g, T beta,
+                                                     const cplx_t<T>* __restrict__ fields, int64_t G, int mode,
+                                                     double* grad, double2* out2, int accumulate,
                                                      const int* __restrict__ status) {
   const bool bad = status != nullptr && ((*status) & STATUS_NONFINITE_INPUT);
   const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
   for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < N; j += int64_t(gridDim.x) * blockDim.x) {
+    const Rec<D, T> rec = recs[j];
     int c0, c1, c2;
-    unpack_cell(D, sp.cell[j], c0, c1, c2);
+    unpack_cell(D, rec.cell, c0, c1, c2);
     T k0[W], k1[W], k2[W];
     int ix[W];
-    const int s0 = es_taps<W, T>(sp.frac[0][j], beta, k0);
+    const int s0 = es_taps<W, T>(rec.f[0], beta, k0);
 #pragma unroll
     for (int m = 0; m < W; ++m) ix[m] = wrap_index(c0 + s0 + m, nf0);
     int s1 = 0, s2 = 0;
-    if (D >= 2) s1 = es_taps<W, T>(sp.frac[1][j], beta, k1);
-    if (D >= 3) s2 = es_taps<W, T>(sp.frac[2][j], beta, k2);
+    if (D >= 2) s1 = es_taps<W, T>(rec.f[D >= 2 ? 1 : 0], beta, k1);
+    if (D >= 3) s2 = es_taps<W, T>(rec.f[D >= 3 ? 2 : 0], beta, k2);
     T v0r = 0, v0i = 0, v1r = 0, v1i = 0;
     const int nz = (D == 3) ? W : 1;
     const int ny = (D >= 2) ? W : 1;
@@ -289,15 +521,15 @@ __global__ void __launch_bounds__(256) interp_kernel(SortedPts<T> sp, int64_t N,
       for (int m1 = 0; m1 < ny; ++m1) {
         const int iy = (D >= 2) ? wrap_index(c1 + s1 + m1, nf1) : 0;
         const T wy = (D >= 2) ? wz * k1[m1] : T(1);
-        const cplx_t<T>* row = fields + (int64_t(iz) * nf1 + iy) * nf0;
+        const cplx_t<T>* rowp = fields + (int64_t(iz) * nf1 + iy) * nf0;
         T rr = 0, ri = 0, qr = 0, qi = 0;
 #pragma unroll
         for (int m0 = 0; m0 < W; ++m0) {
-          const cplx_t<T> a = __ldg(row + ix[m0]);
+          const cplx_t<T> a = __ldg(rowp + ix[m0]);
           rr += a.x * k0[m0];
           ri += a.y * k0[m0];
           if (NF == 2) {
-            const cplx_t<T> b = __ldg(row + G + ix[m0]);
+            const cplx_t<T> b = __ldg(rowp + G + ix[m0]);
             qr += b.x * k0[m0];
             qi += b.y * k0[m0];
           }
@@ -310,19 +542,8 @@ __global__ void __launch_bounds__(256) interp_kernel(SortedPts<T> sp, int64_t N,
         }
       }
     }
-    const uint32_t o = sp.idx[j];
-    if (mode == INTERP_GRAD) {
-      const double cw = double(sp.cw[j]);
-      double gv[3] = {cw * double(v0r), cw * double(v0i), cw * double(v1r)};
-#pragma unroll
-      for (int a = 0; a < D; ++a) {
-        double val = bad ? __longlong_as_double(0x7ff8000000000000ULL) : gv[a];
-        double* dst = grad + int64_t(o) * D + a;
-        *dst = accumulate ? *dst + val : val;
-      }
-    } else {
-      out2[o] = make_double2(double(v0r), double(v0i));
-    }
+    const T wgt = (mode == INTERP_GRAD) ? (weights ? weights[rec.idx] : uniform) : T(1);
+    interp_store<D, T>(mode, rec.idx, wgt, v0r, v0i, v1r, bad, grad, out2, accumulate);
   }
 }
 
@@ -335,145 +556,202 @@ inline int point_grid(int64_t n, int per_sm = 8) {
   return int(std::min<int64_t>(want, int64_t(sm_count()) * per_sm));
 }
 
-template <typename T>
-void bin_sort(const double* pts, int64_t N, const MapParams& mp, const Geom& g, const double* weights,
-              double uniform_weight, SortBufs& sb, SortedStore<T>& out, int* status, cudaStream_t s) {
+template <int D, typename T>
+void bin_sort_d(const double* pts, int64_t N, const MapParams& mp, const Geom& g, SortBufs& sb, void* recs, int* status,
+                cudaStream_t s) {
   const int nbins = int(g.nbins());
-  FB_CUDA(cudaMemsetAsync(sb.bin_count.p, 0, sizeof(int) * nbins, s));
+  const int64_t nh = int64_t(nbins) * sb.NB;
+  const size_t smem = sizeof(int) * size_t(nbins);
   if (N > 0) {
-    const int grid = point_grid(N);
-    switch (g.D) {
-      case 1: bin_count_kernel<1><<<grid, kSortThreads, 0, s>>>(pts, N, mp, g, sb.bin_count.p, sb.rank.p, status); break;
-      case 2: bin_count_kernel<2><<<grid, kSortThreads, 0, s>>>(pts, N, mp, g, sb.bin_count.p, sb.rank.p, status); break;
-      default: bin_count_kernel<3><<<grid, kSortThreads, 0, s>>>(pts, N, mp, g, sb.bin_count.p, sb.rank.p, status); break;
-    }
+    auto k1 = local_hist_kernel<D>;
+    if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k1<<<sb.NB, kSortThreads, smem, s>>>(pts, N, sb.chunk, mp, g, sb.hist.p, sb.rank.p, status);
     FB_LAUNCH_CHECK();
+  } else {
+    FB_CUDA(cudaMemsetAsync(sb.hist.p, 0, sizeof(int) * nh, s));
   }
-  build_subproblems_kernel<<<1, 1024, 0, s>>>(nbins, sb.bin_count.p, sb.bin_start.p, sb.sub_bin.p, sb.sub_start.p,
-                                              sb.sub_count.p, sb.num_sub.p, int(sb.max_sub));
+  FB_CUDA(cudaMemsetAsync(sb.hist.p + nh, 0, sizeof(int), s));
+  exclusive_scan(sb.hist.p, sb.offs.p, sb.scan_tmp.p, nh + 1, s);
+  build_subproblems_kernel<<<1, 1024, 0, s>>>(nbins, sb.NB, sb.offs.p, sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p,
+                                              sb.num_sub.p, int(sb.max_sub));
   FB_LAUNCH_CHECK();
   if (N > 0) {
-    const int grid = point_grid(N);
-    SortedPts<T> v = out.view();
-    switch (g.D) {
-      case 1: scatter_kernel<1, T><<<grid, kSortThreads, 0, s>>>(pts, N, mp, g, weights, uniform_weight, sb.rank.p, sb.bin_start.p, v); break;
-      case 2: scatter_kernel<2, T><<<grid, kSortThreads, 0, s>>>(pts, N, mp, g, weights, uniform_weight, sb.rank.p, sb.bin_start.p, v); break;
-      default: scatter_kernel<3, T><<<grid, kSortThreads, 0, s>>>(pts, N, mp, g, weights, uniform_weight, sb.rank.p, sb.bin_start.p, v); break;
-    }
+    scatter_kernel<D, T><<<sb.NB, kSortThreads, 0, s>>>(pts, N, sb.chunk, mp, g, sb.rank.p, sb.offs.p,
+                                                        static_cast<Rec<D, T>*>(recs));
     FB_LAUNCH_CHECK();
   }
 }
 
+template <typename T>
+void bin_sort(const double* pts, int64_t N, const MapParams& mp, const Geom& g, SortBufs& sb, void* recs, int* status,
+              cudaStream_t s) {
+  switch (g.D) {
+    case 1: bin_sort_d<1, T>(pts, N, mp, g, sb, recs, status, s); break;
+    case 2: bin_sort_d<2, T>(pts, N, mp, g, sb, recs, status, s); break;
+    default: bin_sort_d<3, T>(pts, N, mp, g, sb, recs, status, s); break;
+  }
+}
+
+template <int W, typename T, bool CPLX>
+void launch_spread2d(const void* recs, const T* weights, T uniform, const cplx_t<T>* strengths, const SortBufs& sb,
+                     const Geom& g, double beta, T* grid_real, cplx_t<T>* grid_cplx, cudaStream_t s) {
+  using P = Phased2D<W>;
+  constexpr int TW = kTile2D + W;
+  const size_t smem = sizeof(T) * TW * TW * (CPLX ? 2 : 1) + sizeof(int) * (2 * kMaxSub + 2 * P::NSB * P::NSB);
+  auto kern = spread2d_phased_kernel<W, T, CPLX>;
+  if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  kern<<<unsigned(sb.max_sub), P::THREADS, smem, s>>>(static_cast<const Rec<2, T>*>(recs), weights, uniform, strengths,
+                                                       sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g,
+                                                       T(beta), grid_real, grid_cplx);
+  FB_LAUNCH_CHECK();
+}
+
 template <int D, int W, typename T, bool CPLX>
-void launch_spread_w(const SortedPts<T>& sp, const SortBufs& sb, const Geom& g, double beta,
-                     const cplx_t<T>* strengths, T* grid_real, cplx_t<T>* grid_cplx, cudaStream_t s) {
+void launch_spread_generic(const void* recs, const T* weights, T uniform, const cplx_t<T>* strengths,
+                           const SortBufs& sb, const Geom& g, double beta, T* grid_real, cplx_t<T>* grid_cplx,
+                           cudaStream_t s) {
   const size_t smem = size_t(g.tile_cells()) * sizeof(T) * (CPLX ? 2 : 1);
   auto kern = spread_kernel<D, W, T, CPLX>;
   if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  kern<<<unsigned(sb.max_sub), 256, smem, s>>>(sp, sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g,
-                                                T(beta), strengths, grid_real, grid_cplx);
+  kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<D, T>*>(recs), weights, uniform, strengths,
+                                                sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g, T(beta),
+                                                grid_real, grid_cplx);
+  FB_LAUNCH_CHECK();
+}
+
+template <int W, typename T>
+void launch_interp2d(const void* recs, const T* weights, T uniform, const SortBufs& sb, const Geom& g, double beta,
+                     const cplx_t<T>* field, int mode, double* grad, double2* out2, int acc, const int* status,
+                     cudaStream_t s) {
+  constexpr int TW = kTile2D + W;
+  const size_t smem = sizeof(cplx_t<T>) * TW * TW;
+  auto kern = interp2d_tile_kernel<W, T>;
+  if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<2, T>*>(recs), weights, uniform, sb.sub_bin.p,
+                                                sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g, T(beta), field, mode,
+                                                grad, out2, acc, status);
   FB_LAUNCH_CHECK();
 }
 
 template <int D, int W, typename T>
-void launch_interp_w(const SortedPts<T>& sp, int64_t N, const Geom& g, double beta, const cplx_t<T>* fields,
-                     int nfields, int mode, double* grad, double2* out2, int acc, const int* status,
-                     cudaStream_t s) {
+void launch_interp_generic(const void* recs, int64_t N, const T* weights, T uniform, const Geom& g, double beta,
+                           const cplx_t<T>* fields, int nfields, int mode, double* grad, double2* out2, int acc,
+                           const int* status, cudaStream_t s) {
   if (N <= 0) return;
   const int grid = point_grid(N, 16);
+  const Rec<D, T>* r = static_cast<const Rec<D, T>*>(recs);
   if (nfields == 2) {
-    interp_kernel<D, W, T, 2><<<grid, 256, 0, s>>>(sp, N, g, T(beta), fields, g.G(), mode, grad, out2, acc, status);
+    interp_kernel<D, W, T, 2><<<grid, 256, 0, s>>>(r, N, weights, uniform, g, T(beta), fields, g.G(), mode, grad, out2,
+                                                   acc, status);
   } else {
-    interp_kernel<D, W, T, 1><<<grid, 256, 0, s>>>(sp, N, g, T(beta), fields, g.G(), mode, grad, out2, acc, status);
+    interp_kernel<D, W, T, 1><<<grid, 256, 0, s>>>(r, N, weights, uniform, g, T(beta), fields, g.G(), mode, grad, out2,
+                                                   acc, status);
   }
   FB_LAUNCH_CHECK();
 }
 
-#define FB_FOR_W(T, X)                                                                    \
-  switch (g.w) {                                                                          \
-    case 2: X(2); break;                                                                  \
-    case 3: X(3); break;                                                                  \
-    case 4: X(4); break;                                                                  \
-    case 5: X(5); break;                                                                  \
-    case 6: X(6); break;                                                                  \
-    case 7: X(7); break;                                                                  \
-    case 8: X(8); break;                                                                  \
-    case 9: X(9); break;                                                                  \
-    case 10: X(10); break;                                                                \
-    default:                                                                              \
-      if (sizeof(T) == 8) {                                                               \
-        switch (g.w) {                                                                    \
-          case 11: X(11); break;                                                          \
-          case 12: X(12); break;                                                          \
-          case 13: X(13); break;                                                          \
-          case 14: X(14); break;                                                          \
-          case 15: X(15); break;                                                          \
-          case 16: X(16); break;                                                          \
-          default: throw InvalidArgument("unsupported kernel width");                     \
-        }                                                                                 \
-      } else {                                                                            \
-        throw InvalidArgument("unsupported kernel width for FP32");                       \
-      }                                                                                   \
+#define FB_FOR_W(T, X)                                                \
+  switch (g.w) {                                                      \
+    case 2: X(2); break;                                              \
+    case 3: X(3); break;                                              \
+    case 4: X(4); break;                                              \
+    case 5: X(5); break;                                              \
+    case 6: X(6); break;                                              \
+    case 7: X(7); break;                                              \
+    case 8: X(8); break;                                              \
+    case 9: X(9); break;                                              \
+    case 10: X(10); break;                                            \
+    default:                                                          \
+      if (sizeof(T) == 8) {                                           \
+        switch (g.w) {                                                \
+          case 11: X(11); break;                                      \
+          case 12: X(12); break;                                      \
+          case 13: X(13); break;                                      \
+          case 14: X(14); break;                                      \
+          case 15: X(15); break;                                      \
+          case 16: X(16); break;                                      \
+          default: throw InvalidArgument("unsupported kernel width"); \
+        }                                                             \
+      } else {                                                        \
+        throw InvalidArgument("unsupported kernel width for FP32");   \
+      }                                                               \
   }
 
-template <typename T, int D, bool CPLX>
-void spread_dispatch(const SortedPts<T>& sp, const SortBufs& sb, const Geom& g, double beta,
-                     const cplx_t<T>* strengths, T* grid_real, cplx_t<T>* grid_cplx, cudaStream_t s) {
-#define FB_SPREAD_W(WW)                                                                       \
-  launch_spread_w<D, (sizeof(T) == 4 && WW > 10) ? 10 : WW, T, CPLX>(sp, sb, g, beta, strengths, \
-                                                                      grid_real, grid_cplx, s)
-  FB_FOR_W(T, FB_SPREAD_W)
-#undef FB_SPREAD_W
-}
+#define FB_WCLAMP(T, WW) ((sizeof(T) == 4 && (WW) > 10) ? 10 : (WW))
 
-template <typename T, int D>
-void interp_dispatch(const SortedPts<T>& sp, int64_t N, const Geom& g, double beta, const cplx_t<T>* fields,
-                     int nfields, int mode, double* grad, double2* out2, int acc, const int* status,
-                     cudaStream_t s) {
-#define FB_INTERP_W(WW)                                                                           \
-  launch_interp_w<D, (sizeof(T) == 4 && WW > 10) ? 10 : WW, T>(sp, N, g, beta, fields, nfields, mode, \
-                                                                grad, out2, acc, status, s)
-  FB_FOR_W(T, FB_INTERP_W)
-#undef FB_INTERP_W
+template <typename T, bool CPLX>
+void spread_dispatch(const void* recs, const T* weights, T uniform, const cplx_t<T>* strengths, const SortBufs& sb,
+                     const Geom& g, double beta, T* grid_real, cplx_t<T>* grid_cplx, cudaStream_t s) {
+  if (g.D == 2) {
+#define FB_S2(WW) \
+  launch_spread2d<FB_WCLAMP(T, WW), T, CPLX>(recs, weights, uniform, strengths, sb, g, beta, grid_real, grid_cplx, s)
+    FB_FOR_W(T, FB_S2)
+#undef FB_S2
+  } else if (g.D == 1) {
+#define FB_S1(WW)                                                                                                \
+  launch_spread_generic<1, FB_WCLAMP(T, WW), T, CPLX>(recs, weights, uniform, strengths, sb, g, beta, grid_real, \
+                                                      grid_cplx, s)
+    FB_FOR_W(T, FB_S1)
+#undef FB_S1
+  } else {
+#define FB_S3(WW)                                                                                                \
+  launch_spread_generic<3, FB_WCLAMP(T, WW), T, CPLX>(recs, weights, uniform, strengths, sb, g, beta, grid_real, \
+                                                      grid_cplx, s)
+    FB_FOR_W(T, FB_S3)
+#undef FB_S3
+  }
 }
 
 template <typename T>
-void spread_real(const SortedPts<T>& sp, const SortBufs& sb, const Geom& g, double beta, T* grid,
+void spread_real(const void* recs, const T* weights, T uniform, const SortBufs& sb, const Geom& g, double beta, T* grid,
                  cudaStream_t s) {
-  switch (g.D) {
-    case 1: spread_dispatch<T, 1, false>(sp, sb, g, beta, nullptr, grid, nullptr, s); break;
-    case 2: spread_dispatch<T, 2, false>(sp, sb, g, beta, nullptr, grid, nullptr, s); break;
-    default: spread_dispatch<T, 3, false>(sp, sb, g, beta, nullptr, grid, nullptr, s); break;
-  }
+  spread_dispatch<T, false>(recs, weights, uniform, nullptr, sb, g, beta, grid, nullptr, s);
 }
 
 template <typename T>
-void spread_cplx(const SortedPts<T>& sp, const SortBufs& sb, const Geom& g, double beta,
-                 const cplx_t<T>* strengths, cplx_t<T>* grid, cudaStream_t s) {
-  switch (g.D) {
-    case 1: spread_dispatch<T, 1, true>(sp, sb, g, beta, strengths, nullptr, grid, s); break;
-    case 2: spread_dispatch<T, 2, true>(sp, sb, g, beta, strengths, nullptr, grid, s); break;
-    default: spread_dispatch<T, 3, true>(sp, sb, g, beta, strengths, nullptr, grid, s); break;
-  }
+void spread_cplx(const void* recs, const cplx_t<T>* strengths, const SortBufs& sb, const Geom& g, double beta,
+                 cplx_t<T>* grid, cudaStream_t s) {
+  spread_dispatch<T, true>(recs, nullptr, T(1), strengths, sb, g, beta, nullptr, grid, s);
 }
 
 template <typename T>
-void interp(const SortedPts<T>& sp, int64_t N, const Geom& g, double beta, const cplx_t<T>* fields, int nfields,
-            int mode, double* grad, double2* out2, int accumulate, const int* status, cudaStream_t s) {
-  switch (g.D) {
-    case 1: interp_dispatch<T, 1>(sp, N, g, beta, fields, nfields, mode, grad, out2, accumulate, status, s); break;
-    case 2: interp_dispatch<T, 2>(sp, N, g, beta, fields, nfields, mode, grad, out2, accumulate, status, s); break;
-    default: interp_dispatch<T, 3>(sp, N, g, beta, fields, nfields, mode, grad, out2, accumulate, status, s); break;
+void interp(const void* recs, int64_t N, const T* weights, T uniform, const SortBufs& sb, const Geom& g, double beta,
+            const cplx_t<T>* fields, int nfields, int mode, double* grad, double2* out2, int accumulate,
+            const int* status, cudaStream_t s) {
+  if (g.D == 2 && nfields == 1) {
+#define FB_I2(WW)                                                                                                  \
+  launch_interp2d<FB_WCLAMP(T, WW), T>(recs, weights, uniform, sb, g, beta, fields, mode, grad, out2, accumulate, \
+                                       status, s)
+    FB_FOR_W(T, FB_I2)
+#undef FB_I2
+  } else if (g.D == 1) {
+#define FB_I1(WW)                                                                                             \
+  launch_interp_generic<1, FB_WCLAMP(T, WW), T>(recs, N, weights, uniform, g, beta, fields, nfields, mode, grad, \
+                                                out2, accumulate, status, s)
+    FB_FOR_W(T, FB_I1)
+#undef FB_I1
+  } else if (g.D == 2) {
+#define FB_I2G(WW)                                                                                            \
+  launch_interp_generic<2, FB_WCLAMP(T, WW), T>(recs, N, weights, uniform, g, beta, fields, nfields, mode, grad, \
+                                                out2, accumulate, status, s)
+    FB_FOR_W(T, FB_I2G)
+#undef FB_I2G
+  } else {
+#define FB_I3(WW)                                                                                             \
+  launch_interp_generic<3, FB_WCLAMP(T, WW), T>(recs, N, weights, uniform, g, beta, fields, nfields, mode, grad, \
+                                                out2, accumulate, status, s)
+    FB_FOR_W(T, FB_I3)
+#undef FB_I3
   }
 }
 
-#define FB_INSTANTIATE_NUFFT(T)                                                                           \
-  template void bin_sort<T>(const double*, int64_t, const MapParams&, const Geom&, const double*, double,    \
-                            SortBufs&, SortedStore<T>&, int*, cudaStream_t);                                 \
-  template void spread_real<T>(const SortedPts<T>&, const SortBufs&, const Geom&, double, T*, cudaStream_t); \
-  template void spread_cplx<T>(const SortedPts<T>&, const SortBufs&, const Geom&, double, const cplx_t<T>*, \
-                               cplx_t<T>*, cudaStream_t);                                                    \
-  template void interp<T>(const SortedPts<T>&, int64_t, const Geom&, double, const cplx_t<T>*, int, int,     \
-                          double*, double2*, int, const int*, cudaStream_t);
+#define FB_INSTANTIATE_NUFFT(T)                                                                                     \
+  template void bin_sort<T>(const double*, int64_t, const MapParams&, const Geom&, SortBufs&, void*, int*,          \
+                            cudaStream_t);                                                                           \
+  template void spread_real<T>(const void*, const T*, T, const SortBufs&, const Geom&, double, T*, cudaStream_t);   \
+  template void spread_cplx<T>(const void*, const cplx_t<T>*, const SortBufs&, const Geom&, double, cplx_t<T>*,     \
+                               cudaStream_t);                                                                        \
+  template void interp<T>(const void*, int64_t, const T*, T, const SortBufs&, const Geom&, double, const cplx_t<T>*, \
+                          int, int, double*, double2*, int, const int*, cudaStream_t);
 
 }  // namespace fb

@@ -144,10 +144,11 @@ class NUwUImpl final : public Potential {
       if (c[i] != c[0]) uniform = false;
     }
     if (uniform && !c.empty()) {
-      uniform_c_ = c[0];
+      uniform_c_ = T(c[0]);
     } else if (!c.empty()) {
+      std::vector<T> ct(c.begin(), c.end());
       cw_.alloc(c.size());
-      FB_CUDA(cudaMemcpy(cw_.p, c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice));
+      FB_CUDA(cudaMemcpy(cw_.p, ct.data(), sizeof(T) * c.size(), cudaMemcpyHostToDevice));
     }
 
     // ES kernel and fine grid
@@ -156,12 +157,12 @@ class NUwUImpl final : public Potential {
     for (int a = 0; a < D; ++a) nf[a] = fine_grid_size(n_, es_.w);
     int tile[3];
     if (D == 1) { tile[0] = 1024; tile[1] = tile[2] = 1; }
-    else if (D == 2) { tile[0] = 32; tile[1] = 32; tile[2] = 1; }
+    else if (D == 2) { tile[0] = kTile2D; tile[1] = kTile2D; tile[2] = 1; }
     else if (sizeof(T) == 4) { tile[0] = 16; tile[1] = 16; tile[2] = 8; }
     else { tile[0] = 8; tile[1] = 8; tile[2] = 8; }
     geom_ = make_geom(D, nf, es_.w, tile);
     alloc_sort(sort_, N_, geom_);
-    pts_.alloc(std::max<int64_t>(N_, 1), D);
+    recs_.alloc(std::max<int64_t>(N_, 1) * rec_bytes(D, sizeof(T) == 4));
 
     const int64_t G = geom_.G();
     nh0_ = geom_.nf[0] / 2 + 1;
@@ -264,10 +265,10 @@ class NUwUImpl final : public Potential {
     mp.kind = 0;
     mp.stride = D;
     for (int a = 0; a < D; ++a) mp.L[a] = L_[a];
-    bin_sort<T>(x, N_, mp, geom_, cw_.p, uniform_c_, sort_, pts_, status_.p, s);
+    bin_sort<T>(x, N_, mp, geom_, sort_, recs_.p, status_.p, s);
     timer_mark("sort", s);
     FB_CUDA(cudaMemsetAsync(spread_grid_.p, 0, spread_grid_.bytes(), s));
-    spread_real<T>(pts_.view(), sort_, geom_, es_.beta, spread_grid_.p, s);
+    spread_real<T>(recs_.p, cw_.p, uniform_c_, sort_, geom_, es_.beta, spread_grid_.p, s);
     timer_mark("spread", s);
     FB_CUFFT(cufftSetStream(plan_r2c_, s));
     if (sizeof(T) == 4) {
@@ -302,8 +303,8 @@ class NUwUImpl final : public Potential {
                             reinterpret_cast<cufftDoubleComplex*>(ggrid_.p), CUFFT_FORWARD));
     }
     timer_mark("fft_type2", s);
-    interp<T>(pts_.view(), N_, geom_, es_.beta, ggrid_.p, nfields_, INTERP_GRAD, g, nullptr, acc ? 1 : 0,
-              status_.p, s);
+    interp<T>(recs_.p, N_, cw_.p, uniform_c_, sort_, geom_, es_.beta, ggrid_.p, nfields_, INTERP_GRAD, g, nullptr,
+              acc ? 1 : 0, status_.p, s);
     timer_mark("interp", s);
   }
 
@@ -312,12 +313,12 @@ class NUwUImpl final : public Potential {
   double L_[3] = {1, 1, 1};
   int K_ = 0, n_ = 1;
   int64_t nmodes_ = 1;
-  double uniform_c_ = 1.0;
-  DevBuf<double> cw_;
+  T uniform_c_ = T(1);
+  DevBuf<T> cw_;
   ESParams es_;
   Geom geom_;
   SortBufs sort_;
-  SortedStore<T> pts_;
+  DevBuf<unsigned char> recs_;
   int nh0_ = 1;
   int nfields_ = 1;
   DevBuf<T> spread_grid_;

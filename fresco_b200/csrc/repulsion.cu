@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "potential.cuh"
+#include "scan.cuh"
 
 namespace fb {
 
@@ -104,52 +105,6 @@ __global__ void __launch_bounds__(kThreads) cell_scatter_kernel(const double* __
     sidx[dest] = uint32_t(j);
     scell[dest] = cell;
   }
-}
-
-// Exclusive scan of n ints in three launches (block scan, scan of block sums, add).
-__global__ void __launch_bounds__(1024) scan_block_kernel(const int* __restrict__ in, int* out, int* block_sums,
-                                                          int64_t n) {
-  __shared__ int s[1024];
-  const int64_t i = int64_t(blockIdx.x) * 1024 + threadIdx.x;
-  const int v = i < n ? in[i] : 0;
-  s[threadIdx.x] = v;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    const int t = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
-    __syncthreads();
-    s[threadIdx.x] += t;
-    __syncthreads();
-  }
-  if (i < n) out[i] = s[threadIdx.x] - v;
-  if (threadIdx.x == 1023) block_sums[blockIdx.x] = s[1023];
-}
-
-__global__ void __launch_bounds__(1024) scan_sums_kernel(int* block_sums, int nb) {
-  __shared__ int s[1024];
-  __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  for (int base = 0; base < nb; base += 1024) {
-    const int i = base + threadIdx.x;
-    const int v = i < nb ? block_sums[i] : 0;
-    s[threadIdx.x] = v;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-      const int t = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
-      __syncthreads();
-      s[threadIdx.x] += t;
-      __syncthreads();
-    }
-    if (i < nb) block_sums[i] = carry + s[threadIdx.x] - v;
-    __syncthreads();
-    if (threadIdx.x == 1023) carry += s[1023];
-    __syncthreads();
-  }
-}
-
-__global__ void scan_add_kernel(int* out, const int* __restrict__ block_sums, int64_t n) {
-  const int64_t i = int64_t(blockIdx.x) * 1024 + threadIdx.x;
-  if (i < n) out[i] += block_sums[blockIdx.x];
 }
 
 // One thread per cell-sorted point; neighbours from the 3^D surrounding cells.
@@ -383,9 +338,7 @@ class InversePowerImpl final : public Potential {
     } else {
       FB_CUDA(cudaMemsetAsync(cell_count_.p, 0, sizeof(int) * ncells_, s));
       cell_count_kernel<D><<<grid, kThreads, 0, s>>>(x, N_, box_, cell_count_.p, rank_.p, status_.p);
-      scan_block_kernel<<<nscan_, 1024, 0, s>>>(cell_count_.p, cell_start_.p, block_sums_.p, ncells_);
-      scan_sums_kernel<<<1, 1024, 0, s>>>(block_sums_.p, nscan_);
-      scan_add_kernel<<<nscan_, 1024, 0, s>>>(cell_start_.p, block_sums_.p, ncells_);
+      exclusive_scan(cell_count_.p, cell_start_.p, block_sums_.p, ncells_, s);
       cell_scatter_kernel<D><<<grid, kThreads, 0, s>>>(x, radii_.p, N_, box_, rank_.p, cell_start_.p, sx_.p, sr_.p,
                                                        sidx_.p, scell_.p);
       FB_LAUNCH_CHECK();

@@ -75,15 +75,20 @@ def test_lbfgs_run_stop_and_reset():
 
 
 def test_lbfgs_config1_converges_below_1e12():
-    """2D NUwU, N=4096, 65x65 modes, S0=0 on 0<|k|<=16, M=10, FP64, run in chunks until E < 1e-12."""
+    """2D NUwU, N=4096 seeded uniform points, 65x65 modes, S0=0 on 0<|k|<=16, M=10, FP64, run in
+    chunks until E < 1e-12.  The box is expressed in the reference's own L=1 convention
+    (examples/NUwU.ipynb): with L=2pi the reference map (p - round(p/L)) 2pi/L (nuwu.hpp:219) jumps by
+    one radian at p = pi, the energy is discontinuous there and LBFGS stalls in the reference too."""
     from fresco_b200 import NUwU
     from fresco_b200.optimize import LBFGS_CPP
 
     d = dict(np.load(os.path.join(GOLDEN, "nuwu_2d_n4096.npz")))
-    pot = NUwU(d["radii"], 32, d["Sk"], d["V"], d["L"], eps=1e-13)
-    e0, _ = pot.get_energy_gradient(d["x"])
-    assert abs(e0 - float(d["energy"])) <= 1e-10 * abs(float(d["energy"]))
-    opt = LBFGS_CPP(d["x"], pot, tol=0.0, M=10, nsteps=100000)
+    x = d["x"] / (2 * np.pi)
+    pot = NUwU(d["radii"], 32, d["Sk"], d["V"], np.ones(2), eps=1e-13)
+    ref = O.NUwU(d["radii"], 32, d["Sk"], d["V"], np.ones(2))
+    e0, _ = pot.get_energy_gradient(x)
+    assert abs(e0 - ref.get_energy(x)) <= 1e-10 * abs(e0)
+    opt = LBFGS_CPP(x, pot, tol=0.0, M=10, nsteps=100000)
     energy = e0
     for _ in range(40):
         res = opt.run(250)
@@ -91,6 +96,7 @@ def test_lbfgs_config1_converges_below_1e12():
         if energy < 1e-12:
             break
     assert energy < 1e-12, energy
+    assert ref.get_energy(res.coords) < 1e-11
 
 
 def test_fire_matches_oracle():
@@ -111,18 +117,29 @@ def test_fire_matches_oracle():
     assert res.nfev == oref.nfev
 
 
-def test_fire_one_iteration_before_run_keeps_zero_state():
+def test_fire_one_iteration_before_run_matches_reference_sequence():
+    """MODIFIED_FIRE::one_iteration does not initialise f, g (modified_fire.hpp:160-178): the first call
+    steps from f = 0, g = 0.  Through the Python API, get_result() then calls success(), which
+    initialises them (opt.pyx:81-93, optimizer.hpp:169, 174-180), exactly as in the reference."""
     from fresco_b200 import NUwU
     from fresco_b200.optimize import ModifiedFireCPP
 
     x, radii, Sk, V, L = O.stealthy_nuwu_inputs(100, 4, 3, ndim=2, seed=11)
-    pot = NUwU(radii, 4, Sk, V, L)
+    pot = NUwU(radii, 4, Sk, V, L, eps=1e-13)
     opt = ModifiedFireCPP(x, pot)
-    for _ in range(3):
-        opt.one_iteration()
-    r = opt.get_result()
-    assert r.energy == 0.0 and r.rms == 1e10 and r.nfev == 3
-    assert np.array_equal(r.coords, x)
+    r1 = opt.one_iteration()
+    assert r1.energy == 0.0 and r1.nfev == 1
+    assert np.array_equal(r1.coords, x)
+    oref = O.ModifiedFire(x, O.NUwU(radii, 4, Sk, V, L))
+    oref.one_iteration()
+    oref.stop_criterion_satisfied()  # what get_result() triggers
+    for _ in range(4):
+        r = opt.one_iteration()
+        oref.one_iteration()
+        oref.stop_criterion_satisfied()
+        assert rel(r.energy, oref.f) < 1e-9
+    assert r.nfev == oref.nfev
+    assert rel(r.coords, oref.x) < 1e-9
 
 
 def test_result_container_and_events():
