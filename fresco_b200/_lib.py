@@ -47,6 +47,7 @@ _SIGNATURES = {
     "fresco_potential_energy_gradient_device": (C.c_int, [handle_t, c_void_p, c_int64, c_void_p, c_void_p, C.c_int,
                                                           c_void_p]),
     "fresco_potential_status": (C.c_int, [handle_t, c_void_p, c_int_p]),
+    "fresco_potential_set_gradient_mode": (C.c_int, [handle_t, C.c_int]),
     "fresco_potential_set_timing": (C.c_int, [handle_t, C.c_int]),
     "fresco_potential_get_timing": (C.c_int, [handle_t, C.c_int, C.c_char_p, C.c_int, c_double_p, c_int_p, c_int_p]),
     "fresco_potential_describe": (C.c_int, [handle_t, C.c_char_p, C.c_int]),
@@ -76,7 +77,7 @@ def _load():
     if not _LIB_PATH.exists():
         raise ImportError(
             f"fresco_b200 CUDA library not built: {_LIB_PATH} is missing "
-            "(run `python -m fresco_b200.build`); there is no CPU fallback"
+            "(run `python fresco_b200/build.py`); there is no CPU fallback"
         )
     lib = C.CDLL(str(_LIB_PATH), mode=os.RTLD_NOW | getattr(os, "RTLD_GLOBAL", 0))
     for name, (res, args) in _SIGNATURES.items():

@@ -1,6 +1,6 @@
 """Builds the fresco_b200 CUDA library in-tree with nvcc for sm_100a.
 
-``python -m fresco_b200.build`` (or ``build()``) compiles every ``csrc/*.cu``
+``python fresco_b200/build.py`` (or ``build()``) compiles every ``csrc/*.cu``
 to an object under ``fresco_b200/_build/`` (rebuilt only when the source or a
 header changed) and links ``fresco_b200/libfresco_b200.so`` against cuFFT and
 the CUDA runtime.  No JIT cache is involved, so the built library travels with

@@ -226,6 +226,15 @@ int fresco_potential_status(fresco_potential p, void* stream, int* status) {
   });
 }
 
+int fresco_potential_set_gradient_mode(fresco_potential p, int mode) {
+  return guarded([&] {
+    if (!p) throw fb::InvalidArgument("null handle");
+    if (mode != 0 && mode != 1) throw fb::InvalidArgument("gradient mode must be 0 (reference) or 1 (exact)");
+    p->pot->set_gradient_mode(mode);
+    return FRESCO_OK;
+  });
+}
+
 int fresco_potential_set_timing(fresco_potential p, int enabled) {
   return guarded([&] {
     if (!p) throw fb::InvalidArgument("null handle");

@@ -85,4 +85,42 @@ std::vector<double> es_correction(const ESParams& es, int64_t nf, int64_t kmin, 
   return out;
 }
 
+std::vector<double> es_poly_coefficients(const ESParams& es, int W) {
+  const int Q = W + 2;
+  const int n = 4 * Q + 40;  // Chebyshev nodes for the fit
+  const double pi = 3.14159265358979323846;
+  std::vector<double> out(size_t(W) * (Q + 1), 0.0);
+  std::vector<double> xk(n), cheb(Q + 1);
+  for (int j = 0; j < n; ++j) xk[j] = std::cos(pi * (j + 0.5) / n);  // in [-1, 1], u = x / 2
+  for (int m = 0; m < W; ++m) {
+    const double a = m - 0.5 * (W - 1);
+    // Chebyshev coefficients of g(x) = phi((a - x/2) * 2/W) from the discrete orthogonality sums
+    for (int k = 0; k <= Q; ++k) {
+      double sum = 0.0;
+      for (int j = 0; j < n; ++j) sum += es_phi((a - 0.5 * xk[j]) * 2.0 / W, es.beta) * std::cos(k * pi * (j + 0.5) / n);
+      cheb[k] = (k == 0 ? 1.0 : 2.0) * sum / n;
+    }
+    // sum_k cheb_k T_k(x) -> monomials in x (T_{k+1} = 2x T_k - T_{k-1}) -> monomials in u (x = 2u)
+    std::vector<double> tkm1(Q + 1, 0.0), tk(Q + 1, 0.0), mono(Q + 1, 0.0);
+    tkm1[0] = 1.0;      // T_0
+    tk[1] = 1.0;        // T_1
+    mono[0] += cheb[0];
+    if (Q >= 1) mono[1] += cheb[1];
+    for (int k = 1; k < Q; ++k) {
+      std::vector<double> tn(Q + 1, 0.0);
+      for (int d = 0; d < Q; ++d) tn[d + 1] += 2.0 * tk[d];
+      for (int d = 0; d <= Q; ++d) tn[d] -= tkm1[d];
+      for (int d = 0; d <= Q; ++d) mono[d] += cheb[k + 1] * tn[d];
+      tkm1 = tk;
+      tk = tn;
+    }
+    double scale = 1.0;
+    for (int d = 0; d <= Q; ++d) {
+      out[size_t(m) * (Q + 1) + d] = mono[d] * scale;
+      scale *= 2.0;
+    }
+  }
+  return out;
+}
+
 }  // namespace fb

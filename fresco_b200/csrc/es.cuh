@@ -49,31 +49,65 @@ inline double es_phi(double t, double beta) {
   return a >= 0.0 ? std::exp(beta * (std::sqrt(a) - 1.0)) : 0.0;
 }
 
-#ifdef __CUDACC__
-// Device evaluation of the w kernel values for a point at fractional cell
-// offset f in [0, 1): taps m = 0..w-1 sit at grid offsets s+m relative to the
-// point's cell, with z = s + m - f in (-w/2, w/2].  Returns s.
+// Piecewise-polynomial form of the kernel taps (the approach of the ES paper,
+// section on fast kernel evaluation): with the fractional cell offset f of a
+// point, the W taps sit at z_m = (m - (W-1)/2) - u, where u = f - 1/2 for even
+// W and u = f (f <= 1/2) or f - 1 (f > 1/2) for odd W, so u lies in
+// [-1/2, 1/2].  Each tap is a degree-(W+2) polynomial in u, fitted at set-up
+// by Chebyshev interpolation and evaluated with Horner's rule; the fit error
+// is about 30x below the kernel's own truncation error for every W.
+template <int W>
+struct EsPolyDeg {
+  static constexpr int Q = W + 2;
+};
+
+// Monomial coefficients c[m * (Q+1) + d] of tap m in powers u^d.
+std::vector<double> es_poly_coefficients(const ESParams& es, int W);
+
 template <int W, typename T>
-__device__ __forceinline__ int es_taps(T f, T beta, T (&kv)[W]) {
-  int s;
+struct EsPoly {
+  T c[W][EsPolyDeg<W>::Q + 1];
+};
+
+template <int W, typename T>
+inline EsPoly<W, T> make_es_poly(const std::vector<double>& coef) {
+  constexpr int Q = EsPolyDeg<W>::Q;
+  EsPoly<W, T> p;
+  for (int m = 0; m < W; ++m)
+    for (int d = 0; d <= Q; ++d) p.c[m][d] = T(coef[size_t(m) * (Q + 1) + d]);
+  return p;
+}
+
+#ifdef __CUDACC__
+// Start offset s of the W taps (relative to the point's cell) and the
+// polynomial variable u for a fractional offset f in [0, 1).
+template <int W, typename T>
+__device__ __forceinline__ int es_start(T f, T& u) {
   if (W % 2 == 0) {
-    s = -W / 2 + (f > T(0) ? 1 : 0);
-  } else {
-    s = -(W - 1) / 2 + (f > T(0.5) ? 1 : 0);
+    u = f - T(0.5);
+    return -W / 2 + 1;
   }
-  const T inv_half = T(2) / T(W);
+  const bool hi = f > T(0.5);
+  u = hi ? f - T(1) : f;
+  return -(W - 1) / 2 + (hi ? 1 : 0);
+}
+
+template <int W, typename T>
+__device__ __forceinline__ T es_poly_tap(const EsPoly<W, T>& p, int m, T u) {
+  constexpr int Q = EsPolyDeg<W>::Q;
+  T v = p.c[m][Q];
 #pragma unroll
-  for (int m = 0; m < W; ++m) {
-    const T z = (T(s + m) - f) * inv_half;
-    const T a = T(1) - z * z;
-    T v;
-    if (sizeof(T) == 4) {
-      v = a >= T(0) ? expf(float(beta) * (sqrtf(float(a)) - 1.0f)) : T(0);
-    } else {
-      v = a >= T(0) ? exp(double(beta) * (sqrt(double(a)) - 1.0)) : T(0);
-    }
-    kv[m] = v;
-  }
+  for (int d = Q - 1; d >= 0; --d) v = fma(v, u, p.c[m][d]);
+  return v;
+}
+
+// All W tap values of a point at fractional offset f; returns the start offset.
+template <int W, typename T>
+__device__ __forceinline__ int es_taps(T f, const EsPoly<W, T>& p, T (&kv)[W]) {
+  T u;
+  const int s = es_start<W, T>(f, u);
+#pragma unroll
+  for (int m = 0; m < W; ++m) kv[m] = es_poly_tap<W, T>(p, m, u);
   return s;
 }
 #endif

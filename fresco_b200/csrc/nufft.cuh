@@ -18,6 +18,7 @@
 #pragma once
 
 #include <algorithm>
+#include <vector>
 
 #include "common.cuh"
 #include "es.cuh"
@@ -100,16 +101,18 @@ template <typename T>
 void bin_sort(const double* pts, int64_t N, const MapParams& mp, const Geom& g, SortBufs& sb, void* recs, int* status,
               cudaStream_t s);
 
+// `poly` holds the kernel-tap polynomial coefficients (es_poly_coefficients).
+
 // Spreads real strengths (weights[idx], or `uniform` when weights is null)
 // onto a real fine grid (accumulated into; the caller zeroes it).
 template <typename T>
-void spread_real(const void* recs, const T* weights, T uniform, const SortBufs& sb, const Geom& g, double beta, T* grid,
-                 cudaStream_t s);
+void spread_real(const void* recs, const T* weights, T uniform, const SortBufs& sb, const Geom& g,
+                 const std::vector<double>& poly, T* grid, cudaStream_t s);
 
 // Spreads complex strengths (original point order) onto a complex fine grid.
 template <typename T>
-void spread_cplx(const void* recs, const cplx_t<T>* strengths, const SortBufs& sb, const Geom& g, double beta,
-                 cplx_t<T>* grid, cudaStream_t s);
+void spread_cplx(const void* recs, const cplx_t<T>* strengths, const SortBufs& sb, const Geom& g,
+                 const std::vector<double>& poly, cplx_t<T>* grid, cudaStream_t s);
 
 // Interpolation epilogues.
 enum InterpOut : int {
@@ -117,10 +120,15 @@ enum InterpOut : int {
   INTERP_CPLX = 1,  // out2[idx] = value of field 0 (double2)
 };
 
+// Per-dimension factors applied to INTERP_GRAD outputs.
+struct GradScale {
+  double s[3] = {1.0, 1.0, 1.0};
+};
+
 // Interpolates `nfields` complex fine grids (field stride G) at the sorted points.
 template <typename T>
-void interp(const void* recs, int64_t N, const T* weights, T uniform, const SortBufs& sb, const Geom& g, double beta,
-            const cplx_t<T>* fields, int nfields, int mode, double* grad, double2* out2, int accumulate,
-            const int* status, cudaStream_t s);
+void interp(const void* recs, int64_t N, const T* weights, T uniform, const SortBufs& sb, const Geom& g,
+            const std::vector<double>& poly, const cplx_t<T>* fields, int nfields, int mode, double* grad,
+            double2* out2, int accumulate, const int* status, cudaStream_t s, GradScale gs = GradScale());
 
 }  // namespace fb

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <algorithm>
+#include <vector>
 
 #include "nufft.cuh"
 #include "scan.cuh"
@@ -225,16 +226,16 @@ template <int W, typename T, bool CPLX>
 __global__ void __launch_bounds__(Phased2D<W>::THREADS) spread2d_phased_kernel(
     const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, T uniform,
     const cplx_t<T>* __restrict__ strengths, const int* __restrict__ sub_bin, const int* __restrict__ sub_start,
-    const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g, T beta, T* grid_real,
+    const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g, const EsPoly<W, T> poly, T* grid_real,
     cplx_t<T>* grid_cplx) {
   using P = Phased2D<W>;
   constexpr int NC = CPLX ? 2 : 1;
   constexpr int PAD = W / 2;
   constexpr int TW = kTile2D + W;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* tile = reinterpret_cast<T*>(smem_raw);
-  int* list = reinterpret_cast<int*>(tile + TW * TW * NC);
-  int* code = list + kMaxSub;
+  Rec<2, T>* srec = reinterpret_cast<Rec<2, T>*>(smem_raw);  // subproblem's records, grouped by sub-block
+  T* tile = reinterpret_cast<T*>(srec + kMaxSub);
+  int* code = reinterpret_cast<int*>(tile + TW * TW * NC);
   int* sb_count = code + kMaxSub;
   int* sb_start = sb_count + P::NSB * P::NSB;
 
@@ -263,55 +264,76 @@ __global__ void __launch_bounds__(Phased2D<W>::THREADS) spread2d_phased_kernel(
     }
   }
   __syncthreads();
-  for (int p = threadIdx.x; p < cnt; p += blockDim.x) list[sb_start[code[p] >> 16] + (code[p] & 0xffff)] = p;
+  for (int p = threadIdx.x; p < cnt; p += blockDim.x) srec[sb_start[code[p] >> 16] + (code[p] & 0xffff)] = recs[start + p];
   __syncthreads();
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int grp = lane / P::GROUP, row = lane % P::GROUP;
   const int q = warp * P::GPW + grp;  // this lane group's slot within a phase
   const int qa = q % (P::NSB / 2), qb = q / (P::NSB / 2);
-  const T inv_half = T(2) / T(W);
+  // each lane evaluates one tap (its footprint row) for every point: keep that
+  // tap's polynomial in registers (idle lanes take a valid row)
+  constexpr int Q = EsPolyDeg<W>::Q;
+  T cr[Q + 1];
+  {
+    const int trow = row < W ? row : W - 1;
+#pragma unroll
+    for (int m = 0; m < W; ++m)
+      if (m == trow) {
+#pragma unroll
+        for (int d = 0; d <= Q; ++d) cr[d] = poly.c[m][d];
+      }
+  }
   for (int phase = 0; phase < 4; ++phase) {
     const int sbi = (2 * qa + (phase & 1)) + P::NSB * (2 * qb + (phase >> 1));
     const int my_n = sb_count[sbi], my_base = sb_start[sbi];
     int n_max = my_n;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) n_max = max(n_max, __shfl_xor_sync(0xffffffffu, n_max, o));
+    // software pipeline: the taps of point it+1 are formed before point it is added
+    T kx = T(0), wr = T(0), wi = T(0);
+    int base = 0;
+    bool active = false;
+#define FB_PHASED_LOAD(IT, KX, WR, WI, BASE, ACT)                                      \
+  {                                                                                    \
+    ACT = (IT) < my_n;                                                                 \
+    KX = T(0);                                                                         \
+    WR = T(0);                                                                         \
+    WI = T(0);                                                                         \
+    BASE = 0;                                                                          \
+    if (ACT) {                                                                         \
+      const Rec<2, T> r_ = srec[my_base + (IT)];                                       \
+      int c0_, c1_, c2_;                                                               \
+      unpack_cell(2, r_.cell, c0_, c1_, c2_);                                          \
+      T u0_, u1_;                                                                      \
+      const int s0_ = es_start<W, T>(r_.f[0], u0_);                                    \
+      const int s1_ = es_start<W, T>(r_.f[1], u1_);                                    \
+      T a_ = cr[Q], b_ = cr[Q];                                                        \
+      _Pragma("unroll") for (int d_ = Q - 1; d_ >= 0; --d_) {                          \
+        a_ = fma(a_, u0_, cr[d_]);                                                     \
+        b_ = fma(b_, u1_, cr[d_]);                                                     \
+      }                                                                                \
+      KX = a_;                                                                         \
+      T sr_, si_ = T(0);                                                               \
+      if (CPLX) {                                                                      \
+        const cplx_t<T> v_ = strengths[r_.idx];                                        \
+        sr_ = v_.x;                                                                    \
+        si_ = v_.y;                                                                    \
+      } else {                                                                         \
+        sr_ = weights ? weights[r_.idx] : uniform;                                     \
+      }                                                                                \
+      WR = sr_ * b_;                                                                   \
+      WI = si_ * b_;                                                                   \
+      BASE = ((c1_ - org1 + s1_ + PAD + row) * TW + (c0_ - org0 + s0_ + PAD)) * NC;    \
+    }                                                                                  \
+  }
+    FB_PHASED_LOAD(0, kx, wr, wi, base, active)
     for (int it = 0; it < n_max; ++it) {
-      const bool active = it < my_n;
-      T kx = T(0), ky = T(0), sr = T(0), si = T(0);
-      int l0 = 0, l1 = 0;
-      if (active) {
-        const int p = list[my_base + it];
-        const Rec<2, T> r = recs[start + p];
-        int c0, c1, c2;
-        unpack_cell(2, r.cell, c0, c1, c2);
-        const T f0 = r.f[0], f1 = r.f[1];
-        const int s0 = (W % 2 == 0) ? (-W / 2 + (f0 > T(0) ? 1 : 0)) : (-(W - 1) / 2 + (f0 > T(0.5) ? 1 : 0));
-        const int s1 = (W % 2 == 0) ? (-W / 2 + (f1 > T(0) ? 1 : 0)) : (-(W - 1) / 2 + (f1 > T(0.5) ? 1 : 0));
-        l0 = c0 - org0 + s0 + PAD;
-        l1 = c1 - org1 + s1 + PAD;
-        if (row < W) {
-          const T zx = (T(s0 + row) - f0) * inv_half, zy = (T(s1 + row) - f1) * inv_half;
-          const T ax = T(1) - zx * zx, ay = T(1) - zy * zy;
-          if (sizeof(T) == 4) {
-            kx = ax >= T(0) ? T(expf(float(beta) * (sqrtf(float(ax)) - 1.0f))) : T(0);
-            ky = ay >= T(0) ? T(expf(float(beta) * (sqrtf(float(ay)) - 1.0f))) : T(0);
-          } else {
-            kx = ax >= T(0) ? T(exp(double(beta) * (sqrt(double(ax)) - 1.0))) : T(0);
-            ky = ay >= T(0) ? T(exp(double(beta) * (sqrt(double(ay)) - 1.0))) : T(0);
-          }
-        }
-        if (CPLX) {
-          const cplx_t<T> v = strengths[r.idx];
-          sr = v.x;
-          si = v.y;
-        } else {
-          sr = weights ? weights[r.idx] : uniform;
-        }
-      }
-      const T wr = sr * ky, wi = si * ky;
-      T* rowp = tile + ((l1 + row) * TW + l0) * NC;
+      T nkx, nwr, nwi;
+      int nbase;
+      bool nact;
+      FB_PHASED_LOAD(it + 1, nkx, nwr, nwi, nbase, nact)
+      T* rowp = tile + base;
 #pragma unroll
       for (int m = 0; m < W; ++m) {
         const T km = __shfl_sync(0xffffffffu, kx, grp * P::GROUP + m);
@@ -325,7 +347,13 @@ __global__ void __launch_bounds__(Phased2D<W>::THREADS) spread2d_phased_kernel(
         }
       }
       __syncwarp();
+      kx = nkx;
+      wr = nwr;
+      wi = nwi;
+      base = nbase;
+      active = nact;
     }
+#undef FB_PHASED_LOAD
     __syncthreads();
   }
   Geom gt = g;
@@ -341,7 +369,8 @@ __global__ void __launch_bounds__(256) spread_kernel(const Rec<D, T>* __restrict
                                                      T uniform, const cplx_t<T>* __restrict__ strengths,
                                                      const int* __restrict__ sub_bin, const int* __restrict__ sub_start,
                                                      const int* __restrict__ sub_count, const int* __restrict__ num_sub,
-                                                     Geom g, T beta, T* grid_real, cplx_t<T>* grid_cplx) {
+                                                     Geom g, const EsPoly<W, T> poly, T* grid_real,
+                                                     cplx_t<T>* grid_cplx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tile = reinterpret_cast<T*>(smem_raw);
   const int sub = blockIdx.x;
@@ -374,7 +403,7 @@ __global__ void __launch_bounds__(256) spread_kernel(const Rec<D, T>* __restrict
       sr = weights ? weights[rec.idx] : uniform;
     }
     T k0[W];
-    const int l0 = c0 - org0 + es_taps<W, T>(rec.f[0], beta, k0) + PAD;
+    const int l0 = c0 - org0 + es_taps<W, T>(rec.f[0], poly, k0) + PAD;
     if (D == 1) {
 #pragma unroll
       for (int m0 = 0; m0 < W; ++m0) {
@@ -388,12 +417,12 @@ __global__ void __launch_bounds__(256) spread_kernel(const Rec<D, T>* __restrict
       continue;
     }
     T k1[W];
-    const int l1 = c1 - org1 + es_taps<W, T>(rec.f[D >= 2 ? 1 : 0], beta, k1) + PAD;
+    const int l1 = c1 - org1 + es_taps<W, T>(rec.f[D >= 2 ? 1 : 0], poly, k1) + PAD;
     int nz = 1;
     T k2[W];
     int l2 = 0;
     if (D == 3) {
-      l2 = c2 - org2 + es_taps<W, T>(rec.f[D >= 3 ? 2 : 0], beta, k2) + PAD;
+      l2 = c2 - org2 + es_taps<W, T>(rec.f[D >= 3 ? 2 : 0], poly, k2) + PAD;
       nz = W;
     }
     for (int m2 = 0; m2 < nz; ++m2) {
@@ -422,10 +451,10 @@ __global__ void __launch_bounds__(256) spread_kernel(const Rec<D, T>* __restrict
 // Epilogue shared by the interpolation kernels.
 template <int D, typename T>
 __device__ __forceinline__ void interp_store(int mode, uint32_t o, T wgt, T v0r, T v0i, T v1r, bool bad, double* grad,
-                                             double2* out2, int accumulate) {
+                                             double2* out2, int accumulate, const GradScale& gs) {
   if (mode == INTERP_GRAD) {
     const double cw = double(wgt);
-    const double gv[3] = {cw * double(v0r), cw * double(v0i), cw * double(v1r)};
+    const double gv[3] = {cw * double(v0r) * gs.s[0], cw * double(v0i) * gs.s[1], cw * double(v1r) * gs.s[2]};
 #pragma unroll
     for (int a = 0; a < D; ++a) {
       const double val = bad ? __longlong_as_double(0x7ff8000000000000ULL) : gv[a];
@@ -442,9 +471,9 @@ __device__ __forceinline__ void interp_store(int mode, uint32_t o, T wgt, T v0r,
 template <int W, typename T>
 __global__ void __launch_bounds__(256) interp2d_tile_kernel(
     const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, T uniform, const int* __restrict__ sub_bin,
-    const int* __restrict__ sub_start, const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g, T beta,
-    const cplx_t<T>* __restrict__ field, int mode, double* grad, double2* out2, int accumulate,
-    const int* __restrict__ status) {
+    const int* __restrict__ sub_start, const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g,
+    const EsPoly<W, T> poly, const cplx_t<T>* __restrict__ field, int mode, double* grad, double2* out2, int accumulate,
+    const int* __restrict__ status, const GradScale gs) {
   constexpr int PAD = W / 2;
   constexpr int TW = kTile2D + W;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -467,8 +496,8 @@ __global__ void __launch_bounds__(256) interp2d_tile_kernel(
     int c0, c1, c2;
     unpack_cell(2, r.cell, c0, c1, c2);
     T k0[W], k1[W];
-    const int s0 = es_taps<W, T>(r.f[0], beta, k0);
-    const int s1 = es_taps<W, T>(r.f[1], beta, k1);
+    const int s0 = es_taps<W, T>(r.f[0], poly, k0);
+    const int s1 = es_taps<W, T>(r.f[1], poly, k1);
     const int l0 = c0 - org0 + s0 + PAD, l1 = c1 - org1 + s1 + PAD;
     T vr = 0, vi = 0;
 #pragma unroll
@@ -485,7 +514,7 @@ __global__ void __launch_bounds__(256) interp2d_tile_kernel(
       vi += k1[m1] * ri;
     }
     const T wgt = (mode == INTERP_GRAD) ? (weights ? weights[r.idx] : uniform) : T(1);
-    interp_store<2, T>(mode, r.idx, wgt, vr, vi, T(0), bad, grad, out2, accumulate);
+    interp_store<2, T>(mode, r.idx, wgt, vr, vi, T(0), bad, grad, out2, accumulate, gs);
   }
 }
 
@@ -493,10 +522,11 @@ __global__ void __launch_bounds__(256) interp2d_tile_kernel(
 // directly from HBM/L2 (neighbouring threads share footprints).
 template <int D, int W, typename T, int NF>
 __global__ void __launch_bounds__(256) interp_kernel(const Rec<D, T>* __restrict__ recs, int64_t N,
-                                                     const T* __restrict__ weights, T uniform, Geom g, T beta,
-                                                     const cplx_t<T>* __restrict__ fields, int64_t G, int mode,
+                                                     const T* __restrict__ weights, T uniform, Geom g,
+                                                     const EsPoly<W, T> poly, const cplx_t<T>* __restrict__ fields,
+                                                     int64_t G, int mode,
                                                      double* grad, double2* out2, int accumulate,
-                                                     const int* __restrict__ status) {
+                                                     const int* __restrict__ status, const GradScale gs) {
   const bool bad = status != nullptr && ((*status) & STATUS_NONFINITE_INPUT);
   const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
   for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < N; j += int64_t(gridDim.x) * blockDim.x) {
@@ -505,12 +535,12 @@ __global__ void __launch_bounds__(256) interp_kernel(const Rec<D, T>* __restrict
     unpack_cell(D, rec.cell, c0, c1, c2);
     T k0[W], k1[W], k2[W];
     int ix[W];
-    const int s0 = es_taps<W, T>(rec.f[0], beta, k0);
+    const int s0 = es_taps<W, T>(rec.f[0], poly, k0);
 #pragma unroll
     for (int m = 0; m < W; ++m) ix[m] = wrap_index(c0 + s0 + m, nf0);
     int s1 = 0, s2 = 0;
-    if (D >= 2) s1 = es_taps<W, T>(rec.f[D >= 2 ? 1 : 0], beta, k1);
-    if (D >= 3) s2 = es_taps<W, T>(rec.f[D >= 3 ? 2 : 0], beta, k2);
+    if (D >= 2) s1 = es_taps<W, T>(rec.f[D >= 2 ? 1 : 0], poly, k1);
+    if (D >= 3) s2 = es_taps<W, T>(rec.f[D >= 3 ? 2 : 0], poly, k2);
     T v0r = 0, v0i = 0, v1r = 0, v1i = 0;
     const int nz = (D == 3) ? W : 1;
     const int ny = (D >= 2) ? W : 1;
@@ -543,7 +573,7 @@ __global__ void __launch_bounds__(256) interp_kernel(const Rec<D, T>* __restrict
       }
     }
     const T wgt = (mode == INTERP_GRAD) ? (weights ? weights[rec.idx] : uniform) : T(1);
-    interp_store<D, T>(mode, rec.idx, wgt, v0r, v0i, v1r, bad, grad, out2, accumulate);
+    interp_store<D, T>(mode, rec.idx, wgt, v0r, v0i, v1r, bad, grad, out2, accumulate, gs);
   }
 }
 
@@ -594,58 +624,61 @@ void bin_sort(const double* pts, int64_t N, const MapParams& mp, const Geom& g, 
 
 template <int W, typename T, bool CPLX>
 void launch_spread2d(const void* recs, const T* weights, T uniform, const cplx_t<T>* strengths, const SortBufs& sb,
-                     const Geom& g, double beta, T* grid_real, cplx_t<T>* grid_cplx, cudaStream_t s) {
+                     const Geom& g, const std::vector<double>& poly, T* grid_real, cplx_t<T>* grid_cplx,
+                     cudaStream_t s) {
   using P = Phased2D<W>;
   constexpr int TW = kTile2D + W;
-  const size_t smem = sizeof(T) * TW * TW * (CPLX ? 2 : 1) + sizeof(int) * (2 * kMaxSub + 2 * P::NSB * P::NSB);
+  const size_t smem = sizeof(Rec<2, T>) * kMaxSub + sizeof(T) * TW * TW * (CPLX ? 2 : 1) +
+                      sizeof(int) * (kMaxSub + 2 * P::NSB * P::NSB);
   auto kern = spread2d_phased_kernel<W, T, CPLX>;
   if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   kern<<<unsigned(sb.max_sub), P::THREADS, smem, s>>>(static_cast<const Rec<2, T>*>(recs), weights, uniform, strengths,
                                                        sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g,
-                                                       T(beta), grid_real, grid_cplx);
+                                                       make_es_poly<W, T>(poly), grid_real, grid_cplx);
   FB_LAUNCH_CHECK();
 }
 
 template <int D, int W, typename T, bool CPLX>
 void launch_spread_generic(const void* recs, const T* weights, T uniform, const cplx_t<T>* strengths,
-                           const SortBufs& sb, const Geom& g, double beta, T* grid_real, cplx_t<T>* grid_cplx,
-                           cudaStream_t s) {
+                           const SortBufs& sb, const Geom& g, const std::vector<double>& poly, T* grid_real,
+                           cplx_t<T>* grid_cplx, cudaStream_t s) {
   const size_t smem = size_t(g.tile_cells()) * sizeof(T) * (CPLX ? 2 : 1);
   auto kern = spread_kernel<D, W, T, CPLX>;
   if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<D, T>*>(recs), weights, uniform, strengths,
-                                                sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g, T(beta),
-                                                grid_real, grid_cplx);
+                                                sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g,
+                                                make_es_poly<W, T>(poly), grid_real, grid_cplx);
   FB_LAUNCH_CHECK();
 }
 
 template <int W, typename T>
-void launch_interp2d(const void* recs, const T* weights, T uniform, const SortBufs& sb, const Geom& g, double beta,
-                     const cplx_t<T>* field, int mode, double* grad, double2* out2, int acc, const int* status,
-                     cudaStream_t s) {
+void launch_interp2d(const void* recs, const T* weights, T uniform, const SortBufs& sb, const Geom& g,
+                     const std::vector<double>& poly, const cplx_t<T>* field, int mode, double* grad, double2* out2,
+                     int acc, const int* status, cudaStream_t s, const GradScale& gs) {
   constexpr int TW = kTile2D + W;
   const size_t smem = sizeof(cplx_t<T>) * TW * TW;
   auto kern = interp2d_tile_kernel<W, T>;
   if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<2, T>*>(recs), weights, uniform, sb.sub_bin.p,
-                                                sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g, T(beta), field, mode,
-                                                grad, out2, acc, status);
+                                                sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g,
+                                                make_es_poly<W, T>(poly), field, mode, grad, out2, acc, status, gs);
   FB_LAUNCH_CHECK();
 }
 
 template <int D, int W, typename T>
-void launch_interp_generic(const void* recs, int64_t N, const T* weights, T uniform, const Geom& g, double beta,
-                           const cplx_t<T>* fields, int nfields, int mode, double* grad, double2* out2, int acc,
-                           const int* status, cudaStream_t s) {
+void launch_interp_generic(const void* recs, int64_t N, const T* weights, T uniform, const Geom& g,
+                           const std::vector<double>& poly, const cplx_t<T>* fields, int nfields, int mode,
+                           double* grad, double2* out2, int acc, const int* status, cudaStream_t s,
+                           const GradScale& gs) {
   if (N <= 0) return;
   const int grid = point_grid(N, 16);
   const Rec<D, T>* r = static_cast<const Rec<D, T>*>(recs);
   if (nfields == 2) {
-    interp_kernel<D, W, T, 2><<<grid, 256, 0, s>>>(r, N, weights, uniform, g, T(beta), fields, g.G(), mode, grad, out2,
-                                                   acc, status);
+    interp_kernel<D, W, T, 2><<<grid, 256, 0, s>>>(r, N, weights, uniform, g, make_es_poly<W, T>(poly), fields, g.G(),
+                                                   mode, grad, out2, acc, status, gs);
   } else {
-    interp_kernel<D, W, T, 1><<<grid, 256, 0, s>>>(r, N, weights, uniform, g, T(beta), fields, g.G(), mode, grad, out2,
-                                                   acc, status);
+    interp_kernel<D, W, T, 1><<<grid, 256, 0, s>>>(r, N, weights, uniform, g, make_es_poly<W, T>(poly), fields, g.G(),
+                                                   mode, grad, out2, acc, status, gs);
   }
   FB_LAUNCH_CHECK();
 }
@@ -681,21 +714,21 @@ void launch_interp_generic(const void* recs, int64_t N, const T* weights, T unif
 
 template <typename T, bool CPLX>
 void spread_dispatch(const void* recs, const T* weights, T uniform, const cplx_t<T>* strengths, const SortBufs& sb,
-                     const Geom& g, double beta, T* grid_real, cplx_t<T>* grid_cplx, cudaStream_t s) {
+                     const Geom& g, const std::vector<double>& poly, T* grid_real, cplx_t<T>* grid_cplx, cudaStream_t s) {
   if (g.D == 2) {
 #define FB_S2(WW) \
-  launch_spread2d<FB_WCLAMP(T, WW), T, CPLX>(recs, weights, uniform, strengths, sb, g, beta, grid_real, grid_cplx, s)
+  launch_spread2d<FB_WCLAMP(T, WW), T, CPLX>(recs, weights, uniform, strengths, sb, g, poly, grid_real, grid_cplx, s)
     FB_FOR_W(T, FB_S2)
 #undef FB_S2
   } else if (g.D == 1) {
 #define FB_S1(WW)                                                                                                \
-  launch_spread_generic<1, FB_WCLAMP(T, WW), T, CPLX>(recs, weights, uniform, strengths, sb, g, beta, grid_real, \
+  launch_spread_generic<1, FB_WCLAMP(T, WW), T, CPLX>(recs, weights, uniform, strengths, sb, g, poly, grid_real, \
                                                       grid_cplx, s)
     FB_FOR_W(T, FB_S1)
 #undef FB_S1
   } else {
 #define FB_S3(WW)                                                                                                \
-  launch_spread_generic<3, FB_WCLAMP(T, WW), T, CPLX>(recs, weights, uniform, strengths, sb, g, beta, grid_real, \
+  launch_spread_generic<3, FB_WCLAMP(T, WW), T, CPLX>(recs, weights, uniform, strengths, sb, g, poly, grid_real, \
                                                       grid_cplx, s)
     FB_FOR_W(T, FB_S3)
 #undef FB_S3
@@ -703,43 +736,43 @@ void spread_dispatch(const void* recs, const T* weights, T uniform, const cplx_t
 }
 
 template <typename T>
-void spread_real(const void* recs, const T* weights, T uniform, const SortBufs& sb, const Geom& g, double beta, T* grid,
-                 cudaStream_t s) {
-  spread_dispatch<T, false>(recs, weights, uniform, nullptr, sb, g, beta, grid, nullptr, s);
+void spread_real(const void* recs, const T* weights, T uniform, const SortBufs& sb, const Geom& g,
+                 const std::vector<double>& poly, T* grid, cudaStream_t s) {
+  spread_dispatch<T, false>(recs, weights, uniform, nullptr, sb, g, poly, grid, nullptr, s);
 }
 
 template <typename T>
-void spread_cplx(const void* recs, const cplx_t<T>* strengths, const SortBufs& sb, const Geom& g, double beta,
-                 cplx_t<T>* grid, cudaStream_t s) {
-  spread_dispatch<T, true>(recs, nullptr, T(1), strengths, sb, g, beta, nullptr, grid, s);
+void spread_cplx(const void* recs, const cplx_t<T>* strengths, const SortBufs& sb, const Geom& g,
+                 const std::vector<double>& poly, cplx_t<T>* grid, cudaStream_t s) {
+  spread_dispatch<T, true>(recs, nullptr, T(1), strengths, sb, g, poly, nullptr, grid, s);
 }
 
 template <typename T>
-void interp(const void* recs, int64_t N, const T* weights, T uniform, const SortBufs& sb, const Geom& g, double beta,
-            const cplx_t<T>* fields, int nfields, int mode, double* grad, double2* out2, int accumulate,
-            const int* status, cudaStream_t s) {
+void interp(const void* recs, int64_t N, const T* weights, T uniform, const SortBufs& sb, const Geom& g,
+            const std::vector<double>& poly, const cplx_t<T>* fields, int nfields, int mode, double* grad,
+            double2* out2, int accumulate, const int* status, cudaStream_t s, GradScale gs) {
   if (g.D == 2 && nfields == 1) {
 #define FB_I2(WW)                                                                                                  \
-  launch_interp2d<FB_WCLAMP(T, WW), T>(recs, weights, uniform, sb, g, beta, fields, mode, grad, out2, accumulate, \
-                                       status, s)
+  launch_interp2d<FB_WCLAMP(T, WW), T>(recs, weights, uniform, sb, g, poly, fields, mode, grad, out2, accumulate, \
+                                       status, s, gs)
     FB_FOR_W(T, FB_I2)
 #undef FB_I2
   } else if (g.D == 1) {
 #define FB_I1(WW)                                                                                             \
-  launch_interp_generic<1, FB_WCLAMP(T, WW), T>(recs, N, weights, uniform, g, beta, fields, nfields, mode, grad, \
-                                                out2, accumulate, status, s)
+  launch_interp_generic<1, FB_WCLAMP(T, WW), T>(recs, N, weights, uniform, g, poly, fields, nfields, mode, grad, \
+                                                out2, accumulate, status, s, gs)
     FB_FOR_W(T, FB_I1)
 #undef FB_I1
   } else if (g.D == 2) {
 #define FB_I2G(WW)                                                                                            \
-  launch_interp_generic<2, FB_WCLAMP(T, WW), T>(recs, N, weights, uniform, g, beta, fields, nfields, mode, grad, \
-                                                out2, accumulate, status, s)
+  launch_interp_generic<2, FB_WCLAMP(T, WW), T>(recs, N, weights, uniform, g, poly, fields, nfields, mode, grad, \
+                                                out2, accumulate, status, s, gs)
     FB_FOR_W(T, FB_I2G)
 #undef FB_I2G
   } else {
 #define FB_I3(WW)                                                                                             \
-  launch_interp_generic<3, FB_WCLAMP(T, WW), T>(recs, N, weights, uniform, g, beta, fields, nfields, mode, grad, \
-                                                out2, accumulate, status, s)
+  launch_interp_generic<3, FB_WCLAMP(T, WW), T>(recs, N, weights, uniform, g, poly, fields, nfields, mode, grad, \
+                                                out2, accumulate, status, s, gs)
     FB_FOR_W(T, FB_I3)
 #undef FB_I3
   }
@@ -748,10 +781,11 @@ void interp(const void* recs, int64_t N, const T* weights, T uniform, const Sort
 #define FB_INSTANTIATE_NUFFT(T)                                                                                     \
   template void bin_sort<T>(const double*, int64_t, const MapParams&, const Geom&, SortBufs&, void*, int*,          \
                             cudaStream_t);                                                                           \
-  template void spread_real<T>(const void*, const T*, T, const SortBufs&, const Geom&, double, T*, cudaStream_t);   \
-  template void spread_cplx<T>(const void*, const cplx_t<T>*, const SortBufs&, const Geom&, double, cplx_t<T>*,     \
-                               cudaStream_t);                                                                        \
-  template void interp<T>(const void*, int64_t, const T*, T, const SortBufs&, const Geom&, double, const cplx_t<T>*, \
-                          int, int, double*, double2*, int, const int*, cudaStream_t);
+  template void spread_real<T>(const void*, const T*, T, const SortBufs&, const Geom&, const std::vector<double>&,    \
+                               T*, cudaStream_t);                                                                    \
+  template void spread_cplx<T>(const void*, const cplx_t<T>*, const SortBufs&, const Geom&,                         \
+                               const std::vector<double>&, cplx_t<T>*, cudaStream_t);                                \
+  template void interp<T>(const void*, int64_t, const T*, T, const SortBufs&, const Geom&, const std::vector<double>&, \
+                          const cplx_t<T>*, int, int, double*, double2*, int, const int*, cudaStream_t, GradScale);
 
 }  // namespace fb

@@ -1,0 +1,276 @@
+// NUwNU: structure-factor loss of a point pattern at non-uniform k-points
+// (source/fresco/nuwnu.hpp:17-291).
+//
+// Reference semantics: x_j = (p_j - round(p_j/L) + L) 2 pi / L in both the
+// energy and the gradient (nuwnu.hpp:134, 193), frequencies s_k = K_k used
+// as given (no 2 pi / L, nuwnu.hpp:47-76), rho_k = sum_j c_j exp(+i s_k.x_j)
+// (type 3, iflag +1), S = |rho|^2/N, d = (S - S0)/S0', phi = sum V d^2,
+// factor_k = (-4i/N) V d rho / S0' and grad[D j + a] =
+// Re(sum_k s_k[a] factor_k exp(-i s_k.x_j)) (type 3, iflag -1; the reference
+// omits conj(c_j) here, nuwnu.hpp:269, and so does this implementation).
+//
+// B200 form: both transforms are evaluated as exact FP64 direct sums, O(N M),
+// which is the fastest form for the few-peak targets this loss is used with
+// (examples/NUwNU.ipynb: 5 k-points) and more accurate than a type-3 NUFFT.
+// The forward sum runs over (point chunks) x (frequency chunks) with block
+// reductions; the adjoint is one thread per point with the frequencies
+// staged in shared memory.  The `precision` argument is accepted; the
+// arithmetic is FP64 either way.
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "potential.cuh"
+
+namespace fb {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kFreqChunk = 8;    // frequencies per block in the forward sum
+constexpr int kAdjTile = 512;    // frequencies staged per shared-memory tile in the adjoint
+constexpr double kPi = 3.14159265358979323846;
+
+__device__ __forceinline__ double nuwnu_coord(const double* __restrict__ p, int64_t j, int a, int D, double L) {
+  const double v = p[j * D + a];
+  return (v - round(v / L) + L) * 2 * kPi / L;  // nuwnu.hpp:134 / 193, same operation order
+}
+
+template <int D>
+__global__ void __launch_bounds__(kThreads) nuwnu_forward_kernel(const double* __restrict__ pts, int64_t N,
+                                                                  const double* __restrict__ s, int64_t M,
+                                                                  const double* __restrict__ c, double cu,
+                                                                  double L0, double L1, double L2, double2* rho,
+                                                                  int* status) {
+  const int64_t k0 = int64_t(blockIdx.y) * kFreqChunk;
+  double sk[kFreqChunk][D];
+#pragma unroll
+  for (int q = 0; q < kFreqChunk; ++q)
+#pragma unroll
+    for (int a = 0; a < D; ++a) sk[q][a] = (k0 + q < M) ? s[(k0 + q) * D + a] : 0.0;
+  double re[kFreqChunk], im[kFreqChunk];
+#pragma unroll
+  for (int q = 0; q < kFreqChunk; ++q) re[q] = im[q] = 0.0;
+  const double Ls[3] = {L0, L1, L2};
+  bool bad = false;
+  for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < N; j += int64_t(gridDim.x) * blockDim.x) {
+    double x[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      x[a] = nuwnu_coord(pts, j, a, D, Ls[a]);
+      bad |= !isfinite(x[a]);
+    }
+    const double cj = c ? c[j] : cu;
+#pragma unroll
+    for (int q = 0; q < kFreqChunk; ++q) {
+      double ph = 0.0;
+#pragma unroll
+      for (int a = 0; a < D; ++a) ph += sk[q][a] * x[a];
+      double sn, cs;
+      sincos(ph, &sn, &cs);
+      re[q] += cj * cs;
+      im[q] += cj * sn;
+    }
+  }
+  if (bad && blockIdx.y == 0) raise_status(status, STATUS_NONFINITE_INPUT);
+  __shared__ double red[2 * kFreqChunk][kThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < kFreqChunk; ++q) {
+    const double a = warp_sum(re[q]), b = warp_sum(im[q]);
+    if (lane == 0) {
+      red[2 * q][wid] = a;
+      red[2 * q + 1][wid] = b;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * kFreqChunk) {
+    double t = 0.0;
+    for (int w = 0; w < int(blockDim.x) / 32; ++w) t += red[threadIdx.x][w];
+    const int q = threadIdx.x / 2;
+    if (k0 + q < M) atomicAdd((threadIdx.x & 1) ? &rho[k0 + q].y : &rho[k0 + q].x, t);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) nuwnu_loss_kernel(const double2* __restrict__ rho, int64_t M, double invN,
+                                                              const double* __restrict__ sk,
+                                                              const double* __restrict__ v, double* energy,
+                                                              double2* factor, const int* __restrict__ status) {
+  double phi = 0.0;
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < M; k += int64_t(gridDim.x) * blockDim.x) {
+    const double2 r = rho[k];
+    const double s0 = sk[k];
+    const double dn = s0 != 0.0 ? s0 : 1.0;
+    const double d = ((r.x * r.x + r.y * r.y) * invN - s0) / dn;
+    phi += v[k] * d * d;
+    // factor = (-4i/N) V d rho / S0'
+    const double a = 4.0 * invN * v[k] * d / dn;
+    factor[k] = make_double2(a * r.y, -a * r.x);
+  }
+  block_sum_atomic(phi, energy);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && ((*status) & STATUS_NONFINITE_INPUT))
+    atomicAdd(energy, __longlong_as_double(0x7ff8000000000000ULL));
+}
+
+template <int D>
+__global__ void __launch_bounds__(kThreads) nuwnu_adjoint_kernel(const double* __restrict__ pts, int64_t N,
+                                                                  const double* __restrict__ s, int64_t M,
+                                                                  const double2* __restrict__ factor, double L0,
+                                                                  double L1, double L2, double* grad, int accumulate,
+                                                                  const int* __restrict__ status,
+                                                                  const double* __restrict__ c, double cu, int exact) {
+  __shared__ double ss[kAdjTile * D];
+  __shared__ double2 sf[kAdjTile];
+  const double Ls[3] = {L0, L1, L2};
+  const bool bad = (*status) & STATUS_NONFINITE_INPUT;
+  for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < N; base += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t j = base + threadIdx.x;
+    const bool active = j < N;
+    double x[D], g[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      x[a] = active ? nuwnu_coord(pts, j, a, D, Ls[a]) : 0.0;
+      g[a] = 0.0;
+    }
+    for (int64_t t0 = 0; t0 < M; t0 += kAdjTile) {
+      __syncthreads();
+      const int cnt = int((M - t0) < kAdjTile ? (M - t0) : kAdjTile);
+      for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+#pragma unroll
+        for (int a = 0; a < D; ++a) ss[q * D + a] = s[(t0 + q) * D + a];
+        sf[q] = factor[t0 + q];
+      }
+      __syncthreads();
+      if (active) {
+        for (int q = 0; q < cnt; ++q) {
+          double ph = 0.0;
+#pragma unroll
+          for (int a = 0; a < D; ++a) ph += ss[q * D + a] * x[a];
+          double sn, cs;
+          sincos(-ph, &sn, &cs);
+          const double2 fq = sf[q];
+          const double re = fq.x * cs - fq.y * sn;  // Re(factor * exp(-i ph))
+#pragma unroll
+          for (int a = 0; a < D; ++a) g[a] += ss[q * D + a] * re;
+        }
+      }
+    }
+    if (active) {
+      const double nan = __longlong_as_double(0x7ff8000000000000ULL);
+      // exact derivative: c_j * (2 pi / L) times the reference's value
+      const double cj = exact ? (c ? c[j] : cu) : 1.0;
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        double* dst = grad + j * D + a;
+        const double v = bad ? nan : (exact ? g[a] * cj * 2 * kPi / Ls[a] : g[a]);
+        *dst = accumulate ? *dst + v : v;
+      }
+    }
+  }
+}
+
+template <int D>
+class NUwNUImpl final : public Potential {
+ public:
+  NUwNUImpl(const std::vector<double>& radii, const std::vector<double>& kpts, const std::vector<double>& sk,
+            const std::vector<double>& v, const std::vector<double>& L)
+      : N_(int64_t(radii.size())) {
+    init_status();
+    if (sk.size() != v.size()) throw InvalidArgument("len(Sk) must equal len(V)");
+    M_ = int64_t(kpts.size()) / D;  // nuwnu.hpp:40
+    if (int64_t(sk.size()) < M_) throw InvalidArgument("Sk/V need one value per k-point");
+    for (int a = 0; a < D; ++a) L_[a] = L[a];
+    // weights, nuwnu.hpp:81-105 (area factor applied once per dimension)
+    std::vector<double> c(radii.size(), 1.0);
+    double sum = 0.0;
+    for (size_t i = 0; i < c.size(); ++i) {
+      for (int j = 0; j < D; ++j) {
+        if (D == 2) c[i] = c[i] * M_PI * radii[i] * radii[i];
+        else if (D == 3) c[i] = c[i] * M_PI * radii[i] * radii[i] * radii[i] * 4.0 / 3.0;
+      }
+      sum += c[i];
+    }
+    bool uniform = true;
+    for (size_t i = 0; i < c.size(); ++i) {
+      c[i] *= double(c.size()) / sum;
+      if (c[i] != c[0]) uniform = false;
+    }
+    if (uniform && !c.empty()) {
+      cu_ = c[0];
+    } else if (!c.empty()) {
+      c_.alloc(c.size());
+      FB_CUDA(cudaMemcpy(c_.p, c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice));
+    }
+    s_.alloc(std::max<int64_t>(M_ * D, 1));
+    sk_.alloc(std::max<int64_t>(M_, 1));
+    v_.alloc(std::max<int64_t>(M_, 1));
+    rho_.alloc(std::max<int64_t>(M_, 1));
+    factor_.alloc(std::max<int64_t>(M_, 1));
+    if (M_) {
+      FB_CUDA(cudaMemcpy(s_.p, kpts.data(), sizeof(double) * M_ * D, cudaMemcpyHostToDevice));
+      FB_CUDA(cudaMemcpy(sk_.p, sk.data(), sizeof(double) * M_, cudaMemcpyHostToDevice));
+      FB_CUDA(cudaMemcpy(v_.p, v.data(), sizeof(double) * M_, cudaMemcpyHostToDevice));
+    }
+  }
+
+  int64_t ndof() const override { return N_ * D; }
+  std::string kind() const override { return "NUwNU"; }
+  std::string describe() const override {
+    return "NUwNU D=" + std::to_string(D) + " N=" + std::to_string(N_) + " kpoints=" + std::to_string(M_) +
+           " exact FP64 direct sums";
+  }
+
+  void energy(const double* x, int64_t n, double* e, bool acc, cudaStream_t s) override { run(x, nullptr, e, acc, s); }
+  void energy_gradient(const double* x, int64_t n, double* g, double* e, bool acc, cudaStream_t s) override {
+    run(x, g, e, acc, s);
+  }
+
+ private:
+  void run(const double* x, double* g, double* e, bool acc, cudaStream_t s) {
+    timer_begin(s);
+    begin_eval_status(s);
+    if (!acc) FB_CUDA(cudaMemsetAsync(e, 0, sizeof(double), s));
+    if (M_ == 0 || N_ == 0) {
+      if (g && !acc) FB_CUDA(cudaMemsetAsync(g, 0, sizeof(double) * N_ * D, s));
+      return;
+    }
+    FB_CUDA(cudaMemsetAsync(rho_.p, 0, sizeof(double2) * M_, s));
+    const int pblocks = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(N_, kThreads), 2 * int64_t(sm_count()))));
+    dim3 fg(pblocks, unsigned(ceil_div(M_, kFreqChunk)));
+    nuwnu_forward_kernel<D><<<fg, kThreads, 0, s>>>(x, N_, s_.p, M_, c_.p, cu_, L_[0], L_[1], L_[2], rho_.p,
+                                                    status_.p);
+    FB_LAUNCH_CHECK();
+    const int mg = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(M_, kThreads), int64_t(sm_count()) * 4)));
+    nuwnu_loss_kernel<<<mg, kThreads, 0, s>>>(rho_.p, M_, 1.0 / double(N_), sk_.p, v_.p, e, factor_.p, status_.p);
+    FB_LAUNCH_CHECK();
+    timer_mark("forward", s);
+    if (!g) return;
+    const int ag = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(N_, kThreads), int64_t(sm_count()) * 8)));
+    nuwnu_adjoint_kernel<D><<<ag, kThreads, 0, s>>>(x, N_, s_.p, M_, factor_.p, L_[0], L_[1], L_[2], g,
+                                                    acc ? 1 : 0, status_.p, c_.p, cu_, grad_mode_ == 1 ? 1 : 0);
+    FB_LAUNCH_CHECK();
+    timer_mark("adjoint", s);
+  }
+
+  int64_t N_, M_ = 0;
+  double L_[3] = {1, 1, 1};
+  double cu_ = 1.0;
+  DevBuf<double> c_, s_, sk_, v_;
+  DevBuf<double2> rho_, factor_;
+};
+
+}  // namespace
+
+PotentialPtr make_nuwnu(const std::vector<double>& radii, const std::vector<double>& kpts,
+                        const std::vector<double>& sk, const std::vector<double>& v, const std::vector<double>& L,
+                        double eps, int precision) {
+  (void)eps;
+  (void)precision;
+  const int D = int(L.size());
+  if (D == 1) return PotentialPtr(new NUwNUImpl<1>(radii, kpts, sk, v, L));
+  if (D == 2) return PotentialPtr(new NUwNUImpl<2>(radii, kpts, sk, v, L));
+  if (D == 3) return PotentialPtr(new NUwNUImpl<3>(radii, kpts, sk, v, L));
+  throw std::runtime_error("Invalid dimension: " + std::to_string(D));
+}
+
+}  // namespace fb

@@ -153,6 +153,7 @@ class NUwUImpl final : public Potential {
 
     // ES kernel and fine grid
     es_ = es_params(eps, sizeof(T) == 4 ? 10 : 16);
+    poly_ = es_poly_coefficients(es_, es_.w);
     int64_t nf[3] = {1, 1, 1};
     for (int a = 0; a < D; ++a) nf[a] = fine_grid_size(n_, es_.w);
     int tile[3];
@@ -268,7 +269,7 @@ class NUwUImpl final : public Potential {
     bin_sort<T>(x, N_, mp, geom_, sort_, recs_.p, status_.p, s);
     timer_mark("sort", s);
     FB_CUDA(cudaMemsetAsync(spread_grid_.p, 0, spread_grid_.bytes(), s));
-    spread_real<T>(recs_.p, cw_.p, uniform_c_, sort_, geom_, es_.beta, spread_grid_.p, s);
+    spread_real<T>(recs_.p, cw_.p, uniform_c_, sort_, geom_, poly_, spread_grid_.p, s);
     timer_mark("spread", s);
     FB_CUFFT(cufftSetStream(plan_r2c_, s));
     if (sizeof(T) == 4) {
@@ -303,8 +304,11 @@ class NUwUImpl final : public Potential {
                             reinterpret_cast<cufftDoubleComplex*>(ggrid_.p), CUFFT_FORWARD));
     }
     timer_mark("fft_type2", s);
-    interp<T>(recs_.p, N_, cw_.p, uniform_c_, sort_, geom_, es_.beta, ggrid_.p, nfields_, INTERP_GRAD, g, nullptr,
-              acc ? 1 : 0, status_.p, s);
+    GradScale gs;  // exact mode: x = (p - round(p/L)) 2 pi / L, so d/dp = (2 pi / L) d/dx
+    if (grad_mode_ == 1)
+      for (int a = 0; a < D; ++a) gs.s[a] = 2.0 * M_PI / L_[a];
+    interp<T>(recs_.p, N_, cw_.p, uniform_c_, sort_, geom_, poly_, ggrid_.p, nfields_, INTERP_GRAD, g, nullptr,
+              acc ? 1 : 0, status_.p, s, gs);
     timer_mark("interp", s);
   }
 
@@ -316,6 +320,7 @@ class NUwUImpl final : public Potential {
   T uniform_c_ = T(1);
   DevBuf<T> cw_;
   ESParams es_;
+  std::vector<double> poly_;
   Geom geom_;
   SortBufs sort_;
   DevBuf<unsigned char> recs_;

@@ -98,6 +98,11 @@ void CombinedPotential::energy_gradient(const double* x, int64_t n, double* g, d
   }
 }
 
+void CombinedPotential::set_gradient_mode(int mode) {
+  grad_mode_ = mode;
+  for (auto& p : parts_) p->set_gradient_mode(mode);
+}
+
 int CombinedPotential::read_and_clear_status(cudaStream_t s) {
   int st = 0;
   for (auto& p : parts_) st |= p->read_and_clear_status(s);

@@ -32,6 +32,15 @@ class Potential {
   virtual int read_and_clear_status(cudaStream_t s);
 
   virtual std::string kind() const = 0;
+
+  // Gradient convention: 0 = the reference's own formula (default, drop-in
+  // parity), 1 = the exact derivative of the energy with respect to the input
+  // coordinates (what automatic differentiation needs).  They differ by the
+  // reference's scalings: NUwU and NUwNU return d/dx of the 2 pi-scaled NUFFT
+  // coordinate, UwNU divides by 2 pi, NUwNU drops conj(c_j), UwU halves the
+  // rho term and drops the d(1/R) term.
+  virtual void set_gradient_mode(int mode) { grad_mode_ = mode; }
+  int gradient_mode() const { return grad_mode_; }
   // Human-readable set-up summary (kernel width, grids, ...).
   virtual std::string describe() const { return kind(); }
 
@@ -55,6 +64,7 @@ class Potential {
   void timer_collect();                              // host sync; accumulates elapsed times
 
  protected:
+  int grad_mode_ = 0;
   DevBuf<int> status_;  // [0] current evaluation, [1] accumulated for the host
   void init_status();
   void begin_eval_status(cudaStream_t s) { FB_CUDA(cudaMemsetAsync(status_.p, 0, sizeof(int), s)); }
@@ -71,6 +81,7 @@ class CombinedPotential : public Potential {
   void energy(const double* x, int64_t n, double* e, bool acc, cudaStream_t s) override;
   void energy_gradient(const double* x, int64_t n, double* g, double* e, bool acc, cudaStream_t s) override;
   int read_and_clear_status(cudaStream_t s) override;
+  void set_gradient_mode(int mode) override;
   std::string kind() const override { return "CombinedPotential"; }
   const std::vector<PotentialPtr>& parts() const { return parts_; }
 

@@ -82,10 +82,10 @@ __global__ void __launch_bounds__(kThreads) uwu_modes_kernel(int64_t n_active, c
                                                              const UwuCoef* __restrict__ coef,
                                                              const cplx_t<T>* __restrict__ X, cplx_t<T>* H,
                                                              const double* __restrict__ part, int P, double* energy,
-                                                             int want_grad) {
+                                                             int want_grad, int exact, double* csum) {
   const double R = sum_partials(part, P);
   const double invR = 1.0 / R;
-  double phi = 0.0;
+  double phi = 0.0, cterm = 0.0;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n_active;
        i += int64_t(gridDim.x) * blockDim.x) {
     const int64_t h = hidx[i];
@@ -95,8 +95,10 @@ __global__ void __launch_bounds__(kThreads) uwu_modes_kernel(int64_t n_active, c
     const UwuCoef c = coef[i];
     const double d1 = q - c.s0, d2 = q - c.s0m;
     phi += c.w2 * d1 * d1 + c.w2m * d2 * d2;
+    // exact derivative: C = sum_k 2 V d S / (R S0') over all k (the d(1/R) term)
+    cterm += 2.0 * invR * q * (c.w2 * d1 + c.w2m * d2);
     if (want_grad) {
-      const double a = (c.A * q - c.B) * invR;
+      const double a = (c.A * q - c.B) * invR * (exact ? 2.0 : 1.0);
       cplx_t<T> out;
       out.x = T(xr * a);
       out.y = T(xi * a);
@@ -104,6 +106,14 @@ __global__ void __launch_bounds__(kThreads) uwu_modes_kernel(int64_t n_active, c
     }
   }
   block_sum_atomic(phi, energy);
+  if (exact) block_sum_atomic(cterm, csum);
+}
+
+// Exact derivative: subtract C from every output by lowering the k = 0 term
+// of the C2R input (its real part reaches every grid point once).
+template <typename T>
+__global__ void uwu_offset_kernel(cplx_t<T>* H, const double* __restrict__ csum) {
+  H[0].x = T(double(H[0].x) - *csum);
 }
 
 template <typename T>
@@ -177,6 +187,7 @@ class UwUImpl final : public Potential {
     }
     P_ = std::max(1, std::min(1024, 2 * sm_count()));
     part_.alloc(P_);
+    csum_.alloc(1);
     grid_.alloc(G_);
     X_.alloc(GH_);
     H_.alloc(GH_);
@@ -227,9 +238,15 @@ class UwUImpl final : public Potential {
     // zeros everywhere, then the active modes.
     if (g) FB_CUDA(cudaMemsetAsync(H_.p, 0, H_.bytes(), s));
     const int mgrid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n_active_, kThreads), 4 * sm_count())));
+    const int exact = (g != nullptr && grad_mode_ == 1) ? 1 : 0;
+    if (exact) FB_CUDA(cudaMemsetAsync(csum_.p, 0, sizeof(double), s));
     uwu_modes_kernel<T><<<mgrid, kThreads, 0, s>>>(n_active_, hidx_.p, coef_.p, X_.p, H_.p, part_.p, P_, e,
-                                                   g != nullptr);
+                                                   g != nullptr, exact, csum_.p);
     FB_LAUNCH_CHECK();
+    if (exact) {
+      uwu_offset_kernel<T><<<1, 1, 0, s>>>(H_.p, csum_.p);
+      FB_LAUNCH_CHECK();
+    }
     timer_mark("modes", s);
     if (!g) return;
     FB_CUFFT(cufftSetStream(c2r_, s));
@@ -252,7 +269,7 @@ class UwUImpl final : public Potential {
   int64_t n_active_ = 0;
   DevBuf<int64_t> hidx_;
   DevBuf<UwuCoef> coef_;
-  DevBuf<double> part_;
+  DevBuf<double> part_, csum_;
   DevBuf<T> grid_;
   DevBuf<cplx_t<T>> X_, H_;
   cufftHandle r2c_ = 0, c2r_ = 0;

@@ -99,12 +99,20 @@ class BasePotential:
         check(lib.fresco_potential_energy(self._h, dptr(xa), xa.size, C.byref(e)))
         return e.value
 
-    def get_energy_gradient(self, x):
+    def get_energy_gradient(self, x, out=None):
+        """(energy, gradient).  ``out``: optional C-contiguous float64 array that receives the
+        gradient (e.g. page-locked memory for faster transfers); it is also returned."""
         if _is_torch_cuda(x):
-            e, g = self.energy_gradient_device(x)
+            e, g = self.energy_gradient_device(x, grad=out)
             return float(e.item()), g
         xa = _f64(x)
-        grad = np.empty_like(xa)
+        if out is None:
+            grad = np.empty_like(xa)
+        else:
+            grad = out
+            if (not isinstance(grad, np.ndarray) or grad.dtype != np.float64 or grad.size != xa.size
+                    or not grad.flags["C_CONTIGUOUS"]):
+                raise ValueError("out must be a C-contiguous float64 array of the coordinates' size")
         e = C.c_double(0.0)
         check(lib.fresco_potential_energy_gradient(self._h, dptr(xa), xa.size, dptr(grad), C.byref(e)))
         return e.value, grad
@@ -137,6 +145,16 @@ class BasePotential:
         check(lib.fresco_potential_energy_gradient_device(self._h, x.data_ptr(), x.numel(), grad.data_ptr(),
                                                           out.data_ptr(), int(accumulate), s))
         return out, grad
+
+    def set_gradient_mode(self, mode):
+        """'reference' (default): the reference's own gradient formula; 'exact': the derivative of the
+        energy with respect to the input coordinates (used by fresco_b200.autograd)."""
+        m = {"reference": 0, "exact": 1}.get(str(mode).lower(), mode)
+        check(lib.fresco_potential_set_gradient_mode(self._h, int(m)))
+        self._grad_mode = int(m)
+
+    def gradient_mode(self) -> str:
+        return "exact" if getattr(self, "_grad_mode", 0) == 1 else "reference"
 
     def status(self, stream=None) -> int:
         st = C.c_int(0)

@@ -118,6 +118,15 @@ int fresco_potential_energy_gradient_device(fresco_potential p, const double* d_
  * are ignored at source/fresco/nuwu.hpp:191-192, 256-258). */
 int fresco_potential_status(fresco_potential p, void* stream, int* status);
 
+/* Gradient convention of the handle: 0 (default) returns the reference's own
+ * gradient formula (drop-in parity); 1 returns the exact derivative of the
+ * energy with respect to the input coordinates, as automatic differentiation
+ * needs.  No reference counterpart: the reference only has convention 0
+ * (NUwU/NUwNU differentiate the 2 pi-scaled coordinate, nuwu.hpp:219; UwNU
+ * divides by 2 pi, uwnu.hpp:352; NUwNU omits conj(c_j), nuwnu.hpp:269; UwU
+ * halves the rho term and drops d(1/R), uwu.hpp:178). */
+int fresco_potential_set_gradient_mode(fresco_potential p, int mode);
+
 /* Per-stage device timing of the next evaluations (CUDA events). */
 int fresco_potential_set_timing(fresco_potential p, int enabled);
 /* Copies up to max_stages (name, total ms, count) triples; names are

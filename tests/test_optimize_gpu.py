@@ -60,7 +60,8 @@ def test_lbfgs_run_stop_and_reset():
     from fresco_b200 import NUwU
     from fresco_b200.optimize import LBFGS_CPP
 
-    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(200, 5, 3, ndim=2, seed=9)
+    # L = 1 (continuous map; see test_lbfgs_config1_converges_below_1e12)
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(200, 5, 3, ndim=2, seed=9, L=np.ones(2))
     pot = NUwU(radii, 5, Sk, V, L, eps=1e-13)
     opt = LBFGS_CPP(x, pot, tol=1e-4, M=8, nsteps=500)
     res = opt.run()
