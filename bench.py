@@ -128,6 +128,26 @@ def algorithmic_bytes(geom_nf, n_active, N, s_r, s_c, s_w, d=2, d_f=2):
     return b_points + b_grid + b_modes, per_kernel
 
 
+def reduce_max(value, device):
+    """Max of a per-rank scalar over all ranks (the job time is the slowest rank's)."""
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    try:
+        import torch.distributed as dist
+
+        if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    except ImportError:
+        pass
+    return float(t.item())
+
+
+def job_value(world_size, steps, job_ms):
+    """Whole-job throughput: every rank's steps over the slowest rank's time."""
+    return world_size * steps / (job_ms / 1000.0)
+
+
 def run_ours(args):
     import torch
 
@@ -195,12 +215,9 @@ def run_ours(args):
     g32 = g.clone()
 
     # slowest rank decides the job time
-    tt = torch.tensor([t32_ms], dtype=torch.float64, device=dev)
-    if ws > 1:
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-    t_job_ms = float(tt.item())
+    t_job_ms = reduce_max(t32_ms, dev)
     ms_per_step = t_job_ms / args.steps
-    value = ws * args.steps / (t_job_ms / 1000.0)
+    value = job_value(ws, args.steps, t_job_ms)
 
     # FP64 form (same eps) and the FP64 reference gradient (eps = 1e-12)
     pot64 = NUwU(radii, K_MODES, Sk, V, L, eps=EPS, precision="fp64")
@@ -228,10 +245,7 @@ def run_ours(args):
     for _ in range(ne2e):
         eh, gh = pot32.get_energy_gradient(x_host, out=g_host)
     e2e_s = (time.perf_counter() - t0) / ne2e
-    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if ws > 1:
-        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = ws / float(e2e_t.item())
+    e2e_value = ws / reduce_max(e2e_s, dev)
 
     # roofline: per-stage device times from CUDA events on the launch stream
     b_eval, per_kernel = algorithmic_bytes(nf, n_active, N_POINTS, 4, 8, 8)
