@@ -218,6 +218,17 @@ int fresco_potential_energy_gradient_device(fresco_potential p, const double* d_
   });
 }
 
+int fresco_nuwnu_energy_gradient_noalloc(const double* d_x, int64_t n_points, int ndim, const double* d_weights,
+                                         const double* d_kpts, const double* d_sk, const double* d_v, int64_t n_k,
+                                         const double* L, int gradient_mode, double* d_grad, double* d_energy,
+                                         int accumulate, void* stream) {
+  return guarded([&] {
+    fb::nuwnu_energy_gradient_noalloc(d_x, n_points, ndim, d_weights, d_kpts, d_sk, d_v, n_k, L, gradient_mode,
+                                      d_grad, d_energy, accumulate != 0, static_cast<cudaStream_t>(stream));
+    return FRESCO_OK;
+  });
+}
+
 int fresco_potential_status(fresco_potential p, void* stream, int* status) {
   return guarded([&] {
     if (!p || !status) throw fb::InvalidArgument("null argument");

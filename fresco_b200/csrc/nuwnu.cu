@@ -17,6 +17,7 @@
 // staged in shared memory.  The `precision` argument is accepted; the
 // arithmetic is FP64 either way.
 #include <cmath>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -260,6 +261,111 @@ class NUwNUImpl final : public Potential {
 };
 
 }  // namespace
+
+// ---- allocation-free form --------------------------------------------------
+//
+// fresco_nuwnu_energy_gradient_noalloc evaluates the same loss and gradient as
+// a NUwNU handle without any device allocation: no handle is created, the
+// caller's device arrays are read directly, and the per-k-point sums (rho and
+// the loss factor) plus the status word live in the file-scope array below.
+// The array is part of the library's device image, so every GPU that loads
+// the library holds its 128 KiB until the process exits.  All calls share it:
+// two calls whose work overlaps on the GPU (different streams, or different
+// host threads on one device) race on it and both results are undefined.
+constexpr int64_t kNoAllocMaxK = 4096;
+static __device__ __align__(256) double2 g_nuwnu_noalloc_scratch[2 * kNoAllocMaxK + 1];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double2* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  The first call
+// on a device looks it up (cudaGetSymbolAddress, which may load the library's
+// device code onto that device); later calls reuse the cached address.
+double2* noalloc_scratch_on_current_device() {
+  int dev = -1;
+  FB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    throw std::runtime_error("device index " + std::to_string(dev) + " is beyond the " +
+                             std::to_string(kNoAllocMaxDevices) + " devices the allocation-free entry point supports");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr = nullptr;
+    const cudaError_t rc = cudaGetSymbolAddress(&ptr, g_nuwnu_noalloc_scratch);
+    if (rc != cudaSuccess || !ptr)
+      throw std::runtime_error(std::string("cudaGetSymbolAddress of the NUwNU scratch array failed: ") +
+                               cudaGetErrorString(rc));
+    g_noalloc_ptr[dev] = static_cast<double2*>(ptr);
+  }
+  return g_noalloc_ptr[dev];
+}
+
+template <int D>
+void noalloc_launch(const double* x, int64_t N, const double* c, const double* s, const double* sk, const double* v,
+                    int64_t M, const double* L, int mode, double* g, double* e, bool acc, double2* scratch,
+                    cudaStream_t st) {
+  double2* rho = scratch;
+  double2* factor = scratch + kNoAllocMaxK;
+  int* status = reinterpret_cast<int*>(scratch + 2 * kNoAllocMaxK);
+  // the array keeps the previous call's sums and status: clear what must start at zero
+  FB_CUDA(cudaMemsetAsync(status, 0, 2 * sizeof(int), st));
+  if (!acc) FB_CUDA(cudaMemsetAsync(e, 0, sizeof(double), st));
+  if (M == 0 || N == 0) {
+    if (g && !acc) FB_CUDA(cudaMemsetAsync(g, 0, sizeof(double) * N * D, st));
+    return;
+  }
+  FB_CUDA(cudaMemsetAsync(rho, 0, sizeof(double2) * M, st));
+  const double L0 = L[0], L1 = D > 1 ? L[1] : 1.0, L2 = D > 2 ? L[2] : 1.0;
+  const int pblocks = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(N, kThreads), 2 * int64_t(sm_count()))));
+  dim3 fg(pblocks, unsigned(ceil_div(M, kFreqChunk)));
+  nuwnu_forward_kernel<D><<<fg, kThreads, 0, st>>>(x, N, s, M, c, 1.0, L0, L1, L2, rho, status);
+  FB_LAUNCH_CHECK();
+  const int mg = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(M, kThreads), int64_t(sm_count()) * 4)));
+  nuwnu_loss_kernel<<<mg, kThreads, 0, st>>>(rho, M, 1.0 / double(N), sk, v, e, factor, status);
+  FB_LAUNCH_CHECK();
+  if (!g) return;
+  const int ag = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(N, kThreads), int64_t(sm_count()) * 8)));
+  nuwnu_adjoint_kernel<D><<<ag, kThreads, 0, st>>>(x, N, s, M, factor, L0, L1, L2, g, acc ? 1 : 0, status, c, 1.0,
+                                                   mode == 1 ? 1 : 0);
+  FB_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+int64_t nuwnu_noalloc_max_kpoints() { return kNoAllocMaxK; }
+
+void nuwnu_energy_gradient_noalloc(const double* d_x, int64_t n_points, int ndim, const double* d_weights,
+                                   const double* d_kpts, const double* d_sk, const double* d_v, int64_t n_k,
+                                   const double* L, int gradient_mode, double* d_grad, double* d_energy,
+                                   bool accumulate, cudaStream_t stream) {
+  if (ndim < 1 || ndim > 3) throw InvalidArgument("Invalid dimension: " + std::to_string(ndim));
+  if (n_points < 0 || n_k < 0) throw InvalidArgument("negative size");
+  if (n_k > kNoAllocMaxK)
+    throw InvalidArgument("n_k = " + std::to_string(n_k) + " exceeds the allocation-free NUwNU maximum of " +
+                          std::to_string(kNoAllocMaxK) + " k-points; use a NUwNU handle for more");
+  if (gradient_mode != 0 && gradient_mode != 1) throw InvalidArgument("gradient mode must be 0 or 1");
+  if (!L) throw InvalidArgument("null box lengths");
+  if (!d_energy) throw InvalidArgument("null energy pointer");
+  if (n_points > 0 && !d_x) throw InvalidArgument("null coordinate array");
+  if (n_k > 0 && (!d_kpts || !d_sk || !d_v)) throw InvalidArgument("null k-point, Sk or V array");
+  double2* scratch = noalloc_scratch_on_current_device();
+  switch (ndim) {
+    case 1:
+      noalloc_launch<1>(d_x, n_points, d_weights, d_kpts, d_sk, d_v, n_k, L, gradient_mode, d_grad, d_energy,
+                        accumulate, scratch, stream);
+      break;
+    case 2:
+      noalloc_launch<2>(d_x, n_points, d_weights, d_kpts, d_sk, d_v, n_k, L, gradient_mode, d_grad, d_energy,
+                        accumulate, scratch, stream);
+      break;
+    default:
+      noalloc_launch<3>(d_x, n_points, d_weights, d_kpts, d_sk, d_v, n_k, L, gradient_mode, d_grad, d_energy,
+                        accumulate, scratch, stream);
+      break;
+  }
+}
 
 PotentialPtr make_nuwnu(const std::vector<double>& radii, const std::vector<double>& kpts,
                         const std::vector<double>& sk, const std::vector<double>& v, const std::vector<double>& L,

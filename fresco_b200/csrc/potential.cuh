@@ -99,6 +99,14 @@ PotentialPtr make_uwnu(const std::vector<int>& grid, const std::vector<double>& 
 PotentialPtr make_nuwnu(const std::vector<double>& radii, const std::vector<double>& kpts,
                         const std::vector<double>& sk, const std::vector<double>& v, const std::vector<double>& L,
                         double eps, int precision);
+// NUwNU loss and gradient from caller-owned device arrays with no device
+// allocation; the per-k-point sums use a fixed static device array, so n_k is
+// limited to nuwnu_noalloc_max_kpoints().
+int64_t nuwnu_noalloc_max_kpoints();
+void nuwnu_energy_gradient_noalloc(const double* d_x, int64_t n_points, int ndim, const double* d_weights,
+                                   const double* d_kpts, const double* d_sk, const double* d_v, int64_t n_k,
+                                   const double* L, int gradient_mode, double* d_grad, double* d_energy,
+                                   bool accumulate, cudaStream_t stream);
 PotentialPtr make_inversepower(double a, double eps, const std::vector<double>& radii,
                                const std::vector<double>& boxv, bool periodic, bool use_cell_lists,
                                double ncellx_scale);

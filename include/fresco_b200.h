@@ -113,6 +113,40 @@ int fresco_potential_energy_device(fresco_potential p, const double* d_x, int64_
 int fresco_potential_energy_gradient_device(fresco_potential p, const double* d_x, int64_t n, double* d_grad,
                                             double* d_energy, int accumulate, void* stream);
 
+/* Allocation-free NUwNU loss and gradient.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory at the point where they need
+ * the loss: a host that hands the whole GPU to its own memory pool (so that
+ * cudaMalloc would fail), or a time-stepping loop that must not call cudaFree
+ * because it waits for all work on the device.  Every other entry point
+ * allocates when its handle is created; this one takes no handle.  It
+ * computes exactly what a NUwNU handle computes (fresco_nuwnu_create, then
+ * fresco_potential_energy_gradient_device), reading only the caller's arrays:
+ *   d_x        n_points*ndim coordinates (device),
+ *   d_weights  n_points per-point weights c_j as the reference derives them
+ *              from the radii ((pi r^2)^ndim in 2D, (4/3 pi r^3)^ndim in 3D,
+ *              then scaled to sum to n_points; nuwnu.hpp:81-105), or NULL for
+ *              equal radii (c_j = 1),
+ *   d_kpts     n_k*ndim k-points, d_sk and d_v n_k values each (device),
+ *   L          ndim box lengths (HOST array),
+ *   d_grad     n_points*ndim gradient out (device; NULL: energy only),
+ *   d_energy   one double out (device).
+ * gradient_mode is 0 (reference convention) or 1 (exact derivative), as in
+ * fresco_potential_set_gradient_mode; accumulate != 0 adds into the outputs.
+ * The per-k-point sums live in a static device array of 128 KiB that the
+ * library holds on every GPU it is loaded on until the process exits, so
+ * n_k may not exceed 4096 (FRESCO_ERR_INVALID beyond that).  All calls share
+ * that array: calls whose work overlaps on the GPU (two streams, or two host
+ * threads on one device) race and give undefined results.  The first call on
+ * a device looks up the array's device address (and may load the library's
+ * device code there); make that first call before any stream capture begins.
+ * Works on the current device and enqueues on `stream` without waiting.  A
+ * non-finite coordinate makes the energy and the gradient NaN. */
+int fresco_nuwnu_energy_gradient_noalloc(const double* d_x, int64_t n_points, int ndim, const double* d_weights,
+                                         const double* d_kpts, const double* d_sk, const double* d_v, int64_t n_k,
+                                         const double* L, int gradient_mode, double* d_grad, double* d_energy,
+                                         int accumulate, void* stream);
+
 /* Sticky status bits raised since the last call (1: non-finite input).
  * Synchronises `stream`.  No reference counterpart (FINUFFT's return codes
  * are ignored at source/fresco/nuwu.hpp:191-192, 256-258). */
