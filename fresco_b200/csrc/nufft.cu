@@ -61,16 +61,15 @@ void alloc_sort(SortBufs& sb, int64_t N, const Geom& g) {
   const int sms = sm_count();
   sb.NB = int(std::max<int64_t>(1, std::min<int64_t>(2 * sms, ceil_div(std::max<int64_t>(N, 1), 1024))));
   sb.chunk = ceil_div(std::max<int64_t>(N, 1), sb.NB);
-  const int64_t nh = nb * sb.NB + 1;
-  sb.hist.alloc(nh);
-  sb.offs.alloc(nh);
-  sb.scan_tmp.alloc(scan_tmp_size(nh));
+  sb.bin_total.alloc(nb);
+  FB_CUDA(cudaMemset(sb.bin_total.p, 0, sizeof(int) * nb));
+  sb.blk_off.alloc(nb * sb.NB);
+  sb.bin_start.alloc(nb + 1);
   sb.max_sub = nb + ceil_div(std::max<int64_t>(N, 1), kMaxSub);
   sb.sub_bin.alloc(sb.max_sub);
   sb.sub_start.alloc(sb.max_sub);
   sb.sub_count.alloc(sb.max_sub);
   sb.num_sub.alloc(1);
-  sb.rank.alloc(std::max<int64_t>(N, 1));
 }
 
 }  // namespace fb

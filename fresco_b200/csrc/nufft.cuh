@@ -73,11 +73,10 @@ inline size_t rec_bytes(int D, bool f32) {
 struct SortBufs {
   int NB = 1;            // sort blocks (each owns a contiguous chunk of points)
   int64_t chunk = 1;     // points per sort block
-  DevBuf<int> hist;      // nbins * NB + 1 counts, bin-major; scanned in place into offsets
-  DevBuf<int> offs;      // exclusive scan of hist
-  DevBuf<int> scan_tmp;
+  DevBuf<int> bin_total; // nbins point counts; zero between sorts (the plan pass clears it)
+  DevBuf<int> blk_off;   // NB * nbins: each block's offset inside each bin (block-major)
+  DevBuf<int> bin_start; // nbins + 1: first record of each bin
   DevBuf<int> sub_bin, sub_start, sub_count, num_sub;
-  DevBuf<uint32_t> rank;
   int64_t max_sub = 0;
 };
 

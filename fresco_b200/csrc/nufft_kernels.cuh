@@ -30,25 +30,28 @@ __device__ __forceinline__ int wrap_index(int x, int n) {
 // stay in bounds).
 __device__ __forceinline__ bool map_coord(const double* __restrict__ pts, int64_t j, const MapParams& mp, int nf, int a,
                                           int& c, double& f) {
+  // Every operation is an explicitly rounded intrinsic: the counting and the
+  // scattering pass of the sort evaluate this map separately and must agree
+  // bit for bit, whatever the compiler's contraction choices in each kernel.
   const double p = pts[j * mp.stride + a];
   const double L = mp.L[a];
   double x;
   if (mp.kind == 0) {
     // same operation order as source/fresco/nuwu.hpp:219
-    x = (p - round(p / L)) * 2 * kPi / L;
+    x = __ddiv_rn(__dmul_rn(__dmul_rn(__dsub_rn(p, round(__ddiv_rn(p, L))), 2.0), kPi), L);
   } else {
-    x = p * 2 * kPi / L;  // uwnu.hpp:245
+    x = __ddiv_rn(__dmul_rn(__dmul_rn(p, 2.0), kPi), L);  // uwnu.hpp:245
   }
-  double u = x * (double(nf) / (2.0 * kPi));
+  double u = __dmul_rn(x, double(nf) / (2.0 * kPi));
   if (!isfinite(u)) {
     c = 0;
     f = 0.0;
     return false;
   }
-  u -= double(nf) * floor(u / double(nf));
+  u = __dsub_rn(u, __dmul_rn(double(nf), floor(__ddiv_rn(u, double(nf)))));
   const double fl = floor(u);
   int ci = int(fl);
-  f = u - fl;
+  f = __dsub_rn(u, fl);
   if (ci >= nf) ci -= nf;
   if (ci < 0) ci += nf;
   if (ci < 0 || ci >= nf) {
@@ -68,15 +71,43 @@ __device__ __forceinline__ int point_bin(const double* __restrict__ pts, int64_t
   return c[0] / g.tile[0] + g.nb[0] * (c[1] / g.tile[1] + g.nb[1] * (c[2] / g.tile[2]));
 }
 
-// Pass 1: per-block histogram in shared memory; rank = position among the
-// block's points of the same bin.  hist is bin-major: hist[bin * NB + block].
+// Block-wide exclusive scan of one int per thread (blockDim.x a multiple of
+// 32, at most 1024); returns the prefix and writes the block total.
+__device__ __forceinline__ int block_exclusive_scan(int v, int* total, int* s_warp) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) s_warp[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    int w = lane < nw ? s_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    if (lane < nw) s_warp[lane] = w;  // inclusive warp totals
+  }
+  __syncthreads();
+  const int before = wid > 0 ? s_warp[wid - 1] : 0;
+  *total = s_warp[nw - 1];
+  __syncthreads();
+  return before + inc - v;
+}
+
+// Sort pass 1: block-local histogram of the block's chunk of points in
+// shared memory, then one global atomic per non-empty bin reserves the
+// block's segment inside that bin (blk_off, block-major).
 template <int D>
-__global__ void __launch_bounds__(kSortThreads) local_hist_kernel(const double* __restrict__ pts, int64_t N,
-                                                                  int64_t chunk, MapParams mp, Geom g, int* hist,
-                                                                  uint32_t* rank, int* status) {
+__global__ void __launch_bounds__(kSortThreads) sort_count_kernel(const double* __restrict__ pts, int64_t N,
+                                                                  int64_t chunk, MapParams mp, Geom g, int* bin_total,
+                                                                  int* blk_off, int* status) {
   extern __shared__ int sh_hist[];
   const int nbins = int(g.nbins());
-  const int NB = gridDim.x;
   for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh_hist[i] = 0;
   __syncthreads();
   const int64_t j0 = int64_t(blockIdx.x) * chunk, j1 = min(N, j0 + chunk);
@@ -87,26 +118,81 @@ __global__ void __launch_bounds__(kSortThreads) local_hist_kernel(const double* 
     bool ok;
     const int bin = point_bin<D>(pts, j, mp, g, c, f, ok);
     bad |= !ok;
-    rank[j] = uint32_t(atomicAdd(&sh_hist[bin], 1));
+    atomicAdd(&sh_hist[bin], 1);
   }
   if (bad) raise_status(status, STATUS_NONFINITE_INPUT);
   __syncthreads();
-  for (int i = threadIdx.x; i < nbins; i += blockDim.x) hist[int64_t(i) * NB + blockIdx.x] = sh_hist[i];
+  int* my_off = blk_off + int64_t(blockIdx.x) * nbins;
+  for (int i = threadIdx.x; i < nbins; i += blockDim.x) {
+    const int cnt = sh_hist[i];
+    if (cnt) my_off[i] = atomicAdd(&bin_total[i], cnt);
+  }
 }
 
-// Pass 3: packed records at offs[bin * NB + block] + rank.
+// Sort pass 2 (one block of 1024 threads): bin starts (exclusive scan of the
+// bin totals), the subproblem table (each bin cut into chunks of at most
+// kMaxSub points), and bin_total cleared for the next sort.
+static __global__ void __launch_bounds__(1024) sort_plan_kernel(int nbins, int* bin_total, int* bin_start,
+                                                                int* sub_bin, int* sub_start, int* sub_count,
+                                                                int* num_sub, int max_sub) {
+  __shared__ int s_warp[32];
+  const int per = (nbins + int(blockDim.x) - 1) / int(blockDim.x);
+  const int b0 = min(nbins, int(threadIdx.x) * per), b1 = min(nbins, b0 + per);
+  int npts = 0, nsub = 0;
+  for (int b = b0; b < b1; ++b) {
+    const int c = bin_total[b];
+    npts += c;
+    nsub += (c + kMaxSub - 1) / kMaxSub;
+  }
+  int tot_pts, tot_sub;
+  int start = block_exclusive_scan(npts, &tot_pts, s_warp);
+  int sbase = block_exclusive_scan(nsub, &tot_sub, s_warp);
+  for (int b = b0; b < b1; ++b) {
+    const int c = bin_total[b];
+    bin_start[b] = start;
+    bin_total[b] = 0;
+    for (int q = 0; q * kMaxSub < c; ++q) {
+      if (sbase < max_sub) {
+        sub_bin[sbase] = b;
+        sub_start[sbase] = start + q * kMaxSub;
+        sub_count[sbase] = min(kMaxSub, c - q * kMaxSub);
+      }
+      ++sbase;
+    }
+    start += c;
+  }
+  if (threadIdx.x == 0) {
+    bin_start[nbins] = tot_pts;
+    *num_sub = min(tot_sub, max_sub);
+  }
+}
+
+// Sort pass 3: each block hands out the slots of its segments again with
+// shared-memory cursors (the counts are those of pass 1, so every slot is
+// written exactly once) and stores the packed records.
 template <int D, typename T>
-__global__ void __launch_bounds__(kSortThreads) scatter_kernel(const double* __restrict__ pts, int64_t N, int64_t chunk,
-                                                               MapParams mp, Geom g, const uint32_t* __restrict__ rank,
-                                                               const int* __restrict__ offs, Rec<D, T>* out) {
-  const int NB = gridDim.x;
+__global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(const double* __restrict__ pts, int64_t N,
+                                                                    int64_t chunk, MapParams mp, Geom g,
+                                                                    const int* __restrict__ bin_start,
+                                                                    const int* __restrict__ blk_off, Rec<D, T>* out,
+                                                                    int* status) {
+  extern __shared__ int sh_cur[];
+  const int nbins = int(g.nbins());
+  const int* my_off = blk_off + int64_t(blockIdx.x) * nbins;
+  // bins this block has no points in hold stale offsets that are never used
+  for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh_cur[i] = bin_start[i] + my_off[i];
+  __syncthreads();
   const int64_t j0 = int64_t(blockIdx.x) * chunk, j1 = min(N, j0 + chunk);
   for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
     int c[3] = {0, 0, 0};
     double f[3] = {0, 0, 0};
     bool ok;
     const int bin = point_bin<D>(pts, j, mp, g, c, f, ok);
-    const int64_t dest = int64_t(offs[int64_t(bin) * NB + blockIdx.x]) + rank[j];
+    const int dest = atomicAdd(&sh_cur[bin], 1);
+    if (dest < 0 || int64_t(dest) >= N) {
+      raise_status(status, STATUS_OVERFLOW);
+      continue;
+    }
     Rec<D, T> r;
     r.cell = pack_cell(D, c[0], c[1], c[2]);
 #pragma unroll
@@ -114,45 +200,6 @@ __global__ void __launch_bounds__(kSortThreads) scatter_kernel(const double* __r
     r.idx = uint32_t(j);
     out[dest] = r;
   }
-}
-
-// One block: subproblem table (each bin cut into chunks of at most kMaxSub
-// points) from the scanned per-block offsets (bin b starts at offs[b * NB]).
-static __global__ void __launch_bounds__(1024) build_subproblems_kernel(int nbins, int NB, const int* __restrict__ offs,
-                                                                        int* sub_bin, int* sub_start, int* sub_count,
-                                                                        int* num_sub, int max_sub) {
-  __shared__ int s_sub[1024];
-  const int tid = threadIdx.x;
-  const int per = (nbins + blockDim.x - 1) / blockDim.x;
-  const int b0 = min(nbins, tid * per), b1 = min(nbins, b0 + per);
-  int ns = 0;
-  for (int b = b0; b < b1; ++b) {
-    const int c = offs[int64_t(b + 1) * NB] - offs[int64_t(b) * NB];
-    ns += (c + kMaxSub - 1) / kMaxSub;
-  }
-  s_sub[tid] = ns;
-  __syncthreads();
-  for (int off = 1; off < int(blockDim.x); off <<= 1) {
-    const int b = tid >= off ? s_sub[tid - off] : 0;
-    __syncthreads();
-    s_sub[tid] += b;
-    __syncthreads();
-  }
-  int sbase = s_sub[tid] - ns;
-  for (int b = b0; b < b1; ++b) {
-    const int start = offs[int64_t(b) * NB];
-    const int c = offs[int64_t(b + 1) * NB] - start;
-    const int nsub = (c + kMaxSub - 1) / kMaxSub;
-    for (int s = 0; s < nsub; ++s) {
-      if (sbase < max_sub) {
-        sub_bin[sbase] = b;
-        sub_start[sbase] = start + s * kMaxSub;
-        sub_count[sbase] = min(kMaxSub, c - s * kMaxSub);
-      }
-      ++sbase;
-    }
-  }
-  if (tid == int(blockDim.x) - 1) *num_sub = min(s_sub[tid], max_sub);
 }
 
 template <typename T>
@@ -590,24 +637,23 @@ template <int D, typename T>
 void bin_sort_d(const double* pts, int64_t N, const MapParams& mp, const Geom& g, SortBufs& sb, void* recs, int* status,
                 cudaStream_t s) {
   const int nbins = int(g.nbins());
-  const int64_t nh = int64_t(nbins) * sb.NB;
   const size_t smem = sizeof(int) * size_t(nbins);
-  if (N > 0) {
-    auto k1 = local_hist_kernel<D>;
-    if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    k1<<<sb.NB, kSortThreads, smem, s>>>(pts, N, sb.chunk, mp, g, sb.hist.p, sb.rank.p, status);
-    FB_LAUNCH_CHECK();
-  } else {
-    FB_CUDA(cudaMemsetAsync(sb.hist.p, 0, sizeof(int) * nh, s));
+  auto k1 = sort_count_kernel<D>;
+  auto k3 = sort_scatter_kernel<D, T>;
+  if (smem > 48 * 1024) {
+    FB_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    FB_CUDA(cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   }
-  FB_CUDA(cudaMemsetAsync(sb.hist.p + nh, 0, sizeof(int), s));
-  exclusive_scan(sb.hist.p, sb.offs.p, sb.scan_tmp.p, nh + 1, s);
-  build_subproblems_kernel<<<1, 1024, 0, s>>>(nbins, sb.NB, sb.offs.p, sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p,
-                                              sb.num_sub.p, int(sb.max_sub));
+  if (N > 0) {
+    k1<<<sb.NB, kSortThreads, smem, s>>>(pts, N, sb.chunk, mp, g, sb.bin_total.p, sb.blk_off.p, status);
+    FB_LAUNCH_CHECK();
+  }
+  sort_plan_kernel<<<1, 1024, 0, s>>>(nbins, sb.bin_total.p, sb.bin_start.p, sb.sub_bin.p, sb.sub_start.p,
+                                      sb.sub_count.p, sb.num_sub.p, int(sb.max_sub));
   FB_LAUNCH_CHECK();
   if (N > 0) {
-    scatter_kernel<D, T><<<sb.NB, kSortThreads, 0, s>>>(pts, N, sb.chunk, mp, g, sb.rank.p, sb.offs.p,
-                                                        static_cast<Rec<D, T>*>(recs));
+    k3<<<sb.NB, kSortThreads, smem, s>>>(pts, N, sb.chunk, mp, g, sb.bin_start.p, sb.blk_off.p,
+                                         static_cast<Rec<D, T>*>(recs), status);
     FB_LAUNCH_CHECK();
   }
 }
