@@ -54,6 +54,7 @@ struct MapParams {
   int kind = 0;
   double L[3] = {1, 1, 1};
   int stride = 2;  // doubles between consecutive points (interleaved layout)
+  double scale[3] = {1, 1, 1};  // fine-grid cells per unit length, nf / L (set by the sort)
 };
 
 // Packed sorted-point records (16 or 32 bytes, read with one vector load).
@@ -77,6 +78,7 @@ struct SortBufs {
   DevBuf<int> blk_off;   // NB * nbins: each block's offset inside each bin (block-major)
   DevBuf<int> bin_start; // nbins + 1: first record of each bin
   DevBuf<int> sub_bin, sub_start, sub_count, num_sub;
+  DevBuf<unsigned char> unsorted;  // N records in input order (written by the counting pass)
   int64_t max_sub = 0;
 };
 

@@ -25,50 +25,69 @@ __device__ __forceinline__ int wrap_index(int x, int n) {
   return x;
 }
 
-// Maps coordinate a of point j to (cell, fraction).  Returns false for a
-// non-finite coordinate (then cell = 0, fraction = 0 so all later accesses
-// stay in bounds).
-__device__ __forceinline__ bool map_coord(const double* __restrict__ pts, int64_t j, const MapParams& mp, int nf, int a,
-                                          int& c, double& f) {
-  // Every operation is an explicitly rounded intrinsic: the counting and the
-  // scattering pass of the sort evaluate this map separately and must agree
-  // bit for bit, whatever the compiler's contraction choices in each kernel.
-  const double p = pts[j * mp.stride + a];
-  const double L = mp.L[a];
-  double x;
-  if (mp.kind == 0) {
-    // same operation order as source/fresco/nuwu.hpp:219
-    x = __ddiv_rn(__dmul_rn(__dmul_rn(__dsub_rn(p, round(__ddiv_rn(p, L))), 2.0), kPi), L);
-  } else {
-    x = __ddiv_rn(__dmul_rn(__dmul_rn(p, 2.0), kPi), L);  // uwnu.hpp:245
+// Maps coordinate a of a point to (fine-grid cell, fraction in [0, 1)).
+// Returns false for a non-finite coordinate (then cell = 0, fraction = 0 so
+// all later accesses stay in bounds).
+//
+// NUwU/NUwNU (kind 0) use x = (p - round(p/L)) 2 pi / L (source/fresco/
+// nuwu.hpp:219: the period count is subtracted, not its multiple of L); UwNU
+// k-points (kind 1) use x = p 2 pi / L (uwnu.hpp:245).  The fine-grid
+// coordinate x nf / (2 pi) is formed as t * (nf / L) with t = p - round(p/L)
+// (or p): one multiplication instead of the reference's divide-and-rescale
+// chain, within a few ulp of it.  round(p/L) keeps the exact division, so a
+// coordinate on a half period rounds as in the reference.
+__device__ __forceinline__ bool map_coord(double p, const MapParams& mp, int nf, int a, int& c, double& f) {
+  const double t = mp.kind == 0 ? p - round(p / mp.L[a]) : p;
+  double u = t * mp.scale[a];
+  if (!(fabs(u) < 1.0e9)) {
+    if (!isfinite(u)) {
+      c = 0;
+      f = 0.0;
+      return false;
+    }
+    u -= double(nf) * floor(u / double(nf));  // far outside the box: fold first
   }
-  double u = __dmul_rn(x, double(nf) / (2.0 * kPi));
-  if (!isfinite(u)) {
-    c = 0;
-    f = 0.0;
-    return false;
-  }
-  u = __dsub_rn(u, __dmul_rn(double(nf), floor(__ddiv_rn(u, double(nf)))));
   const double fl = floor(u);
+  f = u - fl;  // exact
   int ci = int(fl);
-  f = __dsub_rn(u, fl);
-  if (ci >= nf) ci -= nf;
   if (ci < 0) ci += nf;
+  else if (ci >= nf) ci -= nf;
   if (ci < 0 || ci >= nf) {
-    ci = 0;
-    f = 0.0;
+    ci %= nf;
+    if (ci < 0) ci += nf;
   }
   c = ci;
   return true;
 }
 
 template <int D>
-__device__ __forceinline__ int point_bin(const double* __restrict__ pts, int64_t j, const MapParams& mp, const Geom& g,
-                                         int (&c)[3], double (&f)[3], bool& ok) {
+__device__ __forceinline__ int bin_of_cell(const int (&c)[3], const Geom& g) {
+  if (D == 2) return (c[0] / kTile2D) + g.nb[0] * (c[1] / kTile2D);
+  return c[0] / g.tile[0] + g.nb[0] * (c[1] / g.tile[1] + g.nb[1] * (c[2] / g.tile[2]));
+}
+
+template <int D>
+__device__ __forceinline__ int point_bin(const double (&p)[D], const MapParams& mp, const Geom& g, int (&c)[3],
+                                         double (&f)[3], bool& ok) {
   ok = true;
 #pragma unroll
-  for (int a = 0; a < D; ++a) ok &= map_coord(pts, j, mp, g.nf[a], a, c[a], f[a]);
-  return c[0] / g.tile[0] + g.nb[0] * (c[1] / g.tile[1] + g.nb[1] * (c[2] / g.tile[2]));
+  for (int a = 0; a < D; ++a) ok &= map_coord(p[a], mp, g.nf[a], a, c[a], f[a]);
+  return bin_of_cell<D>(c, g);
+}
+
+// Points per thread per round in the sort passes: the coordinates of a round
+// are loaded before any of them is used, so their latencies overlap.
+constexpr int kSortBatch = 4;
+
+template <int D>
+__device__ __forceinline__ void load_batch(const double* __restrict__ pts, int64_t jb, int64_t j1, int64_t step,
+                                           int stride, double (&p)[kSortBatch][D]) {
+#pragma unroll
+  for (int u = 0; u < kSortBatch; ++u) {
+    const int64_t j = jb + u * step;
+#pragma unroll
+    for (int a = 0; a < D; ++a) p[u][a] = j < j1 ? pts[j * stride + a] : 0.0;
+  }
 }
 
 // Block-wide exclusive scan of one int per thread (blockDim.x a multiple of
@@ -99,26 +118,40 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total, int* s_wa
   return before + inc - v;
 }
 
-// Sort pass 1: block-local histogram of the block's chunk of points in
-// shared memory, then one global atomic per non-empty bin reserves the
-// block's segment inside that bin (blk_off, block-major).
-template <int D>
+// Sort pass 1: maps every point once (cell, fraction), writes its packed
+// record in input order, and counts the block's points per bin in shared
+// memory; one global atomic per non-empty bin then reserves the block's
+// segment inside that bin (blk_off, block-major).
+template <int D, typename T>
 __global__ void __launch_bounds__(kSortThreads) sort_count_kernel(const double* __restrict__ pts, int64_t N,
                                                                   int64_t chunk, MapParams mp, Geom g, int* bin_total,
-                                                                  int* blk_off, int* status) {
+                                                                  int* blk_off, Rec<D, T>* unsorted, int* status) {
   extern __shared__ int sh_hist[];
   const int nbins = int(g.nbins());
   for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh_hist[i] = 0;
   __syncthreads();
   const int64_t j0 = int64_t(blockIdx.x) * chunk, j1 = min(N, j0 + chunk);
   bool bad = false;
-  for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-    int c[3] = {0, 0, 0};
-    double f[3];
-    bool ok;
-    const int bin = point_bin<D>(pts, j, mp, g, c, f, ok);
-    bad |= !ok;
-    atomicAdd(&sh_hist[bin], 1);
+  for (int64_t jb = j0 + threadIdx.x; jb < j1; jb += kSortBatch * int64_t(blockDim.x)) {
+    double p[kSortBatch][D];
+    load_batch<D>(pts, jb, j1, blockDim.x, mp.stride, p);
+#pragma unroll
+    for (int u = 0; u < kSortBatch; ++u) {
+      const int64_t j = jb + u * int64_t(blockDim.x);
+      if (j >= j1) break;
+      int c[3] = {0, 0, 0};
+      double f[3] = {0, 0, 0};
+      bool ok;
+      const int bin = point_bin<D>(p[u], mp, g, c, f, ok);
+      bad |= !ok;
+      atomicAdd(&sh_hist[bin], 1);
+      Rec<D, T> r;
+      r.cell = pack_cell(D, c[0], c[1], c[2]);
+#pragma unroll
+      for (int a = 0; a < D; ++a) r.f[a] = T(f[a]);
+      r.idx = uint32_t(j);
+      unsorted[j] = r;
+    }
   }
   if (bad) raise_status(status, STATUS_NONFINITE_INPUT);
   __syncthreads();
@@ -169,10 +202,10 @@ static __global__ void __launch_bounds__(1024) sort_plan_kernel(int nbins, int* 
 
 // Sort pass 3: each block hands out the slots of its segments again with
 // shared-memory cursors (the counts are those of pass 1, so every slot is
-// written exactly once) and stores the packed records.
+// written exactly once) and moves its records there.
 template <int D, typename T>
-__global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(const double* __restrict__ pts, int64_t N,
-                                                                    int64_t chunk, MapParams mp, Geom g,
+__global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(const Rec<D, T>* __restrict__ unsorted, int64_t N,
+                                                                    int64_t chunk, Geom g,
                                                                     const int* __restrict__ bin_start,
                                                                     const int* __restrict__ blk_off, Rec<D, T>* out,
                                                                     int* status) {
@@ -183,22 +216,25 @@ __global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(const double
   for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh_cur[i] = bin_start[i] + my_off[i];
   __syncthreads();
   const int64_t j0 = int64_t(blockIdx.x) * chunk, j1 = min(N, j0 + chunk);
-  for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-    int c[3] = {0, 0, 0};
-    double f[3] = {0, 0, 0};
-    bool ok;
-    const int bin = point_bin<D>(pts, j, mp, g, c, f, ok);
-    const int dest = atomicAdd(&sh_cur[bin], 1);
-    if (dest < 0 || int64_t(dest) >= N) {
-      raise_status(status, STATUS_OVERFLOW);
-      continue;
-    }
-    Rec<D, T> r;
-    r.cell = pack_cell(D, c[0], c[1], c[2]);
+  for (int64_t jb = j0 + threadIdx.x; jb < j1; jb += kSortBatch * int64_t(blockDim.x)) {
+    Rec<D, T> r[kSortBatch];
 #pragma unroll
-    for (int a = 0; a < D; ++a) r.f[a] = T(f[a]);
-    r.idx = uint32_t(j);
-    out[dest] = r;
+    for (int u = 0; u < kSortBatch; ++u) {
+      const int64_t j = jb + u * int64_t(blockDim.x);
+      if (j < j1) r[u] = unsorted[j];
+    }
+#pragma unroll
+    for (int u = 0; u < kSortBatch; ++u) {
+      if (jb + u * int64_t(blockDim.x) >= j1) break;
+      int c[3];
+      unpack_cell(D, r[u].cell, c[0], c[1], c[2]);
+      const int dest = atomicAdd(&sh_cur[bin_of_cell<D>(c, g)], 1);
+      if (dest < 0 || int64_t(dest) >= N) {
+        raise_status(status, STATUS_OVERFLOW);
+        continue;
+      }
+      out[dest] = r[u];
+    }
   }
 }
 
@@ -247,167 +283,263 @@ __device__ __forceinline__ void flush_tile(const T* tile, const Geom& g, int org
 // ---------------------------------------------------------------------------
 // 2D spreading without shared-memory atomics.
 //
-// The 64 x 64-cell tile is cut into sub-blocks of SB x SB cells (SB = 8 for
-// w <= 8, 16 for w <= 16).  A point's w x w footprint only reaches the
-// neighbouring sub-blocks, so sub-blocks whose (a, b) indices have the same
-// parities never touch the same cell: the tile is spread in four phases, one
-// per parity class.  Within a phase a warp handles GPW sub-blocks at once,
-// one point from each, with one lane per footprint row; a lane adds its row
-// with plain shared-memory read-modify-writes.  Points of one sub-block are
-// taken one after another by the same lane group (__syncwarp between them),
-// so no two lanes ever update the same cell concurrently.
+// One block per subproblem (the points of one 64 x 64-cell tile).  The tile
+// is cut into sub-blocks of SB x SB cells (SB = 8 for w <= 8, 16 for
+// w <= 16).  A point's w x w footprint only reaches the neighbouring
+// sub-blocks, so sub-blocks whose (a, b) indices have the same parities never
+// touch the same cell: the tile is spread in four phases, one per parity
+// class, and within a phase every warp owns whole sub-blocks, whose points
+// it adds one after another (program order within the warp, __syncwarp
+// between points).  So no two threads ever update one cell concurrently and
+// plain shared-memory read-modify-writes suffice.
+//
+// Per point, the whole warp works on its footprint: lanes hold the x and y
+// tap values (one polynomial each, coefficients in registers), the products
+// are formed after two shuffles, and the w x w cells are covered in passes
+// of R = 32 / w rows.  The tile pitch P = 64 + w is congruent to w modulo
+// 32, so the R * w cells of one pass fall in R * w distinct banks: every
+// access is conflict-free.  With w <= 8 two points share one round of tap
+// evaluation (lanes 0-15 and 16-31).
+//
+// Before the phases, the block stages its points in shared memory grouped by
+// sub-block, already converted to (tile offset, polynomial variables,
+// weight).  At the end the tile is added to the fine grid with vector
+// atomics (float4: four real or two complex cells); cells that no
+// neighbouring tile can reach are stored plainly when the subproblem is its
+// tile's only one.
 // ---------------------------------------------------------------------------
 
 template <int W>
-struct Phased2D {
+struct Tile2D {
   static constexpr int SB = W <= 8 ? 8 : 16;
-  static constexpr int NSB = kTile2D / SB;       // sub-blocks per tile edge
-  static constexpr int GROUP = W <= 8 ? 8 : 16;  // lanes per point (one per footprint row)
-  static constexpr int GPW = 32 / GROUP;         // points per warp step
+  static constexpr int NSB = kTile2D / SB;  // sub-blocks per tile edge
   static constexpr int PER_PHASE = (NSB / 2) * (NSB / 2);
-  static constexpr int NWARP = PER_PHASE / GPW;
+  static constexpr int NWARP = 8;
   static constexpr int THREADS = 32 * NWARP;
+  static constexpr int PAD = W / 2;
+  static constexpr int EDGE = kTile2D + W;  // tile rows and pitch (cells), origin org - PAD
+  static constexpr int PPW = W <= 8 ? 2 : 1;  // points per tap round
+  static constexpr int HL = 32 / PPW;         // lanes per point in a tap round
+  static constexpr int R = 32 / W;            // footprint rows per pass
+  static constexpr int NPASS = (W + R - 1) / R;
+};
+
+template <typename T, bool CPLX>
+struct alignas(16) Staged2D {
+  int base;  // tile offset (cells) of the footprint's first cell
+  T u0, u1;  // polynomial variables along x and y
+  T wr;      // weight (real part)
+};
+template <typename T>
+struct alignas(16) Staged2D<T, true> {
+  int base;
+  T u0, u1;
+  T wr, wi;
 };
 
 template <int W, typename T, bool CPLX>
-__global__ void __launch_bounds__(Phased2D<W>::THREADS) spread2d_phased_kernel(
+__host__ __device__ constexpr size_t spread2d_smem_bytes() {
+  using P = Tile2D<W>;
+  return sizeof(Staged2D<T, CPLX>) * kMaxSub + sizeof(T) * (CPLX ? 2 : 1) * P::EDGE * P::EDGE +
+         sizeof(uint16_t) * kMaxSub + sizeof(int) * 2 * P::NSB * P::NSB;
+}
+
+// Adds VW consecutive cells (VW = 4 real or 2 complex: one float4) of the
+// shared tile row to the fine grid; the group's first global column gc is a
+// multiple of VW.
+template <typename T, bool CPLX>
+__device__ __forceinline__ void flush_group_f32(const T* trow, int tc0, int edge, float* gdst, bool plain) {
+  constexpr int NC = CPLX ? 2 : 1;
+  constexpr int VW = 4 / NC;
+  float v[4];
+#pragma unroll
+  for (int e = 0; e < VW; ++e) {
+    const int tc = tc0 + e;
+    const bool in = tc >= 0 && tc < edge;
+#pragma unroll
+    for (int q = 0; q < NC; ++q) v[e * NC + q] = in ? float(trow[tc * NC + q]) : 0.f;
+  }
+  if (v[0] == 0.f && v[1] == 0.f && v[2] == 0.f && v[3] == 0.f) return;
+  const float4 val = make_float4(v[0], v[1], v[2], v[3]);
+  if (plain) {
+    *reinterpret_cast<float4*>(gdst) = val;
+  } else {
+    atomicAdd(reinterpret_cast<float4*>(gdst), val);
+  }
+}
+
+template <int W, typename T, bool CPLX>
+__global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
     const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, T uniform,
     const cplx_t<T>* __restrict__ strengths, const int* __restrict__ sub_bin, const int* __restrict__ sub_start,
-    const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g, const EsPoly<W, T> poly, T* grid_real,
-    cplx_t<T>* grid_cplx) {
-  using P = Phased2D<W>;
+    const int* __restrict__ sub_count, const int* __restrict__ num_sub, const int* __restrict__ bin_start, Geom g,
+    const EsPoly<W, T> poly, T* grid_real, cplx_t<T>* grid_cplx) {
+  using P = Tile2D<W>;
+  using S = Staged2D<T, CPLX>;
   constexpr int NC = CPLX ? 2 : 1;
-  constexpr int PAD = W / 2;
-  constexpr int TW = kTile2D + W;
+  constexpr int E = P::EDGE;
+  constexpr int NSB2 = P::NSB * P::NSB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Rec<2, T>* srec = reinterpret_cast<Rec<2, T>*>(smem_raw);  // subproblem's records, grouped by sub-block
+  S* srec = reinterpret_cast<S*>(smem_raw);
   T* tile = reinterpret_cast<T*>(srec + kMaxSub);
-  int* code = reinterpret_cast<int*>(tile + TW * TW * NC);
-  int* sb_count = code + kMaxSub;
-  int* sb_start = sb_count + P::NSB * P::NSB;
+  uint16_t* rank = reinterpret_cast<uint16_t*>(tile + E * E * NC);
+  int* sb_count = reinterpret_cast<int*>(rank + kMaxSub);
+  int* sb_start = sb_count + NSB2;
 
   const int sub = blockIdx.x;
   if (sub >= *num_sub) return;
   const int bin = sub_bin[sub];
   const int start = sub_start[sub], cnt = sub_count[sub];
   const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
+  const int tid = threadIdx.x;
 
-  for (int i = threadIdx.x; i < TW * TW * NC; i += blockDim.x) tile[i] = T(0);
-  for (int i = threadIdx.x; i < P::NSB * P::NSB; i += blockDim.x) sb_count[i] = 0;
+  for (int i = tid; i < E * E * NC; i += P::THREADS) tile[i] = T(0);
+  for (int i = tid; i < NSB2; i += P::THREADS) sb_count[i] = 0;
   __syncthreads();
-  // group the subproblem's points by sub-block (integer shared atomics)
-  for (int p = threadIdx.x; p < cnt; p += blockDim.x) {
+  // rank of each point inside its sub-block
+  for (int p = tid; p < cnt; p += P::THREADS) {
     int c0, c1, c2;
     unpack_cell(2, recs[start + p].cell, c0, c1, c2);
     const int sbi = ((c0 - org0) / P::SB) + P::NSB * ((c1 - org1) / P::SB);
-    code[p] = (sbi << 16) | atomicAdd(&sb_count[sbi], 1);
+    rank[p] = uint16_t(atomicAdd(&sb_count[sbi], 1));
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int acc = 0;
-    for (int i = 0; i < P::NSB * P::NSB; ++i) {
-      sb_start[i] = acc;
-      acc += sb_count[i];
+  if (tid < 32) {  // exclusive scan of the sub-block counts (one warp)
+    constexpr int PER = (NSB2 + 31) / 32;
+    int v[PER], tot = 0;
+#pragma unroll
+    for (int e = 0; e < PER; ++e) {
+      const int i = tid * PER + e;
+      v[e] = i < NSB2 ? sb_count[i] : 0;
+      tot += v[e];
+    }
+    int inc = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (tid >= o) inc += t;
+    }
+    int run = inc - tot;
+#pragma unroll
+    for (int e = 0; e < PER; ++e) {
+      const int i = tid * PER + e;
+      if (i < NSB2) sb_start[i] = run;
+      run += v[e];
     }
   }
   __syncthreads();
-  for (int p = threadIdx.x; p < cnt; p += blockDim.x) srec[sb_start[code[p] >> 16] + (code[p] & 0xffff)] = recs[start + p];
+  // stage: grouped by sub-block, converted to (tile offset, u0, u1, weight)
+  for (int p = tid; p < cnt; p += P::THREADS) {
+    const Rec<2, T> r = recs[start + p];
+    int c0, c1, c2;
+    unpack_cell(2, r.cell, c0, c1, c2);
+    const int sbi = ((c0 - org0) / P::SB) + P::NSB * ((c1 - org1) / P::SB);
+    S st;
+    const int s0 = es_start<W, T>(r.f[0], st.u0);
+    const int s1 = es_start<W, T>(r.f[1], st.u1);
+    st.base = (c1 - org1 + s1 + P::PAD) * E + (c0 - org0 + s0 + P::PAD);
+    if constexpr (CPLX) {
+      const cplx_t<T> v = strengths[r.idx];
+      st.wr = v.x;
+      st.wi = v.y;
+    } else {
+      st.wr = weights ? weights[r.idx] : uniform;
+    }
+    srec[sb_start[sbi] + rank[p]] = st;
+  }
   __syncthreads();
 
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int grp = lane / P::GROUP, row = lane % P::GROUP;
-  const int q = warp * P::GPW + grp;  // this lane group's slot within a phase
-  const int qa = q % (P::NSB / 2), qb = q / (P::NSB / 2);
-  // each lane evaluates one tap (its footprint row) for every point: keep that
-  // tap's polynomial in registers (idle lanes take a valid row)
+  const int warp = tid >> 5, lane = tid & 31;
+  // tap roles: lane hl of each half evaluates x tap hl (hl < W) or y tap hl - W
+  const int half = lane / P::HL, hl = lane % P::HL;
+  const bool xl = hl < W;
+  const int m = xl ? hl : (hl < 2 * W ? hl - W : 0);
   constexpr int Q = EsPolyDeg<W>::Q;
   T cr[Q + 1];
-  {
-    const int trow = row < W ? row : W - 1;
 #pragma unroll
-    for (int m = 0; m < W; ++m)
-      if (m == trow) {
+  for (int mm = 0; mm < W; ++mm)
+    if (mm == m) {
 #pragma unroll
-        for (int d = 0; d <= Q; ++d) cr[d] = poly.c[m][d];
-      }
-  }
+      for (int d = 0; d <= Q; ++d) cr[d] = poly.c[mm][d];
+    }
+  // cell roles: lane = rr * W + cc covers row rr (+ k R) and column cc
+  const int rr = lane / W, cc = lane % W;
+  const bool cell_lane = lane < P::R * W;
+  const int lane_off = rr * E + cc;
+
   for (int phase = 0; phase < 4; ++phase) {
-    const int sbi = (2 * qa + (phase & 1)) + P::NSB * (2 * qb + (phase >> 1));
-    const int my_n = sb_count[sbi], my_base = sb_start[sbi];
-    int n_max = my_n;
+    for (int q = warp; q < P::PER_PHASE; q += P::NWARP) {
+      const int qa = q % (P::NSB / 2), qb = q / (P::NSB / 2);
+      const int sbi = (2 * qa + (phase & 1)) + P::NSB * (2 * qb + (phase >> 1));
+      const int n = sb_count[sbi], b0 = sb_start[sbi];
+      for (int it = 0; it < n; it += P::PPW) {
+        const int pi = it + half;
+        const S st = srec[b0 + (pi < n ? pi : 0)];
+        const T u = xl ? st.u0 : st.u1;
+        T tap = cr[Q];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) n_max = max(n_max, __shfl_xor_sync(0xffffffffu, n_max, o));
-    // software pipeline: the taps of point it+1 are formed before point it is added
-    T kx = T(0), wr = T(0), wi = T(0);
-    int base = 0;
-    bool active = false;
-#define FB_PHASED_LOAD(IT, KX, WR, WI, BASE, ACT)                                      \
-  {                                                                                    \
-    ACT = (IT) < my_n;                                                                 \
-    KX = T(0);                                                                         \
-    WR = T(0);                                                                         \
-    WI = T(0);                                                                         \
-    BASE = 0;                                                                          \
-    if (ACT) {                                                                         \
-      const Rec<2, T> r_ = srec[my_base + (IT)];                                       \
-      int c0_, c1_, c2_;                                                               \
-      unpack_cell(2, r_.cell, c0_, c1_, c2_);                                          \
-      T u0_, u1_;                                                                      \
-      const int s0_ = es_start<W, T>(r_.f[0], u0_);                                    \
-      const int s1_ = es_start<W, T>(r_.f[1], u1_);                                    \
-      T a_ = cr[Q], b_ = cr[Q];                                                        \
-      _Pragma("unroll") for (int d_ = Q - 1; d_ >= 0; --d_) {                          \
-        a_ = fma(a_, u0_, cr[d_]);                                                     \
-        b_ = fma(b_, u1_, cr[d_]);                                                     \
-      }                                                                                \
-      KX = a_;                                                                         \
-      T sr_, si_ = T(0);                                                               \
-      if (CPLX) {                                                                      \
-        const cplx_t<T> v_ = strengths[r_.idx];                                        \
-        sr_ = v_.x;                                                                    \
-        si_ = v_.y;                                                                    \
-      } else {                                                                         \
-        sr_ = weights ? weights[r_.idx] : uniform;                                     \
-      }                                                                                \
-      WR = sr_ * b_;                                                                   \
-      WI = si_ * b_;                                                                   \
-      BASE = ((c1_ - org1 + s1_ + PAD + row) * TW + (c0_ - org0 + s0_ + PAD)) * NC;    \
-    }                                                                                  \
-  }
-    FB_PHASED_LOAD(0, kx, wr, wi, base, active)
-    for (int it = 0; it < n_max; ++it) {
-      T nkx, nwr, nwi;
-      int nbase;
-      bool nact;
-      FB_PHASED_LOAD(it + 1, nkx, nwr, nwi, nbase, nact)
-      T* rowp = tile + base;
+        for (int d = Q - 1; d >= 0; --d) tap = fma(tap, u, cr[d]);
+        const T tr = xl ? tap * st.wr : tap;
+        T ti = T(0);
+        if constexpr (CPLX) ti = xl ? tap * st.wi : T(0);
 #pragma unroll
-      for (int m = 0; m < W; ++m) {
-        const T km = __shfl_sync(0xffffffffu, kx, grp * P::GROUP + m);
-        if (active && row < W) {
-          if (CPLX) {
-            rowp[2 * m] += wr * km;
-            rowp[2 * m + 1] += wi * km;
-          } else {
-            rowp[m] += wr * km;
+        for (int h = 0; h < P::PPW; ++h) {
+          if (it + h >= n) break;
+          const int src = h * P::HL;
+          const int base = __shfl_sync(0xffffffffu, st.base, src);
+          const T kxr = __shfl_sync(0xffffffffu, tr, src + cc);
+          T kxi = T(0);
+          if constexpr (CPLX) kxi = __shfl_sync(0xffffffffu, ti, src + cc);
+#pragma unroll
+          for (int k = 0; k < P::NPASS; ++k) {
+            const int row = k * P::R + rr;
+            const T ky = __shfl_sync(0xffffffffu, tr, src + W + (row < W ? row : W - 1));
+            if (cell_lane && row < W) {
+              T* c = tile + (base + lane_off + k * P::R * E) * NC;
+              c[0] += kxr * ky;
+              if constexpr (CPLX) c[1] += kxi * ky;
+            }
           }
+          __syncwarp();
         }
       }
-      __syncwarp();
-      kx = nkx;
-      wr = nwr;
-      wi = nwi;
-      base = nbase;
-      active = nact;
     }
-#undef FB_PHASED_LOAD
     __syncthreads();
   }
-  Geom gt = g;
-  gt.tw[0] = TW;
-  gt.tw[1] = TW;
-  gt.tw[2] = 1;
-  flush_tile<2, T, CPLX>(tile, gt, org0, org1, 0, PAD, grid_real, grid_cplx);
+
+  // flush
+  const int nf0 = g.nf[0], nf1 = g.nf[1];
+  if (sizeof(T) == 4 && nf0 % (4 / NC) == 0) {
+    constexpr int VW = 4 / NC;                          // cells per float4
+    constexpr int LEFT = (VW - P::PAD % VW) % VW;       // cells left of the tile origin in the first group
+    constexpr int NG = (E + LEFT + VW - 1) / VW;        // groups per tile row
+    // cells [W, 64) of the tile (relative to org - PAD) along both axes are
+    // out of reach of every other tile; with one subproblem in the bin and
+    // whole tiles (nf a multiple of 64) they are written with plain stores
+    const bool sole = cnt == bin_start[bin + 1] - bin_start[bin] && nf0 % kTile2D == 0 && nf1 % kTile2D == 0;
+    for (int i = tid; i < E * NG; i += P::THREADS) {
+      const int ty = i / NG, j = i - ty * NG;
+      const int tc0 = j * VW - LEFT;
+      const int gy = wrap_index(org1 - P::PAD + ty, nf1);
+      const int gx = wrap_index(org0 - P::PAD + tc0, nf0);
+      const bool plain = sole && ty >= W && ty < kTile2D && tc0 >= W && tc0 + VW <= kTile2D;
+      float* dst = CPLX ? reinterpret_cast<float*>(grid_cplx + int64_t(gy) * nf0 + gx)
+                        : reinterpret_cast<float*>(grid_real + int64_t(gy) * nf0 + gx);
+      flush_group_f32<T, CPLX>(tile + ty * E * NC, tc0, E, dst, plain);
+    }
+  } else {
+    for (int i = tid; i < E * E; i += P::THREADS) {
+      const int ty = i / E, tc = i - ty * E;
+      const int64_t gi = int64_t(wrap_index(org1 - P::PAD + ty, nf1)) * nf0 + wrap_index(org0 - P::PAD + tc, nf0);
+      if constexpr (CPLX) {
+        const T re = tile[2 * i], im = tile[2 * i + 1];
+        if (re != T(0) || im != T(0)) atomic_add_cplx<T>(grid_cplx + gi, re, im);
+      } else {
+        const T v = tile[i];
+        if (v != T(0)) atomicAdd(grid_real + gi, v);
+      }
+    }
+  }
 }
 
 // Generic spreading (1D, 3D): one thread per point, shared-memory atomics.
@@ -538,8 +670,12 @@ __global__ void __launch_bounds__(256) interp2d_tile_kernel(
     tile[i] = field[int64_t(a1) * nf0 + a0];
   }
   __syncthreads();
+  // the next record is loaded while the current point is interpolated
+  Rec<2, T> nxt;
+  if (int(threadIdx.x) < cnt) nxt = recs[start + threadIdx.x];
   for (int p = threadIdx.x; p < cnt; p += blockDim.x) {
-    const Rec<2, T> r = recs[start + p];
+    const Rec<2, T> r = nxt;
+    if (p + int(blockDim.x) < cnt) nxt = recs[start + p + blockDim.x];
     int c0, c1, c2;
     unpack_cell(2, r.cell, c0, c1, c2);
     T k0[W], k1[W];
@@ -638,21 +774,24 @@ void bin_sort_d(const double* pts, int64_t N, const MapParams& mp, const Geom& g
                 cudaStream_t s) {
   const int nbins = int(g.nbins());
   const size_t smem = sizeof(int) * size_t(nbins);
-  auto k1 = sort_count_kernel<D>;
+  auto k1 = sort_count_kernel<D, T>;
   auto k3 = sort_scatter_kernel<D, T>;
+  MapParams m2 = mp;
+  for (int a = 0; a < D; ++a) m2.scale[a] = double(g.nf[a]) / mp.L[a];
+  Rec<D, T>* unsorted = reinterpret_cast<Rec<D, T>*>(sb.unsorted.p);
   if (smem > 48 * 1024) {
     FB_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     FB_CUDA(cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   }
   if (N > 0) {
-    k1<<<sb.NB, kSortThreads, smem, s>>>(pts, N, sb.chunk, mp, g, sb.bin_total.p, sb.blk_off.p, status);
+    k1<<<sb.NB, kSortThreads, smem, s>>>(pts, N, sb.chunk, m2, g, sb.bin_total.p, sb.blk_off.p, unsorted, status);
     FB_LAUNCH_CHECK();
   }
   sort_plan_kernel<<<1, 1024, 0, s>>>(nbins, sb.bin_total.p, sb.bin_start.p, sb.sub_bin.p, sb.sub_start.p,
                                       sb.sub_count.p, sb.num_sub.p, int(sb.max_sub));
   FB_LAUNCH_CHECK();
   if (N > 0) {
-    k3<<<sb.NB, kSortThreads, smem, s>>>(pts, N, sb.chunk, mp, g, sb.bin_start.p, sb.blk_off.p,
+    k3<<<sb.NB, kSortThreads, smem, s>>>(unsorted, N, sb.chunk, g, sb.bin_start.p, sb.blk_off.p,
                                          static_cast<Rec<D, T>*>(recs), status);
     FB_LAUNCH_CHECK();
   }
@@ -672,15 +811,12 @@ template <int W, typename T, bool CPLX>
 void launch_spread2d(const void* recs, const T* weights, T uniform, const cplx_t<T>* strengths, const SortBufs& sb,
                      const Geom& g, const std::vector<double>& poly, T* grid_real, cplx_t<T>* grid_cplx,
                      cudaStream_t s) {
-  using P = Phased2D<W>;
-  constexpr int TW = kTile2D + W;
-  const size_t smem = sizeof(Rec<2, T>) * kMaxSub + sizeof(T) * TW * TW * (CPLX ? 2 : 1) +
-                      sizeof(int) * (kMaxSub + 2 * P::NSB * P::NSB);
-  auto kern = spread2d_phased_kernel<W, T, CPLX>;
+  constexpr size_t smem = spread2d_smem_bytes<W, T, CPLX>();
+  auto kern = spread2d_tile_kernel<W, T, CPLX>;
   if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  kern<<<unsigned(sb.max_sub), P::THREADS, smem, s>>>(static_cast<const Rec<2, T>*>(recs), weights, uniform, strengths,
-                                                       sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g,
-                                                       make_es_poly<W, T>(poly), grid_real, grid_cplx);
+  kern<<<unsigned(sb.max_sub), Tile2D<W>::THREADS, smem, s>>>(
+      static_cast<const Rec<2, T>*>(recs), weights, uniform, strengths, sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p,
+      sb.num_sub.p, sb.bin_start.p, g, make_es_poly<W, T>(poly), grid_real, grid_cplx);
   FB_LAUNCH_CHECK();
 }
 

@@ -221,15 +221,35 @@ class NUwUImpl final : public Potential {
     int dims[3];
     for (int a = 0; a < D; ++a) dims[a] = geom_.nf[D - 1 - a];
     const bool f32 = sizeof(T) == 4;
-    FB_CUFFT(cufftPlanMany(&plan_r2c_, D, dims, nullptr, 1, 0, nullptr, 1, 0, f32 ? CUFFT_R2C : CUFFT_D2Z, 1));
-    FB_CUFFT(cufftPlanMany(&plan_c2c_, D, dims, nullptr, 1, int(G), nullptr, 1, int(G),
-                           f32 ? CUFFT_C2C : CUFFT_Z2Z, nfields_));
+    const cufftType r2c = f32 ? CUFFT_R2C : CUFFT_D2Z, c2c = f32 ? CUFFT_C2C : CUFFT_Z2Z;
+    // 2D: row/column passes pruned to the columns |k_x| <= kx_max that hold
+    // active modes (the type-1 column pass needs only k_x in [0, kx_max]; the
+    // type-2 input is zero outside k_x in [-kx_max, kx_max])
+    int kx_max = 0;
+    for (int i = 0; i < n_active_; ++i) kx_max = std::max(kx_max, std::abs(idx[i] % n_ - K_));
+    pruned_ = (D == 2) && n_active_ > 0 && 2 * kx_max + 1 < geom_.nf[0];
+    if (pruned_) {
+      const int nf0 = geom_.nf[0], nf1 = geom_.nf[1];
+      kx_max_ = kx_max;
+      int n0 = nf0, n1 = nf1, emb0 = nf0, embh = nh0_, emb1 = nf1;
+      FB_CUFFT(cufftPlanMany(&plan_r2c_, 1, &n0, &emb0, 1, nf0, &embh, 1, nh0_, r2c, nf1));
+      FB_CUFFT(cufftPlanMany(&plan_col1_, 1, &n1, &emb1, nh0_, 1, &emb1, nh0_, 1, c2c, kx_max + 1));
+      FB_CUFFT(cufftPlanMany(&plan_col2a_, 1, &n1, &emb1, nf0, 1, &emb1, nf0, 1, c2c, kx_max + 1));
+      if (kx_max > 0) FB_CUFFT(cufftPlanMany(&plan_col2b_, 1, &n1, &emb1, nf0, 1, &emb1, nf0, 1, c2c, kx_max));
+      FB_CUFFT(cufftPlanMany(&plan_c2c_, 1, &n0, &emb0, 1, nf0, &emb0, 1, nf0, c2c, nf1));
+      // column-pass output: the columns outside the active band stay zero for good
+      tgrid_.alloc(G);
+      FB_CUDA(cudaMemset(tgrid_.p, 0, tgrid_.bytes()));
+    } else {
+      FB_CUFFT(cufftPlanMany(&plan_r2c_, D, dims, nullptr, 1, 0, nullptr, 1, 0, r2c, 1));
+      FB_CUFFT(cufftPlanMany(&plan_c2c_, D, dims, nullptr, 1, int(G), nullptr, 1, int(G), c2c, nfields_));
+    }
     FB_CUDA(cudaDeviceSynchronize());
   }
 
   ~NUwUImpl() override {
-    if (plan_r2c_) cufftDestroy(plan_r2c_);
-    if (plan_c2c_) cufftDestroy(plan_c2c_);
+    for (cufftHandle h : {plan_r2c_, plan_c2c_, plan_col1_, plan_col2a_, plan_col2b_})
+      if (h) cufftDestroy(h);
   }
 
   int64_t ndof() const override { return N_ * D; }
@@ -250,6 +270,7 @@ class NUwUImpl final : public Potential {
     s += " tile=";
     for (int a = 0; a < D; ++a) s += (a ? "x" : "") + std::to_string(geom_.tile[a]);
     s += " bins=" + std::to_string(geom_.nbins()) + " active_modes=" + std::to_string(n_active_);
+    if (pruned_) s += " fft=columns|kx|<=" + std::to_string(kx_max_);
     return s;
   }
 
@@ -279,6 +300,7 @@ class NUwUImpl final : public Potential {
       FB_CUFFT(cufftExecD2Z(plan_r2c_, reinterpret_cast<cufftDoubleReal*>(spread_grid_.p),
                             reinterpret_cast<cufftDoubleComplex*>(bhat_.p)));
     }
+    if (pruned_) exec_c2c(plan_col1_, bhat_.p, bhat_.p, s);  // columns k_x = 0..kx_max, in place
     timer_mark("fft_type1", s);
     if (n_active_ > 0) {
       const int grid = int(std::min<int64_t>(ceil_div(n_active_, 256), int64_t(sm_count()) * 8));
@@ -295,13 +317,14 @@ class NUwUImpl final : public Potential {
     }
     timer_mark("modes", s);
     if (!g) return;
-    FB_CUFFT(cufftSetStream(plan_c2c_, s));
-    if (sizeof(T) == 4) {
-      FB_CUFFT(cufftExecC2C(plan_c2c_, reinterpret_cast<cufftComplex*>(hgrid_.p),
-                            reinterpret_cast<cufftComplex*>(ggrid_.p), CUFFT_FORWARD));
+    if (pruned_) {
+      // columns k_x in [0, kx_max] and [nf0 - kx_max, nf0), then every row
+      const int off = geom_.nf[0] - kx_max_;
+      exec_c2c(plan_col2a_, hgrid_.p, tgrid_.p, s);
+      if (kx_max_ > 0) exec_c2c(plan_col2b_, hgrid_.p + off, tgrid_.p + off, s);
+      exec_c2c(plan_c2c_, tgrid_.p, ggrid_.p, s);
     } else {
-      FB_CUFFT(cufftExecZ2Z(plan_c2c_, reinterpret_cast<cufftDoubleComplex*>(hgrid_.p),
-                            reinterpret_cast<cufftDoubleComplex*>(ggrid_.p), CUFFT_FORWARD));
+      exec_c2c(plan_c2c_, hgrid_.p, ggrid_.p, s);
     }
     timer_mark("fft_type2", s);
     GradScale gs;  // exact mode: x = (p - round(p/L)) 2 pi / L, so d/dp = (2 pi / L) d/dx
@@ -310,6 +333,18 @@ class NUwUImpl final : public Potential {
     interp<T>(recs_.p, N_, cw_.p, uniform_c_, sort_, geom_, poly_, ggrid_.p, nfields_, INTERP_GRAD, g, nullptr,
               acc ? 1 : 0, status_.p, s, gs);
     timer_mark("interp", s);
+  }
+
+  // forward (sign -1) complex transform on stream s
+  static void exec_c2c(cufftHandle plan, cplx_t<T>* in, cplx_t<T>* out, cudaStream_t s) {
+    FB_CUFFT(cufftSetStream(plan, s));
+    if (sizeof(T) == 4) {
+      FB_CUFFT(cufftExecC2C(plan, reinterpret_cast<cufftComplex*>(in), reinterpret_cast<cufftComplex*>(out),
+                            CUFFT_FORWARD));
+    } else {
+      FB_CUFFT(cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(in),
+                            reinterpret_cast<cufftDoubleComplex*>(out), CUFFT_FORWARD));
+    }
   }
 
   int64_t N_;
@@ -327,12 +362,14 @@ class NUwUImpl final : public Potential {
   int nh0_ = 1;
   int nfields_ = 1;
   DevBuf<T> spread_grid_;
-  DevBuf<cplx_t<T>> bhat_, hgrid_, ggrid_;
+  DevBuf<cplx_t<T>> bhat_, hgrid_, ggrid_, tgrid_;
   DevBuf<double> corr_[3];
   DevBuf<int> mode_idx_;
   DevBuf<ModeCoef> coef_;
   int n_active_ = 0;
-  cufftHandle plan_r2c_ = 0, plan_c2c_ = 0;
+  cufftHandle plan_r2c_ = 0, plan_c2c_ = 0, plan_col1_ = 0, plan_col2a_ = 0, plan_col2b_ = 0;
+  bool pruned_ = false;
+  int kx_max_ = 0;
 };
 
 }  // namespace
