@@ -174,7 +174,7 @@ int fresco_potential_energy(fresco_potential p, const double* x, int64_t n, doub
     check_n(p, n);
     ensure_io(p, n);
     FB_CUDA(cudaMemcpyAsync(p->dx.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, p->stream));
-    p->pot->energy(p->dx.p, n, p->de.p, false, p->stream);
+    p->pot->eval(p->dx.p, n, nullptr, p->de.p, false, p->stream);
     p->pot->timer_collect();
     FB_CUDA(cudaMemcpyAsync(energy, p->de.p, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
     FB_CUDA(cudaStreamSynchronize(p->stream));
@@ -189,7 +189,7 @@ int fresco_potential_energy_gradient(fresco_potential p, const double* x, int64_
     check_n(p, n);
     ensure_io(p, n);
     FB_CUDA(cudaMemcpyAsync(p->dx.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, p->stream));
-    p->pot->energy_gradient(p->dx.p, n, p->dg.p, p->de.p, false, p->stream);
+    p->pot->eval(p->dx.p, n, p->dg.p, p->de.p, false, p->stream);
     p->pot->timer_collect();
     FB_CUDA(cudaMemcpyAsync(grad, p->dg.p, sizeof(double) * n, cudaMemcpyDeviceToHost, p->stream));
     FB_CUDA(cudaMemcpyAsync(energy, p->de.p, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
@@ -203,7 +203,7 @@ int fresco_potential_energy_device(fresco_potential p, const double* d_x, int64_
   return guarded([&] {
     if (!p || !d_energy || (n > 0 && !d_x)) throw fb::InvalidArgument("null argument");
     check_n(p, n);
-    p->pot->energy(d_x, n, d_energy, accumulate != 0, static_cast<cudaStream_t>(stream));
+    p->pot->eval(d_x, n, nullptr, d_energy, accumulate != 0, static_cast<cudaStream_t>(stream));
     return FRESCO_OK;
   });
 }
@@ -213,7 +213,7 @@ int fresco_potential_energy_gradient_device(fresco_potential p, const double* d_
   return guarded([&] {
     if (!p || !d_energy || (n > 0 && (!d_x || !d_grad))) throw fb::InvalidArgument("null argument");
     check_n(p, n);
-    p->pot->energy_gradient(d_x, n, d_grad, d_energy, accumulate != 0, static_cast<cudaStream_t>(stream));
+    p->pot->eval(d_x, n, d_grad, d_energy, accumulate != 0, static_cast<cudaStream_t>(stream));
     return FRESCO_OK;
   });
 }

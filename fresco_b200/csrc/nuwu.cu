@@ -290,6 +290,7 @@ class NUwUImpl final : public Potential {
     bin_sort<T>(x, N_, mp, geom_, sort_, recs_.p, status_.p, s);
     timer_mark("sort", s);
     FB_CUDA(cudaMemsetAsync(spread_grid_.p, 0, spread_grid_.bytes(), s));
+    timer_mark("zero_grid", s);
     spread_real<T>(recs_.p, cw_.p, uniform_c_, sort_, geom_, poly_, spread_grid_.p, s);
     timer_mark("spread", s);
     FB_CUFFT(cufftSetStream(plan_r2c_, s));

@@ -686,7 +686,7 @@ Optimizer::~Optimizer() {
   if (host_) cudaFreeHost(host_);
 }
 
-void Optimizer::eval(const double* x, double* g, double* e) { pot_->energy_gradient(x, n_, g, e, false, s_); }
+void Optimizer::eval(const double* x, double* g, double* e) { pot_->eval(x, n_, g, e, false, s_); }
 
 void Optimizer::run(int niter) {
   if (!func_initialized_) initialize_func_gradient();

@@ -3,6 +3,73 @@
 
 namespace fb {
 
+Potential::~Potential() {
+  invalidate_graphs();
+  if (capture_stream_) cudaStreamDestroy(capture_stream_);
+}
+
+void Potential::invalidate_graphs() {
+  for (auto& ge : graphs_)
+    if (ge.exec) cudaGraphExecDestroy(ge.exec);
+  graphs_.clear();
+}
+
+void Potential::set_graphs_enabled(bool on) {
+  graphs_enabled_ = on;
+  if (!on) invalidate_graphs();
+}
+
+void Potential::eval(const double* x, int64_t n, double* g, double* e, bool acc, cudaStream_t s) {
+  auto direct = [&](cudaStream_t st) {
+    if (g) energy_gradient(x, n, g, e, acc, st);
+    else energy(x, n, e, acc, st);
+  };
+  if (!graphs_enabled_ || timing_active()) {
+    direct(s);
+    return;
+  }
+  ++graph_clock_;
+  GraphEntry* hit = nullptr;
+  for (auto& ge : graphs_)
+    if (ge.x == x && ge.g == g && ge.e == e && ge.n == n && ge.acc == acc && ge.mode == grad_mode_) hit = &ge;
+  if (hit && hit->exec) {
+    hit->last_use = graph_clock_;
+    FB_CUDA(cudaGraphLaunch(hit->exec, s));
+    return;
+  }
+  if (!hit) {  // first sighting: remember the key, run directly
+    if (graphs_.size() == kMaxGraphs) {
+      size_t old = 0;
+      for (size_t i = 1; i < graphs_.size(); ++i)
+        if (graphs_[i].last_use < graphs_[old].last_use) old = i;
+      if (graphs_[old].exec) cudaGraphExecDestroy(graphs_[old].exec);
+      graphs_.erase(graphs_.begin() + old);
+    }
+    graphs_.push_back(GraphEntry{x, g, e, n, acc, grad_mode_, graph_clock_, nullptr});
+    direct(s);
+    return;
+  }
+  // second sighting: capture on the private stream, then launch on s
+  if (!capture_stream_) FB_CUDA(cudaStreamCreateWithFlags(&capture_stream_, cudaStreamNonBlocking));
+  FB_CUDA(cudaStreamBeginCapture(capture_stream_, cudaStreamCaptureModeRelaxed));
+  cudaGraph_t graph = nullptr;
+  try {
+    direct(capture_stream_);
+  } catch (...) {
+    cudaStreamEndCapture(capture_stream_, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  FB_CUDA(cudaStreamEndCapture(capture_stream_, &graph));
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t rc = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  FB_CUDA(rc);
+  hit->exec = exec;
+  hit->last_use = graph_clock_;
+  FB_CUDA(cudaGraphLaunch(exec, s));
+}
+
 void Potential::init_status() {
   FB_CUDA(cudaGetDevice(&device));
   status_.alloc(2);
@@ -71,6 +138,14 @@ CombinedPotential::CombinedPotential() { init_status(); }
 void CombinedPotential::add(PotentialPtr p) {
   if (!p) throw InvalidArgument("cannot add a null potential");
   parts_.push_back(std::move(p));
+  invalidate_graphs();
+}
+
+bool CombinedPotential::timing_active() const {
+  if (timer.enabled) return true;
+  for (auto& p : parts_)
+    if (p->timing_active()) return true;
+  return false;
 }
 
 int64_t CombinedPotential::ndof() const {

@@ -14,7 +14,7 @@ namespace fb {
 
 class Potential {
  public:
-  virtual ~Potential() = default;
+  virtual ~Potential();
 
   // Number of coordinates the potential expects (-1: any).
   virtual int64_t ndof() const = 0;
@@ -27,6 +27,14 @@ class Potential {
   // without the temporary vector).
   virtual void energy_gradient(const double* x, int64_t n, double* grad, double* energy, bool accumulate,
                                cudaStream_t s) = 0;
+
+  // energy_gradient (grad != nullptr) or energy, replayed as a CUDA graph
+  // when the same call (buffers, accumulate flag, gradient mode) repeats: the
+  // second call with a given set captures the launches on a private stream,
+  // and that call and every later one launch the instantiated graph on s.
+  // One-off buffer sets run directly.  Stage timing bypasses the graphs.
+  void eval(const double* x, int64_t n, double* grad, double* energy, bool accumulate, cudaStream_t s);
+  void set_graphs_enabled(bool on);
 
   // Sticky status bits (StatusBits) raised by kernels since the last read.
   virtual int read_and_clear_status(cudaStream_t s);
@@ -62,12 +70,31 @@ class Potential {
   void timer_begin(cudaStream_t s);
   void timer_mark(const char* name, cudaStream_t s);  // records the end of a stage
   void timer_collect();                              // host sync; accumulates elapsed times
+  virtual bool timing_active() const { return timer.enabled; }
 
  protected:
+  void invalidate_graphs();
   int grad_mode_ = 0;
   DevBuf<int> status_;  // [0] current evaluation, [1] accumulated for the host
   void init_status();
   void begin_eval_status(cudaStream_t s) { FB_CUDA(cudaMemsetAsync(status_.p, 0, sizeof(int), s)); }
+
+ private:
+  struct GraphEntry {
+    const double* x;
+    double* g;
+    double* e;
+    int64_t n;
+    bool acc;
+    int mode;
+    uint64_t last_use;
+    cudaGraphExec_t exec;  // null until the second call with this key
+  };
+  static constexpr size_t kMaxGraphs = 8;
+  std::vector<GraphEntry> graphs_;
+  uint64_t graph_clock_ = 0;
+  bool graphs_enabled_ = true;
+  cudaStream_t capture_stream_ = nullptr;
 };
 
 using PotentialPtr = std::shared_ptr<Potential>;
@@ -82,6 +109,7 @@ class CombinedPotential : public Potential {
   void energy_gradient(const double* x, int64_t n, double* g, double* e, bool acc, cudaStream_t s) override;
   int read_and_clear_status(cudaStream_t s) override;
   void set_gradient_mode(int mode) override;
+  bool timing_active() const override;
   std::string kind() const override { return "CombinedPotential"; }
   const std::vector<PotentialPtr>& parts() const { return parts_; }
 

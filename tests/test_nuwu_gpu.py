@@ -120,3 +120,46 @@ def test_nuwu_bad_arguments():
         pot.get_energy_gradient(x[:-1])
     with pytest.raises(ValueError):
         NUwU(radii, 3, Sk, V, L, precision="fp16")
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_nuwu_graph_replay_follows_buffer_contents(prec):
+    """Repeated calls on the same buffers are replayed as a CUDA graph (captured at the second call); the
+    replay must read the buffers' current contents, exactly as a direct evaluation does."""
+    import torch
+
+    from fresco_b200 import CombinedPotential, InversePower, NUwU
+
+    N, K, kmax = 3000, 24, 10
+    # spreading sums in a run-dependent order, so repeated evaluations agree to rounding only
+    tol = 1e-5 if prec == "fp32" else 1e-11
+    x0, radii, Sk, V, L = O.stealthy_nuwu_inputs(N, K, kmax, ndim=2, seed=11)
+    rng = np.random.default_rng(3)
+    pot = NUwU(radii, K, Sk, V, L, precision=prec)
+    xt = torch.tensor(x0, device="cuda")
+    g = torch.empty_like(xt)
+    e = torch.zeros((), dtype=torch.float64, device="cuda")
+    for it in range(5):
+        xi = x0 + 0.01 * it * rng.standard_normal(x0.size)
+        xt.copy_(torch.from_numpy(xi))
+        pot.energy_gradient_device(xt, g, e)
+        torch.cuda.synchronize()
+        fresh = NUwU(radii, K, Sk, V, L, precision=prec)  # first call: direct launches
+        e0, g0 = fresh.get_energy_gradient(xi)
+        assert float(e.item()) == pytest.approx(e0, rel=tol), it
+        np.testing.assert_allclose(g.cpu().numpy(), g0, rtol=0, atol=tol * np.abs(g0).max())
+
+    # a combined potential replays all its parts
+    box = np.array([2 * np.pi, 2 * np.pi])
+    rep = InversePower(2.0, 1.0, 0.02 * np.ones(N), box)
+    comb = CombinedPotential()
+    comb.add_potential(pot)
+    comb.add_potential(rep)
+    for it in range(4):
+        xi = x0 + 0.02 * it
+        xt.copy_(torch.from_numpy(xi))
+        comb.energy_gradient_device(xt, g, e)
+        torch.cuda.synchronize()
+        e_parts = NUwU(radii, K, Sk, V, L, precision=prec).get_energy_gradient(xi)[0]
+        e_parts += InversePower(2.0, 1.0, 0.02 * np.ones(N), box).get_energy_gradient(xi)[0]
+        assert float(e.item()) == pytest.approx(e_parts, rel=tol), it
