@@ -94,16 +94,21 @@ __device__ inline double warp_sum(double v) {
   return v;
 }
 
+// Linear thread index and thread count of the block (any block shape whose
+// x extent is a multiple of 32 when y or z exceed 1).
+__device__ __forceinline__ int block_tid() { return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z); }
+__device__ __forceinline__ int block_threads() { return blockDim.x * blockDim.y * blockDim.z; }
+
 // Adds the block-wide sum of v into *out (one atomic per block).  Every
 // thread of the block must call it.
 __device__ inline void block_sum_atomic(double v, double* out) {
   __shared__ double red[32];
   v = warp_sum(v);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int lane = block_tid() & 31, wid = block_tid() >> 5;
   if (lane == 0) red[wid] = v;
   __syncthreads();
   if (wid == 0) {
-    const int nw = (blockDim.x + 31) >> 5;
+    const int nw = (block_threads() + 31) >> 5;
     double s = lane < nw ? red[lane] : 0.0;
     s = warp_sum(s);
     if (lane == 0 && s != 0.0) atomicAdd(out, s);
@@ -115,7 +120,7 @@ __device__ inline void block_sum_atomic(double v, double* out) {
 template <int K>
 __device__ inline void block_sum_atomic_k(double (&v)[K], double* out) {
   __shared__ double red[K][32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int lane = block_tid() & 31, wid = block_tid() >> 5;
 #pragma unroll
   for (int i = 0; i < K; ++i) {
     double s = warp_sum(v[i]);
@@ -123,7 +128,7 @@ __device__ inline void block_sum_atomic_k(double (&v)[K], double* out) {
   }
   __syncthreads();
   if (wid == 0) {
-    const int nw = (blockDim.x + 31) >> 5;
+    const int nw = (block_threads() + 31) >> 5;
 #pragma unroll
     for (int i = 0; i < K; ++i) {
       double s = lane < nw ? red[i][lane] : 0.0;

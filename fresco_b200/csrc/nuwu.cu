@@ -24,6 +24,7 @@
 #include <string>
 #include <vector>
 
+#include "fft_block.cuh"
 #include "nufft.cuh"
 #include "potential.cuh"
 
@@ -103,6 +104,145 @@ __global__ void __launch_bounds__(256) nuwu_modes_kernel(
   if (blockIdx.x == 0 && threadIdx.x == 0 && status != nullptr && ((*status) & STATUS_NONFINITE_INPUT)) {
     atomicAdd(energy, __longlong_as_double(0x7ff8000000000000ULL));
   }
+}
+
+// ---------------------------------------------------------------------------
+// 2D band transforms.  The loss only reads modes with |k_x| <= Kx and
+// |k_y| <= Ky (the active band), so the 2D transforms are split into passes
+// that touch only what the band needs (all forward, sign -1, as cuFFT; fine
+// grid N x N with N a power of two, RegFft<T, N>):
+//   rows_r2c:   per transform two real fine-grid rows (z = a + i b), keeps
+//               k_x = 0..Kx of each row                        -> band1[N][Kx+1]
+//   band_modes: one k_x >= 0 per block: column FFT of band1, the mode pass for
+//               +k_x and -k_x (deconvolve, S, d, phi, packed field h), and the
+//               column FFTs of the two h columns              -> band2[N][2Kx+1]
+//   rows_c2c:   per transform one band2 row placed at k_x mod N -> the full
+//               type-2 output row.
+// Each block runs two transforms (threadIdx.y = 0, 1) of N / 16 threads with
+// their own named barriers.
+// ---------------------------------------------------------------------------
+
+template <typename T, int N>
+__global__ void __launch_bounds__(N / 8) band_rows_r2c_kernel(const T* __restrict__ grid,
+                                                               const cplx_t<T>* __restrict__ tw, int KB,
+                                                               cplx_t<T>* __restrict__ band1) {
+  using F = RegFft<T, N>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx_t<T>* buf = reinterpret_cast<cplx_t<T>*>(smem_raw) + threadIdx.y * fft_padded(N);
+  const int t = threadIdx.x;
+  const int64_t y = 2 * (2 * int64_t(blockIdx.x) + threadIdx.y);
+  const T* ra = grid + y * N;
+  const T* rb = ra + N;
+  cplx_t<T> v[F::E];
+#pragma unroll
+  for (int j = 0; j < F::E; ++j) {
+    v[j].x = ra[t + j * (N / F::E)];
+    v[j].y = rb[t + j * (N / F::E)];
+  }
+  F::run(v, buf, tw, t, 1 + threadIdx.y);
+  // A(k) = (Z(k) + conj Z(-k)) / 2, B(k) = (Z(k) - conj Z(-k)) / (2i)
+  for (int k = t; k < KB; k += F::TPB) {
+    const cplx_t<T> zk = buf[fpad(k)], zm = buf[fpad(k == 0 ? 0 : N - k)];
+    cplx_t<T> A, B;
+    A.x = T(0.5) * (zk.x + zm.x);
+    A.y = T(0.5) * (zk.y - zm.y);
+    B.x = T(0.5) * (zk.y + zm.y);
+    B.y = T(0.5) * (zm.x - zk.x);
+    band1[y * KB + k] = A;
+    band1[(y + 1) * KB + k] = B;
+  }
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(N / 8) band_modes_kernel(
+    const cplx_t<T>* __restrict__ band1, const cplx_t<T>* __restrict__ tw, int Kx, int Ky, int K,
+    const ModeCoef* __restrict__ coef, const double* __restrict__ corr0, const double* __restrict__ corr1, double invN,
+    cplx_t<T>* __restrict__ band2, double* energy, const int* __restrict__ status, int want_grad) {
+  using F = RegFft<T, N>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx_t<T>* col = reinterpret_cast<cplx_t<T>*>(smem_raw);
+  cplx_t<T>* h1 = col + fft_padded(N);  // field column +k_x
+  cplx_t<T>* h2 = h1 + fft_padded(N);   // field column -k_x
+  const int t = threadIdx.x, grp = threadIdx.y;
+  const int tid = grp * F::TPB + t, nthr = 2 * F::TPB;
+  const int kx = blockIdx.x;
+  const int KB = Kx + 1, NB2 = 2 * Kx + 1, NY = 2 * Ky + 1;
+  if (want_grad)
+    for (int i = tid; i < N; i += nthr) {
+      h1[fpad(i)] = cplx_t<T>{T(0), T(0)};
+      h2[fpad(i)] = cplx_t<T>{T(0), T(0)};
+    }
+  if (grp == 0) {  // B(k_x, k_y) for all k_y (mod N)
+    cplx_t<T> v[F::E];
+#pragma unroll
+    for (int j = 0; j < F::E; ++j) v[j] = band1[int64_t(t + j * (N / F::E)) * KB + kx];
+    F::run(v, col, tw, t, 1);
+  }
+  __syncthreads();
+  double phi = 0.0;
+  for (int i = tid; i < NY; i += nthr) {
+    const int ky = i - Ky;
+    const double py = corr1[ky + K];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      if (side == 1 && kx == 0) break;
+      const int kxs = side == 0 ? kx : -kx;
+      const ModeCoef c = coef[int64_t(kxs + Kx) * NY + i];
+      if (c.w2 == 0.0 && c.A == 0.0 && c.B == 0.0) continue;  // outside the active set
+      const double p = corr0[kxs + K] * py;
+      // rho(k) = conj(B(k)) for k_x >= 0; rho(-|k_x|, k_y) = B(|k_x|, -k_y)
+      const int yy = side == 0 ? (ky < 0 ? ky + N : ky) : (ky > 0 ? N - ky : -ky);
+      const cplx_t<T> bv = col[fpad(yy)];
+      const double rr = double(bv.x) / p;
+      const double ri = (side == 0 ? -double(bv.y) : double(bv.y)) / p;
+      const double q = (rr * rr + ri * ri) * invN;
+      const double dq = q - c.s0;
+      phi += c.w2 * dq * dq;
+      if (want_grad) {
+        const double a = (c.A * q - c.B) * (2.0 * invN) / p;  // includes the type-2 pre-correction 1/p
+        const double fr = rr * a, fi = ri * a;
+        cplx_t<T> h;  // F (k_y - i k_x)
+        h.x = T(fr * ky + fi * kxs);
+        h.y = T(fi * ky - fr * kxs);
+        (side == 0 ? h1 : h2)[fpad(ky < 0 ? ky + N : ky)] = h;
+      }
+    }
+  }
+  block_sum_atomic(phi, energy);  // ends with __syncthreads
+  if (blockIdx.x == 0 && tid == 0 && status != nullptr && ((*status) & STATUS_NONFINITE_INPUT))
+    atomicAdd(energy, __longlong_as_double(0x7ff8000000000000ULL));
+  if (!want_grad) return;
+  if (grp == 1 && kx == 0) return;  // k_x = 0 has one column
+  cplx_t<T>* h = grp == 0 ? h1 : h2;
+  cplx_t<T> v[F::E];
+#pragma unroll
+  for (int j = 0; j < F::E; ++j) v[j] = h[fpad(t + j * (N / F::E))];
+  group_sync(1 + grp, F::TPB);  // every input is in registers before h is reused
+  F::run(v, h, tw, t, 1 + grp);
+  const int c = grp == 0 ? Kx + kx : Kx - kx;
+  for (int y = t; y < N; y += F::TPB) band2[int64_t(y) * NB2 + c] = h[fpad(y)];
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(N / 8) band_rows_c2c_kernel(const cplx_t<T>* __restrict__ band2, int Kx,
+                                                               const cplx_t<T>* __restrict__ tw,
+                                                               cplx_t<T>* __restrict__ out) {
+  using F = RegFft<T, N>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx_t<T>* buf = reinterpret_cast<cplx_t<T>*>(smem_raw) + threadIdx.y * fft_padded(N);
+  const int t = threadIdx.x;
+  const int64_t y = 2 * int64_t(blockIdx.x) + threadIdx.y;
+  const int NB2 = 2 * Kx + 1;
+  const cplx_t<T>* row = band2 + y * NB2;
+  cplx_t<T> v[F::E];
+#pragma unroll
+  for (int j = 0; j < F::E; ++j) {
+    const int x = t + j * (N / F::E);  // k_x = x for x <= Kx, x - N for x >= N - Kx, else no mode
+    v[j] = x <= Kx ? row[Kx + x] : (x >= N - Kx ? row[Kx + x - N] : cplx_t<T>{T(0), T(0)});
+  }
+  F::run(v, buf, tw, t, 1 + threadIdx.y);
+  cplx_t<T>* o = out + y * N;
+  for (int x = t; x < N; x += F::TPB) o[x] = buf[fpad(x)];
 }
 
 template <int D, typename T>
@@ -227,8 +367,11 @@ class NUwUImpl final : public Potential {
     // type-2 input is zero outside k_x in [-kx_max, kx_max])
     int kx_max = 0;
     for (int i = 0; i < n_active_; ++i) kx_max = std::max(kx_max, std::abs(idx[i] % n_ - K_));
-    pruned_ = (D == 2) && n_active_ > 0 && 2 * kx_max + 1 < geom_.nf[0];
-    if (pruned_) {
+    setup_band(idx, coef);
+    pruned_ = !band_ && (D == 2) && n_active_ > 0 && 2 * kx_max + 1 < geom_.nf[0];
+    if (band_) {
+      // no cuFFT plans: the band kernels do all transforms
+    } else if (pruned_) {
       const int nf0 = geom_.nf[0], nf1 = geom_.nf[1];
       kx_max_ = kx_max;
       int n0 = nf0, n1 = nf1, emb0 = nf0, embh = nh0_, emb1 = nf1;
@@ -270,6 +413,7 @@ class NUwUImpl final : public Potential {
     s += " tile=";
     for (int a = 0; a < D; ++a) s += (a ? "x" : "") + std::to_string(geom_.tile[a]);
     s += " bins=" + std::to_string(geom_.nbins()) + " active_modes=" + std::to_string(n_active_);
+    if (band_) s += " fft=band|kx|<=" + std::to_string(Kx_) + ",|ky|<=" + std::to_string(Ky_);
     if (pruned_) s += " fft=columns|kx|<=" + std::to_string(kx_max_);
     return s;
   }
@@ -293,6 +437,10 @@ class NUwUImpl final : public Potential {
     timer_mark("zero_grid", s);
     spread_real<T>(recs_.p, cw_.p, uniform_c_, sort_, geom_, poly_, spread_grid_.p, s);
     timer_mark("spread", s);
+    if (band_) {
+      run_band(e, g, acc, s);
+      return;
+    }
     FB_CUFFT(cufftSetStream(plan_r2c_, s));
     if (sizeof(T) == 4) {
       FB_CUFFT(cufftExecR2C(plan_r2c_, reinterpret_cast<cufftReal*>(spread_grid_.p),
@@ -336,6 +484,97 @@ class NUwUImpl final : public Potential {
     timer_mark("interp", s);
   }
 
+  // 2D band transforms (see band_rows_r2c_kernel): used when the fine grid is
+  // N x N with N a power of two in 512..8192.
+  template <int N>
+  void band_attrs() {
+    const size_t cb = sizeof(cplx_t<T>);
+    smem_rows_ = 2 * size_t(fft_padded(N)) * cb;
+    smem_modes_ = 3 * size_t(fft_padded(N)) * cb;
+    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(band_rows_r2c_kernel<T, N>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_rows_)));
+    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(band_rows_c2c_kernel<T, N>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_rows_)));
+    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(band_modes_kernel<T, N>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_modes_)));
+  }
+
+  void setup_band(const std::vector<int>& idx, const std::vector<ModeCoef>& coef) {
+    band_ = false;
+    if (D != 2 || n_active_ == 0) return;
+    const int nf0 = geom_.nf[0], nf1 = geom_.nf[1];
+    if (nf0 != nf1 || nf0 < 512 || nf0 > 8192 || (nf0 & (nf0 - 1)) != 0) return;
+    if (3 * size_t(fft_padded(nf0)) * sizeof(cplx_t<T>) > 200 * 1024) return;
+    int kxm = 0, kym = 0;
+    for (int m : idx) {
+      kxm = std::max(kxm, std::abs(m % n_ - K_));
+      kym = std::max(kym, std::abs(m / n_ - K_));
+    }
+    if (2 * kxm + 1 > nf0 / 2) return;
+    Kx_ = kxm;
+    Ky_ = kym;
+    const std::vector<double> t = fft_twiddles(nf0);
+    std::vector<cplx_t<T>> h(nf0);
+    for (int j = 0; j < nf0; ++j) {
+      h[j].x = T(t[2 * size_t(j)]);
+      h[j].y = T(t[2 * size_t(j) + 1]);
+    }
+    tw_.alloc(nf0);
+    FB_CUDA(cudaMemcpy(tw_.p, h.data(), sizeof(cplx_t<T>) * nf0, cudaMemcpyHostToDevice));
+    const int NY = 2 * Ky_ + 1, NX = 2 * Kx_ + 1;
+    std::vector<ModeCoef> box(size_t(NX) * NY, ModeCoef{0.0, 0.0, 0.0, 0.0});
+    for (size_t i = 0; i < idx.size(); ++i) {
+      const int kx = idx[i] % n_ - K_, ky = idx[i] / n_ - K_;
+      box[size_t(kx + Kx_) * NY + (ky + Ky_)] = coef[i];
+    }
+    coef_box_.alloc(box.size());
+    FB_CUDA(cudaMemcpy(coef_box_.p, box.data(), sizeof(ModeCoef) * box.size(), cudaMemcpyHostToDevice));
+    band1_.alloc(int64_t(nf1) * (Kx_ + 1));
+    band2_.alloc(int64_t(nf1) * NX);
+    switch (nf0) {
+      case 512: band_attrs<512>(); break;
+      case 1024: band_attrs<1024>(); break;
+      case 2048: band_attrs<2048>(); break;
+      case 4096: band_attrs<4096>(); break;
+      default: band_attrs<8192>(); break;
+    }
+    band_ = true;
+  }
+
+  template <int N>
+  void run_band_n(double* e, double* g, cudaStream_t s) {
+    const dim3 blk(N / 16, 2);
+    band_rows_r2c_kernel<T, N><<<N / 4, blk, smem_rows_, s>>>(spread_grid_.p, tw_.p, Kx_ + 1, band1_.p);
+    FB_LAUNCH_CHECK();
+    timer_mark("fft_type1", s);
+    band_modes_kernel<T, N><<<Kx_ + 1, blk, smem_modes_, s>>>(band1_.p, tw_.p, Kx_, Ky_, K_, coef_box_.p, corr_[0].p,
+                                                               corr_[1].p, 1.0 / double(N_), band2_.p, e, status_.p,
+                                                               g != nullptr);
+    FB_LAUNCH_CHECK();
+    timer_mark("modes", s);
+    if (!g) return;
+    band_rows_c2c_kernel<T, N><<<N / 2, blk, smem_rows_, s>>>(band2_.p, Kx_, tw_.p, ggrid_.p);
+    FB_LAUNCH_CHECK();
+    timer_mark("fft_type2", s);
+  }
+
+  void run_band(double* e, double* g, bool acc, cudaStream_t s) {
+    switch (geom_.nf[0]) {
+      case 512: run_band_n<512>(e, g, s); break;
+      case 1024: run_band_n<1024>(e, g, s); break;
+      case 2048: run_band_n<2048>(e, g, s); break;
+      case 4096: run_band_n<4096>(e, g, s); break;
+      default: run_band_n<8192>(e, g, s); break;
+    }
+    if (!g) return;
+    GradScale gs;
+    if (grad_mode_ == 1)
+      for (int a = 0; a < D; ++a) gs.s[a] = 2.0 * M_PI / L_[a];
+    interp<T>(recs_.p, N_, cw_.p, uniform_c_, sort_, geom_, poly_, ggrid_.p, nfields_, INTERP_GRAD, g, nullptr,
+              acc ? 1 : 0, status_.p, s, gs);
+    timer_mark("interp", s);
+  }
+
   // forward (sign -1) complex transform on stream s
   static void exec_c2c(cufftHandle plan, cplx_t<T>* in, cplx_t<T>* out, cudaStream_t s) {
     FB_CUFFT(cufftSetStream(plan, s));
@@ -371,6 +610,11 @@ class NUwUImpl final : public Potential {
   cufftHandle plan_r2c_ = 0, plan_c2c_ = 0, plan_col1_ = 0, plan_col2a_ = 0, plan_col2b_ = 0;
   bool pruned_ = false;
   int kx_max_ = 0;
+  bool band_ = false;
+  int Kx_ = 0, Ky_ = 0;
+  DevBuf<cplx_t<T>> tw_, band1_, band2_;
+  DevBuf<ModeCoef> coef_box_;
+  size_t smem_rows_ = 0, smem_modes_ = 0;
 };
 
 }  // namespace

@@ -56,6 +56,27 @@ def test_nuwu_asymmetric_targets(prec, eps, tol, ndim):
     _check(pot, ref, x, tol)
 
 
+@pytest.mark.parametrize("prec,eps,tol", PRECISIONS)
+@pytest.mark.parametrize("K,kmax,random_weights,band", [(128, 80, False, True), (128, 100, True, True),
+                                                        (64, 40, True, False), (128, 128, True, False)])
+def test_nuwu_2d_band_transforms(prec, eps, tol, K, kmax, random_weights, band):
+    """Power-of-two fine grids of 512 and more take the band transforms (register FFTs over
+    |k_x| <= kmax); a 256 grid, or a band as wide as the grid allows, falls back to the cuFFT passes."""
+    from fresco_b200 import NUwU
+
+    N = 1500
+    x, radii, Sk, V, L = _inputs(2, N, K, kmax, seed=K + kmax, random_weights=random_weights)
+    if random_weights:  # keep the asymmetric targets inside the band
+        n = 2 * K + 1
+        k = np.arange(n) - K
+        inside = (np.abs(k)[None, :] <= kmax) & (np.abs(k)[:, None] <= kmax)
+        V = np.where(inside.reshape(V.shape), V, 0.0)
+    ref = O.NUwU(radii, K, Sk, V, L)
+    pot = NUwU(radii, K, Sk, V, L, eps=eps, precision=prec)
+    assert ("fft=band" in pot.describe()) == band, pot.describe()
+    _check(pot, ref, x, tol)
+
+
 @pytest.mark.parametrize("L", [1.0, 2 * np.pi, 3.7])
 def test_nuwu_box_map_quirk(L):
     """Points inside and outside the box under the reference's coordinate map (nuwu.hpp:216-250)."""
