@@ -25,7 +25,7 @@
 
 namespace fb {
 
-constexpr int kMaxSub = 1024;     // points per spreading/interpolation subproblem
+constexpr int kMaxSub = 1280;     // points per spreading/interpolation subproblem
 constexpr int kMaxBins = 32768;   // bins per geometry (block-local histograms live in shared memory)
 constexpr int kTile2D = 64;       // 2D tile edge (phased spreading needs a multiple of the sub-block edge)
 

@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(256) nuwu_modes_kernel(
 // that touch only what the band needs (all forward, sign -1, as cuFFT; fine
 // grid N x N with N a power of two, RegFft<T, N>):
 //   rows_r2c:   per transform two real fine-grid rows (z = a + i b), keeps
-//               k_x = 0..Kx of each row                        -> band1[N][Kx+1]
+//               k_x = 0..Kx of each row                        -> band1[Kx+1][N]
 //   band_modes: one k_x >= 0 per block: column FFT of band1, the mode pass for
 //               +k_x and -k_x (deconvolve, S, d, phi, packed field h), and the
 //               column FFTs of the two h columns              -> band2[N][2Kx+1]
@@ -148,8 +148,8 @@ __global__ void __launch_bounds__(N / 8) band_rows_r2c_kernel(const T* __restric
     A.y = T(0.5) * (zk.y - zm.y);
     B.x = T(0.5) * (zk.y + zm.y);
     B.y = T(0.5) * (zm.x - zk.x);
-    band1[y * KB + k] = A;
-    band1[(y + 1) * KB + k] = B;
+    band1[int64_t(k) * N + y] = A;
+    band1[int64_t(k) * N + y + 1] = B;
   }
 }
 
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(N / 8) band_modes_kernel(
   const int t = threadIdx.x, grp = threadIdx.y;
   const int tid = grp * F::TPB + t, nthr = 2 * F::TPB;
   const int kx = blockIdx.x;
-  const int KB = Kx + 1, NB2 = 2 * Kx + 1, NY = 2 * Ky + 1;
+  const int NB2 = 2 * Kx + 1, NY = 2 * Ky + 1;
   if (want_grad)
     for (int i = tid; i < N; i += nthr) {
       h1[fpad(i)] = cplx_t<T>{T(0), T(0)};
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(N / 8) band_modes_kernel(
   if (grp == 0) {  // B(k_x, k_y) for all k_y (mod N)
     cplx_t<T> v[F::E];
 #pragma unroll
-    for (int j = 0; j < F::E; ++j) v[j] = band1[int64_t(t + j * (N / F::E)) * KB + kx];
+    for (int j = 0; j < F::E; ++j) v[j] = band1[int64_t(kx) * N + t + j * (N / F::E)];
     F::run(v, col, tw, t, 1);
   }
   __syncthreads();
