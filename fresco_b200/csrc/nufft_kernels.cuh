@@ -290,7 +290,7 @@ __device__ __forceinline__ void flush_tile(const T* tile, const Geom& g, int org
 // touch the same cell: the tile is spread in four phases, one per parity
 // class, and within a phase every warp owns whole sub-blocks, whose points
 // it adds one after another (program order within the warp, __syncwarp
-// between points).  So no two threads ever update one cell concurrently and
+// between rounds).  So no two threads ever update one cell concurrently and
 // plain shared-memory read-modify-writes suffice.
 //
 // Per point, the whole warp works on its footprint: lanes hold the x and y
@@ -298,8 +298,9 @@ __device__ __forceinline__ void flush_tile(const T* tile, const Geom& g, int org
 // are formed after two shuffles, and the w x w cells are covered in passes
 // of R = 32 / w rows.  The tile pitch P = 64 + w is congruent to w modulo
 // 32, so the R * w cells of one pass fall in R * w distinct banks: every
-// access is conflict-free.  With w <= 8 two points share one round of tap
-// evaluation (lanes 0-15 and 16-31).
+// access is conflict-free.  With w <= 8 two points, one from each of two
+// sub-blocks of the phase, share one round of tap evaluation (lanes 0-15 and
+// 16-31).
 //
 // Before the phases, the block stages its points in shared memory grouped by
 // sub-block, already converted to (tile offset, polynomial variables,
@@ -467,26 +468,49 @@ __global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
   const bool cell_lane = lane < P::R * W;
   const int lane_off = rr * E + cc;
 
-  for (int phase = 0; phase < 4; ++phase) {
-    for (int q = warp; q < P::PER_PHASE; q += P::NWARP) {
-      const int qa = q % (P::NSB / 2), qb = q / (P::NSB / 2);
-      const int sbi = (2 * qa + (phase & 1)) + P::NSB * (2 * qb + (phase >> 1));
-      const int n = sb_count[sbi], b0 = sb_start[sbi];
-      for (int it = 0; it < n; it += P::PPW) {
-        const int pi = it + half;
-        const S st = srec[b0 + (pi < n ? pi : 0)];
-        const T u = xl ? st.u0 : st.u1;
-        T tap = cr[Q];
+  // Within a phase the PPW lane halves of a warp take different sub-blocks,
+  // whose footprints never overlap, so their points are added without a
+  // barrier between them; the taps of the next points are formed before the
+  // current ones are added.
+  auto taps = [&](int n, int b0, int it, T& tr, T& ti, int& base) {
+    const S st = srec[it < n ? b0 + it : 0];
+    const T u = xl ? st.u0 : st.u1;
+    T tap = cr[Q];
 #pragma unroll
-        for (int d = Q - 1; d >= 0; --d) tap = fma(tap, u, cr[d]);
-        const T tr = xl ? tap * st.wr : tap;
-        T ti = T(0);
-        if constexpr (CPLX) ti = xl ? tap * st.wi : T(0);
+    for (int d = Q - 1; d >= 0; --d) tap = fma(tap, u, cr[d]);
+    tr = xl ? tap * st.wr : tap;
+    ti = T(0);
+    if constexpr (CPLX) ti = xl ? tap * st.wi : T(0);
+    base = st.base;
+  };
+  for (int phase = 0; phase < 4; ++phase) {
+    for (int q0 = warp * P::PPW; q0 < P::PER_PHASE; q0 += P::NWARP * P::PPW) {
+      const int q = q0 + half;
+      int n = 0, b0 = 0;
+      if (q < P::PER_PHASE) {
+        const int qa = q % (P::NSB / 2), qb = q / (P::NSB / 2);
+        const int sbi = (2 * qa + (phase & 1)) + P::NSB * (2 * qb + (phase >> 1));
+        n = sb_count[sbi];
+        b0 = sb_start[sbi];
+      }
+      int nh[P::PPW], nmax = 0;
+#pragma unroll
+      for (int h = 0; h < P::PPW; ++h) {
+        nh[h] = __shfl_sync(0xffffffffu, n, h * P::HL);
+        nmax = max(nmax, nh[h]);
+      }
+      T tr, ti;
+      int base;
+      taps(n, b0, 0, tr, ti, base);
+      for (int it = 0; it < nmax; ++it) {
+        T ntr, nti;
+        int nbase;
+        taps(n, b0, it + 1, ntr, nti, nbase);
 #pragma unroll
         for (int h = 0; h < P::PPW; ++h) {
-          if (it + h >= n) break;
+          if (it >= nh[h]) continue;  // warp-uniform
           const int src = h * P::HL;
-          const int base = __shfl_sync(0xffffffffu, st.base, src);
+          const int bh = __shfl_sync(0xffffffffu, base, src);
           const T kxr = __shfl_sync(0xffffffffu, tr, src + cc);
           T kxi = T(0);
           if constexpr (CPLX) kxi = __shfl_sync(0xffffffffu, ti, src + cc);
@@ -495,13 +519,16 @@ __global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
             const int row = k * P::R + rr;
             const T ky = __shfl_sync(0xffffffffu, tr, src + W + (row < W ? row : W - 1));
             if (cell_lane && row < W) {
-              T* c = tile + (base + lane_off + k * P::R * E) * NC;
+              T* c = tile + (bh + lane_off + k * P::R * E) * NC;
               c[0] += kxr * ky;
               if constexpr (CPLX) c[1] += kxi * ky;
             }
           }
-          __syncwarp();
         }
+        __syncwarp();
+        tr = ntr;
+        ti = nti;
+        base = nbase;
       }
     }
     __syncthreads();
@@ -647,6 +674,13 @@ __device__ __forceinline__ void interp_store(int mode, uint32_t o, T wgt, T v0r,
 
 // 2D interpolation: one block per subproblem stages the tile (+ halo) of the
 // field in shared memory, then one thread per point sums its w x w taps.
+//
+// Every tap address of a point is its footprint's first cell `base` plus an
+// offset that is the same for all points, so a group of lanes served by one
+// shared-memory wavefront (16 lanes for 8-byte cells, 8 for 16-byte cells)
+// reads without bank conflicts when the bases of its points are distinct
+// modulo the group size.  The block therefore buckets its points by
+// base mod G and lane c of every group takes points of class c only.
 template <int W, typename T>
 __global__ void __launch_bounds__(256) interp2d_tile_kernel(
     const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, T uniform, const int* __restrict__ sub_bin,
@@ -655,27 +689,57 @@ __global__ void __launch_bounds__(256) interp2d_tile_kernel(
     const int* __restrict__ status, const GradScale gs) {
   constexpr int PAD = W / 2;
   constexpr int TW = kTile2D + W;
+  constexpr int G = 128 / int(sizeof(cplx_t<T>));  // lanes per wavefront = bank classes
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx_t<T>* tile = reinterpret_cast<cplx_t<T>*>(smem_raw);
+  uint16_t* code = reinterpret_cast<uint16_t*>(tile + TW * TW);  // class << 12 | rank in class
+  uint16_t* order = code + kMaxSub;                               // points grouped by class
+  __shared__ int cls_count[G], cls_start[G];
   const int sub = blockIdx.x;
   if (sub >= *num_sub) return;
+  const int tid = threadIdx.x;
   const bool bad = status != nullptr && ((*status) & STATUS_NONFINITE_INPUT);
   const int bin = sub_bin[sub];
   const int start = sub_start[sub], cnt = sub_count[sub];
   const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
   const int nf0 = g.nf[0], nf1 = g.nf[1];
-  for (int i = threadIdx.x; i < TW * TW; i += blockDim.x) {
+  if (tid < G) cls_count[tid] = 0;
+  __syncthreads();
+  for (int i = tid; i < TW * TW; i += blockDim.x) {
     const int i0 = i % TW, i1 = i / TW;
     const int a0 = wrap_index(org0 - PAD + i0, nf0), a1 = wrap_index(org1 - PAD + i1, nf1);
     tile[i] = field[int64_t(a1) * nf0 + a0];
   }
+  for (int p = tid; p < cnt; p += blockDim.x) {
+    const Rec<2, T> r = recs[start + p];
+    int c0, c1, c2;
+    unpack_cell(2, r.cell, c0, c1, c2);
+    T u;
+    const int l0 = c0 - org0 + es_start<W, T>(r.f[0], u) + PAD;
+    const int l1 = c1 - org1 + es_start<W, T>(r.f[1], u) + PAD;
+    const int cls = (l1 * TW + l0) & (G - 1);
+    code[p] = uint16_t((cls << 12) | atomicAdd(&cls_count[cls], 1));
+  }
   __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+    for (int c = 0; c < G; ++c) {
+      cls_start[c] = acc;
+      acc += cls_count[c];
+    }
+  }
+  __syncthreads();
+  for (int p = tid; p < cnt; p += blockDim.x) order[cls_start[code[p] >> 12] + (code[p] & 0xfff)] = uint16_t(p);
+  __syncthreads();
+  const int cls = tid % G, grp = tid / G, ngrp = int(blockDim.x) / G;
+  const int n_c = cls_count[cls];
+  const uint16_t* mine = order + cls_start[cls];
   // the next record is loaded while the current point is interpolated
   Rec<2, T> nxt;
-  if (int(threadIdx.x) < cnt) nxt = recs[start + threadIdx.x];
-  for (int p = threadIdx.x; p < cnt; p += blockDim.x) {
+  if (grp < n_c) nxt = recs[start + mine[grp]];
+  for (int j = grp; j < n_c; j += ngrp) {
     const Rec<2, T> r = nxt;
-    if (p + int(blockDim.x) < cnt) nxt = recs[start + p + blockDim.x];
+    if (j + ngrp < n_c) nxt = recs[start + mine[j + ngrp]];
     int c0, c1, c2;
     unpack_cell(2, r.cell, c0, c1, c2);
     T k0[W], k1[W];
@@ -838,7 +902,7 @@ void launch_interp2d(const void* recs, const T* weights, T uniform, const SortBu
                      const std::vector<double>& poly, const cplx_t<T>* field, int mode, double* grad, double2* out2,
                      int acc, const int* status, cudaStream_t s, const GradScale& gs) {
   constexpr int TW = kTile2D + W;
-  const size_t smem = sizeof(cplx_t<T>) * TW * TW;
+  const size_t smem = sizeof(cplx_t<T>) * TW * TW + 2 * sizeof(uint16_t) * kMaxSub;
   auto kern = interp2d_tile_kernel<W, T>;
   if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<2, T>*>(recs), weights, uniform, sb.sub_bin.p,
