@@ -705,20 +705,41 @@ __global__ void __launch_bounds__(256) interp2d_tile_kernel(
   const int nf0 = g.nf[0], nf1 = g.nf[1];
   if (tid < G) cls_count[tid] = 0;
   __syncthreads();
-  for (int i = tid; i < TW * TW; i += blockDim.x) {
-    const int i0 = i % TW, i1 = i / TW;
-    const int a0 = wrap_index(org0 - PAD + i0, nf0), a1 = wrap_index(org1 - PAD + i1, nf1);
-    tile[i] = field[int64_t(a1) * nf0 + a0];
+  // tile and records are read in batches of 4 loads per thread so that their
+  // latencies overlap
+  constexpr int BT = 4;
+  const int nthr = blockDim.x;
+  for (int i0 = tid; i0 < TW * TW; i0 += BT * nthr) {
+    cplx_t<T> v[BT];
+#pragma unroll
+    for (int b = 0; b < BT; ++b) {
+      const int i = i0 + b * nthr;
+      if (i < TW * TW) {
+        const int x = i % TW, y = i / TW;
+        v[b] = field[int64_t(wrap_index(org1 - PAD + y, nf1)) * nf0 + wrap_index(org0 - PAD + x, nf0)];
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < BT; ++b)
+      if (i0 + b * nthr < TW * TW) tile[i0 + b * nthr] = v[b];
   }
-  for (int p = tid; p < cnt; p += blockDim.x) {
-    const Rec<2, T> r = recs[start + p];
-    int c0, c1, c2;
-    unpack_cell(2, r.cell, c0, c1, c2);
-    T u;
-    const int l0 = c0 - org0 + es_start<W, T>(r.f[0], u) + PAD;
-    const int l1 = c1 - org1 + es_start<W, T>(r.f[1], u) + PAD;
-    const int cls = (l1 * TW + l0) & (G - 1);
-    code[p] = uint16_t((cls << 12) | atomicAdd(&cls_count[cls], 1));
+  for (int p0 = tid; p0 < cnt; p0 += BT * nthr) {
+    Rec<2, T> r[BT];
+#pragma unroll
+    for (int b = 0; b < BT; ++b)
+      if (p0 + b * nthr < cnt) r[b] = recs[start + p0 + b * nthr];
+#pragma unroll
+    for (int b = 0; b < BT; ++b) {
+      const int p = p0 + b * nthr;
+      if (p >= cnt) break;
+      int c0, c1, c2;
+      unpack_cell(2, r[b].cell, c0, c1, c2);
+      T u;
+      const int l0 = c0 - org0 + es_start<W, T>(r[b].f[0], u) + PAD;
+      const int l1 = c1 - org1 + es_start<W, T>(r[b].f[1], u) + PAD;
+      const int cls = (l1 * TW + l0) & (G - 1);
+      code[p] = uint16_t((cls << 12) | atomicAdd(&cls_count[cls], 1));
+    }
   }
   __syncthreads();
   if (tid == 0) {

@@ -122,22 +122,28 @@ __global__ void __launch_bounds__(256) nuwu_modes_kernel(
 // their own named barriers.
 // ---------------------------------------------------------------------------
 
+// The rows are zeroed once read: the next evaluation spreads into a clean grid
+// without a separate memset.
 template <typename T, int N>
-__global__ void __launch_bounds__(N / 8) band_rows_r2c_kernel(const T* __restrict__ grid,
-                                                               const cplx_t<T>* __restrict__ tw, int KB,
-                                                               cplx_t<T>* __restrict__ band1) {
+__global__ void __launch_bounds__(N / 8) band_rows_r2c_kernel(T* __restrict__ grid, const cplx_t<T>* __restrict__ tw,
+                                                               int KB, cplx_t<T>* __restrict__ band1) {
   using F = RegFft<T, N>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx_t<T>* buf = reinterpret_cast<cplx_t<T>*>(smem_raw) + threadIdx.y * fft_padded(N);
   const int t = threadIdx.x;
   const int64_t y = 2 * (2 * int64_t(blockIdx.x) + threadIdx.y);
-  const T* ra = grid + y * N;
-  const T* rb = ra + N;
+  T* ra = grid + y * N;
+  T* rb = ra + N;
   cplx_t<T> v[F::E];
 #pragma unroll
   for (int j = 0; j < F::E; ++j) {
     v[j].x = ra[t + j * (N / F::E)];
     v[j].y = rb[t + j * (N / F::E)];
+  }
+#pragma unroll
+  for (int j = 0; j < F::E; ++j) {
+    ra[t + j * (N / F::E)] = T(0);
+    rb[t + j * (N / F::E)] = T(0);
   }
   F::run(v, buf, tw, t, 1 + threadIdx.y);
   // A(k) = (Z(k) + conj Z(-k)) / 2, B(k) = (Z(k) - conj Z(-k)) / (2i)
@@ -433,8 +439,10 @@ class NUwUImpl final : public Potential {
     for (int a = 0; a < D; ++a) mp.L[a] = L_[a];
     bin_sort<T>(x, N_, mp, geom_, sort_, recs_.p, status_.p, s);
     timer_mark("sort", s);
-    FB_CUDA(cudaMemsetAsync(spread_grid_.p, 0, spread_grid_.bytes(), s));
-    timer_mark("zero_grid", s);
+    if (!band_) {  // the band row transform leaves the grid zeroed for the next evaluation
+      FB_CUDA(cudaMemsetAsync(spread_grid_.p, 0, spread_grid_.bytes(), s));
+      timer_mark("zero_grid", s);
+    }
     spread_real<T>(recs_.p, cw_.p, uniform_c_, sort_, geom_, poly_, spread_grid_.p, s);
     timer_mark("spread", s);
     if (band_) {
@@ -538,6 +546,7 @@ class NUwUImpl final : public Potential {
       case 4096: band_attrs<4096>(); break;
       default: band_attrs<8192>(); break;
     }
+    FB_CUDA(cudaMemset(spread_grid_.p, 0, spread_grid_.bytes()));
     band_ = true;
   }
 
