@@ -71,6 +71,8 @@ void alloc_sort(SortBufs& sb, int64_t N, const Geom& g) {
   sb.sub_count.alloc(sb.max_sub);
   sb.num_sub.alloc(1);
   sb.unsorted.alloc(std::max<int64_t>(N, 1) * 32);  // the largest record is 32 bytes
+  sb.done.alloc(1);
+  FB_CUDA(cudaMemset(sb.done.p, 0, sizeof(unsigned)));
 }
 
 }  // namespace fb

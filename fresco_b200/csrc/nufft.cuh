@@ -55,6 +55,7 @@ struct MapParams {
   double L[3] = {1, 1, 1};
   int stride = 2;  // doubles between consecutive points (interleaved layout)
   double scale[3] = {1, 1, 1};  // fine-grid cells per unit length, nf / L (set by the sort)
+  double invL[3] = {1, 1, 1};   // 1 / L (set by the sort)
 };
 
 // Packed sorted-point records (16 or 32 bytes, read with one vector load).
@@ -79,6 +80,7 @@ struct SortBufs {
   DevBuf<int> bin_start; // nbins + 1: first record of each bin
   DevBuf<int> sub_bin, sub_start, sub_count, num_sub;
   DevBuf<unsigned char> unsorted;  // N records in input order (written by the counting pass)
+  DevBuf<unsigned> done;           // blocks of the scattering pass that finished (reset by the last one)
   int64_t max_sub = 0;
 };
 

@@ -36,8 +36,20 @@ __device__ __forceinline__ int wrap_index(int x, int n) {
 // (or p): one multiplication instead of the reference's divide-and-rescale
 // chain, within a few ulp of it.  round(p/L) keeps the exact division, so a
 // coordinate on a half period rounds as in the reference.
+// round(p / L): the quotient is formed with the reciprocal, which is within an
+// ulp of p / L and so rounds the same way unless p / L lies within 1e-9 of a
+// half-integer; there the exact division decides.
+static __device__ __noinline__ double round_exact_quotient(double p, double L) { return round(p / L); }
+
+__device__ __forceinline__ double round_quotient(double p, double L, double invL) {
+  const double q = p * invL;
+  const double fr = q - floor(q);
+  if (fabs(fr - 0.5) < 1e-9) return round_exact_quotient(p, L);  // rare: a call, never speculated
+  return round(q);
+}
+
 __device__ __forceinline__ bool map_coord(double p, const MapParams& mp, int nf, int a, int& c, double& f) {
-  const double t = mp.kind == 0 ? p - round(p / mp.L[a]) : p;
+  const double t = mp.kind == 0 ? p - round_quotient(p, mp.L[a], mp.invL[a]) : p;
   double u = t * mp.scale[a];
   if (!(fabs(u) < 1.0e9)) {
     if (!isfinite(u)) {
@@ -162,61 +174,64 @@ __global__ void __launch_bounds__(kSortThreads) sort_count_kernel(const double* 
   }
 }
 
-// Sort pass 2 (one block of 1024 threads): bin starts (exclusive scan of the
-// bin totals), the subproblem table (each bin cut into chunks of at most
-// kMaxSub points), and bin_total cleared for the next sort.
-static __global__ void __launch_bounds__(1024) sort_plan_kernel(int nbins, int* bin_total, int* bin_start,
-                                                                int* sub_bin, int* sub_start, int* sub_count,
-                                                                int* num_sub, int max_sub) {
+// Sort pass 2: every block scans the bin totals itself (bin starts), block 0
+// also publishes them and the subproblem table (each bin cut into chunks of
+// at most kMaxSub points); then each block hands out the slots of its
+// segments with shared-memory cursors (the counts are those of pass 1, so
+// every slot is written exactly once) and moves its records there.  The last
+// block to finish clears bin_total for the next sort.
+template <int D, typename T>
+__global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(
+    const Rec<D, T>* __restrict__ unsorted, int64_t N, int64_t chunk, Geom g, int* bin_total,
+    const int* __restrict__ blk_off, int* bin_start, int* sub_bin, int* sub_start, int* sub_count, int* num_sub,
+    int max_sub, unsigned* done, Rec<D, T>* out, int* status) {
+  extern __shared__ int sh_cur[];
   __shared__ int s_warp[32];
+  __shared__ bool s_last;
+  const int nbins = int(g.nbins());
+  const int tid = threadIdx.x;
+  const int* my_off = blk_off + int64_t(blockIdx.x) * nbins;
   const int per = (nbins + int(blockDim.x) - 1) / int(blockDim.x);
-  const int b0 = min(nbins, int(threadIdx.x) * per), b1 = min(nbins, b0 + per);
+  const int b0 = min(nbins, tid * per), b1 = min(nbins, b0 + per);
   int npts = 0, nsub = 0;
   for (int b = b0; b < b1; ++b) {
     const int c = bin_total[b];
     npts += c;
     nsub += (c + kMaxSub - 1) / kMaxSub;
   }
-  int tot_pts, tot_sub;
-  int start = block_exclusive_scan(npts, &tot_pts, s_warp);
-  int sbase = block_exclusive_scan(nsub, &tot_sub, s_warp);
+  int tot_pts;
+  int run = block_exclusive_scan(npts, &tot_pts, s_warp);
+  const int first_start = run;  // start of bin b0
+  // bins this block has no points in get stale offsets that are never used
   for (int b = b0; b < b1; ++b) {
-    const int c = bin_total[b];
-    bin_start[b] = start;
-    bin_total[b] = 0;
-    for (int q = 0; q * kMaxSub < c; ++q) {
-      if (sbase < max_sub) {
-        sub_bin[sbase] = b;
-        sub_start[sbase] = start + q * kMaxSub;
-        sub_count[sbase] = min(kMaxSub, c - q * kMaxSub);
+    sh_cur[b] = run + my_off[b];
+    if (blockIdx.x == 0) bin_start[b] = run;
+    run += bin_total[b];
+  }
+  if (blockIdx.x == 0) {
+    int tot_sub;
+    int sbase = block_exclusive_scan(nsub, &tot_sub, s_warp);
+    int st = first_start;
+    for (int b = b0; b < b1; ++b) {
+      const int c = bin_total[b];
+      for (int q = 0; q * kMaxSub < c; ++q) {
+        if (sbase < max_sub) {
+          sub_bin[sbase] = b;
+          sub_start[sbase] = st + q * kMaxSub;
+          sub_count[sbase] = min(kMaxSub, c - q * kMaxSub);
+        }
+        ++sbase;
       }
-      ++sbase;
+      st += c;
     }
-    start += c;
+    if (tid == 0) {
+      bin_start[nbins] = tot_pts;
+      *num_sub = min(tot_sub, max_sub);
+    }
   }
-  if (threadIdx.x == 0) {
-    bin_start[nbins] = tot_pts;
-    *num_sub = min(tot_sub, max_sub);
-  }
-}
-
-// Sort pass 3: each block hands out the slots of its segments again with
-// shared-memory cursors (the counts are those of pass 1, so every slot is
-// written exactly once) and moves its records there.
-template <int D, typename T>
-__global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(const Rec<D, T>* __restrict__ unsorted, int64_t N,
-                                                                    int64_t chunk, Geom g,
-                                                                    const int* __restrict__ bin_start,
-                                                                    const int* __restrict__ blk_off, Rec<D, T>* out,
-                                                                    int* status) {
-  extern __shared__ int sh_cur[];
-  const int nbins = int(g.nbins());
-  const int* my_off = blk_off + int64_t(blockIdx.x) * nbins;
-  // bins this block has no points in hold stale offsets that are never used
-  for (int i = threadIdx.x; i < nbins; i += blockDim.x) sh_cur[i] = bin_start[i] + my_off[i];
   __syncthreads();
   const int64_t j0 = int64_t(blockIdx.x) * chunk, j1 = min(N, j0 + chunk);
-  for (int64_t jb = j0 + threadIdx.x; jb < j1; jb += kSortBatch * int64_t(blockDim.x)) {
+  for (int64_t jb = j0 + tid; jb < j1; jb += kSortBatch * int64_t(blockDim.x)) {
     Rec<D, T> r[kSortBatch];
 #pragma unroll
     for (int u = 0; u < kSortBatch; ++u) {
@@ -235,6 +250,17 @@ __global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(const Rec<D,
       }
       out[dest] = r[u];
     }
+  }
+  // every block has read bin_total before it counts itself done
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    for (int b = tid; b < nbins; b += blockDim.x) bin_total[b] = 0;
+    if (tid == 0) *done = 0u;
   }
 }
 
@@ -862,7 +888,10 @@ void bin_sort_d(const double* pts, int64_t N, const MapParams& mp, const Geom& g
   auto k1 = sort_count_kernel<D, T>;
   auto k3 = sort_scatter_kernel<D, T>;
   MapParams m2 = mp;
-  for (int a = 0; a < D; ++a) m2.scale[a] = double(g.nf[a]) / mp.L[a];
+  for (int a = 0; a < D; ++a) {
+    m2.scale[a] = double(g.nf[a]) / mp.L[a];
+    m2.invL[a] = 1.0 / mp.L[a];
+  }
   Rec<D, T>* unsorted = reinterpret_cast<Rec<D, T>*>(sb.unsorted.p);
   if (smem > 48 * 1024) {
     FB_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
@@ -872,14 +901,10 @@ void bin_sort_d(const double* pts, int64_t N, const MapParams& mp, const Geom& g
     k1<<<sb.NB, kSortThreads, smem, s>>>(pts, N, sb.chunk, m2, g, sb.bin_total.p, sb.blk_off.p, unsorted, status);
     FB_LAUNCH_CHECK();
   }
-  sort_plan_kernel<<<1, 1024, 0, s>>>(nbins, sb.bin_total.p, sb.bin_start.p, sb.sub_bin.p, sb.sub_start.p,
-                                      sb.sub_count.p, sb.num_sub.p, int(sb.max_sub));
+  k3<<<sb.NB, kSortThreads, smem, s>>>(unsorted, N, sb.chunk, g, sb.bin_total.p, sb.blk_off.p, sb.bin_start.p,
+                                       sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, int(sb.max_sub),
+                                       sb.done.p, static_cast<Rec<D, T>*>(recs), status);
   FB_LAUNCH_CHECK();
-  if (N > 0) {
-    k3<<<sb.NB, kSortThreads, smem, s>>>(unsorted, N, sb.chunk, g, sb.bin_start.p, sb.blk_off.p,
-                                         static_cast<Rec<D, T>*>(recs), status);
-    FB_LAUNCH_CHECK();
-  }
 }
 
 template <typename T>
