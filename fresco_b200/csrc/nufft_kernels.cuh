@@ -135,7 +135,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total, int* s_wa
 // memory; one global atomic per non-empty bin then reserves the block's
 // segment inside that bin (blk_off, block-major).
 template <int D, typename T>
-__global__ void __launch_bounds__(kSortThreads) sort_count_kernel(const double* __restrict__ pts, int64_t N,
+__global__ void __launch_bounds__(kSortThreads, 2) sort_count_kernel(const double* __restrict__ pts, int64_t N,
                                                                   int64_t chunk, MapParams mp, Geom g, int* bin_total,
                                                                   int* blk_off, Rec<D, T>* unsorted, int* status) {
   extern __shared__ int sh_hist[];
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_count_kernel(const double* 
 // every slot is written exactly once) and moves its records there.  The last
 // block to finish clears bin_total for the next sort.
 template <int D, typename T>
-__global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(
+__global__ void __launch_bounds__(kSortThreads, 2) sort_scatter_kernel(
     const Rec<D, T>* __restrict__ unsorted, int64_t N, int64_t chunk, Geom g, int* bin_total,
     const int* __restrict__ blk_off, int* bin_start, int* sub_bin, int* sub_start, int* sub_count, int* num_sub,
     int max_sub, unsigned* done, Rec<D, T>* out, int* status) {

@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(N / 8) band_modes_kernel(
 }
 
 template <typename T, int N>
-__global__ void __launch_bounds__(N / 8) band_rows_c2c_kernel(const cplx_t<T>* __restrict__ band2, int Kx,
+__global__ void __launch_bounds__(N / 8, sizeof(T) == 4 ? 3 : 2) band_rows_c2c_kernel(const cplx_t<T>* __restrict__ band2, int Kx,
                                                                const cplx_t<T>* __restrict__ tw,
                                                                cplx_t<T>* __restrict__ out) {
   using F = RegFft<T, N>;
