@@ -105,7 +105,8 @@ class Clocks:
 
 
 def algorithmic_bytes(geom_nf, n_active, N, s_r, s_c, s_w, d=2, d_f=2):
-    """Per-eval algorithmic bytes (SURVEY 8(d) formula) and per-kernel figures."""
+    """Per-eval algorithmic bytes of the loss-and-gradient path (each array read or written once) and the
+    per-stage figures: points N, fine grid G = nf^2, real/complex/weight sizes s_r, s_c, s_w."""
     G = geom_nf * geom_nf
     n_modes = (2 * K_MODES + 1) ** 2
     b_points = N * (4 * d * s_r + 12)
@@ -256,10 +257,11 @@ def run_ours(args):
     top_ms = stage_ms.get(top, ms_per_step)
     achieved = per_kernel.get(top, b_eval) / (top_ms * 1e-3) / 1e9
     traffic = None
-    try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+    try:  # DRAM bytes per launch from an ncu capture of this workload (profiles/traffic.txt: "stage bytes")
+        with open(os.path.join(ROOT, "profiles", "traffic.txt")) as fh:
+            prof = {ln.split()[0]: int(ln.split()[1]) for ln in fh if ln.strip() and not ln.startswith("#")}
         traffic = prof.get(top)
-    except Exception:
+    except (OSError, ValueError, IndexError):
         pass
     roofline = {"kernel": top, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                 "frac": round(achieved / hbm_peak, 4), "traffic": traffic, "peak_source": peak_src,
@@ -272,8 +274,8 @@ def run_ours(args):
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(x, radii, Sk, V, L, samples=args.cpu_samples)
 
-    # kernels of ours per eval: bin_count, build_subproblems, scatter, spread, modes, interp
-    launches = 6 * args.steps
+    # kernels of ours per eval: sort count, sort scatter, spread, band row r2c, band modes, band row c2c, interp
+    launches = 7 * args.steps
     out = {
         "metric": METRIC,
         "value": round(value, 2),
