@@ -10,7 +10,7 @@ namespace fb {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;  // streaming kernels: more loads in flight per block
 
 // Sum of P block partials, the same value on every thread (fixed order).
 __device__ double sum_parts(const double* __restrict__ part, int P) {
@@ -108,7 +108,7 @@ __global__ void lb_start(const double* __restrict__ g, double* __restrict__ step
     step[i] = gi;
     v[0] += s_i[i] * gi;
   }
-  const int sl[1] = {S_OUT};
+  const int sl[1] = {S_IN};
   block_partials<1>(v, part, P, sl);
 }
 
@@ -117,10 +117,12 @@ __global__ void lb_start(const double* __restrict__ g, double* __restrict__ step
 //  forward : b = -rho_i (y_i . step); step -= (alpha_i - b) s_i
 // followed by the next dot product (dnext . step), or for the final forward
 // update the line-search dots (step . g, step . step).
+// The incoming dot product is in slot in_slot, the next one goes to out_slot
+// (the two alternate between consecutive updates).
 __global__ void lb_update(int forward, int last, double* __restrict__ step, const double* __restrict__ vec,
                           const double* __restrict__ dnext, const double* __restrict__ g, int64_t n, LbState* st,
-                          double* rho, double* alpha, int mi, double* part, int P) {
-  const double dotin = sum_parts(part + int64_t(S_IN) * P, P);
+                          double* rho, double* alpha, int mi, double* part, int P, int in_slot, int out_slot) {
+  const double dotin = sum_parts(part + int64_t(in_slot) * P, P);
   double coef;
   if (!forward) {
     coef = rho[mi] * dotin;
@@ -149,14 +151,9 @@ __global__ void lb_update(int forward, int last, double* __restrict__ step, cons
     block_partials<2>(v, part, P, sl);
   } else {
     double w[1] = {v[0]};
-    const int sl[1] = {S_OUT};
+    const int sl[1] = {out_slot};
     block_partials<1>(w, part, P, sl);
   }
-}
-
-// Moves the S_OUT partials to S_IN (between two-loop steps).
-__global__ void lb_shift(double* part, int P) {
-  for (int i = threadIdx.x; i < P; i += blockDim.x) part[int64_t(S_IN) * P + i] = part[int64_t(S_OUT) * P + i];
 }
 
 // Trial point of the backtracking line search (lbfgs.cpp:176-204).
@@ -485,9 +482,8 @@ class Lbfgs final : public Optimizer {
         const bool last = (t == m - 1);
         const int inext = last ? (jmin % M) : ((j - 1) % M);
         const double* dnext = last ? ym_.p + int64_t(inext) * n_ : sm_.p + int64_t(inext) * n_;
-        lb_shift<<<1, 256, 0, s_>>>(part_.p, P_);
         lb_update<<<P_, kThreads, 0, s_>>>(0, last, step_.p, ym_.p + int64_t(i) * n_, dnext, g, n_, st_.p, rho_.p,
-                                           alpha_.p, i, part_.p, P_);
+                                           alpha_.p, i, part_.p, P_, t % 2 ? S_OUT : S_IN, t % 2 ? S_IN : S_OUT);
       }
       for (int t = 0; t < m; ++t) {
         const int j = jmin + t;
@@ -495,9 +491,9 @@ class Lbfgs final : public Optimizer {
         const bool last = (t == m - 1);
         const int inext = (j + 1) % M;
         const double* dnext = last ? nullptr : ym_.p + int64_t(inext) * n_;
-        lb_shift<<<1, 256, 0, s_>>>(part_.p, P_);
+        const int u = m + t;  // update index over both loops
         lb_update<<<P_, kThreads, 0, s_>>>(1, last, step_.p, sm_.p + int64_t(i) * n_, dnext, g, n_, st_.p, rho_.p,
-                                           alpha_.p, i, part_.p, P_);
+                                           alpha_.p, i, part_.p, P_, u % 2 ? S_OUT : S_IN, u % 2 ? S_IN : S_OUT);
       }
     }
     FB_LAUNCH_CHECK();

@@ -5,11 +5,12 @@
 //
 // Periodic boxes with at least 3 cells per dimension use a cell list built by
 // a counting sort (cell edge >= r_cut = 2 max(r_i), inversepower_potential.
-// hpp:115), then one thread per (cell-sorted) point gathers its neighbours
-// from the 3^d surrounding cells: no atomics on the gradient, and each pair's
-// energy is counted once (by its lower original index), as in
-// EnergyGradientAccumulator::insert_atom_pair (cell_list_potential.hpp:
-// 154-181).  Smaller periodic boxes and the Cartesian distance use a tiled
+// hpp:115) into packed 32-byte point records, then one thread per
+// (cell-sorted) point gathers its neighbours from the 3^d surrounding cells;
+// the three cells of a row along x are one contiguous range of records.  No
+// atomics on the gradient, and each pair's energy is counted once (by its
+// lower original index), as in EnergyGradientAccumulator::insert_atom_pair
+// (cell_list_potential.hpp:154-181).  Smaller periodic boxes and the Cartesian distance use a tiled
 // all-pairs kernel.  Distances follow periodic_distance::get_rij
 // (distance.hpp:179-185): dr = x_i - x_j, dr -= round(dr / L) L.
 #include <algorithm>
@@ -48,134 +49,143 @@ struct Box {
   double L[3] = {1, 1, 1};
   double invL[3] = {1, 1, 1};
   int nc[3] = {1, 1, 1};
-  double cw[3] = {1, 1, 1};  // cell width
+  double cw[3] = {1, 1, 1};     // cell width
+  double inv_cw[3] = {1, 1, 1};
 };
+
+// A cell-sorted point: position, radius, original index and cell.
+template <int D>
+struct alignas(16) PairRec {
+  double x[D];
+  double r;
+  uint32_t idx;
+  int cell;
+};
+
+// Cell of a position (the same expression in the counting and the scattering
+// pass, so both agree); false for a non-finite coordinate (cell 0).
+template <int D>
+__device__ __forceinline__ bool cell_of(const double* __restrict__ p, const Box& b, int& cell) {
+  bool ok = true;
+  int stride = 1;
+  cell = 0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    const double v = p[a];
+    int c = 0;
+    if (isfinite(v)) {
+      const double u = v - floor(v * b.invL[a]) * b.L[a];
+      c = min(max(int(u * b.inv_cw[a]), 0), b.nc[a] - 1);
+    } else {
+      ok = false;
+    }
+    cell += c * stride;
+    stride *= b.nc[a];
+  }
+  return ok;
+}
 
 template <int D>
 __global__ void __launch_bounds__(kThreads) cell_count_kernel(const double* __restrict__ x, int64_t N, Box b,
                                                               int* cell_count, uint32_t* rank, int* status) {
+  bool bad = false;
   for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < N; j += int64_t(gridDim.x) * blockDim.x) {
-    int cell = 0, stride = 1;
-    bool ok = true;
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      const double v = x[j * D + a];
-      int c = 0;
-      if (isfinite(v)) {
-        double u = v - floor(v * b.invL[a]) * b.L[a];
-        c = int(u / b.cw[a]);
-        c = min(max(c, 0), b.nc[a] - 1);
-      } else {
-        ok = false;
-      }
-      cell += c * stride;
-      stride *= b.nc[a];
-    }
-    if (!ok) raise_status(status, STATUS_NONFINITE_INPUT);
+    int cell;
+    bad |= !cell_of<D>(x + j * D, b, cell);
     rank[j] = uint32_t(atomicAdd(&cell_count[cell], 1));
   }
+  if (bad) raise_status(status, STATUS_NONFINITE_INPUT);
 }
 
 template <int D>
 __global__ void __launch_bounds__(kThreads) cell_scatter_kernel(const double* __restrict__ x,
                                                                 const double* __restrict__ radii, int64_t N, Box b,
                                                                 const uint32_t* __restrict__ rank,
-                                                                const int* __restrict__ cell_start, double* sx,
-                                                                double* sr, uint32_t* sidx, int* scell) {
+                                                                const int* __restrict__ cell_start, PairRec<D>* recs) {
   for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < N; j += int64_t(gridDim.x) * blockDim.x) {
-    int cell = 0, stride = 1;
-    double p[D];
+    PairRec<D> r;
 #pragma unroll
-    for (int a = 0; a < D; ++a) {
-      const double v = x[j * D + a];
-      p[a] = v;
-      int c = 0;
-      if (isfinite(v)) {
-        double u = v - floor(v * b.invL[a]) * b.L[a];
-        c = int(u / b.cw[a]);
-        c = min(max(c, 0), b.nc[a] - 1);
-      }
-      cell += c * stride;
-      stride *= b.nc[a];
-    }
-    const int64_t dest = int64_t(cell_start[cell]) + rank[j];
-#pragma unroll
-    for (int a = 0; a < D; ++a) sx[dest * D + a] = p[a];
-    sr[dest] = radii[j];
-    sidx[dest] = uint32_t(j);
-    scell[dest] = cell;
+    for (int a = 0; a < D; ++a) r.x[a] = x[j * D + a];
+    cell_of<D>(r.x, b, r.cell);
+    r.r = radii[j];
+    r.idx = uint32_t(j);
+    recs[int64_t(cell_start[r.cell]) + rank[j]] = r;
   }
 }
 
 // One thread per cell-sorted point; neighbours from the 3^D surrounding cells.
+// cell_start has ncells + 1 entries (the last is N), so cells c..c+2 of a row
+// are the records [cell_start[c], cell_start[c + 3]).
 template <int D>
-__global__ void __launch_bounds__(kThreads) cell_pair_kernel(const double* __restrict__ sx,
-                                                             const double* __restrict__ sr,
-                                                             const uint32_t* __restrict__ sidx,
-                                                             const int* __restrict__ scell,
-                                                             const int* __restrict__ cell_start,
-                                                             const int* __restrict__ cell_count, int64_t N, Box b,
+__global__ void __launch_bounds__(kThreads) cell_pair_kernel(const PairRec<D>* __restrict__ recs,
+                                                             const int* __restrict__ cell_start, int64_t N, Box b,
                                                              double a_pow, double eps, double* grad, double* energy,
                                                              int accumulate, const int* __restrict__ status) {
   const bool bad = (*status) & STATUS_NONFINITE_INPUT;
   double e_loc = 0.0;
+  const int nc0 = b.nc[0];
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += int64_t(gridDim.x) * blockDim.x) {
-    double xi[D], gi[D];
+    const PairRec<D> me = recs[i];
+    double gi[D];
 #pragma unroll
-    for (int a = 0; a < D; ++a) {
-      xi[a] = sx[i * D + a];
-      gi[a] = 0.0;
-    }
-    const double ri = sr[i];
-    const uint32_t oi = sidx[i];
+    for (int a = 0; a < D; ++a) gi[a] = 0.0;
     int ci[3] = {0, 0, 0};
     {
-      int c = scell[i];
+      int c = me.cell;
 #pragma unroll
       for (int a = 0; a < D; ++a) {
         ci[a] = c % b.nc[a];
         c /= b.nc[a];
       }
     }
+    auto visit = [&](int s0, int s1) {
+      for (int j = s0; j < s1; ++j) {
+        if (j == int(i)) continue;
+        const PairRec<D> o = recs[j];
+        double dr[D], r2 = 0.0;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          dr[a] = min_image(me.x[a] - o.x[a], b.L[a], b.invL[a], true);
+          r2 += dr[a] * dr[a];
+        }
+        double gij;
+        const double e = pair_energy_gradient(r2, me.r + o.r, a_pow, eps, &gij);
+        if (gij != 0.0) {
+#pragma unroll
+          for (int a = 0; a < D; ++a) gi[a] -= dr[a] * gij;
+        }
+        if (o.idx > me.idx) e_loc += e;
+      }
+    };
     const int n1 = D >= 2 ? 3 : 1, n2 = D >= 3 ? 3 : 1;
     for (int o2 = 0; o2 < n2; ++o2)
-      for (int o1 = 0; o1 < n1; ++o1)
-        for (int o0 = 0; o0 < 3; ++o0) {
-          int c0 = ci[0] + o0 - 1;
-          c0 += c0 < 0 ? b.nc[0] : (c0 >= b.nc[0] ? -b.nc[0] : 0);
-          int cell = c0;
-          if (D >= 2) {
-            int c1 = ci[1] + o1 - 1;
-            c1 += c1 < 0 ? b.nc[1] : (c1 >= b.nc[1] ? -b.nc[1] : 0);
-            cell += c1 * b.nc[0];
-          }
-          if (D >= 3) {
-            int c2 = ci[2] + o2 - 1;
-            c2 += c2 < 0 ? b.nc[2] : (c2 >= b.nc[2] ? -b.nc[2] : 0);
-            cell += c2 * b.nc[0] * b.nc[1];
-          }
-          const int s0 = cell_start[cell], s1 = s0 + cell_count[cell];
-          for (int j = s0; j < s1; ++j) {
-            if (j == i) continue;
-            double dr[D], r2 = 0.0;
-#pragma unroll
-            for (int a = 0; a < D; ++a) {
-              dr[a] = min_image(xi[a] - sx[int64_t(j) * D + a], b.L[a], b.invL[a], true);
-              r2 += dr[a] * dr[a];
-            }
-            double gij;
-            const double e = pair_energy_gradient(r2, ri + sr[j], a_pow, eps, &gij);
-            if (gij != 0.0) {
-#pragma unroll
-              for (int a = 0; a < D; ++a) gi[a] -= dr[a] * gij;
-            }
-            if (sidx[j] > oi) e_loc += e;
-          }
+      for (int o1 = 0; o1 < n1; ++o1) {
+        int row = 0;
+        if (D >= 2) {
+          int c1 = ci[1] + o1 - 1;
+          c1 += c1 < 0 ? b.nc[1] : (c1 >= b.nc[1] ? -b.nc[1] : 0);
+          row = c1 * nc0;
         }
+        if (D >= 3) {
+          int c2 = ci[2] + o2 - 1;
+          c2 += c2 < 0 ? b.nc[2] : (c2 >= b.nc[2] ? -b.nc[2] : 0);
+          row += c2 * nc0 * b.nc[1];
+        }
+        const int c0 = ci[0];
+        if (c0 >= 1 && c0 <= nc0 - 2) {
+          visit(cell_start[row + c0 - 1], cell_start[row + c0 + 2]);
+        } else if (c0 == 0) {  // x wraps on the left
+          visit(cell_start[row], cell_start[row + 2]);
+          visit(cell_start[row + nc0 - 1], cell_start[row + nc0]);
+        } else {  // c0 == nc0 - 1: x wraps on the right
+          visit(cell_start[row + nc0 - 2], cell_start[row + nc0]);
+          visit(cell_start[row], cell_start[row + 1]);
+        }
+      }
     const double nan = __longlong_as_double(0x7ff8000000000000ULL);
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-      double* dst = grad + int64_t(oi) * D + a;
+      double* dst = grad + int64_t(me.idx) * D + a;
       const double v = bad ? nan : gi[a];
       *dst = accumulate ? *dst + v : v;
     }
@@ -278,11 +288,13 @@ class InversePowerImpl final : public Potential {
       // not depend on the cell size; the reference picks its own via ncellx_scale)
       const double target = std::max(1.0, std::floor(std::pow(double(std::max<int64_t>(N_, 1)), 1.0 / D)));
       for (int a = 0; a < D; ++a) {
-        int nc = rcut > 0 ? int(std::floor(box_.L[a] / rcut)) : 1;
+        // the margin keeps every cell at least r_cut wide after rounding
+        int nc = rcut > 0 ? int(std::floor(box_.L[a] / (rcut * (1.0 + 1e-9)))) : 1;
         nc = std::max(1, std::min(nc, int(target)));
         if (nc < 3) use_cells_ = false;
         box_.nc[a] = nc;
         box_.cw[a] = box_.L[a] / nc;
+        box_.inv_cw[a] = nc / box_.L[a];
         ncells *= nc;
       }
     }
@@ -291,15 +303,11 @@ class InversePowerImpl final : public Potential {
     if (N_) FB_CUDA(cudaMemcpy(radii_.p, radii.data(), sizeof(double) * N_, cudaMemcpyHostToDevice));
     if (use_cells_) {
       ncells_ = ncells;
-      cell_count_.alloc(ncells);
-      cell_start_.alloc(ncells);
-      nscan_ = int(ceil_div(ncells, 1024));
-      block_sums_.alloc(nscan_);
+      cell_count_.alloc(ncells + 1);  // the extra zero count makes cell_start[ncells] = N
+      cell_start_.alloc(ncells + 1);
+      block_sums_.alloc(scan_tmp_size(ncells + 1));
       rank_.alloc(std::max<int64_t>(N_, 1));
-      sx_.alloc(std::max<int64_t>(N_, 1) * D);
-      sr_.alloc(std::max<int64_t>(N_, 1));
-      sidx_.alloc(std::max<int64_t>(N_, 1));
-      scell_.alloc(std::max<int64_t>(N_, 1));
+      recs_.alloc(std::max<int64_t>(N_, 1));
     }
   }
 
@@ -336,15 +344,14 @@ class InversePowerImpl final : public Potential {
                                                   acc_grad ? 1 : 0, status_.p);
       FB_LAUNCH_CHECK();
     } else {
-      FB_CUDA(cudaMemsetAsync(cell_count_.p, 0, sizeof(int) * ncells_, s));
+      FB_CUDA(cudaMemsetAsync(cell_count_.p, 0, sizeof(int) * (ncells_ + 1), s));
       cell_count_kernel<D><<<grid, kThreads, 0, s>>>(x, N_, box_, cell_count_.p, rank_.p, status_.p);
-      exclusive_scan(cell_count_.p, cell_start_.p, block_sums_.p, ncells_, s);
-      cell_scatter_kernel<D><<<grid, kThreads, 0, s>>>(x, radii_.p, N_, box_, rank_.p, cell_start_.p, sx_.p, sr_.p,
-                                                       sidx_.p, scell_.p);
+      exclusive_scan(cell_count_.p, cell_start_.p, block_sums_.p, ncells_ + 1, s);
+      cell_scatter_kernel<D><<<grid, kThreads, 0, s>>>(x, radii_.p, N_, box_, rank_.p, cell_start_.p, recs_.p);
       FB_LAUNCH_CHECK();
       timer_mark("cell_sort", s);
-      cell_pair_kernel<D><<<grid, kThreads, 0, s>>>(sx_.p, sr_.p, sidx_.p, scell_.p, cell_start_.p, cell_count_.p,
-                                                    N_, box_, a_, eps_, g, e, acc_grad ? 1 : 0, status_.p);
+      cell_pair_kernel<D><<<grid, kThreads, 0, s>>>(recs_.p, cell_start_.p, N_, box_, a_, eps_, g, e,
+                                                    acc_grad ? 1 : 0, status_.p);
       FB_LAUNCH_CHECK();
     }
     nan_fill_kernel<<<grid, kThreads, 0, s>>>(status_.p, g, N_ * D, e);
@@ -358,10 +365,10 @@ class InversePowerImpl final : public Potential {
   bool use_cells_ = false;
   Box box_;
   int64_t ncells_ = 0;
-  int nscan_ = 0;
-  DevBuf<double> radii_, sx_, sr_, scratch_grad_;
-  DevBuf<int> cell_count_, cell_start_, block_sums_, scell_;
-  DevBuf<uint32_t> rank_, sidx_;
+  DevBuf<double> radii_, scratch_grad_;
+  DevBuf<int> cell_count_, cell_start_, block_sums_;
+  DevBuf<uint32_t> rank_;
+  DevBuf<PairRec<D>> recs_;
 };
 
 }  // namespace

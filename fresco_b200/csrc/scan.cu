@@ -3,43 +3,57 @@
 
 namespace fb {
 
+namespace {
+
+// Inclusive scan of v over the 1024 threads of the block (warp shuffles, then
+// the 32 warp totals); *total gets the block sum.
+__device__ __forceinline__ int block_inclusive_scan_1024(int v, int* total) {
+  __shared__ int warp_tot[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  if (lane == 31) warp_tot[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    int w = warp_tot[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    warp_tot[lane] = w;
+  }
+  __syncthreads();
+  const int r = v + (wid > 0 ? warp_tot[wid - 1] : 0);
+  *total = warp_tot[31];
+  __syncthreads();
+  return r;
+}
+
+}  // namespace
+
 __global__ void __launch_bounds__(1024) scan_block_kernel(const int* __restrict__ in, int* out, int* block_sums,
                                                           int64_t n) {
-  __shared__ int s[1024];
   const int64_t i = int64_t(blockIdx.x) * 1024 + threadIdx.x;
   const int v = i < n ? in[i] : 0;
-  s[threadIdx.x] = v;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    const int t = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
-    __syncthreads();
-    s[threadIdx.x] += t;
-    __syncthreads();
-  }
-  if (i < n) out[i] = s[threadIdx.x] - v;
-  if (threadIdx.x == 1023) block_sums[blockIdx.x] = s[1023];
+  int tot;
+  const int inc = block_inclusive_scan_1024(v, &tot);
+  if (i < n) out[i] = inc - v;
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = tot;
 }
 
 __global__ void __launch_bounds__(1024) scan_sums_kernel(int* block_sums, int nb) {
-  __shared__ int s[1024];
-  __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
+  int carry = 0;
   for (int base = 0; base < nb; base += 1024) {
     const int i = base + threadIdx.x;
     const int v = i < nb ? block_sums[i] : 0;
-    s[threadIdx.x] = v;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-      const int t = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
-      __syncthreads();
-      s[threadIdx.x] += t;
-      __syncthreads();
-    }
-    if (i < nb) block_sums[i] = carry + s[threadIdx.x] - v;
-    __syncthreads();
-    if (threadIdx.x == 1023) carry += s[1023];
-    __syncthreads();
+    int tot;
+    const int inc = block_inclusive_scan_1024(v, &tot);
+    if (i < nb) block_sums[i] = carry + inc - v;
+    carry += tot;
   }
 }
 
