@@ -14,6 +14,7 @@
 // all-pairs kernel.  Distances follow periodic_distance::get_rij
 // (distance.hpp:179-185): dr = x_i - x_j, dr -= round(dr / L) L.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -51,13 +52,17 @@ struct Box {
   int nc[3] = {1, 1, 1};
   double cw[3] = {1, 1, 1};     // cell width
   double inv_cw[3] = {1, 1, 1};
+  float Lf[3] = {1, 1, 1}, invLf[3] = {1, 1, 1};
+  float reject2 = 0.f;  // squared FP32 distance beyond which no pair can interact (r_cut with a margin)
 };
 
-// A cell-sorted point: position, radius, original index and cell.
+// A cell-sorted point (32 bytes in 2D): position, an FP32 copy of the position
+// wrapped into the box (for a cheap distance pre-check), original index (the
+// radius is read from the radius array by it) and cell.
 template <int D>
 struct alignas(16) PairRec {
   double x[D];
-  double r;
+  float xf[D];
   uint32_t idx;
   int cell;
 };
@@ -85,14 +90,25 @@ __device__ __forceinline__ bool cell_of(const double* __restrict__ p, const Box&
   return ok;
 }
 
+constexpr int kCellBatch = 4;  // points per thread per round: their loads overlap
+
 template <int D>
 __global__ void __launch_bounds__(kThreads) cell_count_kernel(const double* __restrict__ x, int64_t N, Box b,
                                                               int* cell_count, uint32_t* rank, int* status) {
   bool bad = false;
-  for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < N; j += int64_t(gridDim.x) * blockDim.x) {
-    int cell;
-    bad |= !cell_of<D>(x + j * D, b, cell);
-    rank[j] = uint32_t(atomicAdd(&cell_count[cell], 1));
+  const int64_t step = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t j0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j0 < N; j0 += kCellBatch * step) {
+    double p[kCellBatch][D];
+#pragma unroll
+    for (int u = 0; u < kCellBatch; ++u)
+#pragma unroll
+      for (int a = 0; a < D; ++a) p[u][a] = j0 + u * step < N ? x[(j0 + u * step) * D + a] : 0.0;
+    int cell[kCellBatch];
+#pragma unroll
+    for (int u = 0; u < kCellBatch; ++u) {
+      bad |= !cell_of<D>(p[u], b, cell[u]);
+      if (j0 + u * step < N) rank[j0 + u * step] = uint32_t(atomicAdd(&cell_count[cell[u]], 1));
+    }
   }
   if (bad) raise_status(status, STATUS_NONFINITE_INPUT);
 }
@@ -102,93 +118,311 @@ __global__ void __launch_bounds__(kThreads) cell_scatter_kernel(const double* __
                                                                 const double* __restrict__ radii, int64_t N, Box b,
                                                                 const uint32_t* __restrict__ rank,
                                                                 const int* __restrict__ cell_start, PairRec<D>* recs) {
-  for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < N; j += int64_t(gridDim.x) * blockDim.x) {
-    PairRec<D> r;
+  const int64_t step = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t j0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j0 < N; j0 += kCellBatch * step) {
+    PairRec<D> r[kCellBatch];
+    uint32_t rk[kCellBatch];
 #pragma unroll
-    for (int a = 0; a < D; ++a) r.x[a] = x[j * D + a];
-    cell_of<D>(r.x, b, r.cell);
-    r.r = radii[j];
-    r.idx = uint32_t(j);
-    recs[int64_t(cell_start[r.cell]) + rank[j]] = r;
+    for (int u = 0; u < kCellBatch; ++u) {
+      const int64_t j = j0 + u * step;
+      if (j < N) {
+#pragma unroll
+        for (int a = 0; a < D; ++a) r[u].x[a] = x[j * D + a];
+        rk[u] = rank[j];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kCellBatch; ++u) {
+      const int64_t j = j0 + u * step;
+      if (j >= N) break;
+      cell_of<D>(r[u].x, b, r[u].cell);
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        const double v = r[u].x[a];
+        r[u].xf[a] = isfinite(v) ? float(v - floor(v * b.invL[a]) * b.L[a]) : 0.f;
+      }
+      r[u].idx = uint32_t(j);
+      recs[int64_t(cell_start[r[u].cell]) + rk[u]] = r[u];
+    }
   }
 }
 
 // One thread per cell-sorted point; neighbours from the 3^D surrounding cells.
 // cell_start has ncells + 1 entries (the last is N), so cells c..c+2 of a row
 // are the records [cell_start[c], cell_start[c + 3]).
+//
+// Two phases per warp.  (1) Each lane scans its candidates with an FP32
+// distance test on the wrapped positions and queues the ones within reach in
+// a per-lane shared list (candidate counts differ between lanes, but this
+// test is cheap); in 2D the warp first stages the union of its lanes' ranges
+// of each neighbour row in shared memory with coalesced loads.  (2) The warp
+// evaluates all queued pairs in FP64 with every lane busy (32 pairs at a
+// time; a lane finds its pair by a search over the lanes' queue prefix sums)
+// and adds the pair force to the owner's gradient slot in shared memory.
+// Survivors beyond a full list are evaluated afterwards by a rescan of that
+// point alone.
+constexpr int kPairQueue = 16;  // queued pairs per point
+
+template <int D>
+struct PairOut {
+  double g[D];
+  double e;
+};
+
+template <int D>
+__device__ __forceinline__ PairOut<D> pair_term(const PairRec<D>& me, double my_r, const PairRec<D>& o, double o_r,
+                                                const Box& b, double a_pow, double eps) {
+  PairOut<D> out;
+  double dr[D], r2 = 0.0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    dr[a] = min_image(me.x[a] - o.x[a], b.L[a], b.invL[a], true);
+    r2 += dr[a] * dr[a];
+  }
+  double gij;
+  const double e = pair_energy_gradient(r2, my_r + o_r, a_pow, eps, &gij);
+#pragma unroll
+  for (int a = 0; a < D; ++a) out.g[a] = gij != 0.0 ? -dr[a] * gij : 0.0;
+  out.e = o.idx > me.idx ? e : 0.0;
+  return out;
+}
+
+// Radius of original point k: radii[k], or the common value when radii is null.
+__device__ __forceinline__ double radius_of(const double* __restrict__ radii, double r_uniform, uint32_t k) {
+  return radii ? radii[k] : r_uniform;
+}
+
+template <int D>
+__device__ __forceinline__ bool within_reach(const float (&a)[D], const float (&c)[D], const Box& b) {
+  float r2 = 0.f;
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    float d = a[k] - c[k];
+    d -= rintf(d * b.invLf[k]) * b.Lf[k];
+    r2 += d * d;
+  }
+  return r2 <= b.reject2;
+}
+
+// Record ranges of the 3^(D-1) neighbour rows of a cell (two ranges per row
+// when x wraps; the second is empty otherwise), in scan order.
+template <int D>
+struct RowRanges {
+  static constexpr int R = D == 1 ? 1 : (D == 2 ? 3 : 9);
+  int lo[2 * R], hi[2 * R];
+};
+
+template <int D>
+__device__ __forceinline__ RowRanges<D> row_ranges(int cell, const Box& b, const int* __restrict__ cell_start) {
+  RowRanges<D> rr;
+  int ci[3] = {0, 0, 0};
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    ci[a] = cell % b.nc[a];
+    cell /= b.nc[a];
+  }
+  const int nc0 = b.nc[0];
+#pragma unroll
+  for (int r = 0; r < RowRanges<D>::R; ++r) {
+    int row = 0;
+    if (D >= 2) {
+      int c1 = ci[1] + (r % 3) - 1;
+      c1 += c1 < 0 ? b.nc[1] : (c1 >= b.nc[1] ? -b.nc[1] : 0);
+      row = c1 * nc0;
+    }
+    if (D >= 3) {
+      int c2 = ci[2] + (r / 3) - 1;
+      c2 += c2 < 0 ? b.nc[2] : (c2 >= b.nc[2] ? -b.nc[2] : 0);
+      row += c2 * nc0 * b.nc[1];
+    }
+    const int c0 = ci[0];
+    if (c0 >= 1 && c0 <= nc0 - 2) {
+      rr.lo[2 * r] = cell_start[row + c0 - 1];
+      rr.hi[2 * r] = cell_start[row + c0 + 2];
+      rr.lo[2 * r + 1] = rr.hi[2 * r + 1] = 0;
+    } else if (c0 == 0) {  // x wraps on the left
+      rr.lo[2 * r] = cell_start[row];
+      rr.hi[2 * r] = cell_start[row + 2];
+      rr.lo[2 * r + 1] = cell_start[row + nc0 - 1];
+      rr.hi[2 * r + 1] = cell_start[row + nc0];
+    } else {  // x wraps on the right
+      rr.lo[2 * r] = cell_start[row + nc0 - 2];
+      rr.hi[2 * r] = cell_start[row + nc0];
+      rr.lo[2 * r + 1] = cell_start[row];
+      rr.hi[2 * r + 1] = cell_start[row + 1];
+    }
+  }
+  return rr;
+}
+
+// Rescan of one point whose list overflowed: evaluates its survivors from the
+// (skip)-th on, in the scan order of the first phase.
+template <int D>
+__device__ __forceinline__ PairOut<D> overflow_pairs(const PairRec<D>* __restrict__ recs, const double* __restrict__ radii,
+                                                  double r_uniform, const int* __restrict__ cell_start, int64_t i,
+                                                  const Box& b, double a_pow, double eps, int skip) {
+  PairOut<D> acc;
+#pragma unroll
+  for (int a = 0; a < D; ++a) acc.g[a] = 0.0;
+  acc.e = 0.0;
+  const PairRec<D> me = recs[i];
+  const double my_r = radius_of(radii, r_uniform, me.idx);
+  const RowRanges<D> rr = row_ranges<D>(me.cell, b, cell_start);
+  int seen = 0;
+  for (int q = 0; q < 2 * RowRanges<D>::R; ++q)
+    for (int j = rr.lo[q]; j < rr.hi[q]; ++j) {
+      if (j == int(i) || !within_reach<D>(me.xf, recs[j].xf, b)) continue;
+      if (seen++ < skip) continue;
+      const PairOut<D> t = pair_term<D>(me, my_r, recs[j], radius_of(radii, r_uniform, recs[j].idx), b, a_pow, eps);
+#pragma unroll
+      for (int a = 0; a < D; ++a) acc.g[a] += t.g[a];
+      acc.e += t.e;
+    }
+  return acc;
+}
+
 template <int D>
 __global__ void __launch_bounds__(kThreads) cell_pair_kernel(const PairRec<D>* __restrict__ recs,
+                                                             const double* __restrict__ radii, double r_uniform,
                                                              const int* __restrict__ cell_start, int64_t N, Box b,
                                                              double a_pow, double eps, double* grad, double* energy,
                                                              int accumulate, const int* __restrict__ status) {
+  constexpr int NW = kThreads / 32;
+  constexpr int kSpan = 96;  // 2D: staged records per neighbour row and warp
+  __shared__ int queue[NW][32][kPairQueue];
+  __shared__ double gsm[NW][32][D];
+  __shared__ float2 span_xf[D == 2 ? NW : 1][3][kSpan];
   const bool bad = (*status) & STATUS_NONFINITE_INPUT;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double e_loc = 0.0;
   const int nc0 = b.nc[0];
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += int64_t(gridDim.x) * blockDim.x) {
-    const PairRec<D> me = recs[i];
-    double gi[D];
+  // whole warps iterate together (the pair phase needs every lane)
+  const int64_t nwarps_total = int64_t(gridDim.x) * NW;
+  for (int64_t wbase = (int64_t(blockIdx.x) * NW + warp) * 32; wbase < N; wbase += nwarps_total * 32) {
+    const int64_t i = wbase + lane;
+    const bool active = i < N;
+    PairRec<D> me;
+    int nq = 0;
+    if (active) me = recs[i];
+    // phase 1: candidates within reach -> queue
+    bool staged = false;
+    if constexpr (D == 2) {
+      int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+      bool ok = true;
+      if (active) {
+        const int c0 = me.cell % nc0, c1 = me.cell / nc0;
+        ok = c0 >= 1 && c0 <= nc0 - 2;
+        if (ok) {
 #pragma unroll
-    for (int a = 0; a < D; ++a) gi[a] = 0.0;
-    int ci[3] = {0, 0, 0};
-    {
-      int c = me.cell;
+          for (int o1 = 0; o1 < 3; ++o1) {
+            int r1 = c1 + o1 - 1;
+            r1 += r1 < 0 ? b.nc[1] : (r1 >= b.nc[1] ? -b.nc[1] : 0);
+            lo[o1] = cell_start[r1 * nc0 + c0 - 1];
+            hi[o1] = cell_start[r1 * nc0 + c0 + 2];
+          }
+        }
+      }
+      int smin[3], smax[3];
+#pragma unroll
+      for (int o1 = 0; o1 < 3; ++o1) {
+        int mn = active && ok ? lo[o1] : INT_MAX, mx = active && ok ? hi[o1] : INT_MIN;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+          mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        }
+        smin[o1] = mn;
+        smax[o1] = mx;
+      }
+      staged = __all_sync(0xffffffffu, !active || ok) && smax[0] - smin[0] <= kSpan &&
+               smax[1] - smin[1] <= kSpan && smax[2] - smin[2] <= kSpan;
+      if (staged) {
+#pragma unroll
+        for (int o1 = 0; o1 < 3; ++o1)
+          for (int k = lane; k < smax[o1] - smin[o1]; k += 32) {
+            const PairRec<D>& rj = recs[smin[o1] + k];
+            span_xf[warp][o1][k] = make_float2(rj.xf[0], rj.xf[1]);
+          }
+        __syncwarp();
+        if (active) {
+          const float mine_f[2] = {me.xf[0], me.xf[1]};
+#pragma unroll
+          for (int o1 = 0; o1 < 3; ++o1)
+            for (int j = lo[o1]; j < hi[o1]; ++j) {
+              const float2 q = span_xf[warp][o1][j - smin[o1]];
+              const float other_f[2] = {q.x, q.y};
+              if (j != int(i) && within_reach<2>(mine_f, other_f, b)) {
+                if (nq < kPairQueue) queue[warp][lane][nq] = j;
+                ++nq;
+              }
+            }
+        }
+      }
+    }
+    if (active && !staged) {
+      const RowRanges<D> rr = row_ranges<D>(me.cell, b, cell_start);
+#pragma unroll
+      for (int q = 0; q < 2 * RowRanges<D>::R; ++q)
+        for (int j = rr.lo[q]; j < rr.hi[q]; ++j)
+          if (j != int(i) && within_reach<D>(me.xf, recs[j].xf, b)) {
+            if (nq < kPairQueue) queue[warp][lane][nq] = j;
+            ++nq;
+          }
+    }
+    // phase 2: the queued pairs, every lane busy
+    const int nql = min(nq, kPairQueue);
+#pragma unroll
+    for (int a = 0; a < D; ++a) gsm[warp][lane][a] = 0.0;
+    int inc = nql;  // inclusive prefix sum of the queue lengths
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, inc, 31);
+    const int excl = inc - nql;
+    __syncwarp();  // the queues and gradient slots are visible to the whole warp
+    for (int t0 = 0; t0 < total; t0 += 32) {
+      const int t = t0 + lane;
+      // owner of item t: the number of lanes whose inclusive prefix is <= t
+      int owner = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int pre = __shfl_sync(0xffffffffu, inc, owner + step - 1);
+        if (pre <= t) owner += step;
+      }
+      const int first = __shfl_sync(0xffffffffu, excl, owner);
+      if (t < total) {
+        const int j = queue[warp][owner][t - first];
+        const PairRec<D> mine = recs[wbase + owner];
+        const PairOut<D> po = pair_term<D>(mine, radius_of(radii, r_uniform, mine.idx), recs[j],
+                                           radius_of(radii, r_uniform, recs[j].idx), b, a_pow, eps);
+        e_loc += po.e;
+#pragma unroll
+        for (int a = 0; a < D; ++a)
+          if (po.g[a] != 0.0) atomicAdd(&gsm[warp][owner][a], po.g[a]);
+      }
+    }
+    __syncwarp();
+    if (active) {
+      double gi[D];
+#pragma unroll
+      for (int a = 0; a < D; ++a) gi[a] = gsm[warp][lane][a];
+      if (nq > kPairQueue) {  // rare: survivors beyond the list
+        const PairOut<D> extra = overflow_pairs<D>(recs, radii, r_uniform, cell_start, i, b, a_pow, eps, kPairQueue);
+#pragma unroll
+        for (int a = 0; a < D; ++a) gi[a] += extra.g[a];
+        e_loc += extra.e;
+      }
+      const double nan = __longlong_as_double(0x7ff8000000000000ULL);
 #pragma unroll
       for (int a = 0; a < D; ++a) {
-        ci[a] = c % b.nc[a];
-        c /= b.nc[a];
+        double* dst = grad + int64_t(me.idx) * D + a;
+        const double v = bad ? nan : gi[a];
+        *dst = accumulate ? *dst + v : v;
       }
     }
-    auto visit = [&](int s0, int s1) {
-      for (int j = s0; j < s1; ++j) {
-        if (j == int(i)) continue;
-        const PairRec<D> o = recs[j];
-        double dr[D], r2 = 0.0;
-#pragma unroll
-        for (int a = 0; a < D; ++a) {
-          dr[a] = min_image(me.x[a] - o.x[a], b.L[a], b.invL[a], true);
-          r2 += dr[a] * dr[a];
-        }
-        double gij;
-        const double e = pair_energy_gradient(r2, me.r + o.r, a_pow, eps, &gij);
-        if (gij != 0.0) {
-#pragma unroll
-          for (int a = 0; a < D; ++a) gi[a] -= dr[a] * gij;
-        }
-        if (o.idx > me.idx) e_loc += e;
-      }
-    };
-    const int n1 = D >= 2 ? 3 : 1, n2 = D >= 3 ? 3 : 1;
-    for (int o2 = 0; o2 < n2; ++o2)
-      for (int o1 = 0; o1 < n1; ++o1) {
-        int row = 0;
-        if (D >= 2) {
-          int c1 = ci[1] + o1 - 1;
-          c1 += c1 < 0 ? b.nc[1] : (c1 >= b.nc[1] ? -b.nc[1] : 0);
-          row = c1 * nc0;
-        }
-        if (D >= 3) {
-          int c2 = ci[2] + o2 - 1;
-          c2 += c2 < 0 ? b.nc[2] : (c2 >= b.nc[2] ? -b.nc[2] : 0);
-          row += c2 * nc0 * b.nc[1];
-        }
-        const int c0 = ci[0];
-        if (c0 >= 1 && c0 <= nc0 - 2) {
-          visit(cell_start[row + c0 - 1], cell_start[row + c0 + 2]);
-        } else if (c0 == 0) {  // x wraps on the left
-          visit(cell_start[row], cell_start[row + 2]);
-          visit(cell_start[row + nc0 - 1], cell_start[row + nc0]);
-        } else {  // c0 == nc0 - 1: x wraps on the right
-          visit(cell_start[row + nc0 - 2], cell_start[row + nc0]);
-          visit(cell_start[row], cell_start[row + 1]);
-        }
-      }
-    const double nan = __longlong_as_double(0x7ff8000000000000ULL);
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      double* dst = grad + int64_t(me.idx) * D + a;
-      const double v = bad ? nan : gi[a];
-      *dst = accumulate ? *dst + v : v;
-    }
+    __syncwarp();
   }
   block_sum_atomic(e_loc, energy);
   if (blockIdx.x == 0 && threadIdx.x == 0 && bad) atomicAdd(energy, __longlong_as_double(0x7ff8000000000000ULL));
@@ -276,6 +510,9 @@ class InversePowerImpl final : public Potential {
     if (periodic && int(boxv.size()) != D) throw InvalidArgument("box.size() must be equal to ndim");
     double rmax = 0.0;
     for (double r : radii) rmax = std::max(rmax, r);
+    // equal radii (the usual case) are passed as one value instead of gathered
+    uniform_r_ = !radii.empty() && std::all_of(radii.begin(), radii.end(), [&](double r) { return r == radii[0]; });
+    r0_ = radii.empty() ? 0.0 : radii[0];
     const double rcut = 2.0 * rmax;  // inversepower_potential.hpp:115
     use_cells_ = periodic;
     int64_t ncells = 1;
@@ -295,9 +532,15 @@ class InversePowerImpl final : public Potential {
         box_.nc[a] = nc;
         box_.cw[a] = box_.L[a] / nc;
         box_.inv_cw[a] = nc / box_.L[a];
+        box_.Lf[a] = float(box_.L[a]);
+        box_.invLf[a] = float(box_.invL[a]);
         ncells *= nc;
       }
     }
+    // FP32 positions (wrapped into the box) are within a few ulp of the exact
+    // ones; a 0.1% margin on r_cut never rejects an interacting pair
+    const double rej = rcut * (1.0 + 1e-3) + 1e-6 * std::max({box_.L[0], box_.L[1], box_.L[2]});
+    box_.reject2 = float(rej * rej);
     radii_.alloc(std::max<int64_t>(N_, 1));
     scratch_grad_.alloc(std::max<int64_t>(N_ * D, 1));
     if (N_) FB_CUDA(cudaMemcpy(radii_.p, radii.data(), sizeof(double) * N_, cudaMemcpyHostToDevice));
@@ -350,7 +593,8 @@ class InversePowerImpl final : public Potential {
       cell_scatter_kernel<D><<<grid, kThreads, 0, s>>>(x, radii_.p, N_, box_, rank_.p, cell_start_.p, recs_.p);
       FB_LAUNCH_CHECK();
       timer_mark("cell_sort", s);
-      cell_pair_kernel<D><<<grid, kThreads, 0, s>>>(recs_.p, cell_start_.p, N_, box_, a_, eps_, g, e,
+      cell_pair_kernel<D><<<grid, kThreads, 0, s>>>(recs_.p, uniform_r_ ? nullptr : radii_.p, r0_, cell_start_.p, N_,
+                                                    box_, a_, eps_, g, e,
                                                     acc_grad ? 1 : 0, status_.p);
       FB_LAUNCH_CHECK();
     }
@@ -365,6 +609,8 @@ class InversePowerImpl final : public Potential {
   bool use_cells_ = false;
   Box box_;
   int64_t ncells_ = 0;
+  bool uniform_r_ = false;
+  double r0_ = 0.0;
   DevBuf<double> radii_, scratch_grad_;
   DevBuf<int> cell_count_, cell_start_, block_sums_;
   DevBuf<uint32_t> rank_;

@@ -46,13 +46,17 @@ def test_known_answers_small_box():
         assert rel(g, g0) < 1e-12
 
 
-@pytest.mark.parametrize("N,box,a", [(5000, 20.0, 2.0), (3000, 12.0, 2.5), (200, 2.0, 2.0)])
-def test_random_configurations(N, box, a):
+@pytest.mark.parametrize("N,box,a,equal", [(5000, 20.0, 2.0, False), (3000, 12.0, 2.5, False), (200, 2.0, 2.0, False),
+                                           (20000, 40.0, 2.0, True), (4096, 3.0, 2.0, True)])
+def test_random_configurations(N, box, a, equal):
+    """Polydisperse radii (gathered per pair) and equal radii (one value), dense and dilute."""
     from fresco_b200 import InversePower
 
     rng = np.random.default_rng(N)
     x = rng.random(2 * N) * box * 1.5 - 0.25 * box  # some points outside the box
-    radii = 0.2 * (0.7 + 0.6 * rng.random(N))
+    radii = np.full(N, 0.17) if equal else 0.2 * (0.7 + 0.6 * rng.random(N))
+    if equal and box < 10:
+        radii = np.full(N, 0.25 / np.sqrt(N) * box)  # the benchmark's packing
     p = InversePower(a, 1.0, radii, np.full(2, box), use_cell_lists=True)
     e, g = p.get_energy_gradient(x)
     e0, g0 = O.InversePower(a, 1.0, radii, np.full(2, box)).get_energy_gradient(x)
