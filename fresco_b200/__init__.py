@@ -15,19 +15,21 @@ import sys
 import types
 
 from . import _lib  # noqa: F401  (loads the CUDA library; raises ImportError if missing)
-from . import optimize, potentials
+from . import optimize, potentials, utils
 from .potentials import CombinedPotential, InversePower, NUwNU, NUwU, UwNU, UwU
 
-__all__ = ["potentials", "optimize", "install_alias", "NUwU", "UwU", "UwNU", "NUwNU", "InversePower",
+__all__ = ["potentials", "optimize", "utils", "install_alias", "NUwU", "UwU", "UwNU", "NUwNU", "InversePower",
            "CombinedPotential"]
 
 
 def install_alias() -> None:
-    """Makes ``import fresco.potentials`` / ``fresco.optimize`` resolve to this package."""
+    """Makes ``import fresco.potentials`` / ``fresco.optimize`` / ``fresco.utils`` resolve to this package."""
     pkg = types.ModuleType("fresco")
     pkg.__path__ = []  # namespace-like
     pkg.potentials = potentials
     pkg.optimize = optimize
+    pkg.utils = utils
     sys.modules.setdefault("fresco", pkg)
     sys.modules.setdefault("fresco.potentials", potentials)
     sys.modules.setdefault("fresco.optimize", optimize)
+    sys.modules.setdefault("fresco.utils", utils)

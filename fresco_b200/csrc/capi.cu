@@ -229,6 +229,15 @@ int fresco_nuwnu_energy_gradient_noalloc(const double* d_x, int64_t n_points, in
   });
 }
 
+int fresco_export_structure(const double* x, int64_t n_points, int ndim, const double* L, int Nk, const double* radii,
+                            double tol, double* sk, double* gr, double* s_radial, double* g_radial) {
+  return guarded([&] {
+    if (!x || !L || !sk || !gr || !s_radial || !g_radial) throw fb::InvalidArgument("null argument");
+    fb::export_structure(x, n_points, ndim, L, Nk, radii, tol, sk, gr, s_radial, g_radial);
+    return FRESCO_OK;
+  });
+}
+
 int fresco_potential_status(fresco_potential p, void* stream, int* status) {
   return guarded([&] {
     if (!p || !status) throw fb::InvalidArgument("null argument");

@@ -127,6 +127,12 @@ PotentialPtr make_uwnu(const std::vector<int>& grid, const std::vector<double>& 
 PotentialPtr make_nuwnu(const std::vector<double>& radii, const std::vector<double>& kpts,
                         const std::vector<double>& sk, const std::vector<double>& v, const std::vector<double>& L,
                         double eps, int precision);
+// fresco.utils.export_structure on the device (host arrays in and out):
+// sk_out and gr_out hold Nk^ndim values in centred order, s_radial and g_radial
+// Nk/2 + 1 radial averages.
+void export_structure(const double* x, int64_t n_points, int ndim, const double* L, int Nk, const double* radii,
+                      double tol, double* sk_out, double* gr_out, double* s_radial, double* g_radial);
+
 // NUwNU loss and gradient from caller-owned device arrays with no device
 // allocation; the per-k-point sums use a fixed static device array, so n_k is
 // limited to nuwnu_noalloc_max_kpoints().

@@ -147,6 +147,14 @@ int fresco_nuwnu_energy_gradient_noalloc(const double* d_x, int64_t n_points, in
                                          const double* L, int gradient_mode, double* d_grad, double* d_energy,
                                          int accumulate, void* stream);
 
+/* fresco.utils.export_structure(r, L, Nk, radii, tol) (fresco/utils/utils.py:16-52) with
+ * radial_profile (utils.py:138-152), computed on the device.  Host arrays: x holds
+ * n_points*ndim coordinates, L ndim box lengths, radii n_points values or NULL; sk and gr
+ * receive Nk^ndim values (S(k) and g(r) in centred order, dimension 0 slowest),
+ * s_radial and g_radial Nk/2 + 1 radial averages.  ndim is 2 or 3.  Synchronous. */
+int fresco_export_structure(const double* x, int64_t n_points, int ndim, const double* L, int Nk, const double* radii,
+                            double tol, double* sk, double* gr, double* s_radial, double* g_radial);
+
 /* Sticky status bits raised since the last call (1: non-finite input).
  * Synchronises `stream`.  No reference counterpart (FINUFFT's return codes
  * are ignored at source/fresco/nuwu.hpp:191-192, 256-258). */

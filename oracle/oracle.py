@@ -618,3 +618,51 @@ def stealthy_nuwu_inputs(N, K, kmax, ndim=2, seed=1, L=None, radius=1.0):
     Sk = np.zeros_like(V)
     radii = np.full(N, radius)
     return x, radii, Sk, V, L
+
+
+# ---------------------------------------------------------------------------
+# structure measurement (fresco/utils/utils.py:16-52, 138-152), exact sums
+# ---------------------------------------------------------------------------
+
+def radial_profile(data, center=None):
+    """utils.py:138-152: mean over integer radii int(|idx - center|), radii > R = shape[0]/2 pooled and dropped."""
+    data = np.asarray(data)
+    ndim = data.ndim
+    R = int(data.shape[0] / 2)
+    if center is None:
+        center = np.array(data.shape) / 2
+    center = np.asarray(center)
+    for _ in range(ndim):
+        center = np.expand_dims(center, axis=-1)
+    idx = np.indices(data.shape)
+    r = np.sqrt(np.sum((idx - center) ** 2, axis=0)).astype(int)
+    r = np.where(r <= R, r, R + 1)
+    tbin = np.bincount(r.ravel(), data.ravel())
+    nr = np.bincount(r.ravel())
+    return np.unique(r).ravel()[:-1], (tbin / nr)[:-1]
+
+
+def export_structure(r, L, Nk=1001, radii=None):
+    """utils.py:16-52 with the type-1 transform as an exact sum (finufft.nufft{2,3}d1, isign +1)."""
+    ndim = len(L)
+    LL = np.asarray(L, dtype=np.float64).reshape(1, -1)
+    rr = np.array(r, dtype=np.float64).reshape(-1, ndim) / LL
+    if np.amax(rr) > 1:
+        rr -= 0.5
+    rr *= TWO_PI
+    N = rr.shape[0]
+    if radii is None:
+        c = np.ones(N)
+    else:
+        radii = np.asarray(radii, dtype=np.float64)
+        c = np.pi * radii ** 2 if ndim == 2 else 4.0 / 3.0 * np.pi * radii ** 3
+        c = c * (N / np.sum(c))
+    f = nudft1([rr[:, a] for a in range(ndim)], c, [Nk] * ndim, +1)
+    rho = f.reshape((Nk,) * ndim).transpose(tuple(range(ndim))[::-1])  # -> [k0, k1, (k2)]
+    Sk = np.abs(rho) ** 2 / N
+    gr = np.fft.ifftn(np.fft.ifftshift(Sk) - 1.0, (Nk,) * ndim)
+    gr = np.real(np.fft.fftshift(gr)) * (Nk ** ndim) * np.prod(L) / N
+    center = int(Nk / 2)
+    q, S = radial_profile(Sk, center=[center] * ndim)
+    rq, g = radial_profile(gr, center=[center] * ndim)
+    return q, S, Sk, rq / Nk, g, gr

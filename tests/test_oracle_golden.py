@@ -121,3 +121,17 @@ def test_fire_one_iteration_without_run_keeps_zero_state():
         opt.one_iteration()
     assert opt.f == 0.0 and opt.rms == 1e10 and opt.nfev == 3
     assert np.array_equal(opt.x, d["x"])
+
+
+def test_radial_profile_small_case():
+    """The oracle's radial_profile against a hand count (centre at index shape/2, R = shape/2).  The
+    reference drops its last bin, meant to be the one beyond R: on a 4 x 4 grid no cell lies beyond R,
+    so the last real bin (r = 2) is dropped; on 8 x 8 the corners lie beyond R and r = 0..4 remain."""
+    for n, kept in [(4, 2), (8, 5)]:
+        data = np.arange(float(n * n)).reshape(n, n)
+        q, prof = O.radial_profile(data, center=[n // 2, n // 2])
+        idx = np.indices((n, n))
+        r = np.sqrt((idx[0] - n // 2) ** 2 + (idx[1] - n // 2) ** 2).astype(int)
+        expect = [data[r == k].mean() for k in range(kept)]
+        np.testing.assert_array_equal(q, np.arange(kept))
+        np.testing.assert_allclose(prof, expect)
