@@ -15,11 +15,12 @@ import sys
 import types
 
 from . import _lib  # noqa: F401  (loads the CUDA library; raises ImportError if missing)
-from . import optimize, potentials, utils
+from . import ensemble, optimize, potentials, utils
+from .ensemble import EnsembleLBFGS, NUwUEnsemble
 from .potentials import CombinedPotential, InversePower, NUwNU, NUwU, UwNU, UwU
 
-__all__ = ["potentials", "optimize", "utils", "install_alias", "NUwU", "UwU", "UwNU", "NUwNU", "InversePower",
-           "CombinedPotential"]
+__all__ = ["potentials", "optimize", "utils", "ensemble", "install_alias", "NUwU", "UwU", "UwNU", "NUwNU",
+           "InversePower", "CombinedPotential", "NUwUEnsemble", "EnsembleLBFGS"]
 
 
 def install_alias() -> None:

@@ -70,6 +70,24 @@ _SIGNATURES = {
                                              c_int_p, c_int_p, c_double_p]),
     "fresco_optimizer_device_state": (C.c_int, [handle_t, C.POINTER(c_void_p), C.POINTER(c_void_p)]),
     "fresco_optimizer_destroy": (None, [handle_t]),
+    "fresco_nuwu_ensemble_create": (C.c_int, [C.c_int, C.POINTER(c_int64), c_double_p, C.POINTER(c_int64), c_double_p,
+                                              c_double_p, c_double_p, C.c_int, C.c_double, C.c_int,
+                                              C.POINTER(handle_t)]),
+    "fresco_ensemble_info": (C.c_int, [handle_t, c_int_p, C.POINTER(c_int64), C.POINTER(c_int64)]),
+    "fresco_ensemble_energy_gradient": (C.c_int, [handle_t, c_double_p, c_int64, c_double_p, c_double_p]),
+    "fresco_ensemble_energy_gradient_device": (C.c_int, [handle_t, c_void_p, c_int64, c_void_p, c_void_p, c_void_p]),
+    "fresco_ensemble_tune": (C.c_int, [handle_t, c_double_p, c_int64]),
+    "fresco_ensemble_set_split": (C.c_int, [handle_t, C.c_double]),
+    "fresco_ensemble_status": (C.c_int, [handle_t, c_int_p]),
+    "fresco_ensemble_describe": (C.c_int, [handle_t, C.c_char_p, C.c_int]),
+    "fresco_ensemble_destroy": (None, [handle_t]),
+    "fresco_ensemble_lbfgs_create": (C.c_int, [handle_t, c_double_p, c_int64, C.c_double, C.c_int, C.c_double,
+                                               C.c_double, C.c_double, C.c_int, C.POINTER(handle_t)]),
+    "fresco_ensemble_lbfgs_run": (C.c_int, [handle_t, C.c_int, c_int_p]),
+    "fresco_ensemble_lbfgs_steps": (C.c_int, [handle_t, C.c_int]),
+    "fresco_ensemble_lbfgs_state": (C.c_int, [handle_t, c_double_p, c_double_p, c_double_p, c_double_p, c_int_p,
+                                              c_int_p, c_int_p]),
+    "fresco_ensemble_lbfgs_destroy": (None, [handle_t]),
 }
 
 

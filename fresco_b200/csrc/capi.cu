@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "../../include/fresco_b200.h"
+#include "ensemble.cuh"
 #include "optimizer.cuh"
 #include "potential.cuh"
 
@@ -18,6 +19,16 @@ struct fresco_potential_s {
 struct fresco_optimizer_s {
   std::unique_ptr<fb::Optimizer> opt;
   fresco_potential_s* pot = nullptr;  // borrowed; the Python layer keeps it alive
+};
+
+struct fresco_ensemble_s {
+  fb::EnsemblePtr ens;
+  cudaStream_t stream = nullptr;
+  fb::DevBuf<double> dx, dg, de;
+};
+
+struct fresco_ensemble_lbfgs_s {
+  std::unique_ptr<fb::EnsembleLbfgs> opt;
 };
 
 namespace {
@@ -415,5 +426,177 @@ int fresco_optimizer_device_state(fresco_optimizer o, double** d_x, double** d_g
 }
 
 void fresco_optimizer_destroy(fresco_optimizer o) { delete o; }
+
+
+// ---- batched ensembles -----------------------------------------------------
+
+int fresco_nuwu_ensemble_create(int n_patterns, const int64_t* n_points, const double* radii, const int64_t* n_modes,
+                                const double* sk, const double* v, const double* L, int ndim, double eps,
+                                int precision, fresco_ensemble* out) {
+  return guarded([&] {
+    if (!out || !n_points || !radii || !n_modes || !sk || !v || !L) throw fb::InvalidArgument("null argument");
+    if (n_patterns < 1) throw fb::InvalidArgument("an ensemble needs at least one pattern");
+    if (precision != 0 && precision != 1) throw fb::InvalidArgument("precision must be 0 (fp64) or 1 (fp32)");
+    for (int p = 0; p < n_patterns; ++p)
+      if (n_points[p] < 1 || n_modes[p] < 1) throw fb::InvalidArgument("empty pattern or mode grid");
+    auto* h = new fresco_ensemble_s;
+    try {
+      h->ens = fb::make_nuwu_ensemble(n_patterns, n_points, radii, n_modes, sk, v, L, ndim, eps, precision);
+      FB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    return FRESCO_OK;
+  });
+}
+
+int fresco_ensemble_info(fresco_ensemble h, int* n_patterns, int64_t* ndof, int64_t* offsets) {
+  return guarded([&] {
+    if (!h) throw fb::InvalidArgument("null argument");
+    if (n_patterns) *n_patterns = h->ens->n_patterns();
+    if (ndof) *ndof = h->ens->ndof();
+    if (offsets) {
+      const auto& off = h->ens->dof_offsets();
+      std::memcpy(offsets, off.data(), sizeof(int64_t) * off.size());
+    }
+    return FRESCO_OK;
+  });
+}
+
+namespace {
+void ensemble_io(fresco_ensemble_s* h, int64_t n) {
+  if (n != h->ens->ndof())
+    throw fb::InvalidArgument("the coordinate array has size " + std::to_string(n) + ", the ensemble expects " +
+                              std::to_string(h->ens->ndof()));
+  if (!h->dx.p) {
+    h->dx.alloc(n);
+    h->dg.alloc(n);
+    h->de.alloc(h->ens->n_patterns());
+  }
+}
+}  // namespace
+
+int fresco_ensemble_energy_gradient(fresco_ensemble h, const double* x, int64_t n, double* grad, double* energies) {
+  return guarded([&] {
+    if (!h || !x || !energies) throw fb::InvalidArgument("null argument");
+    ensemble_io(h, n);
+    FB_CUDA(cudaMemcpyAsync(h->dx.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    h->ens->eval_graph(h->dx.p, grad ? h->dg.p : nullptr, h->de.p, h->stream);
+    if (grad) FB_CUDA(cudaMemcpyAsync(grad, h->dg.p, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    FB_CUDA(cudaMemcpyAsync(energies, h->de.p, sizeof(double) * h->ens->n_patterns(), cudaMemcpyDeviceToHost,
+                            h->stream));
+    FB_CUDA(cudaStreamSynchronize(h->stream));
+    return FRESCO_OK;
+  });
+}
+
+int fresco_ensemble_energy_gradient_device(fresco_ensemble h, const double* d_x, int64_t n, double* d_grad,
+                                           double* d_energies, void* stream) {
+  return guarded([&] {
+    if (!h || !d_x || !d_energies) throw fb::InvalidArgument("null argument");
+    if (n != h->ens->ndof()) throw fb::InvalidArgument("the coordinate array has the wrong size");
+    h->ens->eval_graph(d_x, d_grad, d_energies, static_cast<cudaStream_t>(stream));
+    return FRESCO_OK;
+  });
+}
+
+int fresco_ensemble_tune(fresco_ensemble h, const double* x, int64_t n) {
+  return guarded([&] {
+    if (!h || !x) throw fb::InvalidArgument("null argument");
+    ensemble_io(h, n);
+    FB_CUDA(cudaMemcpyAsync(h->dx.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    h->ens->tune(h->dx.p, h->dg.p, h->de.p, h->stream);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_ensemble_set_split(fresco_ensemble h, double ratio) {
+  return guarded([&] {
+    if (!h) throw fb::InvalidArgument("null argument");
+    if (!(ratio >= 0.0)) throw fb::InvalidArgument("the split ratio must be >= 0");
+    h->ens->set_split(ratio);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_ensemble_status(fresco_ensemble h, int* status) {
+  return guarded([&] {
+    if (!h || !status) throw fb::InvalidArgument("null argument");
+    h->ens->read_and_clear_status(status, h->stream);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_ensemble_describe(fresco_ensemble h, char* buf, int buf_len) {
+  return guarded([&] {
+    if (!h || !buf || buf_len < 1) throw fb::InvalidArgument("null argument");
+    const std::string d = h->ens->describe();
+    std::strncpy(buf, d.c_str(), size_t(buf_len) - 1);
+    buf[buf_len - 1] = '\0';
+    return FRESCO_OK;
+  });
+}
+
+void fresco_ensemble_destroy(fresco_ensemble h) {
+  if (!h) return;
+  if (h->stream) {
+    cudaStreamSynchronize(h->stream);
+    cudaStreamDestroy(h->stream);
+  }
+  delete h;
+}
+
+int fresco_ensemble_lbfgs_create(fresco_ensemble h, const double* x0, int64_t n, double tol, int M, double maxstep,
+                                 double max_f_rise, double H0, int rel_energy, fresco_ensemble_lbfgs* out) {
+  return guarded([&] {
+    if (!h || !x0 || !out) throw fb::InvalidArgument("null argument");
+    fb::EnsembleLbfgsParams prm;
+    prm.tol = tol;
+    prm.M = M;
+    prm.maxstep = maxstep;
+    prm.max_f_rise = max_f_rise;
+    prm.H0 = H0;
+    prm.rel_energy = rel_energy != 0;
+    auto* o = new fresco_ensemble_lbfgs_s;
+    try {
+      o->opt.reset(new fb::EnsembleLbfgs(h->ens, x0, n, prm));
+    } catch (...) {
+      delete o;
+      throw;
+    }
+    *out = o;
+    return FRESCO_OK;
+  });
+}
+
+int fresco_ensemble_lbfgs_run(fresco_ensemble_lbfgs o, int niter, int* steps_taken) {
+  return guarded([&] {
+    if (!o) throw fb::InvalidArgument("null argument");
+    const int k = o->opt->run(niter);
+    if (steps_taken) *steps_taken = k;
+    return FRESCO_OK;
+  });
+}
+
+int fresco_ensemble_lbfgs_steps(fresco_ensemble_lbfgs o, int n_steps) {
+  return guarded([&] {
+    if (!o) throw fb::InvalidArgument("null argument");
+    o->opt->steps(n_steps);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_ensemble_lbfgs_state(fresco_ensemble_lbfgs o, double* x, double* g, double* f, double* rms, int* niter,
+                                int* nfev, int* active) {
+  return guarded([&] {
+    if (!o) throw fb::InvalidArgument("null argument");
+    o->opt->get_state(x, g, f, rms, niter, nfev, active);
+    return FRESCO_OK;
+  });
+}
+
+void fresco_ensemble_lbfgs_destroy(fresco_ensemble_lbfgs o) { delete o; }
 
 }  // extern "C"

@@ -395,12 +395,14 @@ __device__ __forceinline__ void flush_group_f32(const T* trow, int tc0, int edge
   }
 }
 
+// Body of one 2D spreading subproblem: the cnt records from `start` lie in
+// the 64 x 64-cell tile with origin (org0, org1) of an nf0 x nf1 fine grid;
+// `sole` says the subproblem holds all of its tile's points.
 template <int W, typename T, bool CPLX>
-__global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
-    const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, T uniform,
-    const cplx_t<T>* __restrict__ strengths, const int* __restrict__ sub_bin, const int* __restrict__ sub_start,
-    const int* __restrict__ sub_count, const int* __restrict__ num_sub, const int* __restrict__ bin_start, Geom g,
-    const EsPoly<W, T> poly, T* grid_real, cplx_t<T>* grid_cplx) {
+__device__ __forceinline__ void spread2d_tile_body(const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights,
+                                                   T uniform, const cplx_t<T>* __restrict__ strengths, int start,
+                                                   int cnt, int org0, int org1, bool sole_sub, int nf0, int nf1,
+                                                   const EsPoly<W, T>& poly, T* grid_real, cplx_t<T>* grid_cplx) {
   using P = Tile2D<W>;
   using S = Staged2D<T, CPLX>;
   constexpr int NC = CPLX ? 2 : 1;
@@ -412,12 +414,6 @@ __global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
   uint16_t* rank = reinterpret_cast<uint16_t*>(tile + E * E * NC);
   int* sb_count = reinterpret_cast<int*>(rank + kMaxSub);
   int* sb_start = sb_count + NSB2;
-
-  const int sub = blockIdx.x;
-  if (sub >= *num_sub) return;
-  const int bin = sub_bin[sub];
-  const int start = sub_start[sub], cnt = sub_count[sub];
-  const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
   const int tid = threadIdx.x;
 
   for (int i = tid; i < E * E * NC; i += P::THREADS) tile[i] = T(0);
@@ -561,7 +557,6 @@ __global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
   }
 
   // flush
-  const int nf0 = g.nf[0], nf1 = g.nf[1];
   if (sizeof(T) == 4 && nf0 % (4 / NC) == 0) {
     constexpr int VW = 4 / NC;                          // cells per float4
     constexpr int LEFT = (VW - P::PAD % VW) % VW;       // cells left of the tile origin in the first group
@@ -569,7 +564,7 @@ __global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
     // cells [W, 64) of the tile (relative to org - PAD) along both axes are
     // out of reach of every other tile; with one subproblem in the bin and
     // whole tiles (nf a multiple of 64) they are written with plain stores
-    const bool sole = cnt == bin_start[bin + 1] - bin_start[bin] && nf0 % kTile2D == 0 && nf1 % kTile2D == 0;
+    const bool sole = sole_sub && nf0 % kTile2D == 0 && nf1 % kTile2D == 0;
     for (int i = tid; i < E * NG; i += P::THREADS) {
       const int ty = i / NG, j = i - ty * NG;
       const int tc0 = j * VW - LEFT;
@@ -593,6 +588,22 @@ __global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
       }
     }
   }
+}
+
+template <int W, typename T, bool CPLX>
+__global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
+    const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, T uniform,
+    const cplx_t<T>* __restrict__ strengths, const int* __restrict__ sub_bin, const int* __restrict__ sub_start,
+    const int* __restrict__ sub_count, const int* __restrict__ num_sub, const int* __restrict__ bin_start, Geom g,
+    const EsPoly<W, T> poly, T* grid_real, cplx_t<T>* grid_cplx) {
+  const int sub = blockIdx.x;
+  if (sub >= *num_sub) return;
+  const int bin = sub_bin[sub];
+  const int start = sub_start[sub], cnt = sub_count[sub];
+  const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
+  const bool sole = cnt == bin_start[bin + 1] - bin_start[bin];
+  spread2d_tile_body<W, T, CPLX>(recs, weights, uniform, strengths, start, cnt, org0, org1, sole, g.nf[0], g.nf[1],
+                                 poly, grid_real, grid_cplx);
 }
 
 // Generic spreading (1D, 3D): one thread per point, shared-memory atomics.
@@ -708,11 +719,11 @@ __device__ __forceinline__ void interp_store(int mode, uint32_t o, T wgt, T v0r,
 // modulo the group size.  The block therefore buckets its points by
 // base mod G and lane c of every group takes points of class c only.
 template <int W, typename T>
-__global__ void __launch_bounds__(256) interp2d_tile_kernel(
-    const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, T uniform, const int* __restrict__ sub_bin,
-    const int* __restrict__ sub_start, const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g,
-    const EsPoly<W, T> poly, const cplx_t<T>* __restrict__ field, int mode, double* grad, double2* out2, int accumulate,
-    const int* __restrict__ status, const GradScale gs) {
+__device__ __forceinline__ void interp2d_tile_body(const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights,
+                                                   T uniform, int start, int cnt, int org0, int org1, int nf0, int nf1,
+                                                   const EsPoly<W, T>& poly, const cplx_t<T>* __restrict__ field,
+                                                   int mode, double* grad, double2* out2, int accumulate, bool bad,
+                                                   const GradScale& gs) {
   constexpr int PAD = W / 2;
   constexpr int TW = kTile2D + W;
   constexpr int G = 128 / int(sizeof(cplx_t<T>));  // lanes per wavefront = bank classes
@@ -721,14 +732,7 @@ __global__ void __launch_bounds__(256) interp2d_tile_kernel(
   uint16_t* code = reinterpret_cast<uint16_t*>(tile + TW * TW);  // class << 12 | rank in class
   uint16_t* order = code + kMaxSub;                               // points grouped by class
   __shared__ int cls_count[G], cls_start[G];
-  const int sub = blockIdx.x;
-  if (sub >= *num_sub) return;
   const int tid = threadIdx.x;
-  const bool bad = status != nullptr && ((*status) & STATUS_NONFINITE_INPUT);
-  const int bin = sub_bin[sub];
-  const int start = sub_start[sub], cnt = sub_count[sub];
-  const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
-  const int nf0 = g.nf[0], nf1 = g.nf[1];
   if (tid < G) cls_count[tid] = 0;
   __syncthreads();
   // tile and records are read in batches of 4 loads per thread so that their
@@ -810,6 +814,21 @@ __global__ void __launch_bounds__(256) interp2d_tile_kernel(
     const T wgt = (mode == INTERP_GRAD) ? (weights ? weights[r.idx] : uniform) : T(1);
     interp_store<2, T>(mode, r.idx, wgt, vr, vi, T(0), bad, grad, out2, accumulate, gs);
   }
+}
+
+template <int W, typename T>
+__global__ void __launch_bounds__(256) interp2d_tile_kernel(
+    const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, T uniform, const int* __restrict__ sub_bin,
+    const int* __restrict__ sub_start, const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g,
+    const EsPoly<W, T> poly, const cplx_t<T>* __restrict__ field, int mode, double* grad, double2* out2, int accumulate,
+    const int* __restrict__ status, const GradScale gs) {
+  const int sub = blockIdx.x;
+  if (sub >= *num_sub) return;
+  const bool bad = status != nullptr && ((*status) & STATUS_NONFINITE_INPUT);
+  const int bin = sub_bin[sub];
+  const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
+  interp2d_tile_body<W, T>(recs, weights, uniform, sub_start[sub], sub_count[sub], org0, org1, g.nf[0], g.nf[1], poly,
+                           field, mode, grad, out2, accumulate, bad, gs);
 }
 
 // Generic interpolation (1D, 3D): thread per sorted point, taps gathered

@@ -26,15 +26,12 @@
 
 #include "fft_block.cuh"
 #include "nufft.cuh"
+#include "nuwu_modes.cuh"
 #include "potential.cuh"
 
 namespace fb {
 
 namespace {
-
-struct ModeCoef {
-  double A, B, w2, s0;  // A, B as above; w2 = V/S0'^2, s0 = S0 (phi = w2 (q - s0)^2)
-};
 
 template <int D, typename T>
 __global__ void __launch_bounds__(256) nuwu_modes_kernel(
@@ -43,63 +40,9 @@ __global__ void __launch_bounds__(256) nuwu_modes_kernel(
     const double* __restrict__ corr2, cplx_t<T>* hgrid, int64_t G, double* energy, const int* __restrict__ status,
     int want_grad) {
   double phi = 0.0;
-  const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_active; i += gridDim.x * blockDim.x) {
-    const int m = mode_idx[i];
-    const int kx = m % n - K;
-    const int ky = (D >= 2) ? (m / n) % n - K : 0;
-    const int kz = (D >= 3) ? m / (n * n) - K : 0;
-    double p = corr0[kx + K];
-    if (D >= 2) p *= corr1[ky + K];
-    if (D >= 3) p *= corr2[kz + K];
-    // R2C output holds k_x >= 0; rho(k) = conj(B(k)) for k_x >= 0 (iflag +1
-    // from a sign -1 transform) and rho(k) = B(-k) otherwise.
-    int64_t bi;
-    bool cj;
-    if (kx >= 0) {
-      const int yy = ky < 0 ? ky + nf1 : ky;
-      const int zz = kz < 0 ? kz + nf2 : kz;
-      bi = kx + int64_t(nh0) * (yy + int64_t(nf1) * zz);
-      cj = true;
-    } else {
-      const int yy = ky > 0 ? nf1 - ky : -ky;
-      const int zz = kz > 0 ? nf2 - kz : -kz;
-      bi = -kx + int64_t(nh0) * (yy + int64_t(nf1) * zz);
-      cj = false;
-    }
-    const cplx_t<T> b = bhat[bi];
-    const double rr = double(b.x) / p;
-    const double ri = (cj ? -double(b.y) : double(b.y)) / p;
-    const double q = (rr * rr + ri * ri) * invN;
-    const ModeCoef c = coef[i];
-    const double dq = q - c.s0;
-    phi += c.w2 * dq * dq;
-    if (want_grad) {
-      const double a = (c.A * q - c.B) * (2.0 * invN) / p;  // includes the type-2 pre-correction 1/p
-      const double fr = rr * a, fi = ri * a;                 // F^H / p
-      const int x0 = kx < 0 ? kx + nf0 : kx;
-      const int y0 = ky < 0 ? ky + nf1 : ky;
-      const int z0 = kz < 0 ? kz + nf2 : kz;
-      const int64_t hi = x0 + int64_t(nf0) * (y0 + int64_t(nf1) * z0);
-      cplx_t<T> h;
-      if (D == 1) {
-        // -i kx F
-        h.x = T(fi * kx);
-        h.y = T(-fr * kx);
-      } else {
-        // F (ky - i kx)
-        h.x = T(fr * ky + fi * kx);
-        h.y = T(fi * ky - fr * kx);
-      }
-      hgrid[hi] = h;
-      if (D == 3) {
-        cplx_t<T> h2;
-        h2.x = T(fi * kz);
-        h2.y = T(-fr * kz);
-        hgrid[G + hi] = h2;
-      }
-    }
-  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_active; i += gridDim.x * blockDim.x)
+    phi += nuwu_mode_term<D, T>(mode_idx[i], n, K, coef[i], bhat, nh0, g.nf[0], g.nf[1], g.nf[2], corr0, corr1, corr2,
+                                invN, hgrid, G, want_grad != 0);
   block_sum_atomic(phi, energy);
   if (blockIdx.x == 0 && threadIdx.x == 0 && status != nullptr && ((*status) & STATUS_NONFINITE_INPUT)) {
     atomicAdd(energy, __longlong_as_double(0x7ff8000000000000ULL));
@@ -331,30 +274,7 @@ class NUwUImpl final : public Potential {
     // active modes and their coefficients
     std::vector<int> idx;
     std::vector<ModeCoef> coef;
-    auto mirror = [&](int64_t m) {
-      int64_t r = m, out = 0, stride = 1;
-      for (int a = 0; a < D; ++a) {
-        const int64_t ia = r % n_;
-        r /= n_;
-        out += (n_ - 1 - ia) * stride;
-        stride *= n_;
-      }
-      return out;
-    };
-    for (int64_t m = 0; m < nm; ++m) {
-      const int64_t mm = mirror(m);
-      const double vk = v[m], vm = v[mm];
-      if (vk == 0.0 && vm == 0.0) continue;
-      const double s0k = sk[m], s0m = sk[mm];
-      const double dk = s0k != 0.0 ? s0k : 1.0, dm = s0m != 0.0 ? s0m : 1.0;
-      ModeCoef cc;
-      cc.A = vk / (dk * dk) + vm / (dm * dm);
-      cc.B = vk * s0k / (dk * dk) + vm * s0m / (dm * dm);
-      cc.w2 = vk / (dk * dk);
-      cc.s0 = s0k;
-      idx.push_back(int(m));
-      coef.push_back(cc);
-    }
+    nuwu_mode_table(D, n_, v.data(), sk.data(), idx, coef);
     n_active_ = int(idx.size());
     if (n_active_) {
       mode_idx_.alloc(n_active_);

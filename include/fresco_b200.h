@@ -32,6 +32,8 @@ extern "C" {
 
 typedef struct fresco_potential_s* fresco_potential;
 typedef struct fresco_optimizer_s* fresco_optimizer;
+typedef struct fresco_ensemble_s* fresco_ensemble;
+typedef struct fresco_ensemble_lbfgs_s* fresco_ensemble_lbfgs;
 
 enum {
   FRESCO_OK = 0,
@@ -213,6 +215,54 @@ int fresco_optimizer_get_state(fresco_optimizer o, double* x, double* g, double*
 /* Device pointers of the optimiser's x and g (valid until destroy). */
 int fresco_optimizer_device_state(fresco_optimizer o, double** d_x, double** d_g);
 void fresco_optimizer_destroy(fresco_optimizer o);
+
+/* ---- batched ensembles ---------------------------------------------------- */
+
+/* P independent 2D NUwU patterns evaluated together: the batched form of P
+ * objects fresco.potentials.NUwU(radii_p, K, Sk_p, V_p, L, eps)
+ * (fresco/potentials/nuwu.pyx:10-23, source/fresco/nuwu.hpp:35-149).
+ * n_points[p] points and n_modes[p] = len(V_p) per pattern; radii holds the
+ * sum of n_points values and sk, v the sum of n_modes values, pattern after
+ * pattern; L (ndim = 2 values) is common.  Coordinates of all patterns are
+ * concatenated, pattern p at doubles [offsets[p], offsets[p+1]). */
+int fresco_nuwu_ensemble_create(int n_patterns, const int64_t* n_points, const double* radii, const int64_t* n_modes,
+                                const double* sk, const double* v, const double* L, int ndim, double eps,
+                                int precision, fresco_ensemble* out);
+/* Number of patterns, total coordinate count and the P + 1 offsets (may be NULL). */
+int fresco_ensemble_info(fresco_ensemble h, int* n_patterns, int64_t* ndof, int64_t* offsets);
+/* get_energy_gradient of every pattern (host buffers; grad may be NULL for
+ * energies only): energies[p], grad in the x layout. */
+int fresco_ensemble_energy_gradient(fresco_ensemble h, const double* x, int64_t n, double* grad, double* energies);
+/* Device-buffer form, asynchronous on stream, replayed as a CUDA graph when
+ * the same buffers repeat. */
+int fresco_ensemble_energy_gradient_device(fresco_ensemble h, const double* d_x, int64_t n, double* d_grad,
+                                           double* d_energies, void* stream);
+/* Times the tiled and direct spreading/interpolation split on x and keeps
+ * the fastest per group of equal mode grids. */
+int fresco_ensemble_tune(fresco_ensemble h, const double* x, int64_t n);
+/* Sets the split by hand: patterns whose tap work N w^2 is below ratio x the
+ * tile cells of their bins use the direct kernels (0: all tiled). */
+int fresco_ensemble_set_split(fresco_ensemble h, double ratio);
+/* Per-pattern status bits since the last call (P ints). */
+int fresco_ensemble_status(fresco_ensemble h, int* status);
+int fresco_ensemble_describe(fresco_ensemble h, char* buf, int buf_len);
+void fresco_ensemble_destroy(fresco_ensemble h);
+
+/* LBFGS_CPP(x0_p, NUwU_p, M=M, tol=tol, maxstep=..., maxErise=..., H0=...)
+ * for every pattern at once (fresco/optimize/_lbfgs_cpp.pyx:22-66,
+ * source/lbfgs.cpp:9-258); x0 in the ensemble's layout. */
+int fresco_ensemble_lbfgs_create(fresco_ensemble h, const double* x0, int64_t n, double tol, int M, double maxstep,
+                                 double max_f_rise, double H0, int rel_energy, fresco_ensemble_lbfgs* out);
+/* run(niter) of every pattern (optimizer.hpp:97-112); steps_taken (may be
+ * NULL) receives the number of ensemble evaluations used. */
+int fresco_ensemble_lbfgs_run(fresco_ensemble_lbfgs o, int niter, int* steps_taken);
+/* Exactly n_steps ensemble steps (each pattern iterating at most n_steps times). */
+int fresco_ensemble_lbfgs_steps(fresco_ensemble_lbfgs o, int n_steps);
+/* x, g (ndof doubles) and per-pattern f, rms, iterations, evaluations and
+ * whether the pattern is still iterating; any pointer may be NULL. */
+int fresco_ensemble_lbfgs_state(fresco_ensemble_lbfgs o, double* x, double* g, double* f, double* rms, int* niter,
+                                int* nfev, int* active);
+void fresco_ensemble_lbfgs_destroy(fresco_ensemble_lbfgs o);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

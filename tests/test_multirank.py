@@ -54,3 +54,62 @@ def test_single_process_helpers():
 
     assert bench.reduce_max(3.5, "cpu") == 3.5
     assert bench.job_value(1, 20, 500.0) == pytest.approx(40.0)
+
+
+def test_shard_patterns_covers_every_pattern_once_and_balances():
+    """Longest-processing-time-first sharding of a config-5-like ensemble (256 patterns)."""
+    import numpy as np
+
+    from fresco_b200.ensemble import pattern_cost, shard_patterns
+
+    rng = np.random.default_rng(5)
+    N = np.exp(rng.uniform(np.log(1000), np.log(200000), 256)).astype(int)
+    side = rng.choice([64, 128, 256, 512], 256)
+    costs = [pattern_cost(n, s + 1) for n, s in zip(N, side)]
+    for ws in [1, 2, 3, 8]:
+        parts = shard_patterns(costs, ws)
+        assert len(parts) == ws
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(256))
+        loads = [sum(costs[i] for i in p) for p in parts]
+        assert max(loads) <= sum(costs) / ws + max(costs) + 1e-6
+    with pytest.raises(ValueError):
+        shard_patterns(costs, 0)
+
+
+def _gather_worker(rank, world, port, out):
+    import torch.distributed as dist
+
+    from fresco_b200.ensemble import gather_results, shard_patterns
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        costs = [float(7 * i % 11 + 1) for i in range(23)]
+        mine = shard_patterns(costs, world)[rank]
+        local = [{"pattern": i, "energy": 0.5 * i, "rank": rank} for i in mine]
+        merged = gather_results(local, mine)
+        out.put((rank, [(r["pattern"], r["energy"]) for r in merged], sorted({r["rank"] for r in merged})))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_ensemble_gather():
+    """Each rank keeps its own shard of patterns; the final gather gives every rank all results in order."""
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gather_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+    assert all(p.exitcode == 0 for p in procs)
+    res = sorted(q.get(timeout=5) for _ in range(2))
+    for rank, merged, ranks in res:
+        assert merged == [(i, 0.5 * i) for i in range(23)]
+        assert ranks == [0, 1]
