@@ -44,10 +44,120 @@ WORKLOAD = (
 )
 
 
-def inputs(seed):
-    from oracle import oracle as O
+def stealthy_inputs(n_points, K, kmax, seed, box=2 * np.pi):
+    """Seeded uniform points in [0, box)^2, radii 1, S0 = 0 and V = 1 on 0 < |k| <= kmax of the
+    (2K+1)^2 mode grid."""
+    rng = np.random.default_rng(seed)
+    L = np.full(2, float(box))
+    x = (rng.random((n_points, 2)) * L).ravel()
+    kv = np.arange(-K, K + 1)
+    kx, ky = np.meshgrid(kv, kv, indexing="ij")
+    kmag = np.sqrt(kx.astype(np.float64) ** 2 + ky.astype(np.float64) ** 2)
+    V = ((kmag <= kmax) & (kmag > 0)).astype(np.float64)
+    return x, np.ones(n_points), np.zeros_like(V), V, L
 
-    return O.stealthy_nuwu_inputs(N_POINTS, K_MODES, K_CONSTRAINED, ndim=2, seed=seed)
+
+def inputs(seed):
+    return stealthy_inputs(N_POINTS, K_MODES, K_CONSTRAINED, seed)
+
+
+ENSEMBLE_PATTERNS = 256
+ENSEMBLE_WORKLOAD = (
+    "batched 2D NUwU ensemble: 256 seeded patterns, N log-uniform in [1000, 200000], k-grid side uniform in "
+    "{64,128,256,512} (K = side/2, odd (side+1)^2 modes), stealthy disc S0=0 & V=1 on 0<|k|<=side/8, "
+    "L=2pi, eps=1e-6, FP32 spread/FFT/interp"
+)
+
+
+def ensemble_inputs(seed=5, n_patterns=ENSEMBLE_PATTERNS):
+    """Per-pattern (x, radii, K, Sk, V) of the batched-ensemble workload."""
+    rng = np.random.default_rng(seed)
+    N = np.exp(rng.uniform(np.log(1000), np.log(200000), n_patterns)).astype(np.int64)
+    side = rng.choice([64, 128, 256, 512], n_patterns)
+    pats = []
+    for p in range(n_patterns):
+        K = int(side[p]) // 2
+        x, r, Sk, V, L = stealthy_inputs(int(N[p]), K, int(side[p]) // 8, seed=1000 + p)
+        pats.append((x, r, K, Sk.ravel(), V.ravel()))
+    return pats, np.full(2, 2 * np.pi)
+
+
+def ensemble_report(args, dev, ws, rank):
+    """Batched ensemble: the rank's cost-model shard of the 256 patterns as one NUwUEnsemble (FP32),
+    evaluations of every pattern per second (device-timed graph replays, max over ranks) and
+    per-pattern device LBFGS steps; at one GPU also the same patterns as 256 separate NUwU
+    potentials evaluated one after another (graph replay each)."""
+    import torch
+
+    from fresco_b200 import EnsembleLBFGS, NUwU, NUwUEnsemble
+    from fresco_b200.ensemble import pattern_cost, shard_patterns
+
+    pats, L = ensemble_inputs()
+    costs = [pattern_cost(len(x) // 2, 2 * K + 1) for x, _, K, _, _ in pats]
+    mine = shard_patterns(costs, ws)[rank]
+    sel = [pats[i] for i in mine]
+    ens = NUwUEnsemble([r for _, r, _, _, _ in sel], [K for _, _, K, _, _ in sel], [s for _, _, _, s, _ in sel],
+                       [v for _, _, _, _, v in sel], L, eps=EPS, precision="fp32")
+    xs = [x for x, _, _, _, _ in sel]
+    t0 = time.perf_counter()
+    ens.tune(xs)
+    tune_s = time.perf_counter() - t0
+    dx = torch.tensor(ens.concat(xs), device=dev)
+    dg = torch.empty_like(dx)
+    de = torch.empty(ens.n_patterns, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(max(3, args.warmup)):
+        ens.get_energies_gradient_device(dx, dg, de, stream.cuda_stream)
+    torch.cuda.synchronize()
+    n = max(5, args.steps // 2)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(n):  # the points (154 MB) and grids exceed L2: no flush needed between steps
+        ens.get_energies_gradient_device(dx, dg, de, stream.cuda_stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = reduce_max(a.elapsed_time(b) / n, dev)
+    total_points = sum(len(x) // 2 for x, _, _, _, _ in pats)
+    out = {"workload": ENSEMBLE_WORKLOAD, "patterns": len(pats), "points": int(total_points),
+           "pattern_evals_per_s": round(len(pats) / (ms * 1e-3), 1), "ms_per_ensemble_eval": round(ms, 4),
+           "points_per_s": round(total_points / (ms * 1e-3), 1), "tune_s": round(tune_s, 2),
+           "setup": ens.describe()}
+    # device LBFGS (M = 4) for every pattern: one graph launch per step (host clock around steps())
+    opt = EnsembleLBFGS(xs, ens, M=4, tol=1e-12)
+    opt.steps(3)
+    nst = max(10, args.steps // 2)
+    _, _, f0, _, it0, _, _ = opt.state(False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    opt.steps(nst)
+    lb_s = reduce_max(time.perf_counter() - t0, dev)
+    _, _, f1, _, it1, _, _ = opt.state(False)
+    out["lbfgs"] = {"steps_per_s": round(nst / lb_s, 2), "pattern_iterations_per_s":
+                    round(reduce_sum(float(np.sum(it1 - it0)), dev) / lb_s, 1),
+                    "patterns_lower_energy": int(reduce_sum(float(np.sum(f1 < f0)), dev)), "M": 4,
+                    "timing": "host wall clock around the graph launches of steps(), max over ranks"}
+    del opt
+    if ws == 1 and not args.no_ensemble_loop:
+        # the same patterns as separate potentials, one after another on one stream
+        pots = [NUwU(r, K, s, v, L, eps=EPS, precision="fp32") for _, r, K, s, v in pats]
+        bufs = [(torch.tensor(x, device=dev), torch.empty(len(x), dtype=torch.float64, device=dev),
+                 torch.empty((), dtype=torch.float64, device=dev)) for x, _, _, _, _ in pats]
+        for _ in range(2):
+            for pot, (px, pg, pe) in zip(pots, bufs):
+                pot.energy_gradient_device(px, pg, pe)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(3):
+            for pot, (px, pg, pe) in zip(pots, bufs):
+                pot.energy_gradient_device(px, pg, pe)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms_loop = a.elapsed_time(b) / 3
+        out["separate_potentials"] = {"pattern_evals_per_s": round(len(pats) / (ms_loop * 1e-3), 1),
+                                      "ms_per_ensemble_eval": round(ms_loop, 4)}
+        del pots, bufs
+    del ens
+    return out
 
 
 def dist_env():
@@ -139,6 +249,21 @@ def reduce_max(value, device):
 
         if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    except ImportError:
+        pass
+    return float(t.item())
+
+
+def reduce_sum(value, device):
+    """Sum of a per-rank scalar over all ranks."""
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    try:
+        import torch.distributed as dist
+
+        if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.SUM)
     except ImportError:
         pass
     return float(t.item())
@@ -301,6 +426,8 @@ def run_ours(args):
     roofline_eval = {"bound": "hbm", "algorithmic_bytes": b_eval, "achieved": round(eval_achieved, 1),
                      "peak": hbm_peak, "unit": "GB/s", "frac": round(eval_achieved / hbm_peak, 4)}
 
+    ensemble = None if args.no_ensemble else ensemble_report(args, dev, ws, rank)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(x, radii, Sk, V, L, samples=args.cpu_samples)
@@ -333,6 +460,7 @@ def run_ours(args):
                  "fp32_over_fp64": round(ms64 / ms_per_step, 3)},
         "nuwu_plus_repulsion": {"evals_per_s_per_gpu": round(comb_evals, 2)},
         "lbfgs": lbfgs,
+        "ensemble": ensemble,
         "accuracy": {"grad_rel_err_fp32": err32, "grad_rel_err_fp64_eps1e-6": err64, "energy_rel_err_fp32": eerr32,
                      "oracle": "GPU FP64 form at eps=1e-12 (parity-tested against exact sums)"},
         "clocks": clk,
@@ -414,6 +542,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-samples", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble section")
+    ap.add_argument("--no-ensemble-loop", action="store_true",
+                    help="skip timing the ensemble's patterns as separate potentials")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -225,24 +225,38 @@ __global__ void __launch_bounds__(kEnsSortThreads) ens_sort_scatter_kernel(
   }
 }
 
-// Tiled spreading: block b handles subproblem slot tab[b].y of pattern tab[b].x.
-template <int W, typename T>
-__global__ void __launch_bounds__(Tile2D<W>::THREADS) ens_spread_tiled_kernel(
-    const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, const PatInfo* __restrict__ pats,
-    const int2* __restrict__ tab, const int* __restrict__ sub_bin, const int* __restrict__ sub_start,
-    const int* __restrict__ sub_count, const int* __restrict__ num_sub, const int* __restrict__ bin_start, Geom g,
-    const EsPoly<W, T> poly, T* grid, int64_t G) {
-  const int2 bt = tab[blockIdx.x];
-  if (bt.y >= num_sub[bt.x]) return;
-  const PatInfo pi = pats[bt.x];
-  const int si = pi.sub_base + bt.y;
-  const int bin = sub_bin[si], start = sub_start[si], cnt = sub_count[si];
-  const int* bs = bin_start + int64_t(bt.x) * (g.nbins() + 1);
-  const bool sole = cnt == bs[bin + 1] - bs[bin];
-  const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
-  spread2d_tile_body<W, T, false>(recs, weights, T(pi.uniform), nullptr, start, cnt, org0, org1, sole, g.nf[0],
-                                  g.nf[1], poly, grid + int64_t(bt.x) * G, nullptr);
-}
+// Block b of the tiled kernels handles subproblem slot tab[b].y of pattern
+// tab[b].x of the group; the pattern's grid starts at pattern x G.
+template <typename T>
+struct EnsTileMap {
+  const PatInfo* __restrict__ pats;
+  const int2* __restrict__ tab;
+  const int* __restrict__ sub_bin;
+  const int* __restrict__ sub_start;
+  const int* __restrict__ sub_count;
+  const int* __restrict__ num_sub;
+  const int* __restrict__ bin_start;
+  const int* __restrict__ cur_status;
+  int64_t G;
+  __device__ __forceinline__ bool fetch(const Geom& g, TileWork<T>& w) const {
+    const int2 bt = tab[blockIdx.x];
+    if (bt.y >= num_sub[bt.x]) return false;
+    const PatInfo& pi = pats[bt.x];
+    const int si = pi.sub_base + bt.y;
+    const int bin = sub_bin[si];
+    w.start = sub_start[si];
+    w.cnt = sub_count[si];
+    w.org0 = (bin % g.nb[0]) * kTile2D;
+    w.org1 = (bin / g.nb[0]) * kTile2D;
+    w.bin_range = bin_start + int64_t(bt.x) * (g.nbins() + 1) + bin;
+    w.grid_off = int64_t(bt.x) * G;
+    w.uniform = T(pi.uniform);
+    return true;
+  }
+  __device__ __forceinline__ bool nonfinite(const TileWork<T>&) const {
+    return (cur_status[pats[tab[blockIdx.x].x].pid] & STATUS_NONFINITE_INPUT) != 0;
+  }
+};
 
 // Direct spreading for sparse patterns: thread per sorted point, the w x w
 // taps added to the grid with global atomics.
@@ -294,23 +308,6 @@ __global__ void __launch_bounds__(256) ens_modes_kernel(const PatInfo* __restric
   block_sum_atomic(phi, energy + pi.pid);
   if (blockIdx.x == 0 && threadIdx.x == 0 && (cur_status[pi.pid] & STATUS_NONFINITE_INPUT))
     atomicAdd(energy + pi.pid, __longlong_as_double(0x7ff8000000000000ULL));
-}
-
-template <int W, typename T>
-__global__ void __launch_bounds__(256) ens_interp_tiled_kernel(
-    const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, const PatInfo* __restrict__ pats,
-    const int2* __restrict__ tab, const int* __restrict__ sub_bin, const int* __restrict__ sub_start,
-    const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g, const EsPoly<W, T> poly,
-    const cplx_t<T>* __restrict__ field, int64_t G, double* grad, const int* __restrict__ cur_status) {
-  const int2 bt = tab[blockIdx.x];
-  if (bt.y >= num_sub[bt.x]) return;
-  const PatInfo pi = pats[bt.x];
-  const int si = pi.sub_base + bt.y;
-  const int bin = sub_bin[si];
-  const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
-  const bool bad = (cur_status[pi.pid] & STATUS_NONFINITE_INPUT) != 0;
-  interp2d_tile_body<W, T>(recs, weights, T(pi.uniform), sub_start[si], sub_count[si], org0, org1, g.nf[0], g.nf[1],
-                           poly, field + int64_t(bt.x) * G, INTERP_GRAD, grad, nullptr, 0, bad, GradScale());
 }
 
 template <int W, typename T>
@@ -682,9 +679,9 @@ class NUwUEnsembleImpl final : public Ensemble {
     constexpr size_t ss = spread2d_smem_bytes<W, T, false>();
     constexpr int TW = kTile2D + W;
     constexpr size_t si = sizeof(cplx_t<T>) * TW * TW + 2 * sizeof(uint16_t) * kMaxSub;
-    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(ens_spread_tiled_kernel<W, T>),
+    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(spread2d_tile_kernel<W, T, false, EnsTileMap<T>>),
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, int(ss)));
-    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(ens_interp_tiled_kernel<W, T>),
+    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(interp2d_tile_kernel<W, T, EnsTileMap<T>>),
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, int(si)));
   }
   void smem_attrs() {
@@ -726,11 +723,12 @@ class NUwUEnsembleImpl final : public Ensemble {
     FB_LAUNCH_CHECK();
     FB_CUDA(cudaMemsetAsync(gr.spread.p, 0, gr.spread.bytes(), s));
     const EsPoly<W, T> poly = make_es_poly<W, T>(poly_);
+    const EnsTileMap<T> map{gr.pats.p,     gr.tab.p,       gr.sub_bin.p, gr.sub_start.p, gr.sub_count.p,
+                            gr.num_sub.p, gr.bin_start.p, cur_status_.p, gr.G};
     if (gr.n_tab) {
       constexpr size_t ss = spread2d_smem_bytes<W, T, false>();
-      ens_spread_tiled_kernel<W, T><<<gr.n_tab, Tile2D<W>::THREADS, ss, s>>>(
-          recs, weights_.p, gr.pats.p, gr.tab.p, gr.sub_bin.p, gr.sub_start.p, gr.sub_count.p, gr.num_sub.p,
-          gr.bin_start.p, geo, poly, gr.spread.p, gr.G);
+      spread2d_tile_kernel<W, T, false, EnsTileMap<T>><<<gr.n_tab, Tile2D<W>::THREADS, ss, s>>>(
+          recs, weights_.p, nullptr, map, geo, poly, gr.spread.p, nullptr);
       FB_LAUNCH_CHECK();
     }
     if (gr.n_pitems) {
@@ -763,9 +761,8 @@ class NUwUEnsembleImpl final : public Ensemble {
     if (gr.n_tab) {
       constexpr int TW = kTile2D + W;
       constexpr size_t si = sizeof(cplx_t<T>) * TW * TW + 2 * sizeof(uint16_t) * kMaxSub;
-      ens_interp_tiled_kernel<W, T><<<gr.n_tab, 256, si, s>>>(recs, weights_.p, gr.pats.p, gr.tab.p, gr.sub_bin.p,
-                                                              gr.sub_start.p, gr.sub_count.p, gr.num_sub.p, geo, poly,
-                                                              gr.ggrid.p, gr.G, g, cur_status_.p);
+      interp2d_tile_kernel<W, T, EnsTileMap<T>><<<gr.n_tab, 256, si, s>>>(recs, weights_.p, map, geo, poly, gr.ggrid.p,
+                                                                          INTERP_GRAD, g, nullptr, 0, GradScale());
       FB_LAUNCH_CHECK();
     }
     if (gr.n_pitems) {

@@ -395,14 +395,53 @@ __device__ __forceinline__ void flush_group_f32(const T* trow, int tc0, int edge
   }
 }
 
-// Body of one 2D spreading subproblem: the cnt records from `start` lie in
-// the 64 x 64-cell tile with origin (org0, org1) of an nf0 x nf1 fine grid;
-// `sole` says the subproblem holds all of its tile's points.
-template <int W, typename T, bool CPLX>
-__device__ __forceinline__ void spread2d_tile_body(const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights,
-                                                   T uniform, const cplx_t<T>* __restrict__ strengths, int start,
-                                                   int cnt, int org0, int org1, bool sole_sub, int nf0, int nf1,
-                                                   const EsPoly<W, T>& poly, T* grid_real, cplx_t<T>* grid_cplx) {
+// Work of one block of the 2D tile kernels: the cnt sorted records from
+// `start` lie in the 64 x 64-cell tile with origin (org0, org1); bin_range
+// points at the tile's bin start (bin_range[1] - bin_range[0] is the tile's
+// point count, so the subproblem is its tile's only one when it equals cnt);
+// the fine grid starts grid_off cells after the kernel's grid pointer;
+// uniform is the weight when there are no per-point weights.
+template <typename T>
+struct TileWork {
+  int start, cnt, org0, org1;
+  const int* bin_range;
+  int64_t grid_off;
+  T uniform;
+};
+
+// Block -> work of one pattern's subproblem table (the single-pattern
+// potentials).
+template <typename T>
+struct TileMap1 {
+  const int* __restrict__ sub_bin;
+  const int* __restrict__ sub_start;
+  const int* __restrict__ sub_count;
+  const int* __restrict__ num_sub;
+  const int* __restrict__ bin_start;
+  const int* __restrict__ status;  // evaluation status word (interpolation), may be null
+  T uniform;
+  __device__ __forceinline__ bool fetch(const Geom& g, TileWork<T>& w) const {
+    const int sub = blockIdx.x;
+    if (sub >= *num_sub) return false;
+    const int bin = sub_bin[sub];
+    w.start = sub_start[sub];
+    w.cnt = sub_count[sub];
+    w.org0 = (bin % g.nb[0]) * kTile2D;
+    w.org1 = (bin / g.nb[0]) * kTile2D;
+    w.bin_range = bin_start + bin;
+    w.grid_off = 0;
+    w.uniform = uniform;
+    return true;
+  }
+  __device__ __forceinline__ bool nonfinite(const TileWork<T>&) const {
+    return status != nullptr && ((*status) & STATUS_NONFINITE_INPUT);
+  }
+};
+
+template <int W, typename T, bool CPLX, typename Map>
+__global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
+    const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, const cplx_t<T>* __restrict__ strengths,
+    const Map map, Geom g, const EsPoly<W, T> poly, T* grid_real, cplx_t<T>* grid_cplx) {
   using P = Tile2D<W>;
   using S = Staged2D<T, CPLX>;
   constexpr int NC = CPLX ? 2 : 1;
@@ -414,6 +453,13 @@ __device__ __forceinline__ void spread2d_tile_body(const Rec<2, T>* __restrict__
   uint16_t* rank = reinterpret_cast<uint16_t*>(tile + E * E * NC);
   int* sb_count = reinterpret_cast<int*>(rank + kMaxSub);
   int* sb_start = sb_count + NSB2;
+
+  TileWork<T> wk;
+  if (!map.fetch(g, wk)) return;
+  const int start = wk.start, cnt = wk.cnt, org0 = wk.org0, org1 = wk.org1;
+  const T uniform = wk.uniform;
+  if (grid_real) grid_real += wk.grid_off;
+  if (grid_cplx) grid_cplx += wk.grid_off;
   const int tid = threadIdx.x;
 
   for (int i = tid; i < E * E * NC; i += P::THREADS) tile[i] = T(0);
@@ -557,6 +603,7 @@ __device__ __forceinline__ void spread2d_tile_body(const Rec<2, T>* __restrict__
   }
 
   // flush
+  const int nf0 = g.nf[0], nf1 = g.nf[1];
   if (sizeof(T) == 4 && nf0 % (4 / NC) == 0) {
     constexpr int VW = 4 / NC;                          // cells per float4
     constexpr int LEFT = (VW - P::PAD % VW) % VW;       // cells left of the tile origin in the first group
@@ -564,7 +611,7 @@ __device__ __forceinline__ void spread2d_tile_body(const Rec<2, T>* __restrict__
     // cells [W, 64) of the tile (relative to org - PAD) along both axes are
     // out of reach of every other tile; with one subproblem in the bin and
     // whole tiles (nf a multiple of 64) they are written with plain stores
-    const bool sole = sole_sub && nf0 % kTile2D == 0 && nf1 % kTile2D == 0;
+    const bool sole = cnt == wk.bin_range[1] - wk.bin_range[0] && nf0 % kTile2D == 0 && nf1 % kTile2D == 0;
     for (int i = tid; i < E * NG; i += P::THREADS) {
       const int ty = i / NG, j = i - ty * NG;
       const int tc0 = j * VW - LEFT;
@@ -588,22 +635,6 @@ __device__ __forceinline__ void spread2d_tile_body(const Rec<2, T>* __restrict__
       }
     }
   }
-}
-
-template <int W, typename T, bool CPLX>
-__global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
-    const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, T uniform,
-    const cplx_t<T>* __restrict__ strengths, const int* __restrict__ sub_bin, const int* __restrict__ sub_start,
-    const int* __restrict__ sub_count, const int* __restrict__ num_sub, const int* __restrict__ bin_start, Geom g,
-    const EsPoly<W, T> poly, T* grid_real, cplx_t<T>* grid_cplx) {
-  const int sub = blockIdx.x;
-  if (sub >= *num_sub) return;
-  const int bin = sub_bin[sub];
-  const int start = sub_start[sub], cnt = sub_count[sub];
-  const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
-  const bool sole = cnt == bin_start[bin + 1] - bin_start[bin];
-  spread2d_tile_body<W, T, CPLX>(recs, weights, uniform, strengths, start, cnt, org0, org1, sole, g.nf[0], g.nf[1],
-                                 poly, grid_real, grid_cplx);
 }
 
 // Generic spreading (1D, 3D): one thread per point, shared-memory atomics.
@@ -718,12 +749,12 @@ __device__ __forceinline__ void interp_store(int mode, uint32_t o, T wgt, T v0r,
 // reads without bank conflicts when the bases of its points are distinct
 // modulo the group size.  The block therefore buckets its points by
 // base mod G and lane c of every group takes points of class c only.
-template <int W, typename T>
-__device__ __forceinline__ void interp2d_tile_body(const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights,
-                                                   T uniform, int start, int cnt, int org0, int org1, int nf0, int nf1,
-                                                   const EsPoly<W, T>& poly, const cplx_t<T>* __restrict__ field,
-                                                   int mode, double* grad, double2* out2, int accumulate, bool bad,
-                                                   const GradScale& gs) {
+template <int W, typename T, typename Map>
+__global__ void __launch_bounds__(256) interp2d_tile_kernel(const Rec<2, T>* __restrict__ recs,
+                                                            const T* __restrict__ weights, const Map map, Geom g,
+                                                            const EsPoly<W, T> poly,
+                                                            const cplx_t<T>* __restrict__ field, int mode, double* grad,
+                                                            double2* out2, int accumulate, const GradScale gs) {
   constexpr int PAD = W / 2;
   constexpr int TW = kTile2D + W;
   constexpr int G = 128 / int(sizeof(cplx_t<T>));  // lanes per wavefront = bank classes
@@ -732,6 +763,13 @@ __device__ __forceinline__ void interp2d_tile_body(const Rec<2, T>* __restrict__
   uint16_t* code = reinterpret_cast<uint16_t*>(tile + TW * TW);  // class << 12 | rank in class
   uint16_t* order = code + kMaxSub;                               // points grouped by class
   __shared__ int cls_count[G], cls_start[G];
+  TileWork<T> wk;
+  if (!map.fetch(g, wk)) return;
+  const int start = wk.start, cnt = wk.cnt, org0 = wk.org0, org1 = wk.org1;
+  const T uniform = wk.uniform;
+  const bool bad = map.nonfinite(wk);
+  const int nf0 = g.nf[0], nf1 = g.nf[1];
+  field += wk.grid_off;
   const int tid = threadIdx.x;
   if (tid < G) cls_count[tid] = 0;
   __syncthreads();
@@ -814,21 +852,6 @@ __device__ __forceinline__ void interp2d_tile_body(const Rec<2, T>* __restrict__
     const T wgt = (mode == INTERP_GRAD) ? (weights ? weights[r.idx] : uniform) : T(1);
     interp_store<2, T>(mode, r.idx, wgt, vr, vi, T(0), bad, grad, out2, accumulate, gs);
   }
-}
-
-template <int W, typename T>
-__global__ void __launch_bounds__(256) interp2d_tile_kernel(
-    const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, T uniform, const int* __restrict__ sub_bin,
-    const int* __restrict__ sub_start, const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g,
-    const EsPoly<W, T> poly, const cplx_t<T>* __restrict__ field, int mode, double* grad, double2* out2, int accumulate,
-    const int* __restrict__ status, const GradScale gs) {
-  const int sub = blockIdx.x;
-  if (sub >= *num_sub) return;
-  const bool bad = status != nullptr && ((*status) & STATUS_NONFINITE_INPUT);
-  const int bin = sub_bin[sub];
-  const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
-  interp2d_tile_body<W, T>(recs, weights, uniform, sub_start[sub], sub_count[sub], org0, org1, g.nf[0], g.nf[1], poly,
-                           field, mode, grad, out2, accumulate, bad, gs);
 }
 
 // Generic interpolation (1D, 3D): thread per sorted point, taps gathered
@@ -941,11 +964,11 @@ void launch_spread2d(const void* recs, const T* weights, T uniform, const cplx_t
                      const Geom& g, const std::vector<double>& poly, T* grid_real, cplx_t<T>* grid_cplx,
                      cudaStream_t s) {
   constexpr size_t smem = spread2d_smem_bytes<W, T, CPLX>();
-  auto kern = spread2d_tile_kernel<W, T, CPLX>;
+  auto kern = spread2d_tile_kernel<W, T, CPLX, TileMap1<T>>;
   if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  kern<<<unsigned(sb.max_sub), Tile2D<W>::THREADS, smem, s>>>(
-      static_cast<const Rec<2, T>*>(recs), weights, uniform, strengths, sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p,
-      sb.num_sub.p, sb.bin_start.p, g, make_es_poly<W, T>(poly), grid_real, grid_cplx);
+  const TileMap1<T> map{sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, sb.bin_start.p, nullptr, uniform};
+  kern<<<unsigned(sb.max_sub), Tile2D<W>::THREADS, smem, s>>>(static_cast<const Rec<2, T>*>(recs), weights, strengths,
+                                                              map, g, make_es_poly<W, T>(poly), grid_real, grid_cplx);
   FB_LAUNCH_CHECK();
 }
 
@@ -968,11 +991,11 @@ void launch_interp2d(const void* recs, const T* weights, T uniform, const SortBu
                      int acc, const int* status, cudaStream_t s, const GradScale& gs) {
   constexpr int TW = kTile2D + W;
   const size_t smem = sizeof(cplx_t<T>) * TW * TW + 2 * sizeof(uint16_t) * kMaxSub;
-  auto kern = interp2d_tile_kernel<W, T>;
+  auto kern = interp2d_tile_kernel<W, T, TileMap1<T>>;
   if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<2, T>*>(recs), weights, uniform, sb.sub_bin.p,
-                                                sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g,
-                                                make_es_poly<W, T>(poly), field, mode, grad, out2, acc, status, gs);
+  const TileMap1<T> map{sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, sb.bin_start.p, status, uniform};
+  kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<2, T>*>(recs), weights, map, g,
+                                                make_es_poly<W, T>(poly), field, mode, grad, out2, acc, gs);
   FB_LAUNCH_CHECK();
 }
 
