@@ -83,6 +83,8 @@ _SIGNATURES = {
     "fresco_ensemble_destroy": (None, [handle_t]),
     "fresco_ensemble_lbfgs_create": (C.c_int, [handle_t, c_double_p, c_int64, C.c_double, C.c_int, C.c_double,
                                                C.c_double, C.c_double, C.c_int, C.POINTER(handle_t)]),
+    "fresco_lbfgs_graph_create": (C.c_int, [handle_t, c_double_p, c_int64, C.c_double, C.c_int, C.c_double,
+                                            C.c_double, C.c_double, C.c_int, C.POINTER(handle_t)]),
     "fresco_ensemble_lbfgs_run": (C.c_int, [handle_t, C.c_int, c_int_p]),
     "fresco_ensemble_lbfgs_steps": (C.c_int, [handle_t, C.c_int]),
     "fresco_ensemble_lbfgs_state": (C.c_int, [handle_t, c_double_p, c_double_p, c_double_p, c_double_p, c_int_p,

@@ -571,6 +571,30 @@ int fresco_ensemble_lbfgs_create(fresco_ensemble h, const double* x0, int64_t n,
   });
 }
 
+int fresco_lbfgs_graph_create(fresco_potential p, const double* x0, int64_t n, double tol, int M, double maxstep,
+                              double max_f_rise, double H0, int rel_energy, fresco_ensemble_lbfgs* out) {
+  return guarded([&] {
+    if (!p || !x0 || !out) throw fb::InvalidArgument("null argument");
+    check_n(p, n);
+    fb::EnsembleLbfgsParams prm;
+    prm.tol = tol;
+    prm.M = M;
+    prm.maxstep = maxstep;
+    prm.max_f_rise = max_f_rise;
+    prm.H0 = H0;
+    prm.rel_energy = rel_energy != 0;
+    auto* o = new fresco_ensemble_lbfgs_s;
+    try {
+      o->opt.reset(new fb::EnsembleLbfgs(fb::make_potential_ensemble(p->pot, n), x0, n, prm));
+    } catch (...) {
+      delete o;
+      throw;
+    }
+    *out = o;
+    return FRESCO_OK;
+  });
+}
+
 int fresco_ensemble_lbfgs_run(fresco_ensemble_lbfgs o, int niter, int* steps_taken) {
   return guarded([&] {
     if (!o) throw fb::InvalidArgument("null argument");

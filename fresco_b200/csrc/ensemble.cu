@@ -16,6 +16,10 @@
 //   R2C      one batched cuFFT plan over the group's grids;
 //   modes    the NUwU mode pass of every pattern (its own V, S0, weights);
 //   C2C      one batched cuFFT plan over the packed type-2 fields;
+//            groups whose fine grid is N x N with N a power of two in
+//            512..8192 and whose active modes lie in a narrow band replace
+//            these three by the batched band transforms (band_fft.cuh), which
+//            only touch the columns |k_x| <= Kx the loss reads;
 //   interp   tiled or direct, as for the spread.
 #include <algorithm>
 #include <cmath>
@@ -23,6 +27,7 @@
 #include <string>
 #include <vector>
 
+#include "band_fft.cuh"
 #include "ensemble.cuh"
 #include "es.cuh"
 #include "nufft_kernels.cuh"
@@ -400,6 +405,14 @@ class NUwUEnsembleImpl final : public Ensemble {
     DevBuf<PointItem> pitems;
     int n_pitems = 0;
     cufftHandle r2c = 0, c2c = 0;
+    // band transforms
+    bool band = false;
+    int Kx = 0, Ky = 0;
+    DevBuf<cplx_t<T>> tw, band1, band2;
+    DevBuf<ModeCoef> coef_box;
+    DevBuf<double> invN;
+    DevBuf<int> pid;
+    size_t smem_rows = 0, smem_modes = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t join = nullptr;
   };
@@ -543,7 +556,9 @@ class NUwUEnsembleImpl final : public Ensemble {
       for (char d : gp->direct) nd += d ? 1 : 0;
       out += " [modes/dim=" + std::to_string(gp->n) + " nf=" + std::to_string(gp->geom.nf[0]) +
              " patterns=" + std::to_string(gp->P) + " points=" + std::to_string(gp->NG) +
-             " direct=" + std::to_string(nd) + "]";
+             " direct=" + std::to_string(nd) +
+             (gp->band ? " fft=band|kx|<=" + std::to_string(gp->Kx) + ",|ky|<=" + std::to_string(gp->Ky)
+                       : std::string(" fft=cufft")) + "]";
     }
     return out;
   }
@@ -616,10 +631,14 @@ class NUwUEnsembleImpl final : public Ensemble {
     gr.unsorted.alloc(size_t(gr.NG) * rb);
     gr.recs.alloc(size_t(gr.NG) * rb);
     gr.spread.alloc(size_t(gr.P) * gr.G);
-    gr.bhat.alloc(size_t(gr.P) * gr.GH);
-    gr.hgrid.alloc(size_t(gr.P) * gr.G);
-    FB_CUDA(cudaMemset(gr.hgrid.p, 0, gr.hgrid.bytes()));
+    FB_CUDA(cudaMemset(gr.spread.p, 0, gr.spread.bytes()));
     gr.ggrid.alloc(size_t(gr.P) * gr.G);
+    setup_band(gr, midx, mcoef);
+    if (!gr.band) {
+      gr.bhat.alloc(size_t(gr.P) * gr.GH);
+      gr.hgrid.alloc(size_t(gr.P) * gr.G);
+      FB_CUDA(cudaMemset(gr.hgrid.p, 0, gr.hgrid.bytes()));
+    }
     const std::vector<double> pc = es_correction(es_, nf, -gr.K, n);
     gr.corr.alloc(n);
     FB_CUDA(cudaMemcpy(gr.corr.p, pc.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
@@ -636,17 +655,114 @@ class NUwUEnsembleImpl final : public Ensemble {
     gr.pitems.alloc(std::max<int64_t>(npi, 1));
     gr.direct.assign(gr.P, 0);
     set_split(gr, 1.0);
-    // batched cuFFT plans (rows of nf, dims slowest first)
-    const bool f32 = sizeof(T) == 4;
-    int dims[2] = {int(nf), int(nf)};
-    int emb_r[2] = {int(nf), int(nf)}, emb_h[2] = {int(nf), gr.nh0};
-    FB_CUFFT(cufftPlanMany(&gr.r2c, 2, dims, emb_r, 1, int(gr.G), emb_h, 1, int(gr.GH), f32 ? CUFFT_R2C : CUFFT_D2Z,
-                           gr.P));
-    FB_CUFFT(cufftPlanMany(&gr.c2c, 2, dims, emb_r, 1, int(gr.G), emb_r, 1, int(gr.G), f32 ? CUFFT_C2C : CUFFT_Z2Z,
-                           gr.P));
+    if (!gr.band) {  // batched cuFFT plans (rows of nf, dims slowest first)
+      const bool f32 = sizeof(T) == 4;
+      int dims[2] = {int(nf), int(nf)};
+      int emb_r[2] = {int(nf), int(nf)}, emb_h[2] = {int(nf), gr.nh0};
+      FB_CUFFT(cufftPlanMany(&gr.r2c, 2, dims, emb_r, 1, int(gr.G), emb_h, 1, int(gr.GH),
+                             f32 ? CUFFT_R2C : CUFFT_D2Z, gr.P));
+      FB_CUFFT(cufftPlanMany(&gr.c2c, 2, dims, emb_r, 1, int(gr.G), emb_r, 1, int(gr.G),
+                             f32 ? CUFFT_C2C : CUFFT_Z2Z, gr.P));
+    }
     FB_CUDA(cudaStreamCreateWithFlags(&gr.stream, cudaStreamNonBlocking));
     FB_CUDA(cudaEventCreateWithFlags(&gr.join, cudaEventDisableTiming));
     smem_attrs();
+  }
+
+  // Band transforms for the group when its grid and active modes allow them
+  // (the same conditions as the single-pattern potential).
+  void setup_band(Group& gr, const std::vector<int>& midx, const std::vector<ModeCoef>& mcoef) {
+    gr.band = false;
+    const int nf = gr.geom.nf[0];
+    if (midx.empty() || nf < 512 || nf > 8192 || (nf & (nf - 1)) != 0) return;
+    if (3 * size_t(fft_padded(nf)) * sizeof(cplx_t<T>) > 200 * 1024) return;
+    int kxm = 0, kym = 0;
+    for (int m : midx) {
+      kxm = std::max(kxm, std::abs(m % gr.n - gr.K));
+      kym = std::max(kym, std::abs(m / gr.n - gr.K));
+    }
+    if (2 * kxm + 1 > nf / 2) return;
+    gr.Kx = kxm;
+    gr.Ky = kym;
+    const int NX = 2 * kxm + 1, NY = 2 * kym + 1;
+    std::vector<ModeCoef> box(size_t(gr.P) * NX * NY, ModeCoef{0.0, 0.0, 0.0, 0.0});
+    std::vector<double> invn(gr.P);
+    std::vector<int> pid(gr.P);
+    for (int l = 0; l < gr.P; ++l) {
+      const PatInfo& pi = gr.pats_h[l];
+      invn[l] = pi.invN;
+      pid[l] = pi.pid;
+      for (int i = 0; i < pi.n_active; ++i) {
+        const int m = midx[size_t(pi.mode_base) + i];
+        const int kx = m % gr.n - gr.K, ky = m / gr.n - gr.K;
+        box[size_t(l) * NX * NY + size_t(kx + kxm) * NY + (ky + kym)] = mcoef[size_t(pi.mode_base) + i];
+      }
+    }
+    gr.coef_box.alloc(box.size());
+    FB_CUDA(cudaMemcpy(gr.coef_box.p, box.data(), sizeof(ModeCoef) * box.size(), cudaMemcpyHostToDevice));
+    gr.invN.alloc(gr.P);
+    FB_CUDA(cudaMemcpy(gr.invN.p, invn.data(), sizeof(double) * gr.P, cudaMemcpyHostToDevice));
+    gr.pid.alloc(gr.P);
+    FB_CUDA(cudaMemcpy(gr.pid.p, pid.data(), sizeof(int) * gr.P, cudaMemcpyHostToDevice));
+    const std::vector<double> t = fft_twiddles(nf);
+    std::vector<cplx_t<T>> h(nf);
+    for (int j = 0; j < nf; ++j) {
+      h[j].x = T(t[2 * size_t(j)]);
+      h[j].y = T(t[2 * size_t(j) + 1]);
+    }
+    gr.tw.alloc(nf);
+    FB_CUDA(cudaMemcpy(gr.tw.p, h.data(), sizeof(cplx_t<T>) * nf, cudaMemcpyHostToDevice));
+    gr.band1.alloc(size_t(gr.P) * (kxm + 1) * nf);
+    gr.band2.alloc(size_t(gr.P) * nf * NX);
+    gr.smem_rows = 2 * size_t(fft_padded(nf)) * sizeof(cplx_t<T>);
+    gr.smem_modes = 3 * size_t(fft_padded(nf)) * sizeof(cplx_t<T>);
+    switch (nf) {
+      case 512: band_attrs<512>(gr); break;
+      case 1024: band_attrs<1024>(gr); break;
+      case 2048: band_attrs<2048>(gr); break;
+      case 4096: band_attrs<4096>(gr); break;
+      default: band_attrs<8192>(gr); break;
+    }
+    gr.band = true;
+  }
+
+  template <int N>
+  void band_attrs(const Group& gr) {
+    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(band_rows_r2c_kernel<T, N>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(gr.smem_rows)));
+    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(band_rows_c2c_kernel<T, N>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(gr.smem_rows)));
+    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(band_modes_kernel<T, N>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(gr.smem_modes)));
+  }
+
+  template <int N>
+  void run_band_n(Group& gr, double* g, double* e, cudaStream_t s) {
+    const dim3 blk(N / 16, 2);
+    const int NX = 2 * gr.Kx + 1, NY = 2 * gr.Ky + 1;
+    const BandBatch<T> bb{gr.spread.p, gr.G,         gr.band1.p,           int64_t(gr.Kx + 1) * N,
+                          gr.band2.p,  int64_t(N) * NX, gr.ggrid.p,        gr.G,
+                          gr.coef_box.p, int64_t(NX) * NY, gr.invN.p,      0.0,
+                          e,           cur_status_.p, gr.pid.p};
+    band_rows_r2c_kernel<T, N><<<dim3(N / 4, gr.P), blk, gr.smem_rows, s>>>(gr.spread.p, gr.G, gr.tw.p, gr.Kx + 1,
+                                                                           gr.band1.p, int64_t(gr.Kx + 1) * N);
+    FB_LAUNCH_CHECK();
+    band_modes_kernel<T, N><<<dim3(gr.Kx + 1, gr.P), blk, gr.smem_modes, s>>>(bb, gr.tw.p, gr.Kx, gr.Ky, gr.K,
+                                                                              gr.corr.p, gr.corr.p, g != nullptr);
+    FB_LAUNCH_CHECK();
+    if (!g) return;
+    band_rows_c2c_kernel<T, N><<<dim3(N / 2, gr.P), blk, gr.smem_rows, s>>>(bb, gr.Kx, gr.tw.p);
+    FB_LAUNCH_CHECK();
+  }
+
+  void run_band(Group& gr, double* g, double* e, cudaStream_t s) {
+    switch (gr.geom.nf[0]) {
+      case 512: run_band_n<512>(gr, g, e, s); break;
+      case 1024: run_band_n<1024>(gr, g, e, s); break;
+      case 2048: run_band_n<2048>(gr, g, e, s); break;
+      case 4096: run_band_n<4096>(gr, g, e, s); break;
+      default: run_band_n<8192>(gr, g, e, s); break;
+    }
   }
 
   // Patterns whose tap work N w^2 is below ratio x (tile cells of all bins)
@@ -721,7 +837,7 @@ class NUwUEnsembleImpl final : public Ensemble {
         uns, gr.items.p, gr.pats.p, geo, gr.bin_total.p, gr.blk_off.p, gr.bin_start.p, gr.sub_bin.p, gr.sub_start.p,
         gr.sub_count.p, gr.num_sub.p, gr.done.p, recs, sticky_.p);
     FB_LAUNCH_CHECK();
-    FB_CUDA(cudaMemsetAsync(gr.spread.p, 0, gr.spread.bytes(), s));
+    if (!gr.band) FB_CUDA(cudaMemsetAsync(gr.spread.p, 0, gr.spread.bytes(), s));  // the band row pass re-zeroes
     const EsPoly<W, T> poly = make_es_poly<W, T>(poly_);
     const EnsTileMap<T> map{gr.pats.p,     gr.tab.p,       gr.sub_bin.p, gr.sub_start.p, gr.sub_count.p,
                             gr.num_sub.p, gr.bin_start.p, cur_status_.p, gr.G};
@@ -736,27 +852,32 @@ class NUwUEnsembleImpl final : public Ensemble {
                                                                         geo, poly, gr.spread.p, gr.G);
       FB_LAUNCH_CHECK();
     }
-    FB_CUFFT(cufftSetStream(gr.r2c, s));
-    if (sizeof(T) == 4) {
-      FB_CUFFT(cufftExecR2C(gr.r2c, reinterpret_cast<cufftReal*>(gr.spread.p),
-                            reinterpret_cast<cufftComplex*>(gr.bhat.p)));
+    if (gr.band) {
+      run_band(gr, g, e, s);
+      if (!g) return;
     } else {
-      FB_CUFFT(cufftExecD2Z(gr.r2c, reinterpret_cast<cufftDoubleReal*>(gr.spread.p),
-                            reinterpret_cast<cufftDoubleComplex*>(gr.bhat.p)));
-    }
-    const int gx = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(gr.max_active, 256), 64)));
-    ens_modes_kernel<T><<<dim3(gx, gr.P), 256, 0, s>>>(gr.pats.p, gr.mode_idx.p, gr.coef.p, gr.n, gr.K, gr.bhat.p,
-                                                       gr.nh0, gr.GH, geo.nf[0], gr.corr.p, gr.hgrid.p, gr.G, e,
-                                                       cur_status_.p, g != nullptr);
-    FB_LAUNCH_CHECK();
-    if (!g) return;
-    FB_CUFFT(cufftSetStream(gr.c2c, s));
-    if (sizeof(T) == 4) {
-      FB_CUFFT(cufftExecC2C(gr.c2c, reinterpret_cast<cufftComplex*>(gr.hgrid.p),
-                            reinterpret_cast<cufftComplex*>(gr.ggrid.p), CUFFT_FORWARD));
-    } else {
-      FB_CUFFT(cufftExecZ2Z(gr.c2c, reinterpret_cast<cufftDoubleComplex*>(gr.hgrid.p),
-                            reinterpret_cast<cufftDoubleComplex*>(gr.ggrid.p), CUFFT_FORWARD));
+      FB_CUFFT(cufftSetStream(gr.r2c, s));
+      if (sizeof(T) == 4) {
+        FB_CUFFT(cufftExecR2C(gr.r2c, reinterpret_cast<cufftReal*>(gr.spread.p),
+                              reinterpret_cast<cufftComplex*>(gr.bhat.p)));
+      } else {
+        FB_CUFFT(cufftExecD2Z(gr.r2c, reinterpret_cast<cufftDoubleReal*>(gr.spread.p),
+                              reinterpret_cast<cufftDoubleComplex*>(gr.bhat.p)));
+      }
+      const int gx = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(gr.max_active, 256), 64)));
+      ens_modes_kernel<T><<<dim3(gx, gr.P), 256, 0, s>>>(gr.pats.p, gr.mode_idx.p, gr.coef.p, gr.n, gr.K, gr.bhat.p,
+                                                         gr.nh0, gr.GH, geo.nf[0], gr.corr.p, gr.hgrid.p, gr.G, e,
+                                                         cur_status_.p, g != nullptr);
+      FB_LAUNCH_CHECK();
+      if (!g) return;
+      FB_CUFFT(cufftSetStream(gr.c2c, s));
+      if (sizeof(T) == 4) {
+        FB_CUFFT(cufftExecC2C(gr.c2c, reinterpret_cast<cufftComplex*>(gr.hgrid.p),
+                              reinterpret_cast<cufftComplex*>(gr.ggrid.p), CUFFT_FORWARD));
+      } else {
+        FB_CUFFT(cufftExecZ2Z(gr.c2c, reinterpret_cast<cufftDoubleComplex*>(gr.hgrid.p),
+                              reinterpret_cast<cufftDoubleComplex*>(gr.ggrid.p), CUFFT_FORWARD));
+      }
     }
     if (gr.n_tab) {
       constexpr int TW = kTile2D + W;

@@ -78,6 +78,11 @@ class Ensemble {
 
 using EnsemblePtr = std::shared_ptr<Ensemble>;
 
+class Potential;
+// Any single potential seen as a one-pattern ensemble, so that EnsembleLbfgs
+// gives it a device-resident, graph-captured LBFGS.
+EnsemblePtr make_potential_ensemble(std::shared_ptr<Potential> pot, int64_t n);
+
 // radii: sum N_p values (pattern order); sk, v: sum n_modes[p] values.
 EnsemblePtr make_nuwu_ensemble(int n_patterns, const int64_t* n_points, const double* radii, const int64_t* n_modes,
                                const double* sk, const double* v, const double* L, int ndim, double eps,

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "ensemble.cuh"
+#include "potential.cuh"
 
 namespace fb {
 
@@ -348,6 +349,32 @@ __global__ void bl_finalize(BlState* st, const double* __restrict__ e, double* r
 
 }  // namespace
 
+// One potential as a one-pattern ensemble: eval calls the potential's own
+// launches (not its graph cache), so they are captured into the LBFGS step.
+class PotentialEnsemble final : public Ensemble {
+ public:
+  PotentialEnsemble(PotentialPtr pot, int64_t n) : pot_(std::move(pot)) {
+    if (!pot_) throw InvalidArgument("null potential");
+    if (n <= 0) throw InvalidArgument("empty coordinate array");
+    if (pot_->ndof() >= 0 && pot_->ndof() != n) throw InvalidArgument("x0 has the wrong size for the potential");
+    dof_off_ = {0, n};
+  }
+  void eval(const double* x, double* g, double* e, cudaStream_t s) override {
+    if (g) {
+      pot_->energy_gradient(x, ndof(), g, e, false, s);
+    } else {
+      pot_->energy(x, ndof(), e, false, s);
+    }
+  }
+  void read_and_clear_status(int* out, cudaStream_t s) override { out[0] = pot_->read_and_clear_status(s); }
+  void tune(const double*, double*, double*, cudaStream_t) override {}
+  void set_split(double) override {}
+  std::string describe() const override { return pot_->describe(); }
+
+ private:
+  PotentialPtr pot_;
+};
+
 struct EnsembleLbfgs::Impl {
   EnsemblePtr ens;
   EnsembleLbfgsParams prm;
@@ -532,6 +559,10 @@ void EnsembleLbfgs::get_state(double* x, double* g, double* f, double* rms, int*
     if (nfev) nfev[q] = hs[q].nfev;
     if (active) active[q] = hs[q].active;
   }
+}
+
+EnsemblePtr make_potential_ensemble(std::shared_ptr<Potential> pot, int64_t n) {
+  return EnsemblePtr(new PotentialEnsemble(std::move(pot), n));
 }
 
 }  // namespace fb

@@ -28,7 +28,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import check, dptr, lib
-from .optimize import Result
+from .optimize import DeviceLBFGS, Result
 from .potentials import _f64, _precision
 
 __all__ = ["NUwUEnsemble", "EnsembleLBFGS", "pattern_cost", "shard_patterns", "gather_results"]
@@ -164,7 +164,7 @@ class NUwUEnsemble:
         return buf.value.decode()
 
 
-class EnsembleLBFGS:
+class EnsembleLBFGS(DeviceLBFGS):
     """``LBFGS_CPP.run(niter)`` for every pattern of a ``NUwUEnsemble`` at once.
 
     Parameters and defaults as fresco/optimize/_lbfgs_cpp.pyx:43 (tol, M,
@@ -177,46 +177,13 @@ class EnsembleLBFGS:
             raise TypeError("ensemble must be a NUwUEnsemble")
         self.ensemble = ensemble
         x = ensemble.concat(x0)
+        self._ndof = x.size
+        self._npat = ensemble.n_patterns
         self.tol = float(tol)
         h = _lib.handle_t()
         check(lib.fresco_ensemble_lbfgs_create(ensemble.handle, dptr(x), x.size, self.tol, int(M), float(maxstep),
                                                float(maxErise), float(H0), int(bool(rel_energy)), C.byref(h)))
         self._h = h
-
-    def __del__(self):
-        h, self._h = getattr(self, "_h", None), None
-        if h:
-            try:
-                lib.fresco_ensemble_lbfgs_destroy(h)
-            except Exception:
-                pass
-
-    def run(self, niter):
-        """Every pattern iterates until rms <= tol or ``niter`` more iterations; returns the steps used."""
-        steps = C.c_int(0)
-        check(lib.fresco_ensemble_lbfgs_run(self._h, int(niter), C.byref(steps)))
-        return steps.value
-
-    def steps(self, n):
-        """Exactly ``n`` ensemble steps (one evaluation of every pattern each)."""
-        check(lib.fresco_ensemble_lbfgs_steps(self._h, int(n)))
-
-    def state(self, with_vectors=True):
-        P = self.ensemble.n_patterns
-        n = self.ensemble.ndof
-        x = np.empty(n) if with_vectors else None
-        g = np.empty(n) if with_vectors else None
-        f = np.empty(P)
-        rms = np.empty(P)
-        it = np.zeros(P, dtype=np.int32)
-        nfev = np.zeros(P, dtype=np.int32)
-        active = np.zeros(P, dtype=np.int32)
-        ip = C.POINTER(C.c_int)
-        check(lib.fresco_ensemble_lbfgs_state(self._h, dptr(x) if with_vectors else None,
-                                              dptr(g) if with_vectors else None, dptr(f), dptr(rms),
-                                              it.ctypes.data_as(ip), nfev.ctypes.data_as(ip),
-                                              active.ctypes.data_as(ip)))
-        return x, g, f, rms, it, nfev, active
 
     def get_results(self):
         """One ``Result`` per pattern, as ``LBFGS_CPP.get_result()`` (opt.pyx:81-93)."""

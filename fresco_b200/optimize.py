@@ -23,7 +23,7 @@ from . import _lib
 from ._lib import check, dptr, lib
 from .potentials import BasePotential
 
-__all__ = ["Result", "GradientOptimizer", "LBFGS_CPP", "ModifiedFireCPP"]
+__all__ = ["Result", "GradientOptimizer", "LBFGS_CPP", "ModifiedFireCPP", "LBFGS_Graph"]
 
 
 class Result(dict):
@@ -209,3 +209,83 @@ class ModifiedFireCPP(GradientOptimizer):
             g = np.ascontiguousarray(np.asarray(gradient, dtype=np.float64).ravel())
             check(lib.fresco_optimizer_set_func_gradient(self._h, float(energy), dptr(g), g.size))
         self.events = [] if events is None else events
+
+
+class DeviceLBFGS:
+    """Driver of the device-state LBFGS (ensemble_lbfgs.cu): every pattern's
+    iteration (lbfgs.cpp:9-258) is a state machine on the device, and one
+    step (one evaluation of every pattern) is one CUDA graph launch."""
+
+    _h = None
+    _ndof = 0
+    _npat = 1
+
+    def __del__(self):
+        h, self._h = self._h, None
+        if h:
+            try:
+                lib.fresco_ensemble_lbfgs_destroy(h)
+            except Exception:
+                pass
+
+    def run(self, niter):
+        """Every pattern iterates until rms <= tol or ``niter`` more iterations
+        (optimizer.hpp:97-112); returns the number of evaluation steps used."""
+        steps = C.c_int(0)
+        check(lib.fresco_ensemble_lbfgs_run(self._h, int(niter), C.byref(steps)))
+        return steps.value
+
+    def steps(self, n):
+        """Exactly ``n`` steps (one evaluation of every pattern each)."""
+        check(lib.fresco_ensemble_lbfgs_steps(self._h, int(n)))
+
+    def state(self, with_vectors=True):
+        """(x, g, f, rms, iterations, evaluations, active) with per-pattern arrays."""
+        P, n = self._npat, self._ndof
+        x = np.empty(n) if with_vectors else None
+        g = np.empty(n) if with_vectors else None
+        f = np.empty(P)
+        rms = np.empty(P)
+        it = np.zeros(P, dtype=np.int32)
+        nfev = np.zeros(P, dtype=np.int32)
+        active = np.zeros(P, dtype=np.int32)
+        ip = C.POINTER(C.c_int)
+        check(lib.fresco_ensemble_lbfgs_state(self._h, dptr(x) if with_vectors else None,
+                                              dptr(g) if with_vectors else None, dptr(f), dptr(rms),
+                                              it.ctypes.data_as(ip), nfev.ctypes.data_as(ip),
+                                              active.ctypes.data_as(ip)))
+        return x, g, f, rms, it, nfev, active
+
+
+class LBFGS_Graph(DeviceLBFGS):
+    """``LBFGS_CPP`` (fresco/optimize/_lbfgs_cpp.pyx:38-84) with the whole iteration on the device.
+
+    Same parameters, iterations, evaluation counts and trajectory as
+    ``LBFGS_CPP``; ``run(niter)`` replays one CUDA graph per evaluation
+    (direction, trial point, potential, accept test, memory update) and reads
+    the iteration state back only every few evaluations.  No per-iteration
+    printing or event callbacks.
+    """
+
+    def __init__(self, x0, potential, tol=1e-5, M=4, maxstep=0.1, maxErise=1e-4, H0=0.1, rel_energy=False):
+        self.pot = _as_potential(potential)
+        x = np.ascontiguousarray(np.asarray(x0, dtype=np.float64).ravel())
+        self._ndof = x.size
+        self.tol = float(tol)
+        h = _lib.handle_t()
+        check(lib.fresco_lbfgs_graph_create(self.pot.handle, dptr(x), x.size, self.tol, int(M), float(maxstep),
+                                            float(maxErise), float(H0), int(bool(rel_energy)), C.byref(h)))
+        self._h = h
+
+    def get_result(self):
+        x, g, f, rms, it, nfev, _ = self.state(True)
+        res = Result()
+        res.energy = float(f[0])
+        res.coords = x
+        res.grad = g
+        res.rms = float(rms[0])
+        res.nsteps = int(it[0])
+        res.nfev = int(nfev[0])
+        res.success = bool(rms[0] <= self.tol)
+        return res
+

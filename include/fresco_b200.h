@@ -253,6 +253,12 @@ void fresco_ensemble_destroy(fresco_ensemble h);
  * source/lbfgs.cpp:9-258); x0 in the ensemble's layout. */
 int fresco_ensemble_lbfgs_create(fresco_ensemble h, const double* x0, int64_t n, double tol, int M, double maxstep,
                                  double max_f_rise, double H0, int rel_energy, fresco_ensemble_lbfgs* out);
+/* LBFGS_CPP(x0, potential, ...) (fresco/optimize/_lbfgs_cpp.pyx:22-66,
+ * source/lbfgs.cpp:9-258) for any single potential with its whole iteration
+ * on the device: a one-pattern ensemble optimiser, driven by the
+ * fresco_ensemble_lbfgs_* calls below (one CUDA graph launch per evaluation). */
+int fresco_lbfgs_graph_create(fresco_potential p, const double* x0, int64_t n, double tol, int M, double maxstep,
+                              double max_f_rise, double H0, int rel_energy, fresco_ensemble_lbfgs* out);
 /* run(niter) of every pattern (optimizer.hpp:97-112); steps_taken (may be
  * NULL) receives the number of ensemble evaluations used. */
 int fresco_ensemble_lbfgs_run(fresco_ensemble_lbfgs o, int niter, int* steps_taken);

@@ -9,7 +9,9 @@ pytestmark = pytest.mark.gpu
 
 # (N, K, kmax, polydisperse radii): mixed point counts and mode grids, several patterns per grid
 SPECS = [(40, 8, 4, False), (3000, 8, 5, True), (700, 16, 8, False), (20000, 16, 6, False), (5000, 32, 12, True),
-         (150, 32, 10, False), (9000, 4, 2, False), (60000, 64, 20, False)]
+         (150, 32, 10, False), (9000, 4, 2, False), (60000, 64, 20, False),
+         # 512^2 and 1024^2 fine grids: the batched band transforms (per-pattern active bands differ)
+         (4000, 128, 30, False), (500, 128, 16, True), (30000, 256, 64, False), (2000, 256, 40, False)]
 
 
 def rel(a, b):
@@ -40,6 +42,7 @@ def test_ensemble_matches_single_patterns(precision, eps, tol, split):
     L = np.full(2, 2 * np.pi)
     xs, radii, Ks, Sks, Vs = patterns(SPECS, L, seed=3)
     ens = NUwUEnsemble(radii, Ks, Sks, Vs, L, eps=eps, precision=precision)
+    assert ens.describe().count("fft=band") == 2, ens.describe()
     if split == "tune":
         ens.tune(xs)
     else:
