@@ -204,6 +204,48 @@ class NUwU:
             grad[a :: self.ndim] = np.real(cx * np.conj(self.c))
         return phi, grad
 
+    def active_modes(self):
+        """Flat indices of the modes with V != 0 and their integer k, shape (ndim, A)."""
+        n = self.n
+        act = np.nonzero(self.V[: self.nm])[0]
+        comps = [self.kvec[act % n]]
+        if self.ndim >= 2:
+            comps.append(self.kvec[(act // n) % n])
+        if self.ndim == 3:
+            comps.append(self.kvec[act // (n * n)])
+        return act, np.stack(comps).astype(np.float64)
+
+    def get_energy_gradient_active(self, points, chunk=1 << 15):
+        """``get_energy_gradient`` summed over the modes with V != 0 only (still exact).
+
+        A mode with V = 0 adds nothing to phi (nuwu.hpp:270) and its residual
+        factor (nuwu.hpp:273-276) is zero, so it drops out of the d type-2
+        transforms (nuwu.hpp:291-315).  Restricting the sums to the active
+        modes gives the same energy and gradient in O(N * active) work, which
+        keeps full-size point sets (N ~ 10^6) checkable when V is sparse.
+        The gradient map (nuwu.hpp:216-250) is used for rho, as in
+        get_energy_gradient.
+        """
+        x = coord_map(points, self.L, energy=False)  # (ndim, N)
+        act, kk = self.active_modes()
+        rho = np.zeros(act.size, dtype=np.complex128)
+        for s in range(0, self.N, chunk):
+            ph = x[:, s : s + chunk].T @ kk
+            rho += self.c[s : s + chunk] @ np.exp(1j * ph)
+        sk0 = self.Sk[: self.nm][act]
+        v = self.V[: self.nm][act]
+        d, phi = _loss_terms(np.abs(rho) ** 2 / self.N, sk0, v)
+        factor = (4.0 / self.N) * v * d * rho
+        factor = np.where(sk0 != 0, factor / np.where(sk0 != 0, sk0, 1.0), factor)
+        fa = (-1j * kk * factor[None, :]).T  # (A, ndim): -i k_a F(k)
+        grad = np.zeros(self.N * self.ndim)
+        g = grad.reshape(-1, self.ndim)
+        for s in range(0, self.N, chunk):
+            e = np.exp(-1j * (x[:, s : s + chunk].T @ kk))  # iflag -1
+            cx = e @ fa  # (chunk, ndim)
+            g[s : s + chunk] = np.real(cx * np.conj(self.c[s : s + chunk])[:, None])
+        return phi, grad
+
 
 class UwU:
     """Uniform grid -> uniform k-grid loss (source/fresco/uwu.hpp:17-195).
@@ -269,6 +311,31 @@ class UwNU:
         f = np.where(self.Sk != 0, f / np.where(self.Sk != 0, self.Sk, 1.0), f)
         c = nudft1(self.kt, f, self.N[: self.ndim], -1)
         return phi, np.real(c) / TWO_PI
+
+    def get_energy_gradient_active(self, points):
+        """``get_energy_gradient`` over the k-points with V != 0 only (2D, exact).
+
+        k-points with V = 0 add nothing to phi and have a zero residual
+        f = 4 V d rho / S0' (uwnu.hpp:314-349), so they drop out of the
+        type-1 transform back to the grid (uwnu.hpp:350-355).  The sums over
+        the grid are separable, exp(i (k0 m0 + k1 m1)) = exp(i k0 m0)
+        exp(i k1 m1), so rho and the gradient are two matrix products each:
+        O(G * active) work for a full-size grid.
+        """
+        if self.ndim != 2:
+            raise ValueError("active-k-point sums are written for 2D grids")
+        act = np.nonzero(self.V)[0]
+        k0, k1 = self.kt[0][act], self.kt[1][act]
+        m0, m1 = mode_values(self.N[0]), mode_values(self.N[1])
+        grid = np.asarray(points, dtype=np.float64).reshape(self.N[1], self.N[0])  # dim 0 fastest
+        b = grid @ np.exp(1j * np.outer(m0, k0))  # (N1, A), iflag +1
+        rho = np.sum(b * np.exp(1j * np.outer(m1, k1)), axis=0)
+        sk0, v = self.Sk[act], self.V[act]
+        d, phi = _loss_terms(np.abs(rho) ** 2, sk0, v)
+        f = 4.0 * v * d * rho
+        f = np.where(sk0 != 0, f / np.where(sk0 != 0, sk0, 1.0), f)
+        c = (np.exp(-1j * np.outer(m1, k1)) * f[None, :]) @ np.exp(-1j * np.outer(k0, m0))  # iflag -1
+        return phi, np.real(c).ravel() / TWO_PI
 
 
 class NUwNU:
@@ -368,6 +435,46 @@ class InversePower:
 
     def get_energy(self, x):
         return self.get_energy_gradient(x)[0]
+
+    def get_energy_gradient_tree(self, x):
+        """The same pair sum with the candidate pairs found by a k-d tree (scipy).
+
+        Only pairs closer than twice the largest radius can interact, so
+        searching them with scipy's ``cKDTree`` (periodic ``boxsize`` for the
+        periodic box) leaves the O(N^2) restatement above unchanged in value
+        (summation order aside) and makes N ~ 10^6 checkable.  The pair
+        vectors and the min-image rule are those of ``_pairs``.
+        """
+        from scipy.spatial import cKDTree
+
+        x = np.asarray(x, dtype=np.float64)
+        if not (np.isfinite(x[0]) and np.isfinite(x[-1])):
+            return float("nan"), np.full(x.size, np.nan)
+        p = x.reshape(-1, self.ndim)
+        if self.periodic:
+            w = p - np.floor(p / self.boxv) * self.boxv
+            w = np.where((w >= self.boxv) | (w < 0), 0.0, w)
+            tree = cKDTree(w, boxsize=self.boxv)
+        else:
+            tree = cKDTree(p)
+        ij = tree.query_pairs(2.0 * float(np.max(self.radii)) * (1 + 1e-9), output_type="ndarray")
+        i, j = ij[:, 0], ij[:, 1]
+        dr = p[i] - p[j]
+        if self.periodic:
+            dr = dr - _round_half_even(dr / self.boxv) * self.boxv
+        r2 = np.sum(dr * dr, axis=1)
+        rs = self.radii[i] + self.radii[j]
+        m = r2 < rs * rs
+        r = np.sqrt(r2[m])
+        rsm = rs[m]
+        factor = np.power(1.0 - r / rsm, self.a) * self.eps
+        e = float(np.sum(factor / self.a))
+        gij = -factor / ((r - rsm) * r)
+        contrib = dr[m] * gij[:, None]
+        n = p.shape[0]
+        g = np.stack([np.bincount(i[m], -contrib[:, a], minlength=n) + np.bincount(j[m], contrib[:, a], minlength=n)
+                      for a in range(self.ndim)], axis=1)
+        return e, g.ravel()
 
 
 class CombinedPotential:

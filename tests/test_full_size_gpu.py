@@ -1,0 +1,326 @@
+"""Parity at the benchmark configurations' full sizes (2D N = 2^20, 3D N = 2^21, 4096^2 and 2048^2 grids).
+
+Exact FP64 sums over every mode are out of reach at 10^6 points x 10^6 modes, so the exact oracle is
+restricted to what the loss uses: with V non-zero on a sparse set of modes (or k-points), only those
+enter the energy and the gradient, and the oracle's active-mode sums stay exact
+(``oracle.NUwU.get_energy_gradient_active``, ``oracle.UwNU.get_energy_gradient_active``, pinned to the
+full sums by tests/test_oracle_golden.py).  The device still runs its whole pipeline at full size:
+every point is spread on the full fine grid, the fine-grid transforms are full size, and every point
+is interpolated.  Size-independent checks complete it: the FP32 form against the FP64 form at
+eps = 1e-12 for the dense benchmark targets, central differences of the device energy (3D), a k-d-tree
+pair search for the 2^20-point repulsion, and FIRE steps on the 4096^2 grid.
+
+Each check prints one ``ACCURACY`` line (run with ``-s`` to see them).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TWO_PI = 2 * np.pi
+# (precision, eps, relative tolerance on the energy and on the gradient's 2-norm)
+PRECISIONS = [("fp64", 1e-12, 1e-10), ("fp32", 1e-6, 1e-5)]
+
+
+_ORACLE = {}  # oracle results shared by the FP64 and FP32 cases of one test
+
+
+def _oracle(key, fn):
+    if key not in _ORACLE:
+        _ORACLE[key] = fn()
+    return _ORACLE[key]
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def _report(name, e, e_ref, g, g_ref):
+    de, dg = abs(e - e_ref) / abs(e_ref), _rel(g, g_ref)
+    print(f"ACCURACY {name}: energy_rel_err={de:.3e} grad_rel_err={dg:.3e}")
+    return de, dg
+
+
+def _kgrid(n, ndim):
+    kv = np.arange(n) - n // 2
+    comps = np.meshgrid(*([kv] * ndim), indexing="ij")[::-1]  # flat index: dim 0 fastest
+    return [c.ravel().astype(np.float64) for c in comps]
+
+
+def _sparse_modes(rng, n, ndim, kmax, count, edge):
+    """Flat indices of `count` random modes with 0 < |k| <= kmax plus the given edge modes."""
+    k = _kgrid(n, ndim)
+    mag = np.sqrt(sum(c * c for c in k))
+    cand = np.nonzero((mag > 0) & (mag <= kmax))[0]
+    pick = set(rng.choice(cand, count, replace=False).tolist())
+    K = n // 2
+    for e in edge:
+        pick.add(int(sum((e[a] + K) * n ** a for a in range(ndim))))
+    return np.array(sorted(pick))
+
+
+# ---------------------------------------------------------------------------
+# config 2: 2D NUwU, N = 1,048,576, 1025^2 modes, S0 = 0 on 0 < |k| <= 256; harmonic repulsion
+# ---------------------------------------------------------------------------
+
+N2, K2, KMAX2 = 1 << 20, 512, 256
+
+
+@pytest.fixture(scope="module")
+def config2_points():
+    return np.random.default_rng(2).random(2 * N2) * TWO_PI
+
+
+@pytest.mark.parametrize("prec,eps,tol", PRECISIONS)
+def test_config2_nuwu_sparse_modes_exact(config2_points, prec, eps, tol):
+    """68 active modes (random in the stealthy disc plus the band's corners), random V and S0 (half
+    zero): device energy and gradient against the exact active-mode sums at N = 2^20."""
+    from fresco_b200 import NUwU
+
+    n = 2 * K2 + 1
+    rng = np.random.default_rng(20)
+    act = _sparse_modes(rng, n, 2, KMAX2, 64, [(256, 0), (0, -256), (-181, 181), (181, -181)])
+    V = np.zeros(n * n)
+    Sk = np.zeros(n * n)
+    V[act] = 0.5 + rng.random(act.size)
+    Sk[act] = np.where(rng.random(act.size) < 0.5, 0.0, 0.5 + rng.random(act.size))
+    L = np.full(2, TWO_PI)
+    radii = np.ones(N2)
+    pot = NUwU(radii, K2, Sk, V, L, eps=eps, precision=prec)
+    assert "fft=band|kx|<=256,|ky|<=256" in pot.describe(), pot.describe()
+    e, g = pot.get_energy_gradient(config2_points)
+    assert pot.status() == 0
+    e_ref, g_ref = _oracle("c2", lambda: O.NUwU(radii, K2, Sk, V, L).get_energy_gradient_active(config2_points))
+    de, dg = _report(f"config2 NUwU 68 active modes {prec} eps={eps:g}", e, e_ref, g, g_ref)
+    assert de <= tol and dg <= tol
+
+
+def test_config2_nuwu_dense_fp32_against_fp64(config2_points):
+    """The benchmark's own targets (V = 1 on every mode of the disc): the FP32 form and the FP64 form at
+    eps = 1e-6 against the FP64 form at eps = 1e-12, within 1e-5 (the FP32 gradient bound)."""
+    from fresco_b200 import NUwU
+
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(4, K2, KMAX2, ndim=2, seed=2)
+    radii = np.ones(N2)
+    e_ref, g_ref = NUwU(radii, K2, Sk, V, L, eps=1e-12, precision="fp64").get_energy_gradient(config2_points)
+    for prec in ("fp32", "fp64"):
+        pot = NUwU(radii, K2, Sk, V, L, eps=1e-6, precision=prec)
+        e, g = pot.get_energy_gradient(config2_points)
+        de, dg = _report(f"config2 NUwU dense {prec} eps=1e-6 vs fp64 eps=1e-12", e, e_ref, g, g_ref)
+        assert de <= 1e-5 and dg <= 1e-5
+
+
+def test_config2_repulsion_and_combined(config2_points):
+    """Harmonic repulsion with diameter 0.5/sqrt(N) 2 pi at N = 2^20 against the oracle's pair sum (k-d
+    tree candidates), and CombinedPotential(NUwU + repulsion) = the sum of its parts."""
+    from fresco_b200 import CombinedPotential, InversePower, NUwU
+
+    L = np.full(2, TWO_PI)
+    radii = np.full(N2, 0.25 / np.sqrt(N2) * TWO_PI)
+    rep = InversePower(2.0, 1.0, radii, L, use_cell_lists=True)
+    e, g = rep.get_energy_gradient(config2_points)
+    e_ref, g_ref = O.InversePower(2.0, 1.0, radii, L).get_energy_gradient_tree(config2_points)
+    de, dg = _report("config2 repulsion fp64", e, e_ref, g, g_ref)
+    assert de <= 1e-10 and dg <= 1e-10
+    _, _, Sk, V, _ = O.stealthy_nuwu_inputs(4, K2, KMAX2, ndim=2, seed=2)
+    # the fine grid is accumulated with atomics, so two evaluations agree to the rounding of the form
+    for prec, tol in (("fp64", 1e-12), ("fp32", 1e-6)):
+        nu = NUwU(np.ones(N2), K2, Sk, V, L, eps=1e-6, precision=prec)
+        comb = CombinedPotential()
+        comb.add_potential(nu)
+        comb.add_potential(rep)
+        ec, gc = comb.get_energy_gradient(config2_points)
+        en, gn = nu.get_energy_gradient(config2_points)
+        assert abs(ec - (en + e)) <= tol * abs(ec), prec
+        assert _rel(gc, gn + g) <= tol, prec
+
+
+# ---------------------------------------------------------------------------
+# config 3: 3D NUwU, N = 2,097,152, 129^3 modes, S0 = 1 - exp(-(|k|/16)^2), V = 1/(1+|k|), V(0) = 0
+# ---------------------------------------------------------------------------
+
+N3, K3 = 1 << 21, 64
+
+
+def _radial_targets():
+    n = 2 * K3 + 1
+    mag = np.sqrt(sum(c * c for c in _kgrid(n, 3)))
+    Sk = 1.0 - np.exp(-((mag / 16.0) ** 2))
+    V = np.where(mag > 0, 1.0 / (1.0 + mag), 0.0)
+    return Sk, V
+
+
+@pytest.fixture(scope="module")
+def config3_points():
+    return np.random.default_rng(3).random(3 * N3) * TWO_PI
+
+
+@pytest.mark.parametrize("prec,eps,tol", PRECISIONS)
+def test_config3_nuwu_sparse_modes_exact(config3_points, prec, eps, tol):
+    """The radial S0 and V kept on 68 active modes: device against the exact active-mode sums at N = 2^21."""
+    from fresco_b200 import NUwU
+
+    n = 2 * K3 + 1
+    Sk, Vfull = _radial_targets()
+    act = _sparse_modes(np.random.default_rng(30), n, 3, K3, 64, [(64, 0, 0), (0, -64, 0), (0, 0, 64), (-37, 37, -37)])
+    V = np.zeros_like(Vfull)
+    V[act] = Vfull[act]
+    L = np.full(3, TWO_PI)
+    radii = np.ones(N3)
+    pot = NUwU(radii, K3, Sk, V, L, eps=eps, precision=prec)
+    e, g = pot.get_energy_gradient(config3_points)
+    assert pot.status() == 0
+    e_ref, g_ref = _oracle("c3", lambda: O.NUwU(radii, K3, Sk, V, L).get_energy_gradient_active(config3_points))
+    de, dg = _report(f"config3 NUwU 3D 68 active modes {prec} eps={eps:g}", e, e_ref, g, g_ref)
+    assert de <= tol and dg <= tol
+
+
+def test_config3_autograd_central_differences(config3_points):
+    """All 129^3 radial targets: the gradient through the torch.autograd.Function against central
+    differences (h = 1e-4) of the device energy at 64 seeded coordinates away from the coordinate map's
+    jumps, and against the reference-formula gradient (equal at L = 2 pi); FP32 autograd within 1e-5."""
+    import torch
+
+    from fresco_b200 import NUwU
+    from fresco_b200.autograd import structure_factor_loss
+
+    Sk, V = _radial_targets()
+    L = np.full(3, TWO_PI)
+    radii = np.ones(N3)
+    pot = NUwU(radii, K3, Sk, V, L, eps=1e-12, precision="fp64")
+    xt = torch.tensor(config3_points, device="cuda", requires_grad=True)
+    e = structure_factor_loss(pot, xt)
+    e.backward()
+    g = xt.grad.cpu().numpy()
+    e_ref, g_ref = pot.get_energy_gradient(config3_points)
+    assert abs(float(e.item()) - e_ref) <= 1e-13 * abs(e_ref)
+    assert _rel(g, g_ref) <= 1e-10
+    frac = (config3_points / TWO_PI) % 1.0
+    ok = np.nonzero(np.abs(frac - 0.5) > 1e-3)[0]
+    idx = np.random.default_rng(31).choice(ok, 64, replace=False)
+    h = 1e-4
+    xd = torch.tensor(config3_points, device="cuda")
+    fd = []
+    for i in idx:
+        v = float(xd[i])
+        xd[i] = v + h
+        ep = float(pot.energy_device(xd).item())
+        xd[i] = v - h
+        em = float(pot.energy_device(xd).item())
+        xd[i] = v
+        fd.append((ep - em) / (2 * h))
+    fd = np.array(fd)
+    err = float(np.max(np.abs(fd - g[idx])) / np.max(np.abs(g)))
+    print(f"ACCURACY config3 autograd vs central differences (64 coords, h=1e-4): max_err/max|g|={err:.3e}")
+    assert err <= 1e-5
+    p32 = NUwU(radii, K3, Sk, V, L, eps=1e-6, precision="fp32")
+    x32 = torch.tensor(config3_points, device="cuda", requires_grad=True)
+    e32 = structure_factor_loss(p32, x32)
+    e32.backward()
+    de, dg = _report("config3 NUwU 3D dense fp32 eps=1e-6 (autograd) vs fp64 eps=1e-12", float(e32.item()),
+                     e_ref, x32.grad.cpu().numpy(), g)
+    assert de <= 1e-5 and dg <= 1e-5
+
+
+# ---------------------------------------------------------------------------
+# config 4: UwU on 4096^2 (S0 = 0 in |k| <= 64); UwNU on 2048^2 against 100,000 k-points in |k| <= 512
+# ---------------------------------------------------------------------------
+
+G4 = 4096
+
+
+def _uwu_targets():
+    k = np.arange(G4) - G4 // 2  # centred (fftshift) layout, as the reference's Python layer takes them
+    mag = np.sqrt(k[:, None] ** 2 + k[None, :] ** 2)
+    V = ((mag <= 64) & (mag > 0)).astype(np.float64)
+    return np.zeros_like(V), V
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32", 1e-5)])
+def test_config4_uwu_full_grid(prec, tol):
+    from fresco_b200 import UwU
+
+    x = np.random.default_rng(4).random(G4 * G4)
+    Sk, V = _uwu_targets()
+    shape = np.array([G4, G4])
+    pot = UwU(shape, 64, Sk, V, np.ones(2), precision=prec)
+    e, g = pot.get_energy_gradient(x)
+    e_ref, g_ref = _oracle("uwu", lambda: O.UwU(shape, 64, Sk, V, np.ones(2)).get_energy_gradient(x))
+    de, dg = _report(f"config4 UwU 4096^2 {prec}", e, e_ref, g, g_ref)
+    assert de <= tol and dg <= tol
+
+
+def test_config4_uwu_fire_steps():
+    """Three FIRE iterations on the 4096^2 grid (FP64 form) against the oracle's FIRE driving the
+    oracle's UwU; then the FP32 form's FIRE lowers the loss."""
+    from fresco_b200 import UwU
+    from fresco_b200.optimize import ModifiedFireCPP
+
+    x = np.random.default_rng(4).random(G4 * G4)
+    Sk, V = _uwu_targets()
+    shape = np.array([G4, G4])
+    opt = ModifiedFireCPP(x, UwU(shape, 64, Sk, V, np.ones(2), precision="fp64"))
+    ref = O.ModifiedFire(x, O.UwU(shape, 64, Sk, V, np.ones(2)))
+    for i in range(3):
+        opt.run(1)
+        ref.run(1)
+        r = opt.get_result()
+        assert abs(r.energy - ref.f) <= 1e-10 * abs(ref.f), i
+    assert _rel(opt.get_result().coords, ref.x) <= 1e-10
+    p32 = UwU(shape, 64, Sk, V, np.ones(2), precision="fp32")
+    e0 = p32.get_energy(x)
+    opt32 = ModifiedFireCPP(x, p32)
+    opt32.run(20)
+    e1 = opt32.get_result().energy
+    print(f"ACCURACY config4 UwU fp64 FIRE 3 iterations vs oracle: ok; fp32 FIRE 20 iterations {e0:.6e} -> {e1:.6e}")
+    assert e1 < e0
+
+
+G4U, M4 = 2048, 100_000
+
+
+def _uwnu_inputs():
+    rng = np.random.default_rng(4)
+    x = rng.random(G4U * G4U)
+    r = 512 * np.sqrt(rng.random(M4))
+    t = TWO_PI * rng.random(M4)
+    k = np.stack([r * np.cos(t), r * np.sin(t)], axis=1)  # cycles per box, uniform in the disc
+    Kref = (k / G4U).ravel()  # the reference's K with L = 1: phase 2 pi k.n / 2048
+    peaks = rng.choice(M4, 64, replace=False)
+    Sk = np.zeros(M4)
+    Sk[peaks] = float(np.sum(x))  # "N" read as the grid's total intensity
+    return x, Kref, Sk, peaks
+
+
+@pytest.mark.parametrize("prec,eps,tol", PRECISIONS)
+def test_config4_uwnu_sparse_kpoints_exact(prec, eps, tol):
+    """All 100,000 k-points go through the transforms; V is non-zero on the 64 peaks and 64 other
+    k-points, so the exact separable sums over those give the energy and gradient."""
+    from fresco_b200 import UwNU
+
+    x, Kref, Sk, peaks = _uwnu_inputs()
+    rng = np.random.default_rng(40)
+    others = rng.choice(np.setdiff1d(np.arange(M4), peaks), 64, replace=False)
+    V = np.zeros(M4)
+    V[peaks] = 0.5 + rng.random(64)
+    V[others] = 0.5 + rng.random(64)
+    shape = np.array([G4U, G4U])
+    pot = UwNU(shape, Kref, Sk, V, np.ones(2), eps=eps, precision=prec)
+    e, g = pot.get_energy_gradient(x)
+    e_ref, g_ref = _oracle("uwnu", lambda: O.UwNU(shape, Kref, Sk, V, np.ones(2)).get_energy_gradient_active(x))
+    de, dg = _report(f"config4 UwNU 2048^2 x 1e5 k-points, 128 active {prec} eps={eps:g}", e, e_ref, g, g_ref)
+    assert de <= tol and dg <= tol
+
+
+def test_config4_uwnu_dense_fp32_against_fp64():
+    from fresco_b200 import UwNU
+
+    x, Kref, Sk, _ = _uwnu_inputs()
+    V = np.ones(M4)
+    shape = np.array([G4U, G4U])
+    e_ref, g_ref = UwNU(shape, Kref, Sk, V, np.ones(2), eps=1e-12, precision="fp64").get_energy_gradient(x)
+    e, g = UwNU(shape, Kref, Sk, V, np.ones(2), eps=1e-6, precision="fp32").get_energy_gradient(x)
+    de, dg = _report("config4 UwNU dense fp32 eps=1e-6 vs fp64 eps=1e-12", e, e_ref, g, g_ref)
+    assert de <= 1e-5 and dg <= 1e-5

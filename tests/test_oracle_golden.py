@@ -135,3 +135,39 @@ def test_radial_profile_small_case():
         expect = [data[r == k].mean() for k in range(kept)]
         np.testing.assert_array_equal(q, np.arange(kept))
         np.testing.assert_allclose(prof, expect)
+
+
+def test_active_mode_sums_equal_full_sums():
+    """The oracle's active-mode NUwU/UwNU sums (used at full sizes) equal its full exact sums when V is
+    sparse, and the k-d tree pair search gives the O(N^2) repulsion."""
+    rng = np.random.default_rng(21)
+    for ndim, N, K in [(2, 300, 9), (3, 120, 3)]:
+        x, radii, Sk, V, L = O.stealthy_nuwu_inputs(N, K, K, ndim=ndim, seed=ndim)
+        radii = 0.5 + rng.random(N)
+        V = V * (rng.random(V.shape) < 0.2) * rng.random(V.shape)
+        Sk = rng.random(V.shape) * (rng.random(V.shape) < 0.5)
+        ref = O.NUwU(radii, K, Sk, V, L)
+        e, g = ref.get_energy_gradient(x)
+        ea, ga = ref.get_energy_gradient_active(x, chunk=77)
+        assert abs(ea - e) <= 1e-12 * abs(e)
+        assert np.linalg.norm(ga - g) <= 1e-12 * np.linalg.norm(g)
+    shape = np.array([12, 10])
+    M = 40
+    Kp = rng.random(M * 2) * 4 - 2
+    V = rng.random(M) * (rng.random(M) < 0.5)
+    Sk = rng.random(M) * (rng.random(M) < 0.5)
+    grid = rng.random(int(np.prod(shape)))
+    ref = O.UwNU(shape, Kp, Sk, V, np.array([1.0, 1.3]))
+    e, g = ref.get_energy_gradient(grid)
+    ea, ga = ref.get_energy_gradient_active(grid)
+    assert abs(ea - e) <= 1e-12 * abs(e)
+    assert np.linalg.norm(ga - g) <= 1e-12 * np.linalg.norm(g)
+    for ndim in (2, 3):
+        box = np.full(ndim, 2.0)
+        pts = rng.random(300 * ndim) * 2.0
+        rad = 0.08 + 0.04 * rng.random(300)
+        ip = O.InversePower(2.0, 1.0, rad, box, use_cell_lists=True)
+        e, g = ip.get_energy_gradient(pts)
+        et, gt = ip.get_energy_gradient_tree(pts)
+        assert e > 0 and abs(et - e) <= 1e-12 * e
+        assert np.linalg.norm(gt - g) <= 1e-12 * np.linalg.norm(g)
