@@ -42,6 +42,7 @@ inline void cufft_check(cufftResult r, const char* what, const char* file, int l
 enum StatusBits : int {
   STATUS_NONFINITE_INPUT = 1,  // a coordinate was NaN or +-inf
   STATUS_OVERFLOW = 2,         // a bounded buffer was too small (kernel skipped the excess)
+  STATUS_TIMEOUT = 4,          // a bounded wait gave up (the kernel skipped that work)
 };
 
 // A potential's status block holds two words: [0] the flags of the current

@@ -261,6 +261,9 @@ struct EnsTileMap {
   __device__ __forceinline__ bool nonfinite(const TileWork<T>&) const {
     return (cur_status[pats[tab[blockIdx.x].x].pid] & STATUS_NONFINITE_INPUT) != 0;
   }
+  // tiles are read with plain loads (one grid per pattern)
+  __device__ __forceinline__ const CUtensorMap* tile_tmap() const { return nullptr; }
+  __device__ __forceinline__ int* err_status() const { return nullptr; }
 };
 
 // Direct spreading for sparse patterns: thread per sorted point, the w x w
@@ -793,8 +796,7 @@ class NUwUEnsembleImpl final : public Ensemble {
   template <int W>
   void smem_attrs_w() {
     constexpr size_t ss = spread2d_smem_bytes<W, T, false>();
-    constexpr int TW = kTile2D + W;
-    constexpr size_t si = sizeof(cplx_t<T>) * TW * TW + 2 * sizeof(uint16_t) * kMaxSub;
+    constexpr size_t si = interp2d_smem_bytes<W, T>();
     FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(spread2d_tile_kernel<W, T, false, EnsTileMap<T>>),
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, int(ss)));
     FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(interp2d_tile_kernel<W, T, EnsTileMap<T>>),
@@ -880,8 +882,7 @@ class NUwUEnsembleImpl final : public Ensemble {
       }
     }
     if (gr.n_tab) {
-      constexpr int TW = kTile2D + W;
-      constexpr size_t si = sizeof(cplx_t<T>) * TW * TW + 2 * sizeof(uint16_t) * kMaxSub;
+      constexpr size_t si = interp2d_smem_bytes<W, T>();
       interp2d_tile_kernel<W, T, EnsTileMap<T>><<<gr.n_tab, 256, si, s>>>(recs, weights_.p, map, geo, poly, gr.ggrid.p,
                                                                           INTERP_GRAD, g, nullptr, 0, GradScale());
       FB_LAUNCH_CHECK();

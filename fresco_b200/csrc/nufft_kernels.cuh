@@ -2,6 +2,8 @@
 // precision in nufft_f32.cu / nufft_f64.cu.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (the encoder is fetched from the driver at run time)
+
 #include <algorithm>
 #include <vector>
 
@@ -368,7 +370,7 @@ template <int W, typename T, bool CPLX>
 __host__ __device__ constexpr size_t spread2d_smem_bytes() {
   using P = Tile2D<W>;
   return sizeof(Staged2D<T, CPLX>) * kMaxSub + sizeof(T) * (CPLX ? 2 : 1) * P::EDGE * P::EDGE +
-         sizeof(uint16_t) * kMaxSub + sizeof(int) * 2 * P::NSB * P::NSB;
+         sizeof(int) * 2 * P::NSB * P::NSB;
 }
 
 // Adds VW consecutive cells (VW = 4 real or 2 complex: one float4) of the
@@ -420,6 +422,12 @@ struct TileMap1 {
   const int* __restrict__ bin_start;
   const int* __restrict__ status;  // evaluation status word (interpolation), may be null
   T uniform;
+  int has_tmap = 0;  // interpolation: tmap describes the interpolated fine grid
+  CUtensorMap tmap;
+  // tensor map of the fine grid for tile copies (the kernel parameter must be
+  // __grid_constant__ for its address to be usable), or null
+  __device__ __forceinline__ const CUtensorMap* tile_tmap() const { return has_tmap ? &tmap : nullptr; }
+  __device__ __forceinline__ int* err_status() const { return const_cast<int*>(status); }
   __device__ __forceinline__ bool fetch(const Geom& g, TileWork<T>& w) const {
     const int sub = blockIdx.x;
     if (sub >= *num_sub) return false;
@@ -450,8 +458,7 @@ __global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S* srec = reinterpret_cast<S*>(smem_raw);
   T* tile = reinterpret_cast<T*>(srec + kMaxSub);
-  uint16_t* rank = reinterpret_cast<uint16_t*>(tile + E * E * NC);
-  int* sb_count = reinterpret_cast<int*>(rank + kMaxSub);
+  int* sb_count = reinterpret_cast<int*>(tile + E * E * NC);
   int* sb_start = sb_count + NSB2;
 
   TileWork<T> wk;
@@ -464,13 +471,24 @@ __global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
 
   for (int i = tid; i < E * E * NC; i += P::THREADS) tile[i] = T(0);
   for (int i = tid; i < NSB2; i += P::THREADS) sb_count[i] = 0;
+  // this thread's points are p = tid + THREADS k; their cells are loaded
+  // together (one round of load latency), and their sub-block and rank in it
+  // stay in registers until the sub-block starts are known
+  constexpr int PPT = (kMaxSub + P::THREADS - 1) / P::THREADS;
+  uint32_t cellk[PPT];
+#pragma unroll
+  for (int k = 0; k < PPT; ++k)
+    if (tid + P::THREADS * k < cnt) cellk[k] = recs[start + tid + P::THREADS * k].cell;
+  int slot[PPT];  // sub-block << 16 | rank in sub-block, or -1
   __syncthreads();
-  // rank of each point inside its sub-block
-  for (int p = tid; p < cnt; p += P::THREADS) {
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
+    slot[k] = -1;
+    if (tid + P::THREADS * k >= cnt) continue;
     int c0, c1, c2;
-    unpack_cell(2, recs[start + p].cell, c0, c1, c2);
+    unpack_cell(2, cellk[k], c0, c1, c2);
     const int sbi = ((c0 - org0) / P::SB) + P::NSB * ((c1 - org1) / P::SB);
-    rank[p] = uint16_t(atomicAdd(&sb_count[sbi], 1));
+    slot[k] = (sbi << 16) | atomicAdd(&sb_count[sbi], 1);
   }
   __syncthreads();
   if (tid < 32) {  // exclusive scan of the sub-block counts (one warp)
@@ -497,24 +515,32 @@ __global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
     }
   }
   __syncthreads();
-  // stage: grouped by sub-block, converted to (tile offset, u0, u1, weight)
-  for (int p = tid; p < cnt; p += P::THREADS) {
-    const Rec<2, T> r = recs[start + p];
-    int c0, c1, c2;
-    unpack_cell(2, r.cell, c0, c1, c2);
-    const int sbi = ((c0 - org0) / P::SB) + P::NSB * ((c1 - org1) / P::SB);
-    S st;
-    const int s0 = es_start<W, T>(r.f[0], st.u0);
-    const int s1 = es_start<W, T>(r.f[1], st.u1);
-    st.base = (c1 - org1 + s1 + P::PAD) * E + (c0 - org0 + s0 + P::PAD);
-    if constexpr (CPLX) {
-      const cplx_t<T> v = strengths[r.idx];
-      st.wr = v.x;
-      st.wi = v.y;
-    } else {
-      st.wr = weights ? weights[r.idx] : uniform;
+  // stage: grouped by sub-block, converted to (tile offset, u0, u1, weight);
+  // the records are loaded together as well
+  {
+    Rec<2, T> rk[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k)
+      if (slot[k] >= 0) rk[k] = recs[start + tid + P::THREADS * k];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+      if (slot[k] < 0) continue;
+      const Rec<2, T>& r = rk[k];
+      int c0, c1, c2;
+      unpack_cell(2, r.cell, c0, c1, c2);
+      S st;
+      const int s0 = es_start<W, T>(r.f[0], st.u0);
+      const int s1 = es_start<W, T>(r.f[1], st.u1);
+      st.base = (c1 - org1 + s1 + P::PAD) * E + (c0 - org0 + s0 + P::PAD);
+      if constexpr (CPLX) {
+        const cplx_t<T> v = strengths[r.idx];
+        st.wr = v.x;
+        st.wi = v.y;
+      } else {
+        st.wr = weights ? weights[r.idx] : uniform;
+      }
+      srec[sb_start[slot[k] >> 16] + (slot[k] & 0xffff)] = st;
     }
-    srec[sb_start[sbi] + rank[p]] = st;
   }
   __syncthreads();
 
@@ -740,8 +766,74 @@ __device__ __forceinline__ void interp_store(int mode, uint32_t o, T wgt, T v0r,
   }
 }
 
+// Tile geometry of the 2D interpolation: rows org1 - W/2 .. (64 + W rows);
+// columns start at org0 - XPAD, XPAD = W/2 rounded up to even, and a row
+// holds TWX (even) cells, so that with 8- or 16-byte cells a tile row is a
+// whole number of 16-byte units and starts on a 16-byte boundary of the fine
+// grid (what a tensor copy of the tile needs).
+template <int W>
+struct Interp2D {
+  static constexpr int PAD = W / 2;
+  static constexpr int XPAD = (PAD + 1) & ~1;
+  static constexpr int TWY = kTile2D + W;
+  static constexpr int TWX = (kTile2D + W + (XPAD - PAD) + 1) & ~1;
+};
+
+template <int W, typename T>
+__host__ __device__ constexpr size_t interp2d_smem_bytes() {
+  // + 128: the tile is placed on a 128-byte boundary for the tensor copy
+  return 128 + sizeof(cplx_t<T>) * Interp2D<W>::TWX * Interp2D<W>::TWY + sizeof(uint16_t) * kMaxSub;
+}
+
+// Points per thread of a 2D tile block (256 threads, at most kMaxSub points).
+constexpr int kTilePtsPerThread = (kMaxSub + 255) / 256;
+
+// Bounded polls of the tile copy's mbarrier before a block gives up.
+constexpr int kTileWaitPolls = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Waits for phase `parity` of the barrier for at most kTileWaitPolls polls.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+  for (int i = 0; i < kTileWaitPolls; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// 2D tensor copy global -> shared (x innermost, in elements of the map),
+// completing on `bar` with its byte count.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
 // 2D interpolation: one block per subproblem stages the tile (+ halo) of the
 // field in shared memory, then one thread per point sums its w x w taps.
+// With a tensor map of the field (single pattern, power-of-64 grids), a tile
+// that needs no periodic wrap is copied by one tensor copy, issued before
+// the block classifies its points so the two overlap; edge tiles are read
+// with plain loads.
 //
 // Every tap address of a point is its footprint's first cell `base` plus an
 // offset that is the same for all points, so a group of lanes served by one
@@ -751,17 +843,18 @@ __device__ __forceinline__ void interp_store(int mode, uint32_t o, T wgt, T v0r,
 // base mod G and lane c of every group takes points of class c only.
 template <int W, typename T, typename Map>
 __global__ void __launch_bounds__(256) interp2d_tile_kernel(const Rec<2, T>* __restrict__ recs,
-                                                            const T* __restrict__ weights, const Map map, Geom g,
+                                                            const T* __restrict__ weights,
+                                                            const __grid_constant__ Map map, Geom g,
                                                             const EsPoly<W, T> poly,
                                                             const cplx_t<T>* __restrict__ field, int mode, double* grad,
                                                             double2* out2, int accumulate, const GradScale gs) {
-  constexpr int PAD = W / 2;
-  constexpr int TW = kTile2D + W;
+  using IP = Interp2D<W>;
+  constexpr int PAD = IP::PAD, XPAD = IP::XPAD, TWX = IP::TWX, TWY = IP::TWY;
   constexpr int G = 128 / int(sizeof(cplx_t<T>));  // lanes per wavefront = bank classes
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx_t<T>* tile = reinterpret_cast<cplx_t<T>*>(smem_raw);
-  uint16_t* code = reinterpret_cast<uint16_t*>(tile + TW * TW);  // class << 12 | rank in class
-  uint16_t* order = code + kMaxSub;                               // points grouped by class
+  extern __shared__ unsigned char smem_ip[];
+  __shared__ __align__(8) uint64_t tile_bar;
+  cplx_t<T>* tile = reinterpret_cast<cplx_t<T>*>(smem_ip + ((128u - (smem_addr(smem_ip) & 127u)) & 127u));
+  uint16_t* order = reinterpret_cast<uint16_t*>(tile + TWX * TWY);  // points grouped by class
   __shared__ int cls_count[G], cls_start[G];
   TileWork<T> wk;
   if (!map.fetch(g, wk)) return;
@@ -771,42 +864,69 @@ __global__ void __launch_bounds__(256) interp2d_tile_kernel(const Rec<2, T>* __r
   const int nf0 = g.nf[0], nf1 = g.nf[1];
   field += wk.grid_off;
   const int tid = threadIdx.x;
+  const CUtensorMap* tm = map.tile_tmap();
+  const bool use_tma = tm != nullptr && org0 >= XPAD && org0 - XPAD + TWX <= nf0 && org1 >= PAD &&
+                       org1 - PAD + TWY <= nf1;
   if (tid < G) cls_count[tid] = 0;
+  if (use_tma && tid == 0) mbar_init(&tile_bar, 1);
   __syncthreads();
-  // tile and records are read in batches of 4 loads per thread so that their
-  // latencies overlap
-  constexpr int BT = 4;
-  const int nthr = blockDim.x;
-  for (int i0 = tid; i0 < TW * TW; i0 += BT * nthr) {
-    cplx_t<T> v[BT];
-#pragma unroll
-    for (int b = 0; b < BT; ++b) {
-      const int i = i0 + b * nthr;
-      if (i < TW * TW) {
-        const int x = i % TW, y = i / TW;
-        v[b] = field[int64_t(wrap_index(org1 - PAD + y, nf1)) * nf0 + wrap_index(org0 - PAD + x, nf0)];
-      }
+  if (use_tma) {
+    if (tid == 0) {
+      mbar_expect_tx(&tile_bar, unsigned(sizeof(cplx_t<T>) * TWX * TWY));
+      tma_load_2d(tile, tm, 2 * (org0 - XPAD), org1 - PAD, &tile_bar);
     }
+  } else {
+    // tile read in batches of 4 loads per thread so that their latencies overlap
+    constexpr int BT = 4;
+    const int nthr = blockDim.x;
+    for (int i0 = tid; i0 < TWX * TWY; i0 += BT * nthr) {
+      cplx_t<T> v[BT];
 #pragma unroll
-    for (int b = 0; b < BT; ++b)
-      if (i0 + b * nthr < TW * TW) tile[i0 + b * nthr] = v[b];
+      for (int b = 0; b < BT; ++b) {
+        const int i = i0 + b * nthr;
+        if (i < TWX * TWY) {
+          const int x = i % TWX, y = i / TWX;
+          v[b] = field[int64_t(wrap_index(org1 - PAD + y, nf1)) * nf0 + wrap_index(org0 - XPAD + x, nf0)];
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < BT; ++b)
+        if (i0 + b * nthr < TWX * TWY) tile[i0 + b * nthr] = v[b];
+    }
   }
-  for (int p0 = tid; p0 < cnt; p0 += BT * nthr) {
-    Rec<2, T> r[BT];
+  // class and rank in class of this thread's points (p = tid + 256 k), kept
+  // in registers until the class starts are known
+  constexpr int PPT = kTilePtsPerThread;
+  int code[PPT];
+  {
+    Rec<2, T> r[PPT];
 #pragma unroll
-    for (int b = 0; b < BT; ++b)
-      if (p0 + b * nthr < cnt) r[b] = recs[start + p0 + b * nthr];
+    for (int k = 0; k < PPT; ++k)
+      if (tid + 256 * k < cnt) r[k] = recs[start + tid + 256 * k];
 #pragma unroll
-    for (int b = 0; b < BT; ++b) {
-      const int p = p0 + b * nthr;
-      if (p >= cnt) break;
+    for (int k = 0; k < PPT; ++k) {
+      code[k] = -1;
+      if (tid + 256 * k >= cnt) continue;
       int c0, c1, c2;
-      unpack_cell(2, r[b].cell, c0, c1, c2);
+      unpack_cell(2, r[k].cell, c0, c1, c2);
       T u;
-      const int l0 = c0 - org0 + es_start<W, T>(r[b].f[0], u) + PAD;
-      const int l1 = c1 - org1 + es_start<W, T>(r[b].f[1], u) + PAD;
-      const int cls = (l1 * TW + l0) & (G - 1);
-      code[p] = uint16_t((cls << 12) | atomicAdd(&cls_count[cls], 1));
+      const int l0 = c0 - org0 + es_start<W, T>(r[k].f[0], u) + XPAD;
+      const int l1 = c1 - org1 + es_start<W, T>(r[k].f[1], u) + PAD;
+      const int cls = (l1 * TWX + l0) & (G - 1);
+      code[k] = (cls << 12) | atomicAdd(&cls_count[cls], 1);
+    }
+  }
+  if (use_tma) {
+    // every thread sees the copy complete (bounded); a block that gives up
+    // flags the evaluation, waits once more for its copy and skips its points
+    const bool ok = mbar_wait_bounded(&tile_bar, 0);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        if (int* st = map.err_status()) raise_status(st, STATUS_TIMEOUT);
+        mbar_wait_bounded(&tile_bar, 0);
+      }
+      __syncthreads();
+      return;
     }
   }
   __syncthreads();
@@ -818,7 +938,9 @@ __global__ void __launch_bounds__(256) interp2d_tile_kernel(const Rec<2, T>* __r
     }
   }
   __syncthreads();
-  for (int p = tid; p < cnt; p += blockDim.x) order[cls_start[code[p] >> 12] + (code[p] & 0xfff)] = uint16_t(p);
+#pragma unroll
+  for (int k = 0; k < PPT; ++k)
+    if (code[k] >= 0) order[cls_start[code[k] >> 12] + (code[k] & 0xfff)] = uint16_t(tid + 256 * k);
   __syncthreads();
   const int cls = tid % G, grp = tid / G, ngrp = int(blockDim.x) / G;
   const int n_c = cls_count[cls];
@@ -834,11 +956,11 @@ __global__ void __launch_bounds__(256) interp2d_tile_kernel(const Rec<2, T>* __r
     T k0[W], k1[W];
     const int s0 = es_taps<W, T>(r.f[0], poly, k0);
     const int s1 = es_taps<W, T>(r.f[1], poly, k1);
-    const int l0 = c0 - org0 + s0 + PAD, l1 = c1 - org1 + s1 + PAD;
+    const int l0 = c0 - org0 + s0 + XPAD, l1 = c1 - org1 + s1 + PAD;
     T vr = 0, vi = 0;
 #pragma unroll
     for (int m1 = 0; m1 < W; ++m1) {
-      const cplx_t<T>* rowp = tile + (l1 + m1) * TW + l0;
+      const cplx_t<T>* rowp = tile + (l1 + m1) * TWX + l0;
       T rr = 0, ri = 0;
 #pragma unroll
       for (int m0 = 0; m0 < W; ++m0) {
@@ -985,15 +1107,48 @@ void launch_spread_generic(const void* recs, const T* weights, T uniform, const 
   FB_LAUNCH_CHECK();
 }
 
+// Tensor map of a complex fine grid nf0 x nf1 (cells of two T) for tile
+// copies of box_x T values x box_y rows; returns 0 (plain loads are used) if
+// the driver has no encoder or the grid does not meet the copy rules.
+template <typename T>
+int encode_tile_tmap(CUtensorMap* tm, const void* grid, int64_t nf0, int64_t nf1, int box_x, int box_y) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static const Encode encode = [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return Encode(nullptr);
+    }
+    return reinterpret_cast<Encode>(fn);
+  }();
+  const uint64_t row_bytes = uint64_t(nf0) * 2 * sizeof(T);
+  if (!encode || grid == nullptr || (reinterpret_cast<uintptr_t>(grid) & 15) || row_bytes % 16 ||
+      nf0 % kTile2D || nf1 % kTile2D || box_x > 256 || box_y > 256 || (box_x * sizeof(T)) % 16)
+    return 0;
+  const cuuint64_t dims[2] = {cuuint64_t(2 * nf0), cuuint64_t(nf1)};
+  const cuuint64_t strides[1] = {row_bytes};
+  const cuuint32_t box[2] = {cuuint32_t(box_x), cuuint32_t(box_y)};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  const CUresult r = encode(tm, dt, 2, const_cast<void*>(grid), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 1 : 0;
+}
+
 template <int W, typename T>
 void launch_interp2d(const void* recs, const T* weights, T uniform, const SortBufs& sb, const Geom& g,
                      const std::vector<double>& poly, const cplx_t<T>* field, int mode, double* grad, double2* out2,
                      int acc, const int* status, cudaStream_t s, const GradScale& gs) {
-  constexpr int TW = kTile2D + W;
-  const size_t smem = sizeof(cplx_t<T>) * TW * TW + 2 * sizeof(uint16_t) * kMaxSub;
+  constexpr size_t smem = interp2d_smem_bytes<W, T>();
   auto kern = interp2d_tile_kernel<W, T, TileMap1<T>>;
   if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  const TileMap1<T> map{sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, sb.bin_start.p, status, uniform};
+  TileMap1<T> map{sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, sb.bin_start.p, status, uniform};
+  map.has_tmap = encode_tile_tmap<T>(&map.tmap, field, g.nf[0], g.nf[1], 2 * Interp2D<W>::TWX, Interp2D<W>::TWY);
   kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<2, T>*>(recs), weights, map, g,
                                                 make_es_poly<W, T>(poly), field, mode, grad, out2, acc, gs);
   FB_LAUNCH_CHECK();
