@@ -439,6 +439,16 @@ def run_ours(args):
     roofline = {"kernel": top, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                 "frac": round(achieved / hbm_peak, 4), "traffic": traffic, "peak_source": peak_src,
                 "algorithmic_bytes": per_kernel.get(top)}
+    try:  # the stage's own limiter: L1/shared-memory pipe use from the same kind of ncu capture
+        with open(os.path.join(ROOT, "profiles", "l1tex.txt")) as fh:
+            l1 = {ln.split()[0]: ln.split()[1:] for ln in fh if ln.strip() and not ln.startswith("#")}
+        if top in l1:
+            roofline["l1tex"] = {"frac": round(float(l1[top][0]) / 100.0, 3),
+                                 "shared_wavefronts": int(l1[top][1]),
+                                 "source": "ncu l1tex__throughput.avg.pct_of_peak_sustained_active "
+                                           "(profiles/l1tex.txt)"}
+    except (OSError, ValueError, IndexError):
+        pass
     eval_achieved = b_eval / (ms_per_step * 1e-3) / 1e9
     roofline_eval = {"bound": "hbm", "algorithmic_bytes": b_eval, "achieved": round(eval_achieved, 1),
                      "peak": hbm_peak, "unit": "GB/s", "frac": round(eval_achieved / hbm_peak, 4)}
