@@ -15,12 +15,13 @@ import sys
 import types
 
 from . import _lib  # noqa: F401  (loads the CUDA library; raises ImportError if missing)
-from . import ensemble, optimize, potentials, utils
+from . import ensemble, optimize, potentials, shard, utils
 from .ensemble import EnsembleLBFGS, NUwUEnsemble
 from .potentials import CombinedPotential, InversePower, NUwNU, NUwU, UwNU, UwU
+from .shard import ShardedNUwU
 
-__all__ = ["potentials", "optimize", "utils", "ensemble", "install_alias", "NUwU", "UwU", "UwNU", "NUwNU",
-           "InversePower", "CombinedPotential", "NUwUEnsemble", "EnsembleLBFGS"]
+__all__ = ["potentials", "optimize", "utils", "ensemble", "shard", "install_alias", "NUwU", "UwU", "UwNU", "NUwNU",
+           "InversePower", "CombinedPotential", "NUwUEnsemble", "EnsembleLBFGS", "ShardedNUwU"]
 
 
 def install_alias() -> None:

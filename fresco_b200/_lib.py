@@ -29,6 +29,13 @@ _SIGNATURES = {
     "fresco_abi_version": (C.c_int, []),
     "fresco_nuwu_create": (C.c_int, [c_double_p, c_int64, C.c_double, c_double_p, c_double_p, c_int64, c_double_p,
                                      C.c_int, C.c_double, C.c_int, C.POINTER(handle_t)]),
+    "fresco_nuwu_shard_create": (C.c_int, [c_double_p, c_int64, c_int64, C.c_double, C.c_double, c_double_p,
+                                           c_double_p, c_int64, c_double_p, C.c_int, C.c_double, C.c_int,
+                                           C.POINTER(handle_t)]),
+    "fresco_nuwu_weight_sum": (C.c_int, [c_double_p, c_int64, C.c_int, c_double_p]),
+    "fresco_nuwu_shard_nrho": (C.c_int, [handle_t, C.POINTER(c_int64)]),
+    "fresco_nuwu_shard_rho": (C.c_int, [handle_t, c_void_p, c_int64, c_void_p, c_void_p]),
+    "fresco_nuwu_shard_finish": (C.c_int, [handle_t, c_void_p, c_void_p, c_void_p, c_void_p]),
     "fresco_uwu_create": (C.c_int, [c_int_p, C.c_int, C.c_double, c_double_p, c_double_p, c_int64, c_double_p,
                                     C.c_double, C.c_int, C.POINTER(handle_t)]),
     "fresco_uwnu_create": (C.c_int, [c_int_p, C.c_int, c_double_p, c_int64, c_double_p, c_double_p, c_double_p,

@@ -104,6 +104,64 @@ int fresco_nuwu_create(const double* radii, int64_t n_points, double K, const do
   });
 }
 
+int fresco_nuwu_shard_create(const double* radii_local, int64_t n_local, int64_t n_total, double weight_sum_total,
+                             double K, const double* sk, const double* v, int64_t n_sk, const double* L, int ndim,
+                             double eps, int precision, fresco_potential* out) {
+  return guarded([&] {
+    if (!out) throw fb::InvalidArgument("null output handle");
+    if (ndim < 1 || ndim > 3) throw std::runtime_error("Invalid dimension: " + std::to_string(ndim));
+    auto p = fb::make_nuwu_shard(vec(radii_local, n_local), n_total, weight_sum_total, K, vec(sk, n_sk),
+                                 vec(v, n_sk), vec(L, ndim), eps, precision);
+    *out = wrap(p);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_nuwu_weight_sum(const double* radii, int64_t n, int ndim, double* out) {
+  return guarded([&] {
+    if (!out || (n > 0 && !radii) || n < 0) throw fb::InvalidArgument("null or negative argument");
+    if (ndim < 1 || ndim > 3) throw std::runtime_error("Invalid dimension: " + std::to_string(ndim));
+    *out = fb::nuwu_weight_factor_sum(radii, n, ndim);
+    return FRESCO_OK;
+  });
+}
+
+namespace {
+fb::NUwUShard* shard_of(fresco_potential p) {
+  auto* sh = p ? dynamic_cast<fb::NUwUShard*>(p->pot.get()) : nullptr;
+  if (!sh) throw fb::InvalidArgument("not a sharded NUwU handle");
+  return sh;
+}
+}  // namespace
+
+int fresco_nuwu_shard_nrho(fresco_potential p, int64_t* n_rho) {
+  return guarded([&] {
+    if (!n_rho) throw fb::InvalidArgument("null argument");
+    *n_rho = shard_of(p)->n_rho();
+    return FRESCO_OK;
+  });
+}
+
+int fresco_nuwu_shard_rho(fresco_potential p, const double* d_x, int64_t n, double* d_rho, void* stream) {
+  return guarded([&] {
+    auto* sh = shard_of(p);
+    if ((n > 0 && !d_x) || (sh->n_rho() > 0 && !d_rho)) throw fb::InvalidArgument("null argument");
+    check_n(p, n);
+    sh->shard_rho(d_x, d_rho, static_cast<cudaStream_t>(stream));
+    return FRESCO_OK;
+  });
+}
+
+int fresco_nuwu_shard_finish(fresco_potential p, const double* d_rho, double* d_grad, double* d_energy,
+                             void* stream) {
+  return guarded([&] {
+    auto* sh = shard_of(p);
+    if (!d_energy || (sh->n_rho() > 0 && !d_rho)) throw fb::InvalidArgument("null argument");
+    sh->shard_finish(d_rho, d_grad, d_energy, static_cast<cudaStream_t>(stream));
+    return FRESCO_OK;
+  });
+}
+
 int fresco_uwu_create(const int* grid, int ndim, double K, const double* sk, const double* v, int64_t n_sk,
                       const double* L, double eps, int precision, fresco_potential* out) {
   return guarded([&] {

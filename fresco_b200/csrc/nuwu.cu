@@ -50,12 +50,47 @@ __global__ void __launch_bounds__(256) nuwu_modes_kernel(
   }
 }
 
+// Undeconvolved rho of this point set at every active mode (shard step 1);
+// a non-finite coordinate makes rho[0] NaN so that the sum over shards, and
+// every shard's energy, carries it.
 template <int D, typename T>
-class NUwUImpl final : public Potential {
+__global__ void __launch_bounds__(256) nuwu_gather_rho_kernel(int n, int K, const int* __restrict__ mode_idx,
+                                                              int n_active, const cplx_t<T>* __restrict__ bhat, int nh0,
+                                                              Geom g, double2* rho, const int* __restrict__ status) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_active; i += gridDim.x * blockDim.x) {
+    double2 r = nuwu_mode_rho<D, T>(mode_idx[i], n, K, bhat, nh0, g.nf[1], g.nf[2]);
+    if (i == 0 && status != nullptr && ((*status) & STATUS_NONFINITE_INPUT))
+      r.x = __longlong_as_double(0x7ff8000000000000ULL);
+    rho[i] = r;
+  }
+}
+
+// Mode pass from the summed rho of all shards (shard step 2).
+template <int D, typename T>
+__global__ void __launch_bounds__(256) nuwu_modes_from_rho_kernel(
+    int n, int K, double invN, const int* __restrict__ mode_idx, const ModeCoef* __restrict__ coef, int n_active,
+    const double2* __restrict__ rho, Geom g, const double* __restrict__ corr0, const double* __restrict__ corr1,
+    const double* __restrict__ corr2, cplx_t<T>* hgrid, int64_t G, double* energy, int want_grad) {
+  double phi = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_active; i += gridDim.x * blockDim.x)
+    phi += nuwu_mode_apply<D, T>(mode_idx[i], n, K, coef[i], rho[i], g.nf[0], g.nf[1], g.nf[2], corr0, corr1, corr2,
+                                 invN, hgrid, G, want_grad != 0);
+  block_sum_atomic(phi, energy);
+}
+
+template <int D, typename T>
+class NUwUImpl final : public Potential, public NUwUShard {
  public:
+  // n_total >= 0 makes a shard of a pattern of n_total points whose weight
+  // factors (area^D per point) sum to weight_sum_total over all shards.
   NUwUImpl(const std::vector<double>& radii, double K, const std::vector<double>& sk, const std::vector<double>& v,
-           const std::vector<double>& L, double eps)
+           const std::vector<double>& L, double eps, int64_t n_total = -1, double weight_sum_total = 0.0)
       : N_(int64_t(radii.size())), Karg_(K) {
+    sharded_ = n_total >= 0;
+    n_total_ = sharded_ ? n_total : N_;
+    if (sharded_ && (n_total_ < N_ || !(weight_sum_total > 0.0)))
+      throw InvalidArgument("sharded NUwU: n_total must cover this shard's points and the weight sum be positive");
+    invN_ = 1.0 / double(n_total_);
     init_status();
     if (sk.size() != v.size()) throw InvalidArgument("len(Sk) must equal len(V)");
     if (int(L.size()) != D) throw InvalidArgument("len(L) must equal the dimension");
@@ -84,8 +119,9 @@ class NUwUImpl final : public Potential {
       sum += c[i];
     }
     bool uniform = true;
+    const double scale = sharded_ ? double(n_total_) / weight_sum_total : double(c.size()) / sum;
     for (size_t i = 0; i < c.size(); ++i) {
-      c[i] *= double(c.size()) / sum;
+      c[i] *= scale;
       if (c[i] != c[0]) uniform = false;
     }
     if (uniform && !c.empty()) {
@@ -149,7 +185,7 @@ class NUwUImpl final : public Potential {
     // type-2 input is zero outside k_x in [-kx_max, kx_max])
     int kx_max = 0;
     for (int i = 0; i < n_active_; ++i) kx_max = std::max(kx_max, std::abs(idx[i] % n_ - K_));
-    setup_band(idx, coef);
+    if (!sharded_) setup_band(idx, coef);  // a shard needs rho from the full R2C output
     pruned_ = !band_ && (D == 2) && n_active_ > 0 && 2 * kx_max + 1 < geom_.nf[0];
     if (band_) {
       // no cuFFT plans: the band kernels do all transforms
@@ -187,6 +223,32 @@ class NUwUImpl final : public Potential {
     run(x, g, e, acc, s);
   }
 
+  int64_t n_rho() const override { return n_active_; }
+
+  void shard_rho(const double* x, double* rho, cudaStream_t s) override {
+    begin_eval_status(s);
+    spread_and_transform(x, s);
+    if (n_active_ > 0) {
+      const int grid = int(std::min<int64_t>(ceil_div(n_active_, 256), int64_t(sm_count()) * 8));
+      nuwu_gather_rho_kernel<D, T><<<grid, 256, 0, s>>>(n_, K_, mode_idx_.p, n_active_, bhat_.p, nh0_, geom_,
+                                                         reinterpret_cast<double2*>(rho), status_.p);
+      FB_LAUNCH_CHECK();
+    }
+  }
+
+  void shard_finish(const double* rho, double* g, double* e, cudaStream_t s) override {
+    FB_CUDA(cudaMemsetAsync(e, 0, sizeof(double), s));
+    if (n_active_ > 0) {
+      const int grid = int(std::min<int64_t>(ceil_div(n_active_, 256), int64_t(sm_count()) * 8));
+      nuwu_modes_from_rho_kernel<D, T><<<grid, 256, 0, s>>>(
+          n_, K_, invN_, mode_idx_.p, coef_.p, n_active_, reinterpret_cast<const double2*>(rho), geom_, corr_[0].p,
+          D >= 2 ? corr_[1].p : corr_[0].p, D >= 3 ? corr_[2].p : corr_[0].p, hgrid_.p, geom_.G(), e,
+          g != nullptr);
+      FB_LAUNCH_CHECK();
+    }
+    if (g) type2_and_interp(g, false, s);
+  }
+
   std::string describe() const override {
     std::string s = "NUwU D=" + std::to_string(D) + " precision=" + (sizeof(T) == 4 ? "fp32" : "fp64") +
                     " N=" + std::to_string(N_) + " modes/dim=" + std::to_string(n_) + " w=" + std::to_string(es_.w) +
@@ -205,7 +267,48 @@ class NUwUImpl final : public Potential {
   int n_active() const { return n_active_; }
 
  private:
+  // sort, spread and type-1 transform of the full R2C path (bhat holds the
+  // half spectrum afterwards; pruned 2D grids transform only the columns
+  // k_x <= kx_max)
+  void spread_and_transform(const double* x, cudaStream_t s) {
+    MapParams mp;
+    mp.kind = 0;
+    mp.stride = D;
+    for (int a = 0; a < D; ++a) mp.L[a] = L_[a];
+    bin_sort<T>(x, N_, mp, geom_, sort_, recs_.p, status_.p, s);
+    FB_CUDA(cudaMemsetAsync(spread_grid_.p, 0, spread_grid_.bytes(), s));
+    spread_real<T>(recs_.p, cw_.p, uniform_c_, sort_, geom_, poly_, spread_grid_.p, s);
+    FB_CUFFT(cufftSetStream(plan_r2c_, s));
+    if (sizeof(T) == 4) {
+      FB_CUFFT(cufftExecR2C(plan_r2c_, reinterpret_cast<cufftReal*>(spread_grid_.p),
+                            reinterpret_cast<cufftComplex*>(bhat_.p)));
+    } else {
+      FB_CUFFT(cufftExecD2Z(plan_r2c_, reinterpret_cast<cufftDoubleReal*>(spread_grid_.p),
+                            reinterpret_cast<cufftDoubleComplex*>(bhat_.p)));
+    }
+    if (pruned_) exec_c2c(plan_col1_, bhat_.p, bhat_.p, s);
+  }
+
+  // type-2 transform of the packed field and interpolation at the points
+  void type2_and_interp(double* g, bool acc, cudaStream_t s) {
+    if (pruned_) {
+      const int off = geom_.nf[0] - kx_max_;
+      exec_c2c(plan_col2a_, hgrid_.p, tgrid_.p, s);
+      if (kx_max_ > 0) exec_c2c(plan_col2b_, hgrid_.p + off, tgrid_.p + off, s);
+      exec_c2c(plan_c2c_, tgrid_.p, ggrid_.p, s);
+    } else {
+      exec_c2c(plan_c2c_, hgrid_.p, ggrid_.p, s);
+    }
+    GradScale gs;  // exact mode: x = (p - round(p/L)) 2 pi / L, so d/dp = (2 pi / L) d/dx
+    if (grad_mode_ == 1)
+      for (int a = 0; a < D; ++a) gs.s[a] = 2.0 * M_PI / L_[a];
+    interp<T>(recs_.p, N_, cw_.p, uniform_c_, sort_, geom_, poly_, ggrid_.p, nfields_, INTERP_GRAD, g, nullptr,
+              acc ? 1 : 0, status_.p, s, gs);
+  }
+
   void run(const double* x, double* g, double* e, bool acc, cudaStream_t s) {
+    if (sharded_ && n_total_ != N_)
+      throw InvalidArgument("sharded NUwU: evaluate through the shard calls (rho, sum over shards, finish)");
     timer_begin(s);
     begin_eval_status(s);
     if (!acc) FB_CUDA(cudaMemsetAsync(e, 0, sizeof(double), s));
@@ -238,7 +341,7 @@ class NUwUImpl final : public Potential {
     if (n_active_ > 0) {
       const int grid = int(std::min<int64_t>(ceil_div(n_active_, 256), int64_t(sm_count()) * 8));
       nuwu_modes_kernel<D, T><<<grid, 256, 0, s>>>(
-          n_, K_, 1.0 / double(N_), mode_idx_.p, coef_.p, n_active_, bhat_.p, nh0_, geom_, corr_[0].p,
+          n_, K_, invN_, mode_idx_.p, coef_.p, n_active_, bhat_.p, nh0_, geom_, corr_[0].p,
           D >= 2 ? corr_[1].p : corr_[0].p, D >= 3 ? corr_[2].p : corr_[0].p, hgrid_.p, geom_.G(), e, status_.p,
           g != nullptr);
       FB_LAUNCH_CHECK();
@@ -330,7 +433,7 @@ class NUwUImpl final : public Potential {
   void run_band_n(double* e, double* g, cudaStream_t s) {
     const dim3 blk(N / 16, 2);
     const BandBatch<T> bb{spread_grid_.p, 0,       band1_.p, 0, band2_.p, 0,       ggrid_.p,
-                          0,              coef_box_.p, 0,   nullptr,  1.0 / double(N_), e, status_.p, nullptr};
+                          0,              coef_box_.p, 0,   nullptr,  invN_, e, status_.p, nullptr};
     band_rows_r2c_kernel<T, N><<<N / 4, blk, smem_rows_, s>>>(spread_grid_.p, 0, tw_.p, Kx_ + 1, band1_.p, 0);
     FB_LAUNCH_CHECK();
     timer_mark("fft_type1", s);
@@ -374,6 +477,9 @@ class NUwUImpl final : public Potential {
   }
 
   int64_t N_;
+  bool sharded_ = false;
+  int64_t n_total_ = 0;
+  double invN_ = 1.0;
   double Karg_;
   double L_[3] = {1, 1, 1};
   int K_ = 0, n_ = 1;
@@ -404,6 +510,34 @@ class NUwUImpl final : public Potential {
 };
 
 }  // namespace
+
+double nuwu_weight_factor_sum(const double* radii, int64_t n, int D) {
+  double sum = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    double c = 1.0;
+    for (int j = 0; j < D; ++j) {
+      if (D == 2) c = c * M_PI * radii[i] * radii[i];
+      else if (D == 3) c = c * M_PI * radii[i] * radii[i] * radii[i] * 4.0 / 3.0;
+    }
+    sum += c;
+  }
+  return sum;
+}
+
+PotentialPtr make_nuwu_shard(const std::vector<double>& radii_local, int64_t n_total, double weight_sum_total,
+                             double K, const std::vector<double>& sk, const std::vector<double>& v,
+                             const std::vector<double>& L, double eps, int precision) {
+  const int D = int(L.size());
+  const bool f32 = precision == 1;
+#define FB_SHARD(DD)                                                                                               \
+  return f32 ? PotentialPtr(new NUwUImpl<DD, float>(radii_local, K, sk, v, L, eps, n_total, weight_sum_total))    \
+             : PotentialPtr(new NUwUImpl<DD, double>(radii_local, K, sk, v, L, eps, n_total, weight_sum_total))
+  if (D == 1) FB_SHARD(1);
+  if (D == 2) FB_SHARD(2);
+  if (D == 3) FB_SHARD(3);
+#undef FB_SHARD
+  throw std::runtime_error("Invalid dimension: " + std::to_string(D));
+}
 
 PotentialPtr make_nuwu(const std::vector<double>& radii, double K, const std::vector<double>& sk,
                        const std::vector<double>& v, const std::vector<double>& L, double eps, int precision) {

@@ -50,23 +50,16 @@ inline void nuwu_mode_table(int D, int n, const double* v, const double* sk, std
 }
 
 #ifdef __CUDACC__
-// One active mode m (flat index on the n^D grid, K = n/2): reads rho(k) from
-// the R2C output bhat (sign -1, so rho(k) = conj(B(k)) for k_x >= 0 and
-// B(-k) otherwise), deconvolves it by p(k) = prod corr_a(k_a), returns the
-// mode's phi term and, with want_grad, writes the packed field at k (hgrid,
-// second field at hgrid + G in 3D).
+// rho(k) of active mode m (flat index on the n^D grid, K = n/2) read from the
+// R2C output bhat (sign -1, so rho(k) = conj(B(k)) for k_x >= 0 and B(-k)
+// otherwise), before the deconvolution.  It is linear in the points, so the
+// values of disjoint point sets add up to the value of their union.
 template <int D, typename T>
-__device__ __forceinline__ double nuwu_mode_term(int m, int n, int K, const ModeCoef& c,
-                                                 const cplx_t<T>* __restrict__ bhat, int nh0, int nf0, int nf1,
-                                                 int nf2, const double* __restrict__ corr0,
-                                                 const double* __restrict__ corr1, const double* __restrict__ corr2,
-                                                 double invN, cplx_t<T>* hgrid, int64_t G, bool want_grad) {
+__device__ __forceinline__ double2 nuwu_mode_rho(int m, int n, int K, const cplx_t<T>* __restrict__ bhat, int nh0,
+                                                 int nf1, int nf2) {
   const int kx = m % n - K;
   const int ky = (D >= 2) ? (m / n) % n - K : 0;
   const int kz = (D >= 3) ? m / (n * n) - K : 0;
-  double p = corr0[kx + K];
-  if (D >= 2) p *= corr1[ky + K];
-  if (D >= 3) p *= corr2[kz + K];
   int64_t bi;
   bool cj;
   if (kx >= 0) {
@@ -81,8 +74,25 @@ __device__ __forceinline__ double nuwu_mode_term(int m, int n, int K, const Mode
     cj = false;
   }
   const cplx_t<T> b = bhat[bi];
-  const double rr = double(b.x) / p;
-  const double ri = (cj ? -double(b.y) : double(b.y)) / p;
+  return make_double2(double(b.x), cj ? -double(b.y) : double(b.y));
+}
+
+// The mode's phi term from rho(k) (undeconvolved): deconvolves it by
+// p(k) = prod corr_a(k_a) and, with want_grad, writes the packed field at k
+// (hgrid, second field at hgrid + G in 3D).
+template <int D, typename T>
+__device__ __forceinline__ double nuwu_mode_apply(int m, int n, int K, const ModeCoef& c, double2 rho, int nf0,
+                                                  int nf1, int nf2, const double* __restrict__ corr0,
+                                                  const double* __restrict__ corr1, const double* __restrict__ corr2,
+                                                  double invN, cplx_t<T>* hgrid, int64_t G, bool want_grad) {
+  const int kx = m % n - K;
+  const int ky = (D >= 2) ? (m / n) % n - K : 0;
+  const int kz = (D >= 3) ? m / (n * n) - K : 0;
+  double p = corr0[kx + K];
+  if (D >= 2) p *= corr1[ky + K];
+  if (D >= 3) p *= corr2[kz + K];
+  const double rr = rho.x / p;
+  const double ri = rho.y / p;
   const double q = (rr * rr + ri * ri) * invN;
   const double dq = q - c.s0;
   if (want_grad) {
@@ -111,6 +121,18 @@ __device__ __forceinline__ double nuwu_mode_term(int m, int n, int K, const Mode
     }
   }
   return c.w2 * dq * dq;
+}
+
+// One active mode m: reads rho(k) from bhat, returns the mode's phi term and,
+// with want_grad, writes the packed field at k.
+template <int D, typename T>
+__device__ __forceinline__ double nuwu_mode_term(int m, int n, int K, const ModeCoef& c,
+                                                 const cplx_t<T>* __restrict__ bhat, int nh0, int nf0, int nf1,
+                                                 int nf2, const double* __restrict__ corr0,
+                                                 const double* __restrict__ corr1, const double* __restrict__ corr2,
+                                                 double invN, cplx_t<T>* hgrid, int64_t G, bool want_grad) {
+  return nuwu_mode_apply<D, T>(m, n, K, c, nuwu_mode_rho<D, T>(m, n, K, bhat, nh0, nf1, nf2), nf0, nf1, nf2, corr0,
+                               corr1, corr2, invN, hgrid, G, want_grad);
 }
 #endif
 

@@ -117,7 +117,31 @@ class CombinedPotential : public Potential {
   std::vector<PotentialPtr> parts_;
 };
 
+// One NUwU pattern whose points are split over several processes (GPUs).
+// rho(k) is linear in the points, so each shard computes the undeconvolved
+// rho of its own points at the active modes, the caller sums these over the
+// shards (one all-reduce of 2 n_rho doubles), and each shard finishes the
+// mode pass with the global rho and interpolates its own points.  Weights
+// and 1/N use the totals of all shards.
+class NUwUShard {
+ public:
+  virtual ~NUwUShard() = default;
+  virtual int64_t n_rho() const = 0;  // active modes (complex values in rho)
+  // rho[2 i], rho[2 i + 1] = rho of this shard's points at active mode i
+  virtual void shard_rho(const double* x, double* rho, cudaStream_t s) = 0;
+  // energy (every shard gets the same) and, if grad, this shard's gradient;
+  // rho holds the sum over all shards
+  virtual void shard_finish(const double* rho, double* grad, double* energy, cudaStream_t s) = 0;
+};
+
+// Sum over the points of NUwU's per-point weight factor (area^D with the
+// reference's repeated area product, nuwu.hpp:125-149), in index order.
+double nuwu_weight_factor_sum(const double* radii, int64_t n, int D);
+
 // Factories (defined per potential family).
+PotentialPtr make_nuwu_shard(const std::vector<double>& radii_local, int64_t n_total, double weight_sum_total,
+                             double K, const std::vector<double>& sk, const std::vector<double>& v,
+                             const std::vector<double>& L, double eps, int precision);
 PotentialPtr make_nuwu(const std::vector<double>& radii, double K, const std::vector<double>& sk,
                        const std::vector<double>& v, const std::vector<double>& L, double eps, int precision);
 PotentialPtr make_uwu(const std::vector<int>& grid, double K, const std::vector<double>& sk,

@@ -58,6 +58,33 @@ int fresco_abi_version(void);
 int fresco_nuwu_create(const double* radii, int64_t n_points, double K, const double* sk, const double* v,
                        int64_t n_sk, const double* L, int ndim, double eps, int precision, fresco_potential* out);
 
+/* One NUwU pattern split over processes (GPUs): the loss of
+ * fresco::NUwU::get_energy_gradient (source/fresco/nuwu.hpp:210-317) for the
+ * union of all shards' points, each shard holding radii_local[n_local].
+ * n_total is the pattern's point count and weight_sum_total the sum over all
+ * points of the per-point weight factor (fresco_nuwu_weight_sum of each shard,
+ * summed), so that the weights are normalised as nuwu.hpp:125-149 does for the
+ * whole pattern.  Per evaluation: fresco_nuwu_shard_rho on every shard, a sum
+ * of the rho arrays over the shards (one all-reduce), then
+ * fresco_nuwu_shard_finish on every shard.  The shard uses the cuFFT
+ * transforms (the band path fuses the point where the sum happens). */
+int fresco_nuwu_shard_create(const double* radii_local, int64_t n_local, int64_t n_total, double weight_sum_total,
+                             double K, const double* sk, const double* v, int64_t n_sk, const double* L, int ndim,
+                             double eps, int precision, fresco_potential* out);
+/* Sum over radii[n] of NUwU's per-point weight factor, (pi r^2)^2 in 2D and
+ * (4/3 pi r^3)^3 in 3D (the area factor applied once per dimension, nuwu.hpp:131-141). */
+int fresco_nuwu_weight_sum(const double* radii, int64_t n, int ndim, double* out);
+/* Complex values per rho array (the active modes): d_rho holds 2 * n_rho doubles. */
+int fresco_nuwu_shard_nrho(fresco_potential p, int64_t* n_rho);
+/* rho of this shard's points (d_x[n], device) at the active modes into d_rho
+ * (device), enqueued on stream.  Sums over shards give the pattern's rho. */
+int fresco_nuwu_shard_rho(fresco_potential p, const double* d_x, int64_t n, double* d_rho, void* stream);
+/* With d_rho holding the sum over all shards: *d_energy = the pattern's loss
+ * (the same on every shard) and, if d_grad is not NULL, d_grad[n] = this
+ * shard's gradient.  Uses the points of the last fresco_nuwu_shard_rho call. */
+int fresco_nuwu_shard_finish(fresco_potential p, const double* d_rho, double* d_grad, double* d_energy,
+                             void* stream);
+
 /* fresco::UwU(N, K, Sk, V, L, eps)  (source/fresco/uwu.hpp:34-50; uwu.pxd).
  * sk and v are already ifftshifted (natural FFT order, as uwu.pyx:14-15
  * passes them).  grid holds ndim ints, slowest first (FFTW row-major). */

@@ -226,24 +226,38 @@ class NUwU:
         The gradient map (nuwu.hpp:216-250) is used for rho, as in
         get_energy_gradient.
         """
-        x = coord_map(points, self.L, energy=False)  # (ndim, N)
-        act, kk = self.active_modes()
-        rho = np.zeros(act.size, dtype=np.complex128)
-        for s in range(0, self.N, chunk):
+        rho = self.rho_active(points, self.c, chunk)
+        return self.finish_active(rho, points, self.c, self.N, chunk)
+
+    def rho_active(self, points, c, chunk=1 << 15):
+        """rho at the active modes of the points `points` with weights `c` (gradient map).  It is
+        linear in the points: the values of disjoint point sets add up to that of their union."""
+        x = coord_map(points, self.L, energy=False)  # (ndim, n)
+        _, kk = self.active_modes()
+        rho = np.zeros(kk.shape[1], dtype=np.complex128)
+        for s in range(0, x.shape[1], chunk):
             ph = x[:, s : s + chunk].T @ kk
-            rho += self.c[s : s + chunk] @ np.exp(1j * ph)
+            rho += np.asarray(c[s : s + chunk]) @ np.exp(1j * ph)
+        return rho
+
+    def finish_active(self, rho, points, c, n_total, chunk=1 << 15):
+        """phi of the active modes from rho (nuwu.hpp:260-287, S = |rho|^2 / n_total) and the
+        gradient at the points `points` with weights `c` (nuwu.hpp:291-315)."""
+        x = coord_map(points, self.L, energy=False)
+        act, kk = self.active_modes()
         sk0 = self.Sk[: self.nm][act]
         v = self.V[: self.nm][act]
-        d, phi = _loss_terms(np.abs(rho) ** 2 / self.N, sk0, v)
-        factor = (4.0 / self.N) * v * d * rho
+        d, phi = _loss_terms(np.abs(rho) ** 2 / n_total, sk0, v)
+        factor = (4.0 / n_total) * v * d * rho
         factor = np.where(sk0 != 0, factor / np.where(sk0 != 0, sk0, 1.0), factor)
         fa = (-1j * kk * factor[None, :]).T  # (A, ndim): -i k_a F(k)
-        grad = np.zeros(self.N * self.ndim)
+        n = x.shape[1]
+        grad = np.zeros(n * self.ndim)
         g = grad.reshape(-1, self.ndim)
-        for s in range(0, self.N, chunk):
+        for s in range(0, n, chunk):
             e = np.exp(-1j * (x[:, s : s + chunk].T @ kk))  # iflag -1
             cx = e @ fa  # (chunk, ndim)
-            g[s : s + chunk] = np.real(cx * np.conj(self.c[s : s + chunk])[:, None])
+            g[s : s + chunk] = np.real(cx * np.conj(np.asarray(c[s : s + chunk]))[:, None])
         return phi, grad
 
 

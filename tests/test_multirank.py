@@ -113,3 +113,65 @@ def test_two_rank_ensemble_gather():
     for rank, merged, ranks in res:
         assert merged == [(i, 0.5 * i) for i in range(23)]
         assert ranks == [0, 1]
+
+
+def _shard_worker(rank, world, port, out):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from fresco_b200.shard import shard_totals
+    from oracle import oracle as O
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        x, _, Sk, V, L = O.stealthy_nuwu_inputs(900, 9, 8, ndim=2, seed=12)
+        radii = 0.5 + np.random.default_rng(13).random(900)
+        cut = [0, 350, 900]  # uneven slabs
+        pts = x.reshape(-1, 2)[cut[rank] : cut[rank + 1]].ravel()
+        r_loc = radii[cut[rank] : cut[rank + 1]]
+        n_total, ws = shard_totals(r_loc, 2)  # all-reduce over the gloo group
+        ref = O.NUwU(radii, 9, Sk, V, L)
+        c_loc = (np.pi * r_loc * r_loc) ** 2 * (n_total / ws)  # nuwu.hpp:125-149 over the whole pattern
+        rho = ref.rho_active(pts, c_loc)
+        t = torch.from_numpy(np.stack([rho.real, rho.imag]))
+        dist.all_reduce(t)  # the one exchange per evaluation
+        phi, g = ref.finish_active(t[0].numpy() + 1j * t[1].numpy(), pts, c_loc, n_total)
+        gathered = [None] * world
+        dist.all_gather_object(gathered, g)
+        out.put((rank, n_total, ws, phi, np.concatenate(gathered)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_sharded_pattern_totals_and_loss():
+    """One NUwU pattern split into two uneven slabs over two gloo ranks: the point and weight totals
+    reach every rank, and the rank-local rho summed by one all-reduce gives every rank the whole
+    pattern's loss and each rank its points' share of the gradient (oracle arithmetic standing in for
+    the device steps of fresco_b200.ShardedNUwU)."""
+    import numpy as np
+    import torch.multiprocessing as mp
+
+    from fresco_b200.shard import weight_factor_sum
+    from oracle import oracle as O
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+    assert all(p.exitcode == 0 for p in procs)
+    res = sorted((q.get(timeout=5) for _ in range(2)), key=lambda t: t[0])
+    x, _, Sk, V, L = O.stealthy_nuwu_inputs(900, 9, 8, ndim=2, seed=12)
+    radii = 0.5 + np.random.default_rng(13).random(900)
+    e_ref, g_ref = O.NUwU(radii, 9, Sk, V, L).get_energy_gradient(x)
+    for rank, n_total, ws, phi, g in res:
+        assert n_total == 900
+        assert ws == pytest.approx(weight_factor_sum(radii, 2), rel=1e-14)
+        assert phi == pytest.approx(e_ref, rel=1e-11)
+        assert np.linalg.norm(g - g_ref) <= 1e-11 * np.linalg.norm(g_ref)
