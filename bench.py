@@ -11,7 +11,9 @@ seeded inputs stand in for data (the reference uses none).
 
 Under torchrun (N > 1) every rank evaluates its own independent pattern (the
 batched-ensemble sharding: no data-path collective), timing is the max over
-ranks and ``value`` aggregates all ranks.  ``--impl reference`` times the
+ranks and ``value`` aggregates all ranks.  The ``sharded_pattern`` section
+splits one config-2 pattern over the ranks instead (one all-reduce of rho at
+the active modes per evaluation).  ``--impl reference`` times the
 reference's own CPU implementation (its C++ compiled unchanged against the
 FINUFFT-API shim backed by the CPU ES-kernel NUFFT restatement) on rank 0.
 """
@@ -158,6 +160,46 @@ def ensemble_report(args, dev, ws, rank):
         del pots, bufs
     del ens
     return out
+
+
+def sharded_report(args, dev, ws, rank):
+    """One config-2 pattern (seed 2, N = 2^20) split into equal index slabs over the job's ranks
+    (fresco_b200.ShardedNUwU, FP32): per evaluation every rank computes rho of its slab at the
+    active modes, one NCCL all-reduce sums them, every rank finishes the loss and its slab's
+    gradient.  Device-timed, max over ranks; whole-pattern evaluations per second.  With one rank
+    it is the single-GPU cost of the sharded path (cuFFT transforms; no collective)."""
+    import torch
+
+    from fresco_b200 import ShardedNUwU
+
+    x, radii, Sk, V, L = inputs(seed=2)
+    a, b = rank * N_POINTS // ws, (rank + 1) * N_POINTS // ws
+    sh = ShardedNUwU(radii[a:b], K_MODES, Sk, V, L, eps=EPS, precision="fp32")
+    dx = torch.tensor(x[2 * a : 2 * b], device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def one_eval():
+        r = sh.reduce(sh.rho(dx))
+        return sh.finish(r)
+
+    for _ in range(max(3, args.warmup)):
+        e, _ = one_eval()
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    n = max(5, args.steps)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(n):
+        e, _ = one_eval()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = reduce_max(t0.elapsed_time(t1) / n, dev)
+    return {"workload": "the config-2 NUwU pattern (seed 2) split into equal point slabs, one per rank",
+            "ranks": ws, "points_per_rank": int(b - a), "evals_per_s": round(1000.0 / ms, 2),
+            "ms_per_eval": round(ms, 5), "allreduce_bytes_per_eval": int(16 * sh.n_rho),
+            "energy": float(e.item()), "transforms": "cuFFT (pruned column passes)",
+            "timing": "CUDA events on the launch stream, max over ranks"}
 
 
 def dist_env():
@@ -454,6 +496,7 @@ def run_ours(args):
                      "peak": hbm_peak, "unit": "GB/s", "frac": round(eval_achieved / hbm_peak, 4)}
 
     ensemble = None if args.no_ensemble else ensemble_report(args, dev, ws, rank)
+    sharded = None if args.no_sharded else sharded_report(args, dev, ws, rank)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -488,6 +531,7 @@ def run_ours(args):
         "nuwu_plus_repulsion": {"evals_per_s_per_gpu": round(comb_evals, 2)},
         "lbfgs": lbfgs,
         "ensemble": ensemble,
+        "sharded_pattern": sharded,
         "accuracy": {"grad_rel_err_fp32": err32, "grad_rel_err_fp64_eps1e-6": err64, "energy_rel_err_fp32": eerr32,
                      "oracle": "GPU FP64 form at eps=1e-12 (parity-tested against exact sums)"},
         "clocks": clk,
@@ -570,6 +614,7 @@ def main():
     ap.add_argument("--cpu-samples", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble section")
+    ap.add_argument("--no-sharded", action="store_true", help="skip the sharded single-pattern section")
     ap.add_argument("--no-ensemble-loop", action="store_true",
                     help="skip timing the ensemble's patterns as separate potentials")
     args = ap.parse_args()
