@@ -120,14 +120,42 @@ __global__ void __launch_bounds__(kBlThreads) bl_dot_gg(const double* __restrict
   item_partials<1>(v, part, nitems, sl);
 }
 
+// Block-wide sums of K per-item partial slots over the items [lo, hi) of one
+// pattern (one block per pattern); the totals are valid in thread 0.
+template <int K>
+__device__ __forceinline__ void pattern_totals(const double* __restrict__ part, int nitems, int lo, int hi,
+                                               const int (&slot)[K], double (&tot)[K]) {
+  __shared__ double red[K][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double v = 0.0;
+    for (int i = lo + int(threadIdx.x); i < hi; i += blockDim.x) v += part[int64_t(slot[k]) * nitems + i];
+    v = warp_sum(v);
+    if (lane == 0) red[k][wid] = v;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) tot[k] = warp_sum(lane < nw ? red[k][lane] : 0.0);
+  }
+}
+
+constexpr int kFinThreads = 128;  // one block per pattern in the per-pattern state kernels
+
 // Initial f and rms = sqrt(|g|^2 / n) (optimizer.hpp:203-210).
-__global__ void bl_init_fin(BlState* st, const double* __restrict__ e, const PatRange* __restrict__ pr,
-                            const double* __restrict__ part, int nitems, int P, BlParams prm) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P) return;
+__global__ void __launch_bounds__(kFinThreads) bl_init_fin(BlState* st, const double* __restrict__ e,
+                                                           const PatRange* __restrict__ pr,
+                                                           const double* __restrict__ part, int nitems, int P,
+                                                           BlParams prm) {
+  const int p = blockIdx.x;
+  const int sl[1] = {B_GG};
+  double tot[1] = {0.0};
+  pattern_totals<1>(part, nitems, pr[p].lo, pr[p].hi, sl, tot);
+  if (threadIdx.x != 0) return;
   BlState s = st[p];
-  double gg = 0.0;
-  for (int i = pr[p].lo; i < pr[p].hi; ++i) gg += part[int64_t(B_GG) * nitems + i];
+  const double gg = tot[0];
   s.f = e[p];
   s.rms = sqrt(gg * s.inv_n);
   s.nfev += 1;
@@ -173,6 +201,7 @@ __global__ void __launch_bounds__(kBlThreads) bl_dir_start(const double* __restr
     for (int64_t i = it.i0 + threadIdx.x; i < it.i1; i += blockDim.x) v[0] += g[i] * g[i];
   } else {
     const double* si = S + int64_t((s.k - 1) % M) * nd;
+    #pragma unroll 4
     for (int64_t i = it.i0 + threadIdx.x; i < it.i1; i += blockDim.x) {
       const double gi = g[i];
       step[i] = gi;
@@ -242,6 +271,7 @@ __global__ void __launch_bounds__(kBlThreads) bl_update(int u, double* __restric
   }
   const double h0 = -s.H0;
   double v[2] = {0.0, 0.0};
+  #pragma unroll 4
   for (int64_t i = it.i0 + threadIdx.x; i < it.i1; i += blockDim.x) {
     double x = step[i] - coef * vec[i];
     if (scale) x *= h0;
@@ -280,6 +310,7 @@ __global__ void __launch_bounds__(kBlThreads) bl_trial(const double* __restrict_
   double factor = 1.0;
   if (factor * stepnorm > prm.maxstep) factor = prm.maxstep / stepnorm;
   for (int q = 0; q < s.nred; ++q) factor *= 0.5;
+  #pragma unroll 4
   for (int64_t i = it.i0 + threadIdx.x; i < it.i1; i += blockDim.x) XT[i] = X[i] + factor * (sgn * step[i]);
 }
 
@@ -298,6 +329,7 @@ __global__ void __launch_bounds__(kBlThreads) bl_post(double* __restrict__ X, do
   double* sk = S + int64_t(kl) * nd;
   double* yk = Y + int64_t(kl) * nd;
   double v[3] = {0.0, 0.0, 0.0};
+  #pragma unroll 4
   for (int64_t i = it.i0 + threadIdx.x; i < it.i1; i += blockDim.x) {
     const double gi = GT[i];
     const double yi = gi - G[i];
@@ -315,22 +347,26 @@ __global__ void __launch_bounds__(kBlThreads) bl_post(double* __restrict__ X, do
   item_partials<3>(v, part, nitems, sl);
 }
 
-// Per-pattern state update (lbfgs.cpp:86-104, 206-245).
-__global__ void bl_finalize(BlState* st, const double* __restrict__ e, double* rho, const PatRange* __restrict__ pr,
-                            BlParams prm, const double* __restrict__ part, int nitems, int P) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P) return;
+// Per-pattern state update (lbfgs.cpp:86-104, 206-245); one block per
+// pattern sums the pattern's item partials.
+__global__ void __launch_bounds__(kFinThreads) bl_finalize(BlState* st, const double* __restrict__ e, double* rho,
+                                                           const PatRange* __restrict__ pr, BlParams prm,
+                                                           const double* __restrict__ part, int nitems, int P) {
+  const int p = blockIdx.x;
   BlState s = st[p];
-  if (!s.active) return;
-  s.nfev += 1;
+  if (!s.active) return;  // uniform over the block
   const double fnew = e[p];
-  if (bl_accept(s, fnew, prm)) {
-    double gg = 0.0, ys = 0.0, yy = 0.0;
-    for (int i = pr[p].lo; i < pr[p].hi; ++i) {
-      gg += part[int64_t(B_GG) * nitems + i];
-      ys += part[int64_t(B_YS) * nitems + i];
-      yy += part[int64_t(B_YY) * nitems + i];
-    }
+  const bool accept = bl_accept(s, fnew, prm);
+  double tot[3] = {0.0, 0.0, 0.0};
+  if (accept) {
+    const int sl[3] = {B_GG, B_YS, B_YY};
+    pattern_totals<3>(part, nitems, pr[p].lo, pr[p].hi, sl, tot);
+  }
+  if (threadIdx.x != 0) return;
+  s.nfev += 1;
+  if (accept) {
+    const double gg = tot[0];
+    double ys = tot[1], yy = tot[2];
     s.f = fnew;
     s.rms = sqrt(gg) * s.inv_sqrt_n;
     if (ys == 0.0) ys = 1.0;
@@ -395,7 +431,7 @@ struct EnsembleLbfgs::Impl {
   void initialize() {
     ens->eval(X.p, G.p, E.p, s);
     bl_dot_gg<<<nitems, kBlThreads, 0, s>>>(G.p, items.p, part.p, nitems);
-    bl_init_fin<<<int(ceil_div(P, 128)), 128, 0, s>>>(st.p, E.p, pr.p, part.p, nitems, P, bp);
+    bl_init_fin<<<P, kFinThreads, 0, s>>>(st.p, E.p, pr.p, part.p, nitems, P, bp);
     FB_LAUNCH_CHECK();
     initialized = true;
   }
@@ -410,7 +446,7 @@ struct EnsembleLbfgs::Impl {
     ens->eval(XT.p, GT.p, E.p, q);
     bl_post<<<nitems, kBlThreads, 0, q>>>(X.p, G.p, XT.p, GT.p, S.p, Y.p, nd, items.p, st.p, E.p, bp, part.p,
                                           nitems);
-    bl_finalize<<<int(ceil_div(P, 128)), 128, 0, q>>>(st.p, E.p, rho.p, pr.p, bp, part.p, nitems, P);
+    bl_finalize<<<P, kFinThreads, 0, q>>>(st.p, E.p, rho.p, pr.p, bp, part.p, nitems, P);
     FB_LAUNCH_CHECK();
   }
 
