@@ -202,6 +202,77 @@ def sharded_report(args, dev, ws, rank):
             "timing": "CUDA events on the launch stream, max over ranks"}
 
 
+def other_configs_report(args, dev):
+    """Device-timed loss+gradient evaluations per second of the other configurations' potentials on
+    this GPU (each input exceeds the 126 MB L2 or is evaluated back to back; no flush): config 3 3D
+    NUwU (N = 2^21, 129^3 modes, radial S0 and V) FP32 and FP64, config 4 UwU on 4096^2 and UwNU on
+    2048^2 against 100,000 k-points FP32 and FP64, config 1 NUwU (N = 4096, 65^2 modes) FP64."""
+    import torch
+
+    from fresco_b200 import NUwU, UwNU, UwU
+
+    def rate(pot, x):
+        xd = torch.tensor(x, device=dev)
+        g = torch.empty_like(xd)
+        e = torch.zeros((), dtype=torch.float64, device=dev)
+        for _ in range(3):
+            pot.energy_gradient_device(xd, grad=g, out=e)
+        torch.cuda.synchronize()
+        n = max(5, args.steps // 2)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(n):
+            pot.energy_gradient_device(xd, grad=g, out=e)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / n
+        return {"evals_per_s": round(1000.0 / ms, 2), "ms_per_eval": round(ms, 4)}
+
+    out = {}
+    rng = np.random.default_rng(3)
+    n3, k3 = 1 << 21, 64
+    x3 = rng.random(3 * n3) * 2 * np.pi
+    kv = np.arange(-k3, k3 + 1)
+    kz, ky, kx = np.meshgrid(kv, kv, kv, indexing="ij")
+    mag = np.sqrt(kx ** 2 + ky ** 2 + kz ** 2).ravel().astype(np.float64)
+    sk3, v3 = 1.0 - np.exp(-((mag / 16.0) ** 2)), np.where(mag > 0, 1.0 / (1.0 + mag), 0.0)
+    out["config3_nuwu3d"] = {"workload": "3D NUwU, N=2097152 uniform in [0,2pi)^3, 129^3 modes, "
+                             "S0=1-exp(-(|k|/16)^2), V=1/(1+|k|), V(0)=0, eps=1e-6"}
+    for prec in ("fp32", "fp64"):
+        out["config3_nuwu3d"][prec] = rate(NUwU(np.ones(n3), k3, sk3, v3, np.full(3, 2 * np.pi), eps=EPS,
+                                                precision=prec), x3)
+    del x3, sk3, v3, mag, kx, ky, kz
+    rng = np.random.default_rng(4)
+    g4 = 4096
+    xg = rng.random(g4 * g4)
+    k = np.arange(g4) - g4 // 2
+    m4 = np.sqrt(k[:, None] ** 2 + k[None, :] ** 2)
+    v4 = ((m4 <= 64) & (m4 > 0)).astype(np.float64)
+    out["config4_uwu"] = {"workload": "UwU on a 4096^2 grid, x uniform in [0,1], S0=0 & V=1 on 0<|k|<=64"}
+    for prec in ("fp32", "fp64"):
+        out["config4_uwu"][prec] = rate(UwU(np.array([g4, g4]), 64, np.zeros_like(v4), v4, np.ones(2),
+                                            precision=prec), xg)
+    del xg, m4, v4
+    rng = np.random.default_rng(4)
+    gu, mk = 2048, 100_000
+    xu = rng.random(gu * gu)
+    r = 512 * np.sqrt(rng.random(mk))
+    t = 2 * np.pi * rng.random(mk)
+    kp = (np.stack([r * np.cos(t), r * np.sin(t)], axis=1) / gu).ravel()
+    sku = np.zeros(mk)
+    sku[rng.choice(mk, 64, replace=False)] = float(np.sum(xu))
+    out["config4_uwnu"] = {"workload": "UwNU on a 2048^2 grid against 100,000 k-points uniform in |k|<=512, "
+                                       "S0 = sum(x) at 64 peaks, V=1, eps=1e-6"}
+    for prec in ("fp32", "fp64"):
+        out["config4_uwnu"][prec] = rate(UwNU(np.array([gu, gu]), kp, sku, np.ones(mk), np.ones(2), eps=EPS,
+                                              precision=prec), xu)
+    x1, r1, sk1, v1, l1 = stealthy_inputs(4096, 32, 16, seed=1)
+    out["config1_nuwu"] = {"workload": "2D NUwU, N=4096, 65^2 modes, S0=0 & V=1 on 0<|k|<=16, eps=1e-12",
+                           "fp64": rate(NUwU(r1, 32, sk1.ravel(), v1.ravel(), l1, eps=1e-12, precision="fp64"), x1)}
+    out["timing"] = "CUDA events around back-to-back evaluations on one GPU (graph replay), after 3 warm-ups"
+    return out
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -497,6 +568,7 @@ def run_ours(args):
 
     ensemble = None if args.no_ensemble else ensemble_report(args, dev, ws, rank)
     sharded = None if args.no_sharded else sharded_report(args, dev, ws, rank)
+    others = None if (args.no_other_configs or ws > 1) else other_configs_report(args, dev)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -532,6 +604,7 @@ def run_ours(args):
         "lbfgs": lbfgs,
         "ensemble": ensemble,
         "sharded_pattern": sharded,
+        "other_configs": others,
         "accuracy": {"grad_rel_err_fp32": err32, "grad_rel_err_fp64_eps1e-6": err64, "energy_rel_err_fp32": eerr32,
                      "oracle": "GPU FP64 form at eps=1e-12 (parity-tested against exact sums)"},
         "clocks": clk,
@@ -615,6 +688,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble section")
     ap.add_argument("--no-sharded", action="store_true", help="skip the sharded single-pattern section")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="skip the throughput of the other configurations' potentials")
     ap.add_argument("--no-ensemble-loop", action="store_true",
                     help="skip timing the ensemble's patterns as separate potentials")
     args = ap.parse_args()
