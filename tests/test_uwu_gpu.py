@@ -58,3 +58,55 @@ def test_fire_uwu_golden_trajectory():
     r = opt.get_result()
     assert rel(r.coords, d["x_final"]) < 1e-10
     assert r.nfev == int(d["nfev"])
+
+
+@pytest.mark.parametrize("N,kb", [(512, 40), (1024, 100)])
+def test_uwu_band_transforms(N, kb):
+    """N x N grids (N a power of two >= 512) with the active entries in a narrow band of the
+    half spectrum take the band kernels (register FFTs reading and writing the FP64 arrays):
+    asymmetric targets against the oracle's FFTs, accumulation, the exact gradient mode, and a
+    non-finite intensity."""
+    import torch
+
+    from fresco_b200 import CombinedPotential, UwU
+    from fresco_b200.autograd import structure_factor_loss
+
+    rng = np.random.default_rng(N + kb)
+    x = rng.random(N * N)
+    k = np.fft.fftshift(np.fft.fftfreq(N, 1.0 / N))  # centred layout, as the reference's Python layer takes it
+    inside = (np.abs(k)[:, None] <= kb) & (np.abs(k)[None, :] <= kb)
+    Sk = np.where(inside & (rng.random((N, N)) < 0.5), 1e-3 + 1e-3 * rng.random((N, N)), 0.0)
+    V = np.where(inside & (rng.random((N, N)) < 0.7), rng.random((N, N)), 0.0)
+    V[N // 2, N // 2] = 0.0
+    ref = O.UwU(np.array([N, N]), kb, Sk, V, np.ones(2))
+    e0, g0 = ref.get_energy_gradient(x)
+    for prec, tol in [("fp64", 1e-10), ("fp32", 1e-5)]:
+        p = UwU(np.array([N, N]), kb, Sk, V, np.ones(2), precision=prec)
+        assert "fft=band" in p.describe(), p.describe()
+        e, g = p.get_energy_gradient(x)
+        assert rel(e, e0) < tol, prec
+        assert rel(g, g0) < tol, prec
+        assert rel(p.get_energy(x), e0) < tol, prec
+        assert p.status() == 0
+    # accumulation (CombinedPotential of the same potential twice)
+    p = UwU(np.array([N, N]), kb, Sk, V, np.ones(2))
+    c = CombinedPotential()
+    c.add_potential(p)
+    c.add_potential(p)
+    ec, gc = c.get_energy_gradient(x)
+    assert rel(ec, 2 * e0) < 1e-10 and rel(gc, 2 * g0) < 1e-10
+    # exact mode: autograd against central differences
+    xt = torch.tensor(x, device="cuda", requires_grad=True)
+    structure_factor_loss(p, xt).backward()
+    ga = xt.grad.cpu().numpy()
+    idx = rng.choice(x.size, 8, replace=False)
+    for i in idx:
+        xp, xm = x.copy(), x.copy()
+        xp[i] += 1e-4
+        xm[i] -= 1e-4
+        fd = (p.get_energy(xp) - p.get_energy(xm)) / 2e-4
+        assert abs(fd - ga[i]) <= 1e-5 * np.max(np.abs(ga)), (i, fd, ga[i])
+    xb = x.copy()
+    xb[7] = np.nan
+    eb, gb = p.get_energy_gradient(xb)
+    assert np.isnan(eb) and np.isnan(gb).any() and p.status() != 0
