@@ -315,20 +315,17 @@ __global__ void fi_mix(double* __restrict__ v, const double* __restrict__ g, int
   block_partials<1>(acc, part, P, sl);
 }
 
-// x_old = x, g_old = g, x += dx * factor (modified_fire.hpp:146-155).
-__global__ void fi_step(double* __restrict__ x, double* __restrict__ xo, const double* __restrict__ g,
-                        double* __restrict__ go, const double* __restrict__ v, int64_t n, FiState* st, double* part,
-                        int P) {
+// x_new = x + dx * factor (modified_fire.hpp:146-155), written to the other
+// coordinate buffer: x and its gradient stay where they are for a step back.
+__global__ void fi_step(const double* __restrict__ x, double* __restrict__ xnew, const double* __restrict__ v,
+                        int64_t n, FiState* st, double* part, int P) {
   const double normdx = sqrt(sum_parts(part + int64_t(F_DD) * P, P));
   double factor = 1.0;
   if (normdx > st->maxstep) factor = st->maxstep / normdx;
   const double dt = st->dt;
   GRID_LOOP(i, n) {
-    const double xi = x[i];
-    xo[i] = xi;
-    go[i] = g[i];
     const double dx = dt * v[i];
-    x[i] = xi + dx * factor;
+    xnew[i] = x[i] + dx * factor;
   }
 }
 
@@ -378,18 +375,11 @@ __global__ void fi_fin(FiState* st, const double* __restrict__ e, double* part, 
   out[6] = double(st->fire_iter);
 }
 
-// P <= 0: v = 0 and, with stepback, x = x_old, g = g_old (modified_fire.hpp:204-212).
-__global__ void fi_restore(double* __restrict__ x, const double* __restrict__ xo, double* __restrict__ g,
-                           const double* __restrict__ go, double* __restrict__ v, int64_t n, const FiState* st) {
+// P <= 0: v = 0 (modified_fire.hpp:204-212); the step back to x_old, g_old
+// is the host keeping the previous coordinate and gradient buffers.
+__global__ void fi_restore(double* __restrict__ v, int64_t n, const FiState* st) {
   if (!st->restore) return;
-  const bool sb = st->stepback != 0;
-  GRID_LOOP(i, n) {
-    v[i] = 0.0;
-    if (sb) {
-      x[i] = xo[i];
-      g[i] = go[i];
-    }
-  }
+  GRID_LOOP(i, n) v[i] = 0.0;
 }
 
 // ---------------------------------------------------------------------------
@@ -558,16 +548,16 @@ class Fire final : public Optimizer {
   Fire(PotentialPtr pot, const double* x0, int64_t n, const FireParams& p)
       : Optimizer(pot, n, p.tol, p.maxiter, p.iprint, p.verbosity), prm_(p) {
     const int64_t nn = std::max<int64_t>(n, 1);
-    X_.alloc(nn);
-    XO_.alloc(nn);
-    G_.alloc(nn);
-    GO_.alloc(nn);
+    for (int b = 0; b < 2; ++b) {
+      X_[b].alloc(nn);
+      G_[b].alloc(nn);
+      FB_CUDA(cudaMemsetAsync(G_[b].p, 0, G_[b].bytes(), s_));
+    }
     V_.alloc(nn);
     e_.alloc(1);
     st_.alloc(1);
     part_.alloc(int64_t(F_NSLOT) * P_);
     FB_CUDA(cudaMemsetAsync(V_.p, 0, V_.bytes(), s_));
-    FB_CUDA(cudaMemsetAsync(G_.p, 0, G_.bytes(), s_));
     FB_CUDA(cudaMemsetAsync(part_.p, 0, part_.bytes(), s_));
     FiState h{};
     h.f = 0.0;
@@ -584,17 +574,17 @@ class Fire final : public Optimizer {
     h.Nmin = p.Nmin;
     h.stepback = p.stepback ? 1 : 0;
     FB_CUDA(cudaMemcpyAsync(st_.p, &h, sizeof(h), cudaMemcpyHostToDevice, s_));
-    if (n > 0) FB_CUDA(cudaMemcpyAsync(X_.p, x0, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
+    if (n > 0) FB_CUDA(cudaMemcpyAsync(X_[0].p, x0, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
     FB_CUDA(cudaStreamSynchronize(s_));
   }
 
-  double* device_x() override { return X_.p; }
-  double* device_g() override { return G_.p; }
+  double* device_x() override { return X_[cur_].p; }
+  double* device_g() override { return G_[cur_].p; }
 
   void set_func_gradient(double f, const double* grad, int64_t n) override {
     if (n != n_) throw InvalidArgument("the gradient has the wrong size");
     if (iter_ > 0) std::printf("warning: setting f and grad after the first iteration.  this is dangerous.\n");
-    FB_CUDA(cudaMemcpyAsync(G_.p, grad, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
+    FB_CUDA(cudaMemcpyAsync(G_[cur_].p, grad, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
     FB_CUDA(cudaMemcpyAsync(e_.p, &f, sizeof(double), cudaMemcpyHostToDevice, s_));
     init_from_gradient();
   }
@@ -603,8 +593,8 @@ class Fire final : public Optimizer {
     if (n != n_) throw InvalidArgument("The number of degrees of freedom (x0.size()) cannot change when calling reset()");
     if (!func_initialized_) initialize_func_gradient();
     iter_ = 0;
-    FB_CUDA(cudaMemcpyAsync(X_.p, x0, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
-    eval(X_.p, G_.p, e_.p);
+    FB_CUDA(cudaMemcpyAsync(X_[cur_].p, x0, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
+    eval(X_[cur_].p, G_[cur_].p, e_.p);
     nfev_ = 1;
     FiState h{};
     FB_CUDA(cudaMemcpyAsync(&h, st_.p, sizeof(h), cudaMemcpyDeviceToHost, s_));
@@ -621,15 +611,18 @@ class Fire final : public Optimizer {
   void one_iteration() override {
     ++nfev_;
     ++iter_;
-    fi_mix<<<P_, kThreads, 0, s_>>>(V_.p, G_.p, n_, st_.p, part_.p, P_);
-    fi_step<<<P_, kThreads, 0, s_>>>(X_.p, XO_.p, G_.p, GO_.p, V_.p, n_, st_.p, part_.p, P_);
+    const int nxt = 1 - cur_;
+    fi_mix<<<P_, kThreads, 0, s_>>>(V_.p, G_[cur_].p, n_, st_.p, part_.p, P_);
+    fi_step<<<P_, kThreads, 0, s_>>>(X_[cur_].p, X_[nxt].p, V_.p, n_, st_.p, part_.p, P_);
     FB_LAUNCH_CHECK();
-    eval(X_.p, G_.p, e_.p);
-    fi_post<<<P_, kThreads, 0, s_>>>(V_.p, G_.p, n_, part_.p, P_);
+    eval(X_[nxt].p, G_[nxt].p, e_.p);
+    fi_post<<<P_, kThreads, 0, s_>>>(V_.p, G_[nxt].p, n_, part_.p, P_);
     fi_fin<<<1, 256, 0, s_>>>(st_.p, e_.p, part_.p, P_, host_);
-    fi_restore<<<P_, kThreads, 0, s_>>>(X_.p, XO_.p, G_.p, GO_.p, V_.p, n_, st_.p);
+    fi_restore<<<P_, kThreads, 0, s_>>>(V_.p, n_, st_.p);
     FB_LAUNCH_CHECK();
     FB_CUDA(cudaStreamSynchronize(s_));
+    // the new point stays unless the step was uphill and the step back is on
+    if (host_[4] > 0 || !prm_.stepback) cur_ = nxt;
     f_ = host_[0];
     rms_ = host_[1];
     if (verbosity_ > 1 && !(host_[4] > 0)) std::printf("warning: step direction was uphill.  inverting\n");
@@ -642,7 +635,7 @@ class Fire final : public Optimizer {
 
  private:
   void init_from_gradient() {
-    fi_init_v<<<P_, kThreads, 0, s_>>>(G_.p, V_.p, n_, st_.p, part_.p, P_);
+    fi_init_v<<<P_, kThreads, 0, s_>>>(G_[cur_].p, V_.p, n_, st_.p, part_.p, P_);
     fi_init_fin<<<1, 256, 0, s_>>>(st_.p, e_.p, part_.p, P_, host_);
     FB_LAUNCH_CHECK();
     FB_CUDA(cudaStreamSynchronize(s_));
@@ -653,12 +646,14 @@ class Fire final : public Optimizer {
 
   void initialize_func_gradient() override {
     ++nfev_;
-    eval(X_.p, G_.p, e_.p);
+    eval(X_[cur_].p, G_[cur_].p, e_.p);
     init_from_gradient();
   }
 
   FireParams prm_;
-  DevBuf<double> X_, XO_, G_, GO_, V_, e_;
+  DevBuf<double> X_[2], G_[2];  // current point and its gradient in [cur_], the trial in the other
+  int cur_ = 0;
+  DevBuf<double> V_, e_;
   DevBuf<FiState> st_;
 };
 
