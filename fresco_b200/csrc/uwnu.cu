@@ -16,7 +16,9 @@
 // (complex strengths), one C2C transform (sign -1), and a pass that
 // deconvolves and writes the gradient.
 #include <cmath>
+#include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "nufft.cuh"
@@ -174,11 +176,13 @@ class UwNUImpl final : public Potential {
     int dims[3];
     for (int a = 0; a < D_; ++a) dims[a] = geom_.nf[D_ - 1 - a];
     FB_CUFFT(cufftPlanMany(&plan_, D_, dims, nullptr, 1, 0, nullptr, 1, 0, sizeof(T) == 4 ? CUFFT_C2C : CUFFT_Z2Z, 1));
+    if (D_ == 2) setup_pruned();
     FB_CUDA(cudaDeviceSynchronize());
   }
 
   ~UwNUImpl() override {
     if (plan_) cufftDestroy(plan_);
+    for (auto& kv : plans_) cufftDestroy(kv.second);
   }
 
   int64_t ndof() const override { return G_; }
@@ -188,6 +192,11 @@ class UwNUImpl final : public Potential {
     for (int a = 0; a < D_; ++a) s += (a ? "x" : "") + std::to_string(n_[a]);
     s += " kpoints=" + std::to_string(M_) + " w=" + std::to_string(es_.w) + " nf=";
     for (int a = 0; a < D_; ++a) s += (a ? "x" : "") + std::to_string(geom_.nf[a]);
+    if (pruned_) {
+      int nc = 0;
+      for (auto& r : col_ranges_) nc += r.second;
+      s += " fft=pruned rows=" + std::to_string(n_[1]) + " cols=" + std::to_string(nc);
+    }
     return s;
   }
 
@@ -207,6 +216,90 @@ class UwNUImpl final : public Potential {
     }
   }
 
+  // 2D: the 2D transforms as row and column passes that skip what is zero
+  // or never read.  The input of the type-2 transform is non-zero only on the
+  // rows of the grid modes (k1 in [-n1/2, n1/2)), and the interpolation reads
+  // only the columns that the tiles of the k-points' bins reach (found here
+  // from the k-point sort, which never changes); the type-1 input is
+  // non-zero only on those columns and the extraction reads only the mode
+  // rows.  So: type 2 = row FFTs of the mode rows (H -> T2, whose other rows
+  // stay zero) + column FFTs of the reached columns (in place); type 1 =
+  // column FFTs of the reached columns + row FFTs of the mode rows (in place).
+  void setup_pruned() {
+    pruned_ = false;
+    const int nf0 = int(geom_.nf[0]), nf1 = int(geom_.nf[1]);
+    const int nbins = int(geom_.nbins());
+    std::vector<int> bs(nbins + 1);
+    FB_CUDA(cudaMemcpy(bs.data(), sort_.bin_start.p, sizeof(int) * (nbins + 1), cudaMemcpyDeviceToHost));
+    std::vector<char> col(nf0, 0);
+    const int w = es_.w;
+    for (int b = 0; b < nbins; ++b) {
+      if (bs[b + 1] == bs[b]) continue;
+      const int c0 = (b % geom_.nb[0]) * kTile2D;
+      for (int c = c0 - w - 4; c < c0 + kTile2D + w + 4; ++c) col[((c % nf0) + nf0) % nf0] = 1;
+    }
+    std::vector<std::pair<int, int>> cr;  // [start, length) column ranges
+    for (int c = 0; c < nf0;) {
+      if (!col[c]) { ++c; continue; }
+      int e = c;
+      while (e < nf0 && col[e]) ++e;
+      cr.push_back({c, e - c});
+      c = e;
+    }
+    int ncols = 0;
+    for (auto& r : cr) ncols += r.second;
+    if (cr.size() > 4 || 2 * ncols > 3 * nf0 / 2 + 1) return;  // not worth it
+    col_ranges_ = cr;
+    const int rpos = n_[1] - n_[1] / 2, rneg = n_[1] / 2;  // mode rows [0, rpos) and [nf1 - rneg, nf1)
+    row_ranges_.clear();
+    if (rpos > 0) row_ranges_.push_back({0, rpos});
+    if (rneg > 0) row_ranges_.push_back({nf1 - rneg, rneg});
+    T2_.alloc(geom_.G());
+    FB_CUDA(cudaMemset(T2_.p, 0, T2_.bytes()));
+    const cufftType ty = sizeof(T) == 4 ? CUFFT_C2C : CUFFT_Z2Z;
+    for (auto& r : row_ranges_) plan_for(1, r.second, ty);
+    for (auto& r : col_ranges_) plan_for(0, r.second, ty);
+    pruned_ = true;
+  }
+
+  // batched 1D plan: kind 1 = rows (length nf0, contiguous), 0 = columns (length nf1, stride nf0)
+  cufftHandle plan_for(int kind, int batch, cufftType ty) {
+    const int64_t key = int64_t(kind) << 32 | uint32_t(batch);
+    auto it = plans_.find(key);
+    if (it != plans_.end()) return it->second;
+    const int nf0 = int(geom_.nf[0]), nf1 = int(geom_.nf[1]);
+    cufftHandle h = 0;
+    if (kind == 1) {
+      int n = nf0, emb = nf0;
+      FB_CUFFT(cufftPlanMany(&h, 1, &n, &emb, 1, nf0, &emb, 1, nf0, ty, batch));
+    } else {
+      int n = nf1, emb = nf1;
+      FB_CUFFT(cufftPlanMany(&h, 1, &n, &emb, nf0, 1, &emb, nf0, 1, ty, batch));
+    }
+    plans_[key] = h;
+    return h;
+  }
+
+  void exec1(cufftHandle plan, cplx_t<T>* in, cplx_t<T>* out, int dir, cudaStream_t s) {
+    FB_CUFFT(cufftSetStream(plan, s));
+    if (sizeof(T) == 4) {
+      FB_CUFFT(cufftExecC2C(plan, reinterpret_cast<cufftComplex*>(in), reinterpret_cast<cufftComplex*>(out), dir));
+    } else {
+      FB_CUFFT(cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(in),
+                            reinterpret_cast<cufftDoubleComplex*>(out), dir));
+    }
+  }
+
+  void rows_pass(cplx_t<T>* in, cplx_t<T>* out, int dir, cudaStream_t s) {
+    const cufftType ty = sizeof(T) == 4 ? CUFFT_C2C : CUFFT_Z2Z;
+    const int64_t nf0 = geom_.nf[0];
+    for (auto& r : row_ranges_) exec1(plan_for(1, r.second, ty), in + r.first * nf0, out + r.first * nf0, dir, s);
+  }
+  void cols_pass(cplx_t<T>* buf, int dir, cudaStream_t s) {
+    const cufftType ty = sizeof(T) == 4 ? CUFFT_C2C : CUFFT_Z2Z;
+    for (auto& r : col_ranges_) exec1(plan_for(0, r.second, ty), buf + r.first, buf + r.first, dir, s);
+  }
+
   void run(const double* x, double* g, double* e, bool acc, cudaStream_t s) {
     timer_begin(s);
     begin_eval_status(s);
@@ -215,9 +308,16 @@ class UwNUImpl final : public Potential {
     uwnu_precorrect_kernel<T><<<grid, kThreads, 0, s>>>(x, G_, D_, n_[0], n_[1], n_[2], geom_, corr_[0].p, corr_[1].p,
                                                         corr_[2].p, H_.p, status_.p);
     FB_LAUNCH_CHECK();
-    exec(H_.p, Gf_.p, CUFFT_INVERSE, s);  // sign +1
+    cplx_t<T>* t2 = Gf_.p;
+    if (pruned_) {
+      t2 = T2_.p;
+      rows_pass(H_.p, t2, CUFFT_INVERSE, s);  // sign +1
+      cols_pass(t2, CUFFT_INVERSE, s);
+    } else {
+      exec(H_.p, Gf_.p, CUFFT_INVERSE, s);  // sign +1
+    }
     timer_mark("type2_fft", s);
-    interp<T>(recs_.p, M_, nullptr, T(1), sort_, geom_, poly_, Gf_.p, 1, INTERP_CPLX, nullptr, rho_.p, 0, nullptr,
+    interp<T>(recs_.p, M_, nullptr, T(1), sort_, geom_, poly_, t2, 1, INTERP_CPLX, nullptr, rho_.p, 0, nullptr,
               s);
     timer_mark("type2_interp", s);
     const int mg = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(M_, kThreads), int64_t(sm_count()) * 4)));
@@ -228,7 +328,12 @@ class UwNUImpl final : public Potential {
     FB_CUDA(cudaMemsetAsync(Gf_.p, 0, Gf_.bytes(), s));
     spread_cplx<T>(recs_.p, f_.p, sort_, geom_, poly_, Gf_.p, s);
     timer_mark("type1_spread", s);
-    exec(Gf_.p, Gf_.p, CUFFT_FORWARD, s);  // sign -1, in place
+    if (pruned_) {
+      cols_pass(Gf_.p, CUFFT_FORWARD, s);  // sign -1, in place
+      rows_pass(Gf_.p, Gf_.p, CUFFT_FORWARD, s);
+    } else {
+      exec(Gf_.p, Gf_.p, CUFFT_FORWARD, s);  // sign -1, in place
+    }
     uwnu_extract_kernel<T><<<grid, kThreads, 0, s>>>(Gf_.p, G_, D_, n_[0], n_[1], n_[2], geom_, corr_[0].p,
                                                      corr_[1].p, corr_[2].p, g, acc ? 1 : 0,
                                                      grad_mode_ == 1 ? 1.0 : 1.0 / kTwoPi);
@@ -248,6 +353,10 @@ class UwNUImpl final : public Potential {
   DevBuf<double> corr_[3], sk_, v_;
   DevBuf<double2> rho_;
   cufftHandle plan_ = 0;
+  bool pruned_ = false;
+  DevBuf<cplx_t<T>> T2_;  // type-2 transform output (pruned passes; rows outside the mode rows stay zero)
+  std::vector<std::pair<int, int>> row_ranges_, col_ranges_;
+  std::map<int64_t, cufftHandle> plans_;
 };
 
 }  // namespace
