@@ -1035,6 +1035,101 @@ __global__ void __launch_bounds__(256) interp_kernel(const Rec<D, T>* __restrict
   }
 }
 
+// 3D interpolation: one block per subproblem stages its bin's tile (+ halo,
+// tile + w cells per dimension, origin tile origin - w/2) of one field at a
+// time in shared memory and one thread per point sums its w^3 taps from it
+// (instead of gathering them from L2).  With two fields the first pass keeps
+// each point's sums in registers for the second.
+template <int W, typename T, int NF>
+__global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
+    const Rec<3, T>* __restrict__ recs, const T* __restrict__ weights, T uniform, const int* __restrict__ sub_bin,
+    const int* __restrict__ sub_start, const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g,
+    const EsPoly<W, T> poly, const cplx_t<T>* __restrict__ fields, int mode, double* grad, double2* out2,
+    int accumulate, const int* __restrict__ status, const GradScale gs) {
+  constexpr int PAD = W / 2;
+  constexpr int PPT = (kMaxSub + 255) / 256;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx_t<T>* tile = reinterpret_cast<cplx_t<T>*>(smem_raw);
+  const int sub = blockIdx.x;
+  if (sub >= *num_sub) return;
+  const int bin = sub_bin[sub], start = sub_start[sub], cnt = sub_count[sub];
+  const int bx = bin % g.nb[0], rb = bin / g.nb[0];
+  const int by = rb % g.nb[1], bz = rb / g.nb[1];
+  const int org0 = bx * g.tile[0], org1 = by * g.tile[1], org2 = bz * g.tile[2];
+  const int TX = g.tile[0] + W, TY = g.tile[1] + W, TZ = g.tile[2] + W;
+  const int ncell = TX * TY * TZ;
+  const bool bad = status != nullptr && ((*status) & STATUS_NONFINITE_INPUT);
+  const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
+  const int tid = threadIdx.x;
+  T acc_r[PPT], acc_i[PPT];
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) acc_r[k] = acc_i[k] = T(0);
+  for (int f = 0; f < NF; ++f) {
+    const cplx_t<T>* fld = fields + f * g.G();
+    if (f) __syncthreads();  // every thread is done with the previous field's tile
+    constexpr int BT = 4;    // loads in flight per thread
+    for (int i0 = tid; i0 < ncell; i0 += BT * 256) {
+      cplx_t<T> v[BT];
+#pragma unroll
+      for (int b = 0; b < BT; ++b) {
+        const int i = i0 + b * 256;
+        if (i < ncell) {
+          const int x = i % TX, r = i / TX;
+          const int y = r % TY, z = r / TY;
+          v[b] = fld[(int64_t(wrap_index(org2 - PAD + z, nf2)) * nf1 + wrap_index(org1 - PAD + y, nf1)) * nf0 +
+                     wrap_index(org0 - PAD + x, nf0)];
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < BT; ++b)
+        if (i0 + b * 256 < ncell) tile[i0 + b * 256] = v[b];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+      const int p = tid + 256 * k;
+      if (p >= cnt) break;
+      const Rec<3, T> r = recs[start + p];
+      int c0, c1, c2;
+      unpack_cell(3, r.cell, c0, c1, c2);
+      T k0[W], k1[W], k2[W];
+      const int l0 = c0 - org0 + es_taps<W, T>(r.f[0], poly, k0) + PAD;
+      const int l1 = c1 - org1 + es_taps<W, T>(r.f[1], poly, k1) + PAD;
+      const int l2 = c2 - org2 + es_taps<W, T>(r.f[2], poly, k2) + PAD;
+      T vr = 0, vi = 0;
+      for (int m2 = 0; m2 < W; ++m2) {
+        T pr = 0, pi = 0;
+#pragma unroll
+        for (int m1 = 0; m1 < W; ++m1) {
+          const cplx_t<T>* rowp = tile + (int64_t(l2 + m2) * TY + (l1 + m1)) * TX + l0;
+          T rr = 0, ri = 0;
+#pragma unroll
+          for (int m0 = 0; m0 < W; ++m0) {
+            const cplx_t<T> a = rowp[m0];
+            rr += a.x * k0[m0];
+            ri += a.y * k0[m0];
+          }
+          pr += k1[m1] * rr;
+          pi += k1[m1] * ri;
+        }
+        vr += k2[m2] * pr;
+        vi += k2[m2] * pi;
+      }
+      if (NF == 2 && f == 0) {
+        acc_r[k] = vr;
+        acc_i[k] = vi;
+      } else {
+        const T wgt = (mode == INTERP_GRAD) ? (weights ? weights[r.idx] : uniform) : T(1);
+        if (NF == 2) {
+          interp_store<3, T>(mode, r.idx, wgt, acc_r[k], acc_i[k], vr, bad, grad, out2, accumulate, gs);
+        } else {
+          interp_store<3, T>(mode, r.idx, wgt, vr, vi, T(0), bad, grad, out2, accumulate, gs);
+        }
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
@@ -1154,6 +1249,31 @@ void launch_interp2d(const void* recs, const T* weights, T uniform, const SortBu
   FB_LAUNCH_CHECK();
 }
 
+// 3D FP32: the tile kernel when a bin's tile + halo fits in shared memory
+// (false otherwise, and for FP64, whose w^3 loop needs 255 registers and one
+// block per SM in this form: the caller uses the gathering kernel).
+template <int W, typename T>
+bool launch_interp3d(const void* recs, const T* weights, T uniform, const SortBufs& sb, const Geom& g,
+                     const std::vector<double>& poly, const cplx_t<T>* fields, int nfields, int mode, double* grad,
+                     double2* out2, int acc, const int* status, cudaStream_t s, const GradScale& gs) {
+  if constexpr (sizeof(T) != 4) {
+    return false;
+  } else {
+    const size_t smem = size_t(g.tile[0] + W) * (g.tile[1] + W) * (g.tile[2] + W) * sizeof(cplx_t<T>);
+    if (smem > 160 * 1024 || nfields < 1 || nfields > 2) return false;
+    auto kern2 = interp3d_tile_kernel<W, T, 2>;
+    auto kern1 = interp3d_tile_kernel<W, T, 1>;
+    auto kern = nfields == 2 ? kern2 : kern1;
+    if (smem > 48 * 1024)
+      FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<3, T>*>(recs), weights, uniform, sb.sub_bin.p,
+                                                 sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g,
+                                                 make_es_poly<W, T>(poly), fields, mode, grad, out2, acc, status, gs);
+    FB_LAUNCH_CHECK();
+    return true;
+  }
+}
+
 template <int D, int W, typename T>
 void launch_interp_generic(const void* recs, int64_t N, const T* weights, T uniform, const Geom& g,
                            const std::vector<double>& poly, const cplx_t<T>* fields, int nfields, int mode,
@@ -1259,9 +1379,12 @@ void interp(const void* recs, int64_t N, const T* weights, T uniform, const Sort
     FB_FOR_W(T, FB_I2G)
 #undef FB_I2G
   } else {
-#define FB_I3(WW)                                                                                             \
-  launch_interp_generic<3, FB_WCLAMP(T, WW), T>(recs, N, weights, uniform, g, poly, fields, nfields, mode, grad, \
-                                                out2, accumulate, status, s, gs)
+    if (N <= 0) return;
+#define FB_I3(WW)                                                                                              \
+  if (!launch_interp3d<FB_WCLAMP(T, WW), T>(recs, weights, uniform, sb, g, poly, fields, nfields, mode, grad,     \
+                                            out2, accumulate, status, s, gs))                                     \
+    launch_interp_generic<3, FB_WCLAMP(T, WW), T>(recs, N, weights, uniform, g, poly, fields, nfields, mode, grad, \
+                                                  out2, accumulate, status, s, gs)
     FB_FOR_W(T, FB_I3)
 #undef FB_I3
   }
