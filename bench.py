@@ -567,7 +567,12 @@ def run_ours(args):
                      "peak": hbm_peak, "unit": "GB/s", "frac": round(eval_achieved / hbm_peak, 4)}
 
     ensemble = None if args.no_ensemble else ensemble_report(args, dev, ws, rank)
-    sharded = None if args.no_sharded else sharded_report(args, dev, ws, rank)
+    sharded = None
+    if not args.no_sharded:
+        try:  # an error that every rank meets alike (set-up, memory) is reported instead of ending the run
+            sharded = sharded_report(args, dev, ws, rank)
+        except Exception as exc:  # noqa: BLE001
+            sharded = {"error": f"{type(exc).__name__}: {exc}"[:300]}
     others = None if (args.no_other_configs or ws > 1) else other_configs_report(args, dev)
 
     cpu = None
