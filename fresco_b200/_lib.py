@@ -68,6 +68,9 @@ _SIGNATURES = {
     "fresco_fire_create": (C.c_int, [handle_t, c_double_p, c_int64, C.c_double, C.c_double, C.c_double, C.c_int,
                                      C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
                                      C.c_int, C.c_int, C.POINTER(handle_t)]),
+    "fresco_fire_graph_create": (C.c_int, [handle_t, c_double_p, c_int64, C.c_double, C.c_double, C.c_double,
+                                           C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                           C.c_int, C.c_int, C.POINTER(handle_t)]),
     "fresco_optimizer_set_func_gradient": (C.c_int, [handle_t, C.c_double, c_double_p, c_int64]),
     "fresco_optimizer_run": (C.c_int, [handle_t, C.c_int]),
     "fresco_optimizer_one_iteration": (C.c_int, [handle_t]),

@@ -396,9 +396,10 @@ int fresco_lbfgs_create(fresco_potential p, const double* x0, int64_t n, double 
   });
 }
 
-int fresco_fire_create(fresco_potential p, const double* x0, int64_t n, double dtstart, double dtmax,
-                       double maxstep, int Nmin, double finc, double fdec, double fa, double astart, double tol,
-                       int stepback, int nsteps, int iprint, int verbosity, fresco_optimizer* out) {
+namespace {
+int fire_create(bool graph, fresco_potential p, const double* x0, int64_t n, double dtstart, double dtmax,
+                double maxstep, int Nmin, double finc, double fdec, double fa, double astart, double tol,
+                int stepback, int nsteps, int iprint, int verbosity, fresco_optimizer* out) {
   return guarded([&] {
     if (!p || !out || (n > 0 && !x0)) throw fb::InvalidArgument("null argument");
     check_n(p, n);
@@ -418,10 +419,25 @@ int fresco_fire_create(fresco_potential p, const double* x0, int64_t n, double d
     prm.verbosity = verbosity;
     auto* h = new fresco_optimizer_s;
     h->pot = p;
-    h->opt = fb::make_fire(p->pot, x0, n, prm);
+    h->opt = graph ? fb::make_fire_graph(p->pot, x0, n, prm) : fb::make_fire(p->pot, x0, n, prm);
     *out = h;
     return FRESCO_OK;
   });
+}
+}  // namespace
+
+int fresco_fire_graph_create(fresco_potential p, const double* x0, int64_t n, double dtstart, double dtmax,
+                             double maxstep, int Nmin, double finc, double fdec, double fa, double astart, double tol,
+                             int stepback, int nsteps, fresco_optimizer* out) {
+  return fire_create(true, p, x0, n, dtstart, dtmax, maxstep, Nmin, finc, fdec, fa, astart, tol, stepback, nsteps, -1,
+                     0, out);
+}
+
+int fresco_fire_create(fresco_potential p, const double* x0, int64_t n, double dtstart, double dtmax,
+                       double maxstep, int Nmin, double finc, double fdec, double fa, double astart, double tol,
+                       int stepback, int nsteps, int iprint, int verbosity, fresco_optimizer* out) {
+  return fire_create(false, p, x0, n, dtstart, dtmax, maxstep, Nmin, finc, fdec, fa, astart, tol, stepback, nsteps,
+                     iprint, verbosity, out);
 }
 
 int fresco_optimizer_set_func_gradient(fresco_optimizer o, double f, const double* grad, int64_t n) {

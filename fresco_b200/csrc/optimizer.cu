@@ -263,6 +263,10 @@ struct FiState {
   double f, dt, a, ifnorm, vnorm, rms, P, sqrtN;
   double dtmax, maxstep, finc, fdec, fa, astart;
   int fire_iter, Nmin, stepback, restore;
+  // graph-captured loop only (FireGraph): the loop state on the device; cur is
+  // the buffer parity holding the current point, guard bounds the loop
+  double tol;
+  int active, iter, stop_iter, nfev, cur, guard, guard_limit;
 };
 
 enum FiSlot { F_DD = 0, F_PV = 1, F_GG = 2, F_VV = 3, F_NSLOT = 4 };
@@ -300,8 +304,11 @@ __global__ void fi_init_fin(FiState* st, const double* __restrict__ e, double* p
 }
 
 // Inertial mixing and the forward-Euler velocity update (modified_fire.hpp:172-174, 141-144).
+// GRAPH: part of a captured iteration, a no-op once the loop has stopped.
+template <bool GRAPH>
 __global__ void fi_mix(double* __restrict__ v, const double* __restrict__ g, int64_t n, FiState* st, double* part,
                        int P) {
+  if (GRAPH && !st->active) return;  // uniform over the grid
   const double a = st->a, ifn = st->ifnorm, vn = st->vnorm, dt = st->dt;
   double acc[1] = {0.0};
   GRID_LOOP(i, n) {
@@ -329,7 +336,10 @@ __global__ void fi_step(const double* __restrict__ x, double* __restrict__ xnew,
   }
 }
 
-__global__ void fi_post(const double* __restrict__ v, const double* __restrict__ g, int64_t n, double* part, int P) {
+template <bool GRAPH>
+__global__ void fi_post(const double* __restrict__ v, const double* __restrict__ g, int64_t n, double* part, int P,
+                        const FiState* st) {
+  if (GRAPH && !st->active) return;
   double acc[3] = {0.0, 0.0, 0.0};
   GRID_LOOP(i, n) {
     acc[0] += v[i] * g[i];
@@ -341,7 +351,14 @@ __global__ void fi_post(const double* __restrict__ v, const double* __restrict__
 }
 
 // modified_fire.hpp:180-216.  out: [f, rms, dt, a, P, vnorm, fire_iter]
+// GRAPH: also the loop bookkeeping of GradientOptimizer::run (optimizer.hpp:
+// 97-112): evaluation and iteration counts, and whether to continue.
+template <bool GRAPH>
 __global__ void fi_fin(FiState* st, const double* __restrict__ e, double* part, int P, double* out) {
+  if (GRAPH && !st->active) {
+    if (threadIdx.x == 0) st->restore = 0;
+    return;
+  }
   const double pv = sum_parts(part + int64_t(F_PV) * P, P);
   const double gg = sum_parts(part + int64_t(F_GG) * P, P);
   const double vv = sum_parts(part + int64_t(F_VV) * P, P);
@@ -366,6 +383,12 @@ __global__ void fi_fin(FiState* st, const double* __restrict__ e, double* part, 
     st->restore = 1;
     if (!st->stepback) st->f = *e;
   }
+  if (GRAPH) {
+    st->nfev += 1;
+    st->iter += 1;
+    st->active = !(st->rms <= st->tol) && (st->iter < st->stop_iter);
+    if (Pw > 0 || !st->stepback) st->cur = 1 - st->cur;  // the trial point becomes current
+  }
   out[0] = st->f;
   out[1] = st->rms;
   out[2] = st->dt;
@@ -373,6 +396,29 @@ __global__ void fi_fin(FiState* st, const double* __restrict__ e, double* part, 
   out[4] = Pw;
   out[5] = st->vnorm;
   out[6] = double(st->fire_iter);
+}
+
+// run(niter) of the captured loop: niter more iterations while rms > tol (or
+// exactly one with force, as one_iteration); the loop ends after niter + 2
+// passes of its body whatever the state says.
+__global__ void fi_set_stop(FiState* st, int niter, int iter, int nfev, int force) {
+  st->iter = iter;
+  st->nfev = nfev;
+  st->stop_iter = iter + niter;
+  st->active = (force || !(st->rms <= st->tol)) && (iter < st->stop_iter);
+  st->guard = 0;
+  st->guard_limit = niter + 2;
+}
+
+// End of a loop body pass: the next pass's switch value (the iteration from
+// buffer parity cur, or none, 2, once stopped) and whether to continue, at
+// most guard_limit passes.  The first pass of a launch runs no iteration (the
+// switch starts at its default, 2) and only sets the value.
+__global__ void fi_loop(FiState* st, cudaGraphConditionalHandle h_while, cudaGraphConditionalHandle h_switch) {
+  st->guard += 1;
+  const bool go = st->active && st->guard < st->guard_limit;
+  cudaGraphSetConditional(h_switch, go ? unsigned(st->cur & 1) : 2u);
+  cudaGraphSetConditional(h_while, go ? 1u : 0u);
 }
 
 // P <= 0: v = 0 (modified_fire.hpp:204-212); the step back to x_old, g_old
@@ -612,12 +658,12 @@ class Fire final : public Optimizer {
     ++nfev_;
     ++iter_;
     const int nxt = 1 - cur_;
-    fi_mix<<<P_, kThreads, 0, s_>>>(V_.p, G_[cur_].p, n_, st_.p, part_.p, P_);
+    fi_mix<false><<<P_, kThreads, 0, s_>>>(V_.p, G_[cur_].p, n_, st_.p, part_.p, P_);
     fi_step<<<P_, kThreads, 0, s_>>>(X_[cur_].p, X_[nxt].p, V_.p, n_, st_.p, part_.p, P_);
     FB_LAUNCH_CHECK();
     eval(X_[nxt].p, G_[nxt].p, e_.p);
-    fi_post<<<P_, kThreads, 0, s_>>>(V_.p, G_[nxt].p, n_, part_.p, P_);
-    fi_fin<<<1, 256, 0, s_>>>(st_.p, e_.p, part_.p, P_, host_);
+    fi_post<false><<<P_, kThreads, 0, s_>>>(V_.p, G_[nxt].p, n_, part_.p, P_, st_.p);
+    fi_fin<false><<<1, 256, 0, s_>>>(st_.p, e_.p, part_.p, P_, host_);
     fi_restore<<<P_, kThreads, 0, s_>>>(V_.p, n_, st_.p);
     FB_LAUNCH_CHECK();
     FB_CUDA(cudaStreamSynchronize(s_));
@@ -655,6 +701,208 @@ class Fire final : public Optimizer {
   int cur_ = 0;
   DevBuf<double> V_, e_;
   DevBuf<FiState> st_;
+};
+
+// Modified FIRE with the whole run(niter) loop on the device, one CUDA graph
+// launch: a conditional WHILE node repeats a body whose SWITCH node, keyed by
+// the device state, runs the iteration from coordinate buffer 0 or 1 (mixing,
+// step into the other buffer, the potential's own kernels, the power test and
+// the step back, which keeps the parity); a one-thread kernel after it picks
+// the next pass's branch.  The loop control of
+// GradientOptimizer::run (optimizer.hpp:97-112) is a device state word, so the
+// loop stops on the iteration the host loop would, with no evaluation after it.
+// Same iterations, evaluations and trajectory as Fire.
+class FireGraph final : public Optimizer {
+ public:
+  FireGraph(PotentialPtr pot, const double* x0, int64_t n, const FireParams& p)
+      : Optimizer(pot, n, p.tol, p.maxiter, p.iprint, p.verbosity), prm_(p) {
+    const int64_t nn = std::max<int64_t>(n, 1);
+    for (int b = 0; b < 2; ++b) {
+      X_[b].alloc(nn);
+      G_[b].alloc(nn);
+      FB_CUDA(cudaMemsetAsync(G_[b].p, 0, G_[b].bytes(), s_));
+    }
+    V_.alloc(nn);
+    e_.alloc(1);
+    st_.alloc(1);
+    part_.alloc(int64_t(F_NSLOT) * P_);
+    FB_CUDA(cudaMemsetAsync(V_.p, 0, V_.bytes(), s_));
+    FB_CUDA(cudaMemsetAsync(part_.p, 0, part_.bytes(), s_));
+    FiState h{};
+    h.f = 0.0;
+    h.dt = p.dtstart;
+    h.a = p.astart;
+    h.rms = 1e10;
+    h.sqrtN = std::sqrt(double(n));
+    h.dtmax = p.dtmax;
+    h.maxstep = p.maxstep;
+    h.finc = p.finc;
+    h.fdec = p.fdec;
+    h.fa = p.fa;
+    h.astart = p.astart;
+    h.Nmin = p.Nmin;
+    h.stepback = p.stepback ? 1 : 0;
+    h.tol = p.tol;
+    FB_CUDA(cudaMemcpyAsync(st_.p, &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+    if (n > 0) FB_CUDA(cudaMemcpyAsync(X_[0].p, x0, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
+  }
+  ~FireGraph() override {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    if (cap_) cudaStreamDestroy(cap_);
+  }
+
+  double* device_x() override { return X_[cur_].p; }
+  double* device_g() override { return G_[cur_].p; }
+
+  void set_func_gradient(double f, const double* grad, int64_t n) override {
+    if (n != n_) throw InvalidArgument("the gradient has the wrong size");
+    FB_CUDA(cudaMemcpyAsync(G_[cur_].p, grad, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
+    FB_CUDA(cudaMemcpyAsync(e_.p, &f, sizeof(double), cudaMemcpyHostToDevice, s_));
+    init_from_gradient();
+  }
+
+  void reset(const double* x0, int64_t n) override {
+    if (n != n_) throw InvalidArgument("The number of degrees of freedom (x0.size()) cannot change when calling reset()");
+    if (!func_initialized_) initialize_func_gradient();
+    iter_ = 0;
+    FB_CUDA(cudaMemcpyAsync(X_[cur_].p, x0, sizeof(double) * n, cudaMemcpyHostToDevice, s_));
+    eval(X_[cur_].p, G_[cur_].p, e_.p);
+    nfev_ = 1;
+    FiState h{};
+    FB_CUDA(cudaMemcpyAsync(&h, st_.p, sizeof(h), cudaMemcpyDeviceToHost, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
+    h.fire_iter = 0;
+    h.dt = prm_.dtstart;
+    h.a = prm_.astart;
+    FB_CUDA(cudaMemcpyAsync(st_.p, &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+    init_from_gradient();
+  }
+
+  // As Fire::one_iteration (modified_fire.hpp:160-178): no initialisation, and
+  // one step even below the tolerance.
+  void one_iteration() override { launch(1, true); }
+
+  void run(int niter) override {
+    if (!func_initialized_) initialize_func_gradient();
+    if (niter <= 0) return;
+    launch(niter, false);
+  }
+
+ private:
+  void launch(int niter, bool force) {
+    ensure_graph();
+    fi_set_stop<<<1, 1, 0, s_>>>(st_.p, niter, iter_, nfev_, force ? 1 : 0);
+    FB_LAUNCH_CHECK();
+    FB_CUDA(cudaGraphLaunch(graph_, s_));
+    FiState h{};
+    FB_CUDA(cudaMemcpyAsync(&h, st_.p, sizeof(h), cudaMemcpyDeviceToHost, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
+    f_ = h.f;
+    rms_ = h.rms;
+    iter_ = h.iter;
+    nfev_ = h.nfev;
+    cur_ = h.cur & 1;
+  }
+
+  // One iteration from buffer parity c into body (the trial point goes to 1 - c).
+  void capture_body(cudaGraph_t body, int c) {
+    const int t = 1 - c;
+    FB_CUDA(cudaStreamBeginCaptureToGraph(cap_, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    cudaGraph_t g = nullptr;
+    try {
+      fi_mix<true><<<P_, kThreads, 0, cap_>>>(V_.p, G_[c].p, n_, st_.p, part_.p, P_);
+      fi_step<<<P_, kThreads, 0, cap_>>>(X_[c].p, X_[t].p, V_.p, n_, st_.p, part_.p, P_);
+      pot_->energy_gradient(X_[t].p, n_, G_[t].p, e_.p, false, cap_);  // the potential's own launches
+      fi_post<true><<<P_, kThreads, 0, cap_>>>(V_.p, G_[t].p, n_, part_.p, P_, st_.p);
+      fi_fin<true><<<1, 256, 0, cap_>>>(st_.p, e_.p, part_.p, P_, host_dev_.p);
+      fi_restore<<<P_, kThreads, 0, cap_>>>(V_.p, n_, st_.p);
+    } catch (...) {
+      cudaStreamEndCapture(cap_, &g);
+      throw;
+    }
+    FB_CUDA(cudaStreamEndCapture(cap_, &g));
+  }
+
+  // (re)builds the loop graph when the potential's gradient convention changed
+  void ensure_graph() {
+    if (graph_ && graph_mode_ == pot_->gradient_mode()) return;
+    if (graph_) {
+      cudaGraphExecDestroy(graph_);
+      graph_ = nullptr;
+    }
+    // one evaluation outside the capture, so that the potential's lazy set-up
+    // (plans, workspaces) is done; into the trial buffers, which the next
+    // iteration writes before it reads them
+    pot_->energy_gradient(X_[cur_].p, n_, G_[1 - cur_].p, e_.p, false, s_);
+    FB_CUDA(cudaStreamSynchronize(s_));
+    if (!cap_) FB_CUDA(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking));
+    cudaGraph_t top = nullptr;
+    FB_CUDA(cudaGraphCreate(&top, 0));
+    try {
+      cudaGraphConditionalHandle hw, hs;
+      FB_CUDA(cudaGraphConditionalHandleCreate(&hw, top, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams wp{};
+      wp.type = cudaGraphNodeTypeConditional;
+      wp.conditional.handle = hw;
+      wp.conditional.type = cudaGraphCondTypeWhile;
+      wp.conditional.size = 1;
+      cudaGraphNode_t wn;
+      FB_CUDA(cudaGraphAddNode(&wn, top, nullptr, 0, &wp));
+      cudaGraph_t loop = wp.conditional.phGraph_out[0];
+      FB_CUDA(cudaGraphConditionalHandleCreate(&hs, loop, 2, cudaGraphCondAssignDefault));
+      FiState* stp = st_.p;
+      cudaGraphNodeParams sp{};
+      sp.type = cudaGraphNodeTypeConditional;
+      sp.conditional.handle = hs;
+      sp.conditional.type = cudaGraphCondTypeSwitch;
+      sp.conditional.size = 2;
+      cudaGraphNode_t sw, kloop;
+      FB_CUDA(cudaGraphAddNode(&sw, loop, nullptr, 0, &sp));
+      capture_body(sp.conditional.phGraph_out[0], 0);
+      capture_body(sp.conditional.phGraph_out[1], 1);
+      void* loop_args[] = {&stp, &hw, &hs};
+      cudaKernelNodeParams kp{};
+      kp.func = reinterpret_cast<void*>(fi_loop);
+      kp.gridDim = dim3(1);
+      kp.blockDim = dim3(1);
+      kp.sharedMemBytes = 0;
+      kp.kernelParams = loop_args;
+      FB_CUDA(cudaGraphAddKernelNode(&kloop, loop, &sw, 1, &kp));
+      FB_CUDA(cudaGraphInstantiate(&graph_, top, 0));
+    } catch (...) {
+      cudaGraphDestroy(top);
+      throw;
+    }
+    cudaGraphDestroy(top);
+    graph_mode_ = pot_->gradient_mode();
+  }
+
+  void init_from_gradient() {
+    fi_init_v<<<P_, kThreads, 0, s_>>>(G_[cur_].p, V_.p, n_, st_.p, part_.p, P_);
+    fi_init_fin<<<1, 256, 0, s_>>>(st_.p, e_.p, part_.p, P_, host_);
+    FB_LAUNCH_CHECK();
+    FB_CUDA(cudaStreamSynchronize(s_));
+    f_ = host_[0];
+    rms_ = host_[1];
+    func_initialized_ = true;
+  }
+
+  void initialize_func_gradient() override {
+    ++nfev_;
+    eval(X_[cur_].p, G_[cur_].p, e_.p);
+    init_from_gradient();
+  }
+
+  FireParams prm_;
+  DevBuf<double> X_[2], G_[2];  // current point and its gradient in [cur_], the trial in the other
+  int cur_ = 0;
+  DevBuf<double> V_, e_;
+  DevBuf<double> host_dev_{16};  // scalar mirror written by fi_fin inside the graph (not read)
+  DevBuf<FiState> st_;
+  cudaStream_t cap_ = nullptr;
+  cudaGraphExec_t graph_ = nullptr;
+  int graph_mode_ = -1;
 };
 
 }  // namespace
@@ -713,6 +961,10 @@ std::unique_ptr<Optimizer> make_lbfgs(PotentialPtr pot, const double* x0, int64_
 
 std::unique_ptr<Optimizer> make_fire(PotentialPtr pot, const double* x0, int64_t n, const FireParams& p) {
   return std::unique_ptr<Optimizer>(new Fire(std::move(pot), x0, n, p));
+}
+
+std::unique_ptr<Optimizer> make_fire_graph(PotentialPtr pot, const double* x0, int64_t n, const FireParams& p) {
+  return std::unique_ptr<Optimizer>(new FireGraph(std::move(pot), x0, n, p));
 }
 
 }  // namespace fb

@@ -42,7 +42,7 @@ class Optimizer {
  public:
   virtual ~Optimizer();
   virtual void one_iteration() = 0;
-  void run(int niter);  // optimizer.hpp:97-112
+  virtual void run(int niter);  // optimizer.hpp:97-112
   void run();           // optimizer.hpp:118-121
   bool stop_criterion_satisfied();
   virtual void set_func_gradient(double f, const double* grad, int64_t n) = 0;
@@ -72,5 +72,7 @@ class Optimizer {
 
 std::unique_ptr<Optimizer> make_lbfgs(PotentialPtr pot, const double* x0, int64_t n, const LbfgsParams& p);
 std::unique_ptr<Optimizer> make_fire(PotentialPtr pot, const double* x0, int64_t n, const FireParams& p);
+// Modified FIRE with each iteration one CUDA graph launch (same iterations and trajectory).
+std::unique_ptr<Optimizer> make_fire_graph(PotentialPtr pot, const double* x0, int64_t n, const FireParams& p);
 
 }  // namespace fb

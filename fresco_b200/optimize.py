@@ -23,7 +23,7 @@ from . import _lib
 from ._lib import check, dptr, lib
 from .potentials import BasePotential
 
-__all__ = ["Result", "GradientOptimizer", "LBFGS_CPP", "ModifiedFireCPP", "LBFGS_Graph"]
+__all__ = ["Result", "GradientOptimizer", "LBFGS_CPP", "ModifiedFireCPP", "ModifiedFire_Graph", "LBFGS_Graph"]
 
 
 class Result(dict):
@@ -204,6 +204,27 @@ class ModifiedFireCPP(GradientOptimizer):
                                      float(maxstep), int(Nmin), float(finc), float(fdec), float(fa), float(astart),
                                      float(tol), int(bool(stepback)), int(nsteps), int(iprint), int(verbosity),
                                      C.byref(h)))
+        self._h = h
+        if energy is not None and gradient is not None:
+            g = np.ascontiguousarray(np.asarray(gradient, dtype=np.float64).ravel())
+            check(lib.fresco_optimizer_set_func_gradient(self._h, float(energy), dptr(g), g.size))
+        self.events = [] if events is None else events
+
+
+class ModifiedFire_Graph(GradientOptimizer):
+    """ModifiedFireCPP with each iteration one CUDA graph launch: same arguments (iprint and verbosity
+    are accepted and ignored), same trajectory, iterations and evaluations."""
+
+    def __init__(self, x0, potential, dtstart=0.1, dtmax=1, maxstep=0.5, Nmin=5, finc=1.1, fdec=0.5, fa=0.99,
+                 astart=0.1, tol=1e-3, stepback=True, iprint=-1, energy=None, gradient=None, nsteps=10000,
+                 verbosity=0, events=None):
+        self.pot = _as_potential(potential)
+        x = np.ascontiguousarray(np.asarray(x0, dtype=np.float64).ravel())
+        self._n = x.size
+        h = _lib.handle_t()
+        check(lib.fresco_fire_graph_create(self.pot.handle, dptr(x), x.size, float(dtstart), float(dtmax),
+                                           float(maxstep), int(Nmin), float(finc), float(fdec), float(fa),
+                                           float(astart), float(tol), int(bool(stepback)), int(nsteps), C.byref(h)))
         self._h = h
         if energy is not None and gradient is not None:
             g = np.ascontiguousarray(np.asarray(gradient, dtype=np.float64).ravel())

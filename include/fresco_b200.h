@@ -224,6 +224,15 @@ int fresco_lbfgs_create(fresco_potential p, const double* x0, int64_t n, double 
 int fresco_fire_create(fresco_potential p, const double* x0, int64_t n, double dtstart, double dtmax,
                        double maxstep, int Nmin, double finc, double fdec, double fa, double astart, double tol,
                        int stepback, int nsteps, int iprint, int verbosity, fresco_optimizer* out);
+/* The same modified FIRE (modified_fire.hpp:44-230) with each iteration one
+ * CUDA graph launch: the step, the potential call and the accept/step-back
+ * decision all run on the device, and run(niter) reads the iteration count
+ * back once per batch of launches.  Same trajectory, iterations and nfev as
+ * fresco_fire_create; no progress printing (iprint, verbosity).  Driven by
+ * the fresco_optimizer_* calls below. */
+int fresco_fire_graph_create(fresco_potential p, const double* x0, int64_t n, double dtstart, double dtmax,
+                             double maxstep, int Nmin, double finc, double fdec, double fa, double astart, double tol,
+                             int stepback, int nsteps, fresco_optimizer* out);
 
 /* GradientOptimizer::set_func_gradient(f, grad)  (source/fresco/optimizer.hpp:127-144). */
 int fresco_optimizer_set_func_gradient(fresco_optimizer o, double f, const double* grad, int64_t n);

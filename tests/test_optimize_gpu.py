@@ -203,3 +203,45 @@ def test_graph_lbfgs_matches_lbfgs_cpp_fp32():
         assert rel(rb.coords, ra.coords) < 2e-4
     else:
         assert ra.energy < 1e-2 * e0 and rb.energy < 1e-2 * e0
+
+
+def test_graph_fire_matches_fire_cpp():
+    """ModifiedFire_Graph (one CUDA graph launch per iteration, loop state on the device) against
+    ModifiedFireCPP in FP64: same trajectory, iterations and evaluations, through one_iteration,
+    run(niter) in chunks, the stop at tol, reset and both step-back settings."""
+    from fresco_b200 import NUwU
+    from fresco_b200.optimize import ModifiedFire_Graph, ModifiedFireCPP
+
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(300, 6, 4, ndim=2, seed=10)
+    for stepback in (True, False):
+        kw = dict(dtstart=0.01, dtmax=0.1, maxstep=0.05, tol=1e-12, stepback=stepback)
+        a = ModifiedFireCPP(x, NUwU(radii, 6, Sk, V, L, eps=1e-13), **kw)
+        b = ModifiedFire_Graph(x, NUwU(radii, 6, Sk, V, L, eps=1e-13), **kw)
+        ra, rb = a.one_iteration(), b.one_iteration()  # before run: steps from f = 0, g = 0
+        assert rb.nfev == ra.nfev == 1
+        if stepback:  # P = 0, a step back: f stays 0
+            assert rb.energy == ra.energy == 0.0
+        else:  # f = E(x) from two potential objects, equal up to the order of FP64 sums
+            assert rel(rb.energy, ra.energy) < 1e-12
+        for niter in (1, 3, 7, 40):
+            ra, rb = a.run(niter), b.run(niter)
+            assert rb.nsteps == ra.nsteps and rb.nfev == ra.nfev, (niter, ra.nsteps, rb.nsteps)
+            assert rel(rb.energy, ra.energy) < 1e-8
+            assert rel(rb.coords, ra.coords) < 1e-8
+            assert rel(rb.grad, ra.grad) < 1e-8
+        a.reset(x)
+        b.reset(x)
+        assert b.get_niter() == 0 and b.get_result().nfev == a.get_result().nfev == 1
+        ra, rb = a.run(12), b.run(12)
+        assert rb.nsteps == ra.nsteps == 12 and rb.nfev == ra.nfev
+        assert rel(rb.coords, ra.coords) < 1e-8
+
+    # the stop at tol: both stop on the same iteration
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(200, 5, 3, ndim=2, seed=9, L=np.ones(2))
+    a = ModifiedFireCPP(x, NUwU(radii, 5, Sk, V, L, eps=1e-13), tol=1e-3, nsteps=3000)
+    b = ModifiedFire_Graph(x, NUwU(radii, 5, Sk, V, L, eps=1e-13), tol=1e-3, nsteps=3000)
+    ra, rb = a.run(), b.run()
+    assert ra.success and rb.success and rb.rms <= 1e-3
+    assert rb.nsteps == ra.nsteps and rb.nfev == ra.nfev
+    assert rel(rb.coords, ra.coords) < 1e-8
+    assert b.run(10).nsteps == rb.nsteps  # converged: no iteration
