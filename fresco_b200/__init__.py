@@ -15,23 +15,26 @@ import sys
 import types
 
 from . import _lib  # noqa: F401  (loads the CUDA library; raises ImportError if missing)
-from . import ensemble, optimize, potentials, shard, utils
+from . import distances, ensemble, optimize, potentials, shard, utils
 from .ensemble import EnsembleLBFGS, NUwUEnsemble
 from .potentials import CombinedPotential, InversePower, NUwNU, NUwU, UwNU, UwU
 from .shard import ShardedNUwU
 
-__all__ = ["potentials", "optimize", "utils", "ensemble", "shard", "install_alias", "NUwU", "UwU", "UwNU", "NUwNU",
+__all__ = ["potentials", "optimize", "utils", "distances", "ensemble", "shard", "install_alias", "NUwU", "UwU", "UwNU", "NUwNU",
            "InversePower", "CombinedPotential", "NUwUEnsemble", "EnsembleLBFGS", "ShardedNUwU"]
 
 
 def install_alias() -> None:
-    """Makes ``import fresco.potentials`` / ``fresco.optimize`` / ``fresco.utils`` resolve to this package."""
+    """Makes ``import fresco.potentials`` / ``fresco.optimize`` / ``fresco.utils`` / ``fresco.distances`` resolve
+    to this package."""
     pkg = types.ModuleType("fresco")
     pkg.__path__ = []  # namespace-like
     pkg.potentials = potentials
     pkg.optimize = optimize
     pkg.utils = utils
+    pkg.distances = distances
     sys.modules.setdefault("fresco", pkg)
     sys.modules.setdefault("fresco.potentials", potentials)
     sys.modules.setdefault("fresco.optimize", optimize)
     sys.modules.setdefault("fresco.utils", utils)
+    sys.modules.setdefault("fresco.distances", distances)

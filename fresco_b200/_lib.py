@@ -68,6 +68,17 @@ _SIGNATURES = {
     "fresco_fire_create": (C.c_int, [handle_t, c_double_p, c_int64, C.c_double, C.c_double, C.c_double, C.c_int,
                                      C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
                                      C.c_int, C.c_int, C.POINTER(handle_t)]),
+    "fresco_overlap_create": (C.c_int, [c_double_p, c_int64, c_double_p, C.c_int, C.c_int, C.POINTER(handle_t)]),
+    "fresco_overlap_find": (C.c_int, [handle_t, c_double_p, c_int64, C.POINTER(C.c_int64), c_int64,
+                                      C.POINTER(C.c_uint64), C.POINTER(C.c_int64)]),
+    "fresco_overlap_destroy": (None, [handle_t]),
+    "fresco_window_stats_create": (C.c_int, [c_double_p, c_int64, C.c_int, c_double_p, c_double_p, C.c_int,
+                                             C.c_uint64, C.POINTER(handle_t)]),
+    "fresco_window_stats_run": (C.c_int, [handle_t, c_int64]),
+    "fresco_window_stats_set_seed": (C.c_int, [handle_t, C.c_uint64]),
+    "fresco_window_stats_get": (C.c_int, [handle_t, C.POINTER(C.c_uint64), c_double_p, c_double_p,
+                                          C.POINTER(C.c_uint64)]),
+    "fresco_window_stats_destroy": (None, [handle_t]),
     "fresco_fire_graph_create": (C.c_int, [handle_t, c_double_p, c_int64, C.c_double, C.c_double, C.c_double,
                                            C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                            C.c_int, C.c_int, C.POINTER(handle_t)]),

@@ -7,6 +7,7 @@
 #include "../../include/fresco_b200.h"
 #include "ensemble.cuh"
 #include "optimizer.cuh"
+#include "pointstats.cuh"
 #include "potential.cuh"
 
 struct fresco_potential_s {
@@ -29,6 +30,14 @@ struct fresco_ensemble_s {
 
 struct fresco_ensemble_lbfgs_s {
   std::unique_ptr<fb::EnsembleLbfgs> opt;
+};
+
+struct fresco_overlap_s {
+  std::unique_ptr<fb::OverlapCheck> chk;
+};
+
+struct fresco_window_stats_s {
+  std::unique_ptr<fb::WindowCounts> wc;
 };
 
 namespace {
@@ -696,5 +705,82 @@ int fresco_ensemble_lbfgs_state(fresco_ensemble_lbfgs o, double* x, double* g, d
 }
 
 void fresco_ensemble_lbfgs_destroy(fresco_ensemble_lbfgs o) { delete o; }
+
+int fresco_overlap_create(const double* radii, int64_t n, const double* boxv, int ndim, int periodic,
+                          fresco_overlap* out) {
+  return guarded([&] {
+    if (!out || !boxv || (n > 0 && !radii)) throw fb::InvalidArgument("null argument");
+    if (ndim < 1 || ndim > 3) throw fb::InvalidArgument("CheckOverlap: ndim must be 1, 2 or 3");
+    auto* h = new fresco_overlap_s;
+    try {
+      h->chk = fb::make_overlap_check(std::vector<double>(radii, radii + std::max<int64_t>(n, 0)),
+                                      std::vector<double>(boxv, boxv + ndim), periodic != 0);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    return FRESCO_OK;
+  });
+}
+
+int fresco_overlap_find(fresco_overlap h, const double* x, int64_t ndof, const int64_t* changed, int64_t n_changed,
+                        uint64_t* out, int64_t* count) {
+  return guarded([&] {
+    if (!h || !out || !count || (ndof > 0 && !x) || (n_changed > 0 && !changed))
+      throw fb::InvalidArgument("null argument");
+    *count = h->chk->find(x, ndof, changed, n_changed, out);
+    return FRESCO_OK;
+  });
+}
+
+void fresco_overlap_destroy(fresco_overlap h) { delete h; }
+
+int fresco_window_stats_create(const double* x, int64_t n_points, int ndim, const double* boxv, const double* radii,
+                               int n_radii, uint64_t seed, fresco_window_stats* out) {
+  return guarded([&] {
+    if (!out || !boxv || !radii || (n_points > 0 && !x)) throw fb::InvalidArgument("null argument");
+    if (ndim < 1 || ndim > 3) throw fb::InvalidArgument("point pattern statistics: ndim must be 1, 2 or 3");
+    if (n_radii < 1) throw fb::InvalidArgument("at least one window radius is needed");
+    auto* h = new fresco_window_stats_s;
+    try {
+      h->wc = fb::make_window_counts(x, n_points, std::vector<double>(boxv, boxv + ndim),
+                                     std::vector<double>(radii, radii + n_radii), seed);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    return FRESCO_OK;
+  });
+}
+
+int fresco_window_stats_run(fresco_window_stats h, int64_t n) {
+  return guarded([&] {
+    if (!h) throw fb::InvalidArgument("null handle");
+    if (n < 0) throw fb::InvalidArgument("the number of windows must be non-negative");
+    h->wc->run(n);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_window_stats_set_seed(fresco_window_stats h, uint64_t seed) {
+  return guarded([&] {
+    if (!h) throw fb::InvalidArgument("null handle");
+    h->wc->set_seed(seed);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_window_stats_get(fresco_window_stats h, uint64_t* seed, double* mean, double* var, uint64_t* count) {
+  return guarded([&] {
+    if (!h) throw fb::InvalidArgument("null handle");
+    if (seed) *seed = h->wc->seed();
+    h->wc->moments(mean, var, count);
+    return FRESCO_OK;
+  });
+}
+
+void fresco_window_stats_destroy(fresco_window_stats h) { delete h; }
 
 }  // extern "C"

@@ -34,6 +34,8 @@ typedef struct fresco_potential_s* fresco_potential;
 typedef struct fresco_optimizer_s* fresco_optimizer;
 typedef struct fresco_ensemble_s* fresco_ensemble;
 typedef struct fresco_ensemble_lbfgs_s* fresco_ensemble_lbfgs;
+typedef struct fresco_overlap_s* fresco_overlap;
+typedef struct fresco_window_stats_s* fresco_window_stats;
 
 enum {
   FRESCO_OK = 0,
@@ -305,6 +307,43 @@ int fresco_ensemble_lbfgs_steps(fresco_ensemble_lbfgs o, int n_steps);
 int fresco_ensemble_lbfgs_state(fresco_ensemble_lbfgs o, double* x, double* g, double* f, double* rms, int* niter,
                                 int* nfev, int* active);
 void fresco_ensemble_lbfgs_destroy(fresco_ensemble_lbfgs o);
+
+/* CheckOverlap(radii, boxv, use_cell_lists, ncellx_scale, method)
+ * (fresco/distances/_check_overlap.pyx:29-110; check_overlap.hpp:24-130,
+ * check_overlap_cell_lists.hpp:87-180): the hard-core overlap test on the
+ * device, with cell lists whatever use_cell_lists says (the result does not
+ * depend on it).  periodic: 1 for Distance.PERIODIC (minimum image in the box
+ * boxv), 0 for Distance.CARTESIAN (boxv only gives ndim = 1, 2 or 3).  An
+ * empty radius array raises, as the reference does. */
+int fresco_overlap_create(const double* radii, int64_t n, const double* boxv, int ndim, int periodic,
+                          fresco_overlap* out);
+/* get_overlapping_particles(coords) (check_overlap.hpp:111-115) or, with
+ * n_changed > 0, get_overlapping_particles_ca(coords, changed_atoms)
+ * (:105-109): the particles i with |r_ij|^2 < (r_i + r_j)^2 for some j != i
+ * (only pairs holding a changed atom with changed atoms).  x: ndof host
+ * coordinates (ndof = n * ndim, else the reference's "illegal input" error);
+ * out: room for n indices, written in ascending order (the reference's
+ * unordered_set order is unspecified); *count: how many.  Synchronous. */
+int fresco_overlap_find(fresco_overlap h, const double* x, int64_t ndof, const int64_t* changed, int64_t n_changed,
+                        uint64_t* out, int64_t* count);
+void fresco_overlap_destroy(fresco_overlap h);
+
+/* PointPatternStatistics(coords, boxv, radius, rseed) (n_radii = 1;
+ * point_pattern_statistics.hpp:36-111) and BatchPPS(coords, boxv, radii,
+ * rseed) (batch_pointstats.hpp:29-150): number-variance window counts.
+ * x: n_points * ndim host coordinates, copied; radii ascending.  Windows are
+ * centred at the std::mt19937_64(rseed) stream's points, drawn as the
+ * reference draws them. */
+int fresco_window_stats_create(const double* x, int64_t n_points, int ndim, const double* boxv, const double* radii,
+                               int n_radii, uint64_t seed, fresco_window_stats* out);
+/* run(n): n more windows (point_pattern_statistics.hpp:66-70, batch_pointstats.hpp:73-125). */
+int fresco_window_stats_run(fresco_window_stats h, int64_t n);
+/* set_generator_seed(seed) (point_pattern_statistics.hpp:105-108). */
+int fresco_window_stats_set_seed(fresco_window_stats h, uint64_t seed);
+/* get_seed, and per radius get_mean / get_variance / get_count
+ * (point_pattern_statistics.hpp:92-103); any pointer may be NULL. */
+int fresco_window_stats_get(fresco_window_stats h, uint64_t* seed, double* mean, double* var, uint64_t* count);
+void fresco_window_stats_destroy(fresco_window_stats h);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

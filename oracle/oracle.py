@@ -787,3 +787,168 @@ def export_structure(r, L, Nk=1001, radii=None):
     q, S = radial_profile(Sk, center=[center] * ndim)
     rq, g = radial_profile(gr, center=[center] * ndim)
     return q, S, Sk, rq / Nk, g, gr
+
+
+# ---------------------------------------------------------------------------
+# point-pattern statistics and overlap checks
+# ---------------------------------------------------------------------------
+
+class MT19937_64:
+    """The 64-bit Mersenne Twister of the C++ standard ([rand.eng.mers], std::mt19937_64:
+    w=64, n=312, m=156, r=31; Matsumoto & Nishimura), with its integer seeding.  The reference draws
+    its window centres from it (point_pattern_statistics.hpp:45, 72-77)."""
+
+    _N, _M = 312, 156
+    _A = 0xB5026F5AA96619E9
+    _UPPER, _LOWER = 0xFFFFFFFF80000000, 0x7FFFFFFF
+    _MASK = (1 << 64) - 1
+
+    def __init__(self, seed=5489):
+        self.seed(seed)
+
+    def seed(self, s):
+        mt = [int(s) & self._MASK]
+        for i in range(1, self._N):
+            prev = mt[-1]
+            mt.append((6364136223846793005 * (prev ^ (prev >> 62)) + i) & self._MASK)
+        self._mt = mt
+        self._i = self._N
+
+    def _twist(self):
+        mt, n, m = self._mt, self._N, self._M
+        for i in range(n):
+            y = (mt[i] & self._UPPER) | (mt[(i + 1) % n] & self._LOWER)
+            mt[i] = mt[(i + m) % n] ^ (y >> 1) ^ (self._A if y & 1 else 0)
+        self._i = 0
+
+    def __call__(self):
+        if self._i >= self._N:
+            self._twist()
+        y = self._mt[self._i]
+        self._i += 1
+        y ^= (y >> 29) & 0x5555555555555555
+        y ^= (y << 17) & 0x71D67FFFEDA60000
+        y ^= (y << 37) & 0xFFF7EEE000000000
+        y ^= y >> 43
+        return y & self._MASK
+
+
+def uniform_real(gen, a, b):
+    """std::uniform_real_distribution<double>(a, b)(gen) for a 64-bit engine as libstdc++ computes it:
+    generate_canonical<double, 53> takes one draw, u = double(draw) / 2^64 (u = 1 becomes the largest
+    double below 1), then u * (b - a) + a."""
+    u = float(gen()) / 18446744073709551616.0
+    if u >= 1.0:
+        u = np.nextafter(1.0, 0.0)
+    return u * (b - a) + a
+
+
+def window_centres(gen, boxv, n):
+    """n window centres, in the reference's draw order (point_pattern_statistics.hpp:72-77)."""
+    boxv = [float(v) for v in np.asarray(boxv, dtype=np.float64).ravel()]
+    out = np.empty((n, len(boxv)))
+    for k in range(n):
+        for a, L in enumerate(boxv):
+            out[k, a] = uniform_real(gen, 0.0, L) - L / 2
+    return out
+
+
+def periodic_dist2(r1, r2, boxv):
+    """|r1 - r2|^2 with periodic_distance::get_rij (distance.hpp:170-192; ibox = 1 / L, round half to even)
+    and the dot from 0 in axis order (vecN.hpp:283-291), every operation rounded on its own."""
+    boxv = np.asarray(boxv, dtype=np.float64)
+    d = np.asarray(r1, dtype=np.float64) - np.asarray(r2, dtype=np.float64)
+    ibox = 1.0 / boxv
+    d = d - np.rint(d * ibox) * boxv
+    s = np.zeros(d.shape[:-1])
+    for a in range(d.shape[-1]):
+        s = s + d[..., a] * d[..., a]
+    return s
+
+
+class Moments:
+    """moments.hpp:28-52: running means of x and x^2; variance = E[x^2] - E[x]^2."""
+
+    def __init__(self):
+        self.mean = 0.0
+        self.mean2 = 0.0
+        self.count = 0
+
+    def update(self, v):
+        v = float(v)
+        self.mean = (self.mean * float(self.count) + v) / float(self.count + 1)
+        self.mean2 = (self.mean2 * float(self.count) + v * v) / float(self.count + 1)
+        self.count += 1
+
+    def variance(self):
+        return self.mean2 - self.mean * self.mean
+
+
+def window_counts(coords, boxv, radii, centres):
+    """Number of points within each radius of each centre: counts[k, i] = #{j : dist2(c_k, x_j) <= r_i^2}
+    (point_pattern_statistics.hpp:78-90; batch_pointstats.hpp:82-118 cumulated over sorted radii)."""
+    boxv = np.asarray(boxv, dtype=np.float64)
+    x = np.asarray(coords, dtype=np.float64).reshape(-1, boxv.size)
+    r2 = np.asarray(radii, dtype=np.float64) ** 2
+    out = np.empty((len(centres), r2.size), dtype=np.int64)
+    for k, c in enumerate(centres):
+        d2 = periodic_dist2(c[None, :], x, boxv)
+        out[k] = (d2[:, None] <= r2[None, :]).sum(axis=0)
+    return out
+
+
+class BatchPPS:
+    """PointPatternStatistics / BatchPPS restated (point_pattern_statistics.hpp:36-111,
+    batch_pointstats.hpp:29-150) without the reference's data race on the shared counter
+    (point_pattern_statistics.hpp:82-89) and with its uninitialised loop counters read as 0
+    (batch_pointstats.hpp:50, 76, 130, 139, 148)."""
+
+    def __init__(self, coords, boxv, radii, rseed):
+        self.coords = np.asarray(coords, dtype=np.float64)
+        self.boxv = np.asarray(boxv, dtype=np.float64)
+        self.radii = np.atleast_1d(np.asarray(radii, dtype=np.float64))
+        self.gen = MT19937_64(rseed)
+        self.moments = [Moments() for _ in self.radii]
+
+    def run(self, n):
+        centres = window_centres(self.gen, self.boxv, n)
+        counts = window_counts(self.coords, self.boxv, self.radii, centres)
+        for k in range(n):
+            for i, m in enumerate(self.moments):
+                m.update(counts[k, i])
+        return counts
+
+    def mean(self):
+        return np.array([m.mean for m in self.moments])
+
+    def variance(self):
+        return np.array([m.variance() for m in self.moments])
+
+
+def overlapping_particles(coords, radii, boxv, periodic=True, changed=None):
+    """Sorted indices i with |r_ij|^2 < (r_i + r_j)^2 for some j != i (check_overlap.hpp:53-101); with
+    changed atoms only the pairs (i changed, any j != i) count, and both members are reported."""
+    boxv = np.asarray(boxv, dtype=np.float64)
+    D = boxv.size
+    x = np.asarray(coords, dtype=np.float64).reshape(-1, D)
+    r = np.asarray(radii, dtype=np.float64)
+    N = len(r)
+    hit = np.zeros(N, dtype=bool)
+    rows = range(N) if changed is None else [int(i) for i in changed]
+    rows = list(rows)
+    step = max(1, min(256, (1 << 22) // max(N, 1)))  # rows per block: about 4M pairs
+    for s in range(0, len(rows), step):
+        idx = np.asarray(rows[s:s + step], dtype=np.int64)
+        d = x[idx][:, None, :] - x[None, :, :]
+        if periodic:
+            d = d - np.rint(d * (1.0 / boxv)) * boxv
+        d2 = np.zeros(d.shape[:2])
+        for a in range(D):
+            d2 = d2 + d[..., a] * d[..., a]
+        rs = r[idx][:, None] + r[None, :]
+        ov = d2 < rs * rs
+        ov[np.arange(len(idx)), idx] = False
+        hit[idx[ov.any(axis=1)]] = True
+        if changed is not None:
+            hit |= ov.any(axis=0)
+    return np.nonzero(hit)[0].astype(np.uint64)

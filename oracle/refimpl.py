@@ -60,6 +60,14 @@ def lib():
             "ref_opt_one_iteration": (None, [C.c_void_p]),
             "ref_opt_state": (None, [C.c_void_p, _dp, _dp, _dp, _dp, _ip, _ip, _dp]),
             "ref_opt_destroy": (None, [C.c_void_p]),
+            "ref_pps_create": (C.c_void_p, [_dp, C.c_int64, C.c_int, _dp, C.c_double, C.c_uint64]),
+            "ref_pps_run": (None, [C.c_void_p, C.c_int64]),
+            "ref_pps_set_seed": (None, [C.c_void_p, C.c_uint64]),
+            "ref_pps_get": (None, [C.c_void_p, _dp, _dp, C.POINTER(C.c_uint64)]),
+            "ref_pps_destroy": (None, [C.c_void_p]),
+            "ref_last_error": (C.c_char_p, []),
+            "ref_overlap": (C.c_int64, [_dp, C.c_int64, _dp, C.c_int, C.c_int, C.c_int, C.c_double, _dp,
+                                        C.POINTER(C.c_int64), C.c_int64, C.POINTER(C.c_uint64)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -215,3 +223,45 @@ class ModifiedFire(_RefOpt):
 
 def host_cores() -> int:
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+class PointPatternStatistics:
+    """The reference's PointPatternStatistics<ndim> (point_pattern_statistics.hpp:36-111), built serially."""
+
+    def __init__(self, coords, boxv, radius, rseed):
+        x, xp = _d(coords)
+        b, bp = _d(boxv)
+        self._keep = (x, b)
+        self._h = lib().ref_pps_create(xp, x.size // b.size, b.size, bp, float(radius), C.c_uint64(int(rseed)))
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            lib().ref_pps_destroy(h)
+
+    def run(self, n):
+        lib().ref_pps_run(self._h, int(n))
+
+    def set_generator_seed(self, seed):
+        lib().ref_pps_set_seed(self._h, C.c_uint64(int(seed)))
+
+    def mean_var_count(self):
+        m, v, c = C.c_double(), C.c_double(), C.c_uint64()
+        lib().ref_pps_get(self._h, C.byref(m), C.byref(v), C.byref(c))
+        return m.value, v.value, c.value
+
+
+def overlapping_particles(radii, boxv, coords, periodic=True, cell_lists=False, ncellx_scale=1.0, changed=None):
+    """The reference's CheckOverlap{Periodic,Cartesian}[CellLists] (check_overlap.hpp:24-130,
+    check_overlap_cell_lists.hpp:87-180), sorted indices."""
+    r, rp = _d(radii)
+    b, bp = _d(boxv)
+    x, xp = _d(coords)
+    ch = np.ascontiguousarray(np.asarray([] if changed is None else changed, dtype=np.int64).ravel())
+    out = np.zeros(max(r.size, 1), dtype=np.uint64)
+    n = lib().ref_overlap(rp, r.size, bp, b.size, int(periodic), int(cell_lists), float(ncellx_scale), xp,
+                          ch.ctypes.data_as(C.POINTER(C.c_int64)), ch.size,
+                          out.ctypes.data_as(C.POINTER(C.c_uint64)))
+    if n < 0:
+        raise RuntimeError(lib().ref_last_error().decode())
+    return out[:n].copy()
