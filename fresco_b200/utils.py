@@ -1,5 +1,6 @@
-"""Structure measurement after a minimisation: the counterpart of fresco.utils.export_structure
-(fresco/utils/utils.py:16-52) and radial_profile (utils.py:138-152), computed on the device."""
+"""Structure measurement after a minimisation, computed on the device: the counterparts of
+fresco.utils.export_structure (fresco/utils/utils.py:16-52), radial_profile (utils.py:138-152), and the
+number-variance statistics PointPatternStatistics / BatchPPS (fresco/utils/c_utils.pyx:8-150)."""
 from __future__ import annotations
 
 import ctypes as C

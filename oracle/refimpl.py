@@ -236,8 +236,11 @@ class PointPatternStatistics:
 
     def __del__(self):
         h, self._h = getattr(self, "_h", None), None
-        if h:
-            lib().ref_pps_destroy(h)
+        if h and _lib is not None:
+            try:
+                _lib.ref_pps_destroy(h)
+            except Exception:
+                pass
 
     def run(self, n):
         lib().ref_pps_run(self._h, int(n))
