@@ -252,6 +252,27 @@ def other_configs_report(args, dev):
     for prec in ("fp32", "fp64"):
         out["config4_uwu"][prec] = rate(UwU(np.array([g4, g4]), 64, np.zeros_like(v4), v4, np.ones(2),
                                             precision=prec), xg)
+    # config 4's optimiser: modified FIRE with the reference's defaults on the FP32 UwU, host-driven
+    # iterations and the graph form (the whole run(niter) loop as one CUDA graph launch)
+    from fresco_b200._lib import check as _check, lib as _clib
+    from fresco_b200.optimize import ModifiedFire_Graph, ModifiedFireCPP
+
+    fire = {"workload": "modified FIRE (reference defaults, tol=0) on the FP32 UwU above",
+            "timing": "host wall clock around the C-level run loop"}
+    n_fire = max(20, args.steps)
+    for name, cls in (("ModifiedFireCPP", ModifiedFireCPP), ("ModifiedFire_Graph", ModifiedFire_Graph)):
+        opt = cls(xg, UwU(np.array([g4, g4]), 64, np.zeros_like(v4), v4, np.ones(2), precision="fp32"), tol=0.0)
+        opt.run(3)  # initial evaluation, graph capture, warm-up iterations
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _check(_clib.fresco_optimizer_run(opt._h, n_fire))
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        res = opt.get_result()
+        fire[name] = {"iterations_per_s": round(n_fire / dt, 2), "ms_per_iteration": round(1e3 * dt / n_fire, 4),
+                      "evals": int(res.nfev), "energy": float(res.energy)}
+        del opt
+    out["config4_uwu_fire"] = fire
     del xg, m4, v4
     rng = np.random.default_rng(4)
     gu, mk = 2048, 100_000
