@@ -18,10 +18,10 @@ from . import _lib  # noqa: F401  (loads the CUDA library; raises ImportError if
 from . import distances, ensemble, optimize, potentials, shard, utils
 from .ensemble import EnsembleLBFGS, NUwUEnsemble
 from .potentials import CombinedPotential, InversePower, NUwNU, NUwU, UwNU, UwU
-from .shard import ShardedNUwU
+from .shard import ShardedLBFGS, ShardedNUwU
 
 __all__ = ["potentials", "optimize", "utils", "distances", "ensemble", "shard", "install_alias", "NUwU", "UwU", "UwNU", "NUwNU",
-           "InversePower", "CombinedPotential", "NUwUEnsemble", "EnsembleLBFGS", "ShardedNUwU"]
+           "InversePower", "CombinedPotential", "NUwUEnsemble", "EnsembleLBFGS", "ShardedNUwU", "ShardedLBFGS"]
 
 
 def install_alias() -> None:

@@ -59,6 +59,8 @@ _SIGNATURES = {
     "fresco_export_structure": (C.c_int, [c_double_p, c_int64, C.c_int, c_double_p, C.c_int, c_double_p, C.c_double,
                                           c_double_p, c_double_p, c_double_p, c_double_p]),
     "fresco_potential_status": (C.c_int, [handle_t, c_void_p, c_int_p]),
+    "fresco_potential_set_reducer": (C.c_int, [handle_t, c_void_p, c_void_p]),
+    "fresco_optimizer_set_reducer": (C.c_int, [handle_t, c_void_p, c_void_p, c_int64]),
     "fresco_potential_set_gradient_mode": (C.c_int, [handle_t, C.c_int]),
     "fresco_potential_set_timing": (C.c_int, [handle_t, C.c_int]),
     "fresco_potential_get_timing": (C.c_int, [handle_t, C.c_int, C.c_char_p, C.c_int, c_double_p, c_int_p, c_int_p]),

@@ -316,6 +316,22 @@ int fresco_export_structure(const double* x, int64_t n_points, int ndim, const d
   });
 }
 
+int fresco_potential_set_reducer(fresco_potential p, fresco_reduce_fn fn, void* ctx) {
+  return guarded([&] {
+    if (!p || !fn) throw fb::InvalidArgument("null argument");
+    p->pot->set_reducer(fn, ctx);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_optimizer_set_reducer(fresco_optimizer o, fresco_reduce_fn fn, void* ctx, int64_t global_ndof) {
+  return guarded([&] {
+    if (!o || !fn) throw fb::InvalidArgument("null argument");
+    o->opt->set_reducer(fn, ctx, global_ndof);
+    return FRESCO_OK;
+  });
+}
+
 int fresco_potential_status(fresco_potential p, void* stream, int* status) {
   return guarded([&] {
     if (!p || !status) throw fb::InvalidArgument("null argument");

@@ -306,7 +306,22 @@ class NUwUImpl final : public Potential, public NUwUShard {
               acc ? 1 : 0, status_.p, s, gs);
   }
 
+  void set_reducer(ReduceFn fn, void* ctx) override {
+    if (!sharded_) throw InvalidArgument("NUwU: only a shard of a pattern takes a reducer");
+    reducer_ = fn;
+    reducer_ctx_ = ctx;
+    if (!rho_sum_.p) rho_sum_.alloc(2 * std::max<int64_t>(n_active_, 1));
+    set_graphs_enabled(false);  // the reducer is host code between the shard's launches
+  }
+
   void run(const double* x, double* g, double* e, bool acc, cudaStream_t s) {
+    if (sharded_ && reducer_) {  // this shard's rho, the sum over the shards, the shared mode pass
+      if (acc) throw InvalidArgument("a sharded NUwU cannot accumulate into another potential's result");
+      shard_rho(x, rho_sum_.p, s);
+      reducer_(rho_sum_.p, 2 * n_active_, s, reducer_ctx_);
+      shard_finish(rho_sum_.p, g, e, s);
+      return;
+    }
     if (sharded_ && n_total_ != N_)
       throw InvalidArgument("sharded NUwU: evaluate through the shard calls (rho, sum over shards, finish)");
     timer_begin(s);
@@ -478,6 +493,9 @@ class NUwUImpl final : public Potential, public NUwUShard {
 
   int64_t N_;
   bool sharded_ = false;
+  ReduceFn reducer_ = nullptr;
+  void* reducer_ctx_ = nullptr;
+  DevBuf<double> rho_sum_;
   int64_t n_total_ = 0;
   double invN_ = 1.0;
   double Karg_;

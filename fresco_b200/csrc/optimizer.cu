@@ -472,8 +472,23 @@ class Lbfgs final : public Optimizer {
   double* device_g() override { return G_[cur_].p; }
   double h0() const override { return h0_; }
 
+  void set_reducer(ReduceFn fn, void* ctx, int64_t global_ndof) override {
+    if (global_ndof < n_) throw InvalidArgument("the global coordinate count is below this process's");
+    if (iter_ > 0 || func_initialized_) throw InvalidArgument("set the reducer before the first evaluation");
+    reducer_ = fn;
+    reducer_ctx_ = ctx;
+    global_n_ = global_ndof;
+    LbState h{};
+    FB_CUDA(cudaMemcpyAsync(&h, st_.p, sizeof(h), cudaMemcpyDeviceToHost, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
+    h.inv_sqrt_n = 1.0 / std::sqrt(double(global_ndof));
+    FB_CUDA(cudaMemcpyAsync(st_.p, &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
+  }
+
   void set_func_gradient(double f, const double* grad, int64_t n) override {
     if (n != n_) throw InvalidArgument("the gradient has the wrong size");
+    if (reducer_) throw InvalidArgument("set_func_gradient is not supported over a sharded pattern");
     if (iter_ > 0) std::printf("warning: setting f and grad after the first iteration.  this is dangerous.\n");
     double gnorm = 0.0;
     for (int64_t i = 0; i < n; ++i) gnorm += grad[i] * grad[i];
@@ -506,12 +521,15 @@ class Lbfgs final : public Optimizer {
     // compute_lbfgs_step (lbfgs.cpp:107-170)
     if (k_ == 0) {
       dot_kernel<<<P_, kThreads, 0, s_>>>(g, g, n_, part_.p, P_, S_GG);
+      reduce(S_GG, 1);
       lb_first_step<<<P_, kThreads, 0, s_>>>(g, step_.p, n_, st_.p, part_.p, P_);
+      reduce(S_SG, 2);
     } else {
       const int jmin = std::max(0, k_ - M), jmax = k_;
       const int m = jmax - jmin;
       int i0 = (jmax - 1) % M;
       lb_start<<<P_, kThreads, 0, s_>>>(g, step_.p, sm_.p + int64_t(i0) * n_, n_, part_.p, P_);
+      reduce(S_IN, 1);
       for (int t = 0; t < m; ++t) {
         const int j = jmax - 1 - t;
         const int i = j % M;
@@ -520,6 +538,7 @@ class Lbfgs final : public Optimizer {
         const double* dnext = last ? ym_.p + int64_t(inext) * n_ : sm_.p + int64_t(inext) * n_;
         lb_update<<<P_, kThreads, 0, s_>>>(0, last, step_.p, ym_.p + int64_t(i) * n_, dnext, g, n_, st_.p, rho_.p,
                                            alpha_.p, i, part_.p, P_, t % 2 ? S_OUT : S_IN, t % 2 ? S_IN : S_OUT);
+        reduce(t % 2 ? S_IN : S_OUT, 1);
       }
       for (int t = 0; t < m; ++t) {
         const int j = jmin + t;
@@ -530,6 +549,8 @@ class Lbfgs final : public Optimizer {
         const int u = m + t;  // update index over both loops
         lb_update<<<P_, kThreads, 0, s_>>>(1, last, step_.p, sm_.p + int64_t(i) * n_, dnext, g, n_, st_.p, rho_.p,
                                            alpha_.p, i, part_.p, P_, u % 2 ? S_OUT : S_IN, u % 2 ? S_IN : S_OUT);
+        if (last) reduce(S_SG, 2);  // the line-search dots
+        else reduce(u % 2 ? S_IN : S_OUT, 1);
       }
     }
     FB_LAUNCH_CHECK();
@@ -543,6 +564,7 @@ class Lbfgs final : public Optimizer {
       eval(X_[o].p, G_[o].p, e_.p);
       lb_post<<<P_, kThreads, 0, s_>>>(X_[o].p, X_[c].p, G_[o].p, G_[c].p, sm_.p + int64_t(kl) * n_,
                                        ym_.p + int64_t(kl) * n_, n_, part_.p, P_);
+      reduce(S_GG, 3);
       lb_finalize<<<1, 256, 0, s_>>>(st_.p, e_.p, rho_.p, kl, part_.p, P_, host_);
       FB_LAUNCH_CHECK();
       FB_CUDA(cudaStreamSynchronize(s_));
@@ -573,12 +595,20 @@ class Lbfgs final : public Optimizer {
     ++nfev_;
     eval(X_[cur_].p, G_[cur_].p, e_.p);
     dot_kernel<<<P_, kThreads, 0, s_>>>(G_[cur_].p, G_[cur_].p, n_, part_.p, P_, S_GG);
-    lb_init_fin<<<1, 256, 0, s_>>>(st_.p, e_.p, 1.0 / double(n_), part_.p, P_, host_);
+    reduce(S_GG, 1);
+    lb_init_fin<<<1, 256, 0, s_>>>(st_.p, e_.p, 1.0 / double(global_n_), part_.p, P_, host_);
     FB_LAUNCH_CHECK();
     FB_CUDA(cudaStreamSynchronize(s_));
     f_ = host_[1];
     rms_ = host_[2];
     func_initialized_ = true;
+  }
+
+  // sums `count` partial-sum slots over the processes of a sharded pattern
+  void reduce(int slot, int count) {
+    if (!reducer_) return;
+    FB_LAUNCH_CHECK();
+    reducer_(part_.p + int64_t(slot) * P_, int64_t(count) * P_, s_, reducer_ctx_);
   }
 
   LbfgsParams prm_;
@@ -587,6 +617,9 @@ class Lbfgs final : public Optimizer {
   int cur_ = 0;
   int k_ = 0;
   double h0_ = 0.1;
+  ReduceFn reducer_ = nullptr;
+  void* reducer_ctx_ = nullptr;
+  int64_t global_n_ = n_;
 };
 
 class Fire final : public Optimizer {

@@ -51,6 +51,15 @@ class Optimizer {
   virtual double* device_x() = 0;
   virtual double* device_g() = 0;
   virtual double h0() const { return 0.0; }
+  // One pattern split over processes (each holds a slab of x): every dot
+  // product's block partials are summed over the processes by fn before they
+  // are used, and the rms is taken over global_ndof coordinates.
+  virtual void set_reducer(ReduceFn fn, void* ctx, int64_t global_ndof) {
+    (void)fn;
+    (void)ctx;
+    (void)global_ndof;
+    throw InvalidArgument("this optimiser does not run over a sharded pattern (LBFGS does)");
+  }
 
  protected:
   Optimizer(PotentialPtr pot, int64_t n, double tol, int maxiter, int iprint, int verbosity);

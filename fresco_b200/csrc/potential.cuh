@@ -12,6 +12,8 @@
 
 namespace fb {
 
+using ReduceFn = void (*)(double* data, int64_t count, void* stream, void* ctx);
+
 class Potential {
  public:
   virtual ~Potential();
@@ -48,6 +50,15 @@ class Potential {
   // coordinate, UwNU divides by 2 pi, NUwNU drops conj(c_j), UwU halves the
   // rho term and drops the d(1/R) term.
   virtual void set_gradient_mode(int mode) { grad_mode_ = mode; }
+  // The sum over the processes that share one pattern of a device array, in
+  // place, ordered on `stream` (the caller's all-reduce).  Only a potential
+  // with an exchange step (a NUwU shard) takes one; it then evaluates the
+  // whole pattern's loss through it.
+  virtual void set_reducer(ReduceFn fn, void* ctx) {
+    (void)fn;
+    (void)ctx;
+    throw InvalidArgument(kind() + " has no exchange step between processes");
+  }
   int gradient_mode() const { return grad_mode_; }
   // Human-readable set-up summary (kernel width, grids, ...).
   virtual std::string describe() const { return kind(); }

@@ -23,6 +23,8 @@ from . import _lib
 from ._lib import check, dptr, lib
 from .potentials import _f64, _precision
 
+__all__ = ["ShardedNUwU", "ShardedLBFGS", "Reducer", "shard_totals", "weight_factor_sum"]
+
 
 def _dist(group):
     try:
@@ -164,3 +166,115 @@ class ShardedNUwU:
         st = C.c_int(0)
         check(lib.fresco_potential_status(self._h, None, C.byref(st)))
         return st.value
+
+
+# fresco_reduce_fn: (device address, count, CUDA stream, context)
+REDUCE_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p)
+
+
+class _DeviceArray:
+    """A float64 device array at a raw address, for a zero-copy torch view (CUDA array interface)."""
+
+    def __init__(self, ptr, count):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<f8", "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+class Reducer:
+    """The exchange step of a pattern split over processes, as the library calls it: a fresco_reduce_fn
+    that views the device array as a float64 tensor and sums it over the processes in place, on the
+    library's stream.  `fn(tensor)` does the sum (default: torch.distributed.all_reduce over `group`, a
+    no-op without a multi-rank group).  Exceptions cannot cross the C boundary: they are kept and raised
+    by `check()`."""
+
+    def __init__(self, group=None, fn=None):
+        self.group = group
+        self.fn = fn
+        self.error = None
+        self.calls = 0
+        self.c_fn = REDUCE_FN(self._call)  # kept alive with this object
+
+    def _call(self, ptr, count, stream, ctx):
+        try:
+            self.calls += 1
+            if self.error is not None or count <= 0:
+                return
+            import torch
+
+            t = torch.as_tensor(_DeviceArray(ptr, count), device="cuda")
+            with torch.cuda.stream(torch.cuda.ExternalStream(int(stream or 0), device=t.device)):
+                if self.fn is not None:
+                    self.fn(t)
+                else:
+                    dist = _dist(self.group)
+                    if dist is not None:
+                        dist.all_reduce(t, group=self.group)
+        except BaseException as exc:  # noqa: BLE001 (reported by check())
+            if self.error is None:
+                self.error = exc
+
+    def check(self):
+        if self.error is not None:
+            err, self.error = self.error, None
+            raise RuntimeError(f"the exchange step failed: {err!r}") from err
+
+
+def _enable_reducer(shard, reducer):
+    check(lib.fresco_potential_set_reducer(shard._h, C.cast(reducer.c_fn, C.c_void_p), None))
+    shard._reducer = reducer
+
+
+class ShardedLBFGS:
+    """LBFGS_CPP (fresco/optimize/_lbfgs_cpp.pyx:38-84, source/lbfgs.cpp:9-258) over one pattern split
+    between processes: this rank's coordinates `x_local` and its `ShardedNUwU`.  The device LBFGS runs
+    on every rank with its slab of x; each of its dot products (two-loop recursion, step norm, accept
+    test, rms over all n_total * ndim coordinates) has its block partial sums all-reduced before use,
+    and each evaluation all-reduces the shard's rho.  Every rank therefore sees the same scalars and
+    takes the same steps: the trajectory is the single-process one, up to the order of the sums.
+    `reducer`: a `Reducer` (default: all-reduce over `group`).  The result methods are those of
+    LBFGS_CPP, with this rank's coordinates and gradient."""
+
+    def __init__(self, x_local, shard, tol=1e-5, M=4, maxstep=0.1, maxErise=1e-4, H0=0.1, iprint=-1,
+                 nsteps=10000, verbosity=0, rel_energy=False, group=None, reducer=None, events=None):
+        from .optimize import GradientOptimizer
+
+        x = _f64(x_local)
+        if x.size != shard.N * shard.ndim:
+            raise ValueError(f"expected {shard.N * shard.ndim} coordinates, got {x.size}")
+        self.shard = shard
+        self.reducer = reducer if reducer is not None else Reducer(group)
+        _enable_reducer(shard, self.reducer)
+        h = _lib.handle_t()
+        check(lib.fresco_lbfgs_create(shard._h, dptr(x), x.size, float(tol), int(M), float(maxstep),
+                                      float(maxErise), float(H0), int(bool(rel_energy)), int(nsteps), int(iprint),
+                                      int(verbosity), C.byref(h)))
+        self._opt = GradientOptimizer()
+        self._opt._h = h
+        self._opt._n = x.size
+        self._opt.events = [] if events is None else events
+        check(lib.fresco_optimizer_set_reducer(h, C.cast(self.reducer.c_fn, C.c_void_p), None,
+                                               int(shard.n_total) * shard.ndim))
+
+    def _checked(self, f, *a):
+        try:
+            return f(*a)
+        finally:
+            self.reducer.check()
+
+    def run(self, niter=None):
+        return self._checked(self._opt.run, niter)
+
+    def one_iteration(self):
+        return self._checked(self._opt.one_iteration)
+
+    def get_result(self):
+        return self._checked(self._opt.get_result)
+
+    def stop_criterion_satisfied(self):
+        return self._checked(self._opt.stop_criterion_satisfied)
+
+    def get_niter(self):
+        return self._opt.get_niter()
+
+    def get_maxiter(self):
+        return self._opt.get_maxiter()

@@ -35,6 +35,10 @@ typedef struct fresco_optimizer_s* fresco_optimizer;
 typedef struct fresco_ensemble_s* fresco_ensemble;
 typedef struct fresco_ensemble_lbfgs_s* fresco_ensemble_lbfgs;
 typedef struct fresco_overlap_s* fresco_overlap;
+/* Sums `count` doubles at device address `data` over the processes that share
+ * one pattern, in place, ordered on the CUDA stream `stream` (an all-reduce
+ * supplied by the caller, e.g. NCCL through torch.distributed). */
+typedef void (*fresco_reduce_fn)(double* data, int64_t count, void* stream, void* ctx);
 typedef struct fresco_window_stats_s* fresco_window_stats;
 
 enum {
@@ -186,6 +190,14 @@ int fresco_nuwnu_energy_gradient_noalloc(const double* d_x, int64_t n_points, in
 int fresco_export_structure(const double* x, int64_t n_points, int ndim, const double* L, int Nk, const double* radii,
                             double tol, double* sk, double* gr, double* s_radial, double* g_radial);
 
+/* A NUwU shard (fresco_nuwu_shard_create) with a reducer evaluates the whole
+ * pattern through the ordinary calls and optimisers: its rho, fn over the
+ * active modes' rho (2 * n_rho doubles), the shared mode pass, its own
+ * gradient.  Other potentials have no exchange step and refuse one.  No
+ * reference counterpart (the reference evaluates a pattern in one process,
+ * source/fresco/nuwu.hpp:210-317). */
+int fresco_potential_set_reducer(fresco_potential p, fresco_reduce_fn fn, void* ctx);
+
 /* Sticky status bits raised since the last call (1: non-finite input).
  * Synchronises `stream`.  No reference counterpart (FINUFFT's return codes
  * are ignored at source/fresco/nuwu.hpp:191-192, 256-258). */
@@ -236,6 +248,13 @@ int fresco_fire_graph_create(fresco_potential p, const double* x0, int64_t n, do
                              double maxstep, int Nmin, double finc, double fdec, double fa, double astart, double tol,
                              int stepback, int nsteps, fresco_optimizer* out);
 
+/* LBFGS over a pattern split between processes (each process's optimiser
+ * holds its slab of x and its shard's potential): every dot product of
+ * lbfgs.cpp:9-258 (two-loop recursion, step norm, accept test, rms) has its
+ * block partial sums reduced by fn before use, and the rms is taken over
+ * global_ndof coordinates.  Call before the first evaluation; each process
+ * takes the same steps.  LBFGS handles only. */
+int fresco_optimizer_set_reducer(fresco_optimizer o, fresco_reduce_fn fn, void* ctx, int64_t global_ndof);
 /* GradientOptimizer::set_func_gradient(f, grad)  (source/fresco/optimizer.hpp:127-144). */
 int fresco_optimizer_set_func_gradient(fresco_optimizer o, double f, const double* grad, int64_t n);
 /* GradientOptimizer::run(niter) / run()  (optimizer.hpp:97-121); niter < 0 runs to maxiter. */
