@@ -245,3 +245,29 @@ def test_graph_fire_matches_fire_cpp():
     assert rb.nsteps == ra.nsteps and rb.nfev == ra.nfev
     assert rel(rb.coords, ra.coords) < 1e-8
     assert b.run(10).nsteps == rb.nsteps  # converged: no iteration
+
+
+@pytest.mark.parametrize("graph_first", [False, True])
+def test_graph_fire_combined_potential(graph_first):
+    """The graph FIRE on NUwU + cell-list repulsion (the golden combined inputs): the repulsion's cell
+    sort and pair kernels are captured into the loop's branches; same trajectory as ModifiedFireCPP."""
+    from fresco_b200 import CombinedPotential, InversePower, NUwU
+    from fresco_b200.optimize import ModifiedFire_Graph, ModifiedFireCPP
+
+    d = dict(np.load(os.path.join(GOLDEN, "lbfgs_combined_2d.npz")))
+
+    def comb():
+        c = CombinedPotential()
+        c.add_potential(NUwU(d["radii"], float(d["K"]), d["Sk"], d["V"], d["L"], eps=1e-13))
+        c.add_potential(InversePower(2.0, 1.0, d["rep_radii"], d["L"], use_cell_lists=True))
+        return c
+
+    kw = dict(dtstart=0.01, dtmax=0.1, maxstep=0.05, tol=1e-10)
+    a, b = ModifiedFireCPP(d["x"], comb(), **kw), ModifiedFire_Graph(d["x"], comb(), **kw)
+    if graph_first:
+        rb, ra = b.run(40), a.run(40)
+    else:
+        ra, rb = a.run(40), b.run(40)
+    assert rb.nsteps == ra.nsteps == 40 and rb.nfev == ra.nfev
+    assert rel(rb.energy, ra.energy) < 1e-8
+    assert rel(rb.coords, ra.coords) < 1e-8
