@@ -515,6 +515,30 @@ int fresco_optimizer_get_state(fresco_optimizer o, double* x, double* g, double*
   });
 }
 
+int fresco_optimizer_state_bytes(fresco_optimizer o, int64_t* bytes) {
+  return guarded([&] {
+    if (!o || !bytes) throw fb::InvalidArgument("null argument");
+    *bytes = o->opt->state_bytes();
+    return FRESCO_OK;
+  });
+}
+
+int fresco_optimizer_save_state(fresco_optimizer o, void* image) {
+  return guarded([&] {
+    if (!o || !image) throw fb::InvalidArgument("null argument");
+    o->opt->save_state(static_cast<uint8_t*>(image));
+    return FRESCO_OK;
+  });
+}
+
+int fresco_optimizer_load_state(fresco_optimizer o, const void* image, int64_t bytes) {
+  return guarded([&] {
+    if (!o || !image) throw fb::InvalidArgument("null argument");
+    o->opt->load_state(static_cast<const uint8_t*>(image), bytes);
+    return FRESCO_OK;
+  });
+}
+
 int fresco_optimizer_device_state(fresco_optimizer o, double** d_x, double** d_g) {
   return guarded([&] {
     if (!o) throw fb::InvalidArgument("null handle");

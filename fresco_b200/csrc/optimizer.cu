@@ -1,6 +1,7 @@
 // Device-resident LBFGS and modified FIRE (see optimizer.cuh).
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <cstdio>
 #include <vector>
 
@@ -432,6 +433,20 @@ __global__ void fi_restore(double* __restrict__ v, int64_t n, const FiState* st)
 // host classes
 // ---------------------------------------------------------------------------
 
+// A loaded FIRE state keeps the loading optimiser's parameters.
+void fire_keep_params(FiState& h, const FireParams& p, int64_t n) {
+  h.sqrtN = std::sqrt(double(n));
+  h.dtmax = p.dtmax;
+  h.maxstep = p.maxstep;
+  h.finc = p.finc;
+  h.fdec = p.fdec;
+  h.fa = p.fa;
+  h.astart = p.astart;
+  h.Nmin = p.Nmin;
+  h.stepback = p.stepback ? 1 : 0;
+  h.tol = p.tol;
+}
+
 class Lbfgs final : public Optimizer {
  public:
   Lbfgs(PotentialPtr pot, const double* x0, int64_t n, const LbfgsParams& p)
@@ -604,6 +619,34 @@ class Lbfgs final : public Optimizer {
     func_initialized_ = true;
   }
 
+  int family() const override { return 1; }
+  int memory_length() const override { return prm_.M; }
+  std::vector<Block> image_blocks() override {
+    const int64_t n = n_, M = prm_.M;
+    return {{st_.p, int64_t(sizeof(LbState))},
+            {X_[cur_].p, n * 8},
+            {G_[cur_].p, n * 8},
+            {sm_.p, M * n * 8},
+            {ym_.p, M * n * 8},
+            {rho_.p, M * 8},
+            {e_.p, 8}};
+  }
+  // the loaded state keeps this optimiser's parameters
+  void after_load() override {
+    LbState h{};
+    FB_CUDA(cudaMemcpyAsync(&h, st_.p, sizeof(h), cudaMemcpyDeviceToHost, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
+    h.inv_sqrt_n = 1.0 / std::sqrt(double(global_n_));
+    h.maxstep = prm_.maxstep;
+    h.max_f_rise = prm_.max_f_rise;
+    h.rel = prm_.rel_energy ? 1 : 0;
+    h.M = prm_.M;
+    FB_CUDA(cudaMemcpyAsync(st_.p, &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
+    k_ = h.k;
+    h0_ = h.H0;
+  }
+
   // sums `count` partial-sum slots over the processes of a sharded pattern
   void reduce(int slot, int count) {
     if (!reducer_) return;
@@ -727,6 +770,21 @@ class Fire final : public Optimizer {
     ++nfev_;
     eval(X_[cur_].p, G_[cur_].p, e_.p);
     init_from_gradient();
+  }
+
+  int family() const override { return 2; }
+  std::vector<Block> image_blocks() override {
+    const int64_t n = n_;
+    return {{st_.p, int64_t(sizeof(FiState))}, {X_[cur_].p, n * 8}, {G_[cur_].p, n * 8}, {V_.p, n * 8}, {e_.p, 8}};
+  }
+  void after_load() override {
+    FiState h{};
+    FB_CUDA(cudaMemcpyAsync(&h, st_.p, sizeof(h), cudaMemcpyDeviceToHost, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
+    fire_keep_params(h, prm_, n_);
+    h.cur = cur_;
+    FB_CUDA(cudaMemcpyAsync(st_.p, &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
   }
 
   FireParams prm_;
@@ -927,6 +985,21 @@ class FireGraph final : public Optimizer {
     init_from_gradient();
   }
 
+  int family() const override { return 2; }
+  std::vector<Block> image_blocks() override {
+    const int64_t n = n_;
+    return {{st_.p, int64_t(sizeof(FiState))}, {X_[cur_].p, n * 8}, {G_[cur_].p, n * 8}, {V_.p, n * 8}, {e_.p, 8}};
+  }
+  void after_load() override {
+    FiState h{};
+    FB_CUDA(cudaMemcpyAsync(&h, st_.p, sizeof(h), cudaMemcpyDeviceToHost, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
+    fire_keep_params(h, prm_, n_);
+    h.cur = cur_;
+    FB_CUDA(cudaMemcpyAsync(st_.p, &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+    FB_CUDA(cudaStreamSynchronize(s_));
+  }
+
   FireParams prm_;
   DevBuf<double> X_[2], G_[2];  // current point and its gradient in [cur_], the trial in the other
   int cur_ = 0;
@@ -969,6 +1042,65 @@ void Optimizer::run(int niter) {
 }
 
 void Optimizer::run() { run(maxiter_ - iter_); }
+
+namespace {
+struct ImageHeader {
+  uint32_t magic = 0x54534246u;  // "FBST"
+  uint32_t version = 1;
+  int32_t family = 0, memory = 0;
+  int64_t n = 0;
+  int32_t iter = 0, nfev = 0, func_initialized = 0, pad = 0;
+  double f = 0.0, rms = 0.0;
+};
+}  // namespace
+
+int64_t Optimizer::state_bytes() const {
+  int64_t b = sizeof(ImageHeader);
+  for (const Block& k : const_cast<Optimizer*>(this)->image_blocks()) b += k.bytes;
+  return b;
+}
+
+void Optimizer::save_state(uint8_t* buf) {
+  ImageHeader h;
+  h.family = family();
+  h.memory = memory_length();
+  h.n = n_;
+  h.iter = iter_;
+  h.nfev = nfev_;
+  h.func_initialized = func_initialized_ ? 1 : 0;
+  h.f = f_;
+  h.rms = rms_;
+  std::memcpy(buf, &h, sizeof(h));
+  int64_t off = sizeof(h);
+  for (const Block& k : image_blocks()) {
+    FB_CUDA(cudaMemcpyAsync(buf + off, k.dev, k.bytes, cudaMemcpyDeviceToHost, s_));
+    off += k.bytes;
+  }
+  FB_CUDA(cudaStreamSynchronize(s_));
+}
+
+void Optimizer::load_state(const uint8_t* buf, int64_t bytes) {
+  if (bytes < int64_t(sizeof(ImageHeader))) throw InvalidArgument("optimiser state image too short");
+  ImageHeader h;
+  std::memcpy(&h, buf, sizeof(h));
+  if (h.magic != ImageHeader().magic || h.version != 1) throw InvalidArgument("not an optimiser state image");
+  if (h.family != family()) throw InvalidArgument("the state image is of another optimiser family");
+  if (h.n != n_) throw InvalidArgument("the state image has another number of coordinates");
+  if (h.memory != memory_length()) throw InvalidArgument("the state image has another memory length M");
+  if (bytes != state_bytes()) throw InvalidArgument("optimiser state image has the wrong size");
+  int64_t off = sizeof(h);
+  for (const Block& k : image_blocks()) {
+    FB_CUDA(cudaMemcpyAsync(k.dev, buf + off, k.bytes, cudaMemcpyHostToDevice, s_));
+    off += k.bytes;
+  }
+  FB_CUDA(cudaStreamSynchronize(s_));
+  iter_ = h.iter;
+  nfev_ = h.nfev;
+  func_initialized_ = h.func_initialized != 0;
+  f_ = h.f;
+  rms_ = h.rms;
+  after_load();
+}
 
 bool Optimizer::stop_criterion_satisfied() {
   if (!func_initialized_) initialize_func_gradient();

@@ -11,6 +11,7 @@
 #pragma once
 
 #include <memory>
+#include <vector>
 
 #include "potential.cuh"
 
@@ -48,6 +49,13 @@ class Optimizer {
   virtual void set_func_gradient(double f, const double* grad, int64_t n) = 0;
   virtual void reset(const double* x0, int64_t n) = 0;
   void get_state(double* x, double* g, double* f, double* rms, int* nfev, int* niter, int* maxiter, double* H0);
+  // Exact-resume image of the optimiser's state (coordinates, gradient,
+  // memory, step parameters, counters), host bytes.  An image loads into an
+  // optimiser of the same family, size and memory length; the loaded one
+  // continues the saved trajectory.
+  int64_t state_bytes() const;
+  void save_state(uint8_t* buf);
+  void load_state(const uint8_t* buf, int64_t bytes);
   virtual double* device_x() = 0;
   virtual double* device_g() = 0;
   virtual double h0() const { return 0.0; }
@@ -63,6 +71,17 @@ class Optimizer {
 
  protected:
   Optimizer(PotentialPtr pot, int64_t n, double tol, int maxiter, int iprint, int verbosity);
+  // Image layout after the common header: the device blocks of `image_blocks`
+  // in order.  family: 1 LBFGS, 2 FIRE (both FIRE forms share one layout).
+  struct Block {
+    void* dev;
+    int64_t bytes;
+  };
+  virtual int family() const = 0;
+  virtual int memory_length() const { return 0; }
+  virtual std::vector<Block> image_blocks() = 0;
+  // after a load: re-establish host mirrors and invariants from the device state
+  virtual void after_load() {}
   virtual void initialize_func_gradient() = 0;
   void eval(const double* x, double* g, double* e);  // one potential call (nfev not touched)
 

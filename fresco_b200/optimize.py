@@ -146,6 +146,30 @@ class GradientOptimizer:
         res.success = bool(self.stop_criterion_satisfied())
         return res
 
+    def save_state(self):
+        """Exact-resume image of the optimiser's device state and counters (uint8 array): x, g, the LBFGS
+        memory pairs or the FIRE velocities and step sizes.  No reference counterpart (the reference
+        checkpoints coordinates only, opt.pyx:42-54)."""
+        nb = C.c_int64()
+        check(lib.fresco_optimizer_state_bytes(self._h, C.byref(nb)))
+        img = np.empty(nb.value, dtype=np.uint8)
+        check(lib.fresco_optimizer_save_state(self._h, img.ctypes.data_as(C.c_void_p)))
+        return img
+
+    def load_state(self, image):
+        """Continues the trajectory saved by save_state (same family, coordinate count and memory length;
+        this optimiser keeps its own parameters)."""
+        img = np.ascontiguousarray(np.asarray(image, dtype=np.uint8).ravel())
+        check(lib.fresco_optimizer_load_state(self._h, img.ctypes.data_as(C.c_void_p), img.size))
+        self.res = None
+
+    def save_checkpoint(self, file_name):
+        """save_state() written to `file_name` (numpy .npy)."""
+        np.save(file_name, self.save_state())
+
+    def load_checkpoint(self, file_name):
+        self.load_state(np.load(file_name))
+
     def device_state(self):
         """(x, g) device pointers of the optimiser state."""
         dx = C.c_void_p()

@@ -273,6 +273,12 @@ class ShardedLBFGS:
     def stop_criterion_satisfied(self):
         return self._checked(self._opt.stop_criterion_satisfied)
 
+    def save_state(self):
+        return self._opt.save_state()
+
+    def load_state(self, image):
+        self._opt.load_state(image)
+
     def get_niter(self):
         return self._opt.get_niter()
 

@@ -271,6 +271,16 @@ int fresco_optimizer_get_state(fresco_optimizer o, double* x, double* g, double*
                                int* niter, int* maxiter, double* H0);
 /* Device pointers of the optimiser's x and g (valid until destroy). */
 int fresco_optimizer_device_state(fresco_optimizer o, double** d_x, double** d_g);
+/* Checkpoint for an exact resume (no reference counterpart: the reference
+ * saves coordinates only, opt.pyx:42-54).  The image holds the optimiser's
+ * device state (x, g, LBFGS memory pairs or FIRE velocities, step sizes) and
+ * counters; *bytes receives its size.  An image loads into an optimiser of
+ * the same family (LBFGS, or either FIRE form), coordinate count and memory
+ * length M, which keeps its own parameters and continues the saved
+ * trajectory. */
+int fresco_optimizer_state_bytes(fresco_optimizer o, int64_t* bytes);
+int fresco_optimizer_save_state(fresco_optimizer o, void* image);
+int fresco_optimizer_load_state(fresco_optimizer o, const void* image, int64_t bytes);
 void fresco_optimizer_destroy(fresco_optimizer o);
 
 /* ---- batched ensembles ---------------------------------------------------- */

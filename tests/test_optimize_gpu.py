@@ -271,3 +271,47 @@ def test_graph_fire_combined_potential(graph_first):
     assert rb.nsteps == ra.nsteps == 40 and rb.nfev == ra.nfev
     assert rel(rb.energy, ra.energy) < 1e-8
     assert rel(rb.coords, ra.coords) < 1e-8
+
+
+def test_checkpoint_resumes_exactly(tmp_path):
+    """save_state / load_state: stopping, saving, loading into a fresh optimiser and continuing gives the
+    uninterrupted trajectory (LBFGS memory, FIRE velocities and step sizes, counters); a FIRE image loads
+    into the graph form too; mismatched images are refused."""
+    from fresco_b200 import NUwU
+    from fresco_b200.optimize import LBFGS_CPP, ModifiedFire_Graph, ModifiedFireCPP
+
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(400, 8, 5, ndim=2, seed=13, L=np.ones(2))
+
+    def pot():
+        return NUwU(radii, 8, Sk, V, L, eps=1e-13)
+
+    # tol far below the reachable rms: two potential objects agree to the last few bits, and a stop
+    # decision at the tolerance would turn on those bits; a wrong load diverges at the percent level
+    a = LBFGS_CPP(x, pot(), M=5, tol=1e-12)
+    a.run(10)
+    img = a.save_state()
+    ra = a.run(12)
+    b = LBFGS_CPP(np.zeros_like(x), pot(), M=5, tol=1e-12)
+    b.load_state(img)
+    rb = b.run(12)
+    assert rb.nsteps == ra.nsteps == 22 and rb.nfev == ra.nfev
+    assert rel(rb.energy, ra.energy) < 1e-8 and rel(rb.coords, ra.coords) < 1e-8
+    assert rel(rb.H0, ra.H0) < 1e-6
+    with pytest.raises(ValueError, match="memory length"):
+        LBFGS_CPP(x, pot(), M=4).load_state(img)
+    with pytest.raises(ValueError, match="another optimiser family"):
+        ModifiedFireCPP(x, pot()).load_state(img)
+    with pytest.raises(ValueError, match="another number of coordinates"):
+        LBFGS_CPP(x[:-2], NUwU(radii[:-1], 8, Sk, V, L), M=5).load_state(img)
+
+    kw = dict(dtstart=0.01, dtmax=0.1, maxstep=0.05, tol=1e-12)
+    f = ModifiedFireCPP(x, pot(), **kw)
+    f.run(15)
+    f.save_checkpoint(str(tmp_path / "fire.npy"))
+    rf = f.run(15)
+    for cls in (ModifiedFireCPP, ModifiedFire_Graph):
+        g = cls(np.zeros_like(x), pot(), **kw)
+        g.load_checkpoint(str(tmp_path / "fire.npy"))
+        rg = g.run(15)
+        assert rg.nsteps == rf.nsteps == 30 and rg.nfev == rf.nfev, cls.__name__
+        assert rel(rg.energy, rf.energy) < 1e-8 and rel(rg.coords, rf.coords) < 1e-8, cls.__name__
