@@ -195,11 +195,32 @@ def sharded_report(args, dev, ws, rank):
     t1.record(stream)
     torch.cuda.synchronize()
     ms = reduce_max(t0.elapsed_time(t1) / n, dev)
-    return {"workload": "the config-2 NUwU pattern (seed 2) split into equal point slabs, one per rank",
-            "ranks": ws, "points_per_rank": int(b - a), "evals_per_s": round(1000.0 / ms, 2),
-            "ms_per_eval": round(ms, 5), "allreduce_bytes_per_eval": int(16 * sh.n_rho),
-            "energy": float(e.item()), "transforms": "cuFFT (pruned column passes)",
-            "timing": "CUDA events on the launch stream, max over ranks"}
+    out = {"workload": "the config-2 NUwU pattern (seed 2) split into equal point slabs, one per rank",
+           "ranks": ws, "points_per_rank": int(b - a), "evals_per_s": round(1000.0 / ms, 2),
+           "ms_per_eval": round(ms, 5), "allreduce_bytes_per_eval": int(16 * sh.n_rho),
+           "energy": float(e.item()), "transforms": "cuFFT (pruned column passes)",
+           "timing": "CUDA events on the launch stream, max over ranks"}
+    if ws == 1:
+        # LBFGS over the sharded pattern: the device LBFGS with its dot products and the shard's rho
+        # passed through the exchange hook (a no-op with one rank); one process only, so that a
+        # multi-rank job takes no collective here that its other sections do not
+        from fresco_b200 import ShardedLBFGS
+
+        opt = ShardedLBFGS(x[2 * a : 2 * b], sh, M=4, tol=0.0)
+        opt.run(3)
+        torch.cuda.synchronize()
+        from fresco_b200._lib import check as _check, lib as _clib
+
+        n_it = max(20, args.steps)
+        t_0 = time.perf_counter()
+        _check(_clib.fresco_optimizer_run(opt._opt._h, n_it))  # the iterations only, as the lbfgs section
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t_0
+        res = opt.get_result()
+        out["lbfgs"] = {"iterations_per_s": round(n_it / dt, 2), "iterations": n_it, "evals": int(res.nfev),
+                        "energy": float(res.energy), "exchange_calls": int(opt.reducer.calls), "M": 4,
+                        "timing": "host wall clock around the C-level run loop, one rank"}
+    return out
 
 
 def other_configs_report(args, dev):

@@ -192,7 +192,12 @@ class Reducer:
         self.fn = fn
         self.error = None
         self.calls = 0
+        self._streams = {}
         self.c_fn = REDUCE_FN(self._call)  # kept alive with this object
+
+    def active(self) -> bool:
+        """Whether there is anything to sum: a custom `fn`, or a process group of several ranks."""
+        return self.fn is not None or _dist(self.group) is not None
 
     def _call(self, ptr, count, stream, ctx):
         try:
@@ -202,7 +207,11 @@ class Reducer:
             import torch
 
             t = torch.as_tensor(_DeviceArray(ptr, count), device="cuda")
-            with torch.cuda.stream(torch.cuda.ExternalStream(int(stream or 0), device=t.device)):
+            key = int(stream or 0)
+            st = self._streams.get(key)
+            if st is None:
+                st = self._streams[key] = torch.cuda.ExternalStream(key, device=t.device)
+            with torch.cuda.stream(st):
                 if self.fn is not None:
                     self.fn(t)
                 else:
@@ -243,7 +252,12 @@ class ShardedLBFGS:
             raise ValueError(f"expected {shard.N * shard.ndim} coordinates, got {x.size}")
         self.shard = shard
         self.reducer = reducer if reducer is not None else Reducer(group)
-        _enable_reducer(shard, self.reducer)
+        # one process holding the whole pattern has nothing to exchange: no hooks
+        hooks = self.reducer.active()
+        if not hooks and shard.n_total != shard.N:
+            raise ValueError("a shard of a larger pattern needs a multi-rank process group or a reducer")
+        if hooks:
+            _enable_reducer(shard, self.reducer)
         h = _lib.handle_t()
         check(lib.fresco_lbfgs_create(shard._h, dptr(x), x.size, float(tol), int(M), float(maxstep),
                                       float(maxErise), float(H0), int(bool(rel_energy)), int(nsteps), int(iprint),
@@ -252,8 +266,9 @@ class ShardedLBFGS:
         self._opt._h = h
         self._opt._n = x.size
         self._opt.events = [] if events is None else events
-        check(lib.fresco_optimizer_set_reducer(h, C.cast(self.reducer.c_fn, C.c_void_p), None,
-                                               int(shard.n_total) * shard.ndim))
+        if hooks:
+            check(lib.fresco_optimizer_set_reducer(h, C.cast(self.reducer.c_fn, C.c_void_p), None,
+                                                   int(shard.n_total) * shard.ndim))
 
     def _checked(self, f, *a):
         try:

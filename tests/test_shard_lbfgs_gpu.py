@@ -58,7 +58,19 @@ def test_one_rank_matches_lbfgs_cpp():
         assert rel(rb.energy, ra.energy) < 1e-9
         assert rel(rb.coords, ra.coords) < 1e-9
         assert rel(rb.rms, ra.rms) < 1e-8
-    assert opt.reducer.calls > 0
+    assert opt.reducer.calls == 0  # one process: nothing to exchange, no hooks
+    # the same run through the exchange hooks, with an identity reducer
+    from fresco_b200.shard import Reducer
+
+    shard2 = ShardedNUwU(radii, 16, Sk, V, L, eps=1e-13, totals=(len(radii), weight_factor_sum(radii, 2)))
+    hooked = ShardedLBFGS(x, shard2, M=5, reducer=Reducer(fn=lambda t: None))
+    rh = hooked.run(20)
+    assert hooked.reducer.calls > 0 and rh.nfev == ra.nfev and rh.nsteps == ra.nsteps
+    assert rel(rh.energy, ra.energy) < 1e-9 and rel(rh.coords, ra.coords) < 1e-9
+    # a slab of a larger pattern without a group or a reducer is refused
+    half = ShardedNUwU(radii[:100], 16, Sk, V, L, totals=(len(radii), weight_factor_sum(radii, 2)))
+    with pytest.raises(ValueError, match="process group or a reducer"):
+        ShardedLBFGS(x[:200], half)
 
 
 def test_two_ranks_emulated_match_single_process():
