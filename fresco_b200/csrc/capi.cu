@@ -324,6 +324,20 @@ int fresco_potential_set_reducer(fresco_potential p, fresco_reduce_fn fn, void* 
   });
 }
 
+int fresco_inversepower_shard_create(double a, double eps, const double* radii_all, int64_t n_total,
+                                     const double* boxv, int ndim, int periodic, int64_t lo, int64_t hi,
+                                     fresco_gather_fn gather, fresco_reduce_fn reduce, void* ctx,
+                                     fresco_potential* out) {
+  return guarded([&] {
+    if (!out || !boxv || (n_total > 0 && !radii_all)) throw fb::InvalidArgument("null argument");
+    if (ndim < 1 || ndim > 3) throw fb::InvalidArgument("InversePower: ndim must be 1, 2 or 3");
+    *out = wrap(fb::make_inversepower_shard(a, eps, std::vector<double>(radii_all, radii_all + n_total),
+                                            std::vector<double>(boxv, boxv + ndim), periodic != 0, lo, hi, gather,
+                                            reduce, ctx));
+    return FRESCO_OK;
+  });
+}
+
 int fresco_optimizer_set_reducer(fresco_optimizer o, fresco_reduce_fn fn, void* ctx, int64_t global_ndof) {
   return guarded([&] {
     if (!o || !fn) throw fb::InvalidArgument("null argument");

@@ -390,6 +390,8 @@ __global__ void __launch_bounds__(kFinThreads) bl_finalize(BlState* st, const do
 class PotentialEnsemble final : public Ensemble {
  public:
   PotentialEnsemble(PotentialPtr pot, int64_t n) : pot_(std::move(pot)) {
+    if (pot_ && pot_->host_steps())
+      throw InvalidArgument("a graph-captured optimiser cannot capture a potential that exchanges between processes");
     if (!pot_) throw InvalidArgument("null potential");
     if (n <= 0) throw InvalidArgument("empty coordinate array");
     if (pot_->ndof() >= 0 && pot_->ndof() != n) throw InvalidArgument("x0 has the wrong size for the potential");

@@ -237,6 +237,11 @@ class NUwUImpl final : public Potential, public NUwUShard {
   }
 
   void shard_finish(const double* rho, double* g, double* e, cudaStream_t s) override {
+    shard_finish(rho, g, e, s, false);
+  }
+
+  // acc: the gradient is added to g (e always receives this term's energy alone)
+  void shard_finish(const double* rho, double* g, double* e, cudaStream_t s, bool acc) {
     FB_CUDA(cudaMemsetAsync(e, 0, sizeof(double), s));
     if (n_active_ > 0) {
       const int grid = int(std::min<int64_t>(ceil_div(n_active_, 256), int64_t(sm_count()) * 8));
@@ -246,7 +251,7 @@ class NUwUImpl final : public Potential, public NUwUShard {
           g != nullptr);
       FB_LAUNCH_CHECK();
     }
-    if (g) type2_and_interp(g, false, s);
+    if (g) type2_and_interp(g, acc, s);
   }
 
   std::string describe() const override {
@@ -306,20 +311,22 @@ class NUwUImpl final : public Potential, public NUwUShard {
               acc ? 1 : 0, status_.p, s, gs);
   }
 
+  bool host_steps() const override { return sharded_ && reducer_ != nullptr; }
+
   void set_reducer(ReduceFn fn, void* ctx) override {
     if (!sharded_) throw InvalidArgument("NUwU: only a shard of a pattern takes a reducer");
     reducer_ = fn;
     reducer_ctx_ = ctx;
     if (!rho_sum_.p) rho_sum_.alloc(2 * std::max<int64_t>(n_active_, 1));
-    set_graphs_enabled(false);  // the reducer is host code between the shard's launches
+    if (!e_part_.p) e_part_.alloc(1);
   }
 
   void run(const double* x, double* g, double* e, bool acc, cudaStream_t s) {
     if (sharded_ && reducer_) {  // this shard's rho, the sum over the shards, the shared mode pass
-      if (acc) throw InvalidArgument("a sharded NUwU cannot accumulate into another potential's result");
       shard_rho(x, rho_sum_.p, s);
       reducer_(rho_sum_.p, 2 * n_active_, s, reducer_ctx_);
-      shard_finish(rho_sum_.p, g, e, s);
+      shard_finish(rho_sum_.p, g, acc ? e_part_.p : e, s, acc);
+      if (acc) add_scalar(e_part_.p, e, s);
       return;
     }
     if (sharded_ && n_total_ != N_)
@@ -495,7 +502,7 @@ class NUwUImpl final : public Potential, public NUwUShard {
   bool sharded_ = false;
   ReduceFn reducer_ = nullptr;
   void* reducer_ctx_ = nullptr;
-  DevBuf<double> rho_sum_;
+  DevBuf<double> rho_sum_, e_part_;
   int64_t n_total_ = 0;
   double invN_ = 1.0;
   double Karg_;

@@ -918,6 +918,8 @@ class FireGraph final : public Optimizer {
   // (re)builds the loop graph when the potential's gradient convention changed
   void ensure_graph() {
     if (graph_ && graph_mode_ == pot_->gradient_mode()) return;
+    if (pot_->host_steps())
+      throw InvalidArgument("the graph FIRE cannot capture a potential that exchanges between processes");
     if (graph_) {
       cudaGraphExecDestroy(graph_);
       graph_ = nullptr;

@@ -24,7 +24,7 @@ void Potential::eval(const double* x, int64_t n, double* g, double* e, bool acc,
     if (g) energy_gradient(x, n, g, e, acc, st);
     else energy(x, n, e, acc, st);
   };
-  if (!graphs_enabled_ || timing_active()) {
+  if (!graphs_enabled_ || timing_active() || host_steps()) {
     direct(s);
     return;
   }
@@ -131,6 +131,15 @@ void Potential::timer_collect() {
     }
   }
   timer.used = 0;
+}
+
+namespace {
+__global__ void add_scalar_kernel(const double* __restrict__ src, double* dst) { *dst += *src; }
+}  // namespace
+
+void add_scalar(const double* src, double* dst, cudaStream_t s) {
+  add_scalar_kernel<<<1, 1, 0, s>>>(src, dst);
+  FB_LAUNCH_CHECK();
 }
 
 CombinedPotential::CombinedPotential() { init_status(); }

@@ -13,6 +13,13 @@
 namespace fb {
 
 using ReduceFn = void (*)(double* data, int64_t count, void* stream, void* ctx);
+// Concatenation over the processes of their local arrays, in process order,
+// into `full` (full_count values), ordered on `stream`.
+using GatherFn = void (*)(const double* local, int64_t local_count, double* full, int64_t full_count, void* stream,
+                          void* ctx);
+
+// *dst += *src on stream s (one device scalar)
+void add_scalar(const double* src, double* dst, cudaStream_t s);
 
 class Potential {
  public:
@@ -54,6 +61,9 @@ class Potential {
   // place, ordered on `stream` (the caller's all-reduce).  Only a potential
   // with an exchange step (a NUwU shard) takes one; it then evaluates the
   // whole pattern's loss through it.
+  // Whether an evaluation runs host code between its launches (an exchange
+  // between processes): such a potential is never captured into a CUDA graph.
+  virtual bool host_steps() const { return false; }
   virtual void set_reducer(ReduceFn fn, void* ctx) {
     (void)fn;
     (void)ctx;
@@ -121,6 +131,11 @@ class CombinedPotential : public Potential {
   int read_and_clear_status(cudaStream_t s) override;
   void set_gradient_mode(int mode) override;
   bool timing_active() const override;
+  bool host_steps() const override {
+    for (auto& p : parts_)
+      if (p->host_steps()) return true;
+    return false;
+  }
   std::string kind() const override { return "CombinedPotential"; }
   const std::vector<PotentialPtr>& parts() const { return parts_; }
 
@@ -153,6 +168,13 @@ double nuwu_weight_factor_sum(const double* radii, int64_t n, int D);
 PotentialPtr make_nuwu_shard(const std::vector<double>& radii_local, int64_t n_total, double weight_sum_total,
                              double K, const std::vector<double>& sk, const std::vector<double>& v,
                              const std::vector<double>& L, double eps, int precision);
+// InversePower over a pattern split into index slabs: this process owns points
+// [lo, hi); each evaluation gathers every slab, evaluates the repulsion of the
+// whole pattern and keeps this slab's gradient; the energy is counted once
+// (by the process whose slab starts at point 0) and summed by `reduce`.
+PotentialPtr make_inversepower_shard(double a, double eps, const std::vector<double>& radii_all,
+                                     const std::vector<double>& boxv, bool periodic, int64_t lo, int64_t hi,
+                                     GatherFn gather, ReduceFn reduce, void* ctx);
 PotentialPtr make_nuwu(const std::vector<double>& radii, double K, const std::vector<double>& sk,
                        const std::vector<double>& v, const std::vector<double>& L, double eps, int precision);
 PotentialPtr make_uwu(const std::vector<int>& grid, double K, const std::vector<double>& sk,

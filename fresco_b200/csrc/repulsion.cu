@@ -619,6 +619,93 @@ class InversePowerImpl final : public Potential {
 
 }  // namespace
 
+namespace {
+
+// g (+)= full[0..n)
+__global__ void take_slab_kernel(const double* __restrict__ full, double* __restrict__ g, int64_t n, int acc) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    g[i] = acc ? g[i] + full[i] : full[i];
+}
+
+class InversePowerShard final : public Potential {
+ public:
+  InversePowerShard(double a, double eps, const std::vector<double>& radii_all, const std::vector<double>& boxv,
+                    bool periodic, int64_t lo, int64_t hi, GatherFn gather, ReduceFn reduce, void* ctx)
+      : D_(int(boxv.size())), N_(int64_t(radii_all.size())), lo_(lo), hi_(hi), gather_(gather), reduce_(reduce),
+        ctx_(ctx) {
+    if (!gather || !reduce) throw InvalidArgument("a repulsion shard needs a gather and a reduce function");
+    if (lo < 0 || hi < lo || hi > N_) throw InvalidArgument("the slab [lo, hi) must lie within the pattern");
+    inner_ = make_inversepower(a, eps, radii_all, boxv, periodic, true, 1.0);
+    init_status();
+    xall_.alloc(std::max<int64_t>(N_ * D_, 1));
+    gall_.alloc(std::max<int64_t>(N_ * D_, 1));
+    et_.alloc(1);
+  }
+
+  int64_t ndof() const override { return (hi_ - lo_) * D_; }
+  std::string kind() const override { return "InversePowerShard"; }
+  bool host_steps() const override { return true; }  // the gather and the energy sum
+  std::string describe() const override {
+    return "InversePowerShard points [" + std::to_string(lo_) + ", " + std::to_string(hi_) + ") of " +
+           std::to_string(N_) + "; " + inner_->describe();
+  }
+  void set_gradient_mode(int mode) override {
+    grad_mode_ = mode;
+    inner_->set_gradient_mode(mode);
+  }
+  int read_and_clear_status(cudaStream_t s) override {
+    return Potential::read_and_clear_status(s) | inner_->read_and_clear_status(s);
+  }
+
+  void energy(const double* x, int64_t n, double* e, bool acc, cudaStream_t s) override {
+    run(x, nullptr, e, acc, s);
+  }
+  void energy_gradient(const double* x, int64_t n, double* g, double* e, bool acc, cudaStream_t s) override {
+    run(x, g, e, acc, s);
+  }
+
+ private:
+  void run(const double* x, double* g, double* e, bool acc, cudaStream_t s) {
+    gather_(x, (hi_ - lo_) * D_, xall_.p, N_ * D_, s, ctx_);
+    if (g) inner_->energy_gradient(xall_.p, N_ * D_, gall_.p, et_.p, false, s);
+    else inner_->energy(xall_.p, N_ * D_, et_.p, false, s);
+    // every process evaluates the whole pattern; the one whose slab starts at
+    // point 0 contributes the energy, so the sum holds it once, with the same
+    // bits on every process
+    if (!(lo_ == 0 && hi_ > 0)) FB_CUDA(cudaMemsetAsync(et_.p, 0, sizeof(double), s));
+    reduce_(et_.p, 1, s, ctx_);
+    if (acc) {
+      add_scalar(et_.p, e, s);
+    } else {
+      FB_CUDA(cudaMemcpyAsync(e, et_.p, sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    const int64_t n = (hi_ - lo_) * D_;
+    if (g && n > 0) {
+      const int grid = int(std::min<int64_t>(ceil_div(n, 256), int64_t(sm_count()) * 8));
+      take_slab_kernel<<<grid, 256, 0, s>>>(gall_.p + lo_ * D_, g, n, acc ? 1 : 0);
+      FB_LAUNCH_CHECK();
+    }
+  }
+
+  int D_;
+  int64_t N_, lo_, hi_;
+  GatherFn gather_;
+  ReduceFn reduce_;
+  void* ctx_;
+  PotentialPtr inner_;
+  DevBuf<double> xall_, gall_, et_;
+};
+
+}  // namespace
+
+PotentialPtr make_inversepower_shard(double a, double eps, const std::vector<double>& radii_all,
+                                     const std::vector<double>& boxv, bool periodic, int64_t lo, int64_t hi,
+                                     GatherFn gather, ReduceFn reduce, void* ctx) {
+  const int D = int(boxv.size());
+  if (D < 1 || D > 3) throw std::runtime_error("InversePower: dimension " + std::to_string(D) + " is not supported");
+  return PotentialPtr(new InversePowerShard(a, eps, radii_all, boxv, periodic, lo, hi, gather, reduce, ctx));
+}
+
 PotentialPtr make_inversepower(double a, double eps, const std::vector<double>& radii, const std::vector<double>& boxv,
                                bool periodic, bool use_cell_lists, double ncellx_scale) {
   (void)use_cell_lists;

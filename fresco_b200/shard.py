@@ -21,9 +21,10 @@ import ctypes as C
 
 from . import _lib
 from ._lib import check, dptr, lib
-from .potentials import _f64, _precision
+from .potentials import BasePotential, CombinedPotential, Distance, _f64, _precision
 
-__all__ = ["ShardedNUwU", "ShardedLBFGS", "Reducer", "shard_totals", "weight_factor_sum"]
+__all__ = ["ShardedNUwU", "ShardedInversePower", "ShardedLBFGS", "Reducer", "Exchange", "shard_totals",
+           "weight_factor_sum"]
 
 
 def _dist(group):
@@ -63,7 +64,7 @@ def shard_totals(radii_local, ndim: int, group=None, device=None):
     return int(round(float(t[0]))), float(t[1])
 
 
-class ShardedNUwU:
+class ShardedNUwU(BasePotential):
     """This rank's share of one NUwU pattern (fresco/potentials/nuwu.pyx:10-23 arguments, with
     `radii_local` the radii of this rank's points).
 
@@ -207,11 +208,7 @@ class Reducer:
             import torch
 
             t = torch.as_tensor(_DeviceArray(ptr, count), device="cuda")
-            key = int(stream or 0)
-            st = self._streams.get(key)
-            if st is None:
-                st = self._streams[key] = torch.cuda.ExternalStream(key, device=t.device)
-            with torch.cuda.stream(st):
+            with torch.cuda.stream(self._stream(stream, t.device)):
                 if self.fn is not None:
                     self.fn(t)
                 else:
@@ -222,10 +219,108 @@ class Reducer:
             if self.error is None:
                 self.error = exc
 
+    def _stream(self, stream, device):
+        import torch
+
+        key = int(stream or 0)
+        st = self._streams.get(key)
+        if st is None:
+            st = self._streams[key] = torch.cuda.ExternalStream(key, device=device)
+        return st
+
     def check(self):
         if self.error is not None:
             err, self.error = self.error, None
             raise RuntimeError(f"the exchange step failed: {err!r}") from err
+
+
+# fresco_gather_fn: (local address, local count, full address, full count, CUDA stream, context)
+GATHER_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p)
+
+
+class Exchange(Reducer):
+    """A Reducer that also gathers: the library's fresco_gather_fn concatenates the ranks' local arrays
+    in rank order into a full device array.  `gather_fn(local, full)` does it (default: an NCCL
+    all-gather over `group` of arrays padded to the longest, `counts` doubles per rank; a plain copy
+    without a multi-rank group)."""
+
+    def __init__(self, group=None, fn=None, gather_fn=None, counts=None):
+        super().__init__(group, fn)
+        self.gather_fn = gather_fn
+        self.counts = counts
+        self.c_gather = GATHER_FN(self._gather)
+
+    def active(self) -> bool:
+        return super().active() or self.gather_fn is not None
+
+    def _gather(self, lptr, lcount, fptr, fcount, stream, ctx):
+        try:
+            self.calls += 1
+            if self.error is not None:
+                return
+            import torch
+
+            full = torch.as_tensor(_DeviceArray(fptr, fcount), device="cuda")
+            local = torch.as_tensor(_DeviceArray(lptr, lcount), device="cuda") if lcount > 0 else full[:0]
+            with torch.cuda.stream(self._stream(stream, full.device)):
+                if self.gather_fn is not None:
+                    self.gather_fn(local, full)
+                    return
+                dist = _dist(self.group)
+                if dist is None:
+                    full.copy_(local)
+                    return
+                m = max(self.counts)
+                buf = torch.zeros(m, dtype=torch.float64, device=full.device)
+                buf[:lcount].copy_(local)
+                out = torch.empty(m * len(self.counts), dtype=torch.float64, device=full.device)
+                dist.all_gather_into_tensor(out, buf, group=self.group)
+                off = 0
+                for r, c in enumerate(self.counts):
+                    full[off:off + c].copy_(out[r * m:r * m + c])
+                    off += c
+        except BaseException as exc:  # noqa: BLE001 (reported by check())
+            if self.error is None:
+                self.error = exc
+
+
+class ShardedInversePower(BasePotential):
+    """InversePower (fresco/potentials/inversepower_potential.pyx:16-79, cell lists) over one pattern
+    split into index slabs: this rank owns points [lo, hi) of the pattern whose radii `radii_all` are
+    given, and takes its slab's coordinates.  Each evaluation all-gathers the slabs, evaluates the whole
+    pattern's repulsion and keeps this slab's gradient; the energy is the pattern's on every rank.
+    Combines with a ShardedNUwU in a CombinedPotential for ShardedLBFGS.  The slabs of the ranks, in rank
+    order, must tile [0, n_total)."""
+
+    def __init__(self, a, eps, radii_all, boxv, lo, hi, group=None, exchange=None, method=Distance.PERIODIC):
+        self.a, self.eps = float(a), float(eps)
+        self.radii = _f64(radii_all)
+        self.boxv = _f64(boxv)
+        self.ndim = self.boxv.size
+        self.lo, self.hi = int(lo), int(hi)
+        self.N = self.hi - self.lo
+        self.n_total = self.radii.size
+        if exchange is None:
+            exchange = Exchange(group)
+            dist = _dist(group)
+            if dist is not None:
+                slabs = [None] * dist.get_world_size(group)
+                dist.all_gather_object(slabs, (self.lo, self.hi), group=group)
+                ends = [0] + [h for _, h in slabs]
+                if any(l != e for (l, _), e in zip(slabs, ends)) or ends[-1] != self.n_total:
+                    raise ValueError("the ranks' slabs must tile [0, n_total) in rank order")
+                exchange.counts = [(h - l) * self.ndim for l, h in slabs]
+            elif (self.lo, self.hi) != (0, self.n_total):
+                raise ValueError("a slab of a larger pattern needs a multi-rank process group or an exchange")
+        self.exchange = exchange
+        periodic = method == Distance.PERIODIC if isinstance(method, Distance) else \
+            str(getattr(method, "name", method)).upper().endswith("PERIODIC")
+        h = _lib.handle_t()
+        check(lib.fresco_inversepower_shard_create(self.a, self.eps, dptr(self.radii), self.n_total, dptr(self.boxv),
+                                                   self.ndim, int(periodic), self.lo, self.hi,
+                                                   C.cast(exchange.c_gather, C.c_void_p),
+                                                   C.cast(exchange.c_fn, C.c_void_p), None, C.byref(h)))
+        self._set_handle(h)
 
 
 def _enable_reducer(shard, reducer):
@@ -248,16 +343,24 @@ class ShardedLBFGS:
         from .optimize import GradientOptimizer
 
         x = _f64(x_local)
-        if x.size != shard.N * shard.ndim:
-            raise ValueError(f"expected {shard.N * shard.ndim} coordinates, got {x.size}")
+        parts = list(shard._parts) if isinstance(shard, CombinedPotential) else [shard]
+        nuwu = [p for p in parts if isinstance(p, ShardedNUwU)]
+        rep = [p for p in parts if isinstance(p, ShardedInversePower)]
+        if not nuwu and not rep:
+            raise ValueError("ShardedLBFGS expects a ShardedNUwU or a CombinedPotential of sharded potentials")
+        first = (nuwu or rep)[0]
+        if x.size != first.N * first.ndim:
+            raise ValueError(f"expected {first.N * first.ndim} coordinates, got {x.size}")
+        total_ndof = int(first.n_total) * first.ndim
         self.shard = shard
         self.reducer = reducer if reducer is not None else Reducer(group)
         # one process holding the whole pattern has nothing to exchange: no hooks
         hooks = self.reducer.active()
-        if not hooks and shard.n_total != shard.N:
-            raise ValueError("a shard of a larger pattern needs a multi-rank process group or a reducer")
-        if hooks:
-            _enable_reducer(shard, self.reducer)
+        for p in nuwu:
+            if hooks:
+                _enable_reducer(p, self.reducer)
+            elif p.n_total != p.N:
+                raise ValueError("a shard of a larger pattern needs a multi-rank process group or a reducer")
         h = _lib.handle_t()
         check(lib.fresco_lbfgs_create(shard._h, dptr(x), x.size, float(tol), int(M), float(maxstep),
                                       float(maxErise), float(H0), int(bool(rel_energy)), int(nsteps), int(iprint),
@@ -267,14 +370,17 @@ class ShardedLBFGS:
         self._opt._n = x.size
         self._opt.events = [] if events is None else events
         if hooks:
-            check(lib.fresco_optimizer_set_reducer(h, C.cast(self.reducer.c_fn, C.c_void_p), None,
-                                                   int(shard.n_total) * shard.ndim))
+            check(lib.fresco_optimizer_set_reducer(h, C.cast(self.reducer.c_fn, C.c_void_p), None, total_ndof))
 
     def _checked(self, f, *a):
         try:
             return f(*a)
         finally:
             self.reducer.check()
+            parts = list(self.shard._parts) if isinstance(self.shard, CombinedPotential) else [self.shard]
+            for p in parts:
+                if isinstance(p, ShardedInversePower):
+                    p.exchange.check()
 
     def run(self, niter=None):
         return self._checked(self._opt.run, niter)

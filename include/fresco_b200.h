@@ -39,6 +39,11 @@ typedef struct fresco_overlap_s* fresco_overlap;
  * one pattern, in place, ordered on the CUDA stream `stream` (an all-reduce
  * supplied by the caller, e.g. NCCL through torch.distributed). */
 typedef void (*fresco_reduce_fn)(double* data, int64_t count, void* stream, void* ctx);
+/* Concatenates the processes' local arrays (local_count doubles each) in
+ * process order into the device array `full` (full_count doubles), ordered on
+ * `stream` (an all-gather supplied by the caller). */
+typedef void (*fresco_gather_fn)(const double* local, int64_t local_count, double* full, int64_t full_count,
+                                 void* stream, void* ctx);
 typedef struct fresco_window_stats_s* fresco_window_stats;
 
 enum {
@@ -197,6 +202,18 @@ int fresco_export_structure(const double* x, int64_t n_points, int ndim, const d
  * reference counterpart (the reference evaluates a pattern in one process,
  * source/fresco/nuwu.hpp:210-317). */
 int fresco_potential_set_reducer(fresco_potential p, fresco_reduce_fn fn, void* ctx);
+/* InversePower (inversepower_potential.hpp:104-124, cell lists) over a
+ * pattern split into index slabs: this process owns points [lo, hi) of the
+ * n_total whose radii are given, and takes its slab's coordinates.  Each
+ * evaluation gathers all slabs (gather), evaluates the whole pattern's
+ * repulsion and keeps this slab's gradient; the energy is counted by the
+ * process whose slab starts at point 0 and summed by reduce, so every process
+ * holds the pattern's energy.  Combines with a NUwU shard in a
+ * CombinedPotential. */
+int fresco_inversepower_shard_create(double a, double eps, const double* radii_all, int64_t n_total,
+                                     const double* boxv, int ndim, int periodic, int64_t lo, int64_t hi,
+                                     fresco_gather_fn gather, fresco_reduce_fn reduce, void* ctx,
+                                     fresco_potential* out);
 
 /* Sticky status bits raised since the last call (1: non-finite input).
  * Synchronises `stream`.  No reference counterpart (FINUFFT's return codes

@@ -136,3 +136,121 @@ def test_reducer_is_refused_where_there_is_no_exchange():
     fire = ModifiedFireCPP(x, NUwU(radii, 16, Sk, V, L))
     with pytest.raises(ValueError, match="does not run over a sharded pattern"):
         check(lib.fresco_optimizer_set_reducer(fire._h, C.cast(red.c_fn, C.c_void_p), None, x.size))
+
+
+class HostGather:
+    """The all-gather over `n` emulated ranks: local arrays to the host, a barrier, the rank-ordered
+    concatenation back into each rank's full array."""
+
+    def __init__(self, n):
+        self.bar = threading.Barrier(n, timeout=60)
+        self.bufs = [None] * n
+
+    def fn(self, rank):
+        import torch
+
+        def gather(local, full):
+            self.bufs[rank] = local.cpu()
+            self.bar.wait()
+            cat = torch.cat(self.bufs)
+            self.bar.wait()
+            full.copy_(cat)
+
+        return gather
+
+
+def _golden():
+    import os
+
+    d = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "lbfgs_combined_2d.npz")))
+    return d
+
+
+def test_sharded_repulsion_one_process_equals_inversepower():
+    from fresco_b200 import InversePower
+    from fresco_b200.shard import ShardedInversePower
+
+    d = _golden()
+    n = len(d["rep_radii"])
+    sh = ShardedInversePower(2.0, 1.0, d["rep_radii"], d["L"], 0, n)
+    ref = InversePower(2.0, 1.0, d["rep_radii"], d["L"], use_cell_lists=True)
+    e0, g0 = ref.get_energy_gradient(d["x"])
+    e1, g1 = sh.get_energy_gradient(d["x"])
+    assert e0 > 0 and abs(e1 - e0) <= 1e-12 * e0 and rel(g1, g0) < 1e-12
+    assert abs(sh.get_energy(d["x"]) - e0) <= 1e-12 * e0
+    with pytest.raises(ValueError, match="process group or an exchange"):
+        ShardedInversePower(2.0, 1.0, d["rep_radii"], d["L"], 0, n // 2)
+
+
+def test_two_ranks_nuwu_plus_repulsion_match_single_process():
+    """The golden combined pattern (NUwU + cell-list repulsion) over two emulated ranks: ShardedNUwU and
+    ShardedInversePower in one CombinedPotential per rank, ShardedLBFGS; the concatenated trajectory is
+    the single-process LBFGS_CPP one."""
+    from fresco_b200 import CombinedPotential, InversePower, NUwU
+    from fresco_b200.optimize import LBFGS_CPP
+    from fresco_b200.shard import Exchange, Reducer, ShardedInversePower, ShardedLBFGS, ShardedNUwU, weight_factor_sum
+
+    d = _golden()
+    N = len(d["radii"])
+    cut = 100
+    totals = (N, weight_factor_sum(d["radii"], 2))
+    hs, he, hg = HostSum(2), HostSum(2), HostGather(2)
+    opts, keep = [], []
+    for r, (a, b) in enumerate([(0, cut), (cut, N)]):
+        comb = CombinedPotential()
+        nu = ShardedNUwU(d["radii"][a:b], float(d["K"]), d["Sk"], d["V"], d["L"], eps=1e-13, totals=totals)
+        rp = ShardedInversePower(2.0, 1.0, d["rep_radii"], d["L"], a, b,
+                                 exchange=Exchange(fn=he.fn(r), gather_fn=hg.fn(r)))
+        comb.add_potential(nu)
+        comb.add_potential(rp)
+        keep.append((nu, rp))
+        opts.append(ShardedLBFGS(d["x"][2 * a:2 * b], comb, M=10, tol=1e-12, reducer=Reducer(fn=hs.fn(r))))
+    res, errs = [None, None], []
+
+    def drive(r):
+        try:
+            res[r] = opts[r].run(15)
+        except Exception as e:  # noqa: BLE001
+            errs.append(e)
+            for bar in (hs.bar, he.bar, hg.bar):
+                bar.abort()
+
+    threads = [threading.Thread(target=drive, args=(r,)) for r in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=300)
+    assert not errs, errs
+    ref_comb = CombinedPotential()
+    ref_comb.add_potential(NUwU(d["radii"], float(d["K"]), d["Sk"], d["V"], d["L"], eps=1e-13))
+    ref_comb.add_potential(InversePower(2.0, 1.0, d["rep_radii"], d["L"], use_cell_lists=True))
+    ra = LBFGS_CPP(d["x"], ref_comb, M=10, tol=1e-12).run(15)
+    r0, r1 = res
+    assert r0.energy == r1.energy and r0.rms == r1.rms
+    assert r0.nfev == r1.nfev == ra.nfev and r0.nsteps == r1.nsteps == ra.nsteps == 15
+    assert rel(r0.energy, ra.energy) < 1e-8
+    assert rel(np.concatenate([r0.coords, r1.coords]), ra.coords) < 1e-8
+    assert rel(r0.energy, d["traj_energy"][-1]) < 1e-8  # the reference's own golden trajectory
+
+
+def test_graph_optimisers_refuse_exchange_steps():
+    """A potential with a host exchange step is never captured: the graph-captured optimisers refuse it,
+    and a CombinedPotential holding it evaluates without capture (its result stays right)."""
+    from fresco_b200 import CombinedPotential, InversePower
+    from fresco_b200.optimize import LBFGS_Graph, ModifiedFire_Graph
+    from fresco_b200.shard import ShardedInversePower
+
+    d = _golden()
+    n = len(d["rep_radii"])
+    sh = ShardedInversePower(2.0, 1.0, d["rep_radii"], d["L"], 0, n)
+    with pytest.raises(ValueError, match="exchanges between processes"):
+        ModifiedFire_Graph(d["x"], sh).run(3)
+    with pytest.raises(ValueError, match="exchanges between processes"):
+        LBFGS_Graph(d["x"], sh)
+    comb = CombinedPotential()
+    comb.add_potential(sh)
+    ref = InversePower(2.0, 1.0, d["rep_radii"], d["L"], use_cell_lists=True)
+    e0, g0 = ref.get_energy_gradient(d["x"])
+    for _ in range(3):  # repeated calls: the second would capture a graph
+        e1, g1 = comb.get_energy_gradient(d["x"])
+        assert abs(e1 - e0) <= 1e-12 * e0 and rel(g1, g0) < 1e-12
