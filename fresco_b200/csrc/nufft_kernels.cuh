@@ -748,6 +748,106 @@ __global__ void __launch_bounds__(256) spread_kernel(const Rec<D, T>* __restrict
   flush_tile<D, T, CPLX>(tile, g, org0, org1, org2, PAD, grid_real, grid_cplx);
 }
 
+// 3D spreading of real strengths, w <= 8: one warp per point, so that each
+// shared-memory atomic instruction covers a 4-row x 7-column block of one
+// plane of the footprint (two passes of rows per plane, w planes).  The tile's
+// row pitch tw0p is a multiple of 8 but not of 16, which puts the 4 rows of a
+// pass on disjoint bank ranges: every atomic instruction is free of bank
+// conflicts.  Lane l < 3w evaluates tap l % w of axis l / w (its coefficient
+// row is loaded into registers once) and the others read it by shuffle.
+template <int W, typename T>
+__global__ void __launch_bounds__(256) spread3d_warp_kernel(const Rec<3, T>* __restrict__ recs,
+                                                            const T* __restrict__ weights, T uniform,
+                                                            const int* __restrict__ sub_bin,
+                                                            const int* __restrict__ sub_start,
+                                                            const int* __restrict__ sub_count,
+                                                            const int* __restrict__ num_sub, Geom g,
+                                                            const EsPoly<W, T> poly, int tw0p, T* grid_real) {
+  static_assert(W <= 8, "one pass covers 4 rows of at most 8 columns");
+  constexpr int Q = EsPolyDeg<W>::Q;
+  constexpr int PAD = W / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tile = reinterpret_cast<T*>(smem_raw);
+  const int sub = blockIdx.x;
+  if (sub >= *num_sub) return;
+  const int tw0 = g.tw[0], tw1 = g.tw[1], tw2 = g.tw[2];
+  const int plane = tw1 * tw0p;
+  for (int i = threadIdx.x; i < plane * tw2; i += blockDim.x) tile[i] = T(0);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int tdim = lane / W, tm = lane - (lane / W) * W;  // this lane's tap (tdim < 3 for lane < 3W)
+  T cf[Q + 1];
+#pragma unroll
+  for (int d = 0; d <= Q; ++d) {
+    T v = T(0);
+#pragma unroll
+    for (int m = 0; m < W; ++m)
+      if (m == tm) v = poly.c[m][d];
+    cf[d] = v;
+  }
+  const int r_in = lane >> 3, c_in = lane & 7;
+  const bool col_ok = c_in < W && r_in < W, row1_ok = r_in + 4 < W;
+  __syncthreads();
+
+  const int bin = sub_bin[sub];
+  const int start = sub_start[sub], cnt = sub_count[sub];
+  const int bx = bin % g.nb[0];
+  const int brem = bin / g.nb[0];
+  const int by = brem % g.nb[1];
+  const int bz = brem / g.nb[1];
+  const int org0 = bx * g.tile[0], org1 = by * g.tile[1], org2 = bz * g.tile[2];
+  for (int p = warp; p < cnt; p += nw) {
+    const Rec<3, T> rec = recs[start + p];
+    int c0, c1, c2;
+    unpack_cell(3, rec.cell, c0, c1, c2);
+    const T sr = weights ? weights[rec.idx] : uniform;
+    T u0, u1, u2;
+    const int s0 = es_start<W, T>(rec.f[0], u0);
+    const int s1 = es_start<W, T>(rec.f[1], u1);
+    const int s2 = es_start<W, T>(rec.f[2], u2);
+    const T u = tdim == 0 ? u0 : (tdim == 1 ? u1 : u2);
+    T tap = cf[Q];
+#pragma unroll
+    for (int d = Q - 1; d >= 0; --d) tap = fma(tap, u, cf[d]);
+    const T kx = __shfl_sync(0xffffffffu, tap, col_ok ? c_in : 0);
+    const T ky0 = __shfl_sync(0xffffffffu, tap, W + (r_in < W ? r_in : 0));
+    const T ky1 = __shfl_sync(0xffffffffu, tap, W + (row1_ok ? r_in + 4 : 0));
+    const T a0 = sr * kx * ky0, a1 = sr * kx * ky1;
+    const int l0 = c0 - org0 + s0 + PAD, l1 = c1 - org1 + s1 + PAD, l2 = c2 - org2 + s2 + PAD;
+    const int base0 = (l2 * tw1 + l1 + r_in) * tw0p + l0 + c_in;
+#pragma unroll
+    for (int m2 = 0; m2 < W; ++m2) {
+      const T kz = __shfl_sync(0xffffffffu, tap, 2 * W + m2);
+      if (col_ok) {
+        atomicAdd(&tile[base0 + m2 * plane], a0 * kz);
+        if (row1_ok) atomicAdd(&tile[base0 + m2 * plane + 4 * tw0p], a1 * kz);
+      }
+    }
+  }
+  __syncthreads();
+  // flush (flush_tile with the padded pitch)
+  const int o0 = org0 - PAD, o1 = org1 - PAD, o2 = org2 - PAD;
+  const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
+  for (int i = threadIdx.x; i < tw0 * tw1 * tw2; i += blockDim.x) {
+    const int i0 = i % tw0;
+    const int r = i / tw0;
+    const int i1 = r % tw1;
+    const int i2 = r / tw1;
+    const T v = tile[(i2 * tw1 + i1) * tw0p + i0];
+    if (v != T(0)) {
+      const int64_t gi = (int64_t(wrap_index(o2 + i2, nf2)) * nf1 + wrap_index(o1 + i1, nf1)) * nf0 +
+                         wrap_index(o0 + i0, nf0);
+      atomicAdd(grid_real + gi, v);
+    }
+  }
+}
+
+// Row pitch of spread3d_warp_kernel's tile: >= tw0, a multiple of 8, not of 16.
+inline int spread3d_pitch(int tw0) {
+  int p = (tw0 + 7) / 8 * 8;
+  if (p % 16 == 0) p += 8;
+  return p;
+}
+
 // Epilogue shared by the interpolation kernels.
 template <int D, typename T>
 __device__ __forceinline__ void interp_store(int mode, uint32_t o, T wgt, T v0r, T v0i, T v1r, bool bad, double* grad,
@@ -1193,6 +1293,20 @@ template <int D, int W, typename T, bool CPLX>
 void launch_spread_generic(const void* recs, const T* weights, T uniform, const cplx_t<T>* strengths,
                            const SortBufs& sb, const Geom& g, const std::vector<double>& poly, T* grid_real,
                            cplx_t<T>* grid_cplx, cudaStream_t s) {
+  if constexpr (D == 3 && W <= 8 && !CPLX) {
+    const int pitch = spread3d_pitch(g.tw[0]);
+    const size_t smem3 = size_t(pitch) * g.tw[1] * g.tw[2] * sizeof(T);
+    auto k3 = spread3d_warp_kernel<W, T>;
+    if (smem3 <= 200 * 1024) {
+      if (smem3 > 48 * 1024)
+        FB_CUDA(cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem3)));
+      k3<<<unsigned(sb.max_sub), 256, smem3, s>>>(static_cast<const Rec<3, T>*>(recs), weights, uniform,
+                                                 sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g,
+                                                 make_es_poly<W, T>(poly), pitch, grid_real);
+      FB_LAUNCH_CHECK();
+      return;
+    }
+  }
   const size_t smem = size_t(g.tile_cells()) * sizeof(T) * (CPLX ? 2 : 1);
   auto kern = spread_kernel<D, W, T, CPLX>;
   if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
