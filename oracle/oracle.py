@@ -2,7 +2,7 @@
 
 This module is a plain-numpy restatement of the reference's arithmetic, used
 only by ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
-leg as the checker.  Nothing in the product package imports it.
+leg, to check results against.  Nothing in the product package imports it.
 
 Every transform here is an exact FP64 direct sum (a NUDFT), i.e. the quantity
 FINUFFT approximates to tolerance ``eps``.  The glue around the transforms
