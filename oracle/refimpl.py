@@ -2,7 +2,7 @@
 
 The library is the reference's own C++ for the loss-and-gradient path,
 compiled unchanged by ``oracle/Makefile`` against this folder's FINUFFT/FFTW
-API shim.  It pins the numpy restatement (oracle.py) and
+API shim.  It pins the numpy restatement (oracle.py) and is
 the CPU baseline timed by ``bench.py``.  Transforms run either as exact FP64
 direct sums (``set_mode(EXACT)``) or as the CPU ES-kernel NUFFT restatement at
 the plan tolerance (``set_mode(ES)``); FINUFFT itself is not available here.
