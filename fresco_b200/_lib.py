@@ -59,6 +59,7 @@ _SIGNATURES = {
     "fresco_export_structure": (C.c_int, [c_double_p, c_int64, C.c_int, c_double_p, C.c_int, c_double_p, C.c_double,
                                           c_double_p, c_double_p, c_double_p, c_double_p]),
     "fresco_potential_status": (C.c_int, [handle_t, c_void_p, c_int_p]),
+    "fresco_debug_set_tile_wait_polls": (C.c_int, [C.c_int]),
     "fresco_potential_set_reducer": (C.c_int, [handle_t, c_void_p, c_void_p]),
     "fresco_optimizer_state_bytes": (C.c_int, [handle_t, C.POINTER(C.c_int64)]),
     "fresco_optimizer_save_state": (C.c_int, [handle_t, c_void_p]),
@@ -91,6 +92,7 @@ _SIGNATURES = {
                                            C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                            C.c_int, C.c_int, C.POINTER(handle_t)]),
     "fresco_optimizer_set_func_gradient": (C.c_int, [handle_t, C.c_double, c_double_p, c_int64]),
+    "fresco_lbfgs_set_H0": (C.c_int, [handle_t, C.c_double]),
     "fresco_optimizer_run": (C.c_int, [handle_t, C.c_int]),
     "fresco_optimizer_one_iteration": (C.c_int, [handle_t]),
     "fresco_optimizer_reset": (C.c_int, [handle_t, c_double_p, c_int64]),

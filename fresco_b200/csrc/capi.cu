@@ -6,6 +6,7 @@
 
 #include "../../include/fresco_b200.h"
 #include "ensemble.cuh"
+#include "nufft.cuh"
 #include "optimizer.cuh"
 #include "pointstats.cuh"
 #include "potential.cuh"
@@ -346,6 +347,13 @@ int fresco_optimizer_set_reducer(fresco_optimizer o, fresco_reduce_fn fn, void* 
   });
 }
 
+int fresco_debug_set_tile_wait_polls(int polls) {
+  return guarded([&] {
+    fb::set_tile_wait_polls(polls);
+    return FRESCO_OK;
+  });
+}
+
 int fresco_potential_status(fresco_potential p, void* stream, int* status) {
   return guarded([&] {
     if (!p || !status) throw fb::InvalidArgument("null argument");
@@ -483,6 +491,14 @@ int fresco_optimizer_set_func_gradient(fresco_optimizer o, double f, const doubl
   return guarded([&] {
     if (!o || (n > 0 && !grad)) throw fb::InvalidArgument("null argument");
     o->opt->set_func_gradient(f, grad, n);
+    return FRESCO_OK;
+  });
+}
+
+int fresco_lbfgs_set_H0(fresco_optimizer o, double H0) {
+  return guarded([&] {
+    if (!o) throw fb::InvalidArgument("null handle");
+    o->opt->set_H0(H0);
     return FRESCO_OK;
   });
 }

@@ -42,7 +42,9 @@ inline void cufft_check(cufftResult r, const char* what, const char* file, int l
 enum StatusBits : int {
   STATUS_NONFINITE_INPUT = 1,  // a coordinate was NaN or +-inf
   STATUS_OVERFLOW = 2,         // a bounded buffer was too small (kernel skipped the excess)
-  STATUS_TIMEOUT = 4,          // a bounded wait gave up (the kernel skipped that work)
+  STATUS_TIMEOUT = 4,          // a bounded wait gave up: the evaluation's energy and gradient are NaN
+  STATUS_TILE_RETRY = 8,       // a tile copy outlasted its first bounded wait and was waited for again
+                               // (informational: the results are complete)
 };
 
 // A potential's status block holds two words: [0] the flags of the current

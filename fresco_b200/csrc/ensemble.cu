@@ -264,6 +264,8 @@ struct EnsTileMap {
   // tiles are read with plain loads (one grid per pattern)
   __device__ __forceinline__ const CUtensorMap* tile_tmap() const { return nullptr; }
   __device__ __forceinline__ int* err_status() const { return nullptr; }
+  __device__ __forceinline__ int wait_polls() const { return 0; }
+  __device__ __forceinline__ double* fail_energy() const { return nullptr; }
 };
 
 // Direct spreading for sparse patterns: thread per sorted point, the w x w

@@ -7,6 +7,13 @@
 
 namespace fb {
 
+int& tile_wait_polls_setting() {
+  static int polls = kTileWaitPolls;
+  return polls;
+}
+
+void set_tile_wait_polls(int polls) { tile_wait_polls_setting() = polls >= 0 ? polls : kTileWaitPolls; }
+
 int sm_count() {
   static int cache[16] = {0};
   int dev = 0;

@@ -129,9 +129,20 @@ struct GradScale {
 };
 
 // Interpolates `nfields` complex fine grids (field stride G) at the sorted points.
+// fail_energy (may be null): the evaluation's energy, set to NaN if a tile
+// copy of the 2D kernel never completes (STATUS_TIMEOUT).
 template <typename T>
 void interp(const void* recs, int64_t N, const T* weights, T uniform, const SortBufs& sb, const Geom& g,
             const std::vector<double>& poly, const cplx_t<T>* fields, int nfields, int mode, double* grad,
-            double2* out2, int accumulate, const int* status, cudaStream_t s, GradScale gs = GradScale());
+            double2* out2, int accumulate, const int* status, cudaStream_t s, GradScale gs = GradScale(),
+            double* fail_energy = nullptr);
+
+// Mbarrier polls of the first wait for an interpolation tile copy, used by
+// launches from now on (< 0 restores the default, kTileWaitPolls; 0 makes
+// the first wait run out at once).  Tests lower it to exercise the second,
+// time-bounded wait.
+constexpr int kTileWaitPolls = 1 << 22;
+void set_tile_wait_polls(int polls);
+int& tile_wait_polls_setting();
 
 }  // namespace fb

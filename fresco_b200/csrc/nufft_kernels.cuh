@@ -423,11 +423,15 @@ struct TileMap1 {
   const int* __restrict__ status;  // evaluation status word (interpolation), may be null
   T uniform;
   int has_tmap = 0;  // interpolation: tmap describes the interpolated fine grid
+  int polls = 0;     // first bounded wait for a tile copy (mbarrier polls)
+  double* energy = nullptr;  // the evaluation's energy, made NaN if a tile copy never lands (may be null)
   CUtensorMap tmap;
   // tensor map of the fine grid for tile copies (the kernel parameter must be
   // __grid_constant__ for its address to be usable), or null
   __device__ __forceinline__ const CUtensorMap* tile_tmap() const { return has_tmap ? &tmap : nullptr; }
   __device__ __forceinline__ int* err_status() const { return const_cast<int*>(status); }
+  __device__ __forceinline__ int wait_polls() const { return polls; }
+  __device__ __forceinline__ double* fail_energy() const { return energy; }
   __device__ __forceinline__ bool fetch(const Geom& g, TileWork<T>& w) const {
     const int sub = blockIdx.x;
     if (sub >= *num_sub) return false;
@@ -888,8 +892,10 @@ __host__ __device__ constexpr size_t interp2d_smem_bytes() {
 // Points per thread of a 2D tile block (256 threads, at most kMaxSub points).
 constexpr int kTilePtsPerThread = (kMaxSub + 255) / 256;
 
-// Bounded polls of the tile copy's mbarrier before a block gives up.
-constexpr int kTileWaitPolls = 1 << 22;
+// A block whose first bounded wait for its tile copy (tile_wait_polls_setting()
+// mbarrier polls) runs out waits again, bounded by kTileWaitNs of the global
+// timer, before it fails the evaluation.
+constexpr uint64_t kTileWaitNs = 2000000000ull;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -912,11 +918,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
       : "memory");
   return done != 0;
 }
-// Waits for phase `parity` of the barrier for at most kTileWaitPolls polls.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
-  for (int i = 0; i < kTileWaitPolls; ++i)
+// Waits for phase `parity` of the barrier for at most `polls` polls (none when
+// polls is 0: the wait runs out at once).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, int polls) {
+  for (int i = 0; i < polls; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for phase `parity` of the barrier for at most `ns` nanoseconds.
+__device__ __forceinline__ bool mbar_wait_timed(uint64_t* bar, unsigned parity, uint64_t ns) {
+  const uint64_t t0 = global_ns();
+  do {
+    if (mbar_try_wait(bar, parity)) return true;
+  } while (global_ns() - t0 < ns);
+  return mbar_try_wait(bar, parity);
 }
 // 2D tensor copy global -> shared (x innermost, in elements of the map),
 // completing on `bar` with its byte count.
@@ -1017,16 +1037,29 @@ __global__ void __launch_bounds__(256) interp2d_tile_kernel(const Rec<2, T>* __r
     }
   }
   if (use_tma) {
-    // every thread sees the copy complete (bounded); a block that gives up
-    // flags the evaluation, waits once more for its copy and skips its points
-    const bool ok = mbar_wait_bounded(&tile_bar, 0);
+    // Every thread polls the copy's barrier, bounded.  If any thread's polls
+    // run out, the block records STATUS_TILE_RETRY and every thread waits
+    // again, bounded by time; the copy normally lands then and the block goes
+    // on with a complete tile.  A copy that has still not landed fails the
+    // evaluation: STATUS_TIMEOUT, a NaN energy and NaN results for the
+    // block's points.  The block then returns with its copy possibly in
+    // flight, so once STATUS_TIMEOUT is raised no result of the evaluation is
+    // to be trusted, which the NaN energy makes visible to every caller.
+    const bool ok = mbar_wait_bounded(&tile_bar, 0, map.wait_polls());
     if (__syncthreads_or(!ok)) {
-      if (tid == 0) {
-        if (int* st = map.err_status()) raise_status(st, STATUS_TIMEOUT);
-        mbar_wait_bounded(&tile_bar, 0);
+      if (tid == 0)
+        if (int* st = map.err_status()) raise_status(st, STATUS_TILE_RETRY);
+      const bool ok2 = mbar_wait_timed(&tile_bar, 0, kTileWaitNs);
+      if (__syncthreads_or(!ok2)) {
+        const T nan = T(__longlong_as_double(0x7ff8000000000000ULL));
+        if (tid == 0) {
+          if (int* st = map.err_status()) raise_status(st, STATUS_TIMEOUT);
+          if (double* e = map.fail_energy()) *e = double(nan);
+        }
+        for (int p = tid; p < cnt; p += blockDim.x)
+          interp_store<2, T>(mode, recs[start + p].idx, T(1), nan, nan, nan, true, grad, out2, accumulate, gs);
+        return;
       }
-      __syncthreads();
-      return;
     }
   }
   __syncthreads();
@@ -1352,11 +1385,13 @@ int encode_tile_tmap(CUtensorMap* tm, const void* grid, int64_t nf0, int64_t nf1
 template <int W, typename T>
 void launch_interp2d(const void* recs, const T* weights, T uniform, const SortBufs& sb, const Geom& g,
                      const std::vector<double>& poly, const cplx_t<T>* field, int mode, double* grad, double2* out2,
-                     int acc, const int* status, cudaStream_t s, const GradScale& gs) {
+                     int acc, const int* status, cudaStream_t s, const GradScale& gs, double* fail_energy) {
   constexpr size_t smem = interp2d_smem_bytes<W, T>();
   auto kern = interp2d_tile_kernel<W, T, TileMap1<T>>;
   if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   TileMap1<T> map{sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, sb.bin_start.p, status, uniform};
+  map.polls = tile_wait_polls_setting();
+  map.energy = fail_energy;
   map.has_tmap = encode_tile_tmap<T>(&map.tmap, field, g.nf[0], g.nf[1], 2 * Interp2D<W>::TWX, Interp2D<W>::TWY);
   kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<2, T>*>(recs), weights, map, g,
                                                 make_es_poly<W, T>(poly), field, mode, grad, out2, acc, gs);
@@ -1473,11 +1508,11 @@ void spread_cplx(const void* recs, const cplx_t<T>* strengths, const SortBufs& s
 template <typename T>
 void interp(const void* recs, int64_t N, const T* weights, T uniform, const SortBufs& sb, const Geom& g,
             const std::vector<double>& poly, const cplx_t<T>* fields, int nfields, int mode, double* grad,
-            double2* out2, int accumulate, const int* status, cudaStream_t s, GradScale gs) {
+            double2* out2, int accumulate, const int* status, cudaStream_t s, GradScale gs, double* fail_energy) {
   if (g.D == 2 && nfields == 1) {
 #define FB_I2(WW)                                                                                                  \
   launch_interp2d<FB_WCLAMP(T, WW), T>(recs, weights, uniform, sb, g, poly, fields, mode, grad, out2, accumulate, \
-                                       status, s, gs)
+                                       status, s, gs, fail_energy)
     FB_FOR_W(T, FB_I2)
 #undef FB_I2
   } else if (g.D == 1) {
@@ -1512,6 +1547,7 @@ void interp(const void* recs, int64_t N, const T* weights, T uniform, const Sort
   template void spread_cplx<T>(const void*, const cplx_t<T>*, const SortBufs&, const Geom&,                         \
                                const std::vector<double>&, cplx_t<T>*, cudaStream_t);                                \
   template void interp<T>(const void*, int64_t, const T*, T, const SortBufs&, const Geom&, const std::vector<double>&, \
-                          const cplx_t<T>*, int, int, double*, double2*, int, const int*, cudaStream_t, GradScale);
+                          const cplx_t<T>*, int, int, double*, double2*, int, const int*, cudaStream_t, GradScale, \
+                          double*);
 
 }  // namespace fb

@@ -16,9 +16,12 @@
 // reductions; the adjoint is one thread per point with the frequencies
 // staged in shared memory.  The `precision` argument is accepted; the
 // arithmetic is FP64 either way.
+#include <cuda.h>
+
 #include <cmath>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "potential.cuh"
@@ -43,54 +46,58 @@ __global__ void __launch_bounds__(kThreads) nuwnu_forward_kernel(const double* _
                                                                   const double* __restrict__ c, double cu,
                                                                   double L0, double L1, double L2, double2* rho,
                                                                   int* status) {
-  const int64_t k0 = int64_t(blockIdx.y) * kFreqChunk;
-  double sk[kFreqChunk][D];
-#pragma unroll
-  for (int q = 0; q < kFreqChunk; ++q)
-#pragma unroll
-    for (int a = 0; a < D; ++a) sk[q][a] = (k0 + q < M) ? s[(k0 + q) * D + a] : 0.0;
-  double re[kFreqChunk], im[kFreqChunk];
-#pragma unroll
-  for (int q = 0; q < kFreqChunk; ++q) re[q] = im[q] = 0.0;
-  const double Ls[3] = {L0, L1, L2};
+  // frequency chunks k0 = blockIdx.y * kFreqChunk + gridDim.y * kFreqChunk * t
+  // (gridDim.y is capped at the launch limit, 65535)
+  __shared__ double red[2 * kFreqChunk][kThreads / 32];
   bool bad = false;
-  for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < N; j += int64_t(gridDim.x) * blockDim.x) {
-    double x[D];
+  for (int64_t k0 = int64_t(blockIdx.y) * kFreqChunk; k0 < M; k0 += int64_t(gridDim.y) * kFreqChunk) {
+    double sk[kFreqChunk][D];
 #pragma unroll
-    for (int a = 0; a < D; ++a) {
-      x[a] = nuwnu_coord(pts, j, a, D, Ls[a]);
-      bad |= !isfinite(x[a]);
+    for (int q = 0; q < kFreqChunk; ++q)
+#pragma unroll
+      for (int a = 0; a < D; ++a) sk[q][a] = (k0 + q < M) ? s[(k0 + q) * D + a] : 0.0;
+    double re[kFreqChunk], im[kFreqChunk];
+#pragma unroll
+    for (int q = 0; q < kFreqChunk; ++q) re[q] = im[q] = 0.0;
+    const double Ls[3] = {L0, L1, L2};
+    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < N; j += int64_t(gridDim.x) * blockDim.x) {
+      double x[D];
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        x[a] = nuwnu_coord(pts, j, a, D, Ls[a]);
+        bad |= !isfinite(x[a]);
+      }
+      const double cj = c ? c[j] : cu;
+#pragma unroll
+      for (int q = 0; q < kFreqChunk; ++q) {
+        double ph = 0.0;
+#pragma unroll
+        for (int a = 0; a < D; ++a) ph += sk[q][a] * x[a];
+        double sn, cs;
+        sincos(ph, &sn, &cs);
+        re[q] += cj * cs;
+        im[q] += cj * sn;
+      }
     }
-    const double cj = c ? c[j] : cu;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();  // the previous chunk's partial sums have been read
 #pragma unroll
     for (int q = 0; q < kFreqChunk; ++q) {
-      double ph = 0.0;
-#pragma unroll
-      for (int a = 0; a < D; ++a) ph += sk[q][a] * x[a];
-      double sn, cs;
-      sincos(ph, &sn, &cs);
-      re[q] += cj * cs;
-      im[q] += cj * sn;
+      const double a = warp_sum(re[q]), b = warp_sum(im[q]);
+      if (lane == 0) {
+        red[2 * q][wid] = a;
+        red[2 * q + 1][wid] = b;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * kFreqChunk) {
+      double t = 0.0;
+      for (int w = 0; w < int(blockDim.x) / 32; ++w) t += red[threadIdx.x][w];
+      const int q = threadIdx.x / 2;
+      if (k0 + q < M) atomicAdd((threadIdx.x & 1) ? &rho[k0 + q].y : &rho[k0 + q].x, t);
     }
   }
   if (bad && blockIdx.y == 0) raise_status(status, STATUS_NONFINITE_INPUT);
-  __shared__ double red[2 * kFreqChunk][kThreads / 32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int q = 0; q < kFreqChunk; ++q) {
-    const double a = warp_sum(re[q]), b = warp_sum(im[q]);
-    if (lane == 0) {
-      red[2 * q][wid] = a;
-      red[2 * q + 1][wid] = b;
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < 2 * kFreqChunk) {
-    double t = 0.0;
-    for (int w = 0; w < int(blockDim.x) / 32; ++w) t += red[threadIdx.x][w];
-    const int q = threadIdx.x / 2;
-    if (k0 + q < M) atomicAdd((threadIdx.x & 1) ? &rho[k0 + q].y : &rho[k0 + q].x, t);
-  }
 }
 
 __global__ void __launch_bounds__(kThreads) nuwnu_loss_kernel(const double2* __restrict__ rho, int64_t M, double invN,
@@ -237,7 +244,7 @@ class NUwNUImpl final : public Potential {
     }
     FB_CUDA(cudaMemsetAsync(rho_.p, 0, sizeof(double2) * M_, s));
     const int pblocks = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(N_, kThreads), 2 * int64_t(sm_count()))));
-    dim3 fg(pblocks, unsigned(ceil_div(M_, kFreqChunk)));
+    dim3 fg(pblocks, unsigned(std::min<int64_t>(ceil_div(M_, kFreqChunk), 65535)));
     nuwnu_forward_kernel<D><<<fg, kThreads, 0, s>>>(x, N_, s_.p, M_, c_.p, cu_, L_[0], L_[1], L_[2], rho_.p,
                                                     status_.p);
     FB_LAUNCH_CHECK();
@@ -279,27 +286,64 @@ namespace {
 
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mutex;
-double2* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+struct NoAllocSlot {
+  unsigned long long ctx_id = 0;  // CUDA context the address belongs to (0: none yet)
+  double2* ptr = nullptr;
+};
+NoAllocSlot g_noalloc_slot[kNoAllocMaxDevices];
 
-// Device address of the scratch array on the current device.  The first call
-// on a device looks it up (cudaGetSymbolAddress, which may load the library's
-// device code onto that device); later calls reuse the cached address.
+// Unique id of the calling thread's current CUDA context (cuCtxGetCurrent,
+// cuCtxGetId from the driver), or 0 when the driver offers no id.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static const std::pair<GetCurrent, GetId> fns = [] {
+    void* a = nullptr;
+    void* b = nullptr;
+    cudaDriverEntryPointQueryResult qa, qb;
+    const bool ok = cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) == cudaSuccess &&
+                    qa == cudaDriverEntryPointSuccess &&
+                    cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) == cudaSuccess &&
+                    qb == cudaDriverEntryPointSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      return std::pair<GetCurrent, GetId>(nullptr, nullptr);
+    }
+    return std::pair<GetCurrent, GetId>(reinterpret_cast<GetCurrent>(a), reinterpret_cast<GetId>(b));
+  }();
+  if (!fns.first) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (fns.first(&ctx) != CUDA_SUCCESS || !ctx || fns.second(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of the scratch array in the current device's context.  The
+// first call in a context looks it up (cudaGetSymbolAddress, which may load
+// the library's device code into that context); later calls in the same
+// context reuse the cached address.  A new context on the device (after
+// cudaDeviceReset, or a caller that makes another context current) gets its
+// own lookup, so a cached address is never used outside the context it
+// belongs to.
 double2* noalloc_scratch_on_current_device() {
   int dev = -1;
   FB_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kNoAllocMaxDevices)
     throw std::runtime_error("device index " + std::to_string(dev) + " is beyond the " +
                              std::to_string(kNoAllocMaxDevices) + " devices the allocation-free entry point supports");
+  const unsigned long long ctx = current_context_id();  // 0 before the runtime has made a context current
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
+  NoAllocSlot& slot = g_noalloc_slot[dev];
+  if (!slot.ptr || ctx == 0 || slot.ctx_id != ctx) {
     void* ptr = nullptr;
     const cudaError_t rc = cudaGetSymbolAddress(&ptr, g_nuwnu_noalloc_scratch);
     if (rc != cudaSuccess || !ptr)
       throw std::runtime_error(std::string("cudaGetSymbolAddress of the NUwNU scratch array failed: ") +
                                cudaGetErrorString(rc));
-    g_noalloc_ptr[dev] = static_cast<double2*>(ptr);
+    slot.ptr = static_cast<double2*>(ptr);
+    slot.ctx_id = current_context_id();  // the lookup made the device's context current
   }
-  return g_noalloc_ptr[dev];
+  return slot.ptr;
 }
 
 template <int D>

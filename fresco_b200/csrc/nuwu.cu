@@ -251,7 +251,7 @@ class NUwUImpl final : public Potential, public NUwUShard {
           g != nullptr);
       FB_LAUNCH_CHECK();
     }
-    if (g) type2_and_interp(g, acc, s);
+    if (g) type2_and_interp(g, e, acc, s);
   }
 
   std::string describe() const override {
@@ -295,7 +295,7 @@ class NUwUImpl final : public Potential, public NUwUShard {
   }
 
   // type-2 transform of the packed field and interpolation at the points
-  void type2_and_interp(double* g, bool acc, cudaStream_t s) {
+  void type2_and_interp(double* g, double* e, bool acc, cudaStream_t s) {
     if (pruned_) {
       const int off = geom_.nf[0] - kx_max_;
       exec_c2c(plan_col2a_, hgrid_.p, tgrid_.p, s);
@@ -308,7 +308,7 @@ class NUwUImpl final : public Potential, public NUwUShard {
     if (grad_mode_ == 1)
       for (int a = 0; a < D; ++a) gs.s[a] = 2.0 * M_PI / L_[a];
     interp<T>(recs_.p, N_, cw_.p, uniform_c_, sort_, geom_, poly_, ggrid_.p, nfields_, INTERP_GRAD, g, nullptr,
-              acc ? 1 : 0, status_.p, s, gs);
+              acc ? 1 : 0, status_.p, s, gs, e);
   }
 
   bool host_steps() const override { return sharded_ && reducer_ != nullptr; }
@@ -389,7 +389,7 @@ class NUwUImpl final : public Potential, public NUwUShard {
     if (grad_mode_ == 1)
       for (int a = 0; a < D; ++a) gs.s[a] = 2.0 * M_PI / L_[a];
     interp<T>(recs_.p, N_, cw_.p, uniform_c_, sort_, geom_, poly_, ggrid_.p, nfields_, INTERP_GRAD, g, nullptr,
-              acc ? 1 : 0, status_.p, s, gs);
+              acc ? 1 : 0, status_.p, s, gs, e);
     timer_mark("interp", s);
   }
 
@@ -482,7 +482,7 @@ class NUwUImpl final : public Potential, public NUwUShard {
     if (grad_mode_ == 1)
       for (int a = 0; a < D; ++a) gs.s[a] = 2.0 * M_PI / L_[a];
     interp<T>(recs_.p, N_, cw_.p, uniform_c_, sort_, geom_, poly_, ggrid_.p, nfields_, INTERP_GRAD, g, nullptr,
-              acc ? 1 : 0, status_.p, s, gs);
+              acc ? 1 : 0, status_.p, s, gs, e);
     timer_mark("interp", s);
   }
 

@@ -246,6 +246,8 @@ __global__ void lb_init_fin(LbState* st, const double* __restrict__ e, double in
   out[3] = st->H0;
 }
 
+__global__ void lb_set_h0(LbState* st, double h0) { st->H0 = h0; }
+
 __global__ void lb_set_scalars(LbState* st, double f, double rms, int reset_k, int set_h0, double h0) {
   st->f = f;
   st->rms = rms;
@@ -486,6 +488,17 @@ class Lbfgs final : public Optimizer {
   double* device_x() override { return X_[cur_].p; }
   double* device_g() override { return G_[cur_].p; }
   double h0() const override { return h0_; }
+
+  // lbfgs.hpp:70-76: allowed at any time; after the first iteration with the
+  // reference's warning.  The next step's scale is H0 until the next memory
+  // update replaces it with y.s / y.y (lbfgs.cpp:101).
+  void set_H0(double H0) override {
+    if (iter_ > 0) std::printf("warning: setting H0 after the first iteration.\n");
+    lb_set_h0<<<1, 1, 0, s_>>>(st_.p, H0);
+    FB_LAUNCH_CHECK();
+    FB_CUDA(cudaStreamSynchronize(s_));
+    h0_ = H0;
+  }
 
   void set_reducer(ReduceFn fn, void* ctx, int64_t global_ndof) override {
     if (global_ndof < n_) throw InvalidArgument("the global coordinate count is below this process's");

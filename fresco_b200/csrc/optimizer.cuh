@@ -59,6 +59,11 @@ class Optimizer {
   virtual double* device_x() = 0;
   virtual double* device_g() = 0;
   virtual double h0() const { return 0.0; }
+  // LBFGS::set_H0 (source/fresco/lbfgs.hpp:70-76); other optimisers have no H0
+  virtual void set_H0(double H0) {
+    (void)H0;
+    throw InvalidArgument("set_H0: only LBFGS has an initial inverse-Hessian scale");
+  }
   // One pattern split over processes (each holds a slab of x): every dot
   // product's block partials are summed over the processes by fn before they
   // are used, and the rms is taken over global_ndof coordinates.

@@ -206,7 +206,8 @@ class LBFGS_CPP(GradientOptimizer):
         self.events = [] if events is None else events
 
     def set_H0(self, H0):
-        raise NotImplementedError("set_H0 after construction is not supported; pass H0= to the constructor")
+        """LBFGS::set_H0 (fresco/optimize/_lbfgs_cpp.pyx:72-74): the inverse-Hessian scale of the next step."""
+        check(lib.fresco_lbfgs_set_H0(self._h, float(H0)))
 
     def get_result(self):
         res = super().get_result()

@@ -177,9 +177,11 @@ int fresco_potential_energy_gradient_device(fresco_potential p, const double* d_
  * library holds on every GPU it is loaded on until the process exits, so
  * n_k may not exceed 4096 (FRESCO_ERR_INVALID beyond that).  All calls share
  * that array: calls whose work overlaps on the GPU (two streams, or two host
- * threads on one device) race and give undefined results.  The first call on
- * a device looks up the array's device address (and may load the library's
- * device code there); make that first call before any stream capture begins.
+ * threads on one device) race and give undefined results.  The first call in
+ * a device's CUDA context looks up the array's device address (and may load
+ * the library's device code there); make that first call before any stream
+ * capture begins.  The address is cached per context: after cudaDeviceReset,
+ * or with another context current, the next call looks it up again.
  * Works on the current device and enqueues on `stream` without waiting.  A
  * non-finite coordinate makes the energy and the gradient NaN. */
 int fresco_nuwnu_energy_gradient_noalloc(const double* d_x, int64_t n_points, int ndim, const double* d_weights,
@@ -215,10 +217,21 @@ int fresco_inversepower_shard_create(double a, double eps, const double* radii_a
                                      fresco_gather_fn gather, fresco_reduce_fn reduce, void* ctx,
                                      fresco_potential* out);
 
-/* Sticky status bits raised since the last call (1: non-finite input).
- * Synchronises `stream`.  No reference counterpart (FINUFFT's return codes
- * are ignored at source/fresco/nuwu.hpp:191-192, 256-258). */
+/* Sticky status bits raised since the last call: 1 non-finite input, 2 a
+ * bounded buffer overflowed, 4 a bounded wait gave up (the evaluation's
+ * energy and gradient are then NaN), 8 an interpolation tile copy outlasted
+ * its first bounded wait and was waited for again (the results are
+ * complete).  Synchronises `stream`.  No reference counterpart (FINUFFT's
+ * return codes are ignored at source/fresco/nuwu.hpp:191-192, 256-258). */
 int fresco_potential_status(fresco_potential p, void* stream, int* status);
+
+/* Mbarrier polls of the first bounded wait for a 2D interpolation tile copy,
+ * for kernels launched (or graphs captured) from now on, process-wide; polls
+ * < 0 restores the default (1 << 22), 0 makes the first wait run out at once.
+ * A block whose polls run out raises status bit 8 and waits again, bounded by
+ * two seconds, so 0 exercises that second wait without changing any result.
+ * A diagnostic with no reference counterpart. */
+int fresco_debug_set_tile_wait_polls(int polls);
 
 /* Gradient convention of the handle: 0 (default) returns the reference's own
  * gradient formula (drop-in parity); 1 returns the exact derivative of the
@@ -274,6 +287,12 @@ int fresco_fire_graph_create(fresco_potential p, const double* x0, int64_t n, do
 int fresco_optimizer_set_reducer(fresco_optimizer o, fresco_reduce_fn fn, void* ctx, int64_t global_ndof);
 /* GradientOptimizer::set_func_gradient(f, grad)  (source/fresco/optimizer.hpp:127-144). */
 int fresco_optimizer_set_func_gradient(fresco_optimizer o, double f, const double* grad, int64_t n);
+/* LBFGS::set_H0(H0)  (source/fresco/lbfgs.hpp:70-76; fresco/optimize/_lbfgs_cpp.pyx:72-74): the
+ * initial inverse-Hessian scale used by the next step, until the next memory
+ * update replaces it (lbfgs.cpp:101).  Prints the reference's warning when
+ * called after the first iteration.  LBFGS handles only (FRESCO_ERR_INVALID
+ * otherwise). */
+int fresco_lbfgs_set_H0(fresco_optimizer o, double H0);
 /* GradientOptimizer::run(niter) / run()  (optimizer.hpp:97-121); niter < 0 runs to maxiter. */
 int fresco_optimizer_run(fresco_optimizer o, int niter);
 /* one_iteration()  (lbfgs.cpp:36-64, modified_fire.hpp:160-230). */

@@ -82,6 +82,11 @@ void* ref_fire_create(void* pot, const double* x0, int64_t n, double dtstart, do
   return new RefOpt{std::shared_ptr<fresco::GradientOptimizer>(f), false};
 }
 
+void ref_lbfgs_set_H0(void* o, double H0) {
+  auto* r = static_cast<RefOpt*>(o);
+  if (r->lbfgs) static_cast<fresco::LBFGS*>(r->o.get())->set_H0(H0);
+}
+
 void ref_opt_run(void* o, int niter) { static_cast<RefOpt*>(o)->o->run(niter); }
 void ref_opt_one_iteration(void* o) { static_cast<RefOpt*>(o)->o->one_iteration(); }
 

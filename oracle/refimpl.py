@@ -36,6 +36,7 @@ def lib():
         L = C.CDLL(str(LIB_PATH))
         sig = {
             "fresco_shim_set_mode": (None, [C.c_int]),
+            "fresco_shim_profile": (None, [_dp, C.c_int]),
             "fresco_shim_get_mode": (C.c_int, []),
             "ref_set_threads": (None, [C.c_int]),
             "ref_get_threads": (C.c_int, []),
@@ -56,6 +57,7 @@ def lib():
             "ref_fire_create": (C.c_void_p, [C.c_void_p, _dp, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_int,
                                              C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                                              C.c_int]),
+            "ref_lbfgs_set_H0": (None, [C.c_void_p, C.c_double]),
             "ref_opt_run": (None, [C.c_void_p, C.c_int]),
             "ref_opt_one_iteration": (None, [C.c_void_p]),
             "ref_opt_state": (None, [C.c_void_p, _dp, _dp, _dp, _dp, _ip, _ip, _dp]),
@@ -79,6 +81,13 @@ def lib():
 
 def set_mode(mode: int) -> None:
     lib().fresco_shim_set_mode(int(mode))
+
+
+def shim_profile(reset: bool = True) -> dict:
+    """Seconds spent per stage of the ES-kernel NUFFT since the last reset."""
+    out = (C.c_double * 5)()
+    lib().fresco_shim_profile(out, int(bool(reset)))
+    return dict(zip(("setpts", "spread", "fft", "modes", "interp"), list(out)))
 
 
 def set_threads(n: int) -> None:
@@ -209,6 +218,9 @@ class LBFGS(_RefOpt):
         self.n = x.size
         self.pot = pot
         self._h = lib().ref_lbfgs_create(pot._h, xp, x.size, tol, M, maxstep, maxErise, H0, int(rel_energy), nsteps)
+
+    def set_H0(self, H0):
+        lib().ref_lbfgs_set_H0(self._h, float(H0))
 
 
 class ModifiedFire(_RefOpt):

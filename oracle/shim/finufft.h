@@ -33,6 +33,8 @@ int finufft_destroy(finufft_plan plan);
 /* Oracle controls (not part of FINUFFT): 0 = auto, 1 = exact direct sums,
  * 2 = ES-kernel NUFFT at the plan tolerance. */
 extern "C" void fresco_shim_set_mode(int mode);
+// Per-stage seconds of the ES NUFFT (setpts, spread, FFT, modes, interpolation); reset != 0 clears them.
+extern "C" void fresco_shim_profile(double* out, int reset);
 extern "C" int fresco_shim_get_mode(void);
 
 #endif

@@ -32,6 +32,17 @@ constexpr double kPi = 3.14159265358979323846;
 
 int g_mode = 0;  // 0 auto, 1 exact, 2 ES
 
+// Wall seconds spent per ES stage since the last reset: setpts (coordinate
+// map and bin sort), spread, FFT, mode copy with correction, interpolation.
+enum { kProfSetpts, kProfSpread, kProfFft, kProfModes, kProfInterp, kProfN };
+double g_prof[kProfN] = {0, 0, 0, 0, 0};
+struct ProfScope {
+  int slot;
+  double t0;
+  explicit ProfScope(int s) : slot(s), t0(omp_get_wtime()) {}
+  ~ProfScope() { g_prof[slot] += omp_get_wtime() - t0; }
+};
+
 // ---------------------------------------------------------------------------
 // mixed-radix FFT
 // ---------------------------------------------------------------------------
@@ -61,8 +72,11 @@ struct Fft1 {
     if (r > 1) fac.push_back(r);
   }
 
-  // In-place transform of a contiguous array; work holds n elements.
-  void exec(cd* x, cd* work) const {
+  // In-place transforms of B interleaved lines (element j of line b at
+  // x[j B + b]); work holds n B elements.  Interleaving scales every index
+  // stride of the recursion by B while the twiddles stay those of one line,
+  // so the innermost loops run over s B contiguous elements.
+  void exec(cd* x, cd* work, int B = 1) const {
     cd* a = x;
     cd* b = work;
     long s = 1, L = n;
@@ -71,48 +85,49 @@ struct Fft1 {
     std::vector<cd> gen;
     for (int p : fac) {
       const long m = L / p;
+      const long sb = s * B;
       if (p > 4 && p != 3 && int(gen.size()) < p) gen.resize(2 * p);
       for (long j1 = 0; j1 < m; ++j1) {
-        const cd* in = a + j1 * s;
-        cd* out = b + j1 * s * p;
+        const cd* in = a + j1 * sb;
+        cd* out = b + j1 * sb * p;
         if (p == 4) {
           const cd w1 = tw[size_t(j1 * s)], w2 = tw[size_t(2 * j1 * s)], w3 = tw[size_t(3 * j1 * s)];
-          for (long q = 0; q < s; ++q) {
-            const cd u0 = in[q], u1 = in[m * s + q], u2 = in[2 * m * s + q], u3 = in[3 * m * s + q];
+          for (long q = 0; q < sb; ++q) {
+            const cd u0 = in[q], u1 = in[m * sb + q], u2 = in[2 * m * sb + q], u3 = in[3 * m * sb + q];
             const cd t0 = u0 + u2, t1 = u0 - u2, t2 = u1 + u3, t3 = (u1 - u3) * wi;
             out[q] = t0 + t2;
-            out[s + q] = (t1 + t3) * w1;
-            out[2 * s + q] = (t0 - t2) * w2;
-            out[3 * s + q] = (t1 - t3) * w3;
+            out[sb + q] = (t1 + t3) * w1;
+            out[2 * sb + q] = (t0 - t2) * w2;
+            out[3 * sb + q] = (t1 - t3) * w3;
           }
         } else if (p == 2) {
           const cd w1 = tw[size_t(j1 * s)];
-          for (long q = 0; q < s; ++q) {
-            const cd u0 = in[q], u1 = in[m * s + q];
+          for (long q = 0; q < sb; ++q) {
+            const cd u0 = in[q], u1 = in[m * sb + q];
             out[q] = u0 + u1;
-            out[s + q] = (u0 - u1) * w1;
+            out[sb + q] = (u0 - u1) * w1;
           }
         } else if (p == 3) {
           const cd w1 = tw[size_t(j1 * s)], w2 = tw[size_t(2 * j1 * s)];
-          for (long q = 0; q < s; ++q) {
-            const cd u0 = in[q], u1 = in[m * s + q], u2 = in[2 * m * s + q];
+          for (long q = 0; q < sb; ++q) {
+            const cd u0 = in[q], u1 = in[m * sb + q], u2 = in[2 * m * sb + q];
             const cd t1 = u1 + u2, t2 = u0 - 0.5 * t1, t3 = (u1 - u2) * cd(0.0, s3);
             out[q] = u0 + t1;
-            out[s + q] = (t2 + t3) * w1;
-            out[2 * s + q] = (t2 - t3) * w2;
+            out[sb + q] = (t2 + t3) * w1;
+            out[2 * sb + q] = (t2 - t3) * w2;
           }
         } else {
           cd* u = gen.data();
           cd* v = gen.data() + p;
           const int np = n / p;
-          for (long q = 0; q < s; ++q) {
-            for (int j2 = 0; j2 < p; ++j2) u[j2] = in[j2 * m * s + q];
+          for (long q = 0; q < sb; ++q) {
+            for (int j2 = 0; j2 < p; ++j2) u[j2] = in[j2 * m * sb + q];
             for (int k2 = 0; k2 < p; ++k2) {
               cd acc = 0.0;
               for (int j2 = 0; j2 < p; ++j2) acc += u[j2] * tw[size_t((j2 * k2) % p) * np];
               v[k2] = acc;
             }
-            for (int k2 = 0; k2 < p; ++k2) out[s * k2 + q] = v[k2] * tw[size_t(j1 * k2 * s)];
+            for (int k2 = 0; k2 < p; ++k2) out[sb * k2 + q] = v[k2] * tw[size_t(j1 * k2 * s)];
           }
         }
       }
@@ -120,7 +135,7 @@ struct Fft1 {
       s *= p;
       L = m;
     }
-    if (a != x) std::memcpy(x, a, sizeof(cd) * n);
+    if (a != x) std::memcpy(x, a, sizeof(cd) * size_t(n) * B);
   }
 };
 
@@ -136,8 +151,10 @@ const Fft1& fft_plan_cached(int n, int sign) {
 }
 
 // In-place unnormalised multi-dimensional DFT, row-major dims (last fastest).
-// Lines along a strided axis are gathered in blocks of kBlk neighbouring
-// lines so that every cache line read is fully used.
+// Lines are transformed kBlk at a time, interleaved (Fft1::exec with B =
+// kBlk): along a strided axis kBlk neighbouring lines are gathered so that
+// every cache line read is fully used; along the contiguous axis kBlk rows
+// are transposed into the interleaved layout.
 void fft_nd(cd* data, const std::vector<int>& dims, int sign) {
   constexpr int kBlk = 16;
   const int r = int(dims.size());
@@ -151,18 +168,31 @@ void fft_nd(cd* data, const std::vector<int>& dims, int sign) {
     const size_t nouter = total / (size_t(n) * stride);
     const Fft1& f = fft_plan_cached(n, sign);
     if (stride == 1) {
+      const size_t nblk = (nouter + kBlk - 1) / kBlk;
 #pragma omp parallel
       {
-        std::vector<cd> work(n);
+        std::vector<cd> blk(size_t(n) * kBlk, cd(0.0, 0.0)), work(size_t(n) * kBlk);
 #pragma omp for schedule(static)
-        for (long li = 0; li < long(nouter); ++li) f.exec(data + size_t(li) * n, work.data());
+        for (long bi = 0; bi < long(nblk); ++bi) {
+          const size_t l0 = size_t(bi) * kBlk;
+          const int w = int(std::min<size_t>(kBlk, nouter - l0));
+          for (int b = 0; b < w; ++b) {
+            const cd* line = data + (l0 + b) * size_t(n);
+            for (int j = 0; j < n; ++j) blk[size_t(j) * kBlk + b] = line[j];
+          }
+          f.exec(blk.data(), work.data(), kBlk);
+          for (int b = 0; b < w; ++b) {
+            cd* line = data + (l0 + b) * size_t(n);
+            for (int j = 0; j < n; ++j) line[j] = blk[size_t(j) * kBlk + b];
+          }
+        }
       }
       continue;
     }
     const size_t nblk = (stride + kBlk - 1) / kBlk;
 #pragma omp parallel
     {
-      std::vector<cd> blk(size_t(n) * kBlk), line(n), work(n);
+      std::vector<cd> blk(size_t(n) * kBlk, cd(0.0, 0.0)), work(size_t(n) * kBlk);
 #pragma omp for schedule(static)
       for (long bi = 0; bi < long(nouter * nblk); ++bi) {
         const size_t outer = size_t(bi) / nblk, i0 = (size_t(bi) % nblk) * kBlk;
@@ -170,11 +200,7 @@ void fft_nd(cd* data, const std::vector<int>& dims, int sign) {
         cd* base = data + outer * stride * n + i0;
         for (int j = 0; j < n; ++j)
           for (int b = 0; b < w; ++b) blk[size_t(j) * kBlk + b] = base[size_t(j) * stride + b];
-        for (int b = 0; b < w; ++b) {
-          for (int j = 0; j < n; ++j) line[j] = blk[size_t(j) * kBlk + b];
-          f.exec(line.data(), work.data());
-          for (int j = 0; j < n; ++j) blk[size_t(j) * kBlk + b] = line[j];
-        }
+        f.exec(blk.data(), work.data(), kBlk);
         for (int j = 0; j < n; ++j)
           for (int b = 0; b < w; ++b) base[size_t(j) * stride + b] = blk[size_t(j) * kBlk + b];
       }
@@ -240,10 +266,70 @@ std::vector<double> correction(int w, double beta, int64_t nf, int64_t n) {
   return out;
 }
 
-// Kernel taps of a point at fractional cell offset f (see the device code).
-inline int taps(int w, double beta, double f, double* kv) {
-  const int s = (w % 2 == 0) ? (-w / 2 + (f > 0.0 ? 1 : 0)) : (-(w - 1) / 2 + (f > 0.5 ? 1 : 0));
-  for (int m = 0; m < w; ++m) kv[m] = es_phi((double(s + m) - f) * 2.0 / w, beta);
+// Piecewise-polynomial kernel taps, FINUFFT's default way of evaluating the
+// kernel (Horner's rule on a polynomial per tap; the ES paper's section on
+// fast kernel evaluation).  With the fractional cell offset f of a point the
+// w taps sit at t_m = (m - (w-1)/2 - u) 2/w, where u = f - 1/2 for even w
+// and u = f (f <= 1/2) or f - 1 (f > 1/2) for odd w, so u is in [-1/2, 1/2].
+// Each tap is a degree-(w+3) polynomial in u, fitted once per plan by
+// Chebyshev interpolation at 4(w+3)+40 nodes; the fit error is far below the
+// kernel's own truncation error.
+constexpr int kPolyExtra = 3;
+
+std::vector<double> tap_polynomials(int w, double beta) {
+  const int Q = w + kPolyExtra;
+  const int n = 4 * Q + 40;
+  std::vector<double> out(size_t(w) * (Q + 1), 0.0), cheb(Q + 1);
+  for (int m = 0; m < w; ++m) {
+    const double a = m - 0.5 * (w - 1);
+    for (int k = 0; k <= Q; ++k) {
+      double sum = 0.0;
+      for (int j = 0; j < n; ++j) {
+        const double xj = std::cos(kPi * (j + 0.5) / n);  // node in [-1, 1]; u = xj / 2
+        sum += es_phi((a - 0.5 * xj) * 2.0 / w, beta) * std::cos(k * kPi * (j + 0.5) / n);
+      }
+      cheb[k] = (k == 0 ? 1.0 : 2.0) * sum / n;
+    }
+    // Chebyshev series in x -> monomials in x (three-term recurrence) -> monomials in u = x / 2
+    std::vector<double> tkm1(Q + 1, 0.0), tk(Q + 1, 0.0), mono(Q + 1, 0.0);
+    tkm1[0] = 1.0;
+    tk[1] = 1.0;
+    mono[0] = cheb[0];
+    mono[1] = cheb[1];
+    for (int k = 1; k < Q; ++k) {
+      std::vector<double> tn(Q + 1, 0.0);
+      for (int d = 0; d < Q; ++d) tn[d + 1] += 2.0 * tk[d];
+      for (int d = 0; d <= Q; ++d) tn[d] -= tkm1[d];
+      for (int d = 0; d <= Q; ++d) mono[d] += cheb[k + 1] * tn[d];
+      tkm1 = tk;
+      tk = tn;
+    }
+    double scale = 1.0;
+    for (int d = 0; d <= Q; ++d, scale *= 2.0) out[size_t(m) * (Q + 1) + d] = mono[d] * scale;
+  }
+  return out;
+}
+
+// Kernel taps of a point at fractional cell offset f; returns the offset of
+// the first tap from the point's cell.
+inline int taps(int w, const double* poly, double f, double* kv) {
+  const int Q = w + kPolyExtra;
+  double u;
+  int s;
+  if (w % 2 == 0) {
+    u = f - 0.5;
+    s = -w / 2 + 1;
+  } else {
+    const bool hi = f > 0.5;
+    u = hi ? f - 1.0 : f;
+    s = -(w - 1) / 2 + (hi ? 1 : 0);
+  }
+  for (int m = 0; m < w; ++m) {
+    const double* c = poly + size_t(m) * (Q + 1);
+    double v = c[Q];
+    for (int d = Q - 1; d >= 0; --d) v = v * u + c[d];
+    kv[m] = v;
+  }
   return s;
 }
 
@@ -270,6 +356,7 @@ struct finufft_plan_s {
   double beta = 16.1;
   int64_t nf[3] = {1, 1, 1};
   std::vector<double> corr[3];
+  std::vector<double> poly;    // tap polynomials (tap_polynomials)
   std::vector<int64_t> cell;   // per point, per dim (M*dim)
   std::vector<double> frac;    // per point, per dim
   int tile = 32;
@@ -279,6 +366,14 @@ struct finufft_plan_s {
 };
 
 extern "C" void fresco_shim_set_mode(int mode) { g_mode = mode; }
+// Copies the per-stage seconds (setpts, spread, FFT, modes, interpolation)
+// into out[0..4]; reset != 0 clears them afterwards.
+extern "C" void fresco_shim_profile(double* out, int reset) {
+  for (int i = 0; i < kProfN; ++i) {
+    if (out) out[i] = g_prof[i];
+    if (reset) g_prof[i] = 0.0;
+  }
+}
 extern "C" int fresco_shim_get_mode(void) { return g_mode; }
 
 void finufft_default_opts(finufft_opts* o) {
@@ -311,6 +406,7 @@ int finufft_makeplan(int type, int dim, int64_t* n_modes, int iflag, int ntrans,
       p->nf[a] = next235even(std::max<int64_t>(2 * p->nm[a], 2 * w));
       p->corr[a] = correction(w, p->beta, p->nf[a], p->nm[a]);
     }
+    p->poly = tap_polynomials(w, p->beta);
   }
   *plan = p;
   return 0;
@@ -328,6 +424,7 @@ bool use_exact(const finufft_plan_s* p) {
 }
 
 void es_setpts(finufft_plan_s* p) {
+  ProfScope prof(kProfSetpts);
   const int d = p->dim;
   const int64_t M = p->M;
   p->cell.assign(size_t(M) * d, 0);
@@ -354,16 +451,39 @@ void es_setpts(finufft_plan_s* p) {
     }
     tid[j] = b[0] + p->nb[0] * (b[1] + p->nb[1] * b[2]);
   }
+  // stable counting sort by tile: per-thread histograms of contiguous point
+  // ranges, offsets in (tile, thread) order, then a parallel scatter
+  const int nth = omp_get_max_threads();
+  std::vector<int64_t> hist(size_t(nth) * ntiles, 0);
   p->tstart.assign(ntiles + 1, 0);
-  for (int64_t j = 0; j < M; ++j) p->tstart[tid[j] + 1]++;
-  for (int64_t t = 0; t < ntiles; ++t) p->tstart[t + 1] += p->tstart[t];
-  std::vector<int64_t> pos(p->tstart.begin(), p->tstart.end() - 1);
   p->torder.resize(M);
-  for (int64_t j = 0; j < M; ++j) p->torder[pos[tid[j]]++] = j;
+#pragma omp parallel num_threads(nth)
+  {
+    const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+    const int64_t j0 = M * t / nt, j1 = M * (t + 1) / nt;
+    int64_t* h = hist.data() + size_t(t) * ntiles;
+    for (int64_t j = j0; j < j1; ++j) ++h[tid[j]];
+#pragma omp barrier
+#pragma omp single
+    {
+      int64_t run = 0;
+      for (int64_t b = 0; b < ntiles; ++b) {
+        p->tstart[b] = run;
+        for (int u = 0; u < nt; ++u) {
+          const int64_t c = hist[size_t(u) * ntiles + b];
+          hist[size_t(u) * ntiles + b] = run;
+          run += c;
+        }
+      }
+      p->tstart[ntiles] = run;
+    }
+    for (int64_t j = j0; j < j1; ++j) p->torder[h[tid[j]]++] = j;
+  }
 }
 
 // Spreads complex strengths c onto the fine grid (row-major, dim 0 fastest).
 void es_spread(const finufft_plan_s* p, const cd* c, std::vector<cd>& grid) {
+  ProfScope prof(kProfSpread);
   const int d = p->dim, w = p->w;
   const int64_t nf0 = p->nf[0], nf1 = p->nf[1], nf2 = p->nf[2];
   grid.assign(size_t(nf0 * nf1 * nf2), cd(0.0, 0.0));
@@ -392,18 +512,18 @@ void es_spread(const finufft_plan_s* p, const cd* c, std::vector<cd>& grid) {
       int64_t i0[16], i1[16], i2[16];
       for (int64_t q = p->tstart[t]; q < p->tstart[t + 1]; ++q) {
         const int64_t j = p->torder[q];
-        const int s0 = taps(w, p->beta, p->frac[size_t(j) * d], k0);
+        const int s0 = taps(w, p->poly.data(), p->frac[size_t(j) * d], k0);
         for (int m = 0; m < w; ++m) i0[m] = wrap(p->cell[size_t(j) * d] + s0 + m, nf0);
         int ny = 1, nz = 1;
         k1[0] = k2[0] = 1.0;
         i1[0] = i2[0] = 0;
         if (d >= 2) {
-          const int s1 = taps(w, p->beta, p->frac[size_t(j) * d + 1], k1);
+          const int s1 = taps(w, p->poly.data(), p->frac[size_t(j) * d + 1], k1);
           for (int m = 0; m < w; ++m) i1[m] = wrap(p->cell[size_t(j) * d + 1] + s1 + m, nf1);
           ny = w;
         }
         if (d >= 3) {
-          const int s2 = taps(w, p->beta, p->frac[size_t(j) * d + 2], k2);
+          const int s2 = taps(w, p->poly.data(), p->frac[size_t(j) * d + 2], k2);
           for (int m = 0; m < w; ++m) i2[m] = wrap(p->cell[size_t(j) * d + 2] + s2 + m, nf2);
           nz = w;
         }
@@ -420,6 +540,7 @@ void es_spread(const finufft_plan_s* p, const cd* c, std::vector<cd>& grid) {
 }
 
 void es_interp(const finufft_plan_s* p, const std::vector<cd>& grid, cd* c) {
+  ProfScope prof(kProfInterp);
   const int d = p->dim, w = p->w;
   const int64_t nf0 = p->nf[0], nf1 = p->nf[1], nf2 = p->nf[2];
 #pragma omp parallel for schedule(static)
@@ -427,18 +548,18 @@ void es_interp(const finufft_plan_s* p, const std::vector<cd>& grid, cd* c) {
     const int64_t j = p->torder[q];
     double k0[16], k1[16], k2[16];
     int64_t i0[16], i1[16], i2[16];
-    const int s0 = taps(w, p->beta, p->frac[size_t(j) * d], k0);
+    const int s0 = taps(w, p->poly.data(), p->frac[size_t(j) * d], k0);
     for (int m = 0; m < w; ++m) i0[m] = wrap(p->cell[size_t(j) * d] + s0 + m, nf0);
     int ny = 1, nz = 1;
     k1[0] = k2[0] = 1.0;
     i1[0] = i2[0] = 0;
     if (d >= 2) {
-      const int s1 = taps(w, p->beta, p->frac[size_t(j) * d + 1], k1);
+      const int s1 = taps(w, p->poly.data(), p->frac[size_t(j) * d + 1], k1);
       for (int m = 0; m < w; ++m) i1[m] = wrap(p->cell[size_t(j) * d + 1] + s1 + m, nf1);
       ny = w;
     }
     if (d >= 3) {
-      const int s2 = taps(w, p->beta, p->frac[size_t(j) * d + 2], k2);
+      const int s2 = taps(w, p->poly.data(), p->frac[size_t(j) * d + 2], k2);
       for (int m = 0; m < w; ++m) i2[m] = wrap(p->cell[size_t(j) * d + 2] + s2 + m, nf2);
       nz = w;
     }
@@ -464,7 +585,11 @@ std::vector<int> fft_dims(const finufft_plan_s* p) {
 void es_type1(const finufft_plan_s* p, const cd* c, cd* f) {
   std::vector<cd> grid;
   es_spread(p, c, grid);
-  fft_nd(grid.data(), fft_dims(p), p->iflag);
+  {
+    ProfScope prof(kProfFft);
+    fft_nd(grid.data(), fft_dims(p), p->iflag);
+  }
+  ProfScope prof(kProfModes);
   const int64_t n0 = p->nm[0], n1 = p->nm[1], n2 = p->nm[2];
 #pragma omp parallel for schedule(static)
   for (int64_t i2 = 0; i2 < n2; ++i2)
@@ -483,6 +608,8 @@ void es_type1(const finufft_plan_s* p, const cd* c, cd* f) {
 void es_type2(const finufft_plan_s* p, cd* c, const cd* f) {
   std::vector<cd> grid(size_t(p->nf[0] * p->nf[1] * p->nf[2]), cd(0.0, 0.0));
   const int64_t n0 = p->nm[0], n1 = p->nm[1], n2 = p->nm[2];
+  {
+  ProfScope prof(kProfModes);
 #pragma omp parallel for schedule(static)
   for (int64_t i2 = 0; i2 < n2; ++i2)
     for (int64_t i1 = 0; i1 < n1; ++i1)
@@ -495,7 +622,11 @@ void es_type2(const finufft_plan_s* p, cd* c, const cd* f) {
         if (p->dim >= 3) pc *= p->corr[2][i2];
         grid[size_t((g2 * p->nf[1] + g1) * p->nf[0] + g0)] = f[i0 + n0 * (i1 + n1 * i2)] / pc;
       }
-  fft_nd(grid.data(), fft_dims(p), p->iflag);
+  }
+  {
+    ProfScope prof(kProfFft);
+    fft_nd(grid.data(), fft_dims(p), p->iflag);
+  }
   es_interp(p, grid, c);
 }
 

@@ -1,0 +1,168 @@
+"""Device LBFGS trajectories against the reference's own LBFGS (source/lbfgs.cpp) driving the
+reference's own potentials (nuwu.hpp, inversepower_potential.hpp + cell lists), compiled unchanged in
+oracle/_ref, on the configurations' inputs:
+
+* config 1 in its stated box [0, 2 pi)^2: the same trajectory, and the same stall (the reference's
+  coordinate map x = (p - round(p/L)) 2 pi / L, nuwu.hpp:219, jumps by one radian at p = pi, so the
+  energy is discontinuous and the line search ends up accepting after 10 halvings);
+* config 2 (NUwU + harmonic repulsion) on a 2^14-point subsample: the first 20 iterations of the FP64
+  form;
+* config 2 at full size: 500 iterations of the FP32 form and of the FP64 form;
+* LBFGS_CPP.set_H0 before and during a run (fresco/optimize/_lbfgs_cpp.pyx:72-74).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from oracle import refimpl as R
+
+pytestmark = pytest.mark.gpu
+
+CONFIG1 = "nuwu_2d_n4096.npz"
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def ref():
+    if not R.available():
+        pytest.skip("oracle/_ref (the reference compiled here) is not built")
+    R.set_threads(R.host_cores())
+    return R
+
+
+def test_lbfgs_set_H0_matches_reference(ref):
+    """set_H0 at construction and again after three iterations (with the reference's warning) gives the
+    reference's trajectory: iteration energies, evaluation counts, coordinates and the H0 it reports."""
+    from fresco_b200 import NUwU
+    from fresco_b200.optimize import LBFGS_CPP
+
+    ref.set_mode(ref.EXACT)
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(300, 6, 4, ndim=2, seed=31, L=np.ones(2))
+    pot = NUwU(radii, 6, Sk, V, L, eps=1e-13)
+    rpot = ref.NUwU(radii, 6, Sk, V, L, eps=1e-13)
+    opt = LBFGS_CPP(x, pot, M=5)
+    ropt = ref.LBFGS(x, rpot, M=5)
+    for o in (opt, ropt):
+        o.set_H0(0.02)
+    for it in range(12):
+        if it == 3:
+            opt.set_H0(0.5)
+            ropt.set_H0(0.5)
+        r = opt.one_iteration()
+        ropt.one_iteration()
+        s = ropt.state()
+        assert rel(r.energy, s["energy"]) < 1e-8, it
+        assert r.nfev == s["nfev"], it
+    res, s = opt.get_result(), ropt.state()
+    assert rel(res.coords, s["coords"]) < 1e-8
+    assert rel(res.H0, s["H0"]) < 1e-8
+
+
+def test_lbfgs_set_H0_refused_by_fire():
+    from fresco_b200 import NUwU
+    from fresco_b200.optimize import ModifiedFireCPP
+
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(50, 3, 2, ndim=2, seed=1)
+    opt = ModifiedFireCPP(x, NUwU(radii, 3, Sk, V, L))
+    from fresco_b200._lib import check, lib
+
+    with pytest.raises(ValueError):
+        check(lib.fresco_lbfgs_set_H0(opt._h, 0.3))
+
+
+def test_config1_box_2pi_trajectory_and_stall_match_reference(ref):
+    """Config 1 as stated: N = 4096 seeded uniform points in [0, 2 pi)^2, 65^2 modes, S0 = 0 and V = 1
+    on 0 < |k| <= 16, LBFGS M = 10, FP64.  The device LBFGS and the reference's follow the same
+    trajectory for 300 iterations (energy every 25 iterations, evaluation counts), and then both stall:
+    after 600 iterations the energy is still far above the 1e-12 that the same pattern reaches in the
+    L = 1 convention (test_lbfgs_config1_converges_below_1e12), with several evaluations per iteration
+    (line searches that halve the step up to 10 times and accept anyway, lbfgs.cpp:200-236)."""
+    import os
+
+    from fresco_b200 import NUwU
+    from fresco_b200.optimize import LBFGS_CPP
+
+    d = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", CONFIG1)))
+    L = np.full(2, 2 * np.pi)
+    ref.set_mode(ref.EXACT)
+    pot = NUwU(d["radii"], 32, d["Sk"], d["V"], L, eps=1e-13)
+    rpot = ref.NUwU(d["radii"], 32, d["Sk"], d["V"], L, eps=1e-13)
+    opt = LBFGS_CPP(d["x"], pot, tol=0.0, M=10, nsteps=100000)
+    ropt = ref.LBFGS(d["x"], rpot, tol=0.0, M=10, nsteps=100000)
+    for chunk in range(12):
+        res = opt.run(25)
+        ropt.run(25)
+        s = ropt.state()
+        assert res.nsteps == s["nsteps"] == 25 * (chunk + 1)
+        assert res.nfev == s["nfev"], chunk
+        assert rel(res.energy, s["energy"]) < 1e-7, (chunk, res.energy, s["energy"])
+    n300, rn300 = res.nfev, s["nfev"]
+    res = opt.run(300)
+    ropt.run(300)
+    s = ropt.state()
+    for e, nfev, n0 in ((res.energy, res.nfev, n300), (s["energy"], s["nfev"], rn300)):
+        assert e > 1.0, e  # stalled: the L = 1 form of the same pattern reaches < 1e-12
+        assert nfev - n0 > 3 * 300, nfev - n0  # backtracking on most iterations
+
+
+def test_config2_subsample_fp64_first_20_iterations_match_reference(ref):
+    """Config 2's objective (NUwU with S0 = 0, V = 1 on 0 < |k| <= K/2, plus the harmonic repulsion of
+    diameter 0.5/sqrt(N) 2 pi) on N = 2^14 seeded points with 129^2 modes, LBFGS M = 4 (the reference
+    default): the device FP64 form at eps 1e-12 against the reference's lbfgs.cpp driving its nuwu.hpp
+    (ES-kernel NUFFT restatement at eps 1e-12, within 1e-13 of exact sums) and its cell-list
+    repulsion."""
+    from fresco_b200 import CombinedPotential, InversePower, NUwU
+    from fresco_b200.optimize import LBFGS_CPP
+
+    N, K, kmax = 1 << 14, 64, 32
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(N, K, kmax, ndim=2, seed=2)
+    rr = np.full(N, 0.25 / np.sqrt(N) * 2 * np.pi)
+    comb = CombinedPotential()
+    comb.add_potential(NUwU(radii, K, Sk, V, L, eps=1e-12, precision="fp64"))
+    comb.add_potential(InversePower(2.0, 1.0, rr, L, use_cell_lists=True))
+    ref.set_mode(ref.ES)
+    rcomb = ref.CombinedPotential()
+    rcomb.add_potential(ref.NUwU(radii, K, Sk, V, L, eps=1e-12))
+    rcomb.add_potential(ref.InversePower(2.0, 1.0, rr, L, use_cell_lists=True))
+    opt = LBFGS_CPP(x, comb)
+    ropt = ref.LBFGS(x, rcomb)
+    for it in range(20):
+        r = opt.one_iteration()
+        ropt.one_iteration()
+        s = ropt.state()
+        assert rel(r.energy, s["energy"]) < 1e-8, it
+        assert r.nfev == s["nfev"], it
+    assert rel(opt.get_result().coords, s["coords"]) < 1e-8
+
+
+@pytest.mark.timeout(600)
+def test_config2_500_iterations_fp32_and_fp64():
+    """Config 2 at full size (N = 2^20 seeded uniform points in [0, 2 pi)^2, 1025^2 modes, S0 = 0 and
+    V = 1 on 0 < |k| <= 256, harmonic repulsion of diameter 0.5/sqrt(N) 2 pi, stiffness 1), LBFGS with
+    the reference defaults (M = 4) for 500 iterations in the FP32 spread/FFT/interpolation form (eps
+    1e-6) and in the FP64 form (eps 1e-12).  Both lower the energy by orders of magnitude; their
+    energies agree closely at first and stay within a factor of two of each other at iteration 500."""
+    from fresco_b200 import CombinedPotential, InversePower, NUwU
+    from fresco_b200.optimize import LBFGS_CPP
+
+    N, K, kmax = 1 << 20, 512, 256
+    x, radii, Sk, V, L = O.stealthy_nuwu_inputs(N, K, kmax, ndim=2, seed=2)
+    rr = np.full(N, 0.25 / np.sqrt(N) * 2 * np.pi)
+    out = {}
+    for prec, eps in (("fp32", 1e-6), ("fp64", 1e-12)):
+        comb = CombinedPotential()
+        comb.add_potential(NUwU(radii, K, Sk, V, L, eps=eps, precision=prec))
+        comb.add_potential(InversePower(2.0, 1.0, rr, L, use_cell_lists=True))
+        opt = LBFGS_CPP(x, comb, tol=0.0)
+        e0 = opt.get_result().energy
+        e20 = opt.run(20).energy
+        res = opt.run(480)
+        assert res.nsteps == 500 and np.isfinite(res.energy)
+        out[prec] = (e0, e20, res.energy, res.nfev)
+    (a0, a20, a500, _), (b0, b20, b500, _) = out["fp32"], out["fp64"]
+    assert rel(a0, b0) < 1e-5 and rel(a20, b20) < 1e-3, out
+    assert a500 < 1e-3 * a0 and b500 < 1e-3 * b0, out
+    assert 0.5 < a500 / b500 < 2.0, out

@@ -184,3 +184,33 @@ def test_nuwu_graph_replay_follows_buffer_contents(prec):
         e_parts = NUwU(radii, K, Sk, V, L, precision=prec).get_energy_gradient(xi)[0]
         e_parts += InversePower(2.0, 1.0, 0.02 * np.ones(N), box).get_energy_gradient(xi)[0]
         assert float(e.item()) == pytest.approx(e_parts, rel=tol), it
+
+
+@pytest.mark.parametrize("prec,eps,tol", PRECISIONS)
+def test_interp_tile_copy_second_wait(prec, eps, tol):
+    """With a first wait of zero polls every interior tile copy of the 2D interpolation outlasts it: the
+    blocks raise status bit 8 (retry), wait again bounded by time, see the copy land and finish.  The
+    results equal the default setting's and the oracle's; no timeout (bit 4) is raised."""
+    from fresco_b200 import NUwU
+    from fresco_b200._lib import check, lib
+
+    K, kmax = 128, 80  # 512^2 fine grid: 64 tiles, 36 of them interior (copied by TMA)
+    x, radii, Sk, V, L = _inputs(2, 20000, K, kmax, seed=21, radii_spread=False)
+    ref = O.NUwU(radii, K, Sk, V, L)
+    e_ref, g_ref = ref.get_energy_gradient(x)
+    e0, g0 = NUwU(radii, K, Sk, V, L, eps=eps, precision=prec).get_energy_gradient(x)
+    check(lib.fresco_debug_set_tile_wait_polls(0))
+    try:
+        pot = NUwU(radii, K, Sk, V, L, eps=eps, precision=prec)  # captures its graphs with the new setting
+        results = [pot.get_energy_gradient(x) for _ in range(3)]  # direct launches, capture, replay
+        st = pot.status()
+    finally:
+        check(lib.fresco_debug_set_tile_wait_polls(-1))
+    assert st & 8 and not st & 4, st
+    for e1, g1 in results:
+        assert abs(e1 - e0) <= tol * abs(e0) and abs(e1 - e_ref) <= tol * abs(e_ref)
+        assert np.linalg.norm(g1 - g0) <= tol * np.linalg.norm(g0)
+        assert np.linalg.norm(g1 - g_ref) <= tol * np.linalg.norm(g_ref)
+    after = NUwU(radii, K, Sk, V, L, eps=eps, precision=prec)
+    after.get_energy_gradient(x)
+    assert after.status() == 0

@@ -102,3 +102,100 @@ def test_noalloc_rejects_more_kpoints_than_the_static_array_holds():
                                                    L.ctypes.data_as(C.POINTER(C.c_double)), 0, p(g), p(e), 0, None)
     assert rc == FRESCO_ERR_INVALID
     assert b"4096" in lib.fresco_last_error()
+
+
+def _setup(ndim, N, nk, seed, torch, lib):
+    rng = np.random.default_rng(seed)
+    radii = 0.5 + rng.random(N)
+    K = (rng.random(nk * ndim) - 0.5) * 40
+    Sk = rng.random(nk) * N * (rng.random(nk) < 0.5)
+    V = rng.random(nk)
+    L = 0.7 + rng.random(ndim)
+    h = C.c_void_p()
+    dp = lambda a: np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+    rc = lib.fresco_nuwnu_create(dp(radii), N, dp(K), nk, dp(Sk), dp(V), dp(L), ndim, 1e-12, 0, C.byref(h))
+    assert rc == 0, lib.fresco_last_error()
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()  # noqa: E731
+    arrays = dict(w_d=dev(_weights(radii, ndim)), k_d=dev(K), sk_d=dev(Sk), v_d=dev(V))
+    x_d = dev(rng.random(ndim * N) * 1.4 - 0.2)
+    return h, arrays, L, x_d
+
+
+def _noalloc_raw(lib, x_d, N, ndim, a, nk, L, g, e, acc, stream):
+    Lc = np.ascontiguousarray(L, dtype=np.float64)
+    ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
+    rc = lib.fresco_nuwnu_energy_gradient_noalloc(ptr(x_d), N, ndim, ptr(a["w_d"]), ptr(a["k_d"]), ptr(a["sk_d"]),
+                                                   ptr(a["v_d"]), nk, Lc.ctypes.data_as(C.POINTER(C.c_double)), 0,
+                                                   ptr(g), ptr(e), acc, C.c_void_p(stream))
+    assert rc == 0, lib.fresco_last_error()
+
+
+def test_noalloc_accumulates_into_preset_outputs():
+    """accumulate = 1 adds the loss and gradient to what the output arrays hold, on two calls in a row."""
+    import torch
+
+    from fresco_b200._lib import lib
+
+    ndim, N, nk = 2, 2000, 64
+    h, a, L, x_d = _setup(ndim, N, nk, 7, torch, lib)
+    try:
+        stream = torch.cuda.current_stream().cuda_stream
+        g0, e0 = _handle_eval(lib, h, x_d, N * ndim, stream, torch)
+        for call in range(2):
+            preset_g = torch.linspace(-3.0, 5.0, N * ndim, dtype=torch.float64, device="cuda")
+            preset_e = torch.full((1,), 11.5, dtype=torch.float64, device="cuda")
+            g, e = preset_g.clone(), preset_e.clone()
+            _noalloc_raw(lib, x_d, N, ndim, a, nk, L, g, e, 1, stream)
+            torch.cuda.synchronize()
+            assert _rel((e - preset_e).cpu().numpy(), e0.cpu().numpy()) < 1e-11, call
+            assert _rel((g - preset_g).cpu().numpy(), g0.cpu().numpy()) < 1e-10, call
+    finally:
+        lib.fresco_potential_destroy(h)
+
+
+def test_noalloc_energy_only():
+    """A NULL gradient pointer computes the energy alone, equal to the handle form's."""
+    import torch
+
+    from fresco_b200._lib import lib
+
+    ndim, N, nk = 3, 1200, 100
+    h, a, L, x_d = _setup(ndim, N, nk, 8, torch, lib)
+    try:
+        stream = torch.cuda.current_stream().cuda_stream
+        _, e0 = _handle_eval(lib, h, x_d, N * ndim, stream, torch)
+        for call in range(2):
+            e = torch.full((1,), 7.0, dtype=torch.float64, device="cuda")
+            _noalloc_raw(lib, x_d, N, ndim, a, nk, L, None, e, 0, stream)
+            torch.cuda.synchronize()
+            assert _rel(e.cpu().numpy(), e0.cpu().numpy()) < 1e-11, call
+    finally:
+        lib.fresco_potential_destroy(h)
+
+
+def test_noalloc_nonfinite_call_then_finite_call():
+    """A NaN coordinate makes that call's energy and gradient NaN; the status it leaves in the shared
+    array must not leak into the next, finite call, whose results equal the handle form's."""
+    import torch
+
+    from fresco_b200._lib import lib
+
+    ndim, N, nk = 2, 1500, 50
+    h, a, L, x_d = _setup(ndim, N, nk, 9, torch, lib)
+    try:
+        stream = torch.cuda.current_stream().cuda_stream
+        g0, e0 = _handle_eval(lib, h, x_d, N * ndim, stream, torch)
+        bad = x_d.clone()
+        bad[17] = float("nan")
+        g = torch.empty(N * ndim, dtype=torch.float64, device="cuda")
+        e = torch.empty(1, dtype=torch.float64, device="cuda")
+        _noalloc_raw(lib, bad, N, ndim, a, nk, L, g, e, 0, stream)
+        torch.cuda.synchronize()
+        assert torch.isnan(e).all() and torch.isnan(g).all()
+        _noalloc_raw(lib, x_d, N, ndim, a, nk, L, g, e, 0, stream)
+        torch.cuda.synchronize()
+        assert torch.isfinite(e).all() and torch.isfinite(g).all()
+        assert _rel(e.cpu().numpy(), e0.cpu().numpy()) < 1e-11
+        assert _rel(g.cpu().numpy(), g0.cpu().numpy()) < 1e-10
+    finally:
+        lib.fresco_potential_destroy(h)
