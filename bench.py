@@ -336,7 +336,7 @@ def config2_lbfgs500_report(x, radii, Sk, V, L, n_iter=500):
         comb.add_potential(NUwU(radii, K_MODES, Sk, V, L, eps=eps, precision=prec))
         comb.add_potential(InversePower(2.0, 1.0, rr, np.asarray(L, float), use_cell_lists=True))
         opt = LBFGS_CPP(x, comb, tol=0.0, nsteps=n_iter + 10)
-        e0 = float(opt.get_result().energy)
+        e0 = float(comb.get_energy(x))  # an optimiser that has not iterated reports 0, like the reference
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         _check(_clib.fresco_optimizer_run(opt._h, n_iter))

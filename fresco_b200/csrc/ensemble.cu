@@ -189,12 +189,14 @@ __global__ void __launch_bounds__(kEnsSortThreads) ens_sort_scatter_kernel(
     int st = pi.rec_base + first_start;
     for (int b = b0; b < b1; ++b) {
       const int c = tot[b];
-      for (int q = 0; q * kMaxSub < c; ++q) {
+      const int parts = (c + kMaxSub - 1) / kMaxSub;  // equal parts of at most kMaxSub points
+      for (int q = 0; q < parts; ++q) {
         if (sbase < pi.max_sub) {
           const int si = pi.sub_base + sbase;
+          const int lo = int(int64_t(q) * c / parts), hi = int(int64_t(q + 1) * c / parts);
           sub_bin[si] = b;
-          sub_start[si] = st + q * kMaxSub;
-          sub_count[si] = min(kMaxSub, c - q * kMaxSub);
+          sub_start[si] = st + lo;
+          sub_count[si] = hi - lo;
         }
         ++sbase;
       }

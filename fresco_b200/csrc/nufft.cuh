@@ -25,7 +25,12 @@
 
 namespace fb {
 
-constexpr int kMaxSub = 1280;     // points per spreading/interpolation subproblem
+// Points per spreading/interpolation subproblem at most: a bin is cut into
+// equal parts of at most kMaxSub points.  Each tile block stages its
+// subproblem in shared memory, so kMaxSub also sets how many blocks share an
+// SM; 640 gives the 2D tile kernels seven (FP32 spreading) and about two
+// subproblems per bin at the benchmark's density, close to two full waves.
+constexpr int kMaxSub = 640;
 constexpr int kMaxBins = 32768;   // bins per geometry (block-local histograms live in shared memory)
 constexpr int kTile2D = 64;       // 2D tile edge (phased spreading needs a multiple of the sub-block edge)
 

@@ -177,8 +177,8 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_count_kernel(const doubl
 }
 
 // Sort pass 2: every block scans the bin totals itself (bin starts), block 0
-// also publishes them and the subproblem table (each bin cut into chunks of
-// at most kMaxSub points); then each block hands out the slots of its
+// also publishes them and the subproblem table (each bin cut into equal parts
+// of at most kMaxSub points); then each block hands out the slots of its
 // segments with shared-memory cursors (the counts are those of pass 1, so
 // every slot is written exactly once) and moves its records there.  The last
 // block to finish clears bin_total for the next sort.
@@ -216,11 +216,13 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_scatter_kernel(
     int st = first_start;
     for (int b = b0; b < b1; ++b) {
       const int c = bin_total[b];
-      for (int q = 0; q * kMaxSub < c; ++q) {
+      const int parts = (c + kMaxSub - 1) / kMaxSub;  // equal parts of at most kMaxSub points
+      for (int q = 0; q < parts; ++q) {
         if (sbase < max_sub) {
+          const int lo = int(int64_t(q) * c / parts), hi = int(int64_t(q + 1) * c / parts);
           sub_bin[sbase] = b;
-          sub_start[sbase] = st + q * kMaxSub;
-          sub_count[sbase] = min(kMaxSub, c - q * kMaxSub);
+          sub_start[sbase] = st + lo;
+          sub_count[sbase] = hi - lo;
         }
         ++sbase;
       }
@@ -450,29 +452,21 @@ struct TileMap1 {
   }
 };
 
-template <int W, typename T, bool CPLX, typename Map>
-__global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
-    const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, const cplx_t<T>* __restrict__ strengths,
-    const Map map, Geom g, const EsPoly<W, T> poly, T* grid_real, cplx_t<T>* grid_cplx) {
+// Staging shared by the 2D spreading kernels: zeroes the tile, groups the
+// block's points by 8 x 8-cell sub-block (counts, exclusive scan) and stores
+// each as (tile offset of its footprint, polynomial variables, weight) in
+// sub-block order.
+template <int W, typename T, bool CPLX>
+__device__ __forceinline__ void spread2d_stage(const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights,
+                                               const cplx_t<T>* __restrict__ strengths, const TileWork<T>& wk,
+                                               Staged2D<T, CPLX>* srec, T* tile, int* sb_count, int* sb_start) {
   using P = Tile2D<W>;
   using S = Staged2D<T, CPLX>;
   constexpr int NC = CPLX ? 2 : 1;
   constexpr int E = P::EDGE;
   constexpr int NSB2 = P::NSB * P::NSB;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  S* srec = reinterpret_cast<S*>(smem_raw);
-  T* tile = reinterpret_cast<T*>(srec + kMaxSub);
-  int* sb_count = reinterpret_cast<int*>(tile + E * E * NC);
-  int* sb_start = sb_count + NSB2;
-
-  TileWork<T> wk;
-  if (!map.fetch(g, wk)) return;
   const int start = wk.start, cnt = wk.cnt, org0 = wk.org0, org1 = wk.org1;
-  const T uniform = wk.uniform;
-  if (grid_real) grid_real += wk.grid_off;
-  if (grid_cplx) grid_cplx += wk.grid_off;
   const int tid = threadIdx.x;
-
   for (int i = tid; i < E * E * NC; i += P::THREADS) tile[i] = T(0);
   for (int i = tid; i < NSB2; i += P::THREADS) sb_count[i] = 0;
   // this thread's points are p = tid + THREADS k; their cells are loaded
@@ -541,13 +535,81 @@ __global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
         st.wr = v.x;
         st.wi = v.y;
       } else {
-        st.wr = weights ? weights[r.idx] : uniform;
+        st.wr = weights ? weights[r.idx] : wk.uniform;
       }
       srec[sb_start[slot[k] >> 16] + (slot[k] & 0xffff)] = st;
     }
   }
   __syncthreads();
+}
 
+// Adds the shared tile of one 2D subproblem to the fine grid: float4 vector
+// atomics (four real or two complex cells) for FP32, scalar atomics for FP64;
+// cells that no neighbouring tile can reach are stored plainly when the
+// subproblem is its tile's only one.
+template <int W, typename T, bool CPLX>
+__device__ __forceinline__ void spread2d_flush(const T* tile, const TileWork<T>& wk, const Geom& g, T* grid_real,
+                                               cplx_t<T>* grid_cplx) {
+  using P = Tile2D<W>;
+  constexpr int NC = CPLX ? 2 : 1;
+  constexpr int E = P::EDGE;
+  const int org0 = wk.org0, org1 = wk.org1, tid = threadIdx.x;
+  const int nf0 = g.nf[0], nf1 = g.nf[1];
+  if (sizeof(T) == 4 && nf0 % (4 / NC) == 0) {
+    constexpr int VW = 4 / NC;                          // cells per float4
+    constexpr int LEFT = (VW - P::PAD % VW) % VW;       // cells left of the tile origin in the first group
+    constexpr int NG = (E + LEFT + VW - 1) / VW;        // groups per tile row
+    // cells [W, 64) of the tile (relative to org - PAD) along both axes are
+    // out of reach of every other tile; with one subproblem in the bin and
+    // whole tiles (nf a multiple of 64) they are written with plain stores
+    const bool sole = wk.cnt == wk.bin_range[1] - wk.bin_range[0] && nf0 % kTile2D == 0 && nf1 % kTile2D == 0;
+    for (int i = tid; i < E * NG; i += P::THREADS) {
+      const int ty = i / NG, j = i - ty * NG;
+      const int tc0 = j * VW - LEFT;
+      const int gy = wrap_index(org1 - P::PAD + ty, nf1);
+      const int gx = wrap_index(org0 - P::PAD + tc0, nf0);
+      const bool plain = sole && ty >= W && ty < kTile2D && tc0 >= W && tc0 + VW <= kTile2D;
+      float* dst = CPLX ? reinterpret_cast<float*>(grid_cplx + int64_t(gy) * nf0 + gx)
+                        : reinterpret_cast<float*>(grid_real + int64_t(gy) * nf0 + gx);
+      flush_group_f32<T, CPLX>(tile + ty * E * NC, tc0, E, dst, plain);
+    }
+  } else {
+    for (int i = tid; i < E * E; i += P::THREADS) {
+      const int ty = i / E, tc = i - ty * E;
+      const int64_t gi = int64_t(wrap_index(org1 - P::PAD + ty, nf1)) * nf0 + wrap_index(org0 - P::PAD + tc, nf0);
+      if constexpr (CPLX) {
+        const T re = tile[2 * i], im = tile[2 * i + 1];
+        if (re != T(0) || im != T(0)) atomic_add_cplx<T>(grid_cplx + gi, re, im);
+      } else {
+        const T v = tile[i];
+        if (v != T(0)) atomicAdd(grid_real + gi, v);
+      }
+    }
+  }
+}
+
+template <int W, typename T, bool CPLX, typename Map>
+__global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
+    const Rec<2, T>* __restrict__ recs, const T* __restrict__ weights, const cplx_t<T>* __restrict__ strengths,
+    const Map map, Geom g, const EsPoly<W, T> poly, T* grid_real, cplx_t<T>* grid_cplx) {
+  using P = Tile2D<W>;
+  using S = Staged2D<T, CPLX>;
+  constexpr int NC = CPLX ? 2 : 1;
+  constexpr int E = P::EDGE;
+  constexpr int NSB2 = P::NSB * P::NSB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* srec = reinterpret_cast<S*>(smem_raw);
+  T* tile = reinterpret_cast<T*>(srec + kMaxSub);
+  int* sb_count = reinterpret_cast<int*>(tile + E * E * NC);
+  int* sb_start = sb_count + NSB2;
+
+  TileWork<T> wk;
+  if (!map.fetch(g, wk)) return;
+  if (grid_real) grid_real += wk.grid_off;
+  if (grid_cplx) grid_cplx += wk.grid_off;
+  spread2d_stage<W, T, CPLX>(recs, weights, strengths, wk, srec, tile, sb_count, sb_start);
+
+  const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   // tap roles: lane hl of each half evaluates x tap hl (hl < W) or y tap hl - W
   const int half = lane / P::HL, hl = lane % P::HL;
@@ -632,39 +694,7 @@ __global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
     __syncthreads();
   }
 
-  // flush
-  const int nf0 = g.nf[0], nf1 = g.nf[1];
-  if (sizeof(T) == 4 && nf0 % (4 / NC) == 0) {
-    constexpr int VW = 4 / NC;                          // cells per float4
-    constexpr int LEFT = (VW - P::PAD % VW) % VW;       // cells left of the tile origin in the first group
-    constexpr int NG = (E + LEFT + VW - 1) / VW;        // groups per tile row
-    // cells [W, 64) of the tile (relative to org - PAD) along both axes are
-    // out of reach of every other tile; with one subproblem in the bin and
-    // whole tiles (nf a multiple of 64) they are written with plain stores
-    const bool sole = cnt == wk.bin_range[1] - wk.bin_range[0] && nf0 % kTile2D == 0 && nf1 % kTile2D == 0;
-    for (int i = tid; i < E * NG; i += P::THREADS) {
-      const int ty = i / NG, j = i - ty * NG;
-      const int tc0 = j * VW - LEFT;
-      const int gy = wrap_index(org1 - P::PAD + ty, nf1);
-      const int gx = wrap_index(org0 - P::PAD + tc0, nf0);
-      const bool plain = sole && ty >= W && ty < kTile2D && tc0 >= W && tc0 + VW <= kTile2D;
-      float* dst = CPLX ? reinterpret_cast<float*>(grid_cplx + int64_t(gy) * nf0 + gx)
-                        : reinterpret_cast<float*>(grid_real + int64_t(gy) * nf0 + gx);
-      flush_group_f32<T, CPLX>(tile + ty * E * NC, tc0, E, dst, plain);
-    }
-  } else {
-    for (int i = tid; i < E * E; i += P::THREADS) {
-      const int ty = i / E, tc = i - ty * E;
-      const int64_t gi = int64_t(wrap_index(org1 - P::PAD + ty, nf1)) * nf0 + wrap_index(org0 - P::PAD + tc, nf0);
-      if constexpr (CPLX) {
-        const T re = tile[2 * i], im = tile[2 * i + 1];
-        if (re != T(0) || im != T(0)) atomic_add_cplx<T>(grid_cplx + gi, re, im);
-      } else {
-        const T v = tile[i];
-        if (v != T(0)) atomicAdd(grid_real + gi, v);
-      }
-    }
-  }
+  spread2d_flush<W, T, CPLX>(tile, wk, g, grid_real, grid_cplx);
 }
 
 // Generic spreading (1D, 3D): one thread per point, shared-memory atomics.

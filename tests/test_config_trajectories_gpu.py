@@ -143,8 +143,11 @@ def test_config2_500_iterations_fp32_and_fp64():
     """Config 2 at full size (N = 2^20 seeded uniform points in [0, 2 pi)^2, 1025^2 modes, S0 = 0 and
     V = 1 on 0 < |k| <= 256, harmonic repulsion of diameter 0.5/sqrt(N) 2 pi, stiffness 1), LBFGS with
     the reference defaults (M = 4) for 500 iterations in the FP32 spread/FFT/interpolation form (eps
-    1e-6) and in the FP64 form (eps 1e-12).  Both lower the energy by orders of magnitude; their
-    energies agree closely at first and stay within a factor of two of each other at iteration 500."""
+    1e-6) and in the FP64 form (eps 1e-12).  At L = 2 pi the reference's coordinate map folds the box
+    (x = p - 1 for p >= pi, nuwu.hpp:219), so the start has a large low-k density contrast and the energy
+    falls slowly under the 0.1 maximum step: both forms lower it, and their energies agree to 1e-3 at
+    iterations 0, 20 and 500.  (An optimiser that has not iterated reports energy 0, as the reference's
+    get_result does, opt.pyx:81-93: the start energy is the potential's own.)"""
     from fresco_b200 import CombinedPotential, InversePower, NUwU
     from fresco_b200.optimize import LBFGS_CPP
 
@@ -157,12 +160,12 @@ def test_config2_500_iterations_fp32_and_fp64():
         comb.add_potential(NUwU(radii, K, Sk, V, L, eps=eps, precision=prec))
         comb.add_potential(InversePower(2.0, 1.0, rr, L, use_cell_lists=True))
         opt = LBFGS_CPP(x, comb, tol=0.0)
-        e0 = opt.get_result().energy
+        e0 = comb.get_energy(x)
         e20 = opt.run(20).energy
         res = opt.run(480)
         assert res.nsteps == 500 and np.isfinite(res.energy)
         out[prec] = (e0, e20, res.energy, res.nfev)
     (a0, a20, a500, _), (b0, b20, b500, _) = out["fp32"], out["fp64"]
-    assert rel(a0, b0) < 1e-5 and rel(a20, b20) < 1e-3, out
-    assert a500 < 1e-3 * a0 and b500 < 1e-3 * b0, out
-    assert 0.5 < a500 / b500 < 2.0, out
+    assert rel(a0, b0) < 1e-5 and rel(a20, b20) < 1e-4, out
+    assert a500 < 0.9 * a0 and b500 < 0.9 * b0 and a20 < a0, out
+    assert rel(a500, b500) < 1e-3, out
