@@ -80,6 +80,8 @@ void alloc_sort(SortBufs& sb, int64_t N, const Geom& g) {
   sb.unsorted.alloc(std::max<int64_t>(N, 1) * 32);  // the largest record is 32 bytes
   sb.done.alloc(1);
   FB_CUDA(cudaMemset(sb.done.p, 0, sizeof(unsigned)));
+  sb.bar.alloc(1);
+  FB_CUDA(cudaMemset(sb.bar.p, 0, sizeof(unsigned long long)));
 }
 
 }  // namespace fb

@@ -87,6 +87,13 @@ struct SortBufs {
   DevBuf<unsigned char> unsorted;  // N records in input order (written by the counting pass)
   DevBuf<unsigned> done;           // blocks of the scattering pass that finished (reset by the last one)
   int64_t max_sub = 0;
+  // one-pass sort (a cooperative launch whose blocks keep their points in
+  // shared memory across a grid-wide barrier): blocks and points per block,
+  // decided at the first sort (one_blocks 0: the two-pass sort is used)
+  int one_blocks = -1;
+  int64_t one_N = -1, one_chunk = 0;
+  size_t one_smem = 0;
+  DevBuf<unsigned long long> bar;  // grid barrier arrivals (monotonic)
 };
 
 // Packing of an absolute fine cell (c0, c1, c2) into 32 bits.

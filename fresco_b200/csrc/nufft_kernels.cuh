@@ -27,6 +27,13 @@ __device__ __forceinline__ int wrap_index(int x, int n) {
   return x;
 }
 
+// Nanoseconds of the GPU's global timer (bounds for waits).
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Maps coordinate a of a point to (fine-grid cell, fraction in [0, 1)).
 // Returns false for a non-finite coordinate (then cell = 0, fraction = 0 so
 // all later accesses stay in bounds).
@@ -176,23 +183,16 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_count_kernel(const doubl
   }
 }
 
-// Sort pass 2: every block scans the bin totals itself (bin starts), block 0
-// also publishes them and the subproblem table (each bin cut into equal parts
-// of at most kMaxSub points); then each block hands out the slots of its
-// segments with shared-memory cursors (the counts are those of pass 1, so
-// every slot is written exactly once) and moves its records there.  The last
-// block to finish clears bin_total for the next sort.
-template <int D, typename T>
-__global__ void __launch_bounds__(kSortThreads, 2) sort_scatter_kernel(
-    const Rec<D, T>* __restrict__ unsorted, int64_t N, int64_t chunk, Geom g, int* bin_total,
-    const int* __restrict__ blk_off, int* bin_start, int* sub_bin, int* sub_start, int* sub_count, int* num_sub,
-    int max_sub, unsigned* done, Rec<D, T>* out, int* status) {
-  extern __shared__ int sh_cur[];
-  __shared__ int s_warp[32];
-  __shared__ bool s_last;
-  const int nbins = int(g.nbins());
+// Bin starts from the bin totals, computed by every block of a sort (each
+// thread scans a contiguous share of the bins); the block with `publish` also
+// writes them and the subproblem table (each bin cut into equal parts of at
+// most kMaxSub points).  on_bin(b, start) is called for each bin of the
+// thread's share.
+template <typename F>
+__device__ __forceinline__ void scan_bins(const int* bin_total, int nbins, bool publish, int* bin_start, int* sub_bin,
+                                          int* sub_start, int* sub_count, int* num_sub, int max_sub, int* s_warp,
+                                          F&& on_bin) {
   const int tid = threadIdx.x;
-  const int* my_off = blk_off + int64_t(blockIdx.x) * nbins;
   const int per = (nbins + int(blockDim.x) - 1) / int(blockDim.x);
   const int b0 = min(nbins, tid * per), b1 = min(nbins, b0 + per);
   int npts = 0, nsub = 0;
@@ -203,14 +203,13 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_scatter_kernel(
   }
   int tot_pts;
   int run = block_exclusive_scan(npts, &tot_pts, s_warp);
-  const int first_start = run;  // start of bin b0
-  // bins this block has no points in get stale offsets that are never used
+  const int first_start = run;
   for (int b = b0; b < b1; ++b) {
-    sh_cur[b] = run + my_off[b];
-    if (blockIdx.x == 0) bin_start[b] = run;
+    on_bin(b, run);
+    if (publish) bin_start[b] = run;
     run += bin_total[b];
   }
-  if (blockIdx.x == 0) {
+  if (publish) {
     int tot_sub;
     int sbase = block_exclusive_scan(nsub, &tot_sub, s_warp);
     int st = first_start;
@@ -233,6 +232,27 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_scatter_kernel(
       *num_sub = min(tot_sub, max_sub);
     }
   }
+}
+
+// Sort pass 2: every block scans the bin totals itself (bin starts), block 0
+// also publishes them and the subproblem table; then each block hands out the
+// slots of its segments with shared-memory cursors (the counts are those of
+// pass 1, so every slot is written exactly once) and moves its records
+// there.  The last block to finish clears bin_total for the next sort.
+template <int D, typename T>
+__global__ void __launch_bounds__(kSortThreads, 2) sort_scatter_kernel(
+    const Rec<D, T>* __restrict__ unsorted, int64_t N, int64_t chunk, Geom g, int* bin_total,
+    const int* __restrict__ blk_off, int* bin_start, int* sub_bin, int* sub_start, int* sub_count, int* num_sub,
+    int max_sub, unsigned* done, Rec<D, T>* out, int* status) {
+  extern __shared__ int sh_cur[];
+  __shared__ int s_warp[32];
+  __shared__ bool s_last;
+  const int nbins = int(g.nbins());
+  const int tid = threadIdx.x;
+  const int* my_off = blk_off + int64_t(blockIdx.x) * nbins;
+  // bins this block has no points in get stale offsets that are never used
+  scan_bins(bin_total, nbins, blockIdx.x == 0, bin_start, sub_bin, sub_start, sub_count, num_sub, max_sub, s_warp,
+            [&](int b, int start) { sh_cur[b] = start + my_off[b]; });
   __syncthreads();
   const int64_t j0 = int64_t(blockIdx.x) * chunk, j1 = min(N, j0 + chunk);
   for (int64_t jb = j0 + tid; jb < j1; jb += kSortBatch * int64_t(blockDim.x)) {
@@ -253,6 +273,166 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_scatter_kernel(
         continue;
       }
       out[dest] = r[u];
+    }
+  }
+  // every block has read bin_total before it counts itself done
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    for (int b = tid; b < nbins; b += blockDim.x) bin_total[b] = 0;
+    if (tid == 0) *done = 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One-pass bin sort: one cooperative launch (every block resident at once)
+// does what the two passes above do, with each point's record crossing HBM
+// once each way.  Block b maps the points [b chunk, (b + 1) chunk) and keeps
+// them in shared memory (cell, fractions; struct of arrays) with their rank
+// inside the block's share of their bin (shared histogram atomics).  It
+// reserves its segment in every non-empty bin with one global atomic, lists
+// its points in bin order (block-local exclusive scan of its histogram) and
+// waits at a grid-wide barrier (a monotonic arrival counter, bounded by
+// kGridBarrierNs).  Then every block scans the bin totals, block 0 publishes
+// the bin starts and the subproblem table, and each block writes its records
+// in bin order, so that its run of points in one bin goes out as one
+// contiguous stretch.  The last block to finish clears the bin totals.  A
+// barrier that gives up raises STATUS_TIMEOUT together with
+// STATUS_NONFINITE_INPUT, which makes the evaluation's energy and gradient
+// NaN, and the block writes no records.
+// ---------------------------------------------------------------------------
+constexpr int kOneThreads = 1024;
+constexpr uint64_t kGridBarrierNs = 2000000000ull;
+
+// Waits until all blocks of this launch have arrived: launch k's blocks take
+// the tickets [k n, (k + 1) n) of the counter, which only grows.  Returns false
+// if the wait gave up after kGridBarrierNs.
+__device__ __forceinline__ bool grid_barrier(unsigned long long* bar, unsigned nblocks) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned long long ticket = atomicAdd(bar, 1ull);
+    const unsigned long long target = (ticket / nblocks + 1) * nblocks;
+    const uint64_t t0 = global_ns();
+    int ok = 1;
+    for (;;) {
+      unsigned long long v;
+      asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(bar) : "memory");
+      if (v >= target) break;
+      if (global_ns() - t0 > kGridBarrierNs) {
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Shared memory of the one-pass sort: three int arrays of nbins (rounded up
+// to 16 bytes) and, per point, its fractions, cell, rank and bin-order index.
+template <int D, typename T>
+__host__ __device__ constexpr size_t onepass_point_bytes() {
+  return D * sizeof(T) + sizeof(uint32_t) + 2 * sizeof(uint16_t);
+}
+__host__ __device__ inline size_t onepass_bin_bytes(int nbins) { return (size_t(3 * nbins) * sizeof(int) + 15) & ~size_t(15); }
+
+template <int D, typename T>
+__global__ void __launch_bounds__(kOneThreads, 1) sort_onepass_kernel(
+    const double* __restrict__ pts, int64_t N, int64_t chunk, MapParams mp, Geom g, int* bin_total, int* bin_start,
+    int* sub_bin, int* sub_start, int* sub_count, int* num_sub, int max_sub, unsigned* done,
+    unsigned long long* bar, Rec<D, T>* out, int* status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_warp[32];
+  __shared__ bool s_last;
+  const int nbins = int(g.nbins());
+  const int tid = threadIdx.x;
+  int* hist = reinterpret_cast<int*>(smem_raw);  // block's bin counts, then its segment offsets
+  int* lstart = hist + nbins;                    // block-local bin starts
+  int* gstart = lstart + nbins;                  // global bin starts
+  T* fr = reinterpret_cast<T*>(smem_raw + onepass_bin_bytes(nbins));  // D arrays of chunk fractions
+  uint32_t* cell = reinterpret_cast<uint32_t*>(fr + D * chunk);
+  uint16_t* rank = reinterpret_cast<uint16_t*>(cell + chunk);
+  uint16_t* inv = rank + chunk;
+
+  for (int b = tid; b < nbins; b += blockDim.x) hist[b] = 0;
+  __syncthreads();
+  const int64_t j0 = int64_t(blockIdx.x) * chunk, j1 = min(N, j0 + chunk);
+  const int cnt = j1 > j0 ? int(j1 - j0) : 0;
+  bool bad = false;
+  for (int64_t jb = j0 + tid; jb < j1; jb += kSortBatch * int64_t(blockDim.x)) {
+    double p[kSortBatch][D];
+    load_batch<D>(pts, jb, j1, blockDim.x, mp.stride, p);
+#pragma unroll
+    for (int u = 0; u < kSortBatch; ++u) {
+      const int64_t j = jb + u * int64_t(blockDim.x);
+      if (j >= j1) break;
+      int c[3] = {0, 0, 0};
+      double f[3] = {0, 0, 0};
+      bool ok;
+      const int bin = point_bin<D>(p[u], mp, g, c, f, ok);
+      bad |= !ok;
+      const int i = int(j - j0);
+      rank[i] = uint16_t(atomicAdd(&hist[bin], 1));
+      cell[i] = pack_cell(D, c[0], c[1], c[2]);
+#pragma unroll
+      for (int a = 0; a < D; ++a) fr[a * chunk + i] = T(f[a]);
+    }
+  }
+  if (bad) raise_status(status, STATUS_NONFINITE_INPUT);
+  __syncthreads();
+  {  // block-local bin starts
+    const int per = (nbins + int(blockDim.x) - 1) / int(blockDim.x);
+    const int b0 = min(nbins, tid * per), b1 = min(nbins, b0 + per);
+    int mine = 0;
+    for (int b = b0; b < b1; ++b) mine += hist[b];
+    int tot;
+    int run = block_exclusive_scan(mine, &tot, s_warp);
+    for (int b = b0; b < b1; ++b) {
+      lstart[b] = run;
+      run += hist[b];
+    }
+  }
+  __syncthreads();
+  for (int b = tid; b < nbins; b += blockDim.x) {
+    const int c = hist[b];
+    if (c) hist[b] = atomicAdd(&bin_total[b], c);  // the block's segment inside bin b
+  }
+  for (int i = tid; i < cnt; i += blockDim.x) {
+    int c[3];
+    unpack_cell(D, cell[i], c[0], c[1], c[2]);
+    inv[lstart[bin_of_cell<D>(c, g)] + rank[i]] = uint16_t(i);
+  }
+  const bool arrived = grid_barrier(bar, gridDim.x);
+  if (!arrived) {
+    if (tid == 0) raise_status(status, STATUS_TIMEOUT | STATUS_NONFINITE_INPUT);
+  } else {
+    scan_bins(bin_total, nbins, blockIdx.x == 0, bin_start, sub_bin, sub_start, sub_count, num_sub, max_sub, s_warp,
+              [&](int b, int start) { gstart[b] = start; });
+    __syncthreads();
+    for (int q = tid; q < cnt; q += blockDim.x) {
+      const int i = inv[q];
+      int c[3];
+      unpack_cell(D, cell[i], c[0], c[1], c[2]);
+      const int bin = bin_of_cell<D>(c, g);
+      const int64_t dest = int64_t(gstart[bin]) + hist[bin] + (q - lstart[bin]);
+      if (dest < 0 || dest >= N) {
+        raise_status(status, STATUS_OVERFLOW);
+        continue;
+      }
+      Rec<D, T> r;
+      r.cell = cell[i];
+#pragma unroll
+      for (int a = 0; a < D; ++a) r.f[a] = fr[a * chunk + i];
+      r.idx = uint32_t(j0 + i);
+      out[dest] = r;
     }
   }
   // every block has read bin_total before it counts itself done
@@ -955,11 +1135,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
 // Waits for phase `parity` of the barrier for at most `ns` nanoseconds.
 __device__ __forceinline__ bool mbar_wait_timed(uint64_t* bar, unsigned parity, uint64_t ns) {
   const uint64_t t0 = global_ns();
@@ -1302,6 +1477,39 @@ inline int point_grid(int64_t n, int per_sm = 8) {
   return int(std::min<int64_t>(want, int64_t(sm_count()) * per_sm));
 }
 
+// Decides (once per point count) whether the one-pass sort can run: a
+// cooperative launch of at most one 1024-thread block per SM whose chunk of
+// points fits in shared memory next to the bin arrays (config 2's 2^20
+// points over 148 SMs: 7085 points, 126 KB in FP32, 182 KB in FP64).
+// The barrier's tickets assume one block count for every launch on a
+// counter, so the configuration is fixed at the first sort; a later sort of
+// another point count uses the two-pass sort.
+template <int D, typename T>
+bool onepass_setup(SortBufs& sb, int64_t N, const Geom& g) {
+  if (sb.one_blocks >= 0) return sb.one_blocks > 0 && sb.one_N == N;
+  sb.one_blocks = 0;
+  sb.one_N = N;
+  if (N < 1) return false;
+  int dev = 0, coop = 0, smem_max = 0;
+  FB_CUDA(cudaGetDevice(&dev));
+  FB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  FB_CUDA(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (!coop) return false;
+  const int blocks = int(std::min<int64_t>(sm_count(), ceil_div(N, kOneThreads)));
+  const int64_t chunk = ceil_div(N, blocks);
+  const size_t smem = onepass_bin_bytes(int(g.nbins())) + size_t(chunk) * onepass_point_bytes<D, T>();
+  if (chunk > 65535 || smem + 1024 > size_t(smem_max)) return false;
+  auto kern = sort_onepass_kernel<D, T>;
+  FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  int occ = 0;
+  FB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kOneThreads, smem));
+  if (occ < 1 || blocks > occ * sm_count()) return false;
+  sb.one_blocks = blocks;
+  sb.one_chunk = chunk;
+  sb.one_smem = smem;
+  return true;
+}
+
 template <int D, typename T>
 void bin_sort_d(const double* pts, int64_t N, const MapParams& mp, const Geom& g, SortBufs& sb, void* recs, int* status,
                 cudaStream_t s) {
@@ -1313,6 +1521,22 @@ void bin_sort_d(const double* pts, int64_t N, const MapParams& mp, const Geom& g
   for (int a = 0; a < D; ++a) {
     m2.scale[a] = double(g.nf[a]) / mp.L[a];
     m2.invL[a] = 1.0 / mp.L[a];
+  }
+  if (onepass_setup<D, T>(sb, N, g)) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(sb.one_blocks));
+    cfg.blockDim = dim3(kOneThreads);
+    cfg.dynamicSmemBytes = sb.one_smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    FB_CUDA(cudaLaunchKernelEx(&cfg, sort_onepass_kernel<D, T>, pts, N, sb.one_chunk, m2, g, sb.bin_total.p,
+                               sb.bin_start.p, sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p,
+                               int(sb.max_sub), sb.done.p, sb.bar.p, static_cast<Rec<D, T>*>(recs), status));
+    return;
   }
   Rec<D, T>* unsorted = reinterpret_cast<Rec<D, T>*>(sb.unsorted.p);
   if (smem > 48 * 1024) {
