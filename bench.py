@@ -308,6 +308,22 @@ def other_configs_report(args, dev):
     for prec in ("fp32", "fp64"):
         out["config4_uwnu"][prec] = rate(UwNU(np.array([gu, gu]), kp, sku, np.ones(mk), np.ones(2), eps=EPS,
                                               precision=prec), xu)
+    # NUwNU with many k-points: the type-3 NUFFT path (points x k-points >= 2^22 pairs)
+    from fresco_b200 import NUwNU
+
+    rng = np.random.default_rng(6)
+    n6, m6 = 1 << 16, 100_000
+    x6 = rng.random(2 * n6)
+    k6 = ((rng.random((m6, 2)) * 2 - 1) * 64.0).ravel()
+    s6 = rng.random(m6) * n6 * (rng.random(m6) < 0.3)
+    out["nuwnu_type3"] = {"workload": "NUwNU, N=65536 points uniform in [0,1)^2 (L=1), 100,000 k-points uniform in "
+                                      "[-64,64]^2, S0 random, V=1, type-3 NUFFT both ways"}
+    for prec, eps in (("fp32", EPS), ("fp64", 1e-12)):
+        pot6 = NUwNU(np.ones(n6), k6, s6, np.ones(m6), np.ones(2), eps=eps, precision=prec)
+        out["nuwnu_type3"][prec] = rate(pot6, x6)
+        out["nuwnu_type3"][prec]["eps"] = eps
+        out["nuwnu_type3"]["setup"] = pot6.describe()
+        del pot6
     x1, r1, sk1, v1, l1 = stealthy_inputs(4096, 32, 16, seed=1)
     out["config1_nuwu"] = {"workload": "2D NUwU, N=4096, 65^2 modes, S0=0 & V=1 on 0<|k|<=16, eps=1e-12",
                            "fp64": rate(NUwU(r1, 32, sk1.ravel(), v1.ravel(), l1, eps=1e-12, precision="fp64"), x1)}

@@ -123,4 +123,35 @@ std::vector<double> es_poly_coefficients(const ESParams& es, int W) {
   return out;
 }
 
+double es_fourier(const ESParams& es, double z) {
+  static thread_local int cached_n = 0;
+  static thread_local std::vector<double> xq, wq;
+  const int nq = std::max(64, 8 * es.w + 64) + int(std::ceil(std::fabs(z)));
+  if (nq != cached_n) {
+    gauss_legendre(nq, xq, wq);
+    cached_n = nq;
+  }
+  double s = 0.0;
+  for (int q = 0; q < nq; ++q) s += wq[q] * es_phi(xq[q], es.beta) * std::cos(z * xq[q]);
+  return s;
+}
+
+std::vector<double> es_fourier_chebyshev(const ESParams& es, double zmax) {
+  const double pi = 3.14159265358979323846;
+  // F is entire and of exponential type 1 in z: on [-zmax, zmax] its Chebyshev
+  // coefficients fall off once the degree passes zmax; 40 more terms reach
+  // the FP64 level
+  const int n = int(std::ceil(zmax)) + 40;
+  const int m = 2 * n + 16;  // Chebyshev nodes of the interpolant
+  std::vector<double> f(m);
+  for (int j = 0; j < m; ++j) f[j] = es_fourier(es, zmax * std::cos(pi * (j + 0.5) / m));
+  std::vector<double> c(n + 1);
+  for (int k = 0; k <= n; ++k) {
+    double sum = 0.0;
+    for (int j = 0; j < m; ++j) sum += f[j] * std::cos(k * pi * (j + 0.5) / m);
+    c[k] = (k == 0 ? 1.0 : 2.0) * sum / m;
+  }
+  return c;
+}
+
 }  // namespace fb

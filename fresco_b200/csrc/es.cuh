@@ -43,6 +43,16 @@ std::vector<double> es_correction(const ESParams& es, int64_t nf, int64_t kmin, 
 // Gauss-Legendre nodes/weights on [-1, 1] (Newton iteration on P_n).
 void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& wts);
 
+// Fourier transform of the kernel on its own support, F(z) = int_{-1}^{1}
+// phi(t) cos(z t) dt (Gauss-Legendre quadrature, FP64).  A kernel of
+// half-width a in some coordinate has the transform a F(xi a) at xi.
+double es_fourier(const ESParams& es, double z);
+
+// Chebyshev coefficients c_0..c_n of F on [-zmax, zmax] (F(z) = sum_k c_k
+// T_k(z / zmax)), n large enough that the series matches F to about 1e-15
+// relative to F(0) there; evaluated on the device by Clenshaw's recurrence.
+std::vector<double> es_fourier_chebyshev(const ESParams& es, double zmax);
+
 // Host evaluation of phi(t) (for tests and the quadrature).
 inline double es_phi(double t, double beta) {
   const double a = 1.0 - t * t;

@@ -19,12 +19,14 @@
 #include <cuda.h>
 
 #include <cmath>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
 
 #include "potential.cuh"
+#include "type3.cuh"
 
 namespace fb {
 
@@ -45,7 +47,8 @@ __global__ void __launch_bounds__(kThreads) nuwnu_forward_kernel(const double* _
                                                                   const double* __restrict__ s, int64_t M,
                                                                   const double* __restrict__ c, double cu,
                                                                   double L0, double L1, double L2, double2* rho,
-                                                                  int* status) {
+                                                                  int* status, const int* __restrict__ only_if) {
+  if (only_if != nullptr && *only_if == 0) return;  // runs only when the type-3 path declined this evaluation
   // frequency chunks k0 = blockIdx.y * kFreqChunk + gridDim.y * kFreqChunk * t
   // (gridDim.y is capped at the launch limit, 65535)
   __shared__ double red[2 * kFreqChunk][kThreads / 32];
@@ -126,7 +129,9 @@ __global__ void __launch_bounds__(kThreads) nuwnu_adjoint_kernel(const double* _
                                                                   const double2* __restrict__ factor, double L0,
                                                                   double L1, double L2, double* grad, int accumulate,
                                                                   const int* __restrict__ status,
-                                                                  const double* __restrict__ c, double cu, int exact) {
+                                                                  const double* __restrict__ c, double cu, int exact,
+                                                                  const int* __restrict__ only_if) {
+  if (only_if != nullptr && *only_if == 0) return;  // runs only when the type-3 path declined this evaluation
   __shared__ double ss[kAdjTile * D];
   __shared__ double2 sf[kAdjTile];
   const double Ls[3] = {L0, L1, L2};
@@ -177,11 +182,78 @@ __global__ void __launch_bounds__(kThreads) nuwnu_adjoint_kernel(const double* _
   }
 }
 
-template <int D>
+// Type-3 path helpers.  rho is zeroed for the direct fallback when the
+// window flag says the type-3 result is not to be used.
+__global__ void nuwnu_zero_if_kernel(double2* rho, int64_t M, const int* __restrict__ flag) {
+  if (*flag == 0) return;
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < M; k += int64_t(gridDim.x) * blockDim.x)
+    rho[k] = make_double2(0.0, 0.0);
+}
+
+// Adjoint strengths: vector a holds s_k[a] factor_k (nuwnu.hpp:231-282).
+__global__ void __launch_bounds__(kThreads) nuwnu_t3_strength_kernel(const double* __restrict__ s, int64_t M, int D,
+                                                                     const double2* __restrict__ factor,
+                                                                     double2* str) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < M * D; i += int64_t(gridDim.x) * blockDim.x) {
+    const int a = int(i / M);
+    const int64_t k = i - int64_t(a) * M;
+    const double2 f = factor[k];
+    const double sa = s[k * D + a];
+    str[i] = make_double2(sa * f.x, sa * f.y);
+  }
+}
+
+// grad[D j + a] (+)= Re(out_a(x_j)) (nuwnu.hpp:269, no conj(c_j)); the exact
+// derivative multiplies by c_j 2 pi / L.  Skipped when the window flag sent
+// the evaluation to the direct sums.
+__global__ void __launch_bounds__(kThreads) nuwnu_t3_grad_kernel(const double2* __restrict__ out, int64_t N, int D,
+                                                                 const int* __restrict__ flag,
+                                                                 const int* __restrict__ status,
+                                                                 const double* __restrict__ c, double cu, int exact,
+                                                                 double L0, double L1, double L2, double* grad,
+                                                                 int accumulate) {
+  if (*flag != 0) return;
+  const bool bad = (*status) & STATUS_NONFINITE_INPUT;
+  const double Ls[3] = {L0, L1, L2};
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N * D; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t j = i / D;
+    const int a = int(i - j * D);
+    double v = out[int64_t(a) * N + j].x;
+    if (exact) v *= (c ? c[j] : cu) * 2 * kPi / Ls[a];
+    if (bad) v = __longlong_as_double(0x7ff8000000000000ULL);
+    grad[i] = accumulate ? grad[i] + v : v;
+  }
+}
+
+// Evaluations with at least this many (point, k-point) pairs use the type-3
+// NUFFT; fewer are cheaper as direct sums.
+constexpr double kType3MinPairs = double(1 << 22);
+
+// Range of the reference's coordinate map x = (p - round(p/L) + L) 2 pi / L
+// (nuwnu.hpp:134) over p in [-L, 2L): the window the type-3 plans cover.
+// Points beyond it send that evaluation to the direct sums.
+void nuwnu_map_window(double L, double& lo, double& hi) {
+  lo = INFINITY;
+  hi = -INFINITY;
+  for (int k = -1; k <= 2; ++k) {
+    const double pl = std::max(-L, (k - 0.5) * L), ph = std::min(2.0 * L, (k + 0.5) * L);
+    if (!(ph > pl)) continue;
+    for (double p : {pl, ph}) {
+      const double x = (p - k + L) * 2 * kPi / L;
+      lo = std::min(lo, x);
+      hi = std::max(hi, x);
+    }
+  }
+  const double m = 1e-9 * (hi - lo) + 1e-12;
+  lo -= m;
+  hi += m;
+}
+
+template <int D, typename T>
 class NUwNUImpl final : public Potential {
  public:
   NUwNUImpl(const std::vector<double>& radii, const std::vector<double>& kpts, const std::vector<double>& sk,
-            const std::vector<double>& v, const std::vector<double>& L)
+            const std::vector<double>& v, const std::vector<double>& L, double eps)
       : N_(int64_t(radii.size())) {
     init_status();
     if (sk.size() != v.size()) throw InvalidArgument("len(Sk) must equal len(V)");
@@ -219,13 +291,41 @@ class NUwNUImpl final : public Potential {
       FB_CUDA(cudaMemcpy(sk_.p, sk.data(), sizeof(double) * M_, cudaMemcpyHostToDevice));
       FB_CUDA(cudaMemcpy(v_.p, v.data(), sizeof(double) * M_, cudaMemcpyHostToDevice));
     }
+    // type-3 NUFFT plans: forward (points -> k-points, iflag +1, nuwnu.hpp:77,
+    // 165) and adjoint (k-points -> points, iflag -1, nuwnu.hpp:78, 231-282);
+    // the k-points are sorted and their factors computed once here
+    if (N_ > 0 && M_ > 0 && double(N_) * double(M_) >= kType3MinPairs) {
+      double xlo[3], xhi[3], klo[3], khi[3];
+      for (int a = 0; a < D; ++a) {
+        nuwnu_map_window(L_[a], xlo[a], xhi[a]);
+        klo[a] = INFINITY;
+        khi[a] = -INFINITY;
+        for (int64_t k = 0; k < M_; ++k) {
+          klo[a] = std::min(klo[a], kpts[size_t(k * D + a)]);
+          khi[a] = std::max(khi[a], kpts[size_t(k * D + a)]);
+        }
+        if (!std::isfinite(klo[a]) || !std::isfinite(khi[a])) throw InvalidArgument("non-finite k-point");
+      }
+      fwd_.reset(new Type3<T>(D, N_, M_, xlo, xhi, klo, khi, +1, eps, 1));
+      adj_.reset(new Type3<T>(D, M_, N_, klo, khi, xlo, xhi, -1, eps, D));
+      fwd_->set_targets(s_.p, TYPE3_IDENTITY, nullptr, nullptr);
+      adj_->set_sources(s_.p, TYPE3_IDENTITY, nullptr, nullptr);
+      t3str_.alloc(M_ * D);
+      t3out_.alloc(N_ * D);
+      FB_CUDA(cudaDeviceSynchronize());
+    }
   }
 
   int64_t ndof() const override { return N_ * D; }
   std::string kind() const override { return "NUwNU"; }
   std::string describe() const override {
-    return "NUwNU D=" + std::to_string(D) + " N=" + std::to_string(N_) + " kpoints=" + std::to_string(M_) +
-           " exact FP64 direct sums";
+    std::string s = "NUwNU D=" + std::to_string(D) + " N=" + std::to_string(N_) + " kpoints=" + std::to_string(M_);
+    if (fwd_)
+      s += std::string(" precision=") + (sizeof(T) == 4 ? "fp32" : "fp64") + " forward " + fwd_->describe() +
+           " adjoint " + adj_->describe() + " (exact sums for points outside the planned window)";
+    else
+      s += " exact FP64 direct sums";
+    return s;
   }
 
   void energy(const double* x, int64_t n, double* e, bool acc, cudaStream_t s) override { run(x, nullptr, e, acc, s); }
@@ -242,20 +342,40 @@ class NUwNUImpl final : public Potential {
       if (g && !acc) FB_CUDA(cudaMemsetAsync(g, 0, sizeof(double) * N_ * D, s));
       return;
     }
-    FB_CUDA(cudaMemsetAsync(rho_.p, 0, sizeof(double2) * M_, s));
     const int pblocks = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(N_, kThreads), 2 * int64_t(sm_count()))));
     dim3 fg(pblocks, unsigned(std::min<int64_t>(ceil_div(M_, kFreqChunk), 65535)));
-    nuwnu_forward_kernel<D><<<fg, kThreads, 0, s>>>(x, N_, s_.p, M_, c_.p, cu_, L_[0], L_[1], L_[2], rho_.p,
-                                                    status_.p);
-    FB_LAUNCH_CHECK();
     const int mg = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(M_, kThreads), int64_t(sm_count()) * 4)));
+    const int* flag = nullptr;
+    if (fwd_) {
+      // type 3; the direct sums run instead when a point is outside the plans' window
+      fwd_->set_sources(x, TYPE3_NUWNU_MAP, L_, s);
+      fwd_->execute_real(c_.p, cu_, rho_.p, s);
+      flag = fwd_->window_flag();
+      nuwnu_zero_if_kernel<<<mg, kThreads, 0, s>>>(rho_.p, M_, flag);
+      FB_LAUNCH_CHECK();
+    } else {
+      FB_CUDA(cudaMemsetAsync(rho_.p, 0, sizeof(double2) * M_, s));
+    }
+    nuwnu_forward_kernel<D><<<fg, kThreads, 0, s>>>(x, N_, s_.p, M_, c_.p, cu_, L_[0], L_[1], L_[2], rho_.p,
+                                                    status_.p, flag);
+    FB_LAUNCH_CHECK();
     nuwnu_loss_kernel<<<mg, kThreads, 0, s>>>(rho_.p, M_, 1.0 / double(N_), sk_.p, v_.p, e, factor_.p, status_.p);
     FB_LAUNCH_CHECK();
     timer_mark("forward", s);
     if (!g) return;
     const int ag = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(N_, kThreads), int64_t(sm_count()) * 8)));
+    if (adj_) {
+      const int sg = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(M_ * D, kThreads), int64_t(sm_count()) * 8)));
+      nuwnu_t3_strength_kernel<<<sg, kThreads, 0, s>>>(s_.p, M_, D, factor_.p, t3str_.p);
+      FB_LAUNCH_CHECK();
+      adj_->set_targets(x, TYPE3_NUWNU_MAP, L_, s);
+      adj_->execute_cplx(t3str_.p, t3out_.p, s);
+      nuwnu_t3_grad_kernel<<<ag, kThreads, 0, s>>>(t3out_.p, N_, D, flag, status_.p, c_.p, cu_,
+                                                   grad_mode_ == 1 ? 1 : 0, L_[0], L_[1], L_[2], g, acc ? 1 : 0);
+      FB_LAUNCH_CHECK();
+    }
     nuwnu_adjoint_kernel<D><<<ag, kThreads, 0, s>>>(x, N_, s_.p, M_, factor_.p, L_[0], L_[1], L_[2], g,
-                                                    acc ? 1 : 0, status_.p, c_.p, cu_, grad_mode_ == 1 ? 1 : 0);
+                                                    acc ? 1 : 0, status_.p, c_.p, cu_, grad_mode_ == 1 ? 1 : 0, flag);
     FB_LAUNCH_CHECK();
     timer_mark("adjoint", s);
   }
@@ -265,6 +385,8 @@ class NUwNUImpl final : public Potential {
   double cu_ = 1.0;
   DevBuf<double> c_, s_, sk_, v_;
   DevBuf<double2> rho_, factor_;
+  std::unique_ptr<Type3<T>> fwd_, adj_;  // null: direct sums only
+  DevBuf<double2> t3str_, t3out_;        // adjoint strengths (D x M), outputs (D x N)
 };
 
 }  // namespace
@@ -364,7 +486,7 @@ void noalloc_launch(const double* x, int64_t N, const double* c, const double* s
   const double L0 = L[0], L1 = D > 1 ? L[1] : 1.0, L2 = D > 2 ? L[2] : 1.0;
   const int pblocks = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(N, kThreads), 2 * int64_t(sm_count()))));
   dim3 fg(pblocks, unsigned(ceil_div(M, kFreqChunk)));
-  nuwnu_forward_kernel<D><<<fg, kThreads, 0, st>>>(x, N, s, M, c, 1.0, L0, L1, L2, rho, status);
+  nuwnu_forward_kernel<D><<<fg, kThreads, 0, st>>>(x, N, s, M, c, 1.0, L0, L1, L2, rho, status, nullptr);
   FB_LAUNCH_CHECK();
   const int mg = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(M, kThreads), int64_t(sm_count()) * 4)));
   nuwnu_loss_kernel<<<mg, kThreads, 0, st>>>(rho, M, 1.0 / double(N), sk, v, e, factor, status);
@@ -372,7 +494,7 @@ void noalloc_launch(const double* x, int64_t N, const double* c, const double* s
   if (!g) return;
   const int ag = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(N, kThreads), int64_t(sm_count()) * 8)));
   nuwnu_adjoint_kernel<D><<<ag, kThreads, 0, st>>>(x, N, s, M, factor, L0, L1, L2, g, acc ? 1 : 0, status, c, 1.0,
-                                                   mode == 1 ? 1 : 0);
+                                                   mode == 1 ? 1 : 0, nullptr);
   FB_LAUNCH_CHECK();
 }
 
@@ -414,12 +536,15 @@ void nuwnu_energy_gradient_noalloc(const double* d_x, int64_t n_points, int ndim
 PotentialPtr make_nuwnu(const std::vector<double>& radii, const std::vector<double>& kpts,
                         const std::vector<double>& sk, const std::vector<double>& v, const std::vector<double>& L,
                         double eps, int precision) {
-  (void)eps;
-  (void)precision;
   const int D = int(L.size());
-  if (D == 1) return PotentialPtr(new NUwNUImpl<1>(radii, kpts, sk, v, L));
-  if (D == 2) return PotentialPtr(new NUwNUImpl<2>(radii, kpts, sk, v, L));
-  if (D == 3) return PotentialPtr(new NUwNUImpl<3>(radii, kpts, sk, v, L));
+  const bool f32 = precision == 1;
+#define FB_NUWNU(DD)                                                             \
+  return f32 ? PotentialPtr(new NUwNUImpl<DD, float>(radii, kpts, sk, v, L, eps)) \
+             : PotentialPtr(new NUwNUImpl<DD, double>(radii, kpts, sk, v, L, eps))
+  if (D == 1) FB_NUWNU(1);
+  if (D == 2) FB_NUWNU(2);
+  if (D == 3) FB_NUWNU(3);
+#undef FB_NUWNU
   throw std::runtime_error("Invalid dimension: " + std::to_string(D));
 }
 
