@@ -55,6 +55,44 @@ __device__ inline void raise_status(int* st, int bit) {
   atomicOr(st + 1, bit);
 }
 
+// Nanoseconds of the GPU's global timer (bounds for waits).
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Grid-wide barrier for cooperative launches (every block resident at once).
+constexpr uint64_t kGridBarrierNs = 2000000000ull;
+
+// Waits until all blocks of this launch have arrived: launch k's blocks take
+// the tickets [k n, (k + 1) n) of the counter, which only grows.  Returns false
+// if the wait gave up after kGridBarrierNs.
+__device__ __forceinline__ bool grid_barrier(unsigned long long* bar, unsigned nblocks) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned long long ticket = atomicAdd(bar, 1ull);
+    const unsigned long long target = (ticket / nblocks + 1) * nblocks;
+    const uint64_t t0 = global_ns();
+    int ok = 1;
+    for (;;) {
+      unsigned long long v;
+      asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(bar) : "memory");
+      if (v >= target) break;
+      if (global_ns() - t0 > kGridBarrierNs) {
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
 // RAII device buffer (cudaMalloc'ed once at set-up, never on the evaluation path).
 template <typename T>
 struct DevBuf {

@@ -79,6 +79,7 @@ struct LbState {
   double f, fnew, rms, H0, stepnorm, factor;
   double inv_sqrt_n, maxstep, max_f_rise;
   int k, nred, accepted, rel, M;
+  int fault;  // a grid barrier of the fused direction kernel gave up (the iteration is void)
 };
 
 enum LbSlot { S_IN = 0, S_OUT = 1, S_SG = 2, S_SS = 3, S_GG = 4, S_YS = 5, S_YY = 6, S_TMP = 7, S_NSLOT = 8 };
@@ -157,6 +158,113 @@ __global__ void lb_update(int forward, int last, double* __restrict__ step, cons
   }
 }
 
+// The whole two-loop recursion of an iteration with stored pairs (k > 0,
+// lbfgs.cpp:126-169) in one cooperative launch.  Block b keeps its slice
+// [b chunk, (b + 1) chunk) of the step in shared memory from the copy of g
+// to the final scaling, so the step is neither re-read nor re-written
+// between the updates; each memory vector is read once in each loop.  Every
+// dot product is the sum of the blocks' partials, taken after a grid barrier
+// in block order, so all blocks use the same coefficient; the element-wise
+// updates are those of lb_start / lb_update.  At the end the step goes to
+// HBM and the line-search dots step.g, step.step are left in their slots,
+// padded with zeros to the P partials that lb_trial sums.  A barrier that
+// gives up sets st->fault.
+constexpr int kDirThreads = 1024;
+
+__global__ void __launch_bounds__(kDirThreads, 1) lb_direction_kernel(
+    const double* __restrict__ g, const double* __restrict__ sm, const double* __restrict__ ym, int64_t n,
+    int64_t chunk, int k, int M, LbState* st, const double* __restrict__ rho, double* alpha, double* part, int P,
+    unsigned long long* bar, double* __restrict__ step) {
+  extern __shared__ __align__(16) double q[];  // this block's slice of the step
+  __shared__ double alph[64];                   // alpha_i of the backward loop (M <= 64)
+  const int B = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+  const int64_t e0 = int64_t(b) * chunk, e1 = min(n, e0 + chunk);
+  const int cnt = e1 > e0 ? int(e1 - e0) : 0;
+  const int jmin = max(0, k - M), jmax = k, m = jmax - jmin;
+  bool ok = true;
+  // the sum over the blocks of slot `slot` (fixed order; same value in every block)
+  auto total = [&](int slot) { return sum_parts(part + int64_t(slot) * P, B); };
+  auto partial = [&](double v, int slot) {
+    double w[1] = {v};
+    const int sl[1] = {slot};
+    block_partials<1>(w, part, P, sl);
+  };
+  // lb_start: step = g, first backward dot s_i0 . g
+  {
+    const double* s0 = sm + int64_t((jmax - 1) % M) * n + e0;
+    double v = 0.0;
+    for (int i = tid; i < cnt; i += blockDim.x) {
+      const double gi = g[e0 + i];
+      q[i] = gi;
+      v += s0[i] * gi;
+    }
+    partial(v, S_IN);
+  }
+  ok &= grid_barrier(bar, B);
+  int in_slot = S_IN, out_slot = S_OUT;
+  for (int t = 0; t < m; ++t) {  // backward loop, newest pair first
+    const int j = jmax - 1 - t, mi = j % M;
+    const bool last = t == m - 1;
+    const double coef = rho[mi] * total(in_slot);
+    if (tid == 0) alph[t] = coef;
+    if (b == 0 && tid == 0) alpha[mi] = coef;
+    const double* y = ym + int64_t(mi) * n + e0;
+    const double* dn = (last ? ym + int64_t(jmin % M) * n : sm + int64_t((j - 1) % M) * n) + e0;
+    const double h0 = -st->H0;
+    double v = 0.0;
+    for (int i = tid; i < cnt; i += blockDim.x) {
+      double sv = q[i] - coef * y[i];
+      if (last) sv *= h0;
+      q[i] = sv;
+      v += dn[i] * sv;
+    }
+    partial(v, out_slot);
+    ok &= grid_barrier(bar, B);
+    const int tmp = in_slot;
+    in_slot = out_slot;
+    out_slot = tmp;
+  }
+  __syncthreads();
+  for (int t = 0; t < m; ++t) {  // forward loop, oldest pair first
+    const int j = jmin + t, mi = j % M;
+    const bool last = t == m - 1;
+    const double beta = -rho[mi] * total(in_slot);
+    const double coef = alph[m - 1 - t] - beta;
+    const double* sv_ = sm + int64_t(mi) * n + e0;
+    if (!last) {
+      const double* dn = ym + int64_t((j + 1) % M) * n + e0;
+      double v = 0.0;
+      for (int i = tid; i < cnt; i += blockDim.x) {
+        const double sv = q[i] - coef * sv_[i];
+        q[i] = sv;
+        v += dn[i] * sv;
+      }
+      partial(v, out_slot);
+      ok &= grid_barrier(bar, B);
+      const int tmp = in_slot;
+      in_slot = out_slot;
+      out_slot = tmp;
+    } else {
+      double v[2] = {0.0, 0.0};
+      for (int i = tid; i < cnt; i += blockDim.x) {
+        const double sv = q[i] - coef * sv_[i];
+        step[e0 + i] = sv;
+        v[0] += sv * g[e0 + i];
+        v[1] += sv * sv;
+      }
+      const int sl[2] = {S_SG, S_SS};
+      block_partials<2>(v, part, P, sl);
+    }
+  }
+  // lb_trial sums P partials: the slots of the blocks this launch does not have are zero
+  if (b == 0)
+    for (int i = B + tid; i < P; i += blockDim.x) {
+      part[int64_t(S_SG) * P + i] = 0.0;
+      part[int64_t(S_SS) * P + i] = 0.0;
+    }
+  if (!ok && tid == 0) st->fault = 1;
+}
+
 // Trial point of the backtracking line search (lbfgs.cpp:176-204).
 __global__ void lb_trial(const double* __restrict__ xold, const double* __restrict__ step, double* __restrict__ xnew,
                          int64_t n, LbState* st, double* part, int P) {
@@ -233,6 +341,7 @@ __global__ void lb_finalize(LbState* st, const double* __restrict__ fnew_dev, do
   out[3] = st->H0;
   out[4] = printed;
   out[5] = fnew;
+  out[6] = st->fault;
 }
 
 // Initial f, rms (optimizer.hpp:203-210: rms = sqrt(|g|^2 / n)).
@@ -552,6 +661,21 @@ class Lbfgs final : public Optimizer {
       reduce(S_GG, 1);
       lb_first_step<<<P_, kThreads, 0, s_>>>(g, step_.p, n_, st_.p, part_.p, P_);
       reduce(S_SG, 2);
+    } else if (!reducer_ && direction_setup()) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(unsigned(dir_blocks_));
+      cfg.blockDim = dim3(kDirThreads);
+      cfg.dynamicSmemBytes = size_t(dir_chunk_) * sizeof(double);
+      cfg.stream = s_;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeCooperative;
+      attr[0].val.cooperative = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      FB_CUDA(cudaLaunchKernelEx(&cfg, lb_direction_kernel, static_cast<const double*>(g),
+                                 static_cast<const double*>(sm_.p), static_cast<const double*>(ym_.p), n_,
+                                 dir_chunk_, k_, M, st_.p, static_cast<const double*>(rho_.p), alpha_.p, part_.p, P_,
+                                 bar_.p, step_.p));
     } else {
       const int jmin = std::max(0, k_ - M), jmax = k_;
       const int m = jmax - jmin;
@@ -596,6 +720,7 @@ class Lbfgs final : public Optimizer {
       lb_finalize<<<1, 256, 0, s_>>>(st_.p, e_.p, rho_.p, kl, part_.p, P_, host_);
       FB_LAUNCH_CHECK();
       FB_CUDA(cudaStreamSynchronize(s_));
+      if (host_[6] != 0.0) throw std::runtime_error("LBFGS: a grid barrier of the direction kernel timed out");
       if (verbosity_ > 2 && host_[0] == 0.0) {
         std::printf("energy increased by %.17g to %.17g from %.17g\n", host_[5] - f_, host_[5], f_);
       }
@@ -667,9 +792,40 @@ class Lbfgs final : public Optimizer {
     reducer_(part_.p + int64_t(slot) * P_, int64_t(count) * P_, s_, reducer_ctx_);
   }
 
+  // Whether the fused direction kernel can run: a cooperative launch of at
+  // most one 1024-thread block per SM (and no more than the P partial slots)
+  // whose slice of the step fits in shared memory (config 2's 2^21
+  // coordinates over 148 SMs: 14,170 doubles, 113 KB per block).
+  bool direction_setup() {
+    if (dir_blocks_ >= 0) return dir_blocks_ > 0;
+    dir_blocks_ = 0;
+    if (prm_.M > 64) return false;
+    int dev = 0, coop = 0, smem_max = 0;
+    FB_CUDA(cudaGetDevice(&dev));
+    FB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    FB_CUDA(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (!coop) return false;
+    const int blocks = int(std::min<int64_t>({int64_t(sm_count()), int64_t(P_), ceil_div(n_, kDirThreads)}));
+    const int64_t chunk = ceil_div(n_, blocks);
+    const size_t smem = size_t(chunk) * sizeof(double);
+    if (smem + 2048 > size_t(smem_max)) return false;
+    FB_CUDA(cudaFuncSetAttribute(lb_direction_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int occ = 0;
+    FB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, lb_direction_kernel, kDirThreads, smem));
+    if (occ < 1 || blocks > occ * sm_count()) return false;
+    bar_.alloc(1);
+    FB_CUDA(cudaMemset(bar_.p, 0, sizeof(unsigned long long)));
+    dir_blocks_ = blocks;
+    dir_chunk_ = chunk;
+    return true;
+  }
+
   LbfgsParams prm_;
   DevBuf<double> X_[2], G_[2], step_, sm_, ym_, rho_, alpha_, e_;
   DevBuf<LbState> st_;
+  DevBuf<unsigned long long> bar_;  // grid-barrier arrivals of the direction kernel
+  int dir_blocks_ = -1;             // blocks of the direction kernel (0: the per-update kernels are used)
+  int64_t dir_chunk_ = 0;
   int cur_ = 0;
   int k_ = 0;
   double h0_ = 0.1;
