@@ -369,6 +369,110 @@ def config2_lbfgs500_report(x, radii, Sk, V, L, n_iter=500):
     return out
 
 
+ONLY_WORKLOADS = ("nuwu2d_fp32", "nuwu2d_fp64", "repulsion", "lbfgs", "nuwu3d_fp32", "nuwu3d_fp64", "uwu_fp32",
+                  "uwnu_fp32", "nuwnu_type3_fp32", "ensemble")
+
+
+def run_only(args):
+    """One workload of this file, evaluated --warmup + --steps times on one GPU with nothing else around it
+    (the command that the ncu captures under profiles/ profile), then one line with its mean time."""
+    import torch
+
+    from fresco_b200 import CombinedPotential, InversePower, NUwNU, NUwU, UwNU, UwU
+    from fresco_b200.optimize import LBFGS_CPP
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    name = args.only
+    x, radii, Sk, V, L = inputs(seed=2)
+    rr = np.full(N_POINTS, 0.25 / np.sqrt(N_POINTS) * 2 * np.pi)
+    if name in ("nuwu2d_fp32", "nuwu2d_fp64"):
+        pot = NUwU(radii, K_MODES, Sk, V, L, eps=EPS, precision=name[-4:])
+    elif name == "repulsion":
+        pot = InversePower(2.0, 1.0, rr, np.asarray(L, float), use_cell_lists=True)
+    elif name == "lbfgs":
+        pot = CombinedPotential()
+        pot.add_potential(NUwU(radii, K_MODES, Sk, V, L, eps=EPS, precision="fp32"))
+        pot.add_potential(InversePower(2.0, 1.0, rr, np.asarray(L, float), use_cell_lists=True))
+        opt = LBFGS_CPP(x, pot, tol=0.0)
+        opt.run(args.warmup)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        opt.run(args.steps)
+        torch.cuda.synchronize()
+        print(json.dumps({"only": name, "ms_per_iteration": 1e3 * (time.perf_counter() - t0) / args.steps}))
+        return
+    elif name.startswith("nuwu3d"):
+        rng = np.random.default_rng(3)
+        n3, k3 = 1 << 21, 64
+        x = rng.random(3 * n3) * 2 * np.pi
+        kv = np.arange(-k3, k3 + 1)
+        kz, ky, kx = np.meshgrid(kv, kv, kv, indexing="ij")
+        mag = np.sqrt(kx ** 2 + ky ** 2 + kz ** 2).ravel().astype(np.float64)
+        pot = NUwU(np.ones(n3), k3, 1.0 - np.exp(-((mag / 16.0) ** 2)), np.where(mag > 0, 1.0 / (1.0 + mag), 0.0),
+                   np.full(3, 2 * np.pi), eps=EPS, precision=name[-4:])
+    elif name == "uwu_fp32":
+        rng = np.random.default_rng(4)
+        g4 = 4096
+        x = rng.random(g4 * g4)
+        k = np.arange(g4) - g4 // 2
+        m4 = np.sqrt(k[:, None] ** 2 + k[None, :] ** 2)
+        v4 = ((m4 <= 64) & (m4 > 0)).astype(np.float64)
+        pot = UwU(np.array([g4, g4]), 64, np.zeros_like(v4), v4, np.ones(2), precision="fp32")
+    elif name == "uwnu_fp32":
+        rng = np.random.default_rng(4)
+        gu, mk = 2048, 100_000
+        x = rng.random(gu * gu)
+        r = 512 * np.sqrt(rng.random(mk))
+        t = 2 * np.pi * rng.random(mk)
+        kp = (np.stack([r * np.cos(t), r * np.sin(t)], axis=1) / gu).ravel()
+        sku = np.zeros(mk)
+        sku[rng.choice(mk, 64, replace=False)] = float(np.sum(x))
+        pot = UwNU(np.array([gu, gu]), kp, sku, np.ones(mk), np.ones(2), eps=EPS, precision="fp32")
+    elif name == "nuwnu_type3_fp32":
+        rng = np.random.default_rng(6)
+        n6, m6 = 1 << 16, 100_000
+        x = rng.random(2 * n6)
+        k6 = ((rng.random((m6, 2)) * 2 - 1) * 64.0).ravel()
+        s6 = rng.random(m6) * n6 * (rng.random(m6) < 0.3)
+        pot = NUwNU(np.ones(n6), k6, s6, np.ones(m6), np.ones(2), eps=EPS, precision="fp32")
+    elif name == "ensemble":
+        from fresco_b200 import NUwUEnsemble
+
+        pats, Le = ensemble_inputs()
+        ens = NUwUEnsemble([r for _, r, _, _, _ in pats], [K for _, _, K, _, _ in pats],
+                           [s for _, _, _, s, _ in pats], [v for _, _, _, _, v in pats], Le, eps=EPS,
+                           precision="fp32")
+        xs = [p[0] for p in pats]
+        dx = torch.tensor(ens.concat(xs), device=dev)
+        dg = torch.empty_like(dx)
+        de = torch.empty(ens.n_patterns, dtype=torch.float64, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        for _ in range(args.warmup):
+            ens.get_energies_gradient_device(dx, dg, de, stream)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ens.get_energies_gradient_device(dx, dg, de, stream)
+        torch.cuda.synchronize()
+        print(json.dumps({"only": name, "ms_per_eval": 1e3 * (time.perf_counter() - t0) / args.steps}))
+        return
+    else:
+        raise SystemExit(f"--only: unknown workload {name!r} (one of {', '.join(ONLY_WORKLOADS)})")
+    xt = torch.tensor(x, device=dev)
+    g = torch.empty_like(xt)
+    e = torch.zeros((), dtype=torch.float64, device=dev)
+    for _ in range(args.warmup):
+        pot.energy_gradient_device(xt, g, e)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        pot.energy_gradient_device(xt, g, e)
+    torch.cuda.synchronize()
+    print(json.dumps({"only": name, "ms_per_eval": 1e3 * (time.perf_counter() - t0) / args.steps,
+                      "setup": pot.describe()}))
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -810,11 +914,15 @@ def main():
                     help="skip the throughput of the other configurations' potentials")
     ap.add_argument("--no-ensemble-loop", action="store_true",
                     help="skip timing the ensemble's patterns as separate potentials")
+    ap.add_argument("--only", default=None, choices=ONLY_WORKLOADS,
+                    help="run one workload alone (warmup + steps evaluations; the profiling command)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.only:
+        run_only(args)
     else:
         run_ours(args)
 

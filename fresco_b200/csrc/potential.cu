@@ -21,6 +21,11 @@ void Potential::set_graphs_enabled(bool on) {
 
 void Potential::eval(const double* x, int64_t n, double* g, double* e, bool acc, cudaStream_t s) {
   auto direct = [&](cudaStream_t st) {
+    struct Flag {
+      bool& f;
+      explicit Flag(bool& r) : f(r) { f = true; }
+      ~Flag() { f = false; }
+    } in_eval(in_eval_);
     if (g) energy_gradient(x, n, g, e, acc, st);
     else energy(x, n, e, acc, st);
   };
@@ -142,12 +147,61 @@ void add_scalar(const double* src, double* dst, cudaStream_t s) {
   FB_LAUNCH_CHECK();
 }
 
+namespace {
+// g[i] += side[0][i] + side[1][i] + ... (in part order), e += the side energies.
+__global__ void combine_sides_kernel(double* g, int64_t n, const double* __restrict__ side, int nside, double* e,
+                                     const double* __restrict__ se) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    double v = g[i];
+    for (int k = 0; k < nside; ++k) v += side[int64_t(k) * n + i];
+    g[i] = v;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double v = *e;
+    for (int k = 0; k < nside; ++k) v += se[k];
+    *e = v;
+  }
+}
+}  // namespace
+
 CombinedPotential::CombinedPotential() { init_status(); }
+
+CombinedPotential::~CombinedPotential() {
+  for (cudaStream_t st : side_) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
+  for (cudaEvent_t ev : done_) cudaEventDestroy(ev);
+  if (fork_) cudaEventDestroy(fork_);
+}
 
 void CombinedPotential::add(PotentialPtr p) {
   if (!p) throw InvalidArgument("cannot add a null potential");
   parts_.push_back(std::move(p));
   invalidate_graphs();
+  const int64_t n = ndof();
+  if (parts_.size() >= 2 && n > 0) prepare_side(n);
+}
+
+// Side streams, events and scratch for the parts after the first, made when
+// a part is added (never on the evaluation path).
+void CombinedPotential::prepare_side(int64_t n) {
+  const size_t nside = parts_.size() - 1;
+  if (!fork_) FB_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+  while (side_.size() < nside) {
+    cudaStream_t st;
+    cudaEvent_t ev;
+    FB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    FB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    side_.push_back(st);
+    done_.push_back(ev);
+  }
+  if (scr_n_ != n || gscr_.n < size_t(n) * nside) {
+    FB_CUDA(cudaDeviceSynchronize());  // no launch may still use the old scratch
+    gscr_.alloc(size_t(n) * nside);
+    escr_.alloc(nside);
+    scr_n_ = n;
+  }
 }
 
 bool CombinedPotential::timing_active() const {
@@ -175,11 +229,30 @@ void CombinedPotential::energy_gradient(const double* x, int64_t n, double* g, d
     FB_CUDA(cudaMemsetAsync(e, 0, sizeof(double), s));
     if (parts_.empty()) FB_CUDA(cudaMemsetAsync(g, 0, sizeof(double) * n, s));
   }
-  bool first = true;
-  for (auto& p : parts_) {
-    p->energy_gradient(x, n, g, e, acc || !first, s);
-    first = false;
+  const size_t nside = parts_.empty() ? 0 : parts_.size() - 1;
+  if (!in_eval_ || nside == 0 || n != scr_n_ || side_.size() < nside || host_steps() || timing_active()) {
+    bool first = true;
+    for (auto& p : parts_) {
+      p->energy_gradient(x, n, g, e, acc || !first, s);
+      first = false;
+    }
+    return;
   }
+  // The parts are independent until their results are summed: the first runs
+  // on s into g and e, the others at the same time on side streams into their
+  // own scratch, then the scratch is added in part order, which gives the
+  // same sums as adding the parts one after another.
+  FB_CUDA(cudaEventRecord(fork_, s));
+  for (size_t k = 0; k < nside; ++k) {
+    FB_CUDA(cudaStreamWaitEvent(side_[k], fork_, 0));
+    parts_[k + 1]->energy_gradient(x, n, gscr_.p + int64_t(k) * n, escr_.p + k, false, side_[k]);
+    FB_CUDA(cudaEventRecord(done_[k], side_[k]));
+  }
+  parts_[0]->energy_gradient(x, n, g, e, acc, s);
+  for (size_t k = 0; k < nside; ++k) FB_CUDA(cudaStreamWaitEvent(s, done_[k], 0));
+  const int grid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), int64_t(sm_count()) * 4)));
+  combine_sides_kernel<<<grid, 256, 0, s>>>(g, n, gscr_.p, int(nside), e, escr_.p);
+  FB_LAUNCH_CHECK();
 }
 
 void CombinedPotential::set_gradient_mode(int mode) {

@@ -96,6 +96,10 @@ class Potential {
  protected:
   void invalidate_graphs();
   int grad_mode_ = 0;
+  // True while eval() runs this potential's launches (directly or into its
+  // own graph): only then may they fork onto side streams (a caller that
+  // captures the launches into a graph of its own gets them in one stream).
+  bool in_eval_ = false;
   DevBuf<int> status_;  // [0] current evaluation, [1] accumulated for the host
   void init_status();
   void begin_eval_status(cudaStream_t s) { FB_CUDA(cudaMemsetAsync(status_.p, 0, sizeof(int), s)); }
@@ -124,6 +128,7 @@ using PotentialPtr = std::shared_ptr<Potential>;
 class CombinedPotential : public Potential {
  public:
   CombinedPotential();
+  ~CombinedPotential() override;
   void add(PotentialPtr p);
   int64_t ndof() const override;
   void energy(const double* x, int64_t n, double* e, bool acc, cudaStream_t s) override;
@@ -140,7 +145,15 @@ class CombinedPotential : public Potential {
   const std::vector<PotentialPtr>& parts() const { return parts_; }
 
  private:
+  // Parts after the first run on side streams into their own gradient and
+  // energy (gscr_, escr_), added to the first part's in part order at the join.
+  void prepare_side(int64_t n);
   std::vector<PotentialPtr> parts_;
+  std::vector<cudaStream_t> side_;
+  std::vector<cudaEvent_t> done_;
+  cudaEvent_t fork_ = nullptr;
+  DevBuf<double> gscr_, escr_;
+  int64_t scr_n_ = 0;
 };
 
 // One NUwU pattern whose points are split over several processes (GPUs).
