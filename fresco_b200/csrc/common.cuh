@@ -45,6 +45,8 @@ enum StatusBits : int {
   STATUS_TIMEOUT = 4,          // a bounded wait gave up: the evaluation's energy and gradient are NaN
   STATUS_TILE_RETRY = 8,       // a tile copy outlasted its first bounded wait and was waited for again
                                // (informational: the results are complete)
+  STATUS_EXACT_FALLBACK = 16,  // a point outside a type-3 plan's window: exact sums served the
+                               // evaluation (informational: the results are complete)
 };
 
 // A potential's status block holds two words: [0] the flags of the current

@@ -184,8 +184,9 @@ __global__ void __launch_bounds__(kThreads) nuwnu_adjoint_kernel(const double* _
 
 // Type-3 path helpers.  rho is zeroed for the direct fallback when the
 // window flag says the type-3 result is not to be used.
-__global__ void nuwnu_zero_if_kernel(double2* rho, int64_t M, const int* __restrict__ flag) {
+__global__ void nuwnu_zero_if_kernel(double2* rho, int64_t M, const int* __restrict__ flag, int* status) {
   if (*flag == 0) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) raise_status(status, STATUS_EXACT_FALLBACK);
   for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < M; k += int64_t(gridDim.x) * blockDim.x)
     rho[k] = make_double2(0.0, 0.0);
 }
@@ -351,8 +352,12 @@ class NUwNUImpl final : public Potential {
       fwd_->set_sources(x, TYPE3_NUWNU_MAP, L_, s);
       fwd_->execute_real(c_.p, cu_, rho_.p, s);
       flag = fwd_->window_flag();
-      nuwnu_zero_if_kernel<<<mg, kThreads, 0, s>>>(rho_.p, M_, flag);
+      nuwnu_zero_if_kernel<<<mg, kThreads, 0, s>>>(rho_.p, M_, flag, status_.p);
       FB_LAUNCH_CHECK();
+      // the direct sums below only run when the flag is set; a modest grid
+      // (the kernel strides over the frequency chunks) keeps the launch that
+      // exits at once cheap
+      fg.y = std::min(fg.y, 64u);
     } else {
       FB_CUDA(cudaMemsetAsync(rho_.p, 0, sizeof(double2) * M_, s));
     }

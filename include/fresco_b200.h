@@ -221,7 +221,9 @@ int fresco_inversepower_shard_create(double a, double eps, const double* radii_a
  * bounded buffer overflowed, 4 a bounded wait gave up (the evaluation's
  * energy and gradient are then NaN), 8 an interpolation tile copy outlasted
  * its first bounded wait and was waited for again (the results are
- * complete).  Synchronises `stream`.  No reference counterpart (FINUFFT's
+ * complete), 16 a point outside a type-3 NUFFT plan's window made NUwNU use
+ * exact sums for that evaluation (the results are complete).  Synchronises
+ * `stream`.  No reference counterpart (FINUFFT's
  * return codes are ignored at source/fresco/nuwu.hpp:191-192, 256-258). */
 int fresco_potential_status(fresco_potential p, void* stream, int* status);
 

@@ -59,7 +59,7 @@ def test_type3_2d_1e5_kpoints(case2d, prec, eps, tol):
         assert abs(e - e_ref) <= tol * abs(e_ref), (e, e_ref)
         assert rel(g, g_ref) <= tol
     assert abs(pot.get_energy(x) - e_ref) <= tol * abs(e_ref)
-    assert pot.status() == 0
+    assert pot.status() == 0  # in particular not 16: the type-3 path served every evaluation
 
 
 @pytest.mark.parametrize("prec,eps,tol", PRECISIONS)
@@ -74,6 +74,7 @@ def test_type3_1d_3d(prec, eps, tol, ndim, N, M, kmax, L):
     e, g = pot.get_energy_gradient(x)
     assert abs(e - e_ref) <= tol * abs(e_ref), (e, e_ref)
     assert rel(g, g_ref) <= tol
+    assert pot.status() == 0  # the type-3 path, not the exact fallback (status bit 16)
 
 
 def test_type3_exact_gradient_mode(case2d):
@@ -88,22 +89,26 @@ def test_type3_exact_gradient_mode(case2d):
     assert rel(g, g_ref * np.repeat(c, 2) * 2 * np.pi / L[0]) < 1e-10
 
 
-def test_type3_points_outside_the_plans_window_use_exact_sums():
-    """Points more than a box length outside the box are beyond the plans' window: that evaluation runs
-    the exact sums instead, with the same results; a NaN coordinate gives a NaN energy."""
+@pytest.mark.parametrize("L,fallback_far", [(1.3, True), (1.0, False)])
+def test_type3_points_outside_the_plans_window_use_exact_sums(L, fallback_far):
+    """The reference's map x = (p - round(p/L) + L) 2 pi / L drifts by 2 pi (L - 1) / L per box a point
+    moves away (none for L = 1).  Points more than a box length outside the box are then beyond the plans'
+    window: that evaluation runs the exact sums (status bit 16), with the same results.  A NaN
+    coordinate gives a NaN energy."""
     from fresco_b200 import NUwNU
 
-    x, radii, K, Sk, V, L = _inputs(2, 1200, 5000, 30.0, seed=7, L=1.0)
-    pot = NUwNU(radii, K, Sk, V, L, eps=1e-12)
+    x, radii, K, Sk, V, Lv = _inputs(2, 1200, 5000, 30.0, seed=7, L=L)
+    pot = NUwNU(radii, K, Sk, V, Lv, eps=1e-12)
     assert "type3" in pot.describe()
-    ref = _reference(radii, K, Sk, V, L)
+    ref = _reference(radii, K, Sk, V, Lv)
     far = x.copy()
-    far[::7] += 5.0  # five boxes away
-    for pts in (x, far, x):
+    far[::7] += 5.0 * L  # five boxes away
+    for pts, fallback in ((x, False), (far, fallback_far), (x, False)):
         e_ref, g_ref = ref.get_energy_gradient(pts)
         e, g = pot.get_energy_gradient(pts)
         assert abs(e - e_ref) <= 1e-10 * abs(e_ref)
         assert rel(g, g_ref) <= 1e-10
+        assert bool(pot.status() & 16) == fallback
     bad = x.copy()
     bad[5] = np.nan
     e, g = pot.get_energy_gradient(bad)
