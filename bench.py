@@ -744,15 +744,22 @@ def run_ours(args):
     top_ms = stage_ms.get(top, ms_per_step)
     achieved = per_kernel.get(top, b_eval) / (top_ms * 1e-3) / 1e9
     traffic = None
+    capture = None
     try:  # DRAM bytes per launch from an ncu capture of this workload (profiles/traffic.txt: "stage bytes")
         with open(os.path.join(ROOT, "profiles", "traffic.txt")) as fh:
-            prof = {ln.split()[0]: int(ln.split()[1]) for ln in fh if ln.strip() and not ln.startswith("#")}
+            text = fh.read()
+        prof = {ln.split()[0]: int(ln.split()[1]) for ln in text.splitlines() if ln.strip() and not ln.startswith("#")}
         traffic = prof.get(top)
+        import re
+
+        m = re.search(r"commit ([0-9a-f]{7,40})", text)
+        capture = m.group(1) if m else None
     except (OSError, ValueError, IndexError):
         pass
     roofline = {"kernel": top, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                 "frac": round(achieved / hbm_peak, 4), "traffic": traffic, "peak_source": peak_src,
-                "algorithmic_bytes": per_kernel.get(top)}
+                "algorithmic_bytes": per_kernel.get(top),
+                "traffic_source": f"ncu capture at commit {capture} (profiles/traffic.txt)" if capture else None}
     try:  # the stage's own limiter: L1/shared-memory pipe use from the same kind of ncu capture
         with open(os.path.join(ROOT, "profiles", "l1tex.txt")) as fh:
             l1 = {ln.split()[0]: ln.split()[1:] for ln in fh if ln.strip() and not ln.startswith("#")}
@@ -760,7 +767,7 @@ def run_ours(args):
             roofline["l1tex"] = {"frac": round(float(l1[top][0]) / 100.0, 3),
                                  "shared_wavefronts": int(l1[top][1]),
                                  "source": "ncu l1tex__throughput.avg.pct_of_peak_sustained_active "
-                                           "(profiles/l1tex.txt)"}
+                                           f"(profiles/l1tex.txt, capture at commit {capture})"}
     except (OSError, ValueError, IndexError):
         pass
     eval_achieved = b_eval / (ms_per_step * 1e-3) / 1e9
