@@ -1339,8 +1339,18 @@ __global__ void __launch_bounds__(256) interp_kernel(const Rec<D, T>* __restrict
 // 3D interpolation: one block per subproblem stages its bin's tile (+ halo,
 // tile + w cells per dimension, origin tile origin - w/2) of one field at a
 // time in shared memory and one thread per point sums its w^3 taps from it
-// (instead of gathering them from L2).  With two fields the first pass keeps
-// each point's sums in registers for the second.
+// (instead of gathering them from L2).  As in the 2D kernel, every tap
+// address of a point is its footprint's first cell plus an offset common to
+// all points, so the block buckets its points by that cell modulo the lanes
+// one shared-memory wavefront serves (16 for FP32 complex cells) and lane c
+// of every group of 16 takes points of class c only: the reads of a group
+// fall on distinct banks.  With two fields, each point's sums of the first
+// are kept in shared memory for the second.
+template <int W, typename T, int NF>
+__host__ __device__ constexpr size_t interp3d_extra_bytes() {
+  return (NF == 2 ? sizeof(cplx_t<T>) * kMaxSub : 0) + sizeof(uint16_t) * kMaxSub;
+}
+
 template <int W, typename T, int NF>
 __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
     const Rec<3, T>* __restrict__ recs, const T* __restrict__ weights, T uniform, const int* __restrict__ sub_bin,
@@ -1349,8 +1359,9 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
     int accumulate, const int* __restrict__ status, const GradScale gs) {
   constexpr int PAD = W / 2;
   constexpr int PPT = (kMaxSub + 255) / 256;
+  constexpr int G = 128 / int(sizeof(cplx_t<T>));  // lanes per wavefront = bank classes
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx_t<T>* tile = reinterpret_cast<cplx_t<T>*>(smem_raw);
+  __shared__ int cls_count[G], cls_start[G];
   const int sub = blockIdx.x;
   if (sub >= *num_sub) return;
   const int bin = sub_bin[sub], start = sub_start[sub], cnt = sub_count[sub];
@@ -1359,16 +1370,48 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
   const int org0 = bx * g.tile[0], org1 = by * g.tile[1], org2 = bz * g.tile[2];
   const int TX = g.tile[0] + W, TY = g.tile[1] + W, TZ = g.tile[2] + W;
   const int ncell = TX * TY * TZ;
+  cplx_t<T>* tile = reinterpret_cast<cplx_t<T>*>(smem_raw);
+  cplx_t<T>* first = tile + ncell;  // NF == 2: each point's sums of the first field
+  uint16_t* order = reinterpret_cast<uint16_t*>(first + (NF == 2 ? kMaxSub : 0));  // points grouped by class
   const bool bad = status != nullptr && ((*status) & STATUS_NONFINITE_INPUT);
   const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
   const int tid = threadIdx.x;
-  T acc_r[PPT], acc_i[PPT];
+  // class and rank in class of this thread's points (p = tid + 256 k)
+  if (tid < G) cls_count[tid] = 0;
+  __syncthreads();
+  int code[PPT];
 #pragma unroll
-  for (int k = 0; k < PPT; ++k) acc_r[k] = acc_i[k] = T(0);
+  for (int k = 0; k < PPT; ++k) {
+    const int p = tid + 256 * k;
+    code[k] = -1;
+    if (p >= cnt) continue;
+    const Rec<3, T> r = recs[start + p];
+    int c0, c1, c2;
+    unpack_cell(3, r.cell, c0, c1, c2);
+    T u;
+    const int l0 = c0 - org0 + es_start<W, T>(r.f[0], u) + PAD;
+    const int l1 = c1 - org1 + es_start<W, T>(r.f[1], u) + PAD;
+    const int l2 = c2 - org2 + es_start<W, T>(r.f[2], u) + PAD;
+    const int cls = ((l2 * TY + l1) * TX + l0) & (G - 1);
+    code[k] = (cls << 12) | atomicAdd(&cls_count[cls], 1);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+    for (int c = 0; c < G; ++c) {
+      cls_start[c] = acc;
+      acc += cls_count[c];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < PPT; ++k)
+    if (code[k] >= 0) order[cls_start[code[k] >> 12] + (code[k] & 0xfff)] = uint16_t(tid + 256 * k);
+  const int cls = tid % G, grp = tid / G, ngrp = int(blockDim.x) / G;
   for (int f = 0; f < NF; ++f) {
     const cplx_t<T>* fld = fields + f * g.G();
-    if (f) __syncthreads();  // every thread is done with the previous field's tile
-    constexpr int BT = 4;    // loads in flight per thread
+    __syncthreads();        // the order is complete; every thread is done with the previous field's tile
+    constexpr int BT = 4;  // loads in flight per thread
     for (int i0 = tid; i0 < ncell; i0 += BT * 256) {
       cplx_t<T> v[BT];
 #pragma unroll
@@ -1386,10 +1429,10 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
         if (i0 + b * 256 < ncell) tile[i0 + b * 256] = v[b];
     }
     __syncthreads();
-#pragma unroll
-    for (int k = 0; k < PPT; ++k) {
-      const int p = tid + 256 * k;
-      if (p >= cnt) break;
+    const int n_c = cls_count[cls];
+    const uint16_t* mine = order + cls_start[cls];
+    for (int j = grp; j < n_c; j += ngrp) {
+      const int p = mine[j];
       const Rec<3, T> r = recs[start + p];
       int c0, c1, c2;
       unpack_cell(3, r.cell, c0, c1, c2);
@@ -1417,12 +1460,15 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
         vi += k2[m2] * pi;
       }
       if (NF == 2 && f == 0) {
-        acc_r[k] = vr;
-        acc_i[k] = vi;
+        cplx_t<T> s0;
+        s0.x = vr;
+        s0.y = vi;
+        first[p] = s0;  // read back by this same thread for the second field
       } else {
         const T wgt = (mode == INTERP_GRAD) ? (weights ? weights[r.idx] : uniform) : T(1);
         if (NF == 2) {
-          interp_store<3, T>(mode, r.idx, wgt, acc_r[k], acc_i[k], vr, bad, grad, out2, accumulate, gs);
+          const cplx_t<T> s0 = first[p];
+          interp_store<3, T>(mode, r.idx, wgt, s0.x, s0.y, vr, bad, grad, out2, accumulate, gs);
         } else {
           interp_store<3, T>(mode, r.idx, wgt, vr, vi, T(0), bad, grad, out2, accumulate, gs);
         }
@@ -1625,8 +1671,10 @@ bool launch_interp3d(const void* recs, const T* weights, T uniform, const SortBu
   if constexpr (sizeof(T) != 4) {
     return false;
   } else {
-    const size_t smem = size_t(g.tile[0] + W) * (g.tile[1] + W) * (g.tile[2] + W) * sizeof(cplx_t<T>);
-    if (smem > 160 * 1024 || nfields < 1 || nfields > 2) return false;
+    const size_t tile_bytes = size_t(g.tile[0] + W) * (g.tile[1] + W) * (g.tile[2] + W) * sizeof(cplx_t<T>);
+    if (nfields < 1 || nfields > 2) return false;
+    const size_t smem = tile_bytes + (nfields == 2 ? interp3d_extra_bytes<W, T, 2>() : interp3d_extra_bytes<W, T, 1>());
+    if (smem > 160 * 1024) return false;
     auto kern2 = interp3d_tile_kernel<W, T, 2>;
     auto kern1 = interp3d_tile_kernel<W, T, 1>;
     auto kern = nfields == 2 ? kern2 : kern1;
