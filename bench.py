@@ -38,6 +38,8 @@ N_POINTS = 1 << 20
 K_MODES = 512
 K_CONSTRAINED = 256
 EPS = 1e-6
+# eps whose kernel width (w = 6) the FP32 form needs for a 1e-5 relative gradient error
+EPS_FP32_BOUND = 1e-5
 L2_FLUSH_BYTES = 256 << 20
 
 WORKLOAD = (
@@ -665,6 +667,14 @@ def run_ours(args):
     t64_ms, _ = timed_loop(pot64, max(3, args.steps // 2), 2)
     ms64 = t64_ms / max(3, args.steps // 2)
     g64 = g.clone()
+    # the FP32 form with the kernel width its 1e-5 gradient bound needs (eps = 1e-5: w = 6)
+    pot32w = NUwU(radii, K_MODES, Sk, V, L, eps=EPS_FP32_BOUND, precision="fp32")
+    t32w_ms, _ = timed_loop(pot32w, args.steps, args.warmup)
+    ms32w = reduce_max(t32w_ms, dev) / args.steps
+    e32w = float(e.item())
+    g32w = g.clone()
+    desc32w = pot32w.describe()
+    del pot32w
     potref = NUwU(radii, K_MODES, Sk, V, L, eps=1e-12, precision="fp64")
     potref.energy_gradient_device(xt, g, e)
     torch.cuda.synchronize()
@@ -672,7 +682,14 @@ def run_ours(args):
     gref = g.clone()
     err32 = float(torch.linalg.norm(g32 - gref) / torch.linalg.norm(gref))
     err64 = float(torch.linalg.norm(g64 - gref) / torch.linalg.norm(gref))
+    err32w = float(torch.linalg.norm(g32w - gref) / torch.linalg.norm(gref))
     eerr32 = abs(e32 - eref) / abs(eref)
+    fp32_bound = {"eps": EPS_FP32_BOUND, "w": int(desc32w.split(" w=")[1].split()[0]),
+                  "evals_per_s": round(ws * 1000.0 / ms32w, 2), "ms_per_step": round(ms32w, 5),
+                  "over_fp64": round(ms64 / ms32w, 3), "grad_rel_err": err32w,
+                  "energy_rel_err": abs(e32w - eref) / abs(eref),
+                  "note": "FP32 form at the kernel width chosen for the 1e-5 gradient bound, against the "
+                          "FP64 form at eps=1e-6 (w=7); errors against the FP64 form at eps=1e-12"}
     del potref
 
     # config 2's full potential: NUwU (FP32 form) + cell-list harmonic repulsion (a = 2, eps = 1,
@@ -815,6 +832,7 @@ def run_ours(args):
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "fp64": {"evals_per_s": round(ws * 1000.0 / ms64, 2), "ms_per_step": round(ms64, 5),
                  "fp32_over_fp64": round(ms64 / ms_per_step, 3)},
+        "fp32_width_for_bound": fp32_bound,
         "nuwu_plus_repulsion": {"evals_per_s_per_gpu": round(comb_evals, 2)},
         "lbfgs": lbfgs,
         "config2_lbfgs500": lbfgs500,
