@@ -222,6 +222,37 @@ def sharded_report(args, dev, ws, rank):
         out["lbfgs"] = {"iterations_per_s": round(n_it / dt, 2), "iterations": n_it, "evals": int(res.nfev),
                         "energy": float(res.energy), "exchange_calls": int(opt.reducer.calls), "M": 4,
                         "timing": "host wall clock around the C-level run loop, one rank"}
+    # config 2's repulsion over spatial slabs with the halo exchange: the points in spatial order, one
+    # equal slab per rank; each rank evaluates its own points' pairs against its halo
+    from fresco_b200 import ShardedInversePower
+    from fresco_b200.shard import spatial_order
+
+    rr = np.full(N_POINTS, 0.25 / np.sqrt(N_POINTS) * 2 * np.pi)
+    xs = x.reshape(-1, 2)[spatial_order(x, L)].ravel()
+    rep = ShardedInversePower(2.0, 1.0, rr, L, a, b, halo=True)
+    dxs = torch.tensor(xs[2 * a : 2 * b], device=dev)
+    gs = torch.empty_like(dxs)
+    es = torch.zeros((), dtype=torch.float64, device=dev)
+    for _ in range(3):
+        rep.energy_gradient_device(dxs, grad=gs, out=es)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    n_h = max(5, args.steps)
+    t_0 = time.perf_counter()
+    for _ in range(n_h):
+        rep.energy_gradient_device(dxs, grad=gs, out=es)
+    torch.cuda.synchronize()
+    dt_h = reduce_max(time.perf_counter() - t_0, dev)
+    rep.exchange.check()
+    exported, halo = rep.halo_stats()
+    out["halo_repulsion"] = {
+        "workload": "config-2 repulsion (N=2^20, diameter 0.5/sqrt(N) 2 pi), points in spatial order, one equal "
+                    "slab per rank", "evals_per_s": round(n_h / dt_h, 2), "energy": float(es.item()),
+        "exported_points": exported, "halo_points": halo, "exchange_bytes_per_eval": int(24 * exported),
+        "setup": rep.describe(),
+        "timing": "host wall clock around the evaluations (each reads the exchange sizes back), max over ranks"}
+    del rep
     return out
 
 

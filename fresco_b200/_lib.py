@@ -67,6 +67,10 @@ _SIGNATURES = {
     "fresco_inversepower_shard_create": (C.c_int, [C.c_double, C.c_double, c_double_p, c_int64, c_double_p, C.c_int,
                                                    C.c_int, c_int64, c_int64, c_void_p, c_void_p, c_void_p,
                                                    C.POINTER(handle_t)]),
+    "fresco_inversepower_halo_create": (C.c_int, [C.c_double, C.c_double, c_double_p, c_int64, c_double_p, C.c_int,
+                                                  c_int64, c_int64, C.c_int, C.c_int, c_void_p, c_void_p, c_void_p,
+                                                  C.POINTER(handle_t)]),
+    "fresco_inversepower_halo_stats": (C.c_int, [handle_t, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "fresco_optimizer_set_reducer": (C.c_int, [handle_t, c_void_p, c_void_p, c_int64]),
     "fresco_potential_set_gradient_mode": (C.c_int, [handle_t, C.c_int]),
     "fresco_potential_set_timing": (C.c_int, [handle_t, C.c_int]),

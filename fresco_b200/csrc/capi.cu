@@ -339,6 +339,28 @@ int fresco_inversepower_shard_create(double a, double eps, const double* radii_a
   });
 }
 
+int fresco_inversepower_halo_create(double a, double eps, const double* radii_all, int64_t n_total,
+                                    const double* boxv, int ndim, int64_t lo, int64_t hi, int rank, int nranks,
+                                    fresco_gatherv_fn gatherv, fresco_reduce_fn reduce, void* ctx,
+                                    fresco_potential* out) {
+  return guarded([&] {
+    if (!out || !boxv || (n_total > 0 && !radii_all)) throw fb::InvalidArgument("null argument");
+    if (ndim < 1 || ndim > 3) throw fb::InvalidArgument("InversePower: ndim must be 1, 2 or 3");
+    *out = wrap(fb::make_inversepower_halo(a, eps, std::vector<double>(radii_all, radii_all + n_total),
+                                           std::vector<double>(boxv, boxv + ndim), lo, hi, rank, nranks, gatherv,
+                                           reduce, ctx));
+    return FRESCO_OK;
+  });
+}
+
+int fresco_inversepower_halo_stats(fresco_potential p, int64_t* exported, int64_t* halo) {
+  return guarded([&] {
+    if (!p) throw fb::InvalidArgument("null argument");
+    if (!p->pot->halo_stats(exported, halo)) throw fb::InvalidArgument("not a repulsion halo shard");
+    return FRESCO_OK;
+  });
+}
+
 int fresco_optimizer_set_reducer(fresco_optimizer o, fresco_reduce_fn fn, void* ctx, int64_t global_ndof) {
   return guarded([&] {
     if (!o || !fn) throw fb::InvalidArgument("null argument");

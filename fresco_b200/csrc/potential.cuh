@@ -17,6 +17,11 @@ using ReduceFn = void (*)(double* data, int64_t count, void* stream, void* ctx);
 // into `full` (full_count values), ordered on `stream`.
 using GatherFn = void (*)(const double* local, int64_t local_count, double* full, int64_t full_count, void* stream,
                           void* ctx);
+// Concatenation over the processes of local arrays whose lengths differ, in
+// process order, into `full` (at most full_capacity values); counts[q]
+// (host memory) receives process q's length.  Ordered on `stream`.
+using GatherVFn = void (*)(const double* local, int64_t local_count, double* full, int64_t full_capacity,
+                           int64_t* counts, void* stream, void* ctx);
 
 // *dst += *src on stream s (one device scalar)
 void add_scalar(const double* src, double* dst, cudaStream_t s);
@@ -72,6 +77,13 @@ class Potential {
   int gradient_mode() const { return grad_mode_; }
   // Human-readable set-up summary (kernel width, grids, ...).
   virtual std::string describe() const { return kind(); }
+  // Points exported to and received from the other processes in the last
+  // evaluation (repulsion with a halo exchange); false for other potentials.
+  virtual bool halo_stats(int64_t* exported, int64_t* halo) const {
+    (void)exported;
+    (void)halo;
+    return false;
+  }
 
   int device = 0;
 
@@ -188,6 +200,14 @@ PotentialPtr make_nuwu_shard(const std::vector<double>& radii_local, int64_t n_t
 PotentialPtr make_inversepower_shard(double a, double eps, const std::vector<double>& radii_all,
                                      const std::vector<double>& boxv, bool periodic, int64_t lo, int64_t hi,
                                      GatherFn gather, ReduceFn reduce, void* ctx);
+// InversePower (periodic, cell lists) over spatially compact index slabs:
+// this process owns points [lo, hi) and is process `rank` of `nranks`; each
+// evaluation exchanges only the points next to another process's points (a
+// halo, gathered with `gatherv`), evaluates its own points' pairs and sums the
+// energy with `reduce`.
+PotentialPtr make_inversepower_halo(double a, double eps, const std::vector<double>& radii_all,
+                                    const std::vector<double>& boxv, int64_t lo, int64_t hi, int rank, int nranks,
+                                    GatherVFn gatherv, ReduceFn reduce, void* ctx);
 PotentialPtr make_nuwu(const std::vector<double>& radii, double K, const std::vector<double>& sk,
                        const std::vector<double>& v, const std::vector<double>& L, double eps, int precision);
 PotentialPtr make_uwu(const std::vector<int>& grid, double K, const std::vector<double>& sk,

@@ -117,7 +117,8 @@ template <int D>
 __global__ void __launch_bounds__(kThreads) cell_scatter_kernel(const double* __restrict__ x,
                                                                 const double* __restrict__ radii, int64_t N, Box b,
                                                                 const uint32_t* __restrict__ rank,
-                                                                const int* __restrict__ cell_start, PairRec<D>* recs) {
+                                                                const int* __restrict__ cell_start, PairRec<D>* recs,
+                                                                const uint32_t* __restrict__ gidx) {
   const int64_t step = int64_t(gridDim.x) * blockDim.x;
   for (int64_t j0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j0 < N; j0 += kCellBatch * step) {
     PairRec<D> r[kCellBatch];
@@ -141,7 +142,7 @@ __global__ void __launch_bounds__(kThreads) cell_scatter_kernel(const double* __
         const double v = r[u].x[a];
         r[u].xf[a] = isfinite(v) ? float(v - floor(v * b.invL[a]) * b.L[a]) : 0.f;
       }
-      r[u].idx = uint32_t(j);
+      r[u].idx = gidx ? gidx[j] : uint32_t(j);  // the pattern's index of the point
       recs[int64_t(cell_start[r[u].cell]) + rk[u]] = r[u];
     }
   }
@@ -160,7 +161,9 @@ __global__ void __launch_bounds__(kThreads) cell_scatter_kernel(const double* __
 // time; a lane finds its pair by a search over the lanes' queue prefix sums)
 // and adds the pair force to the owner's gradient slot in shared memory.
 // Survivors beyond a full list are evaluated afterwards by a rescan of that
-// point alone.
+// point alone.  Only points whose pattern index lies in [own_lo, own_lo +
+// own_n) take part as the first point of a pair and get a gradient (at
+// index - own_lo); the others (a halo) are neighbours only.
 constexpr int kPairQueue = 16;  // queued pairs per point
 
 template <int D>
@@ -286,7 +289,8 @@ __global__ void __launch_bounds__(kThreads) cell_pair_kernel(const PairRec<D>* _
                                                              const double* __restrict__ radii, double r_uniform,
                                                              const int* __restrict__ cell_start, int64_t N, Box b,
                                                              double a_pow, double eps, double* grad, double* energy,
-                                                             int accumulate, const int* __restrict__ status) {
+                                                             int accumulate, const int* __restrict__ status,
+                                                             uint32_t own_lo, uint32_t own_n) {
   constexpr int NW = kThreads / 32;
   constexpr int kSpan = 96;  // 2D: staged records per neighbour row and warp
   __shared__ int queue[NW][32][kPairQueue];
@@ -300,10 +304,10 @@ __global__ void __launch_bounds__(kThreads) cell_pair_kernel(const PairRec<D>* _
   const int64_t nwarps_total = int64_t(gridDim.x) * NW;
   for (int64_t wbase = (int64_t(blockIdx.x) * NW + warp) * 32; wbase < N; wbase += nwarps_total * 32) {
     const int64_t i = wbase + lane;
-    const bool active = i < N;
     PairRec<D> me;
     int nq = 0;
-    if (active) me = recs[i];
+    if (i < N) me = recs[i];
+    const bool active = i < N && me.idx - own_lo < own_n;
     // phase 1: candidates within reach -> queue
     bool staged = false;
     if constexpr (D == 2) {
@@ -417,7 +421,7 @@ __global__ void __launch_bounds__(kThreads) cell_pair_kernel(const PairRec<D>* _
       const double nan = __longlong_as_double(0x7ff8000000000000ULL);
 #pragma unroll
       for (int a = 0; a < D; ++a) {
-        double* dst = grad + int64_t(me.idx) * D + a;
+        double* dst = grad + int64_t(me.idx - own_lo) * D + a;
         const double v = bad ? nan : gi[a];
         *dst = accumulate ? *dst + v : v;
       }
@@ -500,6 +504,45 @@ __global__ void nan_fill_kernel(const int* __restrict__ status, double* grad, in
   if (blockIdx.x == 0 && threadIdx.x == 0) *energy = nan;
 }
 
+// Box and cell grid of a pattern: cells of edge >= r_cut = 2 max(r_i)
+// (inversepower_potential.hpp:115), at most about one cell per point (results
+// do not depend on the cell size; the reference picks its own via
+// ncellx_scale).  Returns the cell count; use_cells is false without a
+// periodic box of at least 3 cells per dimension.
+int64_t make_box(int D, const std::vector<double>& radii, const std::vector<double>& boxv, bool periodic, Box& box,
+                 bool& use_cells) {
+  const int64_t N = int64_t(radii.size());
+  double rmax = 0.0;
+  for (double r : radii) rmax = std::max(rmax, r);
+  const double rcut = 2.0 * rmax;
+  use_cells = periodic;
+  int64_t ncells = 1;
+  for (int a = 0; a < D; ++a) {
+    box.L[a] = periodic ? boxv[a] : 1.0;
+    box.invL[a] = 1.0 / box.L[a];
+  }
+  if (periodic) {
+    const double target = std::max(1.0, std::floor(std::pow(double(std::max<int64_t>(N, 1)), 1.0 / D)));
+    for (int a = 0; a < D; ++a) {
+      // the margin keeps every cell at least r_cut wide after rounding
+      int nc = rcut > 0 ? int(std::floor(box.L[a] / (rcut * (1.0 + 1e-9)))) : 1;
+      nc = std::max(1, std::min(nc, int(target)));
+      if (nc < 3) use_cells = false;
+      box.nc[a] = nc;
+      box.cw[a] = box.L[a] / nc;
+      box.inv_cw[a] = nc / box.L[a];
+      box.Lf[a] = float(box.L[a]);
+      box.invLf[a] = float(box.invL[a]);
+      ncells *= nc;
+    }
+  }
+  // FP32 positions (wrapped into the box) are within a few ulp of the exact
+  // ones; a 0.1% margin on r_cut never rejects an interacting pair
+  const double rej = rcut * (1.0 + 1e-3) + 1e-6 * std::max({box.L[0], box.L[1], box.L[2]});
+  box.reject2 = float(rej * rej);
+  return ncells;
+}
+
 template <int D>
 class InversePowerImpl final : public Potential {
  public:
@@ -508,39 +551,10 @@ class InversePowerImpl final : public Potential {
       : N_(int64_t(radii.size())), a_(a), eps_(eps), periodic_(periodic) {
     init_status();
     if (periodic && int(boxv.size()) != D) throw InvalidArgument("box.size() must be equal to ndim");
-    double rmax = 0.0;
-    for (double r : radii) rmax = std::max(rmax, r);
     // equal radii (the usual case) are passed as one value instead of gathered
     uniform_r_ = !radii.empty() && std::all_of(radii.begin(), radii.end(), [&](double r) { return r == radii[0]; });
     r0_ = radii.empty() ? 0.0 : radii[0];
-    const double rcut = 2.0 * rmax;  // inversepower_potential.hpp:115
-    use_cells_ = periodic;
-    int64_t ncells = 1;
-    for (int a = 0; a < D; ++a) {
-      box_.L[a] = periodic ? boxv[a] : 1.0;
-      box_.invL[a] = 1.0 / box_.L[a];
-    }
-    if (periodic) {
-      // cells of edge >= r_cut, at most about one cell per point (results do
-      // not depend on the cell size; the reference picks its own via ncellx_scale)
-      const double target = std::max(1.0, std::floor(std::pow(double(std::max<int64_t>(N_, 1)), 1.0 / D)));
-      for (int a = 0; a < D; ++a) {
-        // the margin keeps every cell at least r_cut wide after rounding
-        int nc = rcut > 0 ? int(std::floor(box_.L[a] / (rcut * (1.0 + 1e-9)))) : 1;
-        nc = std::max(1, std::min(nc, int(target)));
-        if (nc < 3) use_cells_ = false;
-        box_.nc[a] = nc;
-        box_.cw[a] = box_.L[a] / nc;
-        box_.inv_cw[a] = nc / box_.L[a];
-        box_.Lf[a] = float(box_.L[a]);
-        box_.invLf[a] = float(box_.invL[a]);
-        ncells *= nc;
-      }
-    }
-    // FP32 positions (wrapped into the box) are within a few ulp of the exact
-    // ones; a 0.1% margin on r_cut never rejects an interacting pair
-    const double rej = rcut * (1.0 + 1e-3) + 1e-6 * std::max({box_.L[0], box_.L[1], box_.L[2]});
-    box_.reject2 = float(rej * rej);
+    const int64_t ncells = make_box(D, radii, boxv, periodic, box_, use_cells_);
     radii_.alloc(std::max<int64_t>(N_, 1));
     scratch_grad_.alloc(std::max<int64_t>(N_ * D, 1));
     if (N_) FB_CUDA(cudaMemcpy(radii_.p, radii.data(), sizeof(double) * N_, cudaMemcpyHostToDevice));
@@ -590,12 +604,13 @@ class InversePowerImpl final : public Potential {
       FB_CUDA(cudaMemsetAsync(cell_count_.p, 0, sizeof(int) * (ncells_ + 1), s));
       cell_count_kernel<D><<<grid, kThreads, 0, s>>>(x, N_, box_, cell_count_.p, rank_.p, status_.p);
       exclusive_scan(cell_count_.p, cell_start_.p, block_sums_.p, ncells_ + 1, s);
-      cell_scatter_kernel<D><<<grid, kThreads, 0, s>>>(x, radii_.p, N_, box_, rank_.p, cell_start_.p, recs_.p);
+      cell_scatter_kernel<D><<<grid, kThreads, 0, s>>>(x, radii_.p, N_, box_, rank_.p, cell_start_.p, recs_.p,
+                                                       nullptr);
       FB_LAUNCH_CHECK();
       timer_mark("cell_sort", s);
       cell_pair_kernel<D><<<grid, kThreads, 0, s>>>(recs_.p, uniform_r_ ? nullptr : radii_.p, r0_, cell_start_.p, N_,
-                                                    box_, a_, eps_, g, e,
-                                                    acc_grad ? 1 : 0, status_.p);
+                                                    box_, a_, eps_, g, e, acc_grad ? 1 : 0, status_.p, 0u,
+                                                    uint32_t(N_));
       FB_LAUNCH_CHECK();
     }
     nan_fill_kernel<<<grid, kThreads, 0, s>>>(status_.p, g, N_ * D, e);
@@ -696,7 +711,308 @@ class InversePowerShard final : public Potential {
   DevBuf<double> xall_, gall_, et_;
 };
 
+
+// ---------------------------------------------------------------------------
+// Repulsion over spatially compact index slabs, with a halo exchange.
+//
+// This process owns points [lo, hi) of the pattern.  The columns are the cell
+// list's cells along axis 0 (each at least r_cut wide), so a point interacts
+// only with points in its own column and the two beside it.  Per evaluation:
+//  1. each process marks the columns that hold its points; the marks are
+//     gathered from every process;
+//  2. `need` = the columns next to another process's marked columns, `reach`
+//     = the columns next to this process's own (periodic);
+//  3. this process's points in `need` columns are exported (coordinates and
+//     pattern index) and gathered from every process (the sizes differ);
+//  4. the points received from other processes that lie in `reach` columns
+//     join the own points as a halo; one cell list over both gives each own
+//     point its complete gradient and the energy of the pairs whose lower
+//     pattern index is an own point (each pair once, as
+//     cell_list_potential.hpp:154-181 counts it);
+//  5. one sum over the processes gives every process the pattern's energy; a
+//     NaN energy (a non-finite coordinate on any process) makes the gradient
+//     NaN.
+// With the points ordered along axis 0 before the split, each slab is a
+// spatial slab and only the points of the columns at its two ends travel;
+// any other order stays correct and exports more.
+// ---------------------------------------------------------------------------
+
+// Column of a coordinate along axis 0 (the expression cell_of uses).
+__device__ __forceinline__ int column_of(double v, const Box& b) {
+  if (!isfinite(v)) return 0;
+  const double u = v - floor(v * b.invL[0]) * b.L[0];
+  return min(max(int(u * b.inv_cw[0]), 0), b.nc[0] - 1);
+}
+
+__device__ __forceinline__ bool column_bit(const uint32_t* __restrict__ m, int c) { return (m[c >> 5] >> (c & 31)) & 1u; }
+
+// Own points: their columns' marks, and their copy at the head of the combined set.
+template <int D>
+__global__ void halo_own_kernel(const double* __restrict__ x, int64_t n, Box b, uint32_t lo, uint32_t* mask,
+                                double* comb_x, uint32_t* comb_idx) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const int c = column_of(x[i * D], b);
+    atomicOr(mask + (c >> 5), 1u << (c & 31));
+#pragma unroll
+    for (int a = 0; a < D; ++a) comb_x[i * D + a] = x[i * D + a];
+    comb_idx[i] = lo + uint32_t(i);
+  }
+}
+
+__global__ void mask_to_double_kernel(const uint32_t* __restrict__ mask, int nwords, double* out) {
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += gridDim.x * blockDim.x) out[w] = double(mask[w]);
+}
+
+// need / reach from every process's marks (one block).
+__global__ void halo_columns_kernel(const double* __restrict__ marks, int nranks, int rank, int nwords, int ncol,
+                                    uint32_t* need, uint32_t* reach) {
+  for (int w = threadIdx.x; w < nwords; w += blockDim.x) {
+    need[w] = 0u;
+    reach[w] = 0u;
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
+    const int cm = c == 0 ? ncol - 1 : c - 1, cp = c == ncol - 1 ? 0 : c + 1;
+    bool nd = false, rc = false;
+    for (int q = 0; q < nranks; ++q) {
+      const double* m = marks + int64_t(q) * nwords;
+      const uint32_t bits = ((uint32_t(m[cm >> 5]) >> (cm & 31)) | (uint32_t(m[c >> 5]) >> (c & 31)) |
+                             (uint32_t(m[cp >> 5]) >> (cp & 31))) & 1u;
+      if (q == rank) rc = bits != 0u;
+      else nd |= bits != 0u;
+    }
+    if (nd) atomicOr(need + (c >> 5), 1u << (c & 31));
+    if (rc) atomicOr(reach + (c >> 5), 1u << (c & 31));
+  }
+}
+
+// Own points in `need` columns -> export records (D coordinates, pattern index).
+template <int D>
+__global__ void halo_export_kernel(const double* __restrict__ x, int64_t n, Box b, uint32_t lo,
+                                   const uint32_t* __restrict__ need, double* out, int* count) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    if (!column_bit(need, column_of(x[i * D], b))) continue;
+    double* r = out + int64_t(atomicAdd(count, 1)) * (D + 1);  // at most n records
+#pragma unroll
+    for (int a = 0; a < D; ++a) r[a] = x[i * D + a];
+    r[D] = double(lo + uint32_t(i));
+  }
+}
+
+// Received records of the other processes in `reach` columns -> the halo,
+// after the n_own own points of the combined set.
+template <int D>
+__global__ void halo_keep_kernel(const double* __restrict__ recv, int64_t n_recv, int64_t skip_lo, int64_t skip_hi,
+                                 Box b, const uint32_t* __restrict__ reach, int64_t n_own, int64_t cap,
+                                 int64_t n_total, double* comb_x, uint32_t* comb_idx, int* count, int* status) {
+  for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n_recv; k += int64_t(gridDim.x) * blockDim.x) {
+    if (k >= skip_lo && k < skip_hi) continue;  // this process's own export
+    const double* r = recv + k * (D + 1);
+    if (!column_bit(reach, column_of(r[0], b))) continue;
+    const double gi = r[D];
+    if (!(gi >= 0.0 && gi < double(n_total))) {  // not a point of the pattern
+      raise_status(status, STATUS_OVERFLOW);
+      continue;
+    }
+    const int s = atomicAdd(count, 1);
+    if (s >= cap) {  // more than the other processes' points: some were sent twice
+      raise_status(status, STATUS_OVERFLOW);
+      continue;
+    }
+#pragma unroll
+    for (int a = 0; a < D; ++a) comb_x[(n_own + s) * D + a] = r[a];
+    comb_idx[n_own + s] = uint32_t(gi);
+  }
+}
+
+__global__ void nan_if_nan_energy_kernel(const double* __restrict__ e, double* g, int64_t n) {
+  if (!isnan(*e)) return;
+  const double nan = __longlong_as_double(0x7ff8000000000000ULL);
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    g[i] = nan;
+}
+
+template <int D>
+class InversePowerHalo final : public Potential {
+ public:
+  InversePowerHalo(double a, double eps, const std::vector<double>& radii_all, const std::vector<double>& boxv,
+                   int64_t lo, int64_t hi, int rank, int nranks, GatherVFn gatherv, ReduceFn reduce, void* ctx)
+      : N_(int64_t(radii_all.size())), lo_(lo), hi_(hi), rank_(rank), nranks_(nranks), a_(a), eps_(eps),
+        gatherv_(gatherv), reduce_(reduce), ctx_(ctx) {
+    if (!gatherv || !reduce) throw InvalidArgument("a repulsion halo shard needs a gatherv and a reduce function");
+    if (lo < 0 || hi < lo || hi > N_) throw InvalidArgument("the slab [lo, hi) must lie within the pattern");
+    if (nranks < 1 || rank < 0 || rank >= nranks) throw InvalidArgument("rank must lie in [0, nranks)");
+    if (N_ >= (int64_t(1) << 31)) throw InvalidArgument("a halo shard holds fewer than 2^31 points");
+    if (int(boxv.size()) != D) throw InvalidArgument("box.size() must be equal to ndim");
+    init_status();
+    bool use_cells = false;
+    ncells_ = make_box(D, radii_all, boxv, true, box_, use_cells);
+    if (!use_cells)
+      throw InvalidArgument("the halo exchange needs cell lists: a periodic box of at least 3 cells per dimension");
+    uniform_r_ = !radii_all.empty() &&
+                 std::all_of(radii_all.begin(), radii_all.end(), [&](double r) { return r == radii_all[0]; });
+    r0_ = radii_all.empty() ? 0.0 : radii_all[0];
+    ncol_ = box_.nc[0];
+    nwords_ = (ncol_ + 31) / 32;
+    const int64_t n = hi - lo, cap = std::max<int64_t>(N_, 1);
+    radii_.alloc(cap);
+    if (N_) FB_CUDA(cudaMemcpy(radii_.p, radii_all.data(), sizeof(double) * N_, cudaMemcpyHostToDevice));
+    mask_.alloc(nwords_);
+    need_.alloc(nwords_);
+    reach_.alloc(nwords_);
+    mask_d_.alloc(nwords_);
+    marks_.alloc(int64_t(nranks) * nwords_);
+    exp_.alloc(std::max<int64_t>(n, 1) * (D + 1));
+    recv_.alloc(cap * (D + 1));
+    comb_x_.alloc(cap * D);
+    comb_idx_.alloc(cap);
+    counts_dev_.alloc(2);
+    e_part_.alloc(1);
+    scratch_g_.alloc(std::max<int64_t>(n, 1) * D);
+    cell_count_.alloc(ncells_ + 1);  // the extra zero count makes cell_start[ncells] = the point count
+    cell_start_.alloc(ncells_ + 1);
+    block_sums_.alloc(scan_tmp_size(ncells_ + 1));
+    rank_buf_.alloc(cap);
+    recs_.alloc(cap);
+    FB_CUDA(cudaMallocHost(&host_counts_, 2 * sizeof(int)));
+    counts_.assign(size_t(nranks), 0);
+  }
+  ~InversePowerHalo() override {
+    if (host_counts_) cudaFreeHost(host_counts_);
+  }
+
+  int64_t ndof() const override { return (hi_ - lo_) * D; }
+  std::string kind() const override { return "InversePowerHalo"; }
+  bool host_steps() const override { return true; }  // the gathers, the sizes read back and the energy sum
+  std::string describe() const override {
+    std::string s = "InversePowerHalo points [" + std::to_string(lo_) + ", " + std::to_string(hi_) + ") of " +
+                    std::to_string(N_) + " process " + std::to_string(rank_) + "/" + std::to_string(nranks_) +
+                    " D=" + std::to_string(D) + " cells=";
+    for (int a = 0; a < D; ++a) s += (a ? "x" : "") + std::to_string(box_.nc[a]);
+    return s;
+  }
+  bool halo_stats(int64_t* exported, int64_t* halo) const override {
+    if (exported) *exported = exported_;
+    if (halo) *halo = halo_;
+    return true;
+  }
+
+  void energy(const double* x, int64_t n, double* e, bool acc, cudaStream_t s) override { run(x, nullptr, e, acc, s); }
+  void energy_gradient(const double* x, int64_t n, double* g, double* e, bool acc, cudaStream_t s) override {
+    run(x, g, e, acc, s);
+  }
+
+ private:
+  int grid_for(int64_t n) const { return int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, kThreads), int64_t(sm_count()) * 8))); }
+
+  int read_count(int which, cudaStream_t s) {
+    FB_CUDA(cudaMemcpyAsync(host_counts_ + which, counts_dev_.p + which, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FB_CUDA(cudaStreamSynchronize(s));
+    return host_counts_[which];
+  }
+
+  void run(const double* x, double* g, double* e, bool acc, cudaStream_t s) {
+    const int64_t n = hi_ - lo_;
+    double* gout = g ? g : scratch_g_.p;
+    const bool acc_g = g != nullptr && acc;
+    begin_eval_status(s);
+    FB_CUDA(cudaMemsetAsync(mask_.p, 0, sizeof(uint32_t) * nwords_, s));
+    FB_CUDA(cudaMemsetAsync(counts_dev_.p, 0, 2 * sizeof(int), s));
+    FB_CUDA(cudaMemsetAsync(e_part_.p, 0, sizeof(double), s));
+    if (n > 0) {
+      halo_own_kernel<D><<<grid_for(n), kThreads, 0, s>>>(x, n, box_, uint32_t(lo_), mask_.p, comb_x_.p,
+                                                          comb_idx_.p);
+      FB_LAUNCH_CHECK();
+    }
+    mask_to_double_kernel<<<1, 256, 0, s>>>(mask_.p, nwords_, mask_d_.p);
+    FB_LAUNCH_CHECK();
+    // 1. every process's column marks
+    gatherv_(mask_d_.p, nwords_, marks_.p, int64_t(nranks_) * nwords_, counts_.data(), s, ctx_);
+    for (int q = 0; q < nranks_; ++q)
+      if (counts_[size_t(q)] != nwords_) throw CudaError("halo exchange: the processes disagree on the column grid");
+    // 2. need / reach, 3. the export
+    halo_columns_kernel<<<1, 1024, 0, s>>>(marks_.p, nranks_, rank_, nwords_, ncol_, need_.p, reach_.p);
+    FB_LAUNCH_CHECK();
+    if (n > 0) {
+      halo_export_kernel<D><<<grid_for(n), kThreads, 0, s>>>(x, n, box_, uint32_t(lo_), need_.p, exp_.p,
+                                                             counts_dev_.p);
+      FB_LAUNCH_CHECK();
+    }
+    exported_ = read_count(0, s);
+    gatherv_(exp_.p, exported_ * (D + 1), recv_.p, std::max<int64_t>(N_, 1) * (D + 1), counts_.data(), s, ctx_);
+    int64_t total = 0, skip_lo = 0;
+    for (int q = 0; q < nranks_; ++q) {
+      const int64_t c = counts_[size_t(q)];
+      if (c < 0 || c % (D + 1)) throw CudaError("halo exchange: a process sent a partial record");
+      if (q < rank_) skip_lo += c;
+      total += c;
+    }
+    if (counts_[size_t(rank_)] != exported_ * (D + 1) || total > std::max<int64_t>(N_, 1) * (D + 1))
+      throw CudaError("halo exchange: the gathered sizes do not add up");
+    // 4. the halo and the cell list over own + halo points
+    const int64_t n_recv = total / (D + 1);
+    if (n_recv > 0) {
+      halo_keep_kernel<D><<<grid_for(n_recv), kThreads, 0, s>>>(
+          recv_.p, n_recv, skip_lo / (D + 1), skip_lo / (D + 1) + exported_, box_, reach_.p, n, N_ - n, N_,
+          comb_x_.p, comb_idx_.p, counts_dev_.p + 1, status_.p);
+      FB_LAUNCH_CHECK();
+    }
+    halo_ = std::min<int64_t>(read_count(1, s), N_ - n);
+    const int64_t nc = n + halo_;
+    if (nc > 0) {
+      const int grid = grid_for(nc);
+      FB_CUDA(cudaMemsetAsync(cell_count_.p, 0, sizeof(int) * (ncells_ + 1), s));
+      cell_count_kernel<D><<<grid, kThreads, 0, s>>>(comb_x_.p, nc, box_, cell_count_.p, rank_buf_.p, status_.p);
+      exclusive_scan(cell_count_.p, cell_start_.p, block_sums_.p, ncells_ + 1, s);
+      cell_scatter_kernel<D><<<grid, kThreads, 0, s>>>(comb_x_.p, radii_.p, nc, box_, rank_buf_.p, cell_start_.p,
+                                                       recs_.p, comb_idx_.p);
+      FB_LAUNCH_CHECK();
+      cell_pair_kernel<D><<<grid, kThreads, 0, s>>>(recs_.p, uniform_r_ ? nullptr : radii_.p, r0_, cell_start_.p, nc,
+                                                    box_, a_, eps_, gout, e_part_.p, acc_g ? 1 : 0, status_.p,
+                                                    uint32_t(lo_), uint32_t(n));
+      FB_LAUNCH_CHECK();
+    }
+    // 5. the pattern's energy on every process
+    reduce_(e_part_.p, 1, s, ctx_);
+    if (g && n > 0) {
+      nan_if_nan_energy_kernel<<<grid_for(n * D), kThreads, 0, s>>>(e_part_.p, g, n * D);
+      FB_LAUNCH_CHECK();
+    }
+    if (acc) add_scalar(e_part_.p, e, s);
+    else FB_CUDA(cudaMemcpyAsync(e, e_part_.p, sizeof(double), cudaMemcpyDeviceToDevice, s));
+  }
+
+  int64_t N_, lo_, hi_;
+  int rank_, nranks_;
+  double a_, eps_;
+  GatherVFn gatherv_;
+  ReduceFn reduce_;
+  void* ctx_;
+  Box box_;
+  int64_t ncells_ = 0;
+  int ncol_ = 1, nwords_ = 1;
+  bool uniform_r_ = false;
+  double r0_ = 0.0;
+  int64_t exported_ = 0, halo_ = 0;
+  int* host_counts_ = nullptr;
+  std::vector<int64_t> counts_;
+  DevBuf<double> radii_, mask_d_, marks_, exp_, recv_, comb_x_, e_part_, scratch_g_;
+  DevBuf<uint32_t> mask_, need_, reach_, comb_idx_, rank_buf_;
+  DevBuf<int> counts_dev_, cell_count_, cell_start_, block_sums_;
+  DevBuf<PairRec<D>> recs_;
+};
+
 }  // namespace
+
+PotentialPtr make_inversepower_halo(double a, double eps, const std::vector<double>& radii_all,
+                                    const std::vector<double>& boxv, int64_t lo, int64_t hi, int rank, int nranks,
+                                    GatherVFn gatherv, ReduceFn reduce, void* ctx) {
+  const int D = int(boxv.size());
+  if (D == 1) return PotentialPtr(new InversePowerHalo<1>(a, eps, radii_all, boxv, lo, hi, rank, nranks, gatherv, reduce, ctx));
+  if (D == 2) return PotentialPtr(new InversePowerHalo<2>(a, eps, radii_all, boxv, lo, hi, rank, nranks, gatherv, reduce, ctx));
+  if (D == 3) return PotentialPtr(new InversePowerHalo<3>(a, eps, radii_all, boxv, lo, hi, rank, nranks, gatherv, reduce, ctx));
+  throw InvalidArgument("InversePower: dimension " + std::to_string(D) + " is not supported");
+}
 
 PotentialPtr make_inversepower_shard(double a, double eps, const std::vector<double>& radii_all,
                                      const std::vector<double>& boxv, bool periodic, int64_t lo, int64_t hi,

@@ -23,8 +23,8 @@ from . import _lib
 from ._lib import check, dptr, lib
 from .potentials import BasePotential, CombinedPotential, Distance, _f64, _precision
 
-__all__ = ["ShardedNUwU", "ShardedInversePower", "ShardedLBFGS", "Reducer", "Exchange", "shard_totals",
-           "weight_factor_sum"]
+__all__ = ["ShardedNUwU", "ShardedInversePower", "ShardedLBFGS", "Reducer", "Exchange", "HaloExchange",
+           "gather_varying", "spatial_order", "shard_totals", "weight_factor_sum"]
 
 
 def _dist(group):
@@ -284,15 +284,100 @@ class Exchange(Reducer):
                 self.error = exc
 
 
+# fresco_gatherv_fn: (local address, local count, full address, full capacity, host counts, stream, context)
+GATHERV_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.c_void_p,
+                         C.c_void_p)
+
+
+def gather_varying(local, group=None):
+    """All-gather of 1-D tensors whose lengths differ between the ranks of `group`: returns the
+    concatenation in rank order and the list of lengths.  Two collectives (the lengths, then the
+    arrays padded to the longest); CPU tensors over gloo and CUDA tensors over NCCL alike."""
+    import torch
+
+    dist = _dist(group)
+    if dist is None:
+        return local, [int(local.numel())]
+    ws = dist.get_world_size(group)
+    n = torch.tensor([local.numel()], dtype=torch.int64, device=local.device)
+    ns = [torch.zeros_like(n) for _ in range(ws)]
+    dist.all_gather(ns, n, group=group)
+    counts = [int(c.item()) for c in ns]
+    m = max(max(counts), 1)
+    buf = torch.zeros(m, dtype=local.dtype, device=local.device)
+    buf[:local.numel()].copy_(local)
+    outs = [torch.empty_like(buf) for _ in range(ws)]
+    dist.all_gather(outs, buf, group=group)
+    return torch.cat([o[:c] for o, c in zip(outs, counts)]), counts
+
+
+def spatial_order(x, boxv):
+    """Permutation of the points (x flat, D coordinates per point) in the order of their coordinate along
+    axis 0 wrapped into the box: split into equal index slabs after it, every slab is a spatial slab,
+    which is what makes the halo exchange of ShardedInversePower(halo=True) small.  Apply it to the
+    coordinates and the radii alike (the losses do not depend on the order of the points)."""
+    import numpy as np
+
+    boxv = np.asarray(boxv, dtype=np.float64)
+    pts = np.asarray(x, dtype=np.float64).reshape(-1, boxv.size)
+    return np.argsort(np.mod(pts[:, 0], boxv[0]), kind="stable")
+
+
+class HaloExchange(Reducer):
+    """A Reducer that also gathers arrays of varying length (the library's fresco_gatherv_fn): the
+    column marks and the exported points of a ShardedInversePower(halo=True).  `gatherv_fn(local)`
+    returns (concatenation in rank order, lengths) (default: gather_varying over `group`, the local
+    array alone without a multi-rank group)."""
+
+    def __init__(self, group=None, fn=None, gatherv_fn=None):
+        super().__init__(group, fn)
+        self.gatherv_fn = gatherv_fn
+        self.c_gatherv = GATHERV_FN(self._gatherv)
+
+    def active(self) -> bool:
+        return super().active() or self.gatherv_fn is not None
+
+    def _gatherv(self, lptr, lcount, fptr, fcap, counts_ptr, stream, ctx):
+        try:
+            self.calls += 1
+            if self.error is not None:
+                return
+            import torch
+
+            full = torch.as_tensor(_DeviceArray(fptr, fcap), device="cuda")
+            local = torch.as_tensor(_DeviceArray(lptr, lcount), device="cuda") if lcount > 0 else full[:0]
+            with torch.cuda.stream(self._stream(stream, full.device)):
+                if self.gatherv_fn is not None:
+                    cat, counts = self.gatherv_fn(local)
+                else:
+                    cat, counts = gather_varying(local, self.group)
+                if sum(counts) > fcap:
+                    raise RuntimeError(f"gathered {sum(counts)} values into room for {fcap}")
+                full[:cat.numel()].copy_(cat)
+            for r, c in enumerate(counts):
+                counts_ptr[r] = int(c)
+        except BaseException as exc:  # noqa: BLE001 (reported by check())
+            if self.error is None:
+                self.error = exc
+            counts_ptr[0] = -1  # a size the library rejects: the evaluation stops with an error
+
+
 class ShardedInversePower(BasePotential):
     """InversePower (fresco/potentials/inversepower_potential.pyx:16-79, cell lists) over one pattern
     split into index slabs: this rank owns points [lo, hi) of the pattern whose radii `radii_all` are
-    given, and takes its slab's coordinates.  Each evaluation all-gathers the slabs, evaluates the whole
-    pattern's repulsion and keeps this slab's gradient; the energy is the pattern's on every rank.
-    Combines with a ShardedNUwU in a CombinedPotential for ShardedLBFGS.  The slabs of the ranks, in rank
-    order, must tile [0, n_total)."""
+    given, and takes its slab's coordinates.  The slabs of the ranks, in rank order, must tile
+    [0, n_total).  Combines with a ShardedNUwU in a CombinedPotential for ShardedLBFGS; every rank
+    holds the pattern's energy and its slab's gradient.
 
-    def __init__(self, a, eps, radii_all, boxv, lo, hi, group=None, exchange=None, method=Distance.PERIODIC):
+    halo=False: each evaluation all-gathers the slabs and evaluates the whole pattern's repulsion
+    (any box, any order of the points).
+    halo=True (periodic box of at least 3 cells per dimension): each evaluation exchanges only the
+    points next to another rank's points (a halo; see fresco_inversepower_halo_create) and evaluates
+    this slab's pairs.  It is small when the slabs are spatial slabs: order the points with
+    spatial_order before the split.  `rank` and `nranks` default to the group's."""
+
+    def __init__(self, a, eps, radii_all, boxv, lo, hi, group=None, exchange=None, method=Distance.PERIODIC,
+                 halo=False, rank=None, nranks=None):
         self.a, self.eps = float(a), float(eps)
         self.radii = _f64(radii_all)
         self.boxv = _f64(boxv)
@@ -300,27 +385,67 @@ class ShardedInversePower(BasePotential):
         self.lo, self.hi = int(lo), int(hi)
         self.N = self.hi - self.lo
         self.n_total = self.radii.size
-        if exchange is None:
-            exchange = Exchange(group)
-            dist = _dist(group)
-            if dist is not None:
-                slabs = [None] * dist.get_world_size(group)
-                dist.all_gather_object(slabs, (self.lo, self.hi), group=group)
-                ends = [0] + [h for _, h in slabs]
-                if any(l != e for (l, _), e in zip(slabs, ends)) or ends[-1] != self.n_total:
-                    raise ValueError("the ranks' slabs must tile [0, n_total) in rank order")
-                exchange.counts = [(h - l) * self.ndim for l, h in slabs]
-            elif (self.lo, self.hi) != (0, self.n_total):
-                raise ValueError("a slab of a larger pattern needs a multi-rank process group or an exchange")
-        self.exchange = exchange
+        self.halo = bool(halo)
+        dist = _dist(group)
+        slabs = None
+        if dist is not None and exchange is None:
+            slabs = [None] * dist.get_world_size(group)
+            dist.all_gather_object(slabs, (self.lo, self.hi), group=group)
+            ends = [0] + [h for _, h in slabs]
+            if any(l != e for (l, _), e in zip(slabs, ends)) or ends[-1] != self.n_total:
+                raise ValueError("the ranks' slabs must tile [0, n_total) in rank order")
+        elif exchange is None and (self.lo, self.hi) != (0, self.n_total):
+            raise ValueError("a slab of a larger pattern needs a multi-rank process group or an exchange")
         periodic = method == Distance.PERIODIC if isinstance(method, Distance) else \
             str(getattr(method, "name", method)).upper().endswith("PERIODIC")
         h = _lib.handle_t()
-        check(lib.fresco_inversepower_shard_create(self.a, self.eps, dptr(self.radii), self.n_total, dptr(self.boxv),
-                                                   self.ndim, int(periodic), self.lo, self.hi,
-                                                   C.cast(exchange.c_gather, C.c_void_p),
-                                                   C.cast(exchange.c_fn, C.c_void_p), None, C.byref(h)))
+        if self.halo:
+            if not periodic:
+                raise ValueError("the halo exchange needs a periodic box")
+            if exchange is None:
+                exchange = HaloExchange(group)
+            if rank is None or nranks is None:
+                if dist is not None:
+                    rank, nranks = dist.get_rank(group), dist.get_world_size(group)
+                elif exchange.gatherv_fn is None:
+                    rank, nranks = 0, 1
+                else:
+                    raise ValueError("an exchange without a process group needs rank and nranks")
+            self.rank, self.nranks = int(rank), int(nranks)
+            self.exchange = exchange
+            check(lib.fresco_inversepower_halo_create(self.a, self.eps, dptr(self.radii), self.n_total,
+                                                      dptr(self.boxv), self.ndim, self.lo, self.hi, self.rank,
+                                                      self.nranks, C.cast(exchange.c_gatherv, C.c_void_p),
+                                                      C.cast(exchange.c_fn, C.c_void_p), None, C.byref(h)))
+        else:
+            if exchange is None:
+                exchange = Exchange(group)
+                if slabs is not None:
+                    exchange.counts = [(hh - ll) * self.ndim for ll, hh in slabs]
+            self.exchange = exchange
+            check(lib.fresco_inversepower_shard_create(self.a, self.eps, dptr(self.radii), self.n_total,
+                                                       dptr(self.boxv), self.ndim, int(periodic), self.lo, self.hi,
+                                                       C.cast(exchange.c_gather, C.c_void_p),
+                                                       C.cast(exchange.c_fn, C.c_void_p), None, C.byref(h)))
         self._set_handle(h)
+
+    def halo_stats(self):
+        """(points exported, halo points kept) in the last evaluation of a halo=True shard."""
+        e, k = C.c_int64(), C.c_int64()
+        check(lib.fresco_inversepower_halo_stats(self._h, C.byref(e), C.byref(k)))
+        return int(e.value), int(k.value)
+
+    def get_energy(self, x):
+        try:
+            return super().get_energy(x)
+        finally:
+            self.exchange.check()
+
+    def get_energy_gradient(self, x, out=None):
+        try:
+            return super().get_energy_gradient(x, out=out)
+        finally:
+            self.exchange.check()
 
 
 def _enable_reducer(shard, reducer):

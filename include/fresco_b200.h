@@ -44,6 +44,12 @@ typedef void (*fresco_reduce_fn)(double* data, int64_t count, void* stream, void
  * `stream` (an all-gather supplied by the caller). */
 typedef void (*fresco_gather_fn)(const double* local, int64_t local_count, double* full, int64_t full_count,
                                  void* stream, void* ctx);
+/* Concatenates the processes' local arrays, whose lengths differ, in process
+ * order into the device array `full` (at most full_capacity doubles) and
+ * writes process q's length to counts[q] (host memory), ordered on `stream`
+ * (an all-gather of varying sizes supplied by the caller). */
+typedef void (*fresco_gatherv_fn)(const double* local, int64_t local_count, double* full, int64_t full_capacity,
+                                  int64_t* counts, void* stream, void* ctx);
 typedef struct fresco_window_stats_s* fresco_window_stats;
 
 enum {
@@ -216,6 +222,25 @@ int fresco_inversepower_shard_create(double a, double eps, const double* radii_a
                                      const double* boxv, int ndim, int periodic, int64_t lo, int64_t hi,
                                      fresco_gather_fn gather, fresco_reduce_fn reduce, void* ctx,
                                      fresco_potential* out);
+/* InversePower (periodic box, cell lists: inversepower_potential.hpp:104-124,
+ * cell_list_potential.hpp:442-465) over a pattern split into index slabs that
+ * are spatially compact (points ordered along axis 0 before the split): this
+ * process is process `rank` of `nranks` and owns points [lo, hi) of the
+ * n_total whose radii are given.  Each evaluation gathers every process's
+ * occupied columns (cells along axis 0) through gatherv, exports its points
+ * next to another process's columns, gathers the exports (gatherv), keeps the
+ * received points next to its own columns as a halo, evaluates its own
+ * points' pairs over own + halo points and sums the energy with reduce:
+ * every process holds the pattern's energy and its slab's gradient.  Needs
+ * at least 3 cells per dimension (FRESCO_ERR_INVALID otherwise).  Combines
+ * with a NUwU shard in a CombinedPotential. */
+int fresco_inversepower_halo_create(double a, double eps, const double* radii_all, int64_t n_total,
+                                    const double* boxv, int ndim, int64_t lo, int64_t hi, int rank, int nranks,
+                                    fresco_gatherv_fn gatherv, fresco_reduce_fn reduce, void* ctx,
+                                    fresco_potential* out);
+/* Points this process exported and halo points it kept in the last
+ * evaluation of a halo shard (FRESCO_ERR_INVALID for other potentials). */
+int fresco_inversepower_halo_stats(fresco_potential p, int64_t* exported, int64_t* halo);
 
 /* Sticky status bits raised since the last call: 1 non-finite input, 2 a
  * bounded buffer overflowed, 4 a bounded wait gave up (the evaluation's
