@@ -932,6 +932,17 @@ __global__ void __launch_bounds__(256) spread_kernel(const Rec<D, T>* __restrict
 // pass on disjoint bank ranges: every atomic instruction is free of bank
 // conflicts.  Lane l < 3w evaluates tap l % w of axis l / w (its coefficient
 // row is loaded into registers once) and the others read it by shuffle.
+//
+// FP32 accumulates in 32-bit fixed point: a shared-memory float atomic add is
+// a compare-and-swap loop, an integer one a single instruction.  The block
+// scales its contributions by s = 2^21 / 2^e with max |weight| < 2^e, so each
+// is below 2^21 in magnitude (|taps| <= 1) and is rounded to an integer by one
+// FMA against 1.5 * 2^23 (round to nearest: the same half-unit error as one
+// float addition of a value of that size); a cell receives at most one
+// contribution per point of the subproblem (at most kMaxSub = 640 < 2^10), so
+// its sum stays below 2^31 and is exact.  The flush adds sum / s to the grid.
+// A non-finite weight makes the block add NaN to the grid.  FP64 keeps double
+// atomics.
 template <int W, typename T>
 __global__ void __launch_bounds__(256) spread3d_warp_kernel(const Rec<3, T>* __restrict__ recs,
                                                             const T* __restrict__ weights, T uniform,
@@ -941,10 +952,16 @@ __global__ void __launch_bounds__(256) spread3d_warp_kernel(const Rec<3, T>* __r
                                                             const int* __restrict__ num_sub, Geom g,
                                                             const EsPoly<W, T> poly, int tw0p, T* grid_real) {
   static_assert(W <= 8, "one pass covers 4 rows of at most 8 columns");
+  static_assert(kMaxSub < 1024, "fixed-point sums of at most kMaxSub contributions below 2^21 fit 31 bits");
+  constexpr bool FIXED = sizeof(T) == 4;
   constexpr int Q = EsPolyDeg<W>::Q;
   constexpr int PAD = W / 2;
+  constexpr float kRound = 12582912.0f;  // 1.5 * 2^23: x + kRound holds round(x) in its low mantissa bits
+  constexpr int kRoundBits = 0x4B400000;  // the bits of kRound
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tile = reinterpret_cast<T*>(smem_raw);
+  int* itile = reinterpret_cast<int*>(smem_raw);
+  __shared__ float s_red[8];
   const int sub = blockIdx.x;
   if (sub >= *num_sub) return;
   const int tw0 = g.tw[0], tw1 = g.tw[1], tw2 = g.tw[2];
@@ -961,12 +978,45 @@ __global__ void __launch_bounds__(256) spread3d_warp_kernel(const Rec<3, T>* __r
       if (m == tm) v = poly.c[m][d];
     cf[d] = v;
   }
+  // lane (r_in, c_in) covers column c_in of footprint rows r_in and r_in + 4; lanes outside the
+  // footprint add zero to a cell that no other lane of the instruction touches (column c_in < 8 of
+  // the padded row, or row r_in again for the second pass), so the atomics need no branch
   const int r_in = lane >> 3, c_in = lane & 7;
   const bool col_ok = c_in < W && r_in < W, row1_ok = r_in + 4 < W;
-  __syncthreads();
+  const int r_eff = r_in < W ? r_in : 0;
+  const int row1_off = row1_ok ? 4 * tw0p : 0;
 
   const int bin = sub_bin[sub];
   const int start = sub_start[sub], cnt = sub_count[sub];
+  float scale = 1.0f, inv_scale = 1.0f;
+  bool bad_weight = false;
+  if constexpr (FIXED) {  // the block's largest |weight| (NaN if a weight is not finite)
+    float wm = 0.0f;
+    for (int p = threadIdx.x; p < cnt; p += blockDim.x) {
+      const float w = weights ? float(weights[recs[start + p].idx]) : float(uniform);
+      wm = (isfinite(w) && !isnan(wm)) ? fmaxf(wm, fabsf(w)) : __int_as_float(0x7fc00000);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float t = __shfl_xor_sync(0xffffffffu, wm, o);
+      wm = (isnan(wm) || isnan(t)) ? __int_as_float(0x7fc00000) : fmaxf(wm, t);
+    }
+    if (lane == 0) s_red[warp] = wm;
+    __syncthreads();
+    wm = 0.0f;
+    for (int k = 0; k < nw; ++k) wm = (isnan(wm) || isnan(s_red[k])) ? __int_as_float(0x7fc00000) : fmaxf(wm, s_red[k]);
+    bad_weight = isnan(wm);
+    if (!bad_weight && wm > 0.0f) {
+      int e = 0;
+      frexpf(wm, &e);  // wm < 2^e
+      e = max(-100, min(100, e));
+      scale = ldexpf(1.0f, 21 - e);
+      inv_scale = ldexpf(1.0f, e - 21);
+    }
+  } else {
+    __syncthreads();  // the zeroed tile
+  }
+
   const int bx = bin % g.nb[0];
   const int brem = bin / g.nb[0];
   const int by = brem % g.nb[1];
@@ -976,7 +1026,8 @@ __global__ void __launch_bounds__(256) spread3d_warp_kernel(const Rec<3, T>* __r
     const Rec<3, T> rec = recs[start + p];
     int c0, c1, c2;
     unpack_cell(3, rec.cell, c0, c1, c2);
-    const T sr = weights ? weights[rec.idx] : uniform;
+    T sr = weights ? weights[rec.idx] : uniform;
+    if constexpr (FIXED) sr *= scale;
     T u0, u1, u2;
     const int s0 = es_start<W, T>(rec.f[0], u0);
     const int s1 = es_start<W, T>(rec.f[1], u1);
@@ -988,15 +1039,18 @@ __global__ void __launch_bounds__(256) spread3d_warp_kernel(const Rec<3, T>* __r
     const T kx = __shfl_sync(0xffffffffu, tap, col_ok ? c_in : 0);
     const T ky0 = __shfl_sync(0xffffffffu, tap, W + (r_in < W ? r_in : 0));
     const T ky1 = __shfl_sync(0xffffffffu, tap, W + (row1_ok ? r_in + 4 : 0));
-    const T a0 = sr * kx * ky0, a1 = sr * kx * ky1;
+    const T a0 = col_ok ? sr * kx * ky0 : T(0), a1 = (col_ok && row1_ok) ? sr * kx * ky1 : T(0);
     const int l0 = c0 - org0 + s0 + PAD, l1 = c1 - org1 + s1 + PAD, l2 = c2 - org2 + s2 + PAD;
-    const int base0 = (l2 * tw1 + l1 + r_in) * tw0p + l0 + c_in;
+    const int base0 = (l2 * tw1 + l1 + r_eff) * tw0p + l0 + c_in;
 #pragma unroll
     for (int m2 = 0; m2 < W; ++m2) {
       const T kz = __shfl_sync(0xffffffffu, tap, 2 * W + m2);
-      if (col_ok) {
+      if constexpr (FIXED) {
+        atomicAdd(&itile[base0 + m2 * plane], __float_as_int(fmaf(a0, kz, kRound)) - kRoundBits);
+        atomicAdd(&itile[base0 + m2 * plane + row1_off], __float_as_int(fmaf(a1, kz, kRound)) - kRoundBits);
+      } else {
         atomicAdd(&tile[base0 + m2 * plane], a0 * kz);
-        if (row1_ok) atomicAdd(&tile[base0 + m2 * plane + 4 * tw0p], a1 * kz);
+        atomicAdd(&tile[base0 + m2 * plane + row1_off], a1 * kz);
       }
     }
   }
@@ -1009,18 +1063,26 @@ __global__ void __launch_bounds__(256) spread3d_warp_kernel(const Rec<3, T>* __r
     const int r = i / tw0;
     const int i1 = r % tw1;
     const int i2 = r / tw1;
-    const T v = tile[(i2 * tw1 + i1) * tw0p + i0];
+    T v;
+    if constexpr (FIXED) v = T(itile[(i2 * tw1 + i1) * tw0p + i0]) * T(inv_scale);
+    else v = tile[(i2 * tw1 + i1) * tw0p + i0];
     if (v != T(0)) {
       const int64_t gi = (int64_t(wrap_index(o2 + i2, nf2)) * nf1 + wrap_index(o1 + i1, nf1)) * nf0 +
                          wrap_index(o0 + i0, nf0);
       atomicAdd(grid_real + gi, v);
     }
   }
+  if (bad_weight && threadIdx.x == 0) {
+    const int64_t gi = (int64_t(wrap_index(org2, nf2)) * nf1 + wrap_index(org1, nf1)) * nf0 + wrap_index(org0, nf0);
+    atomicAdd(grid_real + gi, T(__int_as_float(0x7fc00000)));
+  }
 }
 
-// Row pitch of spread3d_warp_kernel's tile: >= tw0, a multiple of 8, not of 16.
-inline int spread3d_pitch(int tw0) {
-  int p = (tw0 + 7) / 8 * 8;
+// Row pitch of spread3d_warp_kernel's tile: a multiple of 8, not of 16, with
+// room for the 8 - w columns past a footprint row that the lanes outside the
+// footprint touch (>= tw0 + 8 - w).
+inline int spread3d_pitch(int tw0, int w) {
+  int p = (tw0 + std::max(0, 8 - w) + 7) / 8 * 8;
   if (p % 16 == 0) p += 8;
   return p;
 }
@@ -1590,7 +1652,7 @@ void launch_spread_generic(const void* recs, const T* weights, T uniform, const 
                            const SortBufs& sb, const Geom& g, const std::vector<double>& poly, T* grid_real,
                            cplx_t<T>* grid_cplx, cudaStream_t s) {
   if constexpr (D == 3 && W <= 8 && !CPLX) {
-    const int pitch = spread3d_pitch(g.tw[0]);
+    const int pitch = spread3d_pitch(g.tw[0], W);
     const size_t smem3 = size_t(pitch) * g.tw[1] * g.tw[2] * sizeof(T);
     auto k3 = spread3d_warp_kernel<W, T>;
     if (smem3 <= 200 * 1024) {
