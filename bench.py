@@ -224,8 +224,7 @@ def sharded_report(args, dev, ws, rank):
                         "timing": "host wall clock around the C-level run loop, one rank"}
     # config 2's repulsion over spatial slabs with the halo exchange: the points in spatial order, one
     # equal slab per rank; each rank evaluates its own points' pairs against its halo
-    from fresco_b200 import ShardedInversePower
-    from fresco_b200.shard import spatial_order
+    from fresco_b200.shard import ShardedInversePower, spatial_order
 
     rr = np.full(N_POINTS, 0.25 / np.sqrt(N_POINTS) * 2 * np.pi)
     xs = x.reshape(-1, 2)[spatial_order(x, L)].ravel()

@@ -185,4 +185,14 @@ __device__ inline void block_sum_atomic_k(double (&v)[K], double* out) {
 // Number of SMs of the current device (cached per process for device 0..15).
 int sm_count();
 
+// Raises `kernel`'s dynamic shared-memory limit on the current device to at
+// least `bytes`.  The limit belongs to the function, which every object that
+// launches it shares, so it only ever grows: an object with a smaller need
+// never lowers the limit under another's captured or later launches.
+void ensure_dynamic_smem(const void* kernel, size_t bytes);
+template <typename K>
+inline void ensure_dynamic_smem(K* kernel, size_t bytes) {
+  ensure_dynamic_smem(reinterpret_cast<const void*>(kernel), bytes);
+}
+
 }  // namespace fb

@@ -735,12 +735,9 @@ class NUwUEnsembleImpl final : public Ensemble {
 
   template <int N>
   void band_attrs(const Group& gr) {
-    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(band_rows_r2c_kernel<T, N>),
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(gr.smem_rows)));
-    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(band_rows_c2c_kernel<T, N>),
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(gr.smem_rows)));
-    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(band_modes_kernel<T, N>),
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(gr.smem_modes)));
+    ensure_dynamic_smem(band_rows_r2c_kernel<T, N>, gr.smem_rows);
+    ensure_dynamic_smem(band_rows_c2c_kernel<T, N>, gr.smem_rows);
+    ensure_dynamic_smem(band_modes_kernel<T, N>, gr.smem_modes);
   }
 
   template <int N>
@@ -801,10 +798,8 @@ class NUwUEnsembleImpl final : public Ensemble {
   void smem_attrs_w() {
     constexpr size_t ss = spread2d_smem_bytes<W, T, false>();
     constexpr size_t si = interp2d_smem_bytes<W, T>();
-    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(spread2d_tile_kernel<W, T, false, EnsTileMap<T>>),
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(ss)));
-    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(interp2d_tile_kernel<W, T, EnsTileMap<T>>),
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(si)));
+    ensure_dynamic_smem(spread2d_tile_kernel<W, T, false, EnsTileMap<T>>, ss);
+    ensure_dynamic_smem(interp2d_tile_kernel<W, T, EnsTileMap<T>>, si);
   }
   void smem_attrs() {
 #define FB_X(WW) smem_attrs_w<WW>()
@@ -813,12 +808,8 @@ class NUwUEnsembleImpl final : public Ensemble {
     int most = 0;
     for (const auto& gp : groups_) most = std::max(most, gp->nbins);
     const int sb = int(sizeof(int)) * most;
-    if (sb > 48 * 1024) {
-      FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(ens_sort_count_kernel<T>),
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, sb));
-      FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(ens_sort_scatter_kernel<T>),
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, sb));
-    }
+    ensure_dynamic_smem(ens_sort_count_kernel<T>, size_t(sb));
+    ensure_dynamic_smem(ens_sort_scatter_kernel<T>, size_t(sb));
   }
 
   template <int W>

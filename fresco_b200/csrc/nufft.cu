@@ -1,6 +1,9 @@
 // Precision-independent NUFFT set-up: geometry and sort buffers.
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 
 #include "nufft.cuh"
 #include "scan.cuh"
@@ -23,6 +26,19 @@ int sm_count() {
   FB_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
   if (dev >= 0 && dev < 16) cache[dev] = n;
   return n;
+}
+
+void ensure_dynamic_smem(const void* kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return;  // within the default limit
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> limit;
+  int dev = 0;
+  FB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& cur = limit[{kernel, dev}];
+  if (bytes <= cur) return;
+  FB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+  cur = bytes;
 }
 
 Geom make_geom(int D, const int64_t* nf, int w, const int* tile_pref) {

@@ -1571,7 +1571,7 @@ bool onepass_setup(SortBufs& sb, int64_t N, const Geom& g) {
   const size_t smem = onepass_bin_bytes(int(g.nbins())) + size_t(chunk) * onepass_point_bytes<D, T>();
   if (chunk > 65535 || smem + 1024 > size_t(smem_max)) return false;
   auto kern = sort_onepass_kernel<D, T>;
-  FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  ensure_dynamic_smem(kern, smem);
   int occ = 0;
   FB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kOneThreads, smem));
   if (occ < 1 || blocks > occ * sm_count()) return false;
@@ -1611,8 +1611,8 @@ void bin_sort_d(const double* pts, int64_t N, const MapParams& mp, const Geom& g
   }
   Rec<D, T>* unsorted = reinterpret_cast<Rec<D, T>*>(sb.unsorted.p);
   if (smem > 48 * 1024) {
-    FB_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    FB_CUDA(cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    ensure_dynamic_smem(k1, smem);
+    ensure_dynamic_smem(k3, smem);
   }
   if (N > 0) {
     k1<<<sb.NB, kSortThreads, smem, s>>>(pts, N, sb.chunk, m2, g, sb.bin_total.p, sb.blk_off.p, unsorted, status);
@@ -1640,7 +1640,7 @@ void launch_spread2d(const void* recs, const T* weights, T uniform, const cplx_t
                      cudaStream_t s) {
   constexpr size_t smem = spread2d_smem_bytes<W, T, CPLX>();
   auto kern = spread2d_tile_kernel<W, T, CPLX, TileMap1<T>>;
-  if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  if (smem > 48 * 1024) ensure_dynamic_smem(kern, smem);
   const TileMap1<T> map{sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, sb.bin_start.p, nullptr, uniform};
   kern<<<unsigned(sb.max_sub), Tile2D<W>::THREADS, smem, s>>>(static_cast<const Rec<2, T>*>(recs), weights, strengths,
                                                               map, g, make_es_poly<W, T>(poly), grid_real, grid_cplx);
@@ -1657,7 +1657,7 @@ void launch_spread_generic(const void* recs, const T* weights, T uniform, const 
     auto k3 = spread3d_warp_kernel<W, T>;
     if (smem3 <= 200 * 1024) {
       if (smem3 > 48 * 1024)
-        FB_CUDA(cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem3)));
+        ensure_dynamic_smem(k3, smem3);
       k3<<<unsigned(sb.max_sub), 256, smem3, s>>>(static_cast<const Rec<3, T>*>(recs), weights, uniform,
                                                  sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g,
                                                  make_es_poly<W, T>(poly), pitch, grid_real);
@@ -1667,7 +1667,7 @@ void launch_spread_generic(const void* recs, const T* weights, T uniform, const 
   }
   const size_t smem = size_t(g.tile_cells()) * sizeof(T) * (CPLX ? 2 : 1);
   auto kern = spread_kernel<D, W, T, CPLX>;
-  if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  if (smem > 48 * 1024) ensure_dynamic_smem(kern, smem);
   kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<D, T>*>(recs), weights, uniform, strengths,
                                                 sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g,
                                                 make_es_poly<W, T>(poly), grid_real, grid_cplx);
@@ -1713,7 +1713,7 @@ void launch_interp2d(const void* recs, const T* weights, T uniform, const SortBu
                      int acc, const int* status, cudaStream_t s, const GradScale& gs, double* fail_energy) {
   constexpr size_t smem = interp2d_smem_bytes<W, T>();
   auto kern = interp2d_tile_kernel<W, T, TileMap1<T>>;
-  if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  if (smem > 48 * 1024) ensure_dynamic_smem(kern, smem);
   TileMap1<T> map{sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, sb.bin_start.p, status, uniform};
   map.polls = tile_wait_polls_setting();
   map.energy = fail_energy;
@@ -1741,7 +1741,7 @@ bool launch_interp3d(const void* recs, const T* weights, T uniform, const SortBu
     auto kern1 = interp3d_tile_kernel<W, T, 1>;
     auto kern = nfields == 2 ? kern2 : kern1;
     if (smem > 48 * 1024)
-      FB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      ensure_dynamic_smem(kern, smem);
     kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<3, T>*>(recs), weights, uniform, sb.sub_bin.p,
                                                  sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g,
                                                  make_es_poly<W, T>(poly), fields, mode, grad, out2, acc, status, gs);

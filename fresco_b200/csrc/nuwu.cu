@@ -400,12 +400,9 @@ class NUwUImpl final : public Potential, public NUwUShard {
     const size_t cb = sizeof(cplx_t<T>);
     smem_rows_ = 2 * size_t(fft_padded(N)) * cb;
     smem_modes_ = 3 * size_t(fft_padded(N)) * cb;
-    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(band_rows_r2c_kernel<T, N>),
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_rows_)));
-    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(band_rows_c2c_kernel<T, N>),
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_rows_)));
-    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(band_modes_kernel<T, N>),
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_modes_)));
+    ensure_dynamic_smem(band_rows_r2c_kernel<T, N>, smem_rows_);
+    ensure_dynamic_smem(band_rows_c2c_kernel<T, N>, smem_rows_);
+    ensure_dynamic_smem(band_modes_kernel<T, N>, smem_modes_);
   }
 
   void setup_band(const std::vector<int>& idx, const std::vector<ModeCoef>& coef) {

@@ -809,7 +809,7 @@ class Lbfgs final : public Optimizer {
     const int64_t chunk = ceil_div(n_, blocks);
     const size_t smem = size_t(chunk) * sizeof(double);
     if (smem + 2048 > size_t(smem_max)) return false;
-    FB_CUDA(cudaFuncSetAttribute(lb_direction_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    ensure_dynamic_smem(lb_direction_kernel, smem);
     int occ = 0;
     FB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, lb_direction_kernel, kDirThreads, smem));
     if (occ < 1 || blocks > occ * sm_count()) return false;

@@ -231,7 +231,7 @@ void export_structure_d(const double* x, int64_t N, const double* L, int Nk, con
   FB_CUDA(cudaMemset(rcnt.p, 0, rcnt.bytes()));
   const size_t smem = size_t(nb) * (sizeof(double) + sizeof(unsigned));
   auto rk = radial_sum_kernel<D>;
-  if (smem > 48 * 1024) FB_CUDA(cudaFuncSetAttribute(rk, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  if (smem > 48 * 1024) ensure_dynamic_smem(rk, smem);
   rk<<<blocks, 256, smem, s>>>(sk.p, Nk, rsum.p, rcnt.p);
   rk<<<blocks, 256, smem, s>>>(gr.p, Nk, rsum.p + nb, rcnt.p + nb);
   FB_LAUNCH_CHECK();

@@ -446,12 +446,9 @@ class UwUImpl final : public Potential {
 
   template <int N>
   void band_attrs() {
-    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(uwu_band_rows_fwd<T, N>),
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_)));
-    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(uwu_band_modes<T, N>),
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_)));
-    FB_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(uwu_band_rows_c2r<T, N>),
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_)));
+    ensure_dynamic_smem(uwu_band_rows_fwd<T, N>, smem_);
+    ensure_dynamic_smem(uwu_band_modes<T, N>, smem_);
+    ensure_dynamic_smem(uwu_band_rows_c2r<T, N>, smem_);
   }
 
   template <int N>

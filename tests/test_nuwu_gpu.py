@@ -214,3 +214,26 @@ def test_interp_tile_copy_second_wait(prec, eps, tol):
     after = NUwU(radii, K, Sk, V, L, eps=eps, precision=prec)
     after.get_energy_gradient(x)
     assert after.status() == 0
+
+
+def test_objects_of_different_sizes_interleave():
+    """A kernel's shared-memory limit is shared by every object that launches it: a smaller object
+    made later must not lower it under a larger one (one-pass sorts of 800K and 500K points, and the
+    LBFGS two-loop kernels of their 1.6M and 1M coordinates, interleaved)."""
+    from fresco_b200 import NUwU
+    from fresco_b200.optimize import LBFGS_CPP
+
+    pots, xs = [], []
+    for n in (800_000, 500_000):
+        x, radii, Sk, V, L = O.stealthy_nuwu_inputs(n, 16, 8, ndim=2, seed=n % 97)
+        pots.append(NUwU(radii, 16, Sk, V, L, eps=1e-6, precision="fp32"))
+        xs.append(x)
+    e_big = pots[0].get_energy_gradient(xs[0])[0]
+    e_small = pots[1].get_energy_gradient(xs[1])[0]
+    assert np.isfinite(e_small)
+    assert abs(pots[0].get_energy_gradient(xs[0])[0] - e_big) <= 1e-6 * abs(e_big)
+    opts = [LBFGS_CPP(x, p, M=4) for x, p in zip(xs, pots)]
+    for _ in range(2):
+        for o in opts:
+            o.one_iteration()
+    assert all(np.isfinite(o.get_result().energy) for o in opts)
