@@ -73,6 +73,7 @@ _SIGNATURES = {
     "fresco_inversepower_halo_stats": (C.c_int, [handle_t, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "fresco_optimizer_set_reducer": (C.c_int, [handle_t, c_void_p, c_void_p, c_int64]),
     "fresco_potential_set_gradient_mode": (C.c_int, [handle_t, C.c_int]),
+    "fresco_potential_gradient_mode": (C.c_int, [handle_t, c_int_p]),
     "fresco_potential_set_timing": (C.c_int, [handle_t, C.c_int]),
     "fresco_potential_get_timing": (C.c_int, [handle_t, C.c_int, C.c_char_p, C.c_int, c_double_p, c_int_p, c_int_p]),
     "fresco_potential_describe": (C.c_int, [handle_t, C.c_char_p, C.c_int]),

@@ -100,5 +100,52 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
     return LIB
 
 
+TORCH_OPS_SRC = CSRC / "torch_ops.cpp"
+TORCH_LIB = PKG / "libfresco_torch.so"
+
+
+def build_torch_ops(verbose: bool = False) -> Path:
+    """Compiles the PyTorch operator library (csrc/torch_ops.cpp) against the
+    installed torch's headers and libfresco_b200.so into
+    fresco_b200/libfresco_torch.so."""
+    newest = max(TORCH_OPS_SRC.stat().st_mtime, LIB.stat().st_mtime, _newest_header())
+    if TORCH_LIB.exists() and TORCH_LIB.stat().st_mtime >= newest:
+        return TORCH_LIB
+    import torch
+    from torch.utils import cpp_extension
+
+    torch_lib = Path(torch.__file__).resolve().parent / "lib"
+    tmp = TORCH_LIB.with_suffix(".so.tmp")
+    cmd = [
+        os.environ.get("CXX", "g++"),
+        "-O2",
+        "-std=c++17",
+        "-fPIC",
+        "-shared",
+        f"-D_GLIBCXX_USE_CXX11_ABI={int(torch._C._GLIBCXX_USE_CXX11_ABI)}",
+        *[f"-I{p}" for p in cpp_extension.include_paths()],
+        f"-I{_cuda_home() / 'include'}",
+        f"-I{INCLUDE}",
+        str(TORCH_OPS_SRC),
+        "-o",
+        str(tmp),
+        f"-L{torch_lib}",
+        "-lc10",
+        "-lc10_cuda",
+        "-ltorch_cpu",
+        f"-L{PKG}",
+        "-lfresco_b200",
+        "-Wl,-rpath,$ORIGIN",
+    ]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"torch operator build failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, TORCH_LIB)
+    return TORCH_LIB
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))
+    print(build_torch_ops(verbose="-v" in sys.argv))

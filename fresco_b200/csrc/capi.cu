@@ -393,6 +393,14 @@ int fresco_potential_set_gradient_mode(fresco_potential p, int mode) {
   });
 }
 
+int fresco_potential_gradient_mode(fresco_potential p, int* mode) {
+  return guarded([&] {
+    if (!p || !mode) throw fb::InvalidArgument("null argument");
+    *mode = p->pot->gradient_mode();
+    return FRESCO_OK;
+  });
+}
+
 int fresco_potential_set_timing(fresco_potential p, int enabled) {
   return guarded([&] {
     if (!p) throw fb::InvalidArgument("null handle");

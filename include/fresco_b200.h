@@ -268,6 +268,8 @@ int fresco_debug_set_tile_wait_polls(int polls);
  * divides by 2 pi, uwnu.hpp:352; NUwNU omits conj(c_j), nuwnu.hpp:269; UwU
  * halves the rho term and drops d(1/R), uwu.hpp:178). */
 int fresco_potential_set_gradient_mode(fresco_potential p, int mode);
+/* The handle's current gradient convention (0 or 1). */
+int fresco_potential_gradient_mode(fresco_potential p, int* mode);
 
 /* Per-stage device timing of the next evaluations (CUDA events). */
 int fresco_potential_set_timing(fresco_potential p, int enabled);
