@@ -140,6 +140,18 @@ def ensemble_report(args, dev, ws, rank):
                     round(reduce_sum(float(np.sum(it1 - it0)), dev) / lb_s, 1),
                     "patterns_lower_energy": int(reduce_sum(float(np.sum(f1 < f0)), dev)), "M": 4,
                     "timing": "host wall clock around the graph launches of steps(), max over ranks"}
+    # run(niter): the whole minimisation as ONE graph launch (a conditional WHILE node repeats the step
+    # while a pattern is still iterating)
+    n_run = max(10, args.steps // 2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    used = opt.run(n_run)
+    run_s = reduce_max(time.perf_counter() - t0, dev)
+    _, _, _, _, it2, _, _ = opt.state(False)
+    out["lbfgs"]["run_one_launch"] = {
+        "niter": n_run, "steps": int(used), "steps_per_s": round(used / run_s, 2),
+        "pattern_iterations_per_s": round(reduce_sum(float(np.sum(it2 - it1)), dev) / run_s, 1),
+        "timing": "host wall clock around run(), one graph launch, max over ranks"}
     del opt
     if ws == 1 and not args.no_ensemble_loop:
         # the same patterns as separate potentials, one after another on one stream

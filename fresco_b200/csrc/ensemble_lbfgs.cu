@@ -16,8 +16,12 @@
 //   direction (1 + 2M launches, patterns that need none skip them)
 //   -> trial point -> evaluation of every pattern -> accept test and memory
 //   update (post) -> per-pattern state update (finalize)
-// captured once as a CUDA graph; run() replays it and reads the number of
-// still-iterating patterns every few steps.
+// captured once as a CUDA graph.  steps(n) replays it n times; run(niter) is
+// one graph launch: a conditional WHILE node repeats the step while a
+// pattern is still iterating (checked on the device after every step), so
+// the host waits once per run (the host-driven loop that reads the number of
+// still-iterating patterns every few steps remains for a CUDA build that
+// cannot capture the step into a conditional body).
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -185,6 +189,28 @@ __global__ void bl_count_active(const BlState* __restrict__ st, int P, int* out)
     for (int w = 0; w < int(blockDim.x >> 5); ++w) t += sh[w];
     *out = t;
   }
+}
+
+// The run loop's condition (run(niter) as one graph launch): continue while a
+// pattern is still iterating and fewer than guard[1] steps have run; guard[0]
+// counts the steps.  `first` marks the check before the first step.
+__global__ void bl_loop(const BlState* __restrict__ st, int P, int* guard, cudaGraphConditionalHandle h, int first) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int p = threadIdx.x; p < P; p += blockDim.x)
+    if (st[p].active) any = 1;  // every writer stores the same value
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int taken = first ? 0 : guard[0] + 1;
+    guard[0] = taken;
+    cudaGraphSetConditional(h, (any && taken < guard[1]) ? 1u : 0u);
+  }
+}
+
+__global__ void bl_guard_init(int* guard, int limit) {
+  guard[0] = 0;
+  guard[1] = limit;
 }
 
 // step = g and the first dot: |g|^2 for k = 0, s_(k-1) . g otherwise.
@@ -428,6 +454,12 @@ struct EnsembleLbfgs::Impl {
   cudaStream_t s = nullptr, cap = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_version = -1;
+  // run(niter) as one launch: a conditional WHILE node repeating the step
+  cudaGraphExec_t run_graph = nullptr;
+  int run_graph_version = -1;
+  bool run_graph_unavailable = false;
+  DevBuf<int> guard;
+  int* host_guard = nullptr;
   bool initialized = false;
 
   void initialize() {
@@ -473,6 +505,72 @@ struct EnsembleLbfgs::Impl {
     cudaGraphDestroy(gr);
     FB_CUDA(ie);
     graph_version = ens->version();
+  }
+
+  // Top graph: a check kernel, then a WHILE node whose body is one step and
+  // the check.  Returns false (and keeps the host-driven loop) when this CUDA
+  // build cannot capture the step into a conditional body.
+  bool ensure_run_graph() {
+    if (run_graph_unavailable) return false;
+    if (run_graph && run_graph_version == ens->version()) return true;
+    if (run_graph) {
+      cudaGraphExecDestroy(run_graph);
+      run_graph = nullptr;
+    }
+    if (!cap) FB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaGraph_t top = nullptr;
+    FB_CUDA(cudaGraphCreate(&top, 0));
+    bool ok = false;
+    try {
+      cudaGraphConditionalHandle hw;
+      FB_CUDA(cudaGraphConditionalHandleCreate(&hw, top, 0, cudaGraphCondAssignDefault));
+      BlState* stp = st.p;
+      int* gp = guard.p;
+      int Pv = P, first = 1;
+      void* pre_args[] = {&stp, &Pv, &gp, &hw, &first};
+      cudaKernelNodeParams kp{};
+      kp.func = reinterpret_cast<void*>(bl_loop);
+      kp.gridDim = dim3(1);
+      kp.blockDim = dim3(256);
+      kp.kernelParams = pre_args;
+      cudaGraphNode_t pre;
+      FB_CUDA(cudaGraphAddKernelNode(&pre, top, nullptr, 0, &kp));
+      cudaGraphNodeParams wp{};
+      wp.type = cudaGraphNodeTypeConditional;
+      wp.conditional.handle = hw;
+      wp.conditional.type = cudaGraphCondTypeWhile;
+      wp.conditional.size = 1;
+      cudaGraphNode_t wn;
+      FB_CUDA(cudaGraphAddNode(&wn, top, &pre, 1, &wp));
+      cudaGraph_t body = wp.conditional.phGraph_out[0];
+      FB_CUDA(cudaStreamBeginCaptureToGraph(cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+      cudaGraph_t captured = nullptr;
+      cudaError_t ce = cudaSuccess;
+      try {
+        issue_step(cap);
+        bl_loop<<<1, 256, 0, cap>>>(st.p, P, guard.p, hw, 0);
+        ce = cudaPeekAtLastError();
+      } catch (...) {
+        cudaStreamEndCapture(cap, &captured);
+        throw;
+      }
+      const cudaError_t ee = cudaStreamEndCapture(cap, &captured);
+      if (ce == cudaSuccess && ee == cudaSuccess) ok = cudaGraphInstantiate(&run_graph, top, 0) == cudaSuccess;
+    } catch (const CudaError&) {
+      ok = false;
+    } catch (...) {
+      cudaGraphDestroy(top);
+      throw;
+    }
+    cudaGraphDestroy(top);
+    if (!ok) {
+      cudaGetLastError();  // capture and instantiation errors are not sticky
+      run_graph = nullptr;
+      run_graph_unavailable = true;
+      return false;
+    }
+    run_graph_version = ens->version();
+    return true;
   }
 
   int active_count() {
@@ -537,6 +635,8 @@ EnsembleLbfgs::EnsembleLbfgs(EnsemblePtr ens, const double* x0, int64_t n, const
   I.st.alloc(I.P);
   FB_CUDA(cudaMemcpy(I.st.p, hs.data(), sizeof(BlState) * I.P, cudaMemcpyHostToDevice));
   FB_CUDA(cudaMallocHost(&I.host_count, sizeof(int)));
+  FB_CUDA(cudaMallocHost(&I.host_guard, sizeof(int)));
+  I.guard.alloc(2);
   FB_CUDA(cudaStreamCreateWithFlags(&I.s, cudaStreamNonBlocking));
   FB_CUDA(cudaDeviceSynchronize());
 }
@@ -545,6 +645,8 @@ EnsembleLbfgs::~EnsembleLbfgs() {
   Impl& I = *impl_;
   if (I.s) cudaStreamSynchronize(I.s);
   if (I.graph) cudaGraphExecDestroy(I.graph);
+  if (I.run_graph) cudaGraphExecDestroy(I.run_graph);
+  if (I.host_guard) cudaFreeHost(I.host_guard);
   if (I.cap) cudaStreamDestroy(I.cap);
   if (I.s) cudaStreamDestroy(I.s);
   if (I.host_count) cudaFreeHost(I.host_count);
@@ -567,9 +669,17 @@ int EnsembleLbfgs::run(int niter) {
   if (!I.initialized) I.initialize();
   bl_set_stop<<<int(ceil_div(I.P, 128)), 128, 0, I.s>>>(I.st.p, I.P, niter, I.bp);
   FB_LAUNCH_CHECK();
-  I.ensure_graph();
   // every iteration takes at most ten evaluations
   const int64_t max_steps = int64_t(niter) * 10;
+  if (max_steps < (int64_t(1) << 30) && I.ensure_run_graph()) {  // one launch for the whole run
+    bl_guard_init<<<1, 1, 0, I.s>>>(I.guard.p, int(max_steps));
+    FB_LAUNCH_CHECK();
+    FB_CUDA(cudaGraphLaunch(I.run_graph, I.s));
+    FB_CUDA(cudaMemcpyAsync(I.host_guard, I.guard.p, sizeof(int), cudaMemcpyDeviceToHost, I.s));
+    FB_CUDA(cudaStreamSynchronize(I.s));
+    return *I.host_guard;
+  }
+  I.ensure_graph();
   int64_t taken = 0;
   int chunk = 2;
   while (taken < max_steps && I.active_count() > 0) {
