@@ -308,6 +308,9 @@ __global__ void __launch_bounds__(kThreads) cell_pair_kernel(const PairRec<D>* _
     int nq = 0;
     if (i < N) me = recs[i];
     const bool active = i < N && me.idx - own_lo < own_n;
+    // a warp of halo records only has nothing to do (and no range to stage:
+    // its empty min/max would overflow the span test below)
+    if (!__any_sync(0xffffffffu, active)) continue;
     // phase 1: candidates within reach -> queue
     bool staged = false;
     if constexpr (D == 2) {
@@ -746,16 +749,32 @@ __device__ __forceinline__ int column_of(double v, const Box& b) {
 
 __device__ __forceinline__ bool column_bit(const uint32_t* __restrict__ m, int c) { return (m[c >> 5] >> (c & 31)) & 1u; }
 
-// Own points: their columns' marks, and their copy at the head of the combined set.
+// Own points: their copy at the head of the combined set and, if mask is not
+// null, their columns' marks.  The lanes of a warp that mark the same word
+// combine their bits first (points in spatial order share a few columns), so
+// a warp issues one atomic per distinct word.
 template <int D>
 __global__ void halo_own_kernel(const double* __restrict__ x, int64_t n, Box b, uint32_t lo, uint32_t* mask,
                                 double* comb_x, uint32_t* comb_idx) {
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    const int c = column_of(x[i * D], b);
-    atomicOr(mask + (c >> 5), 1u << (c & 31));
+  const int lane = threadIdx.x & 31;
+  for (int64_t b0 = int64_t(blockIdx.x) * blockDim.x; b0 < n; b0 += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = b0 + threadIdx.x;  // the whole warp iterates together
+    const bool valid = i < n;
+    int word = -1;
+    uint32_t bit = 0u;
+    if (valid) {
+      const int c = column_of(x[i * D], b);
+      word = c >> 5;
+      bit = 1u << (c & 31);
 #pragma unroll
-    for (int a = 0; a < D; ++a) comb_x[i * D + a] = x[i * D + a];
-    comb_idx[i] = lo + uint32_t(i);
+      for (int a = 0; a < D; ++a) comb_x[i * D + a] = x[i * D + a];
+      comb_idx[i] = lo + uint32_t(i);
+    }
+    if (mask) {
+      const unsigned grp = __match_any_sync(0xffffffffu, word);
+      const uint32_t bits = __reduce_or_sync(grp, bit);
+      if (word >= 0 && lane == __ffs(grp) - 1) atomicOr(mask + word, bits);
+    }
   }
 }
 
@@ -903,7 +922,9 @@ class InversePowerHalo final : public Potential {
   }
 
  private:
-  int grid_for(int64_t n) const { return int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, kThreads), int64_t(sm_count()) * 8))); }
+  int grid_for(int64_t n) const {
+    return int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, kThreads), int64_t(sm_count()) * 8)));
+  }
 
   int read_count(int which, cudaStream_t s) {
     FB_CUDA(cudaMemcpyAsync(host_counts_ + which, counts_dev_.p + which, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -920,44 +941,49 @@ class InversePowerHalo final : public Potential {
     FB_CUDA(cudaMemsetAsync(counts_dev_.p, 0, 2 * sizeof(int), s));
     FB_CUDA(cudaMemsetAsync(e_part_.p, 0, sizeof(double), s));
     if (n > 0) {
-      halo_own_kernel<D><<<grid_for(n), kThreads, 0, s>>>(x, n, box_, uint32_t(lo_), mask_.p, comb_x_.p,
-                                                          comb_idx_.p);
+      halo_own_kernel<D><<<grid_for(n), kThreads, 0, s>>>(x, n, box_, uint32_t(lo_), nranks_ > 1 ? mask_.p : nullptr,
+                                                          comb_x_.p, comb_idx_.p);
       FB_LAUNCH_CHECK();
     }
-    mask_to_double_kernel<<<1, 256, 0, s>>>(mask_.p, nwords_, mask_d_.p);
-    FB_LAUNCH_CHECK();
-    // 1. every process's column marks
-    gatherv_(mask_d_.p, nwords_, marks_.p, int64_t(nranks_) * nwords_, counts_.data(), s, ctx_);
-    for (int q = 0; q < nranks_; ++q)
-      if (counts_[size_t(q)] != nwords_) throw CudaError("halo exchange: the processes disagree on the column grid");
-    // 2. need / reach, 3. the export
-    halo_columns_kernel<<<1, 1024, 0, s>>>(marks_.p, nranks_, rank_, nwords_, ncol_, need_.p, reach_.p);
-    FB_LAUNCH_CHECK();
-    if (n > 0) {
-      halo_export_kernel<D><<<grid_for(n), kThreads, 0, s>>>(x, n, box_, uint32_t(lo_), need_.p, exp_.p,
-                                                             counts_dev_.p);
+    exported_ = 0;
+    halo_ = 0;
+    if (nranks_ > 1) {  // one process has no other process to exchange with
+      mask_to_double_kernel<<<1, 256, 0, s>>>(mask_.p, nwords_, mask_d_.p);
       FB_LAUNCH_CHECK();
-    }
-    exported_ = read_count(0, s);
-    gatherv_(exp_.p, exported_ * (D + 1), recv_.p, std::max<int64_t>(N_, 1) * (D + 1), counts_.data(), s, ctx_);
-    int64_t total = 0, skip_lo = 0;
-    for (int q = 0; q < nranks_; ++q) {
-      const int64_t c = counts_[size_t(q)];
-      if (c < 0 || c % (D + 1)) throw CudaError("halo exchange: a process sent a partial record");
-      if (q < rank_) skip_lo += c;
-      total += c;
-    }
-    if (counts_[size_t(rank_)] != exported_ * (D + 1) || total > std::max<int64_t>(N_, 1) * (D + 1))
-      throw CudaError("halo exchange: the gathered sizes do not add up");
-    // 4. the halo and the cell list over own + halo points
-    const int64_t n_recv = total / (D + 1);
-    if (n_recv > 0) {
-      halo_keep_kernel<D><<<grid_for(n_recv), kThreads, 0, s>>>(
-          recv_.p, n_recv, skip_lo / (D + 1), skip_lo / (D + 1) + exported_, box_, reach_.p, n, N_ - n, N_,
-          comb_x_.p, comb_idx_.p, counts_dev_.p + 1, status_.p);
+      // 1. every process's column marks
+      gatherv_(mask_d_.p, nwords_, marks_.p, int64_t(nranks_) * nwords_, counts_.data(), s, ctx_);
+      for (int q = 0; q < nranks_; ++q)
+        if (counts_[size_t(q)] != nwords_)
+          throw CudaError("halo exchange: the processes disagree on the column grid");
+      // 2. need / reach, 3. the export
+      halo_columns_kernel<<<1, 1024, 0, s>>>(marks_.p, nranks_, rank_, nwords_, ncol_, need_.p, reach_.p);
       FB_LAUNCH_CHECK();
+      if (n > 0) {
+        halo_export_kernel<D><<<grid_for(n), kThreads, 0, s>>>(x, n, box_, uint32_t(lo_), need_.p, exp_.p,
+                                                               counts_dev_.p);
+        FB_LAUNCH_CHECK();
+      }
+      exported_ = read_count(0, s);
+      gatherv_(exp_.p, exported_ * (D + 1), recv_.p, std::max<int64_t>(N_, 1) * (D + 1), counts_.data(), s, ctx_);
+      int64_t total = 0, skip_lo = 0;
+      for (int q = 0; q < nranks_; ++q) {
+        const int64_t c = counts_[size_t(q)];
+        if (c < 0 || c % (D + 1)) throw CudaError("halo exchange: a process sent a partial record");
+        if (q < rank_) skip_lo += c;
+        total += c;
+      }
+      if (counts_[size_t(rank_)] != exported_ * (D + 1) || total > std::max<int64_t>(N_, 1) * (D + 1))
+        throw CudaError("halo exchange: the gathered sizes do not add up");
+      // 4. the halo and the cell list over own + halo points
+      const int64_t n_recv = total / (D + 1);
+      if (n_recv > 0) {
+        halo_keep_kernel<D><<<grid_for(n_recv), kThreads, 0, s>>>(
+            recv_.p, n_recv, skip_lo / (D + 1), skip_lo / (D + 1) + exported_, box_, reach_.p, n, N_ - n, N_,
+            comb_x_.p, comb_idx_.p, counts_dev_.p + 1, status_.p);
+        FB_LAUNCH_CHECK();
+      }
+      halo_ = std::min<int64_t>(read_count(1, s), N_ - n);
     }
-    halo_ = std::min<int64_t>(read_count(1, s), N_ - n);
     const int64_t nc = n + halo_;
     if (nc > 0) {
       const int grid = grid_for(nc);
@@ -973,7 +999,7 @@ class InversePowerHalo final : public Potential {
       FB_LAUNCH_CHECK();
     }
     // 5. the pattern's energy on every process
-    reduce_(e_part_.p, 1, s, ctx_);
+    if (nranks_ > 1) reduce_(e_part_.p, 1, s, ctx_);
     if (g && n > 0) {
       nan_if_nan_energy_kernel<<<grid_for(n * D), kThreads, 0, s>>>(e_part_.p, g, n * D);
       FB_LAUNCH_CHECK();
