@@ -794,6 +794,23 @@ def run_ours(args):
         eh, gh = pot32.get_energy_gradient(x_host, out=g_host)
     e2e_s = (time.perf_counter() - t0) / ne2e
     e2e_value = ws / reduce_max(e2e_s, dev)
+    # the host link's own floor for this call: the same bytes copied alone (pinned, CUDA events)
+    xd_link = torch.empty(x.size, dtype=torch.float64, device=dev)
+    x_pin, g_pin = torch.from_numpy(x_host), torch.from_numpy(g_host)
+    link = {}
+    for name, dst, src in (("h2d_gbs", xd_link, x_pin), ("d2h_gbs", g_pin, xd_link)):
+        for _ in range(2):
+            dst.copy_(src, non_blocking=True)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(5):
+            dst.copy_(src, non_blocking=True)
+        b.record(stream)
+        torch.cuda.synchronize()
+        link[name] = round(5 * x.nbytes / (a.elapsed_time(b) * 1e-3) / 1e9, 2)
+    link_ms = x.nbytes / (link["h2d_gbs"] * 1e9) * 1e3 + (x.nbytes + 8) / (link["d2h_gbs"] * 1e9) * 1e3
+    del xd_link
 
     # roofline: per-stage device times from CUDA events on the launch stream
     # d_f = 1: the two gradient fields are interpolated as one Hermitian-packed complex field
@@ -867,7 +884,9 @@ def run_ours(args):
                    "setup": desc, "l2": "flushed between timed steps (256 MiB write)",
                    "parallelism": f"independent pattern per GPU x{ws}"},
         "e2e": {"value": round(e2e_value, 2), "unit": "evals/s", "h2d_bytes_per_step": int(x.nbytes),
-                "d2h_bytes_per_step": int(x.nbytes + 8)},
+                "d2h_bytes_per_step": int(x.nbytes + 8), "host_link": link,
+                "copy_floor_ms": round(link_ms, 4),
+                "copy_plus_device_ms": round(link_ms + ms_per_step, 4), "ms_per_step": round(1e3 / e2e_value, 4)},
         "gpu_launches": launches,
         "roofline": roofline,
         "roofline_eval": roofline_eval,
