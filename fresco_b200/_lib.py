@@ -113,6 +113,7 @@ _SIGNATURES = {
     "fresco_ensemble_energy_gradient": (C.c_int, [handle_t, c_double_p, c_int64, c_double_p, c_double_p]),
     "fresco_ensemble_energy_gradient_device": (C.c_int, [handle_t, c_void_p, c_int64, c_void_p, c_void_p, c_void_p]),
     "fresco_ensemble_tune": (C.c_int, [handle_t, c_double_p, c_int64]),
+    "fresco_ensemble_set_subproblem_cap": (C.c_int, [handle_t, C.c_int]),
     "fresco_ensemble_set_split": (C.c_int, [handle_t, C.c_double]),
     "fresco_ensemble_status": (C.c_int, [handle_t, c_int_p]),
     "fresco_ensemble_describe": (C.c_int, [handle_t, C.c_char_p, C.c_int]),

@@ -704,6 +704,14 @@ int fresco_ensemble_set_split(fresco_ensemble h, double ratio) {
   });
 }
 
+int fresco_ensemble_set_subproblem_cap(fresco_ensemble h, int cap) {
+  return guarded([&] {
+    if (!h) throw fb::InvalidArgument("null argument");
+    h->ens->set_subproblem_cap(cap);
+    return FRESCO_OK;
+  });
+}
+
 int fresco_ensemble_status(fresco_ensemble h, int* status) {
   return guarded([&] {
     if (!h || !status) throw fb::InvalidArgument("null argument");

@@ -80,6 +80,9 @@ namespace {
 constexpr int kEnsSortThreads = 512;
 constexpr int kEnsSortChunk = 2048;  // points per sort block
 constexpr int kDirectPts = 256;      // points per block of the direct spread / interpolation
+// Subproblem sizes (points per tile block) the tuner tries, smallest first;
+// the subproblem slots are sized for the smallest.
+constexpr int kSubCaps[3] = {kMaxSub / 4, kMaxSub / 2, kMaxSub};
 
 // Per pattern of a group (device copy read with one load per block).
 struct alignas(16) PatInfo {
@@ -95,7 +98,7 @@ struct alignas(16) PatInfo {
   int pid;           // pattern index in the ensemble
   int mode_base;     // first active mode in the group's mode table
   int n_active;      // active modes
-  int pad_;
+  int sub_cap;       // points per subproblem at most (<= kMaxSub; tuned per group)
 };
 
 struct SortItem {
@@ -173,7 +176,7 @@ __global__ void __launch_bounds__(kEnsSortThreads) ens_sort_scatter_kernel(
   for (int b = b0; b < b1; ++b) {
     const int c = tot[b];
     npts += c;
-    nsub += (c + kMaxSub - 1) / kMaxSub;
+    nsub += (c + pi.sub_cap - 1) / pi.sub_cap;
   }
   int tot_pts;
   int run = block_exclusive_scan(npts, &tot_pts, s_warp);
@@ -189,7 +192,7 @@ __global__ void __launch_bounds__(kEnsSortThreads) ens_sort_scatter_kernel(
     int st = pi.rec_base + first_start;
     for (int b = b0; b < b1; ++b) {
       const int c = tot[b];
-      const int parts = (c + kMaxSub - 1) / kMaxSub;  // equal parts of at most kMaxSub points
+      const int parts = (c + pi.sub_cap - 1) / pi.sub_cap;  // equal parts of at most sub_cap points
       for (int q = 0; q < parts; ++q) {
         if (sbase < pi.max_sub) {
           const int si = pi.sub_base + sbase;
@@ -392,6 +395,7 @@ class NUwUEnsembleImpl final : public Ensemble {
     int nbins = 1, nh0 = 1;
     int64_t G = 1, GH = 1, NG = 0;
     std::vector<PatInfo> pats_h;
+    int sub_cap = kMaxSub;  // points per subproblem (tune())
     DevBuf<PatInfo> pats;
     int n_items = 0;
     DevBuf<SortItem> items;
@@ -527,21 +531,27 @@ class NUwUEnsembleImpl final : public Ensemble {
     for (auto& gp : groups_) {
       Group& gr = *gp;
       double best_ms = 1e300, best_ratio = gr.ratio;
-      for (double r : {0.0, 0.0625, 0.25, 1.0, 4.0, 16.0, 1e30}) {
-        set_split(gr, r);
-        run_group(gr, x, g, e, s);  // warm-up
-        FB_CUDA(cudaEventRecord(t0, s));
-        for (int rep = 0; rep < 3; ++rep) run_group(gr, x, g, e, s);
-        FB_CUDA(cudaEventRecord(t1, s));
-        FB_CUDA(cudaEventSynchronize(t1));
-        float ms = 0.f;
-        FB_CUDA(cudaEventElapsedTime(&ms, t0, t1));
-        if (ms < best_ms) {
-          best_ms = ms;
-          best_ratio = r;
+      int best_cap = gr.sub_cap;
+      for (int cap : kSubCaps) {  // points per subproblem x direct/tiled split
+        set_cap(gr, cap);
+        for (double r : {0.0, 0.0625, 0.25, 1.0, 4.0, 16.0, 1e30}) {
+          set_split(gr, r);
+          run_group(gr, x, g, e, s);  // warm-up
+          FB_CUDA(cudaEventRecord(t0, s));
+          for (int rep = 0; rep < 3; ++rep) run_group(gr, x, g, e, s);
+          FB_CUDA(cudaEventRecord(t1, s));
+          FB_CUDA(cudaEventSynchronize(t1));
+          float ms = 0.f;
+          FB_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+          if (ms < best_ms) {
+            best_ms = ms;
+            best_ratio = r;
+            best_cap = cap;
+          }
         }
       }
-      set_split(gr, best_ratio);
+      gr.ratio = best_ratio;
+      set_cap(gr, best_cap);
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
@@ -554,6 +564,15 @@ class NUwUEnsembleImpl final : public Ensemble {
     for (auto& gp : groups_) set_split(*gp, ratio);
   }
 
+  void set_subproblem_cap(int cap) override {
+    if (cap < kSubCaps[0] || cap > kMaxSub)
+      throw InvalidArgument("the subproblem size must lie in [" + std::to_string(kSubCaps[0]) + ", " +
+                            std::to_string(kMaxSub) + "]");
+    invalidate_graphs();
+    FB_CUDA(cudaDeviceSynchronize());  // no launch may still read the split tables
+    for (auto& gp : groups_) set_cap(*gp, cap);
+  }
+
   std::string describe() const override {
     std::string out = "NUwU ensemble precision=" + std::string(sizeof(T) == 4 ? "fp32" : "fp64") +
                       " patterns=" + std::to_string(P_) + " w=" + std::to_string(es_.w) +
@@ -563,7 +582,7 @@ class NUwUEnsembleImpl final : public Ensemble {
       for (char d : gp->direct) nd += d ? 1 : 0;
       out += " [modes/dim=" + std::to_string(gp->n) + " nf=" + std::to_string(gp->geom.nf[0]) +
              " patterns=" + std::to_string(gp->P) + " points=" + std::to_string(gp->NG) +
-             " direct=" + std::to_string(nd) +
+             " direct=" + std::to_string(nd) + " subproblem<=" + std::to_string(gp->sub_cap) +
              (gp->band ? " fft=band|kx|<=" + std::to_string(gp->Kx) + ",|ky|<=" + std::to_string(gp->Ky)
                        : std::string(" fft=cufft")) + "]";
     }
@@ -603,7 +622,8 @@ class NUwUEnsembleImpl final : public Ensemble {
         items.push_back(SortItem{pi.pt_base + j, pi.pt_base + std::min<int64_t>(pi.npts, j + kEnsSortChunk), l, 0});
       pi.n_items = int(items.size()) - pi.first_item;
       pi.sub_base = sub;
-      pi.max_sub = int(gr.nbins + ceil_div(pi.npts, kMaxSub));
+      pi.max_sub = int(gr.nbins + ceil_div(pi.npts, kSubCaps[0]));
+      pi.sub_cap = gr.sub_cap;
       pi.pid = p;
       std::vector<int> idx;
       std::vector<ModeCoef> cf;
@@ -769,6 +789,15 @@ class NUwUEnsembleImpl final : public Ensemble {
     }
   }
 
+  // Subproblems of at most cap points (bins cut into equal parts), then the
+  // split tables for them.
+  void set_cap(Group& gr, int cap) {
+    gr.sub_cap = cap;
+    for (PatInfo& pi : gr.pats_h) pi.sub_cap = cap;
+    FB_CUDA(cudaMemcpy(gr.pats.p, gr.pats_h.data(), sizeof(PatInfo) * gr.P, cudaMemcpyHostToDevice));
+    set_split(gr, gr.ratio);
+  }
+
   // Patterns whose tap work N w^2 is below ratio x (tile cells of all bins)
   // take the direct kernels.
   void set_split(Group& gr, double ratio) {
@@ -783,8 +812,9 @@ class NUwUEnsembleImpl final : public Ensemble {
       if (d) {
         for (int s = 0; s < pi.npts; s += kDirectPts)
           pit.push_back(PointItem{pi.rec_base + s, std::min(kDirectPts, pi.npts - s), l, 0});
-      } else {
-        for (int s = 0; s < pi.max_sub; ++s) tab.push_back(make_int2(l, s));
+      } else {  // slots for this cap's subproblems
+        const int slots = int(std::min<int64_t>(pi.max_sub, gr.nbins + ceil_div(pi.npts, gr.sub_cap)));
+        for (int s = 0; s < slots; ++s) tab.push_back(make_int2(l, s));
       }
     }
     gr.n_tab = int(tab.size());

@@ -54,6 +54,11 @@ class Ensemble {
   // tiled, a huge ratio: all direct).
   virtual void set_split(double ratio) = 0;
 
+  // Sets by hand the largest subproblem (points per tile block; bins are cut
+  // into equal parts of at most that many): kMaxSub / 4 .. kMaxSub.  tune()
+  // picks it per group together with the split.
+  virtual void set_subproblem_cap(int cap) { (void)cap; }
+
   virtual std::string describe() const = 0;
 
   // Changes whenever the launch configuration changes (tune()), so that

@@ -152,6 +152,11 @@ class NUwUEnsemble:
         their bins use the direct kernels (0: all tiled; ``tune`` picks it)."""
         check(lib.fresco_ensemble_set_split(self._h, float(ratio)))
 
+    def set_subproblem_cap(self, cap):
+        """Largest subproblem of the tile kernels (points per block, 160..640); ``tune`` picks it
+        per group of equal grids together with the split."""
+        check(lib.fresco_ensemble_set_subproblem_cap(self._h, int(cap)))
+
     def status(self):
         """Per-pattern status bits raised since the last call (1: non-finite coordinate)."""
         st = np.zeros(self.n_patterns, dtype=np.int32)

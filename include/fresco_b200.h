@@ -375,6 +375,11 @@ int fresco_ensemble_tune(fresco_ensemble h, const double* x, int64_t n);
 /* Sets the split by hand: patterns whose tap work N w^2 is below ratio x the
  * tile cells of their bins use the direct kernels (0: all tiled). */
 int fresco_ensemble_set_split(fresco_ensemble h, double ratio);
+/* Sets the largest subproblem of the tile kernels (points per block; each
+ * bin is cut into equal parts of at most cap points), 160..640; tune picks it
+ * per group of equal grids together with the split.  No reference
+ * counterpart (FINUFFT's GPU spreader calls it maxsubprobsize). */
+int fresco_ensemble_set_subproblem_cap(fresco_ensemble h, int cap);
 /* Per-pattern status bits since the last call (P ints). */
 int fresco_ensemble_status(fresco_ensemble h, int* status);
 int fresco_ensemble_describe(fresco_ensemble h, char* buf, int buf_len);

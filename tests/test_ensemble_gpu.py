@@ -33,10 +33,11 @@ def patterns(specs, L, seed=0):
 
 
 @pytest.mark.parametrize("precision,eps,tol", [("fp64", 1e-12, 1e-10), ("fp32", 1e-6, 2e-5)])
-@pytest.mark.parametrize("split", [0.0, 1e30, "tune"])
+@pytest.mark.parametrize("split", [0.0, 1e30, "tune", 160, 320])
 def test_ensemble_matches_single_patterns(precision, eps, tol, split):
     """Every pattern's energy and gradient equal the single-pattern NUwU (FP64 at eps 1e-12 as the
-    reference value), with all patterns tiled, all direct, and the tuned split."""
+    reference value), with all patterns tiled, all direct, the tuned split and subproblem size, and
+    all patterns tiled in subproblems of at most 160 or 320 points (an int split)."""
     from fresco_b200 import NUwU, NUwUEnsemble
 
     L = np.full(2, 2 * np.pi)
@@ -45,6 +46,11 @@ def test_ensemble_matches_single_patterns(precision, eps, tol, split):
     assert ens.describe().count("fft=band") == 2, ens.describe()
     if split == "tune":
         ens.tune(xs)
+        assert "subproblem<=" in ens.describe()
+    elif isinstance(split, int):
+        ens.set_split(0.0)
+        ens.set_subproblem_cap(split)
+        assert ens.describe().count(f"subproblem<={split}") == ens.describe().count("[")
     else:
         ens.set_split(split)
     e, g = ens.get_energies_gradient(xs)
@@ -95,6 +101,8 @@ def test_ensemble_device_buffers_and_layout_errors():
     torch.cuda.synchronize()
     assert rel(de.cpu().numpy(), e) < 1e-6
     assert rel(dg.cpu().numpy(), g) < 1e-5
+    with pytest.raises(ValueError):
+        ens.set_subproblem_cap(100)
     with pytest.raises(ValueError):
         ens.get_energies_gradient(np.zeros(ens.ndof + 2))
     with pytest.raises(ValueError):
