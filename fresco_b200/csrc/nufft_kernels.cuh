@@ -1398,19 +1398,53 @@ __global__ void __launch_bounds__(256) interp_kernel(const Rec<D, T>* __restrict
   }
 }
 
-// 3D interpolation: one block per subproblem stages its bin's tile (+ halo,
-// tile + w cells per dimension, origin tile origin - w/2) of one field at a
-// time in shared memory and one thread per point sums its w^3 taps from it
-// (instead of gathering them from L2).  As in the 2D kernel, every tap
-// address of a point is its footprint's first cell plus an offset common to
-// all points, so the block buckets its points by that cell modulo the lanes
-// one shared-memory wavefront serves (16 for FP32 complex cells) and lane c
-// of every group of 16 takes points of class c only: the reads of a group
-// fall on distinct banks.  With two fields, each point's sums of the first
-// are kept in shared memory for the second.
+// 3D interpolation: one block per subproblem stages its bin's tile (+ halo)
+// of one field at a time in shared memory and one thread per point sums its
+// w^3 taps from it (instead of gathering them from L2).  As in the 2D kernel,
+// every tap address of a point is its footprint's first cell plus an offset
+// common to all points, so the block buckets its points by that cell modulo
+// the lanes one shared-memory wavefront serves (16 for FP32 complex cells)
+// and lane c of every group of 16 takes points of class c only: the reads of
+// a group fall on distinct banks.  With two fields, each point's sums of the
+// first are kept in shared memory for the second.
+//
+// Tile layout: z, y, x with x fastest; x starts XO = pad + (pad & 1) cells
+// before the bin (so that the first float is a multiple of 4: the bin origin
+// is even) and the row holds TXP cells (tile + w rounded up to even, plus the
+// extra cell), y and z start pad cells before it.  A tile that needs no
+// periodic wrap arrives by one 4D tensor copy per field (x in floats, y, z,
+// field; issued for the first field before the block classifies its points,
+// so copy and classification overlap); edge tiles use plain loads.
+template <int W>
+struct Interp3D {
+  static constexpr int PAD = W / 2;
+  static constexpr int XO = PAD + (PAD & 1);
+  __host__ __device__ static constexpr int txp(int tile0) { return (tile0 + W + (PAD & 1) + 1) & ~1; }
+};
+
+// Per-launch data of the 3D tile kernel's tensor copies (a __grid_constant__
+// parameter, so the map's address is usable by the copy).
+struct Tile3Copy {
+  CUtensorMap tmap;   // the fields as (2 nf0 floats, nf1, nf2, nfields)
+  int has_tmap = 0;
+  int polls = 0;      // first bounded wait for a copy (mbarrier polls)
+  double* energy = nullptr;  // the evaluation's energy, made NaN if a copy never lands (may be null)
+};
+
 template <int W, typename T, int NF>
 __host__ __device__ constexpr size_t interp3d_extra_bytes() {
-  return (NF == 2 ? sizeof(cplx_t<T>) * kMaxSub : 0) + sizeof(uint16_t) * kMaxSub;
+  return 128 + (NF == 2 ? sizeof(cplx_t<T>) * kMaxSub : 0) + sizeof(uint16_t) * kMaxSub;
+}
+
+// 4D tensor copy global -> shared (x innermost, in elements of the map),
+// completing on `bar` with its byte count.
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, int x, int y, int z, int f,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(f), "r"(smem_addr(bar))
+      : "memory");
 }
 
 template <int W, typename T, int NF>
@@ -1418,11 +1452,13 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
     const Rec<3, T>* __restrict__ recs, const T* __restrict__ weights, T uniform, const int* __restrict__ sub_bin,
     const int* __restrict__ sub_start, const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g,
     const EsPoly<W, T> poly, const cplx_t<T>* __restrict__ fields, int mode, double* grad, double2* out2,
-    int accumulate, const int* __restrict__ status, const GradScale gs) {
-  constexpr int PAD = W / 2;
+    int accumulate, const int* __restrict__ status, const GradScale gs, const __grid_constant__ Tile3Copy cp) {
+  using IP = Interp3D<W>;
+  constexpr int PAD = IP::PAD, XO = IP::XO;
   constexpr int PPT = (kMaxSub + 255) / 256;
   constexpr int G = 128 / int(sizeof(cplx_t<T>));  // lanes per wavefront = bank classes
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t tile_bar;
   __shared__ int cls_count[G], cls_start[G];
   const int sub = blockIdx.x;
   if (sub >= *num_sub) return;
@@ -1430,17 +1466,25 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
   const int bx = bin % g.nb[0], rb = bin / g.nb[0];
   const int by = rb % g.nb[1], bz = rb / g.nb[1];
   const int org0 = bx * g.tile[0], org1 = by * g.tile[1], org2 = bz * g.tile[2];
-  const int TX = g.tile[0] + W, TY = g.tile[1] + W, TZ = g.tile[2] + W;
+  const int TX = IP::txp(g.tile[0]), TY = g.tile[1] + W, TZ = g.tile[2] + W;
   const int ncell = TX * TY * TZ;
-  cplx_t<T>* tile = reinterpret_cast<cplx_t<T>*>(smem_raw);
+  cplx_t<T>* tile = reinterpret_cast<cplx_t<T>*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
   cplx_t<T>* first = tile + ncell;  // NF == 2: each point's sums of the first field
   uint16_t* order = reinterpret_cast<uint16_t*>(first + (NF == 2 ? kMaxSub : 0));  // points grouped by class
   const bool bad = status != nullptr && ((*status) & STATUS_NONFINITE_INPUT);
   const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
   const int tid = threadIdx.x;
-  // class and rank in class of this thread's points (p = tid + 256 k)
+  const bool use_tma = cp.has_tmap && org0 >= XO && org0 - XO + TX <= nf0 && org1 >= PAD &&
+                       org1 - PAD + TY <= nf1 && org2 >= PAD && org2 - PAD + TZ <= nf2;
+  const unsigned tile_bytes = unsigned(sizeof(cplx_t<T>)) * unsigned(ncell);
   if (tid < G) cls_count[tid] = 0;
+  if (use_tma && tid == 0) mbar_init(&tile_bar, 1);
   __syncthreads();
+  if (use_tma && tid == 0) {
+    mbar_expect_tx(&tile_bar, tile_bytes);
+    tma_load_4d(tile, &cp.tmap, 2 * (org0 - XO), org1 - PAD, org2 - PAD, 0, &tile_bar);
+  }
+  // class and rank in class of this thread's points (p = tid + 256 k)
   int code[PPT];
 #pragma unroll
   for (int k = 0; k < PPT; ++k) {
@@ -1451,7 +1495,7 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
     int c0, c1, c2;
     unpack_cell(3, r.cell, c0, c1, c2);
     T u;
-    const int l0 = c0 - org0 + es_start<W, T>(r.f[0], u) + PAD;
+    const int l0 = c0 - org0 + es_start<W, T>(r.f[0], u) + XO;
     const int l1 = c1 - org1 + es_start<W, T>(r.f[1], u) + PAD;
     const int l2 = c2 - org2 + es_start<W, T>(r.f[2], u) + PAD;
     const int cls = ((l2 * TY + l1) * TX + l0) & (G - 1);
@@ -1472,23 +1516,54 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
   const int cls = tid % G, grp = tid / G, ngrp = int(blockDim.x) / G;
   for (int f = 0; f < NF; ++f) {
     const cplx_t<T>* fld = fields + f * g.G();
-    __syncthreads();        // the order is complete; every thread is done with the previous field's tile
-    constexpr int BT = 4;  // loads in flight per thread
-    for (int i0 = tid; i0 < ncell; i0 += BT * 256) {
-      cplx_t<T> v[BT];
-#pragma unroll
-      for (int b = 0; b < BT; ++b) {
-        const int i = i0 + b * 256;
-        if (i < ncell) {
-          const int x = i % TX, r = i / TX;
-          const int y = r % TY, z = r / TY;
-          v[b] = fld[(int64_t(wrap_index(org2 - PAD + z, nf2)) * nf1 + wrap_index(org1 - PAD + y, nf1)) * nf0 +
-                     wrap_index(org0 - PAD + x, nf0)];
+    if (use_tma) {
+      if (f > 0) {
+        __syncthreads();  // every thread is done with the previous field's tile
+        if (tid == 0) {
+          // the tile's reads through the generic proxy come before the copy's writes
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_expect_tx(&tile_bar, tile_bytes);
+          tma_load_4d(tile, &cp.tmap, 2 * (org0 - XO), org1 - PAD, org2 - PAD, f, &tile_bar);
         }
       }
+      // bounded waits as in the 2D kernel: a retry raises STATUS_TILE_RETRY; a
+      // copy that never lands fails the evaluation (STATUS_TIMEOUT, NaN energy
+      // and NaN results for the block's points)
+      const unsigned parity = unsigned(f & 1);
+      const bool ok = mbar_wait_bounded(&tile_bar, parity, cp.polls);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0 && status != nullptr) raise_status(const_cast<int*>(status), STATUS_TILE_RETRY);
+        const bool ok2 = mbar_wait_timed(&tile_bar, parity, kTileWaitNs);
+        if (__syncthreads_or(!ok2)) {
+          const T nan = T(__longlong_as_double(0x7ff8000000000000ULL));
+          if (tid == 0) {
+            if (status != nullptr) raise_status(const_cast<int*>(status), STATUS_TIMEOUT);
+            if (cp.energy != nullptr) *cp.energy = double(nan);
+          }
+          for (int p = tid; p < cnt; p += blockDim.x)
+            interp_store<3, T>(mode, recs[start + p].idx, T(1), nan, nan, nan, true, grad, out2, accumulate, gs);
+          return;
+        }
+      }
+    } else {
+      __syncthreads();  // the order is complete; every thread is done with the previous field's tile
+      constexpr int BT = 4;  // loads in flight per thread
+      for (int i0 = tid; i0 < ncell; i0 += BT * 256) {
+        cplx_t<T> v[BT];
 #pragma unroll
-      for (int b = 0; b < BT; ++b)
-        if (i0 + b * 256 < ncell) tile[i0 + b * 256] = v[b];
+        for (int b = 0; b < BT; ++b) {
+          const int i = i0 + b * 256;
+          if (i < ncell) {
+            const int x = i % TX, r = i / TX;
+            const int y = r % TY, z = r / TY;
+            v[b] = fld[(int64_t(wrap_index(org2 - PAD + z, nf2)) * nf1 + wrap_index(org1 - PAD + y, nf1)) * nf0 +
+                       wrap_index(org0 - XO + x, nf0)];
+          }
+        }
+#pragma unroll
+        for (int b = 0; b < BT; ++b)
+          if (i0 + b * 256 < ncell) tile[i0 + b * 256] = v[b];
+      }
     }
     __syncthreads();
     const int n_c = cls_count[cls];
@@ -1499,7 +1574,7 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
       int c0, c1, c2;
       unpack_cell(3, r.cell, c0, c1, c2);
       T k0[W], k1[W], k2[W];
-      const int l0 = c0 - org0 + es_taps<W, T>(r.f[0], poly, k0) + PAD;
+      const int l0 = c0 - org0 + es_taps<W, T>(r.f[0], poly, k0) + XO;
       const int l1 = c1 - org1 + es_taps<W, T>(r.f[1], poly, k1) + PAD;
       const int l2 = c2 - org2 + es_taps<W, T>(r.f[2], poly, k2) + PAD;
       T vr = 0, vi = 0;
@@ -1723,28 +1798,72 @@ void launch_interp2d(const void* recs, const T* weights, T uniform, const SortBu
   FB_LAUNCH_CHECK();
 }
 
+// Tensor map of nfields complex fields of nf0 x nf1 x nf2 cells (x fastest)
+// as 4D floats (2 nf0, nf1, nf2, nfields) with a box of (box_x floats,
+// box_y, box_z, 1); 0 when the layout does not allow tensor copies.
+template <typename T>
+int encode_fields_tmap3(CUtensorMap* tm, const void* fields, int64_t nf0, int64_t nf1, int64_t nf2, int nfields,
+                        int box_x, int box_y, int box_z) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static const Encode encode = [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return Encode(nullptr);
+    }
+    return reinterpret_cast<Encode>(fn);
+  }();
+  const uint64_t row = uint64_t(nf0) * 2 * sizeof(T), plane = row * uint64_t(nf1), field = plane * uint64_t(nf2);
+  if (!encode || fields == nullptr || (reinterpret_cast<uintptr_t>(fields) & 15) || row % 16 || plane % 16 ||
+      field % 16 || box_x > 256 || box_y > 256 || box_z > 256 || (box_x * sizeof(T)) % 16 ||
+      box_x > 2 * nf0 || box_y > nf1 || box_z > nf2)
+    return 0;
+  const cuuint64_t dims[4] = {cuuint64_t(2 * nf0), cuuint64_t(nf1), cuuint64_t(nf2), cuuint64_t(nfields)};
+  const cuuint64_t strides[3] = {row, plane, field};
+  const cuuint32_t box[4] = {cuuint32_t(box_x), cuuint32_t(box_y), cuuint32_t(box_z), 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  const CUresult r = encode(tm, dt, 4, const_cast<void*>(fields), dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 1 : 0;
+}
+
 // 3D FP32: the tile kernel when a bin's tile + halo fits in shared memory
 // (false otherwise, and for FP64, whose w^3 loop needs 255 registers and one
 // block per SM in this form: the caller uses the gathering kernel).
 template <int W, typename T>
 bool launch_interp3d(const void* recs, const T* weights, T uniform, const SortBufs& sb, const Geom& g,
                      const std::vector<double>& poly, const cplx_t<T>* fields, int nfields, int mode, double* grad,
-                     double2* out2, int acc, const int* status, cudaStream_t s, const GradScale& gs) {
+                     double2* out2, int acc, const int* status, cudaStream_t s, const GradScale& gs,
+                     double* fail_energy) {
   if constexpr (sizeof(T) != 4) {
     return false;
   } else {
-    const size_t tile_bytes = size_t(g.tile[0] + W) * (g.tile[1] + W) * (g.tile[2] + W) * sizeof(cplx_t<T>);
+    using IP = Interp3D<W>;
+    const int TX = IP::txp(g.tile[0]), TY = g.tile[1] + W, TZ = g.tile[2] + W;
+    const size_t tile_bytes = size_t(TX) * TY * TZ * sizeof(cplx_t<T>);
     if (nfields < 1 || nfields > 2) return false;
     const size_t smem = tile_bytes + (nfields == 2 ? interp3d_extra_bytes<W, T, 2>() : interp3d_extra_bytes<W, T, 1>());
     if (smem > 160 * 1024) return false;
     auto kern2 = interp3d_tile_kernel<W, T, 2>;
     auto kern1 = interp3d_tile_kernel<W, T, 1>;
     auto kern = nfields == 2 ? kern2 : kern1;
-    if (smem > 48 * 1024)
-      ensure_dynamic_smem(kern, smem);
+    ensure_dynamic_smem(kern, smem);
+    Tile3Copy cp;
+    cp.has_tmap = g.tile[0] % 2 == 0 ? encode_fields_tmap3<T>(&cp.tmap, fields, g.nf[0], g.nf[1], g.nf[2], nfields,
+                                                               2 * TX, TY, TZ)
+                                     : 0;
+    cp.polls = tile_wait_polls_setting();
+    cp.energy = fail_energy;
     kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<3, T>*>(recs), weights, uniform, sb.sub_bin.p,
                                                  sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, g,
-                                                 make_es_poly<W, T>(poly), fields, mode, grad, out2, acc, status, gs);
+                                                 make_es_poly<W, T>(poly), fields, mode, grad, out2, acc, status, gs,
+                                                 cp);
     FB_LAUNCH_CHECK();
     return true;
   }
@@ -1858,7 +1977,7 @@ void interp(const void* recs, int64_t N, const T* weights, T uniform, const Sort
     if (N <= 0) return;
 #define FB_I3(WW)                                                                                              \
   if (!launch_interp3d<FB_WCLAMP(T, WW), T>(recs, weights, uniform, sb, g, poly, fields, nfields, mode, grad,     \
-                                            out2, accumulate, status, s, gs))                                     \
+                                            out2, accumulate, status, s, gs, fail_energy))                        \
     launch_interp_generic<3, FB_WCLAMP(T, WW), T>(recs, N, weights, uniform, g, poly, fields, nfields, mode, grad, \
                                                   out2, accumulate, status, s, gs)
     FB_FOR_W(T, FB_I3)

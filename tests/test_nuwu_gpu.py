@@ -216,6 +216,32 @@ def test_interp_tile_copy_second_wait(prec, eps, tol):
     assert after.status() == 0
 
 
+def test_interp3d_tile_copies_and_second_wait():
+    """3D FP32: interior tiles of both fields arrive by 4D tensor copies (the first while the block
+    classifies its points, the second after the first field's sums).  With the default first wait and
+    with a first wait of zero polls (status bit 8: every copy waited for a second time), the results
+    equal the oracle's; no timeout (bit 4) is raised."""
+    from fresco_b200 import NUwU
+    from fresco_b200._lib import check, lib
+
+    K, kmax = 16, 8  # 64^3 fine grid of 16 x 16 x 8 tiles: interior tiles take the copies
+    x, radii, Sk, V, L = _inputs(3, 4000, K, kmax, seed=22, radii_spread=False)
+    e_ref, g_ref = O.NUwU(radii, K, Sk, V, L).get_energy_gradient(x)
+    for polls in (-1, 0):
+        check(lib.fresco_debug_set_tile_wait_polls(polls))
+        try:
+            pot = NUwU(radii, K, Sk, V, L, eps=1e-6, precision="fp32")
+            results = [pot.get_energy_gradient(x) for _ in range(3)]  # direct launches, capture, replay
+            st = pot.status()
+        finally:
+            check(lib.fresco_debug_set_tile_wait_polls(-1))
+        assert not st & 4, st
+        assert bool(st & 8) == (polls == 0), st
+        for e1, g1 in results:
+            assert abs(e1 - e_ref) <= 1e-5 * abs(e_ref)
+            assert np.linalg.norm(g1 - g_ref) <= 1e-5 * np.linalg.norm(g_ref)
+
+
 def test_objects_of_different_sizes_interleave():
     """A kernel's shared-memory limit is shared by every object that launches it: a smaller object
     made later must not lower it under a larger one (one-pass sorts of 800K and 500K points, and the
