@@ -77,6 +77,26 @@ def test_nuwu_2d_band_transforms(prec, eps, tol, K, kmax, random_weights, band):
     _check(pot, ref, x, tol)
 
 
+@pytest.mark.parametrize("prec,eps,tol", PRECISIONS)
+def test_nuwu_2d_clustered_points_wide_weights(prec, eps, tol):
+    """Most points in one corner of the box, so their bins hold several subproblems (at most 640
+    points each) that add to the same fine-grid cells, with weights spanning about four decades
+    (radii 0.05..3): the FP32 spread accumulates each subproblem in fixed point scaled by its own
+    largest weight."""
+    from fresco_b200 import NUwU
+
+    N = 6000
+    x, _, Sk, V, L = _inputs(2, N, 64, 40, seed=31, random_weights=True)
+    rng = np.random.default_rng(31)
+    pts = rng.random((N, 2)) * np.asarray(L)[None, :]
+    pts[:4500] = pts[:4500] * 0.06  # 4500 points in a square of side 0.06 L: a few 64-cell bins
+    x = pts.ravel()
+    radii = 0.05 + 2.95 * rng.random(N) ** 3
+    ref = O.NUwU(radii, 64, Sk, V, L)
+    pot = NUwU(radii, 64, Sk, V, L, eps=eps, precision=prec)
+    _check(pot, ref, x, tol)
+
+
 @pytest.mark.parametrize("L", [1.0, 2 * np.pi, 3.7])
 def test_nuwu_box_map_quirk(L):
     """Points inside and outside the box under the reference's coordinate map (nuwu.hpp:216-250)."""
