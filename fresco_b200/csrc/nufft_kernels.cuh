@@ -840,77 +840,94 @@ __global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
   spread2d_flush<W, T, CPLX>(tile, wk, g, grid_real, grid_cplx);
 }
 
-// FP32 2D spreading of real weights (4 <= W <= 8) with fixed-point shared
-// accumulation.  One block per subproblem (at most kMaxSub points of one
-// 64 x 64-cell bin).  Staging: a thread per point turns its record into
-// (tile offset of the footprint, u0, u1, weight) in shared memory, and the
-// block takes its largest |weight|.  Accumulation: a warp takes two points per
-// round; lanes 0-15 form the taps of the first and lanes 16-31 those of the
-// second (lane hl < W: x tap hl times the scaled weight; W <= hl < 2W: y tap
-// hl - W).  Each point's w x w footprint is then two shared 32-bit integer
-// atomic instructions: lane (r = lane / 8, c = lane % 8) adds to column c of
-// footprint rows r and r + 4.  The tile pitch, 72 cells (8 mod 32), puts the
-// 4 x 8 cells of one instruction on 32 distinct banks.  Lanes outside the
-// footprint add zero to a cell that no other lane of the instruction touches
-// (column c < 8 of the padded row, or row r again), so the atomics need no
-// branch.  Fixed point: contributions are scaled by 2^21 over the power of
-// two above the block's largest |weight| and rounded to integers by one FMA
-// against 1.5 * 2^23 (round to nearest); a cell gets at most one contribution
-// per point (<= kMaxSub < 2^10), so its sum stays below 2^31 and is exact in
-// any order.  The flush adds sum / scale to the grid by float4 atomics (plain
-// float4 stores for the cells no other tile reaches, when the subproblem is its
-// bin's only one).  A non-finite weight makes the block add NaN to the grid.
-constexpr int kFixedPitch2D = 72;
+// FP32 2D spreading of real weights, thread per point (4 <= W <= 8), with
+// fixed-point shared accumulation: contributions are scaled by 2^21 over the
+// power of two above the block's largest |weight| and rounded to integers by
+// one FMA against 1.5 * 2^23 (round to nearest); a cell gets at most one
+// contribution per point (<= kMaxSub < 2^10), so its 32-bit sum stays below
+// 2^31 and is exact in any order, and an integer shared atomic add is one
+// instruction.  A non-finite weight makes the block add NaN to the grid.  One
+// block of 256 threads per subproblem.  Staging: each thread maps its points (at most
+// 3) to (tile offset of the footprint, u0, u1, weight) and ranks them by bank
+// class, the tile offset mod 32 (a footprint cell at (r, c) lies at offset
+// base + r P + c, so two points of different class never share a bank for the
+// same (r, c)); the points are stored in class order, laid out so that round k
+// of thread (warp w, lane l) reads the point at class-order position
+// (8 l + w) R + k (R = rounds, ceil(cnt / 256)): consecutive lanes take points
+// about a class apart, and each round's records are 32 consecutive entries.
+// Accumulation: the thread evaluates its W x taps (times the scaled weight) and
+// W y taps from the polynomial coefficients in the kernel parameters and adds
+// the W^2 cells with 32-bit integer shared atomics.  The tile columns are
+// shifted by LEFT so that the flush reads aligned groups of four cells with
+// one 16-byte load.
+template <int W>
+struct Tpp2D {
+  static constexpr int PAD = W / 2;
+  static constexpr int E = kTile2D + W;                  // tile rows and used columns
+  static constexpr int LEFT = (4 - PAD % 4) % 4;        // column shift: grid-aligned groups of four
+  static constexpr int P = (E + LEFT + 3) / 4 * 4;       // row pitch (cells)
+  static constexpr int NT = 256;
+  static constexpr int RMAX = (kMaxSub + NT - 1) / NT;  // rounds per thread at most
+};
 
 template <int W>
-__host__ __device__ constexpr size_t spread2d_fixed_smem_bytes() {
-  return sizeof(float4) * kMaxSub + sizeof(int) * size_t(kTile2D + W) * kFixedPitch2D;
+__host__ __device__ constexpr size_t spread2d_tpp_smem_bytes() {
+  using C = Tpp2D<W>;
+  return sizeof(float4) * C::RMAX * C::NT + sizeof(int) * size_t(C::E) * C::P;
 }
 
 template <int W>
-__global__ void __launch_bounds__(256, 6) spread2d_fixed_kernel(
+__global__ void __launch_bounds__(256) spread2d_tpp_kernel(
     const Rec<2, float>* __restrict__ recs, const float* __restrict__ weights, float uniform,
     const int* __restrict__ sub_bin, const int* __restrict__ sub_start, const int* __restrict__ sub_count,
     const int* __restrict__ num_sub, const int* __restrict__ bin_start, Geom g, const EsPoly<W, float> poly,
     float* __restrict__ grid_real) {
-  static_assert(W >= 4 && W <= 8, "one instruction covers 4 rows of at most 8 columns");
+  using C = Tpp2D<W>;
+  static_assert(W >= 4 && W <= 8, "kernel widths of the FP32 2D spread");
   static_assert(kMaxSub < 1024, "fixed-point sums of at most kMaxSub contributions below 2^21 fit 31 bits");
   constexpr int Q = EsPolyDeg<W>::Q;
-  constexpr int PAD = W / 2;
-  constexpr int P = kFixedPitch2D;
-  constexpr int E = kTile2D + W;  // tile rows; columns used: E, plus up to 8 - W zero-add columns
-  static_assert(P >= kTile2D + 8 && P % 32 == 8, "pitch: room for the zero-add columns, rows 8 banks apart");
+  constexpr int PAD = C::PAD, E = C::E, LEFT = C::LEFT, P = C::P, NT = C::NT, RMAX = C::RMAX;
   constexpr float kRound = 12582912.0f;   // 1.5 * 2^23: x + kRound holds round(x) in its low mantissa bits
   constexpr int kRoundBits = 0x4B400000;  // the bits of kRound
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float4* srec = reinterpret_cast<float4*>(smem_raw);  // (tile offset bits, u0, u1, weight)
-  int* itile = reinterpret_cast<int*>(srec + kMaxSub);
+  float4* srec = reinterpret_cast<float4*>(smem_raw);  // (tile offset bits, u0, u1, weight), round-major
+  int* itile = reinterpret_cast<int*>(srec + RMAX * NT);
+  __shared__ int cls_count[32], cls_start[32];
   __shared__ float s_red[8];
 
   const int sub = blockIdx.x;
   if (sub >= *num_sub) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  constexpr int NW = 8;
   const int bin = sub_bin[sub];
   const int start = sub_start[sub], cnt = sub_count[sub];
   const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
 
   {
     int4* t4 = reinterpret_cast<int4*>(itile);
-    for (int i = tid; i < E * P / 4; i += 256) t4[i] = make_int4(0, 0, 0, 0);
+    for (int i = tid; i < E * P / 4; i += NT) t4[i] = make_int4(0, 0, 0, 0);
   }
+  if (tid < 32) cls_count[tid] = 0;
+  __syncthreads();
+  float4 mine[RMAX];
+  int key[RMAX];  // class << 16 | rank in class, or -1
   float wm = 0.0f;  // largest |weight| of this thread's points, NaN if one is not finite
-  for (int p = tid; p < cnt; p += 256) {
+#pragma unroll
+  for (int k = 0; k < RMAX; ++k) {
+    key[k] = -1;
+    const int p = tid + k * NT;
+    if (p >= cnt) continue;
     const Rec<2, float> r = recs[start + p];
     int c0, c1, c2;
     unpack_cell(2, r.cell, c0, c1, c2);
     float u0, u1;
     const int s0 = es_start<W, float>(r.f[0], u0);
     const int s1 = es_start<W, float>(r.f[1], u1);
-    const int base = (c1 - org1 + s1 + PAD) * P + (c0 - org0 + s0 + PAD);
+    const int base = (c1 - org1 + s1 + PAD) * P + (c0 - org0 + s0 + PAD + LEFT);
     const float w = weights ? weights[r.idx] : uniform;
     wm = (isfinite(w) && !isnan(wm)) ? fmaxf(wm, fabsf(w)) : __int_as_float(0x7fc00000);
-    srec[p] = make_float4(__int_as_float(base), u0, u1, w);
+    mine[k] = make_float4(__int_as_float(base), u0, u1, w);
+    const int cls = base & 31;
+    key[k] = (cls << 16) | atomicAdd(&cls_count[cls], 1);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -918,10 +935,29 @@ __global__ void __launch_bounds__(256, 6) spread2d_fixed_kernel(
     wm = (isnan(wm) || isnan(t)) ? __int_as_float(0x7fc00000) : fmaxf(wm, t);
   }
   if (lane == 0) s_red[warp] = wm;
-  __syncthreads();  // also: the zeroed tile and the staged points
+  __syncthreads();
+  if (warp == 0) {  // exclusive scan of the class counts
+    const int v = cls_count[lane];
+    int inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    cls_start[lane] = inc - v;
+  }
+  __syncthreads();
+  const int R = (cnt + NT - 1) / NT;
+#pragma unroll
+  for (int k = 0; k < RMAX; ++k) {
+    if (key[k] < 0) continue;
+    const int q = cls_start[key[k] >> 16] + (key[k] & 0xffff);  // class-order position
+    const int s = q / R, kk = q - s * R;                          // thread slot s = 8 lane + warp, round kk
+    srec[kk * NT + (s & 7) * 32 + (s >> 3)] = mine[k];
+  }
   wm = 0.0f;
 #pragma unroll
-  for (int k = 0; k < NW; ++k) wm = (isnan(wm) || isnan(s_red[k])) ? __int_as_float(0x7fc00000) : fmaxf(wm, s_red[k]);
+  for (int k = 0; k < 8; ++k) wm = (isnan(wm) || isnan(s_red[k])) ? __int_as_float(0x7fc00000) : fmaxf(wm, s_red[k]);
   const bool bad_weight = isnan(wm);
   float scale = 1.0f, inv_scale = 1.0f;
   if (!bad_weight && wm > 0.0f) {
@@ -931,75 +967,47 @@ __global__ void __launch_bounds__(256, 6) spread2d_fixed_kernel(
     scale = ldexpf(1.0f, 21 - e);
     inv_scale = ldexpf(1.0f, e - 21);
   }
+  __syncthreads();
 
-  // tap roles: lane hl of each half evaluates x tap hl (hl < W) or y tap hl - W
-  const int half = lane >> 4, hl = lane & 15;
-  const bool xl = hl < W;
-  const int m = xl ? hl : (hl < 2 * W ? hl - W : 0);
-  float cf[Q + 1];
+  const int slot = lane * 8 + warp;
+  for (int kk = 0; kk < R; ++kk) {
+    if (slot * R + kk >= cnt) continue;
+    const float4 st = srec[kk * NT + warp * 32 + lane];
+    const float ws = st.w * scale;
+    float tx[W], ty[W];
 #pragma unroll
-  for (int d = 0; d <= Q; ++d) {
-    float v = 0.0f;
+    for (int m = 0; m < W; ++m) {
+      float a = poly.c[m][Q], b = poly.c[m][Q];
 #pragma unroll
-    for (int mm = 0; mm < W; ++mm)
-      if (mm == m) v = poly.c[mm][d];
-    cf[d] = v;
-  }
-  // cell roles
-  const int r_in = lane >> 3, c_in = lane & 7;
-  const bool col_ok = c_in < W, row1_ok = r_in + 4 < W;
-  const int lane_off = r_in * P + c_in;
-  const int row1_off = row1_ok ? 4 * P : 0;
-  const int kx_src = col_ok ? c_in : 0;
-  const int ky0_src = W + r_in;
-  const int ky1_src = W + (row1_ok ? r_in + 4 : 0);
-
-  for (int p0 = 2 * warp; p0 < cnt; p0 += 2 * NW) {
-    const int p = p0 + half < cnt ? p0 + half : p0;  // an odd last round: the second half repeats the first point
-    const float4 st = srec[p];
-    const float u = xl ? st.y : st.z;
-    float tap = cf[Q];
-#pragma unroll
-    for (int d = Q - 1; d >= 0; --d) tap = fmaf(tap, u, cf[d]);
-    if (xl) tap *= st.w * scale;
-    const int base = __float_as_int(st.x);
-    const int npts = min(2, cnt - p0);
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (h >= npts) break;  // warp-uniform
-      const int src = 16 * h;
-      const int bh = __shfl_sync(0xffffffffu, base, src);
-      const float kx = __shfl_sync(0xffffffffu, tap, src + kx_src);
-      const float ky0 = __shfl_sync(0xffffffffu, tap, src + ky0_src);
-      const float ky1 = __shfl_sync(0xffffffffu, tap, src + ky1_src);
-      const float kxe = col_ok ? kx : 0.0f;
-      const float ky1e = row1_ok ? ky1 : 0.0f;
-      int* c = itile + bh + lane_off;
-      atomicAdd(c, __float_as_int(fmaf(kxe, ky0, kRound)) - kRoundBits);
-      atomicAdd(c + row1_off, __float_as_int(fmaf(kxe, ky1e, kRound)) - kRoundBits);
+      for (int d = Q - 1; d >= 0; --d) {
+        a = fmaf(a, st.y, poly.c[m][d]);
+        b = fmaf(b, st.z, poly.c[m][d]);
+      }
+      tx[m] = a * ws;
+      ty[m] = b;
     }
+    int* cell = itile + __float_as_int(st.x);
+#pragma unroll
+    for (int r = 0; r < W; ++r)
+#pragma unroll
+      for (int c = 0; c < W; ++c) atomicAdd(cell + r * P + c, __float_as_int(fmaf(tx[c], ty[r], kRound)) - kRoundBits);
   }
   __syncthreads();
 
-  // flush: float4 groups aligned to the grid (nf0 % 4 == 0)
-  constexpr int LEFT = (4 - PAD % 4) % 4;  // cells left of the tile origin in the first group
-  constexpr int NG = (E + LEFT + 3) / 4;   // groups per tile row
+  // flush: aligned groups of four cells (grid x = org0 - PAD - LEFT + 4 j, nf0 % 4 == 0)
+  constexpr int NG = P / 4;
   const int nf0 = g.nf[0], nf1 = g.nf[1];
   const bool sole = cnt == bin_start[bin + 1] - bin_start[bin] && nf0 % kTile2D == 0 && nf1 % kTile2D == 0;
-  for (int i = tid; i < E * NG; i += 256) {
+  for (int i = tid; i < E * NG; i += NT) {
     const int ty = i / NG, j = i - ty * NG;
-    const int tc0 = j * 4 - LEFT;
-    float v[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int tc = tc0 + e;
-      v[e] = (tc >= 0 && tc < E) ? float(itile[ty * P + tc]) * inv_scale : 0.0f;
-    }
-    if (v[0] == 0.f && v[1] == 0.f && v[2] == 0.f && v[3] == 0.f) continue;
+    const int4 iv = *reinterpret_cast<const int4*>(itile + ty * P + 4 * j);
+    if ((iv.x | iv.y | iv.z | iv.w) == 0) continue;
+    const int tc0 = 4 * j - LEFT;
     const int gy = wrap_index(org1 - PAD + ty, nf1);
     const int gx = wrap_index(org0 - PAD + tc0, nf0);
     float4* dst = reinterpret_cast<float4*>(grid_real + int64_t(gy) * nf0 + gx);
-    const float4 val = make_float4(v[0], v[1], v[2], v[3]);
+    const float4 val = make_float4(float(iv.x) * inv_scale, float(iv.y) * inv_scale, float(iv.z) * inv_scale,
+                                   float(iv.w) * inv_scale);
     if (sole && ty >= W && ty < kTile2D && tc0 >= W && tc0 + 4 <= kTile2D) *dst = val;
     else atomicAdd(dst, val);
   }
@@ -1882,8 +1890,8 @@ void launch_spread2d(const void* recs, const T* weights, T uniform, const cplx_t
                      cudaStream_t s) {
   if constexpr (sizeof(T) == 4 && !CPLX && W >= 4 && W <= 8) {
     if (g.nf[0] % 4 == 0) {
-      constexpr size_t smem_f = spread2d_fixed_smem_bytes<W>();
-      auto kf = spread2d_fixed_kernel<W>;
+      constexpr size_t smem_f = spread2d_tpp_smem_bytes<W>();
+      auto kf = spread2d_tpp_kernel<W>;
       if (smem_f > 48 * 1024) ensure_dynamic_smem(kf, smem_f);
       kf<<<unsigned(sb.max_sub), 256, smem_f, s>>>(static_cast<const Rec<2, float>*>(recs), weights, uniform,
                                                    sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p,
