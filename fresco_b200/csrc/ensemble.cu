@@ -869,10 +869,21 @@ class NUwUEnsembleImpl final : public Ensemble {
     const EnsTileMap<T> map{gr.pats.p,     gr.tab.p,       gr.sub_bin.p, gr.sub_start.p, gr.sub_count.p,
                             gr.num_sub.p, gr.bin_start.p, cur_status_.p, gr.G};
     if (gr.n_tab) {
-      constexpr size_t ss = spread2d_smem_bytes<W, T, false>();
-      spread2d_tile_kernel<W, T, false, EnsTileMap<T>><<<gr.n_tab, Tile2D<W>::THREADS, ss, s>>>(
-          recs, weights_.p, nullptr, map, geo, poly, gr.spread.p, nullptr);
-      FB_LAUNCH_CHECK();
+      bool done = false;
+      if constexpr (sizeof(T) == 4 && W >= 4 && W <= 8) {
+        if (geo.nf[0] % 4 == 0) {  // thread per point, fixed-point shared atomics
+          spread2d_tpp_kernel<W, EnsTileMap<float>><<<gr.n_tab, Tpp2D<W>::NT, spread2d_tpp_smem_bytes<W>(), s>>>(
+              recs, weights_.p, map, geo, poly, gr.spread.p);
+          FB_LAUNCH_CHECK();
+          done = true;
+        }
+      }
+      if (!done) {
+        constexpr size_t ss = spread2d_smem_bytes<W, T, false>();
+        spread2d_tile_kernel<W, T, false, EnsTileMap<T>><<<gr.n_tab, Tile2D<W>::THREADS, ss, s>>>(
+            recs, weights_.p, nullptr, map, geo, poly, gr.spread.p, nullptr);
+        FB_LAUNCH_CHECK();
+      }
     }
     if (gr.n_pitems) {
       ens_spread_direct_kernel<W, T><<<gr.n_pitems, kDirectPts, 0, s>>>(recs, weights_.p, gr.pats.p, gr.pitems.p,

@@ -876,12 +876,10 @@ __host__ __device__ constexpr size_t spread2d_tpp_smem_bytes() {
   return sizeof(float4) * C::RMAX * C::NT + sizeof(int) * size_t(C::E) * C::P;
 }
 
-template <int W>
-__global__ void __launch_bounds__(256) spread2d_tpp_kernel(
-    const Rec<2, float>* __restrict__ recs, const float* __restrict__ weights, float uniform,
-    const int* __restrict__ sub_bin, const int* __restrict__ sub_start, const int* __restrict__ sub_count,
-    const int* __restrict__ num_sub, const int* __restrict__ bin_start, Geom g, const EsPoly<W, float> poly,
-    float* __restrict__ grid_real) {
+template <int W, typename Map>
+__global__ void __launch_bounds__(256) spread2d_tpp_kernel(const Rec<2, float>* __restrict__ recs,
+                                                           const float* __restrict__ weights, const Map map, Geom g,
+                                                           const EsPoly<W, float> poly, float* grid_real) {
   using C = Tpp2D<W>;
   static_assert(W >= 4 && W <= 8, "kernel widths of the FP32 2D spread");
   static_assert(kMaxSub < 1024, "fixed-point sums of at most kMaxSub contributions below 2^21 fit 31 bits");
@@ -895,12 +893,12 @@ __global__ void __launch_bounds__(256) spread2d_tpp_kernel(
   __shared__ int cls_count[32], cls_start[32];
   __shared__ float s_red[8];
 
-  const int sub = blockIdx.x;
-  if (sub >= *num_sub) return;
+  TileWork<float> wk;
+  if (!map.fetch(g, wk)) return;
+  grid_real += wk.grid_off;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int bin = sub_bin[sub];
-  const int start = sub_start[sub], cnt = sub_count[sub];
-  const int org0 = (bin % g.nb[0]) * kTile2D, org1 = (bin / g.nb[0]) * kTile2D;
+  const int start = wk.start, cnt = wk.cnt, org0 = wk.org0, org1 = wk.org1;
+  const float uniform = wk.uniform;
 
   {
     int4* t4 = reinterpret_cast<int4*>(itile);
@@ -997,7 +995,7 @@ __global__ void __launch_bounds__(256) spread2d_tpp_kernel(
   // flush: aligned groups of four cells (grid x = org0 - PAD - LEFT + 4 j, nf0 % 4 == 0)
   constexpr int NG = P / 4;
   const int nf0 = g.nf[0], nf1 = g.nf[1];
-  const bool sole = cnt == bin_start[bin + 1] - bin_start[bin] && nf0 % kTile2D == 0 && nf1 % kTile2D == 0;
+  const bool sole = cnt == wk.bin_range[1] - wk.bin_range[0] && nf0 % kTile2D == 0 && nf1 % kTile2D == 0;
   for (int i = tid; i < E * NG; i += NT) {
     const int ty = i / NG, j = i - ty * NG;
     const int4 iv = *reinterpret_cast<const int4*>(itile + ty * P + 4 * j);
@@ -1891,11 +1889,12 @@ void launch_spread2d(const void* recs, const T* weights, T uniform, const cplx_t
   if constexpr (sizeof(T) == 4 && !CPLX && W >= 4 && W <= 8) {
     if (g.nf[0] % 4 == 0) {
       constexpr size_t smem_f = spread2d_tpp_smem_bytes<W>();
-      auto kf = spread2d_tpp_kernel<W>;
+      auto kf = spread2d_tpp_kernel<W, TileMap1<float>>;
       if (smem_f > 48 * 1024) ensure_dynamic_smem(kf, smem_f);
-      kf<<<unsigned(sb.max_sub), 256, smem_f, s>>>(static_cast<const Rec<2, float>*>(recs), weights, uniform,
-                                                   sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p,
-                                                   sb.bin_start.p, g, make_es_poly<W, T>(poly), grid_real);
+      const TileMap1<float> map{sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p, sb.num_sub.p, sb.bin_start.p, nullptr,
+                                uniform};
+      kf<<<unsigned(sb.max_sub), 256, smem_f, s>>>(static_cast<const Rec<2, float>*>(recs), weights, map, g,
+                                                   make_es_poly<W, T>(poly), grid_real);
       FB_LAUNCH_CHECK();
       return;
     }
