@@ -830,6 +830,9 @@ def run_ours(args):
 
         m = re.search(r"commit ([0-9a-f]{7,40})", text)
         capture = m.group(1) if m else None
+        # a stage re-captured later is named in the header as "(<stage>: <kernel> at commit <sha>)"
+        m = re.search(r"\(" + top + r": \S+ at commit ([0-9a-f]{7,40})\)", text)
+        capture = m.group(1) if m else capture
     except (OSError, ValueError, IndexError):
         pass
     roofline = {"kernel": top, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
