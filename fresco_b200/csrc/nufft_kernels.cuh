@@ -1251,6 +1251,206 @@ __global__ void __launch_bounds__(256) spread3d_warp_kernel(const Rec<3, T>* __r
   }
 }
 
+// FP32 3D spreading of real weights, thread per point (W <= 8): the 2D
+// thread-per-point scheme (spread2d_tpp_kernel) on a tw0 x tw1 x tw2 tile.
+// Staging ranks the block's points by bank class (tile offset of the
+// footprint mod 32) and stores them round-major in class order; each thread
+// evaluates its 3W taps from the polynomial coefficients in the kernel
+// parameters (the weight folded into the x taps) and adds the W^3 cells with
+// 32-bit integer shared atomics (fixed point as in the 2D kernel).  Row
+// pitch px = tw0 + LEFT rounded up to four cells, LEFT chosen so that the
+// flush reads grid-aligned groups of four cells with one 16-byte load.
+template <int W>
+struct Tpp3D {
+  static constexpr int PAD = W / 2;
+  static constexpr int LEFT = (4 - PAD % 4) % 4;
+  static constexpr int NT = 256;
+  static constexpr int RMAX = (kMaxSub + NT - 1) / NT;
+};
+
+inline int spread3d_tpp_pitch(int tw0, int w) { return (tw0 + (4 - (w / 2) % 4) % 4 + 3) / 4 * 4; }
+
+template <int W>
+inline size_t spread3d_tpp_smem_bytes(const Geom& g) {
+  using C = Tpp3D<W>;
+  return (sizeof(float4) + sizeof(float)) * C::RMAX * C::NT +
+         sizeof(int) * size_t(spread3d_tpp_pitch(g.tw[0], W)) * g.tw[1] * g.tw[2];
+}
+
+template <int W>
+__global__ void __launch_bounds__(256) spread3d_tpp_kernel(const Rec<3, float>* __restrict__ recs,
+                                                           const float* __restrict__ weights, float uniform,
+                                                           const int* __restrict__ sub_bin,
+                                                           const int* __restrict__ sub_start,
+                                                           const int* __restrict__ sub_count,
+                                                           const int* __restrict__ num_sub,
+                                                           const int* __restrict__ bin_start, Geom g,
+                                                           const EsPoly<W, float> poly, int px,
+                                                           float* __restrict__ grid_real) {
+  using C = Tpp3D<W>;
+  static_assert(W <= 8, "kernel widths of the FP32 3D spread");
+  static_assert(kMaxSub < 1024, "fixed-point sums of at most kMaxSub contributions below 2^21 fit 31 bits");
+  constexpr int Q = EsPolyDeg<W>::Q;
+  constexpr int PAD = C::PAD, LEFT = C::LEFT, NT = C::NT, RMAX = C::RMAX;
+  constexpr float kRound = 12582912.0f;   // 1.5 * 2^23: x + kRound holds round(x) in its low mantissa bits
+  constexpr int kRoundBits = 0x4B400000;  // the bits of kRound
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* srec = reinterpret_cast<float4*>(smem_raw);  // (tile offset bits, u0, u1, u2), round-major
+  float* sw = reinterpret_cast<float*>(srec + RMAX * NT);
+  int* itile = reinterpret_cast<int*>(sw + RMAX * NT);
+  __shared__ int cls_count[32], cls_start[32];
+  __shared__ float s_red[8];
+
+  const int sub = blockIdx.x;
+  if (sub >= *num_sub) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int bin = sub_bin[sub];
+  const int start = sub_start[sub], cnt = sub_count[sub];
+  const int tw1 = g.tw[1], tw2 = g.tw[2];
+  const int plane = tw1 * px;
+  const int cells = plane * tw2;
+  const int bx = bin % g.nb[0];
+  const int brem = bin / g.nb[0];
+  const int by = brem % g.nb[1];
+  const int bz = brem / g.nb[1];
+  const int org0 = bx * g.tile[0], org1 = by * g.tile[1], org2 = bz * g.tile[2];
+
+  {
+    int4* t4 = reinterpret_cast<int4*>(itile);
+    for (int i = tid; i < cells / 4; i += NT) t4[i] = make_int4(0, 0, 0, 0);
+  }
+  if (tid < 32) cls_count[tid] = 0;
+  __syncthreads();
+  float4 mine[RMAX];
+  float mw[RMAX];
+  int key[RMAX];  // class << 16 | rank in class, or -1
+  float wm = 0.0f;
+#pragma unroll
+  for (int k = 0; k < RMAX; ++k) {
+    key[k] = -1;
+    const int p = tid + k * NT;
+    if (p >= cnt) continue;
+    const Rec<3, float> r = recs[start + p];
+    int c0, c1, c2;
+    unpack_cell(3, r.cell, c0, c1, c2);
+    float u0, u1, u2;
+    const int s0 = es_start<W, float>(r.f[0], u0);
+    const int s1 = es_start<W, float>(r.f[1], u1);
+    const int s2 = es_start<W, float>(r.f[2], u2);
+    const int base = ((c2 - org2 + s2 + PAD) * tw1 + (c1 - org1 + s1 + PAD)) * px + (c0 - org0 + s0 + PAD + LEFT);
+    const float w = weights ? weights[r.idx] : uniform;
+    wm = (isfinite(w) && !isnan(wm)) ? fmaxf(wm, fabsf(w)) : __int_as_float(0x7fc00000);
+    mine[k] = make_float4(__int_as_float(base), u0, u1, u2);
+    mw[k] = w;
+    const int cls = base & 31;
+    key[k] = (cls << 16) | atomicAdd(&cls_count[cls], 1);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float t = __shfl_xor_sync(0xffffffffu, wm, o);
+    wm = (isnan(wm) || isnan(t)) ? __int_as_float(0x7fc00000) : fmaxf(wm, t);
+  }
+  if (lane == 0) s_red[warp] = wm;
+  __syncthreads();
+  if (warp == 0) {  // exclusive scan of the class counts
+    const int v = cls_count[lane];
+    int inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    cls_start[lane] = inc - v;
+  }
+  __syncthreads();
+  const int R = (cnt + NT - 1) / NT;
+#pragma unroll
+  for (int k = 0; k < RMAX; ++k) {
+    if (key[k] < 0) continue;
+    const int q = cls_start[key[k] >> 16] + (key[k] & 0xffff);  // class-order position
+    const int s = q / R, kk = q - s * R;                          // thread slot s = 8 lane + warp, round kk
+    const int at = kk * NT + (s & 7) * 32 + (s >> 3);
+    srec[at] = mine[k];
+    sw[at] = mw[k];
+  }
+  wm = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) wm = (isnan(wm) || isnan(s_red[k])) ? __int_as_float(0x7fc00000) : fmaxf(wm, s_red[k]);
+  const bool bad_weight = isnan(wm);
+  float scale = 1.0f, inv_scale = 1.0f;
+  if (!bad_weight && wm > 0.0f) {
+    int e = 0;
+    frexpf(wm, &e);  // wm < 2^e
+    e = max(-100, min(100, e));
+    scale = ldexpf(1.0f, 21 - e);
+    inv_scale = ldexpf(1.0f, e - 21);
+  }
+  __syncthreads();
+
+  const int slot = lane * 8 + warp;
+  for (int kk = 0; kk < R; ++kk) {
+    if (slot * R + kk >= cnt) continue;
+    const int at = kk * NT + warp * 32 + lane;
+    const float4 st = srec[at];
+    const float ws = sw[at] * scale;
+    float tx[W], ty[W], tz[W];
+#pragma unroll
+    for (int m = 0; m < W; ++m) {
+      float a = poly.c[m][Q], b = poly.c[m][Q], c = poly.c[m][Q];
+#pragma unroll
+      for (int d = Q - 1; d >= 0; --d) {
+        a = fmaf(a, st.y, poly.c[m][d]);
+        b = fmaf(b, st.z, poly.c[m][d]);
+        c = fmaf(c, st.w, poly.c[m][d]);
+      }
+      tx[m] = a * ws;
+      ty[m] = b;
+      tz[m] = c;
+    }
+    const int base = __float_as_int(st.x);
+#pragma unroll
+    for (int z = 0; z < W; ++z) {
+#pragma unroll
+      for (int y = 0; y < W; ++y) {
+        int* row = itile + base + z * plane + y * px;
+        const float yz = ty[y] * tz[z];
+#pragma unroll
+        for (int x = 0; x < W; ++x) atomicAdd(row + x, __float_as_int(fmaf(tx[x], yz, kRound)) - kRoundBits);
+      }
+    }
+  }
+  __syncthreads();
+
+  // flush: grid-aligned groups of four cells along x (nf0 % 4 == 0, tile[0] % 4 == 0)
+  const int o0 = org0 - PAD - LEFT, o1 = org1 - PAD, o2 = org2 - PAD;
+  const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
+  const int ng = px / 4;
+  const bool sole = cnt == bin_start[bin + 1] - bin_start[bin] && nf0 % g.tile[0] == 0 &&
+                    nf1 % g.tile[1] == 0 && nf2 % g.tile[2] == 0;
+  for (int i = tid; i < tw2 * tw1 * ng; i += NT) {
+    const int j = i % ng;
+    const int r = i / ng;
+    const int i1 = r % tw1;
+    const int i2 = r / tw1;
+    const int4 iv = *reinterpret_cast<const int4*>(itile + (i2 * tw1 + i1) * px + 4 * j);
+    if ((iv.x | iv.y | iv.z | iv.w) == 0) continue;
+    const int tc0 = 4 * j - LEFT;
+    const int64_t gi = (int64_t(wrap_index(o2 + i2, nf2)) * nf1 + wrap_index(o1 + i1, nf1)) * nf0 +
+                       wrap_index(o0 + 4 * j, nf0);
+    float4* dst = reinterpret_cast<float4*>(grid_real + gi);
+    const float4 val = make_float4(float(iv.x) * inv_scale, float(iv.y) * inv_scale, float(iv.z) * inv_scale,
+                                   float(iv.w) * inv_scale);
+    if (sole && i1 >= W && i1 < g.tile[1] && i2 >= W && i2 < g.tile[2] && tc0 >= W && tc0 + 4 <= g.tile[0])
+      *dst = val;
+    else
+      atomicAdd(dst, val);
+  }
+  if (bad_weight && tid == 0) {
+    const int64_t gi = (int64_t(wrap_index(org2, nf2)) * nf1 + wrap_index(org1, nf1)) * nf0 + wrap_index(org0, nf0);
+    atomicAdd(grid_real + gi, __int_as_float(0x7fc00000));
+  }
+}
+
 // Row pitch of spread3d_warp_kernel's tile: a multiple of 8, not of 16, with
 // room for the 8 - w columns past a footprint row that the lanes outside the
 // footprint touch (>= tw0 + 8 - w).
@@ -1912,6 +2112,18 @@ template <int D, int W, typename T, bool CPLX>
 void launch_spread_generic(const void* recs, const T* weights, T uniform, const cplx_t<T>* strengths,
                            const SortBufs& sb, const Geom& g, const std::vector<double>& poly, T* grid_real,
                            cplx_t<T>* grid_cplx, cudaStream_t s) {
+  if constexpr (D == 3 && W <= 8 && !CPLX && sizeof(T) == 4) {
+    const size_t smem_t = spread3d_tpp_smem_bytes<W>(g);
+    if (g.nf[0] % 4 == 0 && g.tile[0] % 4 == 0 && smem_t <= 200 * 1024) {
+      auto kt = spread3d_tpp_kernel<W>;
+      if (smem_t > 48 * 1024) ensure_dynamic_smem(kt, smem_t);
+      kt<<<unsigned(sb.max_sub), Tpp3D<W>::NT, smem_t, s>>>(
+          static_cast<const Rec<3, float>*>(recs), weights, uniform, sb.sub_bin.p, sb.sub_start.p, sb.sub_count.p,
+          sb.num_sub.p, sb.bin_start.p, g, make_es_poly<W, T>(poly), spread3d_tpp_pitch(g.tw[0], W), grid_real);
+      FB_LAUNCH_CHECK();
+      return;
+    }
+  }
   if constexpr (D == 3 && W <= 8 && !CPLX) {
     const int pitch = spread3d_pitch(g.tw[0], W);
     const size_t smem3 = size_t(pitch) * g.tw[1] * g.tw[2] * sizeof(T);

@@ -97,6 +97,23 @@ def test_nuwu_2d_clustered_points_wide_weights(prec, eps, tol):
     _check(pot, ref, x, tol)
 
 
+@pytest.mark.parametrize("prec,eps,tol", PRECISIONS)
+def test_nuwu_3d_clustered_points_wide_weights(prec, eps, tol):
+    """The 3D form of the clustered test: 3000 of 4000 points in a corner cube of side 0.1 L (bins
+    split into several subproblems on a 32^3 fine grid of 16 x 16 x 8-cell tiles), radii 0.05..3."""
+    from fresco_b200 import NUwU
+
+    N = 4000
+    _, _, Sk, V, L = _inputs(3, N, 8, 6, seed=32, random_weights=True)
+    rng = np.random.default_rng(32)
+    pts = rng.random((N, 3)) * np.asarray(L)[None, :]
+    pts[:3000] = pts[:3000] * 0.1
+    radii = 0.05 + 2.95 * rng.random(N) ** 3
+    ref = O.NUwU(radii, 8, Sk, V, L)
+    pot = NUwU(radii, 8, Sk, V, L, eps=eps, precision=prec)
+    _check(pot, ref, pts.ravel(), tol)
+
+
 @pytest.mark.parametrize("L", [1.0, 2 * np.pi, 3.7])
 def test_nuwu_box_map_quirk(L):
     """Points inside and outside the box under the reference's coordinate map (nuwu.hpp:216-250)."""
