@@ -1713,7 +1713,9 @@ __global__ void __launch_bounds__(256) interp2d_tile_kernel(const Rec<2, T>* __r
 }
 
 // Generic interpolation (1D, 3D): thread per sorted point, taps gathered
-// directly from HBM/L2 (neighbouring threads share footprints).
+// directly from HBM/L2 (neighbouring threads share footprints).  With NF == 2
+// the second field is real: G values of T after the G complex cells of the
+// first (the 3D z field, whose type-2 transform is real).
 template <int D, int W, typename T, int NF>
 __global__ void __launch_bounds__(256) interp_kernel(const Rec<D, T>* __restrict__ recs, int64_t N,
                                                      const T* __restrict__ weights, T uniform, Geom g,
@@ -1735,7 +1737,8 @@ __global__ void __launch_bounds__(256) interp_kernel(const Rec<D, T>* __restrict
     int s1 = 0, s2 = 0;
     if (D >= 2) s1 = es_taps<W, T>(rec.f[D >= 2 ? 1 : 0], poly, k1);
     if (D >= 3) s2 = es_taps<W, T>(rec.f[D >= 3 ? 2 : 0], poly, k2);
-    T v0r = 0, v0i = 0, v1r = 0, v1i = 0;
+    T v0r = 0, v0i = 0, v1r = 0;
+    const T* __restrict__ real2 = reinterpret_cast<const T*>(fields + G);  // NF == 2: the real second field
     const int nz = (D == 3) ? W : 1;
     const int ny = (D >= 2) ? W : 1;
     for (int m2 = 0; m2 < nz; ++m2) {
@@ -1745,25 +1748,19 @@ __global__ void __launch_bounds__(256) interp_kernel(const Rec<D, T>* __restrict
       for (int m1 = 0; m1 < ny; ++m1) {
         const int iy = (D >= 2) ? wrap_index(c1 + s1 + m1, nf1) : 0;
         const T wy = (D >= 2) ? wz * k1[m1] : T(1);
-        const cplx_t<T>* rowp = fields + (int64_t(iz) * nf1 + iy) * nf0;
-        T rr = 0, ri = 0, qr = 0, qi = 0;
+        const int64_t row = (int64_t(iz) * nf1 + iy) * nf0;
+        const cplx_t<T>* rowp = fields + row;
+        T rr = 0, ri = 0, qr = 0;
 #pragma unroll
         for (int m0 = 0; m0 < W; ++m0) {
           const cplx_t<T> a = __ldg(rowp + ix[m0]);
           rr += a.x * k0[m0];
           ri += a.y * k0[m0];
-          if (NF == 2) {
-            const cplx_t<T> b = __ldg(rowp + G + ix[m0]);
-            qr += b.x * k0[m0];
-            qi += b.y * k0[m0];
-          }
+          if (NF == 2) qr += __ldg(real2 + row + ix[m0]) * k0[m0];
         }
         v0r += wy * rr;
         v0i += wy * ri;
-        if (NF == 2) {
-          v1r += wy * qr;
-          v1i += wy * qi;
-        }
+        if (NF == 2) v1r += wy * qr;
       }
     }
     const T wgt = (mode == INTERP_GRAD) ? (weights ? weights[rec.idx] : uniform) : T(1);
@@ -1788,25 +1785,44 @@ __global__ void __launch_bounds__(256) interp_kernel(const Rec<D, T>* __restrict
 // periodic wrap arrives by one 4D tensor copy per field (x in floats, y, z,
 // field; issued for the first field before the block classifies its points,
 // so copy and classification overlap); edge tiles use plain loads.
+//
+// With two fields (3D NUwU) the second is real (the z gradient field): its tile
+// holds T per cell, x starts XR = pad rounded up to a multiple of 4 cells before
+// the bin (16-byte aligned copies for FP32), rows of TXR cells (a multiple of
+// 4), copied by a 3D tensor map of the real grid; its pass regroups the points
+// by tile offset mod 32, so each warp's 4-byte reads fall on 32 banks.
 template <int W>
 struct Interp3D {
   static constexpr int PAD = W / 2;
   static constexpr int XO = PAD + (PAD & 1);
+  static constexpr int XR = (PAD + 3) & ~3;
   __host__ __device__ static constexpr int txp(int tile0) { return (tile0 + W + (PAD & 1) + 1) & ~1; }
+  __host__ __device__ static constexpr int txr(int tile0) { return (tile0 + W + (XR - PAD) + 3) & ~3; }
 };
 
 // Per-launch data of the 3D tile kernel's tensor copies (a __grid_constant__
 // parameter, so the map's address is usable by the copy).
 struct Tile3Copy {
-  CUtensorMap tmap;   // the fields as (2 nf0 floats, nf1, nf2, nfields)
+  CUtensorMap tmap;   // the complex field as (2 nf0 floats, nf1, nf2, 1)
+  CUtensorMap tmap2;  // the real second field as (nf0, nf1, nf2)
   int has_tmap = 0;
+  int has_tmap2 = 0;
   int polls = 0;      // first bounded wait for a copy (mbarrier polls)
   double* energy = nullptr;  // the evaluation's energy, made NaN if a copy never lands (may be null)
 };
 
 template <int W, typename T, int NF>
 __host__ __device__ constexpr size_t interp3d_extra_bytes() {
-  return 128 + (NF == 2 ? sizeof(cplx_t<T>) * kMaxSub : 0) + sizeof(uint16_t) * kMaxSub;
+  return 128 + (NF == 2 ? sizeof(cplx_t<T>) * kMaxSub : 0) + sizeof(uint16_t) * kMaxSub * (NF == 2 ? 2 : 1);
+}
+
+// 3D tensor copy global -> shared (x innermost), completing on `bar`.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+      : "memory");
 }
 
 // 4D tensor copy global -> shared (x innermost, in elements of the map),
@@ -1827,52 +1843,67 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
     const EsPoly<W, T> poly, const cplx_t<T>* __restrict__ fields, int mode, double* grad, double2* out2,
     int accumulate, const int* __restrict__ status, const GradScale gs, const __grid_constant__ Tile3Copy cp) {
   using IP = Interp3D<W>;
-  constexpr int PAD = IP::PAD, XO = IP::XO;
+  constexpr int PAD = IP::PAD, XO = IP::XO, XR = IP::XR;
   constexpr int PPT = (kMaxSub + 255) / 256;
-  constexpr int G = 128 / int(sizeof(cplx_t<T>));  // lanes per wavefront = bank classes
+  constexpr int G = 128 / int(sizeof(cplx_t<T>));  // lanes per wavefront = bank classes (complex cells)
+  constexpr int G2 = 32;                            // bank classes of the real field's 4-byte cells
   extern __shared__ unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t tile_bar;
-  __shared__ int cls_count[G], cls_start[G];
+  __shared__ int cls_count[G], cls_start[G], cls2_count[G2], cls2_start[G2];
   const int sub = blockIdx.x;
   if (sub >= *num_sub) return;
   const int bin = sub_bin[sub], start = sub_start[sub], cnt = sub_count[sub];
   const int bx = bin % g.nb[0], rb = bin / g.nb[0];
   const int by = rb % g.nb[1], bz = rb / g.nb[1];
   const int org0 = bx * g.tile[0], org1 = by * g.tile[1], org2 = bz * g.tile[2];
-  const int TX = IP::txp(g.tile[0]), TY = g.tile[1] + W, TZ = g.tile[2] + W;
-  const int ncell = TX * TY * TZ;
+  const int TX = IP::txp(g.tile[0]), TXR = IP::txr(g.tile[0]), TY = g.tile[1] + W, TZ = g.tile[2] + W;
+  const int ncell = TX * TY * TZ, ncell2 = TXR * TY * TZ;
   cplx_t<T>* tile = reinterpret_cast<cplx_t<T>*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
-  cplx_t<T>* first = tile + ncell;  // NF == 2: each point's sums of the first field
+  T* rtile = reinterpret_cast<T*>(tile);  // the real field's tile (same buffer, second pass)
+  const int tile_cells = (NF == 2 && ncell2 * int(sizeof(T)) > ncell * int(sizeof(cplx_t<T>)))
+                             ? (ncell2 * int(sizeof(T)) + int(sizeof(cplx_t<T>)) - 1) / int(sizeof(cplx_t<T>))
+                             : ncell;
+  cplx_t<T>* first = tile + tile_cells;  // NF == 2: each point's sums of the first field
   uint16_t* order = reinterpret_cast<uint16_t*>(first + (NF == 2 ? kMaxSub : 0));  // points grouped by class
+  uint16_t* order2 = order + kMaxSub;  // NF == 2: points grouped by real-tile class
   const bool bad = status != nullptr && ((*status) & STATUS_NONFINITE_INPUT);
   const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
   const int tid = threadIdx.x;
-  const bool use_tma = cp.has_tmap && org0 >= XO && org0 - XO + TX <= nf0 && org1 >= PAD &&
-                       org1 - PAD + TY <= nf1 && org2 >= PAD && org2 - PAD + TZ <= nf2;
+  const bool yz_in = org1 >= PAD && org1 - PAD + TY <= nf1 && org2 >= PAD && org2 - PAD + TZ <= nf2;
+  const bool use_tma = cp.has_tmap && org0 >= XO && org0 - XO + TX <= nf0 && yz_in;
+  const bool use_tma2 = NF == 2 && cp.has_tmap2 && org0 >= XR && org0 - XR + TXR <= nf0 && yz_in;
   const unsigned tile_bytes = unsigned(sizeof(cplx_t<T>)) * unsigned(ncell);
+  const unsigned tile2_bytes = unsigned(sizeof(T)) * unsigned(ncell2);
   if (tid < G) cls_count[tid] = 0;
-  if (use_tma && tid == 0) mbar_init(&tile_bar, 1);
+  if (tid < G2) cls2_count[tid] = 0;
+  if ((use_tma || use_tma2) && tid == 0) mbar_init(&tile_bar, 1);
   __syncthreads();
   if (use_tma && tid == 0) {
     mbar_expect_tx(&tile_bar, tile_bytes);
     tma_load_4d(tile, &cp.tmap, 2 * (org0 - XO), org1 - PAD, org2 - PAD, 0, &tile_bar);
   }
-  // class and rank in class of this thread's points (p = tid + 256 k)
-  int code[PPT];
+  // class and rank in class of this thread's points (p = tid + 256 k), for
+  // the complex tile and (NF == 2) the real one
+  int code[PPT], code2[PPT];
 #pragma unroll
   for (int k = 0; k < PPT; ++k) {
     const int p = tid + 256 * k;
     code[k] = -1;
+    code2[k] = -1;
     if (p >= cnt) continue;
     const Rec<3, T> r = recs[start + p];
     int c0, c1, c2;
     unpack_cell(3, r.cell, c0, c1, c2);
     T u;
-    const int l0 = c0 - org0 + es_start<W, T>(r.f[0], u) + XO;
+    const int b0 = c0 - org0 + es_start<W, T>(r.f[0], u);
     const int l1 = c1 - org1 + es_start<W, T>(r.f[1], u) + PAD;
     const int l2 = c2 - org2 + es_start<W, T>(r.f[2], u) + PAD;
-    const int cls = ((l2 * TY + l1) * TX + l0) & (G - 1);
+    const int cls = ((l2 * TY + l1) * TX + b0 + XO) & (G - 1);
     code[k] = (cls << 12) | atomicAdd(&cls_count[cls], 1);
+    if (NF == 2) {
+      const int c2r = ((l2 * TY + l1) * TXR + b0 + XR) & (G2 - 1);
+      code2[k] = (c2r << 12) | atomicAdd(&cls2_count[c2r], 1);
+    }
   }
   __syncthreads();
   if (tid == 0) {
@@ -1881,28 +1912,38 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
       cls_start[c] = acc;
       acc += cls_count[c];
     }
+  } else if (NF == 2 && tid == 32) {
+    int acc = 0;
+    for (int c = 0; c < G2; ++c) {
+      cls2_start[c] = acc;
+      acc += cls2_count[c];
+    }
   }
   __syncthreads();
 #pragma unroll
-  for (int k = 0; k < PPT; ++k)
+  for (int k = 0; k < PPT; ++k) {
     if (code[k] >= 0) order[cls_start[code[k] >> 12] + (code[k] & 0xfff)] = uint16_t(tid + 256 * k);
-  const int cls = tid % G, grp = tid / G, ngrp = int(blockDim.x) / G;
+    if (NF == 2 && code2[k] >= 0) order2[cls2_start[code2[k] >> 12] + (code2[k] & 0xfff)] = uint16_t(tid + 256 * k);
+  }
+  int tma_phase = 0;  // tensor copies completed on tile_bar
   for (int f = 0; f < NF; ++f) {
-    const cplx_t<T>* fld = fields + f * g.G();
-    if (use_tma) {
+    const bool real_pass = NF == 2 && f == 1;
+    const bool tma_f = real_pass ? use_tma2 : use_tma;
+    if (tma_f) {
       if (f > 0) {
         __syncthreads();  // every thread is done with the previous field's tile
         if (tid == 0) {
           // the tile's reads through the generic proxy come before the copy's writes
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          mbar_expect_tx(&tile_bar, tile_bytes);
-          tma_load_4d(tile, &cp.tmap, 2 * (org0 - XO), org1 - PAD, org2 - PAD, f, &tile_bar);
+          mbar_expect_tx(&tile_bar, tile2_bytes);
+          tma_load_3d(rtile, &cp.tmap2, org0 - XR, org1 - PAD, org2 - PAD, &tile_bar);
         }
       }
       // bounded waits as in the 2D kernel: a retry raises STATUS_TILE_RETRY; a
       // copy that never lands fails the evaluation (STATUS_TIMEOUT, NaN energy
       // and NaN results for the block's points)
-      const unsigned parity = unsigned(f & 1);
+      const unsigned parity = unsigned(tma_phase & 1);
+      ++tma_phase;
       const bool ok = mbar_wait_bounded(&tile_bar, parity, cp.polls);
       if (__syncthreads_or(!ok)) {
         if (tid == 0 && status != nullptr) raise_status(const_cast<int*>(status), STATUS_TILE_RETRY);
@@ -1918,8 +1959,29 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
           return;
         }
       }
+    } else if (real_pass) {
+      __syncthreads();  // every thread is done with the first field's tile
+      const T* fld = reinterpret_cast<const T*>(fields + g.G());
+      constexpr int BT = 4;  // loads in flight per thread
+      for (int i0 = tid; i0 < ncell2; i0 += BT * 256) {
+        T v[BT];
+#pragma unroll
+        for (int b = 0; b < BT; ++b) {
+          const int i = i0 + b * 256;
+          if (i < ncell2) {
+            const int x = i % TXR, r = i / TXR;
+            const int y = r % TY, z = r / TY;
+            v[b] = fld[(int64_t(wrap_index(org2 - PAD + z, nf2)) * nf1 + wrap_index(org1 - PAD + y, nf1)) * nf0 +
+                       wrap_index(org0 - XR + x, nf0)];
+          }
+        }
+#pragma unroll
+        for (int b = 0; b < BT; ++b)
+          if (i0 + b * 256 < ncell2) rtile[i0 + b * 256] = v[b];
+      }
     } else {
-      __syncthreads();  // the order is complete; every thread is done with the previous field's tile
+      __syncthreads();  // the order is complete
+      const cplx_t<T>* fld = fields;
       constexpr int BT = 4;  // loads in flight per thread
       for (int i0 = tid; i0 < ncell; i0 += BT * 256) {
         cplx_t<T> v[BT];
@@ -1939,6 +2001,40 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
       }
     }
     __syncthreads();
+    if (real_pass) {
+      // the real field: lane c of every warp takes points of class c (mod 32)
+      const int cls = tid % G2, grp = tid / G2, ngrp = int(blockDim.x) / G2;
+      const int n_c = cls2_count[cls];
+      const uint16_t* mine = order2 + cls2_start[cls];
+      for (int j = grp; j < n_c; j += ngrp) {
+        const int p = mine[j];
+        const Rec<3, T> r = recs[start + p];
+        int c0, c1, c2;
+        unpack_cell(3, r.cell, c0, c1, c2);
+        T k0[W], k1[W], k2[W];
+        const int l0 = c0 - org0 + es_taps<W, T>(r.f[0], poly, k0) + XR;
+        const int l1 = c1 - org1 + es_taps<W, T>(r.f[1], poly, k1) + PAD;
+        const int l2 = c2 - org2 + es_taps<W, T>(r.f[2], poly, k2) + PAD;
+        T vr = 0;
+        for (int m2 = 0; m2 < W; ++m2) {
+          T pr = 0;
+#pragma unroll
+          for (int m1 = 0; m1 < W; ++m1) {
+            const T* rowp = rtile + (l2 + m2) * TY * TXR + (l1 + m1) * TXR + l0;
+            T rr = 0;
+#pragma unroll
+            for (int m0 = 0; m0 < W; ++m0) rr += rowp[m0] * k0[m0];
+            pr += k1[m1] * rr;
+          }
+          vr += k2[m2] * pr;
+        }
+        const T wgt = (mode == INTERP_GRAD) ? (weights ? weights[r.idx] : uniform) : T(1);
+        const cplx_t<T> s0 = first[p];
+        interp_store<3, T>(mode, r.idx, wgt, s0.x, s0.y, vr, bad, grad, out2, accumulate, gs);
+      }
+      continue;
+    }
+    const int cls = tid % G, grp = tid / G, ngrp = int(blockDim.x) / G;
     const int n_c = cls_count[cls];
     const uint16_t* mine = order + cls_start[cls];
     for (int j = grp; j < n_c; j += ngrp) {
@@ -1969,19 +2065,14 @@ __global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
         vr += k2[m2] * pr;
         vi += k2[m2] * pi;
       }
-      if (NF == 2 && f == 0) {
+      if (NF == 2) {
         cplx_t<T> s0;
         s0.x = vr;
         s0.y = vi;
-        first[p] = s0;  // read back by this same thread for the second field
+        first[p] = s0;  // read back in the real field's pass
       } else {
         const T wgt = (mode == INTERP_GRAD) ? (weights ? weights[r.idx] : uniform) : T(1);
-        if (NF == 2) {
-          const cplx_t<T> s0 = first[p];
-          interp_store<3, T>(mode, r.idx, wgt, s0.x, s0.y, vr, bad, grad, out2, accumulate, gs);
-        } else {
-          interp_store<3, T>(mode, r.idx, wgt, vr, vi, T(0), bad, grad, out2, accumulate, gs);
-        }
+        interp_store<3, T>(mode, r.idx, wgt, vr, vi, T(0), bad, grad, out2, accumulate, gs);
       }
     }
   }
@@ -2231,6 +2322,40 @@ int encode_fields_tmap3(CUtensorMap* tm, const void* fields, int64_t nf0, int64_
   return r == CUDA_SUCCESS ? 1 : 0;
 }
 
+// Tensor map of a real grid of nf0 x nf1 x nf2 values of T (x fastest) with a
+// box of (box_x, box_y, box_z); 0 when the layout does not allow tensor copies.
+template <typename T>
+int encode_real_tmap3(CUtensorMap* tm, const void* grid, int64_t nf0, int64_t nf1, int64_t nf2, int box_x, int box_y,
+                      int box_z) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static const Encode encode = [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return Encode(nullptr);
+    }
+    return reinterpret_cast<Encode>(fn);
+  }();
+  const uint64_t row = uint64_t(nf0) * sizeof(T), plane = row * uint64_t(nf1);
+  if (!encode || grid == nullptr || (reinterpret_cast<uintptr_t>(grid) & 15) || row % 16 || plane % 16 ||
+      box_x > 256 || box_y > 256 || box_z > 256 || (box_x * sizeof(T)) % 16 || box_x > nf0 || box_y > nf1 ||
+      box_z > nf2)
+    return 0;
+  const cuuint64_t dims[3] = {cuuint64_t(nf0), cuuint64_t(nf1), cuuint64_t(nf2)};
+  const cuuint64_t strides[2] = {row, plane};
+  const cuuint32_t box[3] = {cuuint32_t(box_x), cuuint32_t(box_y), cuuint32_t(box_z)};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  const CUresult r = encode(tm, dt, 3, const_cast<void*>(grid), dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 1 : 0;
+}
+
 // 3D FP32: the tile kernel when a bin's tile + halo fits in shared memory
 // (false otherwise, and for FP64, whose w^3 loop needs 255 registers and one
 // block per SM in this form: the caller uses the gathering kernel).
@@ -2243,8 +2368,11 @@ bool launch_interp3d(const void* recs, const T* weights, T uniform, const SortBu
     return false;
   } else {
     using IP = Interp3D<W>;
-    const int TX = IP::txp(g.tile[0]), TY = g.tile[1] + W, TZ = g.tile[2] + W;
-    const size_t tile_bytes = size_t(TX) * TY * TZ * sizeof(cplx_t<T>);
+    const int TX = IP::txp(g.tile[0]), TXR = IP::txr(g.tile[0]), TY = g.tile[1] + W, TZ = g.tile[2] + W;
+    size_t tile_bytes = size_t(TX) * TY * TZ * sizeof(cplx_t<T>);
+    if (nfields == 2)  // the real field's tile shares the buffer (the kernel's tile_cells)
+      tile_bytes = std::max(tile_bytes, (size_t(TXR) * TY * TZ * sizeof(T) + sizeof(cplx_t<T>) - 1) /
+                                            sizeof(cplx_t<T>) * sizeof(cplx_t<T>));
     if (nfields < 1 || nfields > 2) return false;
     const size_t smem = tile_bytes + (nfields == 2 ? interp3d_extra_bytes<W, T, 2>() : interp3d_extra_bytes<W, T, 1>());
     if (smem > 160 * 1024) return false;
@@ -2253,9 +2381,13 @@ bool launch_interp3d(const void* recs, const T* weights, T uniform, const SortBu
     auto kern = nfields == 2 ? kern2 : kern1;
     ensure_dynamic_smem(kern, smem);
     Tile3Copy cp;
-    cp.has_tmap = g.tile[0] % 2 == 0 ? encode_fields_tmap3<T>(&cp.tmap, fields, g.nf[0], g.nf[1], g.nf[2], nfields,
+    cp.has_tmap = g.tile[0] % 2 == 0 ? encode_fields_tmap3<T>(&cp.tmap, fields, g.nf[0], g.nf[1], g.nf[2], 1,
                                                                2 * TX, TY, TZ)
                                      : 0;
+    // the real field's copies start at x = org0 - XR: a multiple of 4 floats when the tile edge is
+    cp.has_tmap2 = (nfields == 2 && g.tile[0] % 4 == 0)
+                       ? encode_real_tmap3<T>(&cp.tmap2, fields + g.G(), g.nf[0], g.nf[1], g.nf[2], TXR, TY, TZ)
+                       : 0;
     cp.polls = tile_wait_polls_setting();
     cp.energy = fail_energy;
     kern<<<unsigned(sb.max_sub), 256, smem, s>>>(static_cast<const Rec<3, T>*>(recs), weights, uniform, sb.sub_bin.p,

@@ -152,8 +152,10 @@ class NUwUImpl final : public Potential, public NUwUShard {
     spread_grid_.alloc(G);
     bhat_.alloc(GH);
     nfields_ = (D == 3) ? 2 : 1;
-    hgrid_.alloc(G * nfields_);
-    ggrid_.alloc(G * nfields_);
+    // 3D: the x/y field (G cells), then the z field's half spectrum (GH cells);
+    // the type-2 output holds the complex x/y grid, then the real z grid
+    hgrid_.alloc(D == 3 ? G + GH : G);
+    ggrid_.alloc(D == 3 ? G + (G + 1) / 2 : G);
     FB_CUDA(cudaMemset(hgrid_.p, 0, hgrid_.bytes()));
 
     // correction factors per dimension, k = -K..K
@@ -203,13 +205,14 @@ class NUwUImpl final : public Potential, public NUwUShard {
       FB_CUDA(cudaMemset(tgrid_.p, 0, tgrid_.bytes()));
     } else {
       FB_CUFFT(cufftPlanMany(&plan_r2c_, D, dims, nullptr, 1, 0, nullptr, 1, 0, r2c, 1));
-      FB_CUFFT(cufftPlanMany(&plan_c2c_, D, dims, nullptr, 1, int(G), nullptr, 1, int(G), c2c, nfields_));
+      FB_CUFFT(cufftPlanMany(&plan_c2c_, D, dims, nullptr, 1, int(G), nullptr, 1, int(G), c2c, 1));
+      if (D == 3) FB_CUFFT(cufftPlanMany(&plan_c2r_, D, dims, nullptr, 1, 0, nullptr, 1, 0, f32 ? CUFFT_C2R : CUFFT_Z2D, 1));
     }
     FB_CUDA(cudaDeviceSynchronize());
   }
 
   ~NUwUImpl() override {
-    for (cufftHandle h : {plan_r2c_, plan_c2c_, plan_col1_, plan_col2a_, plan_col2b_})
+    for (cufftHandle h : {plan_r2c_, plan_c2c_, plan_c2r_, plan_col1_, plan_col2a_, plan_col2b_})
       if (h) cufftDestroy(h);
   }
 
@@ -243,6 +246,7 @@ class NUwUImpl final : public Potential, public NUwUShard {
   // acc: the gradient is added to g (e always receives this term's energy alone)
   void shard_finish(const double* rho, double* g, double* e, cudaStream_t s, bool acc) {
     FB_CUDA(cudaMemsetAsync(e, 0, sizeof(double), s));
+    if (g) clear_z_half(s);
     if (n_active_ > 0) {
       const int grid = int(std::min<int64_t>(ceil_div(n_active_, 256), int64_t(sm_count()) * 8));
       nuwu_modes_from_rho_kernel<D, T><<<grid, 256, 0, s>>>(
@@ -302,7 +306,7 @@ class NUwUImpl final : public Potential, public NUwUShard {
       if (kx_max_ > 0) exec_c2c(plan_col2b_, hgrid_.p + off, tgrid_.p + off, s);
       exec_c2c(plan_c2c_, tgrid_.p, ggrid_.p, s);
     } else {
-      exec_c2c(plan_c2c_, hgrid_.p, ggrid_.p, s);
+      exec_type2_fields(s);
     }
     GradScale gs;  // exact mode: x = (p - round(p/L)) 2 pi / L, so d/dp = (2 pi / L) d/dx
     if (grad_mode_ == 1)
@@ -360,6 +364,7 @@ class NUwUImpl final : public Potential, public NUwUShard {
     }
     if (pruned_) exec_c2c(plan_col1_, bhat_.p, bhat_.p, s);  // columns k_x = 0..kx_max, in place
     timer_mark("fft_type1", s);
+    if (g) clear_z_half(s);
     if (n_active_ > 0) {
       const int grid = int(std::min<int64_t>(ceil_div(n_active_, 256), int64_t(sm_count()) * 8));
       nuwu_modes_kernel<D, T><<<grid, 256, 0, s>>>(
@@ -382,7 +387,7 @@ class NUwUImpl final : public Potential, public NUwUShard {
       if (kx_max_ > 0) exec_c2c(plan_col2b_, hgrid_.p + off, tgrid_.p + off, s);
       exec_c2c(plan_c2c_, tgrid_.p, ggrid_.p, s);
     } else {
-      exec_c2c(plan_c2c_, hgrid_.p, ggrid_.p, s);
+      exec_type2_fields(s);
     }
     timer_mark("fft_type2", s);
     GradScale gs;  // exact mode: x = (p - round(p/L)) 2 pi / L, so d/dp = (2 pi / L) d/dx
@@ -484,6 +489,29 @@ class NUwUImpl final : public Potential, public NUwUShard {
   }
 
   // forward (sign -1) complex transform on stream s
+  // Type-2 transforms of the packed fields (not the pruned 2D passes): the x/y
+  // field C2C; in 3D the z field's half spectrum C2R into the real grid after
+  // the complex one.  A C2R transform overwrites its input, so the mode pass
+  // works on a half spectrum cleared by clear_z_half().
+  void exec_type2_fields(cudaStream_t s) {
+    exec_c2c(plan_c2c_, hgrid_.p, ggrid_.p, s);
+    if (D != 3) return;
+    const int64_t G = geom_.G();
+    FB_CUFFT(cufftSetStream(plan_c2r_, s));
+    if (sizeof(T) == 4) {
+      FB_CUFFT(cufftExecC2R(plan_c2r_, reinterpret_cast<cufftComplex*>(hgrid_.p + G),
+                            reinterpret_cast<cufftReal*>(ggrid_.p + G)));
+    } else {
+      FB_CUFFT(cufftExecZ2D(plan_c2r_, reinterpret_cast<cufftDoubleComplex*>(hgrid_.p + G),
+                            reinterpret_cast<cufftDoubleReal*>(ggrid_.p + G)));
+    }
+  }
+  void clear_z_half(cudaStream_t s) {
+    if (D == 3)
+      FB_CUDA(cudaMemsetAsync(hgrid_.p + geom_.G(), 0,
+                              sizeof(cplx_t<T>) * size_t(nh0_) * geom_.nf[1] * geom_.nf[2], s));
+  }
+
   static void exec_c2c(cufftHandle plan, cplx_t<T>* in, cplx_t<T>* out, cudaStream_t s) {
     FB_CUFFT(cufftSetStream(plan, s));
     if (sizeof(T) == 4) {
@@ -521,7 +549,7 @@ class NUwUImpl final : public Potential, public NUwUShard {
   DevBuf<int> mode_idx_;
   DevBuf<ModeCoef> coef_;
   int n_active_ = 0;
-  cufftHandle plan_r2c_ = 0, plan_c2c_ = 0, plan_col1_ = 0, plan_col2a_ = 0, plan_col2b_ = 0;
+  cufftHandle plan_r2c_ = 0, plan_c2c_ = 0, plan_c2r_ = 0, plan_col1_ = 0, plan_col2a_ = 0, plan_col2b_ = 0;
   bool pruned_ = false;
   int kx_max_ = 0;
   bool band_ = false;

@@ -79,7 +79,7 @@ __device__ __forceinline__ double2 nuwu_mode_rho(int m, int n, int K, const cplx
 
 // The mode's phi term from rho(k) (undeconvolved): deconvolves it by
 // p(k) = prod corr_a(k_a) and, with want_grad, writes the packed field at k
-// (hgrid, second field at hgrid + G in 3D).
+// (hgrid; in 3D the z field's half spectrum k_x >= 0 follows at hgrid + G).
 template <int D, typename T>
 __device__ __forceinline__ double nuwu_mode_apply(int m, int n, int K, const ModeCoef& c, double2 rho, int nf0,
                                                   int nf1, int nf2, const double* __restrict__ corr0,
@@ -113,11 +113,14 @@ __device__ __forceinline__ double nuwu_mode_apply(int m, int n, int K, const Mod
       h.y = T(fi * ky - fr * kx);
     }
     hgrid[hi] = h;
-    if (D == 3) {
+    if (D == 3 && kx >= 0) {
+      // -i kz F^H is Hermitian, so its type-2 transform (exponent -i) is real:
+      // the C2R transform (exponent +i) of the conjugate, stored as the half
+      // spectrum k_x >= 0 (nf0 / 2 + 1 cells per row)
       cplx_t<T> h2;
       h2.x = T(fi * kz);
-      h2.y = T(-fr * kz);
-      hgrid[G + hi] = h2;
+      h2.y = T(fr * kz);
+      hgrid[G + x0 + int64_t(nf0 / 2 + 1) * (y0 + int64_t(nf1) * z0)] = h2;
     }
   }
   return c.w2 * dq * dq;
