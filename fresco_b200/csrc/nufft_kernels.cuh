@@ -1837,7 +1837,7 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, in
 }
 
 template <int W, typename T, int NF>
-__global__ void __launch_bounds__(256, 2) interp3d_tile_kernel(
+__global__ void __launch_bounds__(256, 3) interp3d_tile_kernel(
     const Rec<3, T>* __restrict__ recs, const T* __restrict__ weights, T uniform, const int* __restrict__ sub_bin,
     const int* __restrict__ sub_start, const int* __restrict__ sub_count, const int* __restrict__ num_sub, Geom g,
     const EsPoly<W, T> poly, const cplx_t<T>* __restrict__ fields, int mode, double* grad, double2* out2,
