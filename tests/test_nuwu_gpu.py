@@ -257,8 +257,9 @@ def test_interp_tile_copy_second_wait(prec, eps, tol):
 
 
 def test_interp3d_tile_copies_and_second_wait():
-    """3D FP32: interior tiles of both fields arrive by 4D tensor copies (the first while the block
-    classifies its points, the second after the first field's sums).  With the default first wait and
+    """3D FP32: interior tiles of both fields arrive by tensor copies (the complex x/y field by a 4D
+    copy while the block classifies its points, the real z field by a 3D copy after the first
+    field's sums).  With the default first wait and
     with a first wait of zero polls (status bit 8: every copy waited for a second time), the results
     equal the oracle's; no timeout (bit 4) is raised."""
     from fresco_b200 import NUwU
