@@ -304,3 +304,22 @@ def test_objects_of_different_sizes_interleave():
         for o in opts:
             o.one_iteration()
     assert all(np.isfinite(o.get_result().energy) for o in opts)
+
+
+@pytest.mark.parametrize("prec,eps,tol", PRECISIONS)
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_nuwu_rare_heavy_points(prec, eps, tol, ndim):
+    """A few points of radius ten times the others (weights about 10^4 (2D) or 10^6 (3D) times
+    larger) scattered among many light ones, so that most subproblems hold one heavy point: the
+    light points' contributions must not be quantised at the heavy point's scale."""
+    from fresco_b200 import NUwU
+
+    N, K, kmax = (20000, 64, 40) if ndim == 2 else (12000, 12, 8)
+    _, _, Sk, V, L = _inputs(ndim, N, K, kmax, seed=40 + ndim, random_weights=True)
+    rng = np.random.default_rng(40 + ndim)
+    x = (rng.random((N, ndim)) * np.asarray(L)[None, :]).ravel()
+    radii = np.full(N, 0.1)
+    radii[rng.choice(N, N // 500, replace=False)] = 1.0
+    ref = O.NUwU(radii, K, Sk, V, L)
+    pot = NUwU(radii, K, Sk, V, L, eps=eps, precision=prec)
+    _check(pot, ref, x, tol)
