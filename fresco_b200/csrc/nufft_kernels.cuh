@@ -846,9 +846,10 @@ __global__ void __launch_bounds__(Tile2D<W>::THREADS) spread2d_tile_kernel(
 // one FMA against 1.5 * 2^23 (round to nearest); a cell gets at most one
 // contribution per point (<= kMaxSub < 2^10), so its 32-bit sum stays below
 // 2^31 and is exact in any order, and an integer shared atomic add is one
-// instruction.  A non-finite weight makes the block add NaN to the grid.  One
-// block of 256 threads per subproblem.  Staging: each thread maps its points (at most
-// 3) to (tile offset of the footprint, u0, u1, weight) and ranks them by bank
+// instruction.  A non-finite weight makes the block add NaN to the grid.
+// One block of 256 threads per subproblem (Map: block -> subproblem, as for
+// the phased kernel).  Staging: each thread maps its points (at most 3) to
+// (tile offset of the footprint, u0, u1, weight) and ranks them by bank
 // class, the tile offset mod 32 (a footprint cell at (r, c) lies at offset
 // base + r P + c, so two points of different class never share a bank for the
 // same (r, c)); the points are stored in class order, laid out so that round k
